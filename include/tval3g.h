@@ -1,0 +1,162 @@
+/*
+ * tval3g — TVAL3 total-variation reconstruction on one NVIDIA B200 (sm_100a).
+ *
+ * C ABI of the solver core (libtval3g.so).  Plain C types only; every pointer
+ * is a host pointer unless the function or flag says "device".  All entry
+ * points return TVAL3G_OK (0) or a negative status; tval3g_last_error()
+ * returns the calling thread's last message.
+ *
+ * The C++ drop-in overloads tval3_cpu_2d / tval3_cpu_3d (include/tval3_gpu_2d.h,
+ * include/tval3_gpu_3d.h) forward to tval3g_solve.  What each entry point
+ * replaces in modk/tval3-cpu:
+ *
+ *   tval3g_solve        the 15 + 15 overloads tval3_cpu_2d (2d/tval3_cpu_2d.cpp:16-95,
+ *                       889-1016) and tval3_cpu_3d (3d/tval3_cpu_3d.cpp:32-146,
+ *                       1384-1581) for float data, through the templated driver
+ *                       (2d/tval3_cpu_2d.cpp:752-886, 3d/tval3_cpu_3d.cpp:1172-1378)
+ *   tval3g_solve_batch  no reference counterpart: many independent solves in one
+ *                       batched launch sequence (each one as tval3g_solve)
+ *   tval3g_plan_*       no reference counterpart: the same solves with device-
+ *                       resident operators, data and state, reusable
+ *   tval3g_op_*         the measurement operator gemv(TransA, A, x, y) overloads
+ *                       (2d/mat_mult.h:15-194, 3d/mat_mult.h:17-595)
+ *   tval3g_D / _Dt      D / Dt (2d/tval3_cpu_2d.cpp:268-293, 3d/tval3_cpu_3d.cpp:365-425)
+ *   tval3g_shrink       shrinkage (2d/tval3_cpu_2d.cpp:588-611, 3d/tval3_cpu_3d.cpp:834-871)
+ */
+#ifndef TVAL3G_H_
+#define TVAL3G_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define TVAL3G_OK 0
+#define TVAL3G_ERR_ARGUMENT -1   /* the reference would throw "Argument error: ..." */
+#define TVAL3G_ERR_CUDA -2       /* a CUDA call failed (message says which) */
+#define TVAL3G_ERR_NO_DEVICE -3  /* no usable CUDA device / extension */
+#define TVAL3G_ERR_NONFINITE -4  /* a non-finite step length or objective stopped a solve */
+#define TVAL3G_ERR_INTERNAL -5
+
+/* measurement operator kinds (2d/mat_mult.h, 3d/mat_mult.h) */
+#define TVAL3G_OP_DENSE 0  /* mat<T>: row-major m x n */
+#define TVAL3G_OP_CSR 1    /* sparse_mat<T>: CSR, 0-based int32; the transpose is built on the device */
+#define TVAL3G_OP_RAY2D 2  /* 2D geometry: on-the-fly Bresenham rays */
+#define TVAL3G_OP_RAY3D 3  /* 3D geometry: on-the-fly Bresenham rays */
+
+/* total-variation norm */
+#define TVAL3G_TV_ANISO 0  /* the reference's (only) norm */
+#define TVAL3G_TV_ISO 1
+
+/* flags of tval3g_plan_create / tval3g_solve_batch */
+#define TVAL3G_DEVICE_INPUTS 1  /* A / CSR arrays of the problems are device pointers */
+#define TVAL3G_GRAPH 2          /* run the iteration loop as one CUDA graph with
+                                   conditional nodes (no host round trips) */
+
+/* Options; field meaning as tval3_options<T> (include/tval3/tval3_types.h). */
+typedef struct tval3g_options {
+	double mu, beta, mu0, beta0, tol, tol_inn, c, gamma, gam, rate_gam, rate_cnt;
+	double skipMulRatio, maxRelativeChange;
+	int maxit, maxcnt, nonneg, isreal, numInitIterations, tv_norm;
+} tval3g_options;
+
+/* Result of one solve; fields as tval3_info<T> plus a per-solve status. */
+typedef struct tval3g_info {
+	double secs;      /* wall seconds of the call (batch: of the whole batch) */
+	double rel_chg;   /* last outer relative change */
+	double rel_error; /* ||Ut - U|| / ||Ut|| when Ut was given, else 0 */
+	int outer_iters;
+	int total_iters;
+	int status;       /* TVAL3G_OK or TVAL3G_ERR_NONFINITE */
+	int reserved;
+} tval3g_info;
+
+/* One reconstruction problem.
+ * Image: dims = 2 (dim_z = 1) or 3; element i = x + y*dim_x + z*dim_x*dim_y.
+ * n = dim_y*dim_x*dim_z.
+ * DENSE / CSR: m = rows of A (A.dim_y), n_cols = columns (A.dim_x), layers =
+ *   the reference's "layers" (2d/tval3_cpu_2d.cpp:894: b.len / A.dim_y; 3D
+ *   always 1); valid when n == n_cols*layers and b_len == m*layers.
+ * RAY2D: b_len = num_emitters*num_receivers (uncompacted; 2d/tval3_cpu_2d.cpp:748).
+ * RAY3D: b_len = numPaths*numMPs (3d/tval3_cpu_3d.cpp:1153).
+ * Ray coordinate arrays are host pointers; emitters [numMPs*E], receivers
+ * [numMPs*R] (2D: numMPs = 1, z arrays unused). */
+typedef struct tval3g_problem {
+	int dims;
+	int dim_y, dim_x, dim_z;
+	int op_kind;
+	int m;                          /* DENSE / CSR: rows of A (A.dim_y) */
+	int n_cols;                     /* DENSE / CSR: columns of A (A.dim_x) */
+	int layers;
+	const float *A;                 /* DENSE */
+	long long nnz;                  /* CSR */
+	const int *csr_ptr;             /* [m+1] */
+	const int *csr_ind;             /* [nnz] column (pixel) indices */
+	const float *csr_val;           /* [nnz] */
+	int num_emitters, num_receivers;/* RAY2D / RAY3D */
+	int numMPs, numPaths;           /* RAY3D */
+	const int *use_path;            /* [E*R] */
+	const int *x_emitters, *y_emitters, *z_emitters;
+	const int *x_receivers, *y_receivers, *z_receivers;
+	int ld;                         /* RAY2D row stride of the image */
+	int rv_x, rv_y, rv_z;           /* RAY3D volume extent */
+	float scale_factor;             /* RAY2D / RAY3D weight of one hit */
+} tval3g_problem;
+
+const char *tval3g_last_error(void);
+int tval3g_version(void);
+
+/* One solve with host buffers (the drop-in path): U (n floats, output),
+ * b (b_len floats), Ut (ut_len floats: 0 or n; may be NULL). */
+int tval3g_solve(const tval3g_problem *prob, const float *b, int b_len, const tval3g_options *opts,
+                 const float *Ut, int ut_len, float *U, tval3g_info *info);
+
+/* count independent solves with host buffers, run as one batch (flags:
+ * TVAL3G_GRAPH).  Arrays are indexed by problem; Ut may be NULL. */
+int tval3g_solve_batch(int count, const tval3g_problem *probs, const float *const *b,
+                       const tval3g_options *opts, const float *const *Ut, float *const *U,
+                       tval3g_info *info, int flags);
+
+/* Plans: operators prepared once on the device (dense A copied or borrowed,
+ * CSR transpose built, ray index built), solver state allocated once.
+ * tval3g_plan_solve takes DEVICE pointers for b, Ut (may be NULL) and U and
+ * runs on `stream` (a cudaStream_t, or NULL for the plan's own stream); it
+ * returns after the solve finished and info was filled. */
+typedef struct tval3g_plan tval3g_plan;
+int tval3g_plan_create(tval3g_plan **plan, int count, const tval3g_problem *probs,
+                       const tval3g_options *opts, int flags);
+int tval3g_plan_solve(tval3g_plan *plan, const float *const *d_b, const float *const *d_Ut,
+                      float *const *d_U, tval3g_info *info, void *stream);
+/* Kernel launches issued by the last tval3g_plan_solve (graph mode: kernel
+ * nodes executed, counted on the device), and the plan's device bytes. */
+int tval3g_plan_stats(const tval3g_plan *plan, long long *kernel_launches, long long *device_bytes);
+int tval3g_plan_destroy(tval3g_plan *plan);
+
+/* Operators alone.  tval3g_op_apply: y = A x (trans = 0) or y = A^T x
+ * (trans = 1) with DEVICE x, y (lengths rows/cols as reported). */
+typedef struct tval3g_operator tval3g_operator;
+int tval3g_op_create(tval3g_operator **op, const tval3g_problem *prob, int flags);
+int tval3g_op_shape(const tval3g_operator *op, long long *rows, long long *cols, long long *nnz);
+int tval3g_op_apply(tval3g_operator *op, int trans, const float *d_x, float *d_y, void *stream);
+/* Ray operators: the device-built CSR (rows = b_len, untraced rows empty) of
+ * the Bresenham rasterisation, copied to HOST arrays rowptr [rows+1] and
+ * colind [nnz]; with colind == NULL only rowptr is written. */
+int tval3g_op_ray_csr(const tval3g_operator *op, long long *rowptr, int *colind);
+int tval3g_op_destroy(tval3g_operator *op);
+
+/* Stencils on DEVICE arrays of an image dim_y x dim_x (x dim_z for dims 3).
+ * Dt reproduces the reference's 3D adjoint exactly (including the extra y term
+ * on the first row of every slice z >= 1, 3d/tval3_cpu_3d.cpp:402-413). */
+int tval3g_D(int dims, int dim_y, int dim_x, int dim_z, const float *U, float *Ux, float *Uy,
+             float *Uz, void *stream);
+int tval3g_Dt(int dims, int dim_y, int dim_x, int dim_z, const float *X, const float *Y,
+              const float *Z, float *res, void *stream);
+/* W = shrink(U_c - sigma_c/beta); returns lambda1 in *lam1 (host). */
+int tval3g_shrink(int dims, long long n, int tv_norm, double beta, const float *Ux, const float *Uy,
+                  const float *Uz, const float *sx, const float *sy, const float *sz, float *Wx,
+                  float *Wy, float *Wz, double *lam1, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TVAL3G_H_ */

@@ -1,0 +1,98 @@
+"""C ABI checks that need no GPU: exports, argument errors, no-device error."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from helpers import ROOT
+from tval3g import capi, workloads as W
+
+
+def _declared(header):
+    src = open(os.path.join(ROOT, "include", header)).read()
+    return sorted(set(re.findall(r"\b(tval3g_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = capi.lib()
+    declared = _declared("tval3g.h")
+    assert "tval3g_solve" in declared and len(declared) >= 15
+    for name in declared:
+        assert hasattr(L, name), name
+    assert set(capi.EXPORTS) <= set(declared)
+
+
+def _opts():
+    return W.options(2 ** 8, 2 ** 5, 1e-4, 10, tv_norm=0)
+
+
+def _dense_spec(shape=(4, 4), m=5, ncols=16, layers=1):
+    A = np.zeros((m, ncols), np.float32)
+    return capi.dense_problem(shape, A, layers)
+
+
+@pytest.mark.parametrize("case,msg", [
+    ("ut", "Argument error: U and Ut must have the same size!"),
+    ("u", "Argument error: the length of U must be equal to A.dim_x * layers!"),
+    ("b", "Argument error: b.len must be equal to A.dim_y * layers!"),
+])
+def test_dense_argument_errors_match_reference(case, msg):
+    """Messages and check order of check_params (2d/tval3_cpu_2d.cpp:696-713)."""
+    spec = _dense_spec()
+    b = np.zeros(5, np.float32)
+    Ut = None
+    if case == "ut":
+        Ut = np.zeros(7, np.float32)
+    elif case == "u":
+        spec = _dense_spec(shape=(4, 5))
+    elif case == "b":
+        b = np.zeros(6, np.float32)
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve(spec, b, _opts(), Ut=Ut)
+    assert e.value.code == capi.ERR_ARGUMENT
+    assert str(e.value) == msg
+
+
+def test_ray_argument_errors():
+    g = W.ring_geometry(16, 16)
+    spec = capi.ray2d_problem((16, 16), g)
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve(spec, np.zeros(10, np.float32), _opts())
+    assert str(e.value) == "Argument error: b.len must be equal to A.num_emitters * A.num_receivers!"
+    g2 = dict(g)
+    g2["xr"] = g["xr"] + 100
+    spec = capi.ray2d_problem((16, 16), g2)
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve(spec, np.zeros(256, np.float32), _opts())
+    # the reference indexes out of bounds here; the C ABI refuses
+    assert e.value.code == capi.ERR_ARGUMENT
+    spec = capi.ray2d_problem((16, 16), g)
+    spec.p.layers = 2
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve(spec, np.zeros(256, np.float32), _opts())
+    assert str(e.value) == "Argument error: multilayer reconstruction with dynamic calculation is not supported!"
+
+
+def test_3d_argument_errors():
+    spec = capi.dense_problem((2, 2, 2), np.zeros((3, 8), np.float32))
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve(spec, np.zeros(4, np.float32), _opts())
+    assert str(e.value) == "Argument error: b.len must be equal to A.dim_y!"
+    spec = capi.dense_problem((2, 2, 3), np.zeros((3, 8), np.float32))
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve(spec, np.zeros(3, np.float32), _opts())
+    assert str(e.value) == "Argument error: the length of U must be equal to A.dim_x!"
+
+
+def test_no_device_is_an_error_not_a_fallback():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    spec = _dense_spec()
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve(spec, np.zeros(5, np.float32), _opts())
+    assert e.value.code in (capi.ERR_NO_DEVICE, capi.ERR_CUDA)

@@ -1,0 +1,154 @@
+"""GPU parity of the measurement operators and stencils, through the C ABI.
+
+Bresenham pixel lists are compared bit-exactly with the oracle's sequential
+recurrence; operator applications within 1e-5 relative of the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from golden.cases import api_problem, build_case
+from helpers import relerr
+from tval3g import capi, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+OP_CASES = ["dense2d_s32_it20", "dense2d_layers", "ring2d_s64_it20", "ring2d_s64_skip", "hemi3d_s16_it20",
+            "csr3d_s16", "dense3d_s8"]
+
+
+def _dev(torch, a):
+    return torch.tensor(np.ascontiguousarray(a, np.float32), device="cuda")
+
+
+@pytest.mark.parametrize("name", OP_CASES)
+def test_operator_forward_adjoint(name, torch_cuda):
+    torch = torch_cuda
+    c = build_case(name)
+    op = capi.Operator(api_problem(c, capi))
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(op.cols).astype(np.float32)
+    y = rng.standard_normal(op.rows).astype(np.float32)
+    dy = torch.empty(op.rows, device="cuda")
+    op.apply(_dev(torch, x), dy)
+    ref = c["oracle_op"].apply(x.astype(np.float64))
+    assert relerr(dy.cpu().numpy(), ref) < 1e-5
+    dx = torch.empty(op.cols, device="cuda")
+    op.apply(_dev(torch, y), dx, trans=True)
+    ref = c["oracle_op"].apply(y.astype(np.float64), trans=True)
+    assert relerr(dx.cpu().numpy(), ref) < 1e-5
+    # adjoint identity <A x, y> = <x, A^T y>
+    lhs = float(np.dot(dy.cpu().numpy().astype(np.float64), y))
+    rhs = float(np.dot(x.astype(np.float64), dx.cpu().numpy()))
+    assert abs(lhs - rhs) <= 1e-5 * (abs(lhs) + abs(rhs))
+    # deterministic: a second application is bit-identical
+    dx2 = torch.empty(op.cols, device="cuda")
+    op.apply(_dev(torch, y), dx2, trans=True)
+    assert torch.equal(dx, dx2)
+
+
+def _expected_rows(oracle_op, rows):
+    ray, off, pix = oracle_op.ray_lists()
+    lens = np.zeros(rows, np.int64)
+    lens[ray] = np.diff(off)
+    rowptr = np.zeros(rows + 1, np.int64)
+    np.cumsum(lens, out=rowptr[1:])
+    colind = np.zeros(rowptr[-1], np.int32)
+    for k, r in enumerate(ray):
+        colind[rowptr[r]:rowptr[r + 1]] = pix[off[k]:off[k + 1]]
+    return rowptr, colind
+
+
+@pytest.mark.parametrize("name", ["ring2d_s64_it20", "hemi3d_s16_it20"])
+def test_bresenham_lists_bit_exact(name, torch_cuda):
+    c = build_case(name)
+    op = capi.Operator(api_problem(c, capi))
+    rowptr, colind = op.ray_csr()
+    erp, eci = _expected_rows(c["oracle_op"], op.rows)
+    np.testing.assert_array_equal(rowptr, erp)
+    np.testing.assert_array_equal(colind, eci)
+
+
+def test_bresenham_edge_rays_bit_exact(torch_cuda):
+    """Axis-aligned, 45 degree, steep, zero-length and negative rays, 2D and 3D ties."""
+    x0 = np.array([0, 0, 7, 0, 7, 2, 1, 6, 1, 3, 0, 5])
+    y0 = np.array([0, 0, 7, 0, 0, 3, 1, 3, 6, 0, 7, 2])
+    x1 = np.array([7, 0, 0, 7, 0, 2, 6, 1, 3, 1, 7, 0])
+    y1 = np.array([0, 7, 0, 7, 7, 3, 3, 1, 0, 6, 6, 4])
+    N = len(x0)
+    g = dict(use_path=np.eye(N, dtype=np.int32).ravel(), xe=x0, ye=y0, xr=x1, yr=y1, ld=8, scale=1.0)
+    op = capi.Operator(capi.ray2d_problem((8, 8), g))
+    rowptr, colind = op.ray_csr()
+    erp, eci = _expected_rows(O.Op.ray2d(g, 64), N * N)
+    np.testing.assert_array_equal(rowptr, erp)
+    np.testing.assert_array_equal(colind, eci)
+    p0 = np.array([[0, 0, 0], [0, 0, 0], [0, 0, 0], [5, 5, 5], [1, 2, 3], [7, 0, 3], [3, 3, 3], [0, 7, 7]])
+    p1 = np.array([[7, 7, 0], [0, 7, 7], [7, 0, 7], [0, 0, 0], [6, 4, 7], [0, 7, 5], [3, 3, 3], [7, 0, 0]])
+    N = len(p0)
+    g3 = dict(numMPs=1, numPaths=N, E=N, R=N, use_path=(np.eye(N, dtype=np.int32) * np.arange(1, N + 1)).ravel(),
+              xe=p0[:, 0], ye=p0[:, 1], ze=p0[:, 2], xr=p1[:, 0], yr=p1[:, 1], zr=p1[:, 2], rv_x=8, rv_y=8, rv_z=8,
+              scale=1.0)
+    op = capi.Operator(capi.ray3d_problem((8, 8, 8), g3))
+    rowptr, colind = op.ray_csr()
+    erp, eci = _expected_rows(O.Op.ray3d(g3), N)
+    np.testing.assert_array_equal(rowptr, erp)
+    np.testing.assert_array_equal(colind, eci)
+
+
+def test_full_ring_operator_properties(torch_cuda):
+    """256x256, 512 transducers, 131072 rays: GPU rasterisation == closed form
+    CSR twin bit-exactly; A x and A^T y against the twin; adjoint identity."""
+    torch = torch_cuda
+    w = W.ring2d(seed=1, side=256, T=512)
+    op = capi.Operator(capi.ray2d_problem(w["shape"], w["geom"]))
+    rowptr, colind = op.ray_csr()
+    A = w["csr"]
+    np.testing.assert_array_equal(rowptr, A["rowptr"])
+    np.testing.assert_array_equal(colind, A["colind"])
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(op.cols).astype(np.float32)
+    y = rng.standard_normal(op.rows).astype(np.float32)
+    dy = torch.empty(op.rows, device="cuda")
+    op.apply(_dev(torch, x), dy)
+    assert relerr(dy.cpu().numpy(), W.csr_matvec(A, x)) < 1e-5
+    dx = torch.empty(op.cols, device="cuda")
+    op.apply(_dev(torch, y), dx, trans=True)
+    lhs = float(np.dot(dy.cpu().numpy().astype(np.float64), y))
+    rhs = float(np.dot(x.astype(np.float64), dx.cpu().numpy()))
+    assert abs(lhs - rhs) <= 1e-5 * (abs(lhs) + abs(rhs))
+    # the CSR twin on the GPU gives the same products
+    csr = capi.Operator(capi.csr_problem(w["shape"], A["m"], A["n"], A["rowptr"], A["colind"], A["val"]))
+    dy2 = torch.empty(op.rows, device="cuda")
+    csr.apply(_dev(torch, x), dy2)
+    assert relerr(dy2.cpu().numpy(), dy.cpu().numpy()) < 1e-6
+    dx2 = torch.empty(op.cols, device="cuda")
+    csr.apply(_dev(torch, y), dx2, trans=True)
+    assert relerr(dx2.cpu().numpy(), dx.cpu().numpy()) < 1e-6
+
+
+@pytest.mark.parametrize("shape", [(5, 7), (16, 16), (3, 4, 5), (8, 6, 4)])
+def test_stencils_match_oracle(shape, torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(sum(shape))
+    dims = len(shape)
+    n = int(np.prod(shape))
+    U = rng.standard_normal(shape).astype(np.float32)
+    dU = _dev(torch, U)
+    outs = [torch.empty(n, device="cuda") for _ in range(3)]
+    capi.D(dims, shape, dU, *outs[:dims])
+    ref = O.D(U.astype(np.float64))
+    for k in range(dims):
+        np.testing.assert_allclose(outs[k].cpu().numpy(), ref[k], rtol=0, atol=1e-6)
+    X = [rng.standard_normal(n).astype(np.float32) for _ in range(3)]
+    res = torch.empty(n, device="cuda")
+    capi.Dt(dims, shape, _dev(torch, X[0]), _dev(torch, X[1]), _dev(torch, X[2]) if dims == 3 else None, res)
+    ref = O.Dt(X[0], X[1], X[2] if dims == 3 else None, shape=shape)
+    np.testing.assert_allclose(res.cpu().numpy(), ref, rtol=0, atol=1e-5)
+    for tv in (0, 1):
+        S = [rng.standard_normal(n).astype(np.float32) * 0.1 for _ in range(dims)]
+        Wd = [torch.empty(n, device="cuda") for _ in range(dims)]
+        lam = capi.shrink(dims, n, tv, 8.0, [_dev(torch, x) for x in X[:dims]], [_dev(torch, s) for s in S], Wd)
+        Wr, lamr = O.shrink([x.astype(np.float64) for x in X[:dims]], [s.astype(np.float64) for s in S], 8.0, tv)
+        for k in range(dims):
+            np.testing.assert_allclose(Wd[k].cpu().numpy(), Wr[k], rtol=0, atol=1e-6)
+        assert abs(lam - lamr) < 1e-5 * abs(lamr)

@@ -1,0 +1,168 @@
+"""The oracle pinned against the reference (no GPU).
+
+The reference ships no tests or golden vectors, so the FP64 restatement is
+pinned against the reference itself: its own sources compiled unchanged
+(oracle/_ref), whose outputs on seeded problems are the golden fixtures in
+tests/golden (written by tests/golden/make_golden.py).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import golden, relerr
+from tval3g import workloads as W
+
+from golden.cases import CASES, build_case  # noqa: E402
+
+
+def _checksum(a):
+    a = np.asarray(a, np.float64).ravel()
+    return np.array([a.size, a.sum(), np.abs(a).sum(), (a * np.arange(a.size) % 7.0).sum()])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_inputs_regenerate_bit_identically(name):
+    c = build_case(name)
+    g = golden(f"{name}.npz")
+    np.testing.assert_array_equal(_checksum(c["b"]), g["b_sum"])
+    if "A" in c:
+        np.testing.assert_array_equal(_checksum(c["A"]), g["A_sum"])
+
+
+@pytest.mark.parametrize("name", [n for n in CASES if n != "ring2d_s64_iso"])
+def test_restatement_matches_reference_fp64(name):
+    """FP64 oracle == the reference's double build (same iteration counts)."""
+    c = build_case(name)
+    g = golden(f"{name}.npz")
+    r = O.solve(c["oracle_op"], c["b"].astype(np.float64), c["shape"], c["opts"])
+    assert tuple(g["ref2_iters"]) == (r.outer_iters, r.total_iters)
+    assert relerr(r.U, g["ref2_U"]) < 1e-6
+    np.testing.assert_allclose(r.U, g["oracle_U"], rtol=0, atol=1e-12 * np.abs(g["oracle_U"]).max())
+
+
+def test_reference_float_build_drift_documented():
+    """The reference's own float build drifts from its double build: this is
+    why solver parity tolerances are stated per iteration count."""
+    g = golden("dense2d_s32_it20.npz")
+    assert relerr(g["ref0_U"], g["ref2_U"]) < 1e-3
+    g = golden("dense2d_s32_conv.npz")
+    assert relerr(g["ref0_U"], g["ref2_U"]) < 2e-2
+
+
+@pytest.mark.skipif(not O.ref_available(2), reason="reference not built here")
+def test_reference_live_matches_fixture(tmp_path, monkeypatch):
+    c = build_case("dense2d_s32_it20")
+    g = golden("dense2d_s32_it20.npz")
+    r = O.ref_solve("dense", c["shape"], c["b"], c["opts"], dtype=2, A=c["A"])
+    np.testing.assert_array_equal(r.U, g["ref2_U"])
+
+
+# --------------------------------------------------------------------------
+# Bresenham: closed form (product generator / kernels) == recurrence (oracle)
+# --------------------------------------------------------------------------
+EDGE_RAYS_2D = [  # (x0, y0, x1, y1)
+    (0, 0, 7, 0), (0, 0, 0, 7), (7, 7, 0, 0), (0, 0, 7, 7), (7, 0, 0, 7), (2, 3, 2, 3), (1, 1, 6, 3),
+    (6, 3, 1, 1), (1, 6, 3, 0), (3, 0, 1, 6), (0, 7, 7, 6), (5, 2, 0, 4),
+]
+
+
+def test_bresenham_2d_edge_cases():
+    ld = 8
+    x0, y0, x1, y1 = (np.array(v) for v in zip(*EDGE_RAYS_2D))
+    g = dict(use_path=np.ones(len(x0) * len(x0), np.int32), xe=x0, ye=y0, xr=x1, yr=y1, ld=ld, scale=1.0)
+    # one emitter per ray, paired with its own receiver
+    use = np.eye(len(x0), dtype=np.int32).ravel()
+    g["use_path"] = use
+    op = O.Op.ray2d(g, 64)
+    ray, off, pix = op.ray_lists()
+    coff, cpix = W.bresenham_csr_2d(x0, y0, x1, y1, ld)
+    np.testing.assert_array_equal(off, coff)
+    np.testing.assert_array_equal(pix, cpix)
+    # both endpoints included; zero-length ray has one pixel
+    assert off[6] - off[5] == 1
+
+
+def test_bresenham_3d_ties_and_edges():
+    p0 = np.array([[0, 0, 0], [0, 0, 0], [0, 0, 0], [5, 5, 5], [1, 2, 3], [7, 0, 3], [3, 3, 3], [0, 7, 7]])
+    p1 = np.array([[7, 7, 0], [0, 7, 7], [7, 0, 7], [0, 0, 0], [6, 4, 7], [0, 7, 5], [3, 3, 3], [7, 0, 0]])
+    N = len(p0)
+    g = dict(numMPs=1, numPaths=N, E=N, R=N, use_path=(np.eye(N, dtype=np.int32) * np.arange(1, N + 1)).ravel(),
+             xe=p0[:, 0], ye=p0[:, 1], ze=p0[:, 2], xr=p1[:, 0], yr=p1[:, 1], zr=p1[:, 2], rv_x=8, rv_y=8, rv_z=8,
+             scale=1.0)
+    ray, off, pix = O.Op.ray3d(g).ray_lists()
+    coff, cpix = W.bresenham_csr_3d(p0, p1, 8, 8)
+    np.testing.assert_array_equal(off, coff)
+    np.testing.assert_array_equal(pix, cpix)
+
+
+def test_bresenham_ring_and_hemisphere_geometries():
+    w = W.ring2d(seed=1, side=64, T=64)
+    ray, off, pix = O.Op.ray2d(w["geom"], 64 * 64).ray_lists()
+    A = w["csr"]
+    np.testing.assert_array_equal(pix, A["colind"])
+    np.testing.assert_array_equal(ray, np.nonzero(np.diff(A["rowptr"]))[0])
+    w = W.hemi3d(seed=2, side=16, T=64, receivers=16, csr=True)
+    ray, off, pix = O.Op.ray3d(w["geom"]).ray_lists()
+    A = w["csr"]
+    order = np.argsort(ray, kind="stable")
+    np.testing.assert_array_equal(np.concatenate([pix[off[k]:off[k + 1]] for k in order]), A["colind"])
+
+
+def test_bresenham_full_ring_geometry_lengths():
+    """256x256, 512 transducers: max(|dx|,|dy|)+1 hits per ray (size-independent property)."""
+    g = W.ring_geometry(256, 512)
+    use = g["use_path"].reshape(512, 512)
+    e, r = np.nonzero(use)
+    off, pix = W.bresenham_csr_2d(g["xe"][e], g["ye"][e], g["xr"][r], g["yr"][r], 256)
+    L = np.maximum(np.abs(g["xr"][r] - g["xe"][e]), np.abs(g["yr"][r] - g["ye"][e])) + 1
+    np.testing.assert_array_equal(np.diff(off), L)
+    assert pix.min() >= 0 and pix.max() < 65536
+    assert len(e) == 131072
+
+
+# --------------------------------------------------------------------------
+# stencils
+# --------------------------------------------------------------------------
+def test_D_Dt_adjoint_2d():
+    rng = np.random.default_rng(0)
+    U = rng.standard_normal((5, 7))
+    X, Y = rng.standard_normal(35), rng.standard_normal(35)
+    Ux, Uy = O.D(U)
+    lhs = Ux @ X + Uy @ Y
+    rhs = U.ravel() @ O.Dt(X, Y, shape=(5, 7))
+    assert abs(lhs - rhs) < 1e-12 * (abs(lhs) + 1)
+
+
+def test_Dt_3d_is_the_reference_not_the_adjoint():
+    """The reference's 3D Dt adds X[last row of slice z-1] - X[first row of slice z]
+    on every first row of slices z >= 1 (3d/tval3_cpu_3d.cpp:402-413)."""
+    rng = np.random.default_rng(1)
+    shape = (3, 4, 5)
+    U = rng.standard_normal(shape)
+    X, Y, Z = (rng.standard_normal(60) for _ in range(3))
+    Ux, Uy, Uz = O.D(U)
+    lhs = Ux @ X + Uy @ Y + Uz @ Z
+    res = O.Dt(X, Y, Z, shape=shape)
+    # exact adjoint + the reference's extra term
+    Y3 = Y.reshape(shape)
+    extra = np.zeros(shape)
+    extra[1:, 0, :] = Y3[:-1, -1, :] - Y3[1:, 0, :]
+    assert abs(lhs - U.ravel() @ (res - extra.ravel())) < 1e-12 * (abs(lhs) + 1)
+    assert np.abs(extra).max() > 0
+
+
+def test_shrink_edges():
+    beta = 4.0
+    ux = np.array([0.25, -0.25, 0.0, 1.0, -1.0, 0.3])
+    uy = np.array([0.0, 0.0, 0.0, 0.0, 0.5, -0.1])
+    z = np.zeros(6)
+    (wx, wy), lam = O.shrink([ux, uy], [z, z], beta, 0)
+    # |Ubar| == 1/beta -> 0; 0 -> 0; sign kept
+    assert wx[0] == 0 and wx[1] == 0 and wx[2] == 0
+    assert wx[3] == 0.75 and wx[4] == -0.75 and wy[4] == 0.25
+    (ix, iy), lam_iso = O.shrink([ux, uy], [z, z], beta, 1)
+    n4 = np.hypot(ux[4], uy[4])
+    assert abs(ix[4] - (n4 - 0.25) * ux[4] / n4) < 1e-15
+    assert ix[2] == 0 and iy[2] == 0

@@ -1,0 +1,242 @@
+// Internal declarations of the tval3g engine (sm_100a).
+//
+// Layout in HBM.  A plan holds `count` instances (independent reconstructions).
+// Each instance owns NVN image-sized float vectors and NVM measurement-sized
+// float vectors carved from one arena, a Ctrl block of FP64 scalars and flags,
+// and a slice of the FP64 partial-sum buffer.  Kernels are launched over tile
+// maps: a tile map is a device array of (instance, local tile) pairs, so one
+// launch covers every instance of a batch; per-instance predicates (Ctrl flags)
+// let instances that are done or on another branch skip a launch.
+//
+// Reductions are deterministic: every tile writes its FP64 partial sums, and
+// the last tile of an instance to finish (atomic ticket) sums them in tile
+// order and runs that instance's scalar control step (the reference's host
+// code: step length, Armijo test, stopping tests, continuation).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <climits>
+
+#include <string>
+#include <vector>
+
+#include "../../include/tval3g.h"
+
+namespace tval3g {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+void set_error(const std::string &msg);
+struct Error {
+	int code;
+	std::string msg;
+};
+#define TG_CUDA(call)                                                                               \
+	do {                                                                                            \
+		cudaError_t e_ = (call);                                                                    \
+		if (e_ != cudaSuccess)                                                                      \
+			throw ::tval3g::Error{TVAL3G_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+	} while (0)
+#define TG_ARG(cond, msg)                                                                           \
+	do {                                                                                            \
+		if (!(cond)) throw ::tval3g::Error{TVAL3G_ERR_ARGUMENT, (msg)};                             \
+	} while (0)
+
+// ---------------------------------------------------------------------------
+// per-instance vectors
+// ---------------------------------------------------------------------------
+enum VecN {
+	vU, vUp, vdU, vUUP, vUx, vUy, vUz, vUxp, vUyp, vUzp, vdUx, vdUy, vdUz, vWx, vWy, vWz,
+	vSx, vSy, vSz, vAtb, vD, vG, vGp, vdG, vG2, vG2p, vdG2, vDts, vRcd, NVN
+};
+enum VecM { vB, vAu, vAup, vdAu, vDelta, vLastAu, vAd, NVM };
+
+// scalar state of one instance (the reference's tval3_data scalars and the
+// locals of its driver, 2d/tval3_cpu_2d.cpp:99-196,752-853)
+struct Ctrl {
+	double mu, beta, muDbeta, gam, Q, C, f;
+	double lam1, lam2, lam3, lam4, lam5;
+	double tau, alpha, c_armij, scl, nrmup, relchg, relchg_out, beta0;
+	double dd, dDd;
+	double currSkip;
+	double rel_error;
+	int currInit;
+	int count_outer, count_total;
+	int fst, active, need_bt, bt_cnt, restart, inner_break, need_mlp, need_Ad, skip_adj;
+	int status;
+	unsigned ticket;
+	int pad;
+};
+
+// predicates: which instances take part in a launch
+enum Pred {
+	P_ALL = 0,      // every instance (initialisation)
+	P_ACTIVE,       // not yet converged
+	P_NEED_AD,      // first-iteration step length needs A*d
+	P_NEED_BT,      // Armijo test failed: backtracking (not restarting)
+	P_RESTART,      // five backtracking steps failed: restart from Up
+	P_INNER_BREAK,  // inner loop ended: outer step
+	P_NEED_MLP,     // multiplier update and continuation
+	P_ACTIVE_MUL,   // active and the A^T multiplication is not skipped
+	P_RESTART_MUL,  // restarting (the restart always multiplies)
+};
+
+__device__ __forceinline__ bool pred_ok(const Ctrl &c, int p) {
+	switch (p) {
+	case P_ALL: return true;
+	case P_ACTIVE: return c.active != 0;
+	case P_NEED_AD: return c.need_Ad != 0;
+	case P_NEED_BT: return c.need_bt != 0 && c.restart == 0;
+	case P_RESTART: return c.restart != 0;
+	case P_INNER_BREAK: return c.inner_break != 0;
+	case P_NEED_MLP: return c.need_mlp != 0;
+	case P_ACTIVE_MUL: return c.active != 0 && c.skip_adj == 0;
+	case P_RESTART_MUL: return c.restart != 0;
+	}
+	return false;
+}
+
+// measurement operator of one instance (device side)
+struct OpDev {
+	int kind;
+	int layers;
+	long long m;      // rows of one layer
+	long long n;      // columns of one layer
+	// dense
+	const float *A;
+	int dense_kchunks;     // row chunks of the transposed product
+	long long dense_part;  // offset of this instance in the dense partial buffer (floats)
+	// compressed gather operators: forward rows (CSR) and transpose (CSC)
+	const int *rptr, *rind;
+	const float *rval;      // NULL = implicit unit weights
+	const int *cptr, *cind;
+	const float *cval;      // NULL = implicit unit weights
+	float scale;            // multiplies every implicit weight
+	// rays: packed (x0, y0, z0, dx, dy, dz, out) per traced ray (ops.cuh pack_ray)
+	int nrays;
+	const int4 *rays;
+	int rvx, rvy;           // index = x + y*rvx + z*rvx*rvy (2D: rvx = ld)
+};
+
+// one instance as the kernels see it
+struct Inst {
+	int dims, p, q, r;           // image: dim_y, dim_x, dim_z (r = 1 in 2D)
+	long long n, m;              // vector lengths (n and m include layers)
+	float *vn[NVN];
+	float *vm[NVM];
+	const float *b_user;         // caller's b (device)
+	const float *ut_user;        // caller's Ut (device) or NULL
+	float *u_user;               // caller's U (device)
+	Ctrl *ctrl;
+	double *part;                // this instance's partial sums
+	int ntn, ntm;                // tiles over n and m
+	// options (2d/tval3_cpu_2d.cpp:769-772)
+	double muf, betaf, mu0, beta0, tol, tol_inn, c, gamma, gam0, rate_gam, rate_cnt;
+	double skipRatio, maxRelChange;
+	int maxit, maxcnt, nonneg, tv_norm, numInit, skip_enabled;
+	OpDev op;
+};
+
+constexpr int TILE = 1024;       // elements per tile (256 threads x 4)
+constexpr int BLOCK = 256;
+constexpr int NSUM = 4;          // partial sums per tile
+
+// tile maps
+enum MapKind { MAP_N = 0, MAP_M, MAP_NM, NMAPS };
+
+struct TileMap {
+	const int2 *tiles = nullptr;  // (instance, local tile); local >= ntn means an m tile (MAP_NM)
+	int count = 0;
+};
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+__device__ __forceinline__ float warp_sumf(float v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+
+// Reduce NS per-thread values over the block; thread 0 gets the totals.
+template <int NS>
+__device__ __forceinline__ void block_sums(double (&v)[NS], double *sh /* [NS * 32] */) {
+	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+	for (int s = 0; s < NS; s++) v[s] = warp_sum(v[s]);
+	if (lane == 0)
+#pragma unroll
+		for (int s = 0; s < NS; s++) sh[s * 32 + wid] = v[s];
+	__syncthreads();
+	if (wid == 0) {
+#pragma unroll
+		for (int s = 0; s < NS; s++) {
+			double t = lane < nw ? sh[s * 32 + lane] : 0.0;
+			v[s] = warp_sum(t);
+		}
+	}
+	__syncthreads();
+}
+
+// Write this tile's NS sums; return true (in every thread) in the block that
+// is the last of its instance, with tot[] = the instance totals (summed in
+// tile order).  `ntiles` = tiles of this instance in the launch.
+template <int NS>
+__device__ __forceinline__ bool tile_reduce(const Inst &I, int local, int ntiles, double (&v)[NS],
+                                            double (&tot)[NS]) {
+	__shared__ double sh[NSUM * 32];
+	__shared__ int last;
+	block_sums<NS>(v, sh);
+	if (threadIdx.x == 0) {
+#pragma unroll
+		for (int s = 0; s < NS; s++) I.part[(long long)local * NSUM + s] = v[s];
+		__threadfence();
+		unsigned t = atomicAdd(&I.ctrl->ticket, 1u);
+		last = (t == (unsigned)ntiles - 1);
+	}
+	__syncthreads();
+	if (!last) return false;
+	__threadfence();
+	double acc[NS];
+#pragma unroll
+	for (int s = 0; s < NS; s++) acc[s] = 0.0;
+	// fixed assignment of tiles to threads, then a fixed-shape block tree
+	for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
+#pragma unroll
+		for (int s = 0; s < NS; s++) acc[s] += __ldcg(&I.part[(long long)t * NSUM + s]);
+	block_sums<NS>(acc, sh);
+	if (threadIdx.x == 0) {
+#pragma unroll
+		for (int s = 0; s < NS; s++) tot[s] = acc[s];
+		I.ctrl->ticket = 0;
+	}
+	return true;
+}
+
+// ---------------------------------------------------------------------------
+// host-side launch interfaces (implemented in the .cu files)
+// ---------------------------------------------------------------------------
+struct LaunchCtx {
+	cudaStream_t stream;
+	const Inst *inst;       // device table
+	long long *launches;    // host counter of kernel launches issued
+};
+
+// operators (op_*.cu): y = A x over every instance of the batch whose Pred
+// holds; x, y select vectors of the instance (is_m tells which bank).
+struct VecSel {
+	bool m;   // false: vn[idx], true: vm[idx]
+	int idx;
+};
+
+struct OpBatch;   // per-kind launch data, built by the plan
+void op_forward(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y);
+void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y);
+
+}  // namespace tval3g

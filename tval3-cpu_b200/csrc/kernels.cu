@@ -1,0 +1,847 @@
+// Fused TVAL3 iteration kernels; see kernels.cuh.
+#include <math.h>
+
+#include "kernels.cuh"
+
+namespace tval3g {
+
+// ---------------------------------------------------------------------------
+// prologue / image geometry
+// ---------------------------------------------------------------------------
+#define KPROLOGUE(a)                                                                   \
+	if ((a).launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd((a).launches, 1ull); \
+	const int2 tl_ = (a).map.tiles[blockIdx.x];                                        \
+	const Inst &I = (a).tab[tl_.x];                                                    \
+	const int local = tl_.y;                                                           \
+	if (!pred_ok(*I.ctrl, (a).pred)) return;
+
+struct Geo {
+	int dims, p, q, r;
+	long long S, n;
+	__device__ Geo(const Inst &I) : dims(I.dims), p(I.p), q(I.q), r(I.r), S((long long)I.p * I.q), n(I.n) {}
+	__device__ void coords(long long i, int &x, int &y, int &z) const {
+		long long row = i / q;
+		x = (int)(i - row * q);
+		z = (int)(row / p);
+		y = (int)(row - (long long)z * p);
+	}
+};
+
+// periodic forward differences at i (2d:268-278, 3d:365-389)
+__device__ __forceinline__ float dxf(const float *U, const Geo &g, long long i, int x) {
+	return (x < g.q - 1) ? U[i + 1] - U[i] : U[i - (g.q - 1)] - U[i];
+}
+__device__ __forceinline__ float dyf(const float *U, const Geo &g, long long i, int y) {
+	return (y < g.p - 1) ? U[i + g.q] - U[i] : U[i - (long long)(g.p - 1) * g.q] - U[i];
+}
+__device__ __forceinline__ float dzf(const float *U, const Geo &g, long long i, int z) {
+	return (z < g.r - 1) ? U[i + g.S] - U[i] : U[i - (long long)(g.r - 1) * g.S] - U[i];
+}
+
+// Dt at i with component accessors vx(j), vy(j), vz(j); the float additions
+// are made in the reference's order (2d:280-293, 3d:394-425), including the
+// 3D y term the reference adds on the first row of slices z >= 1.
+template <class FX, class FY, class FZ>
+__device__ __forceinline__ float dt_at(const Geo &g, long long i, int x, int y, int z, FX vx, FY vy,
+                                       FZ vz) {
+	float res = (x > 0) ? vx(i - 1) - vx(i) : vx(i + g.q - 1) - vx(i);
+	if (g.dims == 2) {
+		if (y > 0) { res = res + vy(i - g.q); res = res + (-vy(i)); }
+		else { res = res + vy(i + (long long)(g.p - 1) * g.q); res = res + (-vy(i)); }
+	} else {
+		if (!(z == 0 && y == 0)) { res = res + vy(i - g.q); res = res + (-vy(i)); }
+		if (y == 0) { res = res + vy(i + (long long)(g.p - 1) * g.q); res = res + (-vy(i)); }
+		if (z > 0) { res = res + vz(i - g.S); res = res + (-vz(i)); }
+		else { res = res + vz(i + (long long)(g.r - 1) * g.S); res = res + (-vz(i)); }
+	}
+	return res;
+}
+
+// shrinkage of one pixel: anisotropic 2d:588-611 / 3d:834-871; isotropic:
+// W = max(|Ubar|_2 - 1/beta, 0) * Ubar / |Ubar|_2 (no reference counterpart)
+struct Shrink {
+	float beta, thr;
+	int iso, dims;
+	__device__ Shrink(const Inst &I, double beta_d)
+		: beta((float)beta_d), thr((float)(1.0 / beta_d)), iso(I.tv_norm), dims(I.dims) {}
+	__device__ __forceinline__ float apply(const float (&u)[3], const float (&s)[3], float (&w)[3]) const {
+		float ub[3];
+#pragma unroll
+		for (int c = 0; c < 3; c++) ub[c] = (c < dims) ? u[c] - s[c] / beta : 0.f;
+		if (iso) {
+			float nrm = sqrtf(ub[0] * ub[0] + ub[1] * ub[1] + ub[2] * ub[2]);
+			float t = nrm - thr;
+			t = t >= 0.f ? t : 0.f;
+#pragma unroll
+			for (int c = 0; c < 3; c++) w[c] = nrm > 0.f ? t * ub[c] / nrm : 0.f;
+			return t;
+		}
+		float lam = 0.f;
+#pragma unroll
+		for (int c = 0; c < 3; c++) {
+			float t = fabsf(ub[c]) - thr;
+			t = t >= 0.f ? t : 0.f;
+			if (c < dims) lam += t;
+			w[c] = ub[c] >= 0.f ? t : -t;
+		}
+		return lam;
+	}
+	// one component of W at j, from U_c and sigma_c
+	__device__ __forceinline__ float comp(const Inst &I, long long j, int c) const {
+		float u[3], s[3], w[3];
+		if (iso) {
+			u[0] = I.vn[vUx][j]; u[1] = I.vn[vUy][j]; u[2] = dims == 3 ? I.vn[vUz][j] : 0.f;
+			s[0] = I.vn[vSx][j]; s[1] = I.vn[vSy][j]; s[2] = dims == 3 ? I.vn[vSz][j] : 0.f;
+			apply(u, s, w);
+			return w[c];
+		}
+		float ub = I.vn[vUx + c][j] - I.vn[vSx + c][j] / beta;
+		float t = fabsf(ub) - thr;
+		t = t >= 0.f ? t : 0.f;
+		return ub >= 0.f ? t : -t;
+	}
+};
+
+__device__ __forceinline__ bool bad(double v) { return !isfinite(v); }
+
+// ---------------------------------------------------------------------------
+// scaleb (2d:229-266): first min |b| and first max |b|, scale into [0.5, 1.5]
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void better_min(float &a, long long &ia, float b, long long ib) {
+	if (b < a || (b == a && ib < ia)) { a = b; ia = ib; }
+}
+__device__ __forceinline__ void better_max(float &a, long long &ia, float b, long long ib) {
+	if (b > a || (b == a && ib < ia)) { a = b; ia = ib; }
+}
+
+__global__ void __launch_bounds__(BLOCK) k_scaleb(KArgs a) {
+	KPROLOGUE(a);
+	const long long m = I.m, i0 = (long long)local * TILE;
+	float mn = INFINITY, mx = -INFINITY;
+	long long imn = LLONG_MAX, imx = LLONG_MAX;
+	for (int k = 0; k < TILE / BLOCK; k++) {
+		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+		if (i < m) {
+			float v = fabsf(I.b_user[i]);
+			better_min(mn, imn, v, i);
+			better_max(mx, imx, v, i);
+		}
+	}
+	for (int o = 16; o > 0; o >>= 1) {
+		float v = __shfl_xor_sync(0xffffffffu, mn, o);
+		long long iv = __shfl_xor_sync(0xffffffffu, imn, o);
+		better_min(mn, imn, v, iv);
+		v = __shfl_xor_sync(0xffffffffu, mx, o);
+		iv = __shfl_xor_sync(0xffffffffu, imx, o);
+		better_max(mx, imx, v, iv);
+	}
+	__shared__ float smn[32], smx[32];
+	__shared__ long long simn[32], simx[32];
+	__shared__ int last;
+	int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	if (lane == 0) { smn[wid] = mn; simn[wid] = imn; smx[wid] = mx; simx[wid] = imx; }
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		for (int w = 1; w < BLOCK / 32; w++) {
+			better_min(mn, imn, smn[w], simn[w]);
+			better_max(mx, imx, smx[w], simx[w]);
+		}
+		double *P = I.part + (long long)local * NSUM;
+		P[0] = mn; P[1] = (double)imn; P[2] = mx; P[3] = (double)imx;
+		__threadfence();
+		unsigned t = atomicAdd(&I.ctrl->ticket, 1u);
+		last = (t == (unsigned)I.ntm - 1);
+	}
+	__syncthreads();
+	if (!last || threadIdx.x != 0) return;
+	__threadfence();
+	float gmn = INFINITY, gmx = -INFINITY;
+	long long gimn = LLONG_MAX, gimx = LLONG_MAX;
+	for (int t = 0; t < I.ntm; t++) {   // tiles in index order: first occurrence wins
+		const double *P = I.part + (long long)t * NSUM;
+		better_min(gmn, gimn, (float)__ldcg(P + 0), (long long)__ldcg(P + 1));
+		better_max(gmx, gimx, (float)__ldcg(P + 2), (long long)__ldcg(P + 3));
+	}
+	Ctrl &c = *I.ctrl;
+	double scl = 1.0;
+	if (gimn < m && gimx < m) {   // (all-NaN data leaves no index: no scaling)
+		double dif = fabs((double)I.b_user[gimx] - (double)I.b_user[gimn]);
+		if (dif < 0.5) scl = 0.5 / dif;
+		else if (dif > 1.5) scl = 1.5 / dif;
+	}
+	c.scl = scl;
+	c.ticket = 0;
+}
+
+// ---------------------------------------------------------------------------
+// initial state (2d:767-779): zero the vectors, bs = b*scl, scalar defaults
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(BLOCK) k_init(KArgs a) {
+	KPROLOGUE(a);
+	Ctrl &c = *I.ctrl;
+	if (local < I.ntn) {
+		long long i0 = (long long)local * TILE;
+		for (int k = 0; k < TILE / BLOCK; k++) {
+			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+			if (i < I.n)
+				for (int v = 0; v < NVN; v++) I.vn[v][i] = 0.f;
+		}
+		if (local == 0 && threadIdx.x == 0) {
+			c.mu = I.mu0; c.beta = I.beta0;
+			if (c.mu > I.muf) c.mu = I.muf;
+			if (c.beta > I.betaf) c.beta = I.betaf;
+			c.muDbeta = c.mu / c.beta;
+			c.gam = I.gam0; c.Q = 1; c.C = 0; c.f = 0;
+			c.lam1 = c.lam2 = c.lam3 = c.lam4 = c.lam5 = 0;
+			c.tau = c.alpha = c.c_armij = c.nrmup = c.relchg = c.relchg_out = c.beta0 = 0;
+			c.dd = c.dDd = 0; c.currSkip = 0; c.currInit = 0; c.rel_error = 0;
+			c.count_outer = c.count_total = 0;
+			c.fst = 1; c.active = 1; c.need_bt = c.bt_cnt = c.restart = c.inner_break = 0;
+			c.need_mlp = c.need_Ad = c.skip_adj = 0; c.status = 0;
+		}
+	} else {
+		long long i0 = (long long)(local - I.ntn) * TILE;
+		float scl = (float)c.scl;
+		for (int k = 0; k < TILE / BLOCK; k++) {
+			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+			if (i < I.m) {
+				for (int v = 0; v < NVM; v++) I.vm[v][i] = 0.f;
+				I.vm[vB][i] = scl != 1.f ? I.b_user[i] * scl : I.b_user[i];
+			}
+		}
+	}
+}
+
+// U = Atb, rcdU = U (2d:775,779)
+__global__ void __launch_bounds__(BLOCK) k_init_u(KArgs a) {
+	KPROLOGUE(a);
+	long long i0 = (long long)local * TILE;
+	for (int k = 0; k < TILE / BLOCK; k++) {
+		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+		if (i < I.n) {
+			float u = I.vn[vAtb][i];
+			I.vn[vU][i] = u;
+			I.vn[vRcd][i] = u;
+		}
+	}
+}
+
+// (Ux, Uy[, Uz]) = D U
+__global__ void __launch_bounds__(BLOCK) k_D(KArgs a) {
+	KPROLOGUE(a);
+	Geo g(I);
+	const float *U = I.vn[vU];
+	long long i0 = (long long)local * TILE;
+	for (int k = 0; k < TILE / BLOCK; k++) {
+		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+		if (i >= g.n) continue;
+		int x, y, z;
+		g.coords(i, x, y, z);
+		I.vn[vUx][i] = dxf(U, g, i, x);
+		I.vn[vUy][i] = dyf(U, g, i, y);
+		if (g.dims == 3) I.vn[vUz][i] = dzf(U, g, i, z);
+	}
+}
+
+// ---------------------------------------------------------------------------
+// update_W (2d:651-671): shrinkage, then g2 = Dt(DU - W), lam1, lam2, lam4.
+// The neighbours' W needed by Dt are recomputed from their U and sigma.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(BLOCK) k_shrink_g2(KArgs a) {
+	KPROLOGUE(a);
+	Geo g(I);
+	Ctrl &c = *I.ctrl;
+	Shrink sh(I, c.beta);
+	double v[3] = {0, 0, 0};   // lam1, lam2, lam4
+	long long i0 = (long long)local * TILE;
+	for (int k = 0; k < TILE / BLOCK; k++) {
+		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+		if (i >= g.n) continue;
+		int x, y, z;
+		g.coords(i, x, y, z);
+		float u[3], s[3], w[3];
+		for (int cc = 0; cc < 3; cc++) {
+			u[cc] = cc < g.dims ? I.vn[vUx + cc][i] : 0.f;
+			s[cc] = cc < g.dims ? I.vn[vSx + cc][i] : 0.f;
+		}
+		v[0] += sh.apply(u, s, w);
+		for (int cc = 0; cc < g.dims; cc++) I.vn[vWx + cc][i] = w[cc];
+		auto V = [&](int cc) {
+			return [&, cc](long long j) { return j == i ? u[cc] - w[cc] : I.vn[vUx + cc][j] - sh.comp(I, j, cc); };
+		};
+		I.vn[vG2][i] = dt_at(g, i, x, y, z, V(0), V(1), V(2));
+		for (int cc = 0; cc < g.dims; cc++) {
+			float vv = u[cc] - w[cc];
+			v[1] += (double)vv * vv;
+			v[2] += (double)s[cc] * vv;
+		}
+	}
+	double tot[3];
+	if (!tile_reduce<3>(I, local, I.ntn, v, tot)) return;
+	if (threadIdx.x != 0) return;
+	if (a.stage == ST_LOOP) {
+		c.f -= (c.lam1 + c.beta / 2 * c.lam2 - c.lam4);
+		c.lam1 = tot[0]; c.lam2 = tot[1]; c.lam4 = tot[2];
+		c.f += (c.lam1 + c.beta / 2 * c.lam2 - c.lam4);
+		// nonmonotone reference values (2d:802)
+		double Qp = c.Q;
+		c.Q = c.gam * Qp + 1;
+		c.C = (c.gam * Qp * c.C + c.f) / c.Q;
+	} else {
+		c.lam1 = tot[0]; c.lam2 = tot[1]; c.lam4 = tot[2];
+	}
+}
+
+// ---------------------------------------------------------------------------
+// get_g epilogue (2d:396-423): g -= Atb; V = DU - W; g2 = Dt V; lam2, lam4;
+// Aub = Au - b; lam3, lam5; f.  Descent stage also runs the Armijo test
+// (2d:543-548).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
+	KPROLOGUE(a);
+	Ctrl &c = *I.ctrl;
+	double v[4] = {0, 0, 0, 0};   // lam2, lam4, lam3, lam5
+	if (local < I.ntn) {
+		Geo g(I);
+		long long i0 = (long long)local * TILE;
+		for (int k = 0; k < TILE / BLOCK; k++) {
+			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+			if (i >= g.n) continue;
+			int x, y, z;
+			g.coords(i, x, y, z);
+			I.vn[vG][i] = I.vn[vG][i] - I.vn[vAtb][i];
+			auto V = [&](int cc) { return [&, cc](long long j) { return I.vn[vUx + cc][j] - I.vn[vWx + cc][j]; }; };
+			I.vn[vG2][i] = dt_at(g, i, x, y, z, V(0), V(1), V(2));
+			for (int cc = 0; cc < g.dims; cc++) {
+				float vv = I.vn[vUx + cc][i] - I.vn[vWx + cc][i];
+				v[0] += (double)vv * vv;
+				v[1] += (double)I.vn[vSx + cc][i] * vv;
+			}
+		}
+	} else {
+		long long i0 = (long long)(local - I.ntn) * TILE;
+		for (int k = 0; k < TILE / BLOCK; k++) {
+			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+			if (i >= I.m) continue;
+			float r = I.vm[vAu][i] - I.vm[vB][i];
+			v[2] += (double)r * r;
+			v[3] += (double)I.vm[vDelta][i] * r;
+		}
+	}
+	double tot[4];
+	if (!tile_reduce<4>(I, local, I.ntn + I.ntm, v, tot)) return;
+	if (threadIdx.x != 0) return;
+	c.lam2 = tot[0]; c.lam4 = tot[1]; c.lam3 = tot[2]; c.lam5 = tot[3];
+	c.f = (c.lam1 + c.beta / 2 * c.lam2 + c.mu / 2 * c.lam3) - c.lam4 - c.lam5;
+	if (a.stage == ST_DESCEND) {
+		c.alpha = 1;
+		c.c_armij = c.dd * c.tau * I.c * c.beta;
+		c.need_bt = fabs(c.f) > fabs(c.C - c.alpha * c.c_armij);
+		c.bt_cnt = 0;
+		if (bad(c.f)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; c.need_bt = 0; }
+	} else if (a.stage == ST_RESTART) {
+		c.restart = 0;
+		c.need_bt = 0;
+		if (I.skip_enabled) c.currSkip = 0;
+	} else if (a.stage == ST_INIT) {
+		if (I.skip_enabled) c.currSkip = 0;
+	}
+}
+
+// ---------------------------------------------------------------------------
+// get_gradient (2d:578-585) and the inner stopping test (2d:803-817)
+//   ST_LOOP:  uup = U - Up; d = DtsAtd + g2 + muDbeta*g; RelChg
+//   ST_INIT:  d = DtsAtd + g2 + muDbeta*g (DtsAtd = 0); Q = 1, C = f
+//   ST_OUTER: DtsAtd = (beta0/beta) d; d = ... (2d:844-852)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
+	KPROLOGUE(a);
+	Ctrl &c = *I.ctrl;
+	const float mdb = (float)c.muDbeta;
+	const float bscale = a.stage == ST_OUTER ? (float)(c.beta0 / c.beta) : 1.f;
+	double v[3] = {0, 0, 0};   // |d|^2, |Up|^2, |uup|^2
+	long long i0 = (long long)local * TILE;
+	for (int k = 0; k < TILE / BLOCK; k++) {
+		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+		if (i >= I.n) continue;
+		float dts = I.vn[vDts][i];
+		if (a.stage == ST_OUTER) {
+			dts = I.vn[vD][i] * bscale;
+			I.vn[vDts][i] = dts;
+		}
+		float d = dts + I.vn[vG2][i];
+		d = fmaf(mdb, I.vn[vG][i], d);
+		I.vn[vD][i] = d;
+		v[0] += (double)d * d;
+		if (a.stage == ST_LOOP) {
+			float up = I.vn[vUp][i];
+			float uu = I.vn[vU][i] - up;
+			I.vn[vUUP][i] = uu;
+			v[1] += (double)up * up;
+			v[2] += (double)uu * uu;
+		}
+	}
+	double tot[3];
+	if (!tile_reduce<3>(I, local, I.ntn, v, tot)) return;
+	if (threadIdx.x != 0) return;
+	c.dd = tot[0];
+	if (a.stage == ST_LOOP) {
+		c.count_total++;
+		c.nrmup = sqrt(tot[1]);
+		c.relchg = sqrt(tot[2]) / c.nrmup;
+		bool brk = (c.relchg < I.tol_inn) && !c.fst;
+		c.inner_break = brk || c.count_total >= I.maxit;
+		if (!brk) c.fst = 0;
+		if (bad(c.dd)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; c.inner_break = 0; }
+	} else if (a.stage == ST_INIT) {
+		c.Q = 1; c.C = c.f;
+		c.count_outer = 0; c.count_total = 0; c.fst = 1;
+		c.active = (I.maxcnt > 0 && I.maxit > 0);
+		if (bad(c.f) || bad(c.dd)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; }
+	} else {   // ST_OUTER
+		c.need_mlp = 0; c.fst = 1; c.inner_break = 0;
+		c.gam = I.gam0; c.Q = 1; c.C = c.f;
+	}
+}
+
+// ---------------------------------------------------------------------------
+// get_tau (2d:425-453), first part.  First iteration (or restart): dDd =
+// |D d|^2 and request A d.  Otherwise Barzilai-Borwein from uup, dg, dg2.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(BLOCK) k_tau_prep(KArgs a) {
+	KPROLOGUE(a);
+	Ctrl &c = *I.ctrl;
+	const bool first = c.restart || c.fst;
+	const float mdb = (float)c.muDbeta;
+	Geo g(I);
+	double v[2] = {0, 0};
+	long long i0 = (long long)local * TILE;
+	const float *d = I.vn[vD];
+	for (int k = 0; k < TILE / BLOCK; k++) {
+		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+		if (i >= g.n) continue;
+		if (first) {
+			int x, y, z;
+			g.coords(i, x, y, z);
+			float t = dxf(d, g, i, x);
+			v[0] += (double)t * t;
+			t = dyf(d, g, i, y);
+			v[0] += (double)t * t;
+			if (g.dims == 3) { t = dzf(d, g, i, z); v[0] += (double)t * t; }
+		} else {
+			float dg = I.vn[vG][i] - I.vn[vGp][i];
+			float dg2 = I.vn[vG2][i] - I.vn[vG2p][i];
+			I.vn[vdG][i] = dg;
+			I.vn[vdG2][i] = dg2;
+			float uu = I.vn[vUUP][i];
+			float tmp = fmaf(mdb, dg, dg2);
+			v[0] += (double)uu * uu;
+			v[1] += (double)uu * tmp;
+		}
+	}
+	double tot[2];
+	if (!tile_reduce<2>(I, local, I.ntn, v, tot)) return;
+	if (threadIdx.x != 0) return;
+	if (first) {
+		c.dDd = tot[0];
+		c.need_Ad = 1;
+	} else {
+		c.tau = fabs(tot[0] / tot[1]);
+		if (bad(c.tau)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; }
+	}
+}
+
+// first-iteration step: tau = |dd / (dDd + muDbeta * |A d|^2)| (2d:430-442)
+__global__ void __launch_bounds__(BLOCK) k_tau_first(KArgs a) {
+	KPROLOGUE(a);
+	Ctrl &c = *I.ctrl;
+	double v[1] = {0};
+	long long i0 = (long long)local * TILE;
+	for (int k = 0; k < TILE / BLOCK; k++) {
+		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+		if (i < I.m) { float t = I.vm[vAd][i]; v[0] += (double)t * t; }
+	}
+	double tot[1];
+	if (!tile_reduce<1>(I, local, I.ntm, v, tot)) return;
+	if (threadIdx.x != 0) return;
+	c.tau = fabs(c.dd / (c.dDd + c.muDbeta * tot[0]));
+	c.need_Ad = 0;
+	if (bad(c.tau)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; c.restart = 0; c.need_bt = 0; }
+}
+
+// ---------------------------------------------------------------------------
+// descend (2d:481-493) with the snapshot of min_u (2d:536-537):
+//   ST_DESCEND: Up=U, gp=g, g2p=g2, U[xyz]p=U[xyz], Aup=Au; U = U - tau d
+//   ST_RESTART: U = Up - tau d (2d:565-566)
+// then nonneg (2d:455-465)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
+	KPROLOGUE(a);
+	Ctrl &c = *I.ctrl;
+	const float ntau = (float)(-1 * c.tau);
+	const bool snap = a.stage == ST_DESCEND;
+	if (local < I.ntn) {
+		long long i0 = (long long)local * TILE;
+		for (int k = 0; k < TILE / BLOCK; k++) {
+			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+			if (i >= I.n) continue;
+			float u;
+			if (snap) {
+				u = I.vn[vU][i];
+				I.vn[vUp][i] = u;
+				I.vn[vGp][i] = I.vn[vG][i];
+				I.vn[vG2p][i] = I.vn[vG2][i];
+				for (int cc = 0; cc < I.dims; cc++) I.vn[vUxp + cc][i] = I.vn[vUx + cc][i];
+			} else {
+				u = I.vn[vUp][i];
+			}
+			u = fmaf(ntau, I.vn[vD][i], u);
+			if (I.nonneg) u = u < 0.f ? 0.f : u;
+			I.vn[vU][i] = u;
+		}
+	} else if (snap) {
+		long long i0 = (long long)(local - I.ntn) * TILE;
+		for (int k = 0; k < TILE / BLOCK; k++) {
+			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+			if (i < I.m) I.vm[vAup][i] = I.vm[vAu][i];
+		}
+	}
+}
+
+// backtracking differences (2d:544,550-554)
+__global__ void __launch_bounds__(BLOCK) k_bt_diff(KArgs a) {
+	KPROLOGUE(a);
+	if (local < I.ntn) {
+		long long i0 = (long long)local * TILE;
+		for (int k = 0; k < TILE / BLOCK; k++) {
+			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+			if (i >= I.n) continue;
+			I.vn[vdU][i] = I.vn[vU][i] - I.vn[vUp][i];
+			I.vn[vdG][i] = I.vn[vG][i] - I.vn[vGp][i];
+			I.vn[vdG2][i] = I.vn[vG2][i] - I.vn[vG2p][i];
+			for (int cc = 0; cc < I.dims; cc++) I.vn[vdUx + cc][i] = I.vn[vUx + cc][i] - I.vn[vUxp + cc][i];
+		}
+	} else {
+		long long i0 = (long long)(local - I.ntn) * TILE;
+		for (int k = 0; k < TILE / BLOCK; k++) {
+			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+			if (i < I.m) I.vm[vdAu][i] = I.vm[vAu][i] - I.vm[vAup][i];
+		}
+	}
+}
+
+// one backtracking step: alpha *= gamma; update_g (2d:495-524,558-574)
+__global__ void __launch_bounds__(BLOCK) k_lerp(KArgs a) {
+	KPROLOGUE(a);
+	Ctrl &c = *I.ctrl;
+	const double alpha_new = c.alpha * I.gamma;
+	const float al = (float)alpha_new;
+	double v[4] = {0, 0, 0, 0};   // lam2, lam4, lam3, lam5
+	if (local < I.ntn) {
+		long long i0 = (long long)local * TILE;
+		for (int k = 0; k < TILE / BLOCK; k++) {
+			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+			if (i >= I.n) continue;
+			I.vn[vG][i] = fmaf(al, I.vn[vdG][i], I.vn[vGp][i]);
+			I.vn[vG2][i] = fmaf(al, I.vn[vdG2][i], I.vn[vG2p][i]);
+			I.vn[vU][i] = fmaf(al, I.vn[vdU][i], I.vn[vUp][i]);
+			for (int cc = 0; cc < I.dims; cc++) {
+				float ux = fmaf(al, I.vn[vdUx + cc][i], I.vn[vUxp + cc][i]);
+				I.vn[vUx + cc][i] = ux;
+				float vv = ux - I.vn[vWx + cc][i];
+				v[0] += (double)vv * vv;
+				v[1] += (double)I.vn[vSx + cc][i] * vv;
+			}
+		}
+	} else {
+		long long i0 = (long long)(local - I.ntn) * TILE;
+		for (int k = 0; k < TILE / BLOCK; k++) {
+			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+			if (i >= I.m) continue;
+			float au = fmaf(al, I.vm[vdAu][i], I.vm[vAup][i]);
+			I.vm[vAu][i] = au;
+			float r = au - I.vm[vB][i];
+			v[2] += (double)r * r;
+			v[3] += (double)I.vm[vDelta][i] * r;
+		}
+	}
+	double tot[4];
+	if (!tile_reduce<4>(I, local, I.ntn + I.ntm, v, tot)) return;
+	if (threadIdx.x != 0) return;
+	c.alpha = alpha_new;
+	c.bt_cnt++;
+	c.lam2 = tot[0]; c.lam4 = tot[1]; c.lam3 = tot[2]; c.lam5 = tot[3];
+	c.f = c.lam1 + c.beta / 2 * c.lam2 + c.mu / 2 * c.lam3 - c.lam4 - c.lam5;
+	bool still = fabs(c.f) > fabs(c.C - c.alpha * c.c_armij);
+	if (!still) {
+		c.need_bt = 0;
+	} else if (c.bt_cnt == 5) {   // backtracking not successful (2d:561-567)
+		c.gam *= I.rate_gam;
+		c.restart = 1;
+	}
+	if (bad(c.f)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; c.need_bt = 0; c.restart = 0; }
+}
+
+// outer stopping test (2d:820-828): RelChgOut = |U - rcdU| / nrmup; rcdU = U
+__global__ void __launch_bounds__(BLOCK) k_outer(KArgs a) {
+	KPROLOGUE(a);
+	Ctrl &c = *I.ctrl;
+	double v[1] = {0};
+	long long i0 = (long long)local * TILE;
+	for (int k = 0; k < TILE / BLOCK; k++) {
+		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+		if (i >= I.n) continue;
+		float u = I.vn[vU][i];
+		float dlt = u - I.vn[vRcd][i];
+		v[0] += (double)dlt * dlt;
+		I.vn[vRcd][i] = u;
+	}
+	double tot[1];
+	if (!tile_reduce<1>(I, local, I.ntn, v, tot)) return;
+	if (threadIdx.x != 0) return;
+	c.count_outer++;
+	c.relchg_out = sqrt(tot[0]) / c.nrmup;
+	c.inner_break = 0;
+	// after the last outer step the reference still updates the multipliers,
+	// which no longer changes U; that step is skipped here
+	if (c.relchg_out < I.tol || c.count_outer >= I.maxcnt || c.count_total >= I.maxit) c.active = 0;
+	else c.need_mlp = 1;
+}
+
+// update_mlp (2d:673-694) and the continuation step (2d:834-842)
+__global__ void __launch_bounds__(BLOCK) k_mlp(KArgs a) {
+	KPROLOGUE(a);
+	Ctrl &c = *I.ctrl;
+	const float nbeta = (float)(-1 * c.beta), nmu = (float)(-1 * c.mu);
+	double v[2] = {0, 0};   // lam4, lam5
+	if (local < I.ntn) {
+		long long i0 = (long long)local * TILE;
+		for (int k = 0; k < TILE / BLOCK; k++) {
+			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+			if (i >= I.n) continue;
+			for (int cc = 0; cc < I.dims; cc++) {
+				float vv = I.vn[vUx + cc][i] - I.vn[vWx + cc][i];
+				float s = fmaf(nbeta, vv, I.vn[vSx + cc][i]);
+				I.vn[vSx + cc][i] = s;
+				v[0] += (double)s * vv;
+			}
+		}
+	} else {
+		long long i0 = (long long)(local - I.ntn) * TILE;
+		for (int k = 0; k < TILE / BLOCK; k++) {
+			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+			if (i >= I.m) continue;
+			float r = I.vm[vAu][i] - I.vm[vB][i];
+			float dl = fmaf(nmu, r, I.vm[vDelta][i]);
+			I.vm[vDelta][i] = dl;
+			v[1] += (double)dl * r;
+		}
+	}
+	double tot[2];
+	if (!tile_reduce<2>(I, local, I.ntn + I.ntm, v, tot)) return;
+	if (threadIdx.x != 0) return;
+	c.f += (c.lam4 + c.lam5);
+	c.lam4 = tot[0]; c.lam5 = tot[1];
+	c.f -= (c.lam4 + c.lam5);
+	c.beta0 = c.beta;
+	c.beta *= I.rate_cnt;
+	c.mu *= I.rate_cnt;
+	if (c.beta > I.betaf) c.beta = I.betaf;
+	if (c.mu > I.muf) c.mu = I.muf;
+	c.muDbeta = c.mu / c.beta;
+	c.f = c.lam1 + c.beta / 2 * c.lam2 + c.mu / 2 * c.lam3 - c.lam4 - c.lam5;
+}
+
+// final scaling and rel_error (2d:855-877)
+__global__ void __launch_bounds__(BLOCK) k_final(KArgs a) {
+	KPROLOGUE(a);
+	Ctrl &c = *I.ctrl;
+	const float scl = (float)c.scl;
+	double v[2] = {0, 0};
+	long long i0 = (long long)local * TILE;
+	for (int k = 0; k < TILE / BLOCK; k++) {
+		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+		if (i >= I.n) continue;
+		float u = I.vn[vU][i] / scl;
+		I.u_user[i] = u;
+		if (I.ut_user) {
+			float t = I.ut_user[i];
+			float dlt = t - u;
+			v[0] += (double)dlt * dlt;
+			v[1] += (double)t * t;
+		}
+	}
+	double tot[2];
+	if (!tile_reduce<2>(I, local, I.ntn, v, tot)) return;
+	if (threadIdx.x != 0) return;
+	c.rel_error = I.ut_user ? sqrt(tot[0]) / sqrt(tot[1]) : 0.0;
+}
+
+// A^T-skip heuristic (2d:306-355), decision part (not forced)
+__global__ void __launch_bounds__(BLOCK) k_skip_norms(KArgs a) {
+	KPROLOGUE(a);
+	if (!I.skip_enabled) return;
+	Ctrl &c = *I.ctrl;
+	double v[2] = {0, 0};
+	long long i0 = (long long)local * TILE;
+	for (int k = 0; k < TILE / BLOCK; k++) {
+		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+		if (i >= I.m) continue;
+		float au = I.vm[vAu][i];
+		float dl = au - I.vm[vLastAu][i];
+		v[0] += (double)dl * dl;
+		v[1] += (double)au * au;
+	}
+	double tot[2];
+	if (!tile_reduce<2>(I, local, I.ntm, v, tot)) return;
+	if (threadIdx.x != 0) return;
+	double rel = sqrt(tot[0]) / sqrt(tot[1]);
+	bool mul = true;
+	if (c.currInit < I.numInit) { c.currInit++; c.currSkip = 0; }
+	else if (c.currSkip < 1) { c.currSkip += I.skipRatio; }
+	else if (rel > I.maxRelChange) { }
+	else { mul = false; c.currSkip -= 1; }
+	c.skip_adj = !mul;
+}
+
+__global__ void __launch_bounds__(BLOCK) k_copy_lastau(KArgs a) {
+	KPROLOGUE(a);
+	if (!I.skip_enabled) return;
+	long long i0 = (long long)local * TILE;
+	for (int k = 0; k < TILE / BLOCK; k++) {
+		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
+		if (i < I.m) I.vm[vLastAu][i] = I.vm[vAu][i];
+	}
+}
+
+__global__ void k_cond(const Inst *tab, int count, int pred, int *flag, unsigned long long handle,
+                       unsigned long long *launches) {
+	if (launches && threadIdx.x == 0) atomicAdd(launches, 1ull);
+	int any = 0;
+	for (int i = threadIdx.x; i < count; i += blockDim.x) any |= pred_ok(*tab[i].ctrl, pred) ? 1 : 0;
+	any = __syncthreads_or(any);
+	if (threadIdx.x == 0) {
+		*flag = any;
+		if (handle) cudaGraphSetConditional((cudaGraphConditionalHandle)handle, any ? 1u : 0u);
+	}
+}
+
+// ---------------------------------------------------------------------------
+// standalone stencils
+// ---------------------------------------------------------------------------
+struct PlainGeo {
+	int dims, p, q, r;
+};
+
+__global__ void k_D_plain(PlainGeo pg, const float *U, float *Ux, float *Uy, float *Uz) {
+	Inst I{};
+	I.dims = pg.dims; I.p = pg.p; I.q = pg.q; I.r = pg.r;
+	I.n = (long long)pg.p * pg.q * pg.r;
+	Geo g(I);
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < g.n;
+	     i += (long long)gridDim.x * blockDim.x) {
+		int x, y, z;
+		g.coords(i, x, y, z);
+		Ux[i] = dxf(U, g, i, x);
+		Uy[i] = dyf(U, g, i, y);
+		if (g.dims == 3) Uz[i] = dzf(U, g, i, z);
+	}
+}
+
+__global__ void k_Dt_plain(PlainGeo pg, const float *X, const float *Y, const float *Z, float *res) {
+	Inst I{};
+	I.dims = pg.dims; I.p = pg.p; I.q = pg.q; I.r = pg.r;
+	I.n = (long long)pg.p * pg.q * pg.r;
+	Geo g(I);
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < g.n;
+	     i += (long long)gridDim.x * blockDim.x) {
+		int x, y, z;
+		g.coords(i, x, y, z);
+		res[i] = dt_at(g, i, x, y, z, [&](long long j) { return X[j]; }, [&](long long j) { return Y[j]; },
+		               [&](long long j) { return Z ? Z[j] : 0.f; });
+	}
+}
+
+__global__ void k_shrink_plain(int dims, long long n, int iso, double beta, const float *Ux, const float *Uy,
+                               const float *Uz, const float *sx, const float *sy, const float *sz, float *Wx,
+                               float *Wy, float *Wz, double *lam1) {
+	Inst I{};
+	I.dims = dims; I.tv_norm = iso;
+	Shrink sh(I, beta);
+	double acc[1] = {0};
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+	     i += (long long)gridDim.x * blockDim.x) {
+		float u[3] = {Ux[i], Uy[i], dims == 3 ? Uz[i] : 0.f};
+		float s[3] = {sx[i], sy[i], dims == 3 ? sz[i] : 0.f};
+		float w[3];
+		acc[0] += sh.apply(u, s, w);
+		Wx[i] = w[0]; Wy[i] = w[1];
+		if (dims == 3) Wz[i] = w[2];
+	}
+	__shared__ double sm[NSUM * 32];
+	block_sums<1>(acc, sm);
+	if (threadIdx.x == 0) atomicAdd(lam1, acc[0]);
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+#define LAUNCHER(name, kern)                                                  \
+	void name(cudaStream_t s, const KArgs &a) {                               \
+		if (a.map.count <= 0) return;                                         \
+		kern<<<a.map.count, BLOCK, 0, s>>>(a);                                \
+		TG_CUDA(cudaGetLastError());                                          \
+	}
+LAUNCHER(launch_scaleb, k_scaleb)
+LAUNCHER(launch_init, k_init)
+LAUNCHER(launch_init_u, k_init_u)
+LAUNCHER(launch_D, k_D)
+LAUNCHER(launch_shrink_g2, k_shrink_g2)
+LAUNCHER(launch_getg, k_getg)
+LAUNCHER(launch_grad, k_grad)
+LAUNCHER(launch_tau_prep, k_tau_prep)
+LAUNCHER(launch_tau_first, k_tau_first)
+LAUNCHER(launch_descend, k_descend)
+LAUNCHER(launch_bt_diff, k_bt_diff)
+LAUNCHER(launch_lerp, k_lerp)
+LAUNCHER(launch_outer, k_outer)
+LAUNCHER(launch_mlp, k_mlp)
+LAUNCHER(launch_final, k_final)
+LAUNCHER(launch_skip_norms, k_skip_norms)
+LAUNCHER(launch_copy_lastau, k_copy_lastau)
+
+void launch_cond(cudaStream_t s, const Inst *tab, int count, int pred, int *flag, unsigned long long handle,
+                 unsigned long long *launches) {
+	k_cond<<<1, 128, 0, s>>>(tab, count, pred, flag, handle, launches);
+	TG_CUDA(cudaGetLastError());
+}
+
+static int grid_for(long long n) {
+	long long g = (n + 255) / 256;
+	if (g > 148 * 16) g = 148 * 16;
+	return (int)(g < 1 ? 1 : g);
+}
+
+void launch_D_plain(cudaStream_t s, int dims, int p, int q, int r, const float *U, float *Ux, float *Uy,
+                    float *Uz) {
+	PlainGeo g{dims, p, q, dims == 3 ? r : 1};
+	k_D_plain<<<grid_for((long long)p * q * g.r), 256, 0, s>>>(g, U, Ux, Uy, Uz);
+	TG_CUDA(cudaGetLastError());
+}
+
+void launch_Dt_plain(cudaStream_t s, int dims, int p, int q, int r, const float *X, const float *Y,
+                     const float *Z, float *res) {
+	PlainGeo g{dims, p, q, dims == 3 ? r : 1};
+	k_Dt_plain<<<grid_for((long long)p * q * g.r), 256, 0, s>>>(g, X, Y, Z, res);
+	TG_CUDA(cudaGetLastError());
+}
+
+void launch_shrink_plain(cudaStream_t s, int dims, long long n, int tv_norm, double beta, const float *Ux,
+                         const float *Uy, const float *Uz, const float *sx, const float *sy, const float *sz,
+                         float *Wx, float *Wy, float *Wz, double *lam1_dev) {
+	k_shrink_plain<<<grid_for(n), 256, 0, s>>>(dims, n, tv_norm, beta, Ux, Uy, Uz, sx, sy, sz, Wx, Wy, Wz,
+	                                           lam1_dev);
+	TG_CUDA(cudaGetLastError());
+}
+
+}  // namespace tval3g

@@ -1,0 +1,53 @@
+// Fused TVAL3 iteration kernels (sm_100a).  Each kernel runs over a tile map
+// (every instance of a batch in one launch), skips instances whose predicate
+// is false, and - where the reference computes inner products - reduces FP64
+// partial sums deterministically and runs the instance's scalar control step
+// in its last tile.  Reference lines: 2d = modk/tval3-cpu 2d/tval3_cpu_2d.cpp,
+// 3d = 3d/tval3_cpu_3d.cpp.
+#pragma once
+#include "engine.cuh"
+
+namespace tval3g {
+
+enum Stage { ST_INIT = 0, ST_LOOP, ST_DESCEND, ST_RESTART, ST_OUTER };
+enum TauMode { TAU_ACTIVE = 0, TAU_RESTART };
+
+struct KArgs {
+	const Inst *tab;
+	TileMap map;
+	int pred;
+	int stage;
+	unsigned long long *launches;
+};
+
+void launch_scaleb(cudaStream_t s, const KArgs &a);
+void launch_init(cudaStream_t s, const KArgs &a);
+void launch_init_u(cudaStream_t s, const KArgs &a);
+void launch_D(cudaStream_t s, const KArgs &a);
+void launch_shrink_g2(cudaStream_t s, const KArgs &a);
+void launch_getg(cudaStream_t s, const KArgs &a);
+void launch_grad(cudaStream_t s, const KArgs &a);
+void launch_tau_prep(cudaStream_t s, const KArgs &a);
+void launch_tau_first(cudaStream_t s, const KArgs &a);
+void launch_descend(cudaStream_t s, const KArgs &a);
+void launch_bt_diff(cudaStream_t s, const KArgs &a);
+void launch_lerp(cudaStream_t s, const KArgs &a);
+void launch_outer(cudaStream_t s, const KArgs &a);
+void launch_mlp(cudaStream_t s, const KArgs &a);
+void launch_final(cudaStream_t s, const KArgs &a);
+void launch_skip_norms(cudaStream_t s, const KArgs &a);
+void launch_copy_lastau(cudaStream_t s, const KArgs &a);
+// any instance with pred true -> *flag (device) and the graph conditional
+void launch_cond(cudaStream_t s, const Inst *tab, int count, int pred, int *flag,
+                 unsigned long long handle, unsigned long long *launches);
+
+// standalone stencils (C ABI helpers)
+void launch_D_plain(cudaStream_t s, int dims, int p, int q, int r, const float *U, float *Ux, float *Uy,
+                    float *Uz);
+void launch_Dt_plain(cudaStream_t s, int dims, int p, int q, int r, const float *X, const float *Y,
+                     const float *Z, float *res);
+void launch_shrink_plain(cudaStream_t s, int dims, long long n, int tv_norm, double beta, const float *Ux,
+                         const float *Uy, const float *Uz, const float *sx, const float *sy,
+                         const float *sz, float *Wx, float *Wy, float *Wz, double *lam1_dev);
+
+}  // namespace tval3g

@@ -1,0 +1,689 @@
+// Plans: validation, operator preparation, state layout and the solve program.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "plan.cuh"
+
+namespace tval3g {
+
+// ---------------------------------------------------------------------------
+// validation (2d/tval3_cpu_2d.cpp:696-750, 3d/tval3_cpu_3d.cpp:1028-1165)
+// ---------------------------------------------------------------------------
+long long validate(const tval3g_problem &p, long long b_len, long long ut_len) {
+	TG_ARG(p.dims == 2 || p.dims == 3, "Argument error: dims must be 2 or 3");
+	TG_ARG(p.dim_x >= 1 && p.dim_y >= 1 && (p.dims == 2 || p.dim_z >= 1),
+	       "Argument error: image dimensions must be positive");
+	const long long n = (long long)p.dim_x * p.dim_y * (p.dims == 3 ? p.dim_z : 1);
+	TG_ARG(n < (1LL << 31), "Argument error: the image has more than 2^31-1 elements");
+	TG_ARG(ut_len == 0 || ut_len == n, "Argument error: U and Ut must have the same size!");
+	TG_ARG(b_len >= 1, "Argument error: b must not be empty");
+	switch (p.op_kind) {
+	case TVAL3G_OP_DENSE:
+	case TVAL3G_OP_CSR: {
+		const int layers = p.dims == 3 ? 1 : p.layers;
+		TG_ARG(p.m >= 1 && p.n_cols >= 1, "Argument error: A must not be empty");
+		if (p.dims == 2) {
+			TG_ARG(n == (long long)p.n_cols * layers,
+			       "Argument error: the length of U must be equal to A.dim_x * layers!");
+			TG_ARG(b_len == (long long)p.m * layers, "Argument error: b.len must be equal to A.dim_y * layers!");
+		} else {
+			TG_ARG(n == p.n_cols, "Argument error: the length of U must be equal to A.dim_x!");
+			TG_ARG(b_len == p.m, "Argument error: b.len must be equal to A.dim_y!");
+		}
+		if (p.op_kind == TVAL3G_OP_DENSE) TG_ARG(p.A != nullptr, "Argument error: A is NULL");
+		else
+			TG_ARG(p.csr_ptr && (p.nnz == 0 || (p.csr_ind && p.csr_val)) && p.nnz >= 0 && p.nnz < (1LL << 31),
+			       "Argument error: A must be available in CSR and CSC format!");
+		break;
+	}
+	case TVAL3G_OP_RAY2D:
+		TG_ARG(p.dims == 2, "Argument error: 2D ray geometry needs a 2D image");
+		TG_ARG(p.layers <= 1,
+		       "Argument error: multilayer reconstruction with dynamic calculation is not supported!");
+		TG_ARG(b_len == (long long)p.num_emitters * p.num_receivers,
+		       "Argument error: b.len must be equal to A.num_emitters * A.num_receivers!");
+		TG_ARG(p.use_path && p.x_emitters && p.y_emitters && p.x_receivers && p.y_receivers,
+		       "Argument error: incomplete ray geometry");
+		TG_ARG(p.ld >= 1 && p.ld < 32768, "Argument error: geometry ld must be in [1, 32767]");
+		break;
+	case TVAL3G_OP_RAY3D:
+		TG_ARG(p.dims == 3, "Argument error: 3D ray geometry needs a 3D image");
+		TG_ARG(b_len == (long long)p.numPaths * p.numMPs,
+		       "Argument error: b.len must be equal to A.num_emitters * A.num_receivers!");
+		TG_ARG(p.use_path && p.x_emitters && p.y_emitters && p.z_emitters && p.x_receivers && p.y_receivers &&
+		           p.z_receivers && p.numMPs >= 1,
+		       "Argument error: incomplete ray geometry");
+		TG_ARG(p.rv_x >= 1 && p.rv_y >= 1 && p.rv_z >= 1 && p.rv_x < 32768 && p.rv_y < 32768 && p.rv_z < 32768,
+		       "Argument error: geometry rv_x, rv_y, rv_z must be in [1, 32767]");
+		TG_ARG((long long)p.rv_x * p.rv_y * p.rv_z <= n, "Argument error: the geometry volume exceeds U");
+		break;
+	default:
+		throw Error{TVAL3G_ERR_ARGUMENT, "Argument error: unknown operator kind"};
+	}
+	if (p.op_kind == TVAL3G_OP_RAY2D || p.op_kind == TVAL3G_OP_RAY3D) {
+		// every traced ray must stay inside the image (Bresenham stays inside
+		// the bounding box of its endpoints); the reference does not check
+		const bool is3 = p.op_kind == TVAL3G_OP_RAY3D;
+		const int E = p.num_emitters, R = p.num_receivers, nmp = is3 ? p.numMPs : 1;
+		const long long ny = is3 ? 0 : n / p.ld;
+		for (int mp = 0; mp < nmp; mp++)
+			for (int e = 0; e < E; e++)
+				for (int r = 0; r < R; r++) {
+					const int up = p.use_path[(long long)e * R + r];
+					if (up == 0) continue;
+					if (!is3) {
+						const int x0 = p.x_emitters[e], y0 = p.y_emitters[e], x1 = p.x_receivers[r], y1 = p.y_receivers[r];
+						TG_ARG(x0 >= 0 && x0 < p.ld && x1 >= 0 && x1 < p.ld && y0 >= 0 && y0 < ny && y1 >= 0 && y1 < ny,
+						       "Argument error: a ray endpoint lies outside the image");
+					} else {
+						const long long ie = (long long)mp * E + e, ir = (long long)mp * R + r;
+						const int x0 = p.x_emitters[ie], y0 = p.y_emitters[ie], z0 = p.z_emitters[ie];
+						const int x1 = p.x_receivers[ir], y1 = p.y_receivers[ir], z1 = p.z_receivers[ir];
+						TG_ARG(x0 >= 0 && x0 < p.rv_x && x1 >= 0 && x1 < p.rv_x && y0 >= 0 && y0 < p.rv_y && y1 >= 0 &&
+						           y1 < p.rv_y && z0 >= 0 && z0 < p.rv_z && z1 >= 0 && z1 < p.rv_z,
+						       "Argument error: a ray endpoint lies outside the volume");
+						TG_ARG(up >= 1 && up <= p.numPaths, "Argument error: use_path index exceeds numPaths");
+					}
+				}
+	}
+	return n;
+}
+
+void check_options(const tval3g_options &o) {
+	TG_ARG(o.beta > 0 && o.beta0 > 0 && o.mu > 0 && o.mu0 > 0, "Argument error: mu, beta, mu0, beta0 must be positive");
+	TG_ARG(o.tv_norm == TVAL3G_TV_ANISO || o.tv_norm == TVAL3G_TV_ISO, "Argument error: tv_norm must be 0 or 1");
+	TG_ARG(o.maxit >= 0 && o.maxcnt >= 0, "Argument error: maxit and maxcnt must be >= 0");
+}
+
+// ---------------------------------------------------------------------------
+// operators
+// ---------------------------------------------------------------------------
+template <class T>
+static T *dcopy(cudaStream_t s, OpStore &st, const T *src, long long count, bool borrow) {
+	if (borrow) return const_cast<T *>(src);
+	T *d = nullptr;
+	size_t bytes = sizeof(T) * (size_t)std::max(count, 1LL);
+	TG_CUDA(cudaMalloc(&d, bytes));
+	st.owned.push_back(d);
+	st.bytes += (long long)bytes;
+	if (count > 0) TG_CUDA(cudaMemcpyAsync(d, src, sizeof(T) * (size_t)count, cudaMemcpyHostToDevice, s));
+	return d;
+}
+template <class T>
+static T *dalloc_op(OpStore &st, long long count) {
+	T *d = nullptr;
+	TG_CUDA(cudaMalloc(&d, sizeof(T) * (size_t)std::max(count, 1LL)));
+	st.owned.push_back(d);
+	st.bytes += (long long)(sizeof(T) * (size_t)std::max(count, 1LL));
+	return d;
+}
+
+__global__ void k_map_out(long long nnz, const int4 *rays, int *cind) {
+	long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (k < nnz) cind[k] = rays[cind[k]].w;
+}
+
+void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st, bool keep_ray_csr) {
+	OpDev &d = st.dev;
+	d = OpDev{};
+	d.kind = p.op_kind;
+	d.layers = (p.dims == 2 && (p.op_kind == TVAL3G_OP_DENSE || p.op_kind == TVAL3G_OP_CSR)) ? p.layers : 1;
+	const long long n = (long long)p.dim_x * p.dim_y * (p.dims == 3 ? p.dim_z : 1);
+	const bool borrow = (flags & TVAL3G_DEVICE_INPUTS) != 0;
+	d.scale = 1.f;
+	if (p.op_kind == TVAL3G_OP_DENSE) {
+		d.m = p.m; d.n = p.n_cols;
+		d.A = dcopy(s, st, p.A, (long long)p.m * p.n_cols, borrow);
+		st.b_len = (long long)p.m * d.layers;
+	} else if (p.op_kind == TVAL3G_OP_CSR) {
+		d.m = p.m; d.n = p.n_cols;
+		st.nnz = p.nnz;
+		if (!borrow) {   // host arrays can be checked here (the reference trusts them)
+			TG_ARG(p.csr_ptr[0] == 0 && p.csr_ptr[p.m] == p.nnz, "Argument error: CSR row pointers are inconsistent");
+			for (int i = 0; i < p.m; i++)
+				TG_ARG(p.csr_ptr[i + 1] >= p.csr_ptr[i], "Argument error: CSR row pointers are not monotone");
+			for (long long k = 0; k < p.nnz; k++)
+				TG_ARG(p.csr_ind[k] >= 0 && p.csr_ind[k] < p.n_cols, "Argument error: CSR column index out of range");
+		}
+		d.rptr = dcopy(s, st, p.csr_ptr, (long long)p.m + 1, borrow);
+		d.rind = dcopy(s, st, p.csr_ind, p.nnz, borrow);
+		d.rval = dcopy(s, st, p.csr_val, p.nnz, borrow);
+		int *cptr = dalloc_op<int>(st, d.n + 1);
+		int *cind = dalloc_op<int>(st, p.nnz);
+		float *cval = dalloc_op<float>(st, p.nnz);
+		build_transpose(s, d.m, d.n, p.nnz, d.rptr, d.rind, d.rval, cptr, cind, cval);
+		d.cptr = cptr; d.cind = cind; d.cval = cval;
+		st.b_len = (long long)p.m * d.layers;
+	} else {
+		// traced rays in the reference's loop order (mp, emitter, receiver)
+		std::vector<int4> rays;
+		const bool is3 = p.op_kind == TVAL3G_OP_RAY3D;
+		const int E = p.num_emitters, R = p.num_receivers, nmp = is3 ? p.numMPs : 1;
+		const long long mtot = is3 ? (long long)p.numPaths * p.numMPs : (long long)E * R;
+		const int ny = is3 ? 0 : (int)std::min<long long>(n / p.ld, 32767);
+		st.ray_out.clear();
+		for (int mp = 0; mp < nmp; mp++)
+			for (int e = 0; e < E; e++)
+				for (int r = 0; r < R; r++) {
+					const int up = p.use_path[(long long)e * R + r];
+					if (up == 0) continue;
+					int x0, y0, z0 = 0, x1, y1, z1 = 0;
+					long long out;
+					if (!is3) {
+						x0 = p.x_emitters[e]; y0 = p.y_emitters[e];
+						x1 = p.x_receivers[r]; y1 = p.y_receivers[r];
+						TG_ARG(x0 >= 0 && x0 < p.ld && x1 >= 0 && x1 < p.ld && y0 >= 0 && y0 < ny && y1 >= 0 && y1 < ny,
+						       "Argument error: a ray endpoint lies outside the image");
+						out = (long long)e * R + r;
+					} else {
+						const long long ie = (long long)mp * E + e, ir = (long long)mp * R + r;
+						x0 = p.x_emitters[ie]; y0 = p.y_emitters[ie]; z0 = p.z_emitters[ie];
+						x1 = p.x_receivers[ir]; y1 = p.y_receivers[ir]; z1 = p.z_receivers[ir];
+						TG_ARG(x0 >= 0 && x0 < p.rv_x && x1 >= 0 && x1 < p.rv_x && y0 >= 0 && y0 < p.rv_y && y1 >= 0 &&
+						           y1 < p.rv_y && z0 >= 0 && z0 < p.rv_z && z1 >= 0 && z1 < p.rv_z,
+						       "Argument error: a ray endpoint lies outside the volume");
+						out = (long long)mp * p.numPaths + up - 1;
+						TG_ARG(up >= 1 && out < mtot, "Argument error: use_path index exceeds numPaths");
+					}
+					rays.push_back(pack_ray(x0, y0, z0, x1 - x0, y1 - y0, z1 - z0, (int)out));
+					st.ray_out.push_back((int)out);
+				}
+		TG_ARG(rays.size() < (1u << 31), "Argument error: too many rays");
+		d.nrays = (int)rays.size();
+		d.m = mtot; d.n = n;
+		d.rvx = is3 ? p.rv_x : p.ld;
+		d.rvy = is3 ? p.rv_y : 1;
+		d.scale = p.scale_factor;
+		int4 *drays = dalloc_op<int4>(st, d.nrays);
+		if (d.nrays > 0)
+			TG_CUDA(cudaMemcpyAsync(drays, rays.data(), sizeof(int4) * rays.size(), cudaMemcpyHostToDevice, s));
+		d.rays = drays;
+		// forward CSR over traced rays, then its transpose: the pixel-major
+		// index of the adjoint, entries = measurement indices sorted by ray
+		int *rptr = dalloc_op<int>(st, (long long)d.nrays + 1);
+		long long total = 0;
+		trace_rays(s, d.nrays, drays, d.rvx, d.rvy, rptr, nullptr, &total);
+		int *rind = dalloc_op<int>(st, total);
+		trace_rays(s, d.nrays, drays, d.rvx, d.rvy, rptr, rind, &total);
+		st.nnz = total;
+		int *cptr = dalloc_op<int>(st, n + 1);
+		int *cind = dalloc_op<int>(st, total);
+		build_transpose(s, d.nrays, n, total, rptr, rind, nullptr, cptr, cind, nullptr);
+		if (total > 0) k_map_out<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, drays, cind);
+		TG_CUDA(cudaGetLastError());
+		d.cptr = cptr; d.cind = cind; d.cval = nullptr;
+		st.ray_rptr = rptr; st.ray_rind = rind;
+		st.b_len = mtot;
+		if (!keep_ray_csr) {
+			TG_CUDA(cudaStreamSynchronize(s));
+			for (void *&q : st.owned)
+				if (q == rptr || q == rind) { cudaFree(q); q = nullptr; }
+			st.ray_rptr = st.ray_rind = nullptr;
+		}
+	}
+}
+
+void free_op(OpStore &st) {
+	for (void *q : st.owned)
+		if (q) cudaFree(q);
+	st.owned.clear();
+}
+
+// ---------------------------------------------------------------------------
+// tile maps
+// ---------------------------------------------------------------------------
+struct TileBuilder {
+	std::vector<int2> all;
+	struct Pending { TileMap *map; size_t off; size_t cnt; };
+	std::vector<Pending> pend;
+	std::vector<int2> cur;
+	void add(int inst, long long tiles) {
+		for (long long t = 0; t < tiles; t++) cur.push_back(make_int2(inst, (int)t));
+	}
+	void close(TileMap *m) {
+		pend.push_back({m, all.size(), cur.size()});
+		all.insert(all.end(), cur.begin(), cur.end());
+		cur.clear();
+	}
+	int2 *upload(cudaStream_t s) {
+		int2 *d = nullptr;
+		TG_CUDA(cudaMalloc(&d, sizeof(int2) * std::max<size_t>(all.size(), 1)));
+		if (!all.empty())
+			TG_CUDA(cudaMemcpyAsync(d, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, s));
+		for (auto &p : pend) {
+			p.map->tiles = d + p.off;
+			p.map->count = (int)p.cnt;
+		}
+		return d;
+	}
+};
+
+static int subwarp_for(double avg) {
+	if (avg >= 48) return 32;
+	if (avg >= 20) return 16;
+	if (avg >= 8) return 8;
+	return 4;
+}
+
+// operator tile maps of a batch; returns the dense partial buffer size (floats)
+static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStore> &ops, TileBuilder &tb,
+                               OpBatch &ob) {
+	const int cnt = (int)inst.size();
+	long long dense_part = 0;
+	// dense
+	for (int i = 0; i < cnt; i++) {
+		OpDev &d = inst[i].op;
+		if (d.kind != TVAL3G_OP_DENSE) continue;
+		tb.add(i, d.layers * ((d.m + WARPS - 1) / WARPS));
+	}
+	tb.close(&ob.dense_fwd);
+	for (int i = 0; i < cnt; i++) {
+		OpDev &d = inst[i].op;
+		if (d.kind != TVAL3G_OP_DENSE) continue;
+		long long ct = (d.n + 1023) / 1024;
+		long long K = (4 * 148 + d.layers * ct - 1) / (d.layers * ct);
+		K = std::max(1LL, std::min(K, d.m));
+		d.dense_kchunks = (int)K;
+		d.dense_part = dense_part;
+		dense_part += d.layers * K * d.n;
+		tb.add(i, d.layers * ct * K);
+	}
+	tb.close(&ob.dense_adj);
+	for (int i = 0; i < cnt; i++) {
+		OpDev &d = inst[i].op;
+		if (d.kind != TVAL3G_OP_DENSE) continue;
+		tb.add(i, d.layers * ((d.n + 1023) / 1024));
+	}
+	tb.close(&ob.dense_red);
+	// compressed gathers: each instance in the width class of its own mean
+	// line length (lines per block = 256 / width)
+	static const int widths[4] = {4, 8, 16, 32};
+	auto cls = [](double avg) {
+		int w = subwarp_for(avg);
+		return w == 4 ? 0 : w == 8 ? 1 : w == 16 ? 2 : 3;
+	};
+	for (int c = 0; c < 4; c++) {
+		for (int i = 0; i < cnt; i++) {
+			const OpDev &d = inst[i].op;
+			if (d.kind != TVAL3G_OP_CSR || cls((double)ops[i].nnz / d.m) != c) continue;
+			long long lpb = 256 / widths[c];
+			tb.add(i, d.layers * ((d.m + lpb - 1) / lpb));
+		}
+		tb.close(&ob.csr_fwd[c]);
+		for (int i = 0; i < cnt; i++) {
+			const OpDev &d = inst[i].op;
+			if (d.kind != TVAL3G_OP_CSR || cls((double)ops[i].nnz / d.n) != c) continue;
+			long long lpb = 256 / widths[c];
+			tb.add(i, d.layers * ((d.n + lpb - 1) / lpb));
+		}
+		tb.close(&ob.csc_adj[c]);
+		for (int i = 0; i < cnt; i++) {
+			const OpDev &d = inst[i].op;
+			if ((d.kind != TVAL3G_OP_RAY2D && d.kind != TVAL3G_OP_RAY3D) || cls((double)ops[i].nnz / inst[i].n) != c)
+				continue;
+			long long lpb = 256 / widths[c];
+			tb.add(i, (inst[i].n + lpb - 1) / lpb);
+		}
+		tb.close(&ob.ray_adj[c]);
+	}
+	for (int i = 0; i < cnt; i++) {
+		const OpDev &d = inst[i].op;
+		if (d.kind != TVAL3G_OP_RAY2D && d.kind != TVAL3G_OP_RAY3D) continue;
+		tb.add(i, (d.nrays + WARPS - 1) / WARPS);
+	}
+	tb.close(&ob.ray_fwd);
+	return dense_part;
+}
+
+long long build_op_maps_upload(std::vector<Inst> &inst, const std::vector<OpStore> &ops, OpBatch &ob,
+                               int2 **d_tiles, cudaStream_t s) {
+	TileBuilder tb;
+	long long dense_part = build_op_maps(inst, ops, tb, ob);
+	*d_tiles = tb.upload(s);
+	return dense_part;
+}
+
+// ---------------------------------------------------------------------------
+// Plan
+// ---------------------------------------------------------------------------
+void *Plan::dalloc(size_t bytes) {
+	void *p = nullptr;
+	TG_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+	allocs_.push_back(p);
+	device_bytes_ += (long long)bytes;
+	return p;
+}
+
+Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, int flags)
+	: count_(count), flags_(flags), graph_mode_((flags & TVAL3G_GRAPH) != 0) {
+	TG_ARG(count >= 1, "Argument error: count must be >= 1");
+	int dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess) throw Error{TVAL3G_ERR_NO_DEVICE, "no CUDA device"};
+	for (int i = 0; i < count; i++) check_options(opts[i]);
+	TG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+	ops_.resize(count);
+	h_inst_.assign(count, Inst{});
+	try {
+		// operators and sizes
+		for (int i = 0; i < count; i++) {
+			const tval3g_problem &p = probs[i];
+			long long b_len = (p.op_kind == TVAL3G_OP_RAY2D) ? (long long)p.num_emitters * p.num_receivers
+			                  : (p.op_kind == TVAL3G_OP_RAY3D) ? (long long)p.numPaths * p.numMPs
+			                  : (long long)p.m * (p.dims == 3 ? 1 : p.layers);
+			long long n = validate(p, b_len, 0);
+			prepare_op(stream_, p, flags, ops_[i], false);
+			Inst &I = h_inst_[i];
+			I.dims = p.dims; I.p = p.dim_y; I.q = p.dim_x; I.r = p.dims == 3 ? p.dim_z : 1;
+			I.n = n; I.m = b_len;
+			I.ntn = (int)((n + TILE - 1) / TILE);
+			I.ntm = (int)((b_len + TILE - 1) / TILE);
+			const tval3g_options &o = opts[i];
+			I.muf = o.mu; I.betaf = o.beta; I.mu0 = o.mu0; I.beta0 = o.beta0; I.tol = o.tol; I.tol_inn = o.tol_inn;
+			I.c = o.c; I.gamma = o.gamma; I.gam0 = o.gam; I.rate_gam = o.rate_gam; I.rate_cnt = o.rate_cnt;
+			I.skipRatio = o.skipMulRatio; I.maxRelChange = o.maxRelativeChange;
+			I.maxit = o.maxit; I.maxcnt = o.maxcnt; I.nonneg = o.nonneg != 0; I.tv_norm = o.tv_norm;
+			I.numInit = o.numInitIterations;
+			I.skip_enabled = (o.skipMulRatio != 0 && p.op_kind != TVAL3G_OP_DENSE);
+			any_skip_ |= I.skip_enabled != 0;
+			I.op = ops_[i].dev;
+		}
+		// vectors: one arena, every vector 256-byte aligned
+		long long total = 0;
+		std::vector<long long> base(count);
+		for (int i = 0; i < count; i++) {
+			long long np = (h_inst_[i].n + 63) / 64 * 64, mp = (h_inst_[i].m + 63) / 64 * 64;
+			base[i] = total;
+			total += NVN * np + NVM * mp;
+		}
+		d_arena_ = (float *)dalloc(sizeof(float) * (size_t)total);
+		long long parts = 0;
+		for (int i = 0; i < count; i++) parts += (long long)(h_inst_[i].ntn + h_inst_[i].ntm) * NSUM;
+		d_part_ = (double *)dalloc(sizeof(double) * (size_t)parts);
+		d_ctrl_ = (Ctrl *)dalloc(sizeof(Ctrl) * count);
+		TG_CUDA(cudaMemsetAsync(d_ctrl_, 0, sizeof(Ctrl) * count, stream_));
+		long long poff = 0;
+		for (int i = 0; i < count; i++) {
+			Inst &I = h_inst_[i];
+			long long np = (I.n + 63) / 64 * 64, mp = (I.m + 63) / 64 * 64;
+			float *b0 = d_arena_ + base[i];
+			for (int v = 0; v < NVN; v++) I.vn[v] = b0 + v * np;
+			for (int v = 0; v < NVM; v++) I.vm[v] = b0 + NVN * np + v * mp;
+			I.ctrl = d_ctrl_ + i;
+			I.part = d_part_ + poff;
+			poff += (long long)(I.ntn + I.ntm) * NSUM;
+		}
+		// tile maps
+		TileBuilder tb;
+		for (int i = 0; i < count; i++) tb.add(i, h_inst_[i].ntn);
+		tb.close(&maps_[MAP_N]);
+		for (int i = 0; i < count; i++) tb.add(i, h_inst_[i].ntm);
+		tb.close(&maps_[MAP_M]);
+		for (int i = 0; i < count; i++) tb.add(i, h_inst_[i].ntn + h_inst_[i].ntm);
+		tb.close(&maps_[MAP_NM]);
+		long long dense_part = build_op_maps(h_inst_, ops_, tb, ob_);
+		d_tiles_ = tb.upload(stream_);
+		allocs_.push_back(d_tiles_);
+		if (dense_part > 0) ob_.dense_part = (float *)dalloc(sizeof(float) * (size_t)dense_part);
+		d_inst_ = (Inst *)dalloc(sizeof(Inst) * count);
+		TG_CUDA(cudaMemcpyAsync(d_inst_, h_inst_.data(), sizeof(Inst) * count, cudaMemcpyHostToDevice, stream_));
+		d_flag_ = (int *)dalloc(sizeof(int));
+		d_launches_ = (unsigned long long *)dalloc(sizeof(unsigned long long));
+		TG_CUDA(cudaMallocHost(&h_flag_, sizeof(int)));
+		for (auto &o : ops_) device_bytes_ += o.bytes;
+		TG_CUDA(cudaStreamSynchronize(stream_));
+	} catch (...) {
+		release();
+		throw;
+	}
+}
+
+Plan::~Plan() { release(); }
+
+void Plan::release() {
+	if (exec_) cudaGraphExecDestroy(exec_);
+	if (graph_) cudaGraphDestroy(graph_);
+	exec_ = nullptr; graph_ = nullptr;
+	if (cap_) cudaStreamDestroy(cap_);
+	cap_ = nullptr;
+	if (stream_) cudaStreamSynchronize(stream_);
+	for (void *p : allocs_) cudaFree(p);
+	allocs_.clear();
+	for (auto &o : ops_) free_op(o);
+	ops_.clear();
+	if (h_flag_) cudaFreeHost(h_flag_);
+	h_flag_ = nullptr;
+	if (stream_) cudaStreamDestroy(stream_);
+	stream_ = nullptr;
+}
+
+KArgs Plan::kargs(MapKind mk, int pred, int stage) const {
+	KArgs a;
+	a.tab = d_inst_;
+	a.map = maps_[mk];
+	a.pred = pred;
+	a.stage = stage;
+	a.launches = d_launches_;
+	return a;
+}
+
+LaunchCtx Plan::lctx() const {
+	LaunchCtx L;
+	L.stream = es();
+	L.inst = d_inst_;
+	L.launches = (long long *)d_launches_;
+	return L;
+}
+
+// --- control flow -----------------------------------------------------------
+void Plan::seg_begin() {
+	Frame &f = frames_.back();
+	TG_CUDA(cudaStreamBeginCaptureToGraph(cap_, f.g, f.deps.empty() ? nullptr : f.deps.data(), nullptr,
+	                                      f.deps.size(), cudaStreamCaptureModeRelaxed));
+	capturing_ = true;
+}
+
+void Plan::seg_end() {
+	Frame &f = frames_.back();
+	cudaStreamCaptureStatus st;
+	const cudaGraphNode_t *deps = nullptr;
+	size_t nd = 0;
+	TG_CUDA(cudaStreamGetCaptureInfo(cap_, &st, nullptr, nullptr, &deps, &nd));
+	std::vector<cudaGraphNode_t> d(deps, deps + nd);
+	cudaGraph_t g;
+	TG_CUDA(cudaStreamEndCapture(cap_, &g));
+	f.deps = d;
+	capturing_ = false;
+}
+
+void Plan::if_(int pred, const std::function<void()> &body) {
+	if (!graph_mode_) {
+		launch_cond(cur_, d_inst_, count_, pred, d_flag_, 0, d_launches_);
+		TG_CUDA(cudaMemcpyAsync(h_flag_, d_flag_, sizeof(int), cudaMemcpyDeviceToHost, cur_));
+		TG_CUDA(cudaStreamSynchronize(cur_));
+		if (*h_flag_) body();
+		return;
+	}
+	cudaGraphConditionalHandle h;
+	TG_CUDA(cudaGraphConditionalHandleCreate(&h, frames_.back().g, 0, cudaGraphCondAssignDefault));
+	launch_cond(cap_, d_inst_, count_, pred, d_flag_, (unsigned long long)h, d_launches_);
+	seg_end();
+	alignas(cudaGraphNodeParams) unsigned char np_raw[sizeof(cudaGraphNodeParams)] = {};
+	cudaGraphNodeParams &np = *reinterpret_cast<cudaGraphNodeParams *>(np_raw);
+	np.type = cudaGraphNodeTypeConditional;
+	np.conditional.handle = h;
+	np.conditional.type = cudaGraphCondTypeIf;
+	np.conditional.size = 1;
+	cudaGraphNode_t node;
+	{
+		Frame &f = frames_.back();
+		TG_CUDA(cudaGraphAddNode(&node, f.g, f.deps.empty() ? nullptr : f.deps.data(), f.deps.size(), &np));
+	}
+	frames_.push_back(Frame{np.conditional.phGraph_out[0], {}});
+	seg_begin();
+	body();
+	seg_end();
+	frames_.pop_back();
+	frames_.back().deps.assign(1, node);
+	seg_begin();
+}
+
+void Plan::while_(int pred, const std::function<void()> &body) {
+	if (!graph_mode_) {
+		for (;;) {
+			launch_cond(cur_, d_inst_, count_, pred, d_flag_, 0, d_launches_);
+			TG_CUDA(cudaMemcpyAsync(h_flag_, d_flag_, sizeof(int), cudaMemcpyDeviceToHost, cur_));
+			TG_CUDA(cudaStreamSynchronize(cur_));
+			if (!*h_flag_) break;
+			body();
+		}
+		return;
+	}
+	cudaGraphConditionalHandle h;
+	TG_CUDA(cudaGraphConditionalHandleCreate(&h, frames_.back().g, 0, cudaGraphCondAssignDefault));
+	launch_cond(cap_, d_inst_, count_, pred, d_flag_, (unsigned long long)h, d_launches_);
+	seg_end();
+	alignas(cudaGraphNodeParams) unsigned char np_raw[sizeof(cudaGraphNodeParams)] = {};
+	cudaGraphNodeParams &np = *reinterpret_cast<cudaGraphNodeParams *>(np_raw);
+	np.type = cudaGraphNodeTypeConditional;
+	np.conditional.handle = h;
+	np.conditional.type = cudaGraphCondTypeWhile;
+	np.conditional.size = 1;
+	cudaGraphNode_t node;
+	{
+		Frame &f = frames_.back();
+		TG_CUDA(cudaGraphAddNode(&node, f.g, f.deps.empty() ? nullptr : f.deps.data(), f.deps.size(), &np));
+	}
+	frames_.push_back(Frame{np.conditional.phGraph_out[0], {}});
+	seg_begin();
+	body();
+	launch_cond(cap_, d_inst_, count_, pred, d_flag_, (unsigned long long)h, d_launches_);
+	seg_end();
+	frames_.pop_back();
+	frames_.back().deps.assign(1, node);
+	seg_begin();
+}
+
+// --- the program (2d/tval3_cpu_2d.cpp:752-886) ---------------------------------
+void Plan::emit_program() {
+	cudaStream_t s = es();
+	const LaunchCtx L = lctx();
+	const VecSel U{false, vU}, Atb{false, vAtb}, G{false, vG}, D{false, vD};
+	const VecSel B{true, vB}, Au{true, vAu}, Ad{true, vAd};
+	// initialisation: scaleb, Atb = A'b, U = Atb, D, shrinkage, get_g, gradient
+	launch_scaleb(s, kargs(MAP_M, P_ALL));
+	launch_init(s, kargs(MAP_NM, P_ALL));
+	op_adjoint(L, ob_, P_ALL, B, Atb);
+	launch_init_u(s, kargs(MAP_N, P_ALL));
+	launch_D(s, kargs(MAP_N, P_ALL));
+	launch_shrink_g2(s, kargs(MAP_N, P_ALL, ST_INIT));
+	op_forward(L, ob_, P_ALL, U, Au);
+	if (any_skip_) launch_copy_lastau(s, kargs(MAP_M, P_ALL));
+	op_adjoint(L, ob_, P_ALL, Au, G);
+	launch_getg(s, kargs(MAP_NM, P_ALL, ST_INIT));
+	launch_grad(s, kargs(MAP_N, P_ALL, ST_INIT));
+	(void)D; (void)Ad;
+	while_(P_ACTIVE, [&] { emit_iteration(); });
+	launch_final(es(), kargs(MAP_N, P_ALL));
+}
+
+void Plan::emit_iteration() {
+	const LaunchCtx L = lctx();
+	cudaStream_t s = es();
+	const VecSel U{false, vU}, G{false, vG}, D{false, vD};
+	const VecSel Au{true, vAu}, Ad{true, vAd};
+	// min_u (2d:526-576): step length
+	launch_tau_prep(s, kargs(MAP_N, P_ACTIVE));
+	if_(P_NEED_AD, [&] {
+		op_forward(lctx(), ob_, P_NEED_AD, D, Ad);
+		launch_tau_first(es(), kargs(MAP_M, P_NEED_AD));
+	});
+	// descent step and get_g
+	launch_descend(es(), kargs(MAP_NM, P_ACTIVE, ST_DESCEND));
+	launch_D(es(), kargs(MAP_N, P_ACTIVE));
+	op_forward(lctx(), ob_, P_ACTIVE, U, Au);
+	if (any_skip_) {
+		launch_skip_norms(es(), kargs(MAP_M, P_ACTIVE));
+		launch_copy_lastau(es(), kargs(MAP_M, P_ACTIVE_MUL));
+	}
+	op_adjoint(lctx(), ob_, P_ACTIVE_MUL, Au, G);
+	launch_getg(es(), kargs(MAP_NM, P_ACTIVE, ST_DESCEND));
+	// nonmonotone Armijo backtracking, restart after five failures
+	if_(P_NEED_BT, [&] {
+		launch_bt_diff(es(), kargs(MAP_NM, P_NEED_BT));
+		while_(P_NEED_BT, [&] { launch_lerp(es(), kargs(MAP_NM, P_NEED_BT)); });
+		if_(P_RESTART, [&] {
+			launch_tau_prep(es(), kargs(MAP_N, P_RESTART));
+			op_forward(lctx(), ob_, P_NEED_AD, D, Ad);
+			launch_tau_first(es(), kargs(MAP_M, P_NEED_AD));
+			launch_descend(es(), kargs(MAP_NM, P_RESTART, ST_RESTART));
+			launch_D(es(), kargs(MAP_N, P_RESTART));
+			op_forward(lctx(), ob_, P_RESTART, U, Au);
+			if (any_skip_) launch_copy_lastau(es(), kargs(MAP_M, P_RESTART));
+			op_adjoint(lctx(), ob_, P_RESTART, Au, G);
+			launch_getg(es(), kargs(MAP_NM, P_RESTART, ST_RESTART));
+		});
+	});
+	// update_W, reference values, gradient, inner stopping test
+	launch_shrink_g2(es(), kargs(MAP_N, P_ACTIVE, ST_LOOP));
+	launch_grad(es(), kargs(MAP_N, P_ACTIVE, ST_LOOP));
+	// outer step: stopping test, multipliers, continuation
+	if_(P_INNER_BREAK, [&] {
+		launch_outer(es(), kargs(MAP_N, P_INNER_BREAK));
+		launch_mlp(es(), kargs(MAP_NM, P_NEED_MLP));
+		launch_grad(es(), kargs(MAP_N, P_NEED_MLP, ST_OUTER));
+	});
+	(void)L; (void)s;
+}
+
+void Plan::build_graph() {
+	TG_CUDA(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking));
+	TG_CUDA(cudaGraphCreate(&graph_, 0));
+	frames_.clear();
+	frames_.push_back(Frame{graph_, {}});
+	seg_begin();
+	emit_program();
+	seg_end();
+	frames_.clear();
+	TG_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
+}
+
+void Plan::solve(const float *const *d_b, const float *const *d_Ut, float *const *d_U, tval3g_info *info,
+                 cudaStream_t stream) {
+	auto t0 = std::chrono::steady_clock::now();
+	cur_ = stream ? stream : stream_;
+	for (int i = 0; i < count_; i++) {
+		TG_ARG(d_b && d_b[i] && d_U && d_U[i], "Argument error: b and U must not be NULL");
+		h_inst_[i].b_user = d_b[i];
+		h_inst_[i].ut_user = d_Ut ? d_Ut[i] : nullptr;
+		h_inst_[i].u_user = d_U[i];
+	}
+	TG_CUDA(cudaMemcpyAsync(d_inst_, h_inst_.data(), sizeof(Inst) * count_, cudaMemcpyHostToDevice, cur_));
+	TG_CUDA(cudaMemsetAsync(d_launches_, 0, sizeof(unsigned long long), cur_));
+	if (graph_mode_) {
+		if (!exec_) build_graph();
+		TG_CUDA(cudaGraphLaunch(exec_, cur_));
+	} else {
+		emit_program();
+	}
+	std::vector<Ctrl> hc(count_);
+	unsigned long long nl = 0;
+	TG_CUDA(cudaMemcpyAsync(hc.data(), d_ctrl_, sizeof(Ctrl) * count_, cudaMemcpyDeviceToHost, cur_));
+	TG_CUDA(cudaMemcpyAsync(&nl, d_launches_, sizeof(nl), cudaMemcpyDeviceToHost, cur_));
+	TG_CUDA(cudaStreamSynchronize(cur_));
+	last_launches_ = (long long)nl;
+	double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+	if (info)
+		for (int i = 0; i < count_; i++) {
+			info[i].secs = secs;
+			info[i].outer_iters = hc[i].count_outer;
+			info[i].total_iters = hc[i].count_total;
+			info[i].rel_chg = hc[i].relchg_out;
+			info[i].rel_error = hc[i].rel_error;
+			info[i].status = hc[i].status;
+			info[i].reserved = 0;
+		}
+}
+
+}  // namespace tval3g

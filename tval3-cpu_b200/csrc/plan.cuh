@@ -1,0 +1,93 @@
+// Plans: device-resident operators, state and the emitted solve program.
+#pragma once
+#include <functional>
+#include <memory>
+
+#include "kernels.cuh"
+#include "ops.cuh"
+
+namespace tval3g {
+
+// device operator storage owned by a plan / operator object
+struct OpStore {
+	OpDev dev{};
+	std::vector<void *> owned;   // device allocations to free
+	long long bytes = 0;         // device bytes allocated for the operator
+	long long nnz = 0;           // CSR nnz, or Bresenham hits of a ray operator
+	long long b_len = 0;
+	// ray operators: forward CSR over traced rays (kept on request) and the
+	// host copy of each traced ray's measurement index
+	int *ray_rptr = nullptr, *ray_rind = nullptr;
+	std::vector<int> ray_out;
+};
+
+// validate a problem against (b_len, ut_len) with the reference's messages;
+// returns n (image length)
+long long validate(const tval3g_problem &p, long long b_len, long long ut_len);
+// prepare the device operator of a problem (flags: TVAL3G_DEVICE_INPUTS)
+void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st, bool keep_ray_csr);
+void free_op(OpStore &st);
+void check_options(const tval3g_options &o);
+// operator tile maps of a batch, uploaded to *d_tiles; returns the dense
+// partial-buffer size in floats
+long long build_op_maps_upload(std::vector<Inst> &inst, const std::vector<OpStore> &ops, OpBatch &ob,
+                               int2 **d_tiles, cudaStream_t s);
+
+class Plan {
+public:
+	Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, int flags);
+	~Plan();
+	void solve(const float *const *d_b, const float *const *d_Ut, float *const *d_U, tval3g_info *info,
+	           cudaStream_t stream);
+	long long launches() const { return last_launches_; }
+	long long device_bytes() const { return device_bytes_; }
+
+private:
+	struct Frame {
+		cudaGraph_t g;
+		std::vector<cudaGraphNode_t> deps;
+	};
+	int count_;
+	int flags_;
+	bool graph_mode_;
+	bool any_skip_ = false;
+	cudaStream_t stream_ = nullptr;   // the plan's own stream
+	cudaStream_t cur_ = nullptr;      // stream of the solve in progress
+	std::vector<OpStore> ops_;
+	std::vector<Inst> h_inst_;
+	Inst *d_inst_ = nullptr;
+	Ctrl *d_ctrl_ = nullptr;
+	double *d_part_ = nullptr;
+	float *d_arena_ = nullptr;
+	int2 *d_tiles_ = nullptr;
+	int *d_flag_ = nullptr;
+	int *h_flag_ = nullptr;
+	unsigned long long *d_launches_ = nullptr;
+	TileMap maps_[NMAPS];
+	OpBatch ob_;
+	long long last_launches_ = 0;
+	long long device_bytes_ = 0;
+	std::vector<void *> allocs_;
+	// graph
+	cudaGraph_t graph_ = nullptr;
+	cudaGraphExec_t exec_ = nullptr;
+	cudaStream_t cap_ = nullptr;      // stream used for capture
+	std::vector<Frame> frames_;
+	bool capturing_ = false;
+
+	void *dalloc(size_t bytes);
+	void release();
+	KArgs kargs(MapKind mk, int pred, int stage = 0) const;
+	LaunchCtx lctx() const;
+	void emit_program();
+	void emit_iteration();
+	// control flow: direct execution or graph construction
+	void if_(int pred, const std::function<void()> &body);
+	void while_(int pred, const std::function<void()> &body);
+	void seg_begin();
+	void seg_end();
+	cudaStream_t es() const { return graph_mode_ ? cap_ : cur_; }
+	void build_graph();
+};
+
+}  // namespace tval3g

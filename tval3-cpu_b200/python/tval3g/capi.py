@@ -1,0 +1,327 @@
+"""ctypes binding of libtval3g.so (include/tval3g.h).
+
+Host-buffer solves take numpy arrays; plans, operators and stencils take
+device pointers (torch CUDA tensors are accepted and their data_ptr() used).
+There is no fallback: if the shared library is missing or no GPU is present,
+the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(os.path.dirname(HERE))
+LIB_PATH = os.path.join(PKG, "lib", "libtval3g.so")
+
+OK, ERR_ARGUMENT, ERR_CUDA, ERR_NO_DEVICE, ERR_NONFINITE, ERR_INTERNAL = 0, -1, -2, -3, -4, -5
+OP_DENSE, OP_CSR, OP_RAY2D, OP_RAY3D = 0, 1, 2, 3
+TV_ANISO, TV_ISO = 0, 1
+DEVICE_INPUTS, GRAPH = 1, 2
+
+_OPT_D = ("mu", "beta", "mu0", "beta0", "tol", "tol_inn", "c", "gamma", "gam", "rate_gam", "rate_cnt",
+          "skipMulRatio", "maxRelativeChange")
+_OPT_I = ("maxit", "maxcnt", "nonneg", "isreal", "numInitIterations", "tv_norm")
+
+
+class Options(C.Structure):
+    _fields_ = [(k, C.c_double) for k in _OPT_D] + [(k, C.c_int) for k in _OPT_I]
+
+    @staticmethod
+    def from_dict(d):
+        o = Options()
+        for k in _OPT_D + _OPT_I:
+            setattr(o, k, d[k])
+        return o
+
+
+class Info(C.Structure):
+    _fields_ = [("secs", C.c_double), ("rel_chg", C.c_double), ("rel_error", C.c_double),
+                ("outer_iters", C.c_int), ("total_iters", C.c_int), ("status", C.c_int), ("reserved", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_IP = C.POINTER(C.c_int)
+_FP = C.POINTER(C.c_float)
+
+
+class Problem(C.Structure):
+    _fields_ = [("dims", C.c_int), ("dim_y", C.c_int), ("dim_x", C.c_int), ("dim_z", C.c_int),
+                ("op_kind", C.c_int), ("m", C.c_int), ("n_cols", C.c_int), ("layers", C.c_int),
+                ("A", _FP), ("nnz", C.c_longlong), ("csr_ptr", _IP), ("csr_ind", _IP), ("csr_val", _FP),
+                ("num_emitters", C.c_int), ("num_receivers", C.c_int), ("numMPs", C.c_int), ("numPaths", C.c_int),
+                ("use_path", _IP), ("x_emitters", _IP), ("y_emitters", _IP), ("z_emitters", _IP),
+                ("x_receivers", _IP), ("y_receivers", _IP), ("z_receivers", _IP), ("ld", C.c_int),
+                ("rv_x", C.c_int), ("rv_y", C.c_int), ("rv_z", C.c_int), ("scale_factor", C.c_float)]
+
+
+class TVAL3Error(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise TVAL3Error(ERR_NO_DEVICE, f"{LIB_PATH} is not built (run make in the package directory)")
+        L = C.CDLL(LIB_PATH)
+        vp, i, d, ll = C.c_void_p, C.c_int, C.c_double, C.c_longlong
+        P, O, I = C.POINTER(Problem), C.POINTER(Options), C.POINTER(Info)
+        L.tval3g_last_error.restype = C.c_char_p
+        L.tval3g_solve.argtypes = [P, vp, i, O, vp, i, vp, I]
+        L.tval3g_solve_batch.argtypes = [i, P, C.POINTER(vp), O, C.POINTER(vp), C.POINTER(vp), I, i]
+        L.tval3g_plan_create.argtypes = [C.POINTER(vp), i, P, O, i]
+        L.tval3g_plan_solve.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), I, vp]
+        L.tval3g_plan_stats.argtypes = [vp, C.POINTER(ll), C.POINTER(ll)]
+        L.tval3g_plan_destroy.argtypes = [vp]
+        L.tval3g_op_create.argtypes = [C.POINTER(vp), P, i]
+        L.tval3g_op_shape.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(ll)]
+        L.tval3g_op_apply.argtypes = [vp, i, vp, vp, vp]
+        L.tval3g_op_ray_csr.argtypes = [vp, C.POINTER(ll), _IP]
+        L.tval3g_op_destroy.argtypes = [vp]
+        L.tval3g_D.argtypes = [i, i, i, i, vp, vp, vp, vp, vp]
+        L.tval3g_Dt.argtypes = [i, i, i, i, vp, vp, vp, vp, vp]
+        L.tval3g_shrink.argtypes = [i, ll, i, d, vp, vp, vp, vp, vp, vp, vp, vp, vp, C.POINTER(d), vp]
+        _LIB = L
+    return _LIB
+
+
+def _check(rc):
+    if rc != OK:
+        raise TVAL3Error(rc, lib().tval3g_last_error().decode())
+
+
+EXPORTS = ("tval3g_last_error", "tval3g_version", "tval3g_solve", "tval3g_solve_batch", "tval3g_plan_create",
+           "tval3g_plan_solve", "tval3g_plan_stats", "tval3g_plan_destroy", "tval3g_op_create", "tval3g_op_shape",
+           "tval3g_op_apply", "tval3g_op_ray_csr", "tval3g_op_destroy", "tval3g_D", "tval3g_Dt", "tval3g_shrink")
+
+
+# --------------------------------------------------------------------------
+# problems (keep the numpy arrays alive with the struct)
+# --------------------------------------------------------------------------
+class ProblemSpec:
+    """A Problem struct plus the host arrays it points to."""
+
+    def __init__(self, shape, kind, keep=None, **fields):
+        self.keep = keep or []
+        p = Problem()
+        dims = len(shape)
+        p.dims = dims
+        if dims == 2:
+            p.dim_y, p.dim_x, p.dim_z = shape[0], shape[1], 1
+        else:
+            p.dim_z, p.dim_y, p.dim_x = shape
+        p.op_kind = kind
+        p.layers = 1
+        for k, v in fields.items():
+            setattr(p, k, v)
+        self.p = p
+        self.shape = tuple(shape)
+        self.n = int(np.prod(shape))
+
+    @property
+    def b_len(self):
+        p = self.p
+        if p.op_kind == OP_RAY2D:
+            return p.num_emitters * p.num_receivers
+        if p.op_kind == OP_RAY3D:
+            return p.numPaths * p.numMPs
+        return p.m * (p.layers if p.dims == 2 else 1)
+
+
+def _arr(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def _ptr(a, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def dense_problem(shape, A, layers=1, device_ptr=None):
+    """A: (m, n_cols) float32 host array (or device_ptr with A's shape)."""
+    m, ncols = A.shape
+    if device_ptr is not None:
+        return ProblemSpec(shape, OP_DENSE, [A], m=m, n_cols=ncols, layers=layers,
+                           A=C.cast(C.c_void_p(device_ptr), _FP))
+    A = _arr(A, np.float32)
+    return ProblemSpec(shape, OP_DENSE, [A], m=m, n_cols=ncols, layers=layers, A=_ptr(A, C.c_float))
+
+
+def csr_problem(shape, m, ncols, rowptr, colind, val, layers=1):
+    rowptr, colind, val = _arr(rowptr, np.int32), _arr(colind, np.int32), _arr(val, np.float32)
+    return ProblemSpec(shape, OP_CSR, [rowptr, colind, val], m=m, n_cols=ncols, layers=layers, nnz=len(colind),
+                       csr_ptr=_ptr(rowptr, C.c_int), csr_ind=_ptr(colind, C.c_int), csr_val=_ptr(val, C.c_float))
+
+
+def ray2d_problem(shape, g):
+    a = {k: _arr(g[k], np.int32) for k in ("use_path", "xe", "ye", "xr", "yr")}
+    return ProblemSpec(shape, OP_RAY2D, list(a.values()), num_emitters=len(a["xe"]), num_receivers=len(a["xr"]),
+                       numMPs=1, use_path=_ptr(a["use_path"], C.c_int), x_emitters=_ptr(a["xe"], C.c_int),
+                       y_emitters=_ptr(a["ye"], C.c_int), x_receivers=_ptr(a["xr"], C.c_int),
+                       y_receivers=_ptr(a["yr"], C.c_int), ld=int(g["ld"]), scale_factor=float(g["scale"]))
+
+
+def ray3d_problem(shape, g):
+    a = {k: _arr(g[k], np.int32) for k in ("use_path", "xe", "ye", "ze", "xr", "yr", "zr")}
+    return ProblemSpec(shape, OP_RAY3D, list(a.values()), num_emitters=int(g["E"]), num_receivers=int(g["R"]),
+                       numMPs=int(g["numMPs"]), numPaths=int(g["numPaths"]),
+                       use_path=_ptr(a["use_path"], C.c_int), x_emitters=_ptr(a["xe"], C.c_int),
+                       y_emitters=_ptr(a["ye"], C.c_int), z_emitters=_ptr(a["ze"], C.c_int),
+                       x_receivers=_ptr(a["xr"], C.c_int), y_receivers=_ptr(a["yr"], C.c_int),
+                       z_receivers=_ptr(a["zr"], C.c_int), rv_x=int(g["rv_x"]), rv_y=int(g["rv_y"]),
+                       rv_z=int(g["rv_z"]), scale_factor=float(g["scale"]))
+
+
+def problem_from_workload(w, use_csr=False):
+    """ProblemSpec of a tval3g.workloads configuration dict."""
+    shape = w["shape"]
+    if w["kind"] == "dense":
+        return dense_problem(shape, w["A"], w.get("layers", 1))
+    if use_csr or w["kind"] == "csr":
+        A = w["csr"]
+        return csr_problem(shape, A["m"], A["n"], A["rowptr"], A["colind"], A["val"], w.get("layers", 1))
+    if w["kind"] == "ray2d":
+        return ray2d_problem(shape, w["geom"])
+    return ray3d_problem(shape, w["geom"])
+
+
+# --------------------------------------------------------------------------
+# calls
+# --------------------------------------------------------------------------
+def solve(spec: ProblemSpec, b, opts: dict, Ut=None):
+    """One solve with host buffers; returns (U as spec.shape float32, info dict)."""
+    b = _arr(b, np.float32)
+    U = np.zeros(spec.n, np.float32)
+    Utv = _arr(Ut, np.float32).ravel() if Ut is not None else None
+    info = Info()
+    o = Options.from_dict(opts)
+    rc = lib().tval3g_solve(C.byref(spec.p), b.ctypes.data, len(b), C.byref(o),
+                            Utv.ctypes.data if Utv is not None else None, Utv.size if Utv is not None else 0,
+                            U.ctypes.data, C.byref(info))
+    _check(rc)
+    return U.reshape(spec.shape), info.as_dict()
+
+
+def solve_batch(specs, bs, opts_list, Uts=None, graph=True):
+    n = len(specs)
+    probs = (Problem * n)(*[s.p for s in specs])
+    opts = (Options * n)(*[Options.from_dict(o) for o in opts_list])
+    barr = [_arr(b, np.float32) for b in bs]
+    uarr = [np.zeros(s.n, np.float32) for s in specs]
+    utarr = [(_arr(u, np.float32).ravel() if u is not None else None) for u in (Uts or [None] * n)]
+    bp = (C.c_void_p * n)(*[b.ctypes.data for b in barr])
+    up = (C.c_void_p * n)(*[u.ctypes.data for u in uarr])
+    utp = (C.c_void_p * n)(*[(u.ctypes.data if u is not None else None) for u in utarr])
+    infos = (Info * n)()
+    _check(lib().tval3g_solve_batch(n, probs, bp, opts, utp, up, infos, GRAPH if graph else 0))
+    return [u.reshape(s.shape) for u, s in zip(uarr, specs)], [i.as_dict() for i in infos]
+
+
+def _dptr(t):
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    return int(t)
+
+
+class Plan:
+    """Device-resident solver state for a batch of problems (graph=True: the
+    iteration loop is one CUDA graph with conditional nodes)."""
+
+    def __init__(self, specs, opts_list, graph=True, device_inputs=False):
+        n = len(specs)
+        self.specs = specs
+        self.count = n
+        probs = (Problem * n)(*[s.p for s in specs])
+        opts = (Options * n)(*[Options.from_dict(o) for o in opts_list])
+        h = C.c_void_p()
+        flags = (GRAPH if graph else 0) | (DEVICE_INPUTS if device_inputs else 0)
+        _check(lib().tval3g_plan_create(C.byref(h), n, probs, opts, flags))
+        self.h = h
+
+    def solve(self, d_b, d_U, d_Ut=None, stream=None):
+        n = self.count
+        bp = (C.c_void_p * n)(*[_dptr(x) for x in d_b])
+        up = (C.c_void_p * n)(*[_dptr(x) for x in d_U])
+        utp = (C.c_void_p * n)(*[_dptr(x) for x in d_Ut]) if d_Ut is not None else None
+        infos = (Info * n)()
+        _check(lib().tval3g_plan_solve(self.h, bp, utp, up, infos, _dptr(stream)))
+        return [i.as_dict() for i in infos]
+
+    def stats(self):
+        a, b = C.c_longlong(), C.c_longlong()
+        _check(lib().tval3g_plan_stats(self.h, C.byref(a), C.byref(b)))
+        return {"kernel_launches": a.value, "device_bytes": b.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().tval3g_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Operator:
+    """A measurement operator on the device: apply(x, trans) with torch tensors."""
+
+    def __init__(self, spec: ProblemSpec):
+        h = C.c_void_p()
+        _check(lib().tval3g_op_create(C.byref(h), C.byref(spec.p), 0))
+        self.h = h
+        r, c, z = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        _check(lib().tval3g_op_shape(h, C.byref(r), C.byref(c), C.byref(z)))
+        self.rows, self.cols, self.nnz = r.value, c.value, z.value
+
+    def apply(self, x, y, trans=False, stream=None):
+        _check(lib().tval3g_op_apply(self.h, int(trans), _dptr(x), _dptr(y), _dptr(stream)))
+        return y
+
+    def ray_csr(self):
+        rowptr = np.zeros(self.rows + 1, np.int64)
+        colind = np.zeros(max(self.nnz, 1), np.int32)
+        _check(lib().tval3g_op_ray_csr(self.h, rowptr.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                       colind.ctypes.data_as(_IP)))
+        return rowptr, colind[:self.nnz]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().tval3g_op_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def D(dims, shape, U, Ux, Uy, Uz=None):
+    dz, dy, dx = (1,) + tuple(shape) if dims == 2 else shape
+    _check(lib().tval3g_D(dims, dy, dx, dz, _dptr(U), _dptr(Ux), _dptr(Uy), _dptr(Uz), None))
+
+
+def Dt(dims, shape, X, Y, Z, res):
+    dz, dy, dx = (1,) + tuple(shape) if dims == 2 else shape
+    _check(lib().tval3g_Dt(dims, dy, dx, dz, _dptr(X), _dptr(Y), _dptr(Z), _dptr(res), None))
+
+
+def shrink(dims, n, tv_norm, beta, U, S, W):
+    lam = C.c_double()
+    Uz, Sz, Wz = (U[2], S[2], W[2]) if dims == 3 else (None, None, None)
+    _check(lib().tval3g_shrink(dims, n, tv_norm, beta, _dptr(U[0]), _dptr(U[1]), _dptr(Uz), _dptr(S[0]),
+                               _dptr(S[1]), _dptr(Sz), _dptr(W[0]), _dptr(W[1]), _dptr(Wz), C.byref(lam), None))
+    return lam.value
