@@ -52,6 +52,15 @@ extern "C" {
 #define TVAL3G_DEVICE_INPUTS 1  /* A / CSR arrays of the problems are device pointers */
 #define TVAL3G_GRAPH 2          /* run the iteration loop as one CUDA graph with
                                    conditional nodes (no host round trips) */
+#define TVAL3G_TRACE 4          /* record one tval3g_trace_record per inner
+                                   iteration on the device (tval3g_plan_trace) */
+
+/* Per inner iteration: step length, objective after update_W, relative
+ * change, backtracking steps taken (6 = restart after five failures) and
+ * whether the A^T multiplication was skipped (skipMulRatio heuristic). */
+typedef struct tval3g_trace_record {
+	double tau, f, relchg, backtracks, skipped;
+} tval3g_trace_record;
 
 /* Options; field meaning as tval3_options<T> (include/tval3/tval3_types.h). */
 typedef struct tval3g_options {
@@ -130,6 +139,9 @@ int tval3g_plan_solve(tval3g_plan *plan, const float *const *d_b, const float *c
 /* Kernel launches issued by the last tval3g_plan_solve (graph mode: kernel
  * nodes executed, counted on the device), and the plan's device bytes. */
 int tval3g_plan_stats(const tval3g_plan *plan, long long *kernel_launches, long long *device_bytes);
+/* Trace of instance `index` of the last solve of a plan created with
+ * TVAL3G_TRACE: copies up to `cap` records to out, *count = records written. */
+int tval3g_plan_trace(const tval3g_plan *plan, int index, tval3g_trace_record *out, int cap, int *count);
 int tval3g_plan_destroy(tval3g_plan *plan);
 
 /* Operators alone.  tval3g_op_apply: y = A x (trans = 0) or y = A^T x

@@ -60,7 +60,8 @@ class Info(C.Structure):
 
 
 class Iter(C.Structure):
-    _fields_ = [("tau", C.c_double), ("f", C.c_double), ("relchg", C.c_double), ("backtracks", C.c_int)]
+    _fields_ = [("tau", C.c_double), ("f", C.c_double), ("relchg", C.c_double), ("backtracks", C.c_int),
+                ("skipped", C.c_int)]
 
 
 def _fill(struct, opts: dict):
@@ -234,7 +235,8 @@ def solve(op: Op, b, shape, opts: dict, Ut=None, record=False) -> Result:
         raise ValueError(f"oracle solve rejected its arguments ({rc})")
     rec = None
     if record:
-        rec = [(its[k].tau, its[k].f, its[k].relchg, its[k].backtracks) for k in range(info.total_iters)]
+        rec = [(its[k].tau, its[k].f, its[k].relchg, its[k].backtracks, its[k].skipped)
+               for k in range(info.total_iters)]
     return Result(U.reshape(shape), info.secs, info.outer_iters, info.total_iters, info.rel_chg,
                   info.rel_error, rec)
 

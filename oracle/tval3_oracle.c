@@ -38,6 +38,7 @@ static void *dup(const void *src, size_t bytes) {
 }
 
 static double *zeros(long n) { return (double *)calloc(n > 0 ? n : 1, sizeof(double)); }
+static void materialize_rays(orc_op *op);
 
 orc_op *orc_op_dense(int m, int n, int layers, const double *A) {
 	orc_op *op = (orc_op *)calloc(1, sizeof(orc_op));
@@ -80,6 +81,7 @@ orc_op *orc_op_ray2d(int E, int R, const int *use_path, const int *xe, const int
 	op->ld = ld; op->scale = scale;
 	op->m = E * R;       /* uncompacted, 2d:748 */
 	op->n = n_pixels;    /* the image is the caller's: 2d/mat_mult.h has no size */
+	materialize_rays(op);
 	return op;
 }
 
@@ -98,7 +100,39 @@ orc_op *orc_op_ray3d(int numMPs, int numPaths, int E, int R, const int *use_path
 	op->rvx = rv_x; op->rvy = rv_y; op->rvz = rv_z; op->scale = scale;
 	op->m = numPaths * numMPs;           /* 3d:1153 */
 	op->n = rv_x * rv_y * rv_z;
+	materialize_rays(op);
 	return op;
+}
+
+/* Rasterise every traced ray once with the sequential recurrence and keep the
+ * result as row- and column-compressed index lists (rows = measurements), so
+ * that applications are parallel loops.  Rays that share a measurement index
+ * are concatenated in loop order, as the reference accumulates them. */
+static void materialize_rays(orc_op *op) {
+	long total = 0;
+	int cnt = orc_ray_lists(op, NULL, NULL, NULL, &total);
+	int *ray = (int *)malloc(sizeof(int) * (cnt ? cnt : 1));
+	long *off = (long *)malloc(sizeof(long) * (cnt + 1));
+	int *pix = (int *)malloc(sizeof(int) * (total ? total : 1));
+	orc_ray_lists(op, ray, off, pix, &total);
+	op->nnz = (int)total;
+	op->rowptr = (int *)calloc(op->m + 1, sizeof(int));
+	for (int k = 0; k < cnt; k++) op->rowptr[ray[k] + 1] += (int)(off[k + 1] - off[k]);
+	for (int i = 0; i < op->m; i++) op->rowptr[i + 1] += op->rowptr[i];
+	op->colind = (int *)malloc(sizeof(int) * (total ? total : 1));
+	int *next = (int *)dup(op->rowptr, sizeof(int) * (op->m + 1));
+	for (int k = 0; k < cnt; k++)
+		for (long t = off[k]; t < off[k + 1]; t++) op->colind[next[ray[k]]++] = pix[t];
+	free(next);
+	op->colptr = (int *)calloc(op->n + 1, sizeof(int));
+	op->rowind = (int *)malloc(sizeof(int) * (total ? total : 1));
+	for (long k = 0; k < total; k++) op->colptr[op->colind[k] + 1]++;
+	for (int j = 0; j < op->n; j++) op->colptr[j + 1] += op->colptr[j];
+	next = (int *)dup(op->colptr, sizeof(int) * (op->n + 1));
+	for (int i = 0; i < op->m; i++)
+		for (int k = op->rowptr[i]; k < op->rowptr[i + 1]; k++) op->rowind[next[op->colind[k]]++] = i;
+	free(next);
+	free(ray); free(off); free(pix);
 }
 
 void orc_op_free(orc_op *op) {
@@ -203,10 +237,6 @@ static void walk_rays(const orc_op *op, visit_fn fn, void *ctx, void (*begin)(vo
 			}
 }
 
-typedef struct { const double *x; double *y; double s; } mv_ctx;
-static void vis_fwd(void *c, int ray, long pix) { mv_ctx *m = (mv_ctx *)c; m->y[ray] += m->x[pix] * m->s; }
-static void vis_adj(void *c, int ray, long pix) { mv_ctx *m = (mv_ctx *)c; m->y[pix] += m->x[ray] * m->s; }
-
 typedef struct { int *ray_index; long *offsets; int *pix; long total; int count; } list_ctx;
 static void list_begin(void *c, int ray) {
 	list_ctx *l = (list_ctx *)c;
@@ -268,10 +298,22 @@ static void apply_layer(const orc_op *op, int trans, const double *x, double *y,
 			}
 		}
 		break;
-	default: {               /* rays: 2d/mat_mult.h:95-105, 3d/mat_mult.h:122-139 */
-		mv_ctx c = {x, y, op->scale};
-		walk_rays(op, trans ? vis_adj : vis_fwd, &c, NULL);
-	}
+	default:                 /* rays: y[ray] += x[pix]*scale per hit, 2d/mat_mult.h:95-105 */
+		if (!trans) {
+#pragma omp parallel for schedule(dynamic, 256)
+			for (int i = 0; i < op->m; i++) {
+				double s = 0;
+				for (int k = op->rowptr[i]; k < op->rowptr[i + 1]; k++) s += x[op->colind[k]] * op->scale;
+				y[i] = s;
+			}
+		} else {
+#pragma omp parallel for schedule(dynamic, 256)
+			for (int j = 0; j < op->n; j++) {
+				double s = 0;
+				for (int k = op->colptr[j]; k < op->colptr[j + 1]; k++) s += x[op->rowind[k]] * op->scale;
+				y[j] = s;
+			}
+		}
 	}
 }
 
@@ -375,6 +417,7 @@ typedef struct {
 	double skipRatio, maxRelChange, currSkip;
 	double *last_Au;
 	double *V[3];   /* scratch for Ux - Wx etc. */
+	int last_skip;  /* the last get_g_mult skipped A^T (trace only) */
 	double *tmp_n, *tmp_m;
 	const orc_op *op;
 	int tv_norm;
@@ -399,6 +442,7 @@ static void Dst(st_t *s, const double *U, double *Ux, double *Uy, double *Uz) {
 /* get_g_mult: generic with the A^T-skip heuristic 2d:300-357 / 3d:433-493;
  * dense always multiplies (2d:361-394 / 3d:498-529). */
 static void get_g_mult(st_t *s, const double *U, int force) {
+	s->last_skip = 0;
 	orc_apply(s->op, 0, U, s->Au);
 	if (s->op->kind == ORC_DENSE || s->skipRatio == 0) {
 		orc_apply(s->op, 1, s->Au, s->g);
@@ -416,6 +460,7 @@ static void get_g_mult(st_t *s, const double *U, int force) {
 		cpy(s->m, s->Au, s->last_Au); orc_apply(s->op, 1, s->Au, s->g);
 	} else {
 		s->currSkip -= 1;
+		s->last_skip = 1;
 	}
 }
 
@@ -654,6 +699,7 @@ int orc_solve(int dims, int dim_y, int dim_x, int dim_z, const orc_op *op, const
 			if (iters) {
 				iters[count_total].tau = tau; iters[count_total].f = s->f;
 				iters[count_total].relchg = RelChg; iters[count_total].backtracks = bt;
+				iters[count_total].skipped = s->last_skip;
 			}
 			count_total++;
 			if (RelChg < o->tol_inn && !fst) break;

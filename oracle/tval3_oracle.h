@@ -35,11 +35,13 @@ typedef struct {
 	int outer_iters, total_iters;
 } orc_info;
 
-/* Per inner iteration record (optional): tau, f after update_W, RelChg and the
- * number of backtracking steps (6 = restart after 5 failures). */
+/* Per inner iteration record (optional): tau, f after update_W, RelChg, the
+ * number of backtracking steps (6 = restart after 5 failures) and whether the
+ * descent step skipped the A^T multiplication. */
 typedef struct {
 	double tau, f, relchg;
 	int backtracks;
+	int skipped;
 } orc_iter;
 
 /* Operators (all arrays are copied). */

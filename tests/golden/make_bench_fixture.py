@@ -1,0 +1,50 @@
+"""FP64 solution of the benchmark workload (bench.py), for its relerr check.
+
+Solves the 256x256 ring workload (tval3g.workloads.ring2d with normalize=True,
+isotropic TV, maxit 500) with the FP64 oracle restatement and stores U and the
+iteration counts in tests/golden/ring256_fp64.npz.  Also records the
+reference's own float solver on the CSR twin of the same operator with
+anisotropic TV (the reference has no isotropic TV) for the drift statement.
+
+    python tests/golden/make_bench_fixture.py
+"""
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "tval3-cpu_b200", "python"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import oracle as O  # noqa: E402
+from tval3g import workloads as W  # noqa: E402
+
+
+def main():
+    w = W.ring2d(seed=1, side=256, T=512, tv_norm=1, maxit=500, tol=1e-5, normalize=True)
+    op = O.Op.ray2d(w["geom"], 256 * 256)
+    t = time.time()
+    r = O.solve(op, w["b"].astype(np.float64), w["shape"], w["opts"], Ut=w["u_true"])
+    print(f"FP64 oracle: {r.total_iters} iterations, {r.outer_iters} outer, relerr to phantom {r.rel_error:.4f}, "
+          f"{time.time() - t:.1f} s")
+    out = {"U": r.U.astype(np.float32), "iters": np.array([r.outer_iters, r.total_iters]),
+           "scale": np.array([w["geom"]["scale"]]), "b_sum": np.array([float(np.sum(w["b"], dtype=np.float64))])}
+    if O.ref_available(2):
+        o = dict(w["opts"])
+        o["tv_norm"] = 0
+        A = w["csr"]
+        r64 = O.solve(op, w["b"].astype(np.float64), w["shape"], o)
+        cwd = os.getcwd()
+        rr = O.ref_solve("csr", w["shape"], w["b"], o, dtype=0, csr=(A["m"], A["n"], A["rowptr"], A["colind"], A["val"]))
+        os.chdir(cwd)
+        d = float(np.linalg.norm(rr.U.ravel() - r64.U.ravel()) / np.linalg.norm(r64.U))
+        print(f"aniso: reference float {rr.total_iters} it vs FP64 oracle {r64.total_iters} it, relerr {d:.2e}")
+        out["aniso_ref_f32_vs_fp64"] = np.array([d, rr.total_iters, r64.total_iters])
+    np.savez_compressed(os.path.join(HERE, "ring256_fp64.npz"), **out)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,13 +1,19 @@
 """GPU solver parity through the C ABI.
 
-Tolerances (relative L2 of U):
-* at 20 iterations the float reference and the FP64 restatement agree to
-  ~5e-5, so the GPU solution must be within 1e-3 of both;
-* at convergence (tol-stopped) the reference's own float build is up to ~7e-3
-  away from its double build (tests/test_oracle.py), so the GPU solution must
-  be within 2e-2 of the FP64 oracle and of the float reference;
-* graph and plain execution, and batched and single solves, run the same
-  kernels in the same order with deterministic reductions: bit-identical.
+FP32 trajectories of TVAL3 are sensitive: the reference's own float build
+differs from its own double build by 5e-5 (dense, 20 iterations) up to 5.6e-2
+(2D ring, 20 iterations) and 8.9e-2 (3D, at convergence) - see the golden
+fixtures.  The bar for the FP32 GPU solution (relative L2 of U) is therefore
+
+    |U_gpu - U_fp64| <= max(1e-3, 2 * |U_ref_float - U_ref_double|)
+
+i.e. the GPU result is at least as close to the FP64 solution (oracle and the
+reference's double build, which agree to <2e-7) as the reference's own float
+build is, up to a factor 2, and never looser than 1e-3.  Where the reference
+cannot run (isotropic TV) the bar is 1e-3 against the oracle at an iteration
+count where the float trajectory is stable.
+Graph and plain execution, and batched and single solves, run the same
+kernels in the same order with deterministic reductions: bit-identical.
 """
 import numpy as np
 import pytest
@@ -18,12 +24,11 @@ from tval3g import capi
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"it20": 1e-3, "conv": 2e-2, "layers": 2e-3, "iso": 2e-3, "nonneg": 2e-3, "skip": 2e-3, "s16": 1e-3,
-       "s8": 2e-3}
 
-
-def _tol(name):
-    return TOL[name.split("_")[-1]]
+def _bar(g):
+    if "ref0_U" not in g:
+        return 1e-3
+    return max(1e-3, 2 * relerr(g["ref0_U"], g["ref2_U"]))
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -32,15 +37,44 @@ def test_solve_matches_oracle_and_reference(name, torch_cuda):
     g = golden(f"{name}.npz")
     U, info = capi.solve(api_problem(c, capi), c["b"], c["opts"], Ut=c["u_true"])
     assert info["status"] == 0
+    bar = _bar(g)
     e_or = relerr(U, g["oracle_U"])
-    assert e_or < _tol(name), (name, e_or, info)
-    if "ref0_U" in g:
-        e_ref = relerr(U, g["ref0_U"])
-        assert e_ref < _tol(name), (name, e_ref, info)
+    assert e_or < bar, (name, e_or, bar, info)
+    if "ref2_U" in g:
+        assert relerr(U, g["ref2_U"]) < bar
     if name.endswith("it20"):
         assert info["total_iters"] == 20
     # rel_error is ||Ut - U|| / ||Ut|| of the returned U
     assert abs(info["rel_error"] - relerr(U, c["u_true"])) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["ring2d_s64_conv", "dense2d_s32_conv", "hemi3d_s16_conv", "ring2d_s64_skip"])
+def test_trace_matches_oracle(name, torch_cuda):
+    """The device controller takes the reference's decisions: while the FP32
+    and FP64 trajectories agree (objective within 1e-3), every iteration's
+    backtracking count (6 = restart) and A^T-skip decision are identical and
+    the step length tau agrees to 1e-3 (first 5 iterations) / 1e-2; the first 5
+    iterations always agree."""
+    import oracle as O
+    torch = torch_cuda
+    c = build_case(name)
+    r = O.solve(c["oracle_op"], c["b"].astype(np.float64), c["shape"], c["opts"], record=True)
+    spec = api_problem(c, capi)
+    plan = capi.Plan([spec], [c["opts"]], graph=True, trace=True)
+    du = [torch.empty(spec.n, device="cuda")]
+    plan.solve([torch.tensor(c["b"], device="cuda")], du)
+    tr = plan.trace(0)
+    plan.close()
+    agree = 0
+    for k in range(min(len(tr), len(r.iters))):
+        tau, f, rc, bt, skip = tr[k]
+        otau, of, orc, obt, oskip = r.iters[k]
+        if abs(f - of) > 1e-3 * abs(of):
+            break
+        assert int(bt) == obt and int(skip) == oskip, (k, tr[k], r.iters[k])
+        assert abs(tau - otau) <= (1e-3 if k < 5 else 1e-2) * otau, (k, tau, otau)
+        agree += 1
+    assert agree >= 5, agree
 
 
 def _plan_run(torch, specs, bs, opts, graph):

@@ -162,6 +162,13 @@ int tval3g_plan_stats(const tval3g_plan *plan, long long *kernel_launches, long 
 	CAPI_END
 }
 
+int tval3g_plan_trace(const tval3g_plan *plan, int index, tval3g_trace_record *out, int cap, int *count) {
+	CAPI_BEGIN
+	TG_ARG(plan && plan->p && out && count, "Argument error: NULL argument");
+	*count = plan->p->trace(index, out, cap);
+	CAPI_END
+}
+
 int tval3g_plan_destroy(tval3g_plan *plan) {
 	CAPI_BEGIN
 	if (plan) {

@@ -129,6 +129,7 @@ struct Inst {
 	const float *ut_user;        // caller's Ut (device) or NULL
 	float *u_user;               // caller's U (device)
 	Ctrl *ctrl;
+	double *trace;               // maxit records of 5 doubles, or NULL
 	double *part;                // this instance's partial sums
 	int ntn, ntm;                // tiles over n and m
 	// options (2d/tval3_cpu_2d.cpp:769-772)

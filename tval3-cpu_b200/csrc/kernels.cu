@@ -342,6 +342,7 @@ __global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
 	} else if (a.stage == ST_RESTART) {
 		c.restart = 0;
 		c.need_bt = 0;
+		c.bt_cnt = 6;   // marks the restart in the trace
 		if (I.skip_enabled) c.currSkip = 0;
 	} else if (a.stage == ST_INIT) {
 		if (I.skip_enabled) c.currSkip = 0;
@@ -389,6 +390,11 @@ __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 		c.count_total++;
 		c.nrmup = sqrt(tot[1]);
 		c.relchg = sqrt(tot[2]) / c.nrmup;
+		if (I.trace && c.count_total <= I.maxit) {
+			double *t = I.trace + (long long)(c.count_total - 1) * 5;
+			t[0] = c.tau; t[1] = c.f; t[2] = c.relchg; t[3] = c.bt_cnt; t[4] = c.skip_adj;
+		}
+		c.bt_cnt = 0;
 		bool brk = (c.relchg < I.tol_inn) && !c.fst;
 		c.inner_break = brk || c.count_total >= I.maxit;
 		if (!brk) c.fst = 0;

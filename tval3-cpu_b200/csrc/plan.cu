@@ -403,6 +403,16 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 		d_part_ = (double *)dalloc(sizeof(double) * (size_t)parts);
 		d_ctrl_ = (Ctrl *)dalloc(sizeof(Ctrl) * count);
 		TG_CUDA(cudaMemsetAsync(d_ctrl_, 0, sizeof(Ctrl) * count, stream_));
+		if (flags & TVAL3G_TRACE) {
+			long long recs = 0;
+			for (int i = 0; i < count; i++) {
+				trace_off_.push_back(recs);
+				recs += std::max(h_inst_[i].maxit, 1);
+			}
+			d_trace_ = (double *)dalloc(sizeof(double) * 5 * (size_t)recs);
+			TG_CUDA(cudaMemsetAsync(d_trace_, 0, sizeof(double) * 5 * (size_t)recs, stream_));
+			for (int i = 0; i < count; i++) h_inst_[i].trace = d_trace_ + 5 * trace_off_[i];
+		}
 		long long poff = 0;
 		for (int i = 0; i < count; i++) {
 			Inst &I = h_inst_[i];
@@ -440,6 +450,16 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 }
 
 Plan::~Plan() { release(); }
+
+int Plan::trace(int index, tval3g_trace_record *out, int cap) const {
+	TG_ARG(d_trace_ != nullptr, "Argument error: the plan was created without TVAL3G_TRACE");
+	TG_ARG(index >= 0 && index < count_, "Argument error: instance index out of range");
+	int n = index < (int)last_iters_.size() ? std::min(last_iters_[index], h_inst_[index].maxit) : 0;
+	n = std::min(n, cap);
+	if (n > 0)
+		TG_CUDA(cudaMemcpy(out, d_trace_ + 5 * trace_off_[index], sizeof(double) * 5 * n, cudaMemcpyDeviceToHost));
+	return n;
+}
 
 void Plan::release() {
 	if (exec_) cudaGraphExecDestroy(exec_);
@@ -673,6 +693,8 @@ void Plan::solve(const float *const *d_b, const float *const *d_Ut, float *const
 	TG_CUDA(cudaMemcpyAsync(&nl, d_launches_, sizeof(nl), cudaMemcpyDeviceToHost, cur_));
 	TG_CUDA(cudaStreamSynchronize(cur_));
 	last_launches_ = (long long)nl;
+	last_iters_.resize(count_);
+	for (int i = 0; i < count_; i++) last_iters_[i] = hc[i].count_total;
 	double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 	if (info)
 		for (int i = 0; i < count_; i++) {

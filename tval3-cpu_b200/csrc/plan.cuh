@@ -40,6 +40,7 @@ public:
 	void solve(const float *const *d_b, const float *const *d_Ut, float *const *d_U, tval3g_info *info,
 	           cudaStream_t stream);
 	long long launches() const { return last_launches_; }
+	int trace(int index, tval3g_trace_record *out, int cap) const;
 	long long device_bytes() const { return device_bytes_; }
 
 private:
@@ -66,6 +67,9 @@ private:
 	TileMap maps_[NMAPS];
 	OpBatch ob_;
 	long long last_launches_ = 0;
+	double *d_trace_ = nullptr;
+	std::vector<long long> trace_off_;
+	std::vector<int> last_iters_;
 	long long device_bytes_ = 0;
 	std::vector<void *> allocs_;
 	// graph

@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(PKG, "lib", "libtval3g.so")
 OK, ERR_ARGUMENT, ERR_CUDA, ERR_NO_DEVICE, ERR_NONFINITE, ERR_INTERNAL = 0, -1, -2, -3, -4, -5
 OP_DENSE, OP_CSR, OP_RAY2D, OP_RAY3D = 0, 1, 2, 3
 TV_ANISO, TV_ISO = 0, 1
-DEVICE_INPUTS, GRAPH = 1, 2
+DEVICE_INPUTS, GRAPH, TRACE = 1, 2, 4
 
 _OPT_D = ("mu", "beta", "mu0", "beta0", "tol", "tol_inn", "c", "gamma", "gam", "rate_gam", "rate_cnt",
           "skipMulRatio", "maxRelativeChange")
@@ -82,6 +82,7 @@ def lib():
         L.tval3g_plan_create.argtypes = [C.POINTER(vp), i, P, O, i]
         L.tval3g_plan_solve.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), I, vp]
         L.tval3g_plan_stats.argtypes = [vp, C.POINTER(ll), C.POINTER(ll)]
+        L.tval3g_plan_trace.argtypes = [vp, i, C.POINTER(C.c_double), i, C.POINTER(i)]
         L.tval3g_plan_destroy.argtypes = [vp]
         L.tval3g_op_create.argtypes = [C.POINTER(vp), P, i]
         L.tval3g_op_shape.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(ll)]
@@ -101,7 +102,7 @@ def _check(rc):
 
 
 EXPORTS = ("tval3g_last_error", "tval3g_version", "tval3g_solve", "tval3g_solve_batch", "tval3g_plan_create",
-           "tval3g_plan_solve", "tval3g_plan_stats", "tval3g_plan_destroy", "tval3g_op_create", "tval3g_op_shape",
+           "tval3g_plan_solve", "tval3g_plan_stats", "tval3g_plan_trace", "tval3g_plan_destroy", "tval3g_op_create", "tval3g_op_shape",
            "tval3g_op_apply", "tval3g_op_ray_csr", "tval3g_op_destroy", "tval3g_D", "tval3g_Dt", "tval3g_shrink")
 
 
@@ -238,14 +239,15 @@ class Plan:
     """Device-resident solver state for a batch of problems (graph=True: the
     iteration loop is one CUDA graph with conditional nodes)."""
 
-    def __init__(self, specs, opts_list, graph=True, device_inputs=False):
+    def __init__(self, specs, opts_list, graph=True, device_inputs=False, trace=False):
         n = len(specs)
         self.specs = specs
         self.count = n
+        self.maxit = [int(o["maxit"]) for o in opts_list]
         probs = (Problem * n)(*[s.p for s in specs])
         opts = (Options * n)(*[Options.from_dict(o) for o in opts_list])
         h = C.c_void_p()
-        flags = (GRAPH if graph else 0) | (DEVICE_INPUTS if device_inputs else 0)
+        flags = (GRAPH if graph else 0) | (DEVICE_INPUTS if device_inputs else 0) | (TRACE if trace else 0)
         _check(lib().tval3g_plan_create(C.byref(h), n, probs, opts, flags))
         self.h = h
 
@@ -262,6 +264,14 @@ class Plan:
         a, b = C.c_longlong(), C.c_longlong()
         _check(lib().tval3g_plan_stats(self.h, C.byref(a), C.byref(b)))
         return {"kernel_launches": a.value, "device_bytes": b.value}
+
+    def trace(self, index=0):
+        """Per inner iteration records (tau, f, relchg, backtracks, skipped)."""
+        cap = max(self.maxit[index], 1)
+        buf = (C.c_double * (5 * cap))()
+        cnt = C.c_int()
+        _check(lib().tval3g_plan_trace(self.h, index, buf, cap, C.byref(cnt)))
+        return np.array(buf[:5 * cnt.value]).reshape(cnt.value, 5)
 
     def close(self):
         if getattr(self, "h", None):

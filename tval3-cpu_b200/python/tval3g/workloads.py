@@ -283,9 +283,29 @@ def dense2d(seed=0, side=64, sampling=0.3, noise=0.01, n_ellipses=5, tv_norm=1, 
                 opts=options(2 ** 8, 2 ** 5, tol, maxit, tv_norm=tv_norm))
 
 
+def sigma_max(csr, iters=40):
+    """Largest singular value of a CSR operator (power iteration on A^T A from a
+    seeded start; a few parts in 1e4 after 40 steps)."""
+    import scipy.sparse as sp
+    M = sp.csr_matrix((np.asarray(csr["val"], np.float64), csr["colind"], csr["rowptr"]), shape=(csr["m"], csr["n"]))
+    x = np.random.default_rng(12345).standard_normal(csr["n"])
+    lam = 0.0
+    for _ in range(iters):
+        y = M.T @ (M @ x)
+        lam = float(np.linalg.norm(y))
+        x = y / lam
+    return math.sqrt(lam)
+
+
 def ring2d(seed=1, side=256, T=512, receivers=None, noise=0.005, tv_norm=1, maxit=500, tol=1e-5,
-           mu=2 ** 10, beta=2 ** 6, csr=True):
-    """2D ultrasound-tomography ring (Bresenham projector + CSR twin)."""
+           mu=2 ** 10, beta=2 ** 6, csr=True, normalize=False):
+    """2D ultrasound-tomography ring (Bresenham projector + CSR twin).
+
+    normalize: set the geometry's scale_factor (the weight of every hit) to
+    1/sigma_max(A) so that A has unit spectral norm, as TVAL3's mu and beta
+    assume; with unit weights (normalize=False) sigma_max(A)^2 ~ 1e5 at 256^2
+    and the solve stays in its ill-conditioned transient for hundreds of
+    iterations."""
     rng = np.random.default_rng(seed)
     n = side * side
     g = ring_geometry(side, T, receivers)
@@ -299,6 +319,10 @@ def ring2d(seed=1, side=256, T=512, receivers=None, noise=0.005, tv_norm=1, maxi
         cx, cy, r0 = c + rad * math.cos(ang), c + rad * math.sin(ang), rng.uniform(side / 40, side / 16)
         u[(xx - cx) ** 2 + (yy - cy) ** 2 <= r0 ** 2] = 1.0 + rng.choice([-1, 1]) * 0.15
     A = ray2d_csr(g, n)
+    if normalize:
+        s = 1.0 / sigma_max(A)
+        g["scale"] = float(np.float32(s))
+        A["val"] = np.full(len(A["colind"]), g["scale"], np.float64)
     y = csr_matvec(A, u.ravel())
     live = np.asarray(g["use_path"]) != 0
     b = np.zeros(A["m"])
