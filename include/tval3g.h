@@ -168,6 +168,18 @@ int tval3g_shrink(int dims, long long n, int tv_norm, double beta, const float *
                   const float *Uz, const float *sx, const float *sy, const float *sz, float *Wx,
                   float *Wy, float *Wz, double *lam1, void *stream);
 
+/* y = A^T x for a dense row-major m x n float matrix, with DEVICE pointers,
+ * for callers that cannot allocate device memory at call time (for example
+ * when another allocator has reserved the device's memory, or when a
+ * cudaMalloc's synchronisation is not acceptable).  It allocates nothing: its
+ * partial-sum scratch is a fixed 4 MiB array compiled into the library, so n
+ * may be at most 1048576 (larger n is rejected with TVAL3G_ERR_ARGUMENT).
+ * The first call on each device looks up that array's device address; make it
+ * before any stream capture begins.  All calls share the array: calls whose
+ * work overlaps on the GPU race.  Returns after the product is complete.
+ * No counterpart in the reference (it has no device code). */
+int tval3g_dense_adjoint_static(const float *d_A, int m, int n, const float *d_x, float *d_y, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

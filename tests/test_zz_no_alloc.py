@@ -1,0 +1,58 @@
+"""tval3g_dense_adjoint_static: y = A^T x with no device allocation.
+
+It serves callers that cannot allocate device memory when they call in (their
+device memory is reserved up front by another allocator, or a cudaMalloc's
+synchronisation is not acceptable).  Its scratch is a fixed array inside the
+library, shared by all calls.  This file runs last (pytest collects files in
+name order) and also passes alone in a fresh process.
+
+Checked against the regular dense operator entry point (tval3g_op_apply,
+trans = 1) within the operator tolerance of the suite (1e-5 relative), on two
+calls in a row with different inputs, so stale scratch would show.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from helpers import relerr
+from tval3g import capi
+
+pytestmark = pytest.mark.gpu
+
+
+def _static_adjoint(A_dev, m, n, x_dev, y_dev):
+    L = capi.lib()
+    f = L.tval3g_dense_adjoint_static
+    f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    return f(A_dev.data_ptr(), m, n, x_dev.data_ptr(), y_dev.data_ptr(), None)
+
+
+@pytest.mark.parametrize("m,n", [(1229, 4096), (307, 1021)])
+def test_static_adjoint_matches_operator(m, n, torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(m + n)
+    A = (rng.standard_normal((m, n)) / np.sqrt(m)).astype(np.float32)
+    A_dev = torch.tensor(A, device="cuda")
+    op = capi.Operator(capi.dense_problem((1, n), A))
+    for call in range(2):
+        x = torch.tensor(rng.standard_normal(m).astype(np.float32), device="cuda")
+        want = torch.empty(n, device="cuda")
+        op.apply(x, want, trans=True)
+        got = torch.full((n,), float("nan"), device="cuda")
+        assert _static_adjoint(A_dev, m, n, x, got) == capi.OK, capi.lib().tval3g_last_error()
+        assert relerr(got.cpu().numpy(), want.cpu().numpy()) < 1e-5, call
+        ref = A.astype(np.float64).T @ x.cpu().numpy().astype(np.float64)
+        assert relerr(got.cpu().numpy(), ref) < 1e-5
+    op.close()
+
+
+def test_static_adjoint_rejects_oversize(torch_cuda):
+    torch = torch_cuda
+    n = (1 << 20) + 1
+    A = torch.zeros(1, device="cuda")
+    x = torch.zeros(1, device="cuda")
+    y = torch.zeros(1, device="cuda")
+    rc = _static_adjoint(A, 1, n, x, y)
+    assert rc == capi.ERR_ARGUMENT
+    assert b"static scratch" in capi.lib().tval3g_last_error()
