@@ -49,6 +49,9 @@ def args_():
     p.add_argument("--profile", action="store_true",
                    help="for ncu: build the plan, run --warmup + --steps solves, print nothing else")
     p.add_argument("--maxit", type=int, default=None, help="override maxit (profiling a short solve)")
+    p.add_argument("--plain", action="store_true",
+                   help="with --profile: run the host-driven loop (same kernels, same order) instead of the "
+                        "CUDA graph, whose conditional nodes ncu cannot profile kernel by kernel")
     return p.parse_args()
 
 
@@ -195,21 +198,39 @@ def main():
     if a.maxit is not None:
         opts["maxit"] = a.maxit
     b_host = np.ascontiguousarray(w["b"], np.float32)
+    # a non-default stream: every kernel of the solve is launched on it and
+    # the CUDA events below are recorded on it
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     d_b = torch.tensor(b_host, device=dev)
     d_U = torch.empty(spec.n, device=dev)
     flush = torch.empty(64 * 1024 * 1024, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    ref = fp64_reference()
+    # time-to-solution: stop at the first iteration within 1e-3 of the FP64
+    # solution (given as Ut), else by the reference's own stopping rules
+    d_ref = torch.tensor(ref["U"].ravel().astype(np.float32), device=dev) if ref is not None else None
+    target = 1e-3 if ref is not None else 0.0
 
-    plan = capi.Plan([spec], [opts], graph=True)
+    plan = capi.Plan([spec], [opts], graph=not (a.profile and a.plain), trace=True)
+    plan.set_target(target)
+
+    def solve_timed(p, reps):
+        out, inf = [], None
+        for _ in range(reps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            inf = p.solve([d_b], [d_U], d_Ut=[d_ref] if d_ref is not None else None, stream=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            out.append(e0.elapsed_time(e1))
+        return out, inf
+
     if a.profile:
-        for _ in range(a.warmup + a.steps):
-            plan.solve([d_b], [d_U], stream=stream.cuda_stream)
-        torch.cuda.synchronize(dev)
+        solve_timed(plan, a.warmup + a.steps)
         plan.close()
         return
-    for _ in range(max(a.warmup, 3)):
-        plan.solve([d_b], [d_U], stream=stream.cuda_stream)
-    torch.cuda.synchronize(dev)
+    solve_timed(plan, max(a.warmup, 3))
 
     clocks = Clocks(local)
     if dist:
@@ -218,13 +239,8 @@ def main():
     clocks.start()
     times, launches, infos = [], 0, None
     for _ in range(a.steps):
-        flush.fill_(1.0)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        infos = plan.solve([d_b], [d_U], stream=stream.cuda_stream)
-        e1.record(stream)
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
+        t1, infos = solve_timed(plan, 1)
+        times += t1
         launches += plan.stats()["kernel_launches"]
     torch.cuda.synchronize(dev)
     if dist:
@@ -236,21 +252,20 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = world * 1000.0 / ms
-    U = d_U.cpu().numpy()
     iters = infos[0]["total_iters"]
+    relerr = float(infos[0]["rel_error"]) if ref is not None else None
+    curve = plan.trace(0)[:, 5]
 
-    # the plain (host-driven, no graph) form of the same solve
+    # the full solve under the reference's stopping rules alone
+    plan.set_target(0.0)
+    full_t, full_info = solve_timed(plan, 2)
+    full_relerr = float(full_info[0]["rel_error"]) if ref is not None else None
+
+    # the plain (host-driven, no graph) form of the same time-to-solution
     plan_plain = capi.Plan([spec], [opts], graph=False)
-    plan_plain.solve([d_b], [d_U], stream=stream.cuda_stream)
-    torch.cuda.synchronize(dev)
-    pt = []
-    for _ in range(2):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        plan_plain.solve([d_b], [d_U], stream=stream.cuda_stream)
-        e1.record(stream)
-        e1.synchronize()
-        pt.append(e0.elapsed_time(e1))
+    plan_plain.set_target(target)
+    solve_timed(plan_plain, 1)
+    pt, _ = solve_timed(plan_plain, 2)
     plan_plain.close()
 
     # end to end through the host-buffer C ABI
@@ -269,45 +284,53 @@ def main():
     y = torch.rand(op.rows, device=dev)
     out_m = torch.empty(op.rows, device=dev)
     out_n = torch.empty(op.cols, device=dev)
+    # each launch timed alone after an L2 flush, so its index comes from HBM
     kt = {}
     for name, (src, dst, tr) in {"ray_forward": (x, out_m, False), "ray_adjoint": (y, out_n, True)}.items():
-        for _ in range(3):
-            op.apply(src, dst, trans=tr, stream=stream.cuda_stream)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        flush.fill_(1.0)
-        e0.record(stream)
-        for _ in range(20):
-            op.apply(src, dst, trans=tr, stream=stream.cuda_stream)
-        e1.record(stream)
-        e1.synchronize()
-        kt[name] = e0.elapsed_time(e1) / 20
+        op.apply_n(src, dst, 3, trans=tr, stream=stream.cuda_stream)
+        ts = []
+        for _ in range(10):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            op.apply_n(src, dst, 1, trans=tr, stream=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        kt[name] = float(np.mean(ts))
     nnz, n, m = op.nnz, op.cols, op.rows
-    # algorithmic bytes of the adjoint gather: pixel pointers, ray ids, the
-    # measurement vector once, the image written once
-    adj_bytes = 4 * (n + 1) + 4 * nnz + 4 * m + 4 * n
+    nrays = int(np.count_nonzero(w["geom"]["use_path"]))
+    nchunks = -(-nrays // 32768)
+    # algorithmic bytes of the staged adjoint (compaction + gather): the
+    # measurement vector read once, the traced-ray vector written and read
+    # once, the 16-bit pixel->ray index, the per-pixel chunk offsets, the image
+    # written once
+    adj_bytes = 4 * m + 8 * nrays + 2 * nnz + 4 * n * (nchunks + 1) + 4 * n
     peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = adj_bytes / (kt["ray_adjoint"] * 1e-3) / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "ray_adjoint_gather_ring256.md")
+    prof = os.path.join(ROOT, "profiles", "ray_adjoint_staged_ring256.md")
     if os.path.exists(prof):
         for line in open(prof):
             if line.startswith("traffic_bytes_per_launch:"):
                 traffic = float(line.split(":")[1].split()[0])
 
-    ref = fp64_reference()
-    relerr = float(np.linalg.norm(U.ravel() - ref["U"].ravel()) / np.linalg.norm(ref["U"])) if ref is not None else None
-
     line = {"metric": METRIC, "value": value, "unit": "reconstructions/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded ring phantom, 0.5% noise)", "config": config_dict(),
             "iterations": iters, "time_to_solution_ms": ms, "relerr_vs_fp64": relerr,
+            "reached_target": bool(relerr is not None and relerr <= target), "target": target,
+            "relerr_curve_every_5": [round(float(x), 6) for x in curve[::5]],
+            "full_solve": {"ms": float(np.mean(full_t)), "iterations": full_info[0]["total_iters"],
+                           "relerr_vs_fp64": full_relerr, "rule": "reference stopping rules (tol, tol_inn, maxit)"},
             "plain": {"value": world * 1000.0 / float(np.mean(pt)), "unit": "reconstructions/s",
                       "ms_per_step": float(np.mean(pt)), "form": "host-driven loop, one launch per kernel"},
             "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "reconstructions/s",
                     "h2d_bytes_per_step": int(b_host.nbytes + geom_bytes), "d2h_bytes_per_step": int(spec.n * 4)},
-            "roofline": {"bound": "hbm", "kernel": "k_gather<ray adjoint>", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": "k_ray_compact + k_ray_adj_staged (ray adjoint)",
+                         "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes": adj_bytes, "ms_per_launch": kt["ray_adjoint"],
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",

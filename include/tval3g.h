@@ -56,10 +56,11 @@ extern "C" {
                                    iteration on the device (tval3g_plan_trace) */
 
 /* Per inner iteration: step length, objective after update_W, relative
- * change, backtracking steps taken (6 = restart after five failures) and
- * whether the A^T multiplication was skipped (skipMulRatio heuristic). */
+ * change, backtracking steps taken (6 = restart after five failures), whether
+ * the A^T multiplication was skipped (skipMulRatio heuristic) and, when the
+ * solve was given Ut, ||U/scl - Ut|| / ||Ut|| after the iteration (else 0). */
 typedef struct tval3g_trace_record {
-	double tau, f, relchg, backtracks, skipped;
+	double tau, f, relchg, backtracks, skipped, relerr_ut;
 } tval3g_trace_record;
 
 /* Options; field meaning as tval3_options<T> (include/tval3/tval3_types.h). */
@@ -139,6 +140,12 @@ int tval3g_plan_solve(tval3g_plan *plan, const float *const *d_b, const float *c
 /* Kernel launches issued by the last tval3g_plan_solve (graph mode: kernel
  * nodes executed, counted on the device), and the plan's device bytes. */
 int tval3g_plan_stats(const tval3g_plan *plan, long long *kernel_launches, long long *device_bytes);
+/* Time-to-solution mode: with target > 0, every instance solved with a Ut
+ * also stops after the first inner iteration at which
+ * ||U/scl - Ut|| <= target * ||Ut|| (checked on the device each iteration);
+ * info.rel_error then reports that value.  target = 0 restores the
+ * reference's stopping rules only.  No counterpart in the reference. */
+int tval3g_plan_set_target(tval3g_plan *plan, double target);
 /* Trace of instance `index` of the last solve of a plan created with
  * TVAL3G_TRACE: copies up to `cap` records to out, *count = records written. */
 int tval3g_plan_trace(const tval3g_plan *plan, int index, tval3g_trace_record *out, int cap, int *count);
@@ -150,6 +157,10 @@ typedef struct tval3g_operator tval3g_operator;
 int tval3g_op_create(tval3g_operator **op, const tval3g_problem *prob, int flags);
 int tval3g_op_shape(const tval3g_operator *op, long long *rows, long long *cols, long long *nnz);
 int tval3g_op_apply(tval3g_operator *op, int trans, const float *d_x, float *d_y, void *stream);
+/* The same product `reps` times, enqueued back to back on `stream` (the
+ * result is that of one application); returns without waiting, so events
+ * recorded around it on the stream time the kernels alone. */
+int tval3g_op_apply_n(tval3g_operator *op, int trans, const float *d_x, float *d_y, int reps, void *stream);
 /* Ray operators: the device-built CSR (rows = b_len, untraced rows empty) of
  * the Bresenham rasterisation, copied to HOST arrays rowptr [rows+1] and
  * colind [nnz]; with colind == NULL only rowptr is written. */

@@ -162,6 +162,13 @@ int tval3g_plan_stats(const tval3g_plan *plan, long long *kernel_launches, long 
 	CAPI_END
 }
 
+int tval3g_plan_set_target(tval3g_plan *plan, double target) {
+	CAPI_BEGIN
+	TG_ARG(plan && plan->p && target >= 0, "Argument error: NULL plan or negative target");
+	plan->p->set_target(target);
+	CAPI_END
+}
+
 int tval3g_plan_trace(const tval3g_plan *plan, int index, tval3g_trace_record *out, int cap, int *count) {
 	CAPI_BEGIN
 	TG_ARG(plan && plan->p && out && count, "Argument error: NULL argument");
@@ -232,8 +239,16 @@ int tval3g_op_shape(const tval3g_operator *op, long long *rows, long long *cols,
 }
 
 int tval3g_op_apply(tval3g_operator *op, int trans, const float *d_x, float *d_y, void *stream) {
+	int rc = tval3g_op_apply_n(op, trans, d_x, d_y, 1, stream);
+	if (rc != TVAL3G_OK) return rc;
 	CAPI_BEGIN
-	TG_ARG(op && d_x && d_y, "Argument error: NULL argument");
+	TG_CUDA(cudaStreamSynchronize(stream ? (cudaStream_t)stream : op->s));
+	CAPI_END
+}
+
+int tval3g_op_apply_n(tval3g_operator *op, int trans, const float *d_x, float *d_y, int reps, void *stream) {
+	CAPI_BEGIN
+	TG_ARG(op && d_x && d_y && reps >= 1, "Argument error: NULL argument or reps < 1");
 	cudaStream_t s = stream ? (cudaStream_t)stream : op->s;
 	Inst I = op->h;
 	// x lives in the bank of its length: image vectors vn, measurement vectors vm
@@ -249,9 +264,10 @@ int tval3g_op_apply(tval3g_operator *op, int trans, const float *d_x, float *d_y
 	}
 	TG_CUDA(cudaMemcpyAsync(op->d_inst, &I, sizeof(Inst), cudaMemcpyHostToDevice, s));
 	LaunchCtx L{s, op->d_inst, nullptr};
-	if (!trans) op_forward(L, op->ob, P_ALL, xs, ys);
-	else op_adjoint(L, op->ob, P_ALL, xs, ys);
-	TG_CUDA(cudaStreamSynchronize(s));
+	for (int r = 0; r < reps; r++) {
+		if (!trans) op_forward(L, op->ob, P_ALL, xs, ys);
+		else op_adjoint(L, op->ob, P_ALL, xs, ys);
+	}
 	CAPI_END
 }
 

@@ -61,6 +61,7 @@ struct Ctrl {
 	double dd, dDd;
 	double currSkip;
 	double rel_error;
+	double relerr_ut;            // last |U/scl - Ut| / |Ut| (target mode)
 	int currInit;
 	int count_outer, count_total;
 	int fst, active, need_bt, bt_cnt, restart, inner_break, need_mlp, need_Ad, skip_adj;
@@ -117,11 +118,46 @@ struct OpDev {
 	int nrays;
 	const int4 *rays;
 	int rvx, rvy;           // index = x + y*rvx + z*rvx*rvy (2D: rvx = ld)
+	// 2D ray adjoint staged through shared memory (nchunks > 0): the traced
+	// rays are cut into chunks of RAY_CHUNK; for pixel p and chunk c the hits
+	// are sidx[soff[p*(nchunks+1)+c] .. soff[p*(nchunks+1)+c+1]) as 16-bit
+	// offsets of the ray within the chunk, in ray order
+	int nchunks;
+	int ppb;                // pixels per block of the staged adjoint
+	const unsigned short *sidx;
+	const int *soff;
+	const int *live_out;    // measurement index of each traced ray
+	float *ylive;           // scratch: the adjoint's input compacted to traced rays
+	// 2D forward: y-driven rays read a transposed copy of the image (rows of
+	// length tH = n / ld), in which their steps are contiguous; NULL = off
+	float *xT;
+	int tH;
+};
+
+constexpr int RAY_CHUNK = 32768;       // rays per shared-memory chunk (128 KB)
+constexpr int RAY_MAX_CHUNKS = 8;      // staged adjoint up to 262144 traced rays
+
+// Unsigned 32-bit division by a run-time constant with one multiply-high
+// (Granlund & Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994): sh = ceil(log2 d), mul = 2^32 (2^sh - d) / d + 1,
+// n / d = (umulhi(n, mul) + n) >> sh for every 32-bit n.
+struct FastDiv {
+	unsigned d, mul, sh;
+	void init(unsigned div) {
+		d = div;
+		sh = 0;
+		while ((1ull << sh) < div) sh++;
+		mul = (unsigned)(((1ull << 32) * ((1ull << sh) - div)) / div + 1);
+	}
+	__device__ __forceinline__ unsigned div(unsigned n) const {
+		return (unsigned)(((unsigned long long)__umulhi(n, mul) + n) >> sh);
+	}
 };
 
 // one instance as the kernels see it
 struct Inst {
 	int dims, p, q, r;           // image: dim_y, dim_x, dim_z (r = 1 in 2D)
+	FastDiv fq, fp;              // division by q and by p
 	long long n, m;              // vector lengths (n and m include layers)
 	float *vn[NVN];
 	float *vm[NVM];
@@ -135,13 +171,16 @@ struct Inst {
 	// options (2d/tval3_cpu_2d.cpp:769-772)
 	double muf, betaf, mu0, beta0, tol, tol_inn, c, gamma, gam0, rate_gam, rate_cnt;
 	double skipRatio, maxRelChange;
+	double target;               // > 0: also stop once |U/scl - Ut| <= target |Ut|
 	int maxit, maxcnt, nonneg, tv_norm, numInit, skip_enabled;
 	OpDev op;
 };
 
-constexpr int TILE = 1024;       // elements per tile (256 threads x 4)
+constexpr int TILE = 512;        // elements per tile (256 threads x 2)
 constexpr int BLOCK = 256;
-constexpr int NSUM = 4;          // partial sums per tile
+constexpr int EPT = TILE / BLOCK;
+constexpr int NSUM = 6;          // partial sums per tile
+constexpr int TRACE_DOUBLES = (int)(sizeof(tval3g_trace_record) / sizeof(double));
 
 // tile maps
 enum MapKind { MAP_N = 0, MAP_M, MAP_NM, NMAPS };

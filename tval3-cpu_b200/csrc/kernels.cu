@@ -1,4 +1,9 @@
 // Fused TVAL3 iteration kernels; see kernels.cuh.
+//
+// Every kernel copies its instance descriptor into registers (a by-value
+// Inst: stores to the float vectors cannot alias it, so its pointers are
+// loaded once), indexes with 32-bit integers (image and measurement lengths
+// are below 2^31) and computes image coordinates with multiply-high division.
 #include <math.h>
 
 #include "kernels.cuh"
@@ -8,51 +13,57 @@ namespace tval3g {
 // ---------------------------------------------------------------------------
 // prologue / image geometry
 // ---------------------------------------------------------------------------
-#define KPROLOGUE(a)                                                                   \
+#define KPROLOGUE(a)                                                                        \
 	if ((a).launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd((a).launches, 1ull); \
-	const int2 tl_ = (a).map.tiles[blockIdx.x];                                        \
-	const Inst &I = (a).tab[tl_.x];                                                    \
-	const int local = tl_.y;                                                           \
+	const int2 tl_ = (a).map.tiles[blockIdx.x];                                             \
+	const Inst I = (a).tab[tl_.x];                                                          \
+	const int local = tl_.y;                                                                \
 	if (!pred_ok(*I.ctrl, (a).pred)) return;
 
+// element k of this thread in a tile starting at i0
+#define FOR_TILE(i0, len, i)                                  \
+	_Pragma("unroll") for (int k_ = 0; k_ < EPT; k_++)        \
+		if (const int i = (i0) + (int)threadIdx.x + k_ * BLOCK; i < (len))
+
 struct Geo {
-	int dims, p, q, r;
-	long long S, n;
-	__device__ Geo(const Inst &I) : dims(I.dims), p(I.p), q(I.q), r(I.r), S((long long)I.p * I.q), n(I.n) {}
-	__device__ void coords(long long i, int &x, int &y, int &z) const {
-		long long row = i / q;
-		x = (int)(i - row * q);
-		z = (int)(row / p);
-		y = (int)(row - (long long)z * p);
+	int dims, p, q, r, S, n;
+	FastDiv fq, fp;
+	__device__ Geo(const Inst &I)
+		: dims(I.dims), p(I.p), q(I.q), r(I.r), S(I.p * I.q), n((int)I.n), fq(I.fq), fp(I.fp) {}
+	__device__ __forceinline__ void coords(int i, int &x, int &y, int &z) const {
+		const unsigned row = fq.div((unsigned)i);
+		x = i - (int)row * q;
+		const unsigned zz = fp.div(row);
+		z = (int)zz;
+		y = (int)row - (int)zz * p;
 	}
 };
 
 // periodic forward differences at i (2d:268-278, 3d:365-389)
-__device__ __forceinline__ float dxf(const float *U, const Geo &g, long long i, int x) {
+__device__ __forceinline__ float dxf(const float *__restrict__ U, const Geo &g, int i, int x) {
 	return (x < g.q - 1) ? U[i + 1] - U[i] : U[i - (g.q - 1)] - U[i];
 }
-__device__ __forceinline__ float dyf(const float *U, const Geo &g, long long i, int y) {
-	return (y < g.p - 1) ? U[i + g.q] - U[i] : U[i - (long long)(g.p - 1) * g.q] - U[i];
+__device__ __forceinline__ float dyf(const float *__restrict__ U, const Geo &g, int i, int y) {
+	return (y < g.p - 1) ? U[i + g.q] - U[i] : U[i - (g.p - 1) * g.q] - U[i];
 }
-__device__ __forceinline__ float dzf(const float *U, const Geo &g, long long i, int z) {
-	return (z < g.r - 1) ? U[i + g.S] - U[i] : U[i - (long long)(g.r - 1) * g.S] - U[i];
+__device__ __forceinline__ float dzf(const float *__restrict__ U, const Geo &g, int i, int z) {
+	return (z < g.r - 1) ? U[i + g.S] - U[i] : U[i - (g.r - 1) * g.S] - U[i];
 }
 
 // Dt at i with component accessors vx(j), vy(j), vz(j); the float additions
 // are made in the reference's order (2d:280-293, 3d:394-425), including the
 // 3D y term the reference adds on the first row of slices z >= 1.
 template <class FX, class FY, class FZ>
-__device__ __forceinline__ float dt_at(const Geo &g, long long i, int x, int y, int z, FX vx, FY vy,
-                                       FZ vz) {
+__device__ __forceinline__ float dt_at(const Geo &g, int i, int x, int y, int z, FX vx, FY vy, FZ vz) {
 	float res = (x > 0) ? vx(i - 1) - vx(i) : vx(i + g.q - 1) - vx(i);
 	if (g.dims == 2) {
 		if (y > 0) { res = res + vy(i - g.q); res = res + (-vy(i)); }
-		else { res = res + vy(i + (long long)(g.p - 1) * g.q); res = res + (-vy(i)); }
+		else { res = res + vy(i + (g.p - 1) * g.q); res = res + (-vy(i)); }
 	} else {
 		if (!(z == 0 && y == 0)) { res = res + vy(i - g.q); res = res + (-vy(i)); }
-		if (y == 0) { res = res + vy(i + (long long)(g.p - 1) * g.q); res = res + (-vy(i)); }
+		if (y == 0) { res = res + vy(i + (g.p - 1) * g.q); res = res + (-vy(i)); }
 		if (z > 0) { res = res + vz(i - g.S); res = res + (-vz(i)); }
-		else { res = res + vz(i + (long long)(g.r - 1) * g.S); res = res + (-vz(i)); }
+		else { res = res + vz(i + (g.r - 1) * g.S); res = res + (-vz(i)); }
 	}
 	return res;
 }
@@ -86,16 +97,20 @@ struct Shrink {
 		}
 		return lam;
 	}
-	// one component of W at j, from U_c and sigma_c
-	__device__ __forceinline__ float comp(const Inst &I, long long j, int c) const {
-		float u[3], s[3], w[3];
+	// component c (compile-time after inlining) of W at j, from U_c, sigma_c
+	__device__ __forceinline__ float comp(const float *const (&U)[3], const float *const (&S)[3], int j,
+	                                      int c) const {
 		if (iso) {
-			u[0] = I.vn[vUx][j]; u[1] = I.vn[vUy][j]; u[2] = dims == 3 ? I.vn[vUz][j] : 0.f;
-			s[0] = I.vn[vSx][j]; s[1] = I.vn[vSy][j]; s[2] = dims == 3 ? I.vn[vSz][j] : 0.f;
+			float u[3], s[3], w[3];
+#pragma unroll
+			for (int cc = 0; cc < 3; cc++) {
+				u[cc] = cc < dims ? U[cc][j] : 0.f;
+				s[cc] = cc < dims ? S[cc][j] : 0.f;
+			}
 			apply(u, s, w);
 			return w[c];
 		}
-		float ub = I.vn[vUx + c][j] - I.vn[vSx + c][j] / beta;
+		float ub = U[c][j] - S[c][j] / beta;
 		float t = fabsf(ub) - thr;
 		t = t >= 0.f ? t : 0.f;
 		return ub >= 0.f ? t : -t;
@@ -107,36 +122,33 @@ __device__ __forceinline__ bool bad(double v) { return !isfinite(v); }
 // ---------------------------------------------------------------------------
 // scaleb (2d:229-266): first min |b| and first max |b|, scale into [0.5, 1.5]
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void better_min(float &a, long long &ia, float b, long long ib) {
+__device__ __forceinline__ void better_min(float &a, int &ia, float b, int ib) {
 	if (b < a || (b == a && ib < ia)) { a = b; ia = ib; }
 }
-__device__ __forceinline__ void better_max(float &a, long long &ia, float b, long long ib) {
+__device__ __forceinline__ void better_max(float &a, int &ia, float b, int ib) {
 	if (b > a || (b == a && ib < ia)) { a = b; ia = ib; }
 }
 
 __global__ void __launch_bounds__(BLOCK) k_scaleb(KArgs a) {
 	KPROLOGUE(a);
-	const long long m = I.m, i0 = (long long)local * TILE;
+	const int m = (int)I.m, i0 = local * TILE;
 	float mn = INFINITY, mx = -INFINITY;
-	long long imn = LLONG_MAX, imx = LLONG_MAX;
-	for (int k = 0; k < TILE / BLOCK; k++) {
-		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-		if (i < m) {
-			float v = fabsf(I.b_user[i]);
-			better_min(mn, imn, v, i);
-			better_max(mx, imx, v, i);
-		}
+	int imn = INT_MAX, imx = INT_MAX;
+	FOR_TILE(i0, m, i) {
+		float v = fabsf(I.b_user[i]);
+		better_min(mn, imn, v, i);
+		better_max(mx, imx, v, i);
 	}
 	for (int o = 16; o > 0; o >>= 1) {
 		float v = __shfl_xor_sync(0xffffffffu, mn, o);
-		long long iv = __shfl_xor_sync(0xffffffffu, imn, o);
+		int iv = __shfl_xor_sync(0xffffffffu, imn, o);
 		better_min(mn, imn, v, iv);
 		v = __shfl_xor_sync(0xffffffffu, mx, o);
 		iv = __shfl_xor_sync(0xffffffffu, imx, o);
 		better_max(mx, imx, v, iv);
 	}
 	__shared__ float smn[32], smx[32];
-	__shared__ long long simn[32], simx[32];
+	__shared__ int simn[32], simx[32];
 	__shared__ int last;
 	int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 	if (lane == 0) { smn[wid] = mn; simn[wid] = imn; smx[wid] = mx; simx[wid] = imx; }
@@ -156,11 +168,11 @@ __global__ void __launch_bounds__(BLOCK) k_scaleb(KArgs a) {
 	if (!last || threadIdx.x != 0) return;
 	__threadfence();
 	float gmn = INFINITY, gmx = -INFINITY;
-	long long gimn = LLONG_MAX, gimx = LLONG_MAX;
+	int gimn = INT_MAX, gimx = INT_MAX;
 	for (int t = 0; t < I.ntm; t++) {   // tiles in index order: first occurrence wins
 		const double *P = I.part + (long long)t * NSUM;
-		better_min(gmn, gimn, (float)__ldcg(P + 0), (long long)__ldcg(P + 1));
-		better_max(gmx, gimx, (float)__ldcg(P + 2), (long long)__ldcg(P + 3));
+		better_min(gmn, gimn, (float)__ldcg(P + 0), (int)__ldcg(P + 1));
+		better_max(gmx, gimx, (float)__ldcg(P + 2), (int)__ldcg(P + 3));
 	}
 	Ctrl &c = *I.ctrl;
 	double scl = 1.0;
@@ -180,11 +192,9 @@ __global__ void __launch_bounds__(BLOCK) k_init(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	if (local < I.ntn) {
-		long long i0 = (long long)local * TILE;
-		for (int k = 0; k < TILE / BLOCK; k++) {
-			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-			if (i < I.n)
-				for (int v = 0; v < NVN; v++) I.vn[v][i] = 0.f;
+		FOR_TILE(local * TILE, (int)I.n, i) {
+#pragma unroll
+			for (int v = 0; v < NVN; v++) I.vn[v][i] = 0.f;
 		}
 		if (local == 0 && threadIdx.x == 0) {
 			c.mu = I.mu0; c.beta = I.beta0;
@@ -200,14 +210,11 @@ __global__ void __launch_bounds__(BLOCK) k_init(KArgs a) {
 			c.need_mlp = c.need_Ad = c.skip_adj = 0; c.status = 0;
 		}
 	} else {
-		long long i0 = (long long)(local - I.ntn) * TILE;
-		float scl = (float)c.scl;
-		for (int k = 0; k < TILE / BLOCK; k++) {
-			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-			if (i < I.m) {
-				for (int v = 0; v < NVM; v++) I.vm[v][i] = 0.f;
-				I.vm[vB][i] = scl != 1.f ? I.b_user[i] * scl : I.b_user[i];
-			}
+		const float scl = (float)c.scl;
+		FOR_TILE((local - I.ntn) * TILE, (int)I.m, i) {
+#pragma unroll
+			for (int v = 0; v < NVM; v++) I.vm[v][i] = 0.f;
+			I.vm[vB][i] = scl != 1.f ? I.b_user[i] * scl : I.b_user[i];
 		}
 	}
 }
@@ -215,14 +222,10 @@ __global__ void __launch_bounds__(BLOCK) k_init(KArgs a) {
 // U = Atb, rcdU = U (2d:775,779)
 __global__ void __launch_bounds__(BLOCK) k_init_u(KArgs a) {
 	KPROLOGUE(a);
-	long long i0 = (long long)local * TILE;
-	for (int k = 0; k < TILE / BLOCK; k++) {
-		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-		if (i < I.n) {
-			float u = I.vn[vAtb][i];
-			I.vn[vU][i] = u;
-			I.vn[vRcd][i] = u;
-		}
+	FOR_TILE(local * TILE, (int)I.n, i) {
+		float u = I.vn[vAtb][i];
+		I.vn[vU][i] = u;
+		I.vn[vRcd][i] = u;
 	}
 }
 
@@ -230,16 +233,14 @@ __global__ void __launch_bounds__(BLOCK) k_init_u(KArgs a) {
 __global__ void __launch_bounds__(BLOCK) k_D(KArgs a) {
 	KPROLOGUE(a);
 	Geo g(I);
-	const float *U = I.vn[vU];
-	long long i0 = (long long)local * TILE;
-	for (int k = 0; k < TILE / BLOCK; k++) {
-		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-		if (i >= g.n) continue;
+	const float *__restrict__ U = I.vn[vU];
+	float *__restrict__ ux = I.vn[vUx], *__restrict__ uy = I.vn[vUy], *__restrict__ uz = I.vn[vUz];
+	FOR_TILE(local * TILE, g.n, i) {
 		int x, y, z;
 		g.coords(i, x, y, z);
-		I.vn[vUx][i] = dxf(U, g, i, x);
-		I.vn[vUy][i] = dyf(U, g, i, y);
-		if (g.dims == 3) I.vn[vUz][i] = dzf(U, g, i, z);
+		ux[i] = dxf(U, g, i, x);
+		uy[i] = dyf(U, g, i, y);
+		if (g.dims == 3) uz[i] = dzf(U, g, i, z);
 	}
 }
 
@@ -252,29 +253,35 @@ __global__ void __launch_bounds__(BLOCK) k_shrink_g2(KArgs a) {
 	Geo g(I);
 	Ctrl &c = *I.ctrl;
 	Shrink sh(I, c.beta);
+	const float *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
+	const float *const Sc[3] = {I.vn[vSx], I.vn[vSy], I.vn[vSz]};
+	float *const Wc[3] = {I.vn[vWx], I.vn[vWy], I.vn[vWz]};
+	float *__restrict__ g2 = I.vn[vG2];
 	double v[3] = {0, 0, 0};   // lam1, lam2, lam4
-	long long i0 = (long long)local * TILE;
-	for (int k = 0; k < TILE / BLOCK; k++) {
-		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-		if (i >= g.n) continue;
+	FOR_TILE(local * TILE, g.n, i) {
 		int x, y, z;
 		g.coords(i, x, y, z);
 		float u[3], s[3], w[3];
+#pragma unroll
 		for (int cc = 0; cc < 3; cc++) {
-			u[cc] = cc < g.dims ? I.vn[vUx + cc][i] : 0.f;
-			s[cc] = cc < g.dims ? I.vn[vSx + cc][i] : 0.f;
+			u[cc] = cc < g.dims ? Uc[cc][i] : 0.f;
+			s[cc] = cc < g.dims ? Sc[cc][i] : 0.f;
 		}
 		v[0] += sh.apply(u, s, w);
-		for (int cc = 0; cc < g.dims; cc++) I.vn[vWx + cc][i] = w[cc];
+#pragma unroll
+		for (int cc = 0; cc < 3; cc++)
+			if (cc < g.dims) Wc[cc][i] = w[cc];
 		auto V = [&](int cc) {
-			return [&, cc](long long j) { return j == i ? u[cc] - w[cc] : I.vn[vUx + cc][j] - sh.comp(I, j, cc); };
+			return [&, cc](int j) { return j == i ? u[cc] - w[cc] : Uc[cc][j] - sh.comp(Uc, Sc, j, cc); };
 		};
-		I.vn[vG2][i] = dt_at(g, i, x, y, z, V(0), V(1), V(2));
-		for (int cc = 0; cc < g.dims; cc++) {
-			float vv = u[cc] - w[cc];
-			v[1] += (double)vv * vv;
-			v[2] += (double)s[cc] * vv;
-		}
+		g2[i] = dt_at(g, i, x, y, z, V(0), V(1), V(2));
+#pragma unroll
+		for (int cc = 0; cc < 3; cc++)
+			if (cc < g.dims) {
+				float vv = u[cc] - w[cc];
+				v[1] += (double)vv * vv;
+				v[2] += (double)s[cc] * vv;
+			}
 	}
 	double tot[3];
 	if (!tile_reduce<3>(I, local, I.ntn, v, tot)) return;
@@ -303,29 +310,32 @@ __global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
 	double v[4] = {0, 0, 0, 0};   // lam2, lam4, lam3, lam5
 	if (local < I.ntn) {
 		Geo g(I);
-		long long i0 = (long long)local * TILE;
-		for (int k = 0; k < TILE / BLOCK; k++) {
-			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-			if (i >= g.n) continue;
+		const float *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
+		const float *const Wc[3] = {I.vn[vWx], I.vn[vWy], I.vn[vWz]};
+		const float *const Sc[3] = {I.vn[vSx], I.vn[vSy], I.vn[vSz]};
+		float *__restrict__ gv = I.vn[vG];
+		float *__restrict__ g2 = I.vn[vG2];
+		const float *__restrict__ atb = I.vn[vAtb];
+		FOR_TILE(local * TILE, g.n, i) {
 			int x, y, z;
 			g.coords(i, x, y, z);
-			I.vn[vG][i] = I.vn[vG][i] - I.vn[vAtb][i];
-			auto V = [&](int cc) { return [&, cc](long long j) { return I.vn[vUx + cc][j] - I.vn[vWx + cc][j]; }; };
-			I.vn[vG2][i] = dt_at(g, i, x, y, z, V(0), V(1), V(2));
-			for (int cc = 0; cc < g.dims; cc++) {
-				float vv = I.vn[vUx + cc][i] - I.vn[vWx + cc][i];
-				v[0] += (double)vv * vv;
-				v[1] += (double)I.vn[vSx + cc][i] * vv;
-			}
+			gv[i] = gv[i] - atb[i];
+			auto V = [&](int cc) { return [&, cc](int j) { return Uc[cc][j] - Wc[cc][j]; }; };
+			g2[i] = dt_at(g, i, x, y, z, V(0), V(1), V(2));
+#pragma unroll
+			for (int cc = 0; cc < 3; cc++)
+				if (cc < g.dims) {
+					float vv = Uc[cc][i] - Wc[cc][i];
+					v[0] += (double)vv * vv;
+					v[1] += (double)Sc[cc][i] * vv;
+				}
 		}
 	} else {
-		long long i0 = (long long)(local - I.ntn) * TILE;
-		for (int k = 0; k < TILE / BLOCK; k++) {
-			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-			if (i >= I.m) continue;
-			float r = I.vm[vAu][i] - I.vm[vB][i];
+		const float *__restrict__ au = I.vm[vAu], *__restrict__ bb = I.vm[vB], *__restrict__ dl = I.vm[vDelta];
+		FOR_TILE((local - I.ntn) * TILE, (int)I.m, i) {
+			float r = au[i] - bb[i];
 			v[2] += (double)r * r;
-			v[3] += (double)I.vm[vDelta][i] * r;
+			v[3] += (double)dl[i] * r;
 		}
 	}
 	double tot[4];
@@ -360,44 +370,58 @@ __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 	Ctrl &c = *I.ctrl;
 	const float mdb = (float)c.muDbeta;
 	const float bscale = a.stage == ST_OUTER ? (float)(c.beta0 / c.beta) : 1.f;
-	double v[3] = {0, 0, 0};   // |d|^2, |Up|^2, |uup|^2
-	long long i0 = (long long)local * TILE;
-	for (int k = 0; k < TILE / BLOCK; k++) {
-		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-		if (i >= I.n) continue;
-		float dts = I.vn[vDts][i];
-		if (a.stage == ST_OUTER) {
-			dts = I.vn[vD][i] * bscale;
-			I.vn[vDts][i] = dts;
+	float *__restrict__ dts = I.vn[vDts], *__restrict__ d = I.vn[vD], *__restrict__ uup = I.vn[vUUP];
+	const float *__restrict__ g2 = I.vn[vG2], *__restrict__ gv = I.vn[vG];
+	const float *__restrict__ U = I.vn[vU], *__restrict__ Up = I.vn[vUp];
+	// distance to Ut after the iteration (trace / time-to-solution target)
+	const bool ut = a.stage == ST_LOOP && I.ut_user && (I.trace || I.target > 0);
+	const float scl = (float)c.scl;
+	double v[5] = {0, 0, 0, 0, 0};   // |d|^2, |Up|^2, |uup|^2, |U/scl - Ut|^2, |Ut|^2
+	FOR_TILE(local * TILE, (int)I.n, i) {
+		if (ut) {
+			float t = I.ut_user[i];
+			float e = U[i] / scl - t;
+			v[3] += (double)e * e;
+			v[4] += (double)t * t;
 		}
-		float d = dts + I.vn[vG2][i];
-		d = fmaf(mdb, I.vn[vG][i], d);
-		I.vn[vD][i] = d;
-		v[0] += (double)d * d;
+		float t = dts[i];
+		if (a.stage == ST_OUTER) {
+			t = d[i] * bscale;
+			dts[i] = t;
+		}
+		float dv = t + g2[i];
+		dv = fmaf(mdb, gv[i], dv);
+		d[i] = dv;
+		v[0] += (double)dv * dv;
 		if (a.stage == ST_LOOP) {
-			float up = I.vn[vUp][i];
-			float uu = I.vn[vU][i] - up;
-			I.vn[vUUP][i] = uu;
+			float up = Up[i];
+			float uu = U[i] - up;
+			uup[i] = uu;
 			v[1] += (double)up * up;
 			v[2] += (double)uu * uu;
 		}
 	}
-	double tot[3];
-	if (!tile_reduce<3>(I, local, I.ntn, v, tot)) return;
+	double tot[5];
+	if (!tile_reduce<5>(I, local, I.ntn, v, tot)) return;
 	if (threadIdx.x != 0) return;
 	c.dd = tot[0];
 	if (a.stage == ST_LOOP) {
 		c.count_total++;
 		c.nrmup = sqrt(tot[1]);
 		c.relchg = sqrt(tot[2]) / c.nrmup;
+		c.relerr_ut = ut ? sqrt(tot[3]) / sqrt(tot[4]) : 0.0;
 		if (I.trace && c.count_total <= I.maxit) {
-			double *t = I.trace + (long long)(c.count_total - 1) * 5;
-			t[0] = c.tau; t[1] = c.f; t[2] = c.relchg; t[3] = c.bt_cnt; t[4] = c.skip_adj;
+			double *t = I.trace + (long long)(c.count_total - 1) * TRACE_DOUBLES;
+			t[0] = c.tau; t[1] = c.f; t[2] = c.relchg; t[3] = c.bt_cnt; t[4] = c.skip_adj; t[5] = c.relerr_ut;
 		}
 		c.bt_cnt = 0;
 		bool brk = (c.relchg < I.tol_inn) && !c.fst;
 		c.inner_break = brk || c.count_total >= I.maxit;
 		if (!brk) c.fst = 0;
+		if (ut && I.target > 0 && c.relerr_ut <= I.target) {   // time-to-solution target reached
+			c.active = 0;
+			c.inner_break = 0;
+		}
 		if (bad(c.dd)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; c.inner_break = 0; }
 	} else if (a.stage == ST_INIT) {
 		c.Q = 1; c.C = c.f;
@@ -421,12 +445,9 @@ __global__ void __launch_bounds__(BLOCK) k_tau_prep(KArgs a) {
 	const float mdb = (float)c.muDbeta;
 	Geo g(I);
 	double v[2] = {0, 0};
-	long long i0 = (long long)local * TILE;
-	const float *d = I.vn[vD];
-	for (int k = 0; k < TILE / BLOCK; k++) {
-		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-		if (i >= g.n) continue;
-		if (first) {
+	const float *__restrict__ d = I.vn[vD];
+	if (first) {
+		FOR_TILE(local * TILE, g.n, i) {
 			int x, y, z;
 			g.coords(i, x, y, z);
 			float t = dxf(d, g, i, x);
@@ -434,12 +455,17 @@ __global__ void __launch_bounds__(BLOCK) k_tau_prep(KArgs a) {
 			t = dyf(d, g, i, y);
 			v[0] += (double)t * t;
 			if (g.dims == 3) { t = dzf(d, g, i, z); v[0] += (double)t * t; }
-		} else {
-			float dg = I.vn[vG][i] - I.vn[vGp][i];
-			float dg2 = I.vn[vG2][i] - I.vn[vG2p][i];
-			I.vn[vdG][i] = dg;
-			I.vn[vdG2][i] = dg2;
-			float uu = I.vn[vUUP][i];
+		}
+	} else {
+		const float *__restrict__ gv = I.vn[vG], *__restrict__ gp = I.vn[vGp];
+		const float *__restrict__ g2 = I.vn[vG2], *__restrict__ g2p = I.vn[vG2p], *__restrict__ uup = I.vn[vUUP];
+		float *__restrict__ dgv = I.vn[vdG], *__restrict__ dg2v = I.vn[vdG2];
+		FOR_TILE(local * TILE, g.n, i) {
+			float dg = gv[i] - gp[i];
+			float dg2 = g2[i] - g2p[i];
+			dgv[i] = dg;
+			dg2v[i] = dg2;
+			float uu = uup[i];
 			float tmp = fmaf(mdb, dg, dg2);
 			v[0] += (double)uu * uu;
 			v[1] += (double)uu * tmp;
@@ -462,10 +488,10 @@ __global__ void __launch_bounds__(BLOCK) k_tau_first(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	double v[1] = {0};
-	long long i0 = (long long)local * TILE;
-	for (int k = 0; k < TILE / BLOCK; k++) {
-		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-		if (i < I.m) { float t = I.vm[vAd][i]; v[0] += (double)t * t; }
+	const float *__restrict__ ad = I.vm[vAd];
+	FOR_TILE(local * TILE, (int)I.m, i) {
+		float t = ad[i];
+		v[0] += (double)t * t;
 	}
 	double tot[1];
 	if (!tile_reduce<1>(I, local, I.ntm, v, tot)) return;
@@ -487,30 +513,27 @@ __global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
 	const float ntau = (float)(-1 * c.tau);
 	const bool snap = a.stage == ST_DESCEND;
 	if (local < I.ntn) {
-		long long i0 = (long long)local * TILE;
-		for (int k = 0; k < TILE / BLOCK; k++) {
-			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-			if (i >= I.n) continue;
+		float *__restrict__ U = I.vn[vU], *__restrict__ Up = I.vn[vUp];
+		const float *__restrict__ d = I.vn[vD];
+		FOR_TILE(local * TILE, (int)I.n, i) {
 			float u;
 			if (snap) {
-				u = I.vn[vU][i];
-				I.vn[vUp][i] = u;
+				u = U[i];
+				Up[i] = u;
 				I.vn[vGp][i] = I.vn[vG][i];
 				I.vn[vG2p][i] = I.vn[vG2][i];
-				for (int cc = 0; cc < I.dims; cc++) I.vn[vUxp + cc][i] = I.vn[vUx + cc][i];
+#pragma unroll
+				for (int cc = 0; cc < 3; cc++)
+					if (cc < I.dims) I.vn[vUxp + cc][i] = I.vn[vUx + cc][i];
 			} else {
-				u = I.vn[vUp][i];
+				u = Up[i];
 			}
-			u = fmaf(ntau, I.vn[vD][i], u);
+			u = fmaf(ntau, d[i], u);
 			if (I.nonneg) u = u < 0.f ? 0.f : u;
-			I.vn[vU][i] = u;
+			U[i] = u;
 		}
 	} else if (snap) {
-		long long i0 = (long long)(local - I.ntn) * TILE;
-		for (int k = 0; k < TILE / BLOCK; k++) {
-			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-			if (i < I.m) I.vm[vAup][i] = I.vm[vAu][i];
-		}
+		FOR_TILE((local - I.ntn) * TILE, (int)I.m, i) I.vm[vAup][i] = I.vm[vAu][i];
 	}
 }
 
@@ -518,21 +541,16 @@ __global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
 __global__ void __launch_bounds__(BLOCK) k_bt_diff(KArgs a) {
 	KPROLOGUE(a);
 	if (local < I.ntn) {
-		long long i0 = (long long)local * TILE;
-		for (int k = 0; k < TILE / BLOCK; k++) {
-			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-			if (i >= I.n) continue;
+		FOR_TILE(local * TILE, (int)I.n, i) {
 			I.vn[vdU][i] = I.vn[vU][i] - I.vn[vUp][i];
 			I.vn[vdG][i] = I.vn[vG][i] - I.vn[vGp][i];
 			I.vn[vdG2][i] = I.vn[vG2][i] - I.vn[vG2p][i];
-			for (int cc = 0; cc < I.dims; cc++) I.vn[vdUx + cc][i] = I.vn[vUx + cc][i] - I.vn[vUxp + cc][i];
+#pragma unroll
+			for (int cc = 0; cc < 3; cc++)
+				if (cc < I.dims) I.vn[vdUx + cc][i] = I.vn[vUx + cc][i] - I.vn[vUxp + cc][i];
 		}
 	} else {
-		long long i0 = (long long)(local - I.ntn) * TILE;
-		for (int k = 0; k < TILE / BLOCK; k++) {
-			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-			if (i < I.m) I.vm[vdAu][i] = I.vm[vAu][i] - I.vm[vAup][i];
-		}
+		FOR_TILE((local - I.ntn) * TILE, (int)I.m, i) I.vm[vdAu][i] = I.vm[vAu][i] - I.vm[vAup][i];
 	}
 }
 
@@ -544,26 +562,22 @@ __global__ void __launch_bounds__(BLOCK) k_lerp(KArgs a) {
 	const float al = (float)alpha_new;
 	double v[4] = {0, 0, 0, 0};   // lam2, lam4, lam3, lam5
 	if (local < I.ntn) {
-		long long i0 = (long long)local * TILE;
-		for (int k = 0; k < TILE / BLOCK; k++) {
-			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-			if (i >= I.n) continue;
+		FOR_TILE(local * TILE, (int)I.n, i) {
 			I.vn[vG][i] = fmaf(al, I.vn[vdG][i], I.vn[vGp][i]);
 			I.vn[vG2][i] = fmaf(al, I.vn[vdG2][i], I.vn[vG2p][i]);
 			I.vn[vU][i] = fmaf(al, I.vn[vdU][i], I.vn[vUp][i]);
-			for (int cc = 0; cc < I.dims; cc++) {
-				float ux = fmaf(al, I.vn[vdUx + cc][i], I.vn[vUxp + cc][i]);
-				I.vn[vUx + cc][i] = ux;
-				float vv = ux - I.vn[vWx + cc][i];
-				v[0] += (double)vv * vv;
-				v[1] += (double)I.vn[vSx + cc][i] * vv;
-			}
+#pragma unroll
+			for (int cc = 0; cc < 3; cc++)
+				if (cc < I.dims) {
+					float ux = fmaf(al, I.vn[vdUx + cc][i], I.vn[vUxp + cc][i]);
+					I.vn[vUx + cc][i] = ux;
+					float vv = ux - I.vn[vWx + cc][i];
+					v[0] += (double)vv * vv;
+					v[1] += (double)I.vn[vSx + cc][i] * vv;
+				}
 		}
 	} else {
-		long long i0 = (long long)(local - I.ntn) * TILE;
-		for (int k = 0; k < TILE / BLOCK; k++) {
-			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-			if (i >= I.m) continue;
+		FOR_TILE((local - I.ntn) * TILE, (int)I.m, i) {
 			float au = fmaf(al, I.vm[vdAu][i], I.vm[vAup][i]);
 			I.vm[vAu][i] = au;
 			float r = au - I.vm[vB][i];
@@ -593,14 +607,13 @@ __global__ void __launch_bounds__(BLOCK) k_outer(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	double v[1] = {0};
-	long long i0 = (long long)local * TILE;
-	for (int k = 0; k < TILE / BLOCK; k++) {
-		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-		if (i >= I.n) continue;
-		float u = I.vn[vU][i];
-		float dlt = u - I.vn[vRcd][i];
+	float *__restrict__ rcd = I.vn[vRcd];
+	const float *__restrict__ U = I.vn[vU];
+	FOR_TILE(local * TILE, (int)I.n, i) {
+		float u = U[i];
+		float dlt = u - rcd[i];
 		v[0] += (double)dlt * dlt;
-		I.vn[vRcd][i] = u;
+		rcd[i] = u;
 	}
 	double tot[1];
 	if (!tile_reduce<1>(I, local, I.ntn, v, tot)) return;
@@ -621,22 +634,18 @@ __global__ void __launch_bounds__(BLOCK) k_mlp(KArgs a) {
 	const float nbeta = (float)(-1 * c.beta), nmu = (float)(-1 * c.mu);
 	double v[2] = {0, 0};   // lam4, lam5
 	if (local < I.ntn) {
-		long long i0 = (long long)local * TILE;
-		for (int k = 0; k < TILE / BLOCK; k++) {
-			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-			if (i >= I.n) continue;
-			for (int cc = 0; cc < I.dims; cc++) {
-				float vv = I.vn[vUx + cc][i] - I.vn[vWx + cc][i];
-				float s = fmaf(nbeta, vv, I.vn[vSx + cc][i]);
-				I.vn[vSx + cc][i] = s;
-				v[0] += (double)s * vv;
-			}
+		FOR_TILE(local * TILE, (int)I.n, i) {
+#pragma unroll
+			for (int cc = 0; cc < 3; cc++)
+				if (cc < I.dims) {
+					float vv = I.vn[vUx + cc][i] - I.vn[vWx + cc][i];
+					float s = fmaf(nbeta, vv, I.vn[vSx + cc][i]);
+					I.vn[vSx + cc][i] = s;
+					v[0] += (double)s * vv;
+				}
 		}
 	} else {
-		long long i0 = (long long)(local - I.ntn) * TILE;
-		for (int k = 0; k < TILE / BLOCK; k++) {
-			long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-			if (i >= I.m) continue;
+		FOR_TILE((local - I.ntn) * TILE, (int)I.m, i) {
 			float r = I.vm[vAu][i] - I.vm[vB][i];
 			float dl = fmaf(nmu, r, I.vm[vDelta][i]);
 			I.vm[vDelta][i] = dl;
@@ -664,10 +673,7 @@ __global__ void __launch_bounds__(BLOCK) k_final(KArgs a) {
 	Ctrl &c = *I.ctrl;
 	const float scl = (float)c.scl;
 	double v[2] = {0, 0};
-	long long i0 = (long long)local * TILE;
-	for (int k = 0; k < TILE / BLOCK; k++) {
-		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-		if (i >= I.n) continue;
+	FOR_TILE(local * TILE, (int)I.n, i) {
 		float u = I.vn[vU][i] / scl;
 		I.u_user[i] = u;
 		if (I.ut_user) {
@@ -689,10 +695,7 @@ __global__ void __launch_bounds__(BLOCK) k_skip_norms(KArgs a) {
 	if (!I.skip_enabled) return;
 	Ctrl &c = *I.ctrl;
 	double v[2] = {0, 0};
-	long long i0 = (long long)local * TILE;
-	for (int k = 0; k < TILE / BLOCK; k++) {
-		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-		if (i >= I.m) continue;
+	FOR_TILE(local * TILE, (int)I.m, i) {
 		float au = I.vm[vAu][i];
 		float dl = au - I.vm[vLastAu][i];
 		v[0] += (double)dl * dl;
@@ -713,11 +716,7 @@ __global__ void __launch_bounds__(BLOCK) k_skip_norms(KArgs a) {
 __global__ void __launch_bounds__(BLOCK) k_copy_lastau(KArgs a) {
 	KPROLOGUE(a);
 	if (!I.skip_enabled) return;
-	long long i0 = (long long)local * TILE;
-	for (int k = 0; k < TILE / BLOCK; k++) {
-		long long i = i0 + threadIdx.x + (long long)k * BLOCK;
-		if (i < I.m) I.vm[vLastAu][i] = I.vm[vAu][i];
-	}
+	FOR_TILE(local * TILE, (int)I.m, i) I.vm[vLastAu][i] = I.vm[vAu][i];
 }
 
 __global__ void k_cond(const Inst *tab, int count, int pred, int *flag, unsigned long long handle,
@@ -737,15 +736,20 @@ __global__ void k_cond(const Inst *tab, int count, int pred, int *flag, unsigned
 // ---------------------------------------------------------------------------
 struct PlainGeo {
 	int dims, p, q, r;
+	FastDiv fq, fp;
 };
 
-__global__ void k_D_plain(PlainGeo pg, const float *U, float *Ux, float *Uy, float *Uz) {
+__device__ __forceinline__ Geo plain_geo(const PlainGeo &pg) {
 	Inst I{};
 	I.dims = pg.dims; I.p = pg.p; I.q = pg.q; I.r = pg.r;
 	I.n = (long long)pg.p * pg.q * pg.r;
-	Geo g(I);
-	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < g.n;
-	     i += (long long)gridDim.x * blockDim.x) {
+	I.fq = pg.fq; I.fp = pg.fp;
+	return Geo(I);
+}
+
+__global__ void k_D_plain(PlainGeo pg, const float *U, float *Ux, float *Uy, float *Uz) {
+	Geo g = plain_geo(pg);
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
 		int x, y, z;
 		g.coords(i, x, y, z);
 		Ux[i] = dxf(U, g, i, x);
@@ -755,16 +759,12 @@ __global__ void k_D_plain(PlainGeo pg, const float *U, float *Ux, float *Uy, flo
 }
 
 __global__ void k_Dt_plain(PlainGeo pg, const float *X, const float *Y, const float *Z, float *res) {
-	Inst I{};
-	I.dims = pg.dims; I.p = pg.p; I.q = pg.q; I.r = pg.r;
-	I.n = (long long)pg.p * pg.q * pg.r;
-	Geo g(I);
-	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < g.n;
-	     i += (long long)gridDim.x * blockDim.x) {
+	Geo g = plain_geo(pg);
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
 		int x, y, z;
 		g.coords(i, x, y, z);
-		res[i] = dt_at(g, i, x, y, z, [&](long long j) { return X[j]; }, [&](long long j) { return Y[j]; },
-		               [&](long long j) { return Z ? Z[j] : 0.f; });
+		res[i] = dt_at(g, i, x, y, z, [&](int j) { return X[j]; }, [&](int j) { return Y[j]; },
+		               [&](int j) { return Z ? Z[j] : 0.f; });
 	}
 }
 
@@ -828,16 +828,23 @@ static int grid_for(long long n) {
 	return (int)(g < 1 ? 1 : g);
 }
 
+static PlainGeo plain(int dims, int p, int q, int r) {
+	PlainGeo g{dims, p, q, dims == 3 ? r : 1, {}, {}};
+	g.fq.init((unsigned)q);
+	g.fp.init((unsigned)p);
+	return g;
+}
+
 void launch_D_plain(cudaStream_t s, int dims, int p, int q, int r, const float *U, float *Ux, float *Uy,
                     float *Uz) {
-	PlainGeo g{dims, p, q, dims == 3 ? r : 1};
+	PlainGeo g = plain(dims, p, q, r);
 	k_D_plain<<<grid_for((long long)p * q * g.r), 256, 0, s>>>(g, U, Ux, Uy, Uz);
 	TG_CUDA(cudaGetLastError());
 }
 
 void launch_Dt_plain(cudaStream_t s, int dims, int p, int q, int r, const float *X, const float *Y,
                      const float *Z, float *res) {
-	PlainGeo g{dims, p, q, dims == 3 ? r : 1};
+	PlainGeo g = plain(dims, p, q, r);
 	k_Dt_plain<<<grid_for((long long)p * q * g.r), 256, 0, s>>>(g, X, Y, Z, res);
 	TG_CUDA(cudaGetLastError());
 }

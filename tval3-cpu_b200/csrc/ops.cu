@@ -38,23 +38,23 @@ __global__ void __launch_bounds__(256) k_dense_fwd(const Inst *tab, TileMap map,
 	if (row >= m) return;
 	const float *a = op.A + row * n;
 	const float *x = vsel(I, xs) + layer * n;
-	float acc = 0.f;
+	double acc = 0.0;   // FP64 accumulation of FP32 products
 	if ((n & 3) == 0 && ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(x)) & 15) == 0) {
 		const float4 *a4 = reinterpret_cast<const float4 *>(a);
 		const float4 *x4 = reinterpret_cast<const float4 *>(x);
 		const long long n4 = n >> 2;
 		for (long long j = lane; j < n4; j += 32) {
 			float4 av = __ldg(a4 + j), xv = __ldg(x4 + j);
-			acc = fmaf(av.x, xv.x, acc);
-			acc = fmaf(av.y, xv.y, acc);
-			acc = fmaf(av.z, xv.z, acc);
-			acc = fmaf(av.w, xv.w, acc);
+			acc = fma((double)av.x, (double)xv.x, acc);
+			acc = fma((double)av.y, (double)xv.y, acc);
+			acc = fma((double)av.z, (double)xv.z, acc);
+			acc = fma((double)av.w, (double)xv.w, acc);
 		}
 	} else {
-		for (long long j = lane; j < n; j += 32) acc = fmaf(__ldg(a + j), __ldg(x + j), acc);
+		for (long long j = lane; j < n; j += 32) acc = fma((double)__ldg(a + j), (double)__ldg(x + j), acc);
 	}
-	acc = warp_sumf(acc);
-	if (lane == 0) vselw(I, ys)[layer * m + row] = acc;
+	acc = warp_sum(acc);
+	if (lane == 0) vselw(I, ys)[layer * m + row] = (float)acc;
 }
 
 // partial column sums of A^T x over one row chunk
@@ -72,32 +72,32 @@ __global__ void __launch_bounds__(256) k_dense_adj(const Inst *tab, TileMap map,
 	const long long r0 = kc * rows_per, r1 = min(m, r0 + rows_per);
 	const long long c0 = ct * 1024 + threadIdx.x * 4;
 	const float *x = vsel(I, xs) + layer * m;
-	float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
+	double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;   // FP64 accumulation
 	if ((n & 3) == 0 && (reinterpret_cast<uintptr_t>(op.A) & 15) == 0) {
 		if (c0 < n)
 			for (long long r = r0; r < r1; r++) {
 				float xv = __ldg(x + r);
 				float4 av = __ldg(reinterpret_cast<const float4 *>(op.A + r * n + c0));
-				acc0 = fmaf(av.x, xv, acc0);
-				acc1 = fmaf(av.y, xv, acc1);
-				acc2 = fmaf(av.z, xv, acc2);
-				acc3 = fmaf(av.w, xv, acc3);
+				acc0 = fma((double)av.x, (double)xv, acc0);
+				acc1 = fma((double)av.y, (double)xv, acc1);
+				acc2 = fma((double)av.z, (double)xv, acc2);
+				acc3 = fma((double)av.w, (double)xv, acc3);
 			}
 	} else {
 		for (long long r = r0; r < r1; r++) {
 			float xv = __ldg(x + r);
 			const float *ar = op.A + r * n;
-			if (c0 + 0 < n) acc0 = fmaf(__ldg(ar + c0 + 0), xv, acc0);
-			if (c0 + 1 < n) acc1 = fmaf(__ldg(ar + c0 + 1), xv, acc1);
-			if (c0 + 2 < n) acc2 = fmaf(__ldg(ar + c0 + 2), xv, acc2);
-			if (c0 + 3 < n) acc3 = fmaf(__ldg(ar + c0 + 3), xv, acc3);
+			if (c0 + 0 < n) acc0 = fma((double)__ldg(ar + c0 + 0), (double)xv, acc0);
+			if (c0 + 1 < n) acc1 = fma((double)__ldg(ar + c0 + 1), (double)xv, acc1);
+			if (c0 + 2 < n) acc2 = fma((double)__ldg(ar + c0 + 2), (double)xv, acc2);
+			if (c0 + 3 < n) acc3 = fma((double)__ldg(ar + c0 + 3), (double)xv, acc3);
 		}
 	}
 	float *p = part + op.dense_part + (layer * K + kc) * n;
-	if (c0 + 0 < n) p[c0 + 0] = acc0;
-	if (c0 + 1 < n) p[c0 + 1] = acc1;
-	if (c0 + 2 < n) p[c0 + 2] = acc2;
-	if (c0 + 3 < n) p[c0 + 3] = acc3;
+	if (c0 + 0 < n) p[c0 + 0] = (float)acc0;
+	if (c0 + 1 < n) p[c0 + 1] = (float)acc1;
+	if (c0 + 2 < n) p[c0 + 2] = (float)acc2;
+	if (c0 + 3 < n) p[c0 + 3] = (float)acc3;
 }
 
 __global__ void __launch_bounds__(256) k_dense_red(const Inst *tab, TileMap map, int pred, VecSel xs, VecSel ys,
@@ -113,9 +113,9 @@ __global__ void __launch_bounds__(256) k_dense_red(const Inst *tab, TileMap map,
 	for (int e = 0; e < 4; e++) {
 		long long c = ct * 1024 + e * 256 + threadIdx.x;
 		if (c >= n) continue;
-		float s = 0.f;
+		double s = 0.0;
 		for (int k = 0; k < K; k++) s += p[(long long)k * n + c];
-		y[c] = s;
+		y[c] = (float)s;
 	}
 }
 
@@ -141,17 +141,18 @@ __global__ void __launch_bounds__(256) k_gather(const Inst *tab, TileMap map, in
 	const long long line = (local - layer * lt) * LPB + threadIdx.x / W;
 	const int gl = threadIdx.x % W;
 	const float *x = vsel(I, xs) + layer * xlen;
-	float acc = 0.f;
+	double acc = 0.0;   // FP64 accumulation of FP32 products
 	if (line < lines) {
 		const int k0 = ptr[line], k1 = ptr[line + 1];
 		if (val)
-			for (int k = k0 + gl; k < k1; k += W) acc = fmaf(__ldg(val + k), __ldg(x + __ldg(ind + k)), acc);
+			for (int k = k0 + gl; k < k1; k += W)
+				acc = fma((double)__ldg(val + k), (double)__ldg(x + __ldg(ind + k)), acc);
 		else
 			for (int k = k0 + gl; k < k1; k += W) acc += __ldg(x + __ldg(ind + k));
 	}
 #pragma unroll
 	for (int o = W / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-	if (gl == 0 && line < lines) vselw(I, ys)[layer * ylen + line] = val ? acc : acc * op.scale;
+	if (gl == 0 && line < lines) vselw(I, ys)[layer * ylen + line] = (float)(val ? acc : acc * op.scale);
 }
 
 // ---------------------------------------------------------------------------
@@ -200,25 +201,227 @@ struct MinorStep {
 	}
 };
 
+// Forward projection, SUBW lanes per ray.  Lane l takes the hits j = l,
+// l + SUBW, ...; the linear index advances by SUBW driving steps plus, per
+// minor axis, the exact quotient / remainder increments of the closed form
+// floor((2 j a + M - 1) / (2 M)) - one add and one compare-carry per axis.
+// All index arithmetic is 32-bit (images and volumes are below 2^31 voxels,
+// extents below 2^15).
+template <int SUBW, bool D3>
 __global__ void __launch_bounds__(256) k_ray_fwd(const Inst *tab, TileMap map, int pred, VecSel xs, VecSel ys,
                                                  unsigned long long *launches) {
 	OPROLOGUE();
 	const OpDev &op = I.op;
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const long long ray = local * WARPS + warp;
-	if (ray >= op.nrays) return;
-	RayWalk w(op.rays[ray]);
+	constexpr int RPB = 256 / SUBW;   // rays per block
+	const int gl = threadIdx.x % SUBW;
+	const long long ray = local * RPB + threadIdx.x / SUBW;
 	const float *x = vsel(I, xs);
-	const long long rvxy = (long long)op.rvx * op.rvy;
-	MinorStep s1(lane, w.a1, w.M, 32), s2(lane, w.a2, w.M, 32);
-	float acc = 0.f;
-	for (int j = lane; j <= w.M; j += 32) {
-		acc += __ldg(x + w.index(j, s1.q, s2.q, op.rvx, rvxy));
-		s1.advance();
-		s2.advance();
+	double acc = 0.0;   // FP64 accumulation along the ray
+	int out = -1;
+	if (ray < op.nrays) {
+		int x0, y0, z0, dx, dy, dz;
+		unpack_ray(op.rays[ray], x0, y0, z0, dx, dy, dz, out);
+		const int mx = abs(dx), my = abs(dy), mz = D3 ? abs(dz) : 0;
+		const int sx = dx < 0 ? -1 : 1, sy = (dy < 0 ? -1 : 1) * op.rvx;
+		const int sz = (dz < 0 ? -1 : 1) * op.rvx * op.rvy;
+		// driving axis (3d/mat_mult.h:241,280; 2D: 2d/mat_mult.h:160)
+		int M, a1, a2, sd, s1, s2;
+		int idx = x0 + y0 * op.rvx + z0 * op.rvx * op.rvy;
+		if (mx >= my && mx >= mz) { M = mx; sd = sx; a1 = my; s1 = sy; a2 = mz; s2 = sz; }
+		else if (my >= mx && my >= mz) {
+			M = my; sd = sy; a1 = mx; s1 = sx; a2 = mz; s2 = sz;
+			if (!D3 && op.xT) {   // transposed image: y steps are contiguous
+				x = op.xT;
+				idx = y0 + x0 * op.tH;
+				sd = dy < 0 ? -1 : 1;
+				s1 = (dx < 0 ? -1 : 1) * op.tH;
+			}
+		} else { M = mz; sd = sz; a1 = mx; s1 = sx; a2 = my; s2 = sy; }
+		idx += gl * sd;
+		const int twoM = 2 * M > 0 ? 2 * M : 1;
+		int q1 = 0, r1 = 0, qa1 = 0, ra1 = 0, q2 = 0, r2 = 0, qa2 = 0, ra2 = 0;
+		if (M > 0) {
+			int num = 2 * gl * a1 + M - 1;
+			q1 = num / twoM; r1 = num - q1 * twoM;
+			qa1 = (2 * SUBW * a1) / twoM; ra1 = 2 * SUBW * a1 - qa1 * twoM;
+			idx += q1 * s1;
+			if (D3) {
+				num = 2 * gl * a2 + M - 1;
+				q2 = num / twoM; r2 = num - q2 * twoM;
+				qa2 = (2 * SUBW * a2) / twoM; ra2 = 2 * SUBW * a2 - qa2 * twoM;
+				idx += q2 * s2;
+			}
+		}
+		const int dstep = SUBW * sd + qa1 * s1 + (D3 ? qa2 * s2 : 0);
+#pragma unroll 4
+		for (int j = gl; j <= M; j += SUBW) {
+			acc += __ldg(x + idx);
+			idx += dstep;
+			r1 += ra1;
+			if (r1 >= twoM) { r1 -= twoM; idx += s1; }
+			if (D3) {
+				r2 += ra2;
+				if (r2 >= twoM) { r2 -= twoM; idx += s2; }
+			}
+		}
 	}
-	acc = warp_sumf(acc);
-	if (lane == 0) vselw(I, ys)[w.out] = acc * op.scale;
+#pragma unroll
+	for (int o = SUBW / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+	if (gl == 0 && out >= 0) vselw(I, ys)[out] = (float)(acc * op.scale);
+}
+
+// xT[y + x*tH] = x[x + y*ld] for the 2D forward (32x32 tiles through shared
+// memory; local tile = ty * ceil(ld/32) + tx)
+__global__ void __launch_bounds__(256) k_transpose2d(const Inst *tab, TileMap map, int pred, VecSel xs,
+                                                     unsigned long long *launches) {
+	OPROLOGUE();
+	__shared__ float tile[32][33];
+	const OpDev &op = I.op;
+	const int ld = op.rvx, H = op.tH;
+	const int ntx = (ld + 31) / 32;
+	const int bx = (int)local % ntx, by = (int)local / ntx;
+	const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+	const float *X = vsel(I, xs);
+#pragma unroll
+	for (int j = 0; j < 32; j += 8) {
+		const int x = bx * 32 + tx, y = by * 32 + ty + j;
+		if (x < ld && y < H) tile[ty + j][tx] = X[x + y * ld];
+	}
+	__syncthreads();
+#pragma unroll
+	for (int j = 0; j < 32; j += 8) {
+		const int y = by * 32 + tx, x = bx * 32 + ty + j;
+		if (x < ld && y < H) op.xT[y + x * H] = tile[tx][ty + j];
+	}
+}
+
+// ---------------------------------------------------------------------------
+// staged 2D ray adjoint
+// ---------------------------------------------------------------------------
+// ylive[k] = y[measurement index of traced ray k]
+__global__ void __launch_bounds__(256) k_ray_compact(const Inst *tab, TileMap map, int pred, VecSel xs,
+                                                     unsigned long long *launches) {
+	OPROLOGUE();
+	const OpDev &op = I.op;
+	const int k = (int)local * 256 + threadIdx.x;
+	if (k < op.nrays) op.ylive[k] = vsel(I, xs)[op.live_out[k]];
+}
+
+constexpr int STAGED_THREADS = 512;   // one pixel per thread: ppb <= 512
+constexpr int STAGED_PAD = 8;         // per-chunk segments padded to 8 entries (16 bytes)
+constexpr unsigned short STAGED_SENTINEL = RAY_CHUNK;   // pad entry: reads the zero slot
+
+int staged_smem_bytes(int) { return (int)sizeof(float) * (RAY_CHUNK + STAGED_PAD); }
+
+// g[p] = scale * sum over the rays through p of ylive[ray]: chunk by chunk,
+// the chunk of ylive is copied to shared memory (slot RAY_CHUNK holds 0 for
+// the pad entries) and each thread sums its pixel's entries of the chunk in
+// ray order, reading them eight at a time with 16-byte loads
+__global__ void __launch_bounds__(STAGED_THREADS) k_ray_adj_staged(const Inst *tab, TileMap map, int pred,
+                                                                   VecSel ys, unsigned long long *launches) {
+	OPROLOGUE();
+	extern __shared__ float smem[];
+	float *chunk = smem;
+	const OpDev &op = I.op;
+	const int n = (int)I.n, NC = op.nchunks;
+	const int p = (int)local * op.ppb + threadIdx.x;
+	const bool own = threadIdx.x < op.ppb && p < n;
+	constexpr int V4 = RAY_CHUNK / 4 / STAGED_THREADS;   // float4 per thread per chunk
+	if (threadIdx.x < STAGED_PAD) chunk[RAY_CHUNK + threadIdx.x] = 0.f;
+	const int *so = op.soff + (long long)(own ? p : 0) * (NC + 1);
+	// eight interleaved FP64 partial sums (one per index slot), added by a
+	// fixed tree at the end: deterministic
+	double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+	for (int c = 0; c < NC; c++) {
+		const int c0 = c * RAY_CHUNK, cl = min(RAY_CHUNK, op.nrays - c0);
+		__syncthreads();
+		// all loads of the chunk in flight at once (ylive holds whole chunks)
+		const float4 *src = reinterpret_cast<const float4 *>(op.ylive + c0);
+		float4 r[V4];
+#pragma unroll
+		for (int u = 0; u < V4; u++) {
+			const int t4 = threadIdx.x + u * STAGED_THREADS;
+			r[u] = (4 * t4 < cl) ? __ldcg(src + t4) : make_float4(0.f, 0.f, 0.f, 0.f);
+		}
+#pragma unroll
+		for (int u = 0; u < V4; u++) reinterpret_cast<float4 *>(chunk)[threadIdx.x + u * STAGED_THREADS] = r[u];
+		__syncthreads();
+		if (own) {
+			const int k0 = __ldg(so + c), k1 = __ldg(so + c + 1);
+			const uint4 *ix = reinterpret_cast<const uint4 *>(op.sidx + k0);
+			const int nv = (k1 - k0) / STAGED_PAD;
+#pragma unroll 4
+			for (int v = 0; v < nv; v++) {
+				const uint4 w = __ldg(ix + v);
+				acc[0] += chunk[w.x & 0xffff]; acc[1] += chunk[w.x >> 16];
+				acc[2] += chunk[w.y & 0xffff]; acc[3] += chunk[w.y >> 16];
+				acc[4] += chunk[w.z & 0xffff]; acc[5] += chunk[w.z >> 16];
+				acc[6] += chunk[w.w & 0xffff]; acc[7] += chunk[w.w >> 16];
+			}
+		}
+	}
+	const double sum = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+	if (own) vselw(I, ys)[p] = (float)(sum * op.scale);
+}
+
+// padded length of every pixel's list (each chunk segment rounded up to 8)
+__global__ void k_stage_count(long long n, int nchunks, const int *cptr, const int *cind, long long *plen) {
+	const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (p >= n) return;
+	long long len = 0;
+	int k = cptr[p];
+	const int k1 = cptr[p + 1];
+	for (int c = 0; c < nchunks; c++) {
+		int cnt = 0;
+		while (k < k1 && cind[k] < (c + 1) * RAY_CHUNK) { k++; cnt++; }
+		len += (cnt + STAGED_PAD - 1) / STAGED_PAD * STAGED_PAD;
+	}
+	plen[p] = len;
+}
+
+// write the padded 16-bit lists and the per-pixel chunk boundaries
+__global__ void k_stage_fill(long long n, int nchunks, const int *cptr, const int *cind, const long long *pbase,
+                             unsigned short *sidx, int *soff) {
+	const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (p >= n) return;
+	int k = cptr[p];
+	const int k1 = cptr[p + 1];
+	int *so = soff + p * (nchunks + 1);
+	long long w = pbase[p];
+	for (int c = 0; c < nchunks; c++) {
+		so[c] = (int)w;
+		int cnt = 0;
+		while (k < k1 && cind[k] < (c + 1) * RAY_CHUNK) {
+			sidx[w++] = (unsigned short)(cind[k] - c * RAY_CHUNK);
+			k++; cnt++;
+		}
+		while (cnt % STAGED_PAD) { sidx[w++] = STAGED_SENTINEL; cnt++; }
+	}
+	so[nchunks] = (int)w;
+}
+
+long long build_staged_index(cudaStream_t s, long long n, int nrays, const int *cptr, const int *cind,
+                             unsigned short **sidx_out, int *soff, std::vector<void *> &owned) {
+	const int nchunks = (nrays + RAY_CHUNK - 1) / RAY_CHUNK;
+	long long *plen = nullptr, *pbase = nullptr;
+	TG_CUDA(cudaMallocAsync(&plen, sizeof(long long) * (n + 1), s));
+	TG_CUDA(cudaMallocAsync(&pbase, sizeof(long long) * (n + 1), s));
+	k_stage_count<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, nchunks, cptr, cind, plen);
+	scan_counts(s, plen, pbase, n);
+	long long total = 0;
+	TG_CUDA(cudaMemcpyAsync(&total, pbase + n, sizeof(long long), cudaMemcpyDeviceToHost, s));
+	TG_CUDA(cudaStreamSynchronize(s));
+	unsigned short *sidx = nullptr;
+	TG_CUDA(cudaMalloc(&sidx, sizeof(unsigned short) * (size_t)std::max(total, 8LL)));
+	owned.push_back(sidx);
+	k_stage_fill<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, nchunks, cptr, cind, pbase, sidx, soff);
+	TG_CUDA(cudaGetLastError());
+	TG_CUDA(cudaFreeAsync(plen, s));
+	TG_CUDA(cudaFreeAsync(pbase, s));
+	TG_CUDA(cudaFuncSetAttribute(k_ray_adj_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                             staged_smem_bytes(0)));
+	*sidx_out = sidx;
+	return total;
 }
 
 // ---------------------------------------------------------------------------
@@ -244,8 +447,16 @@ void op_forward(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel
 		TG_CUDA(cudaGetLastError());
 	}
 	gather(L, B.csr_fwd, pred, 0, x, y);
-	if (B.ray_fwd.count > 0) {
-		k_ray_fwd<<<B.ray_fwd.count, 256, 0, L.stream>>>(L.inst, B.ray_fwd, pred, x, y, ctr);
+	if (B.ray2_transpose.count > 0) {
+		k_transpose2d<<<B.ray2_transpose.count, 256, 0, L.stream>>>(L.inst, B.ray2_transpose, pred, x, ctr);
+		TG_CUDA(cudaGetLastError());
+	}
+	if (B.ray2_fwd.count > 0) {
+		k_ray_fwd<32, false><<<B.ray2_fwd.count, 256, 0, L.stream>>>(L.inst, B.ray2_fwd, pred, x, y, ctr);
+		TG_CUDA(cudaGetLastError());
+	}
+	if (B.ray3_fwd.count > 0) {
+		k_ray_fwd<16, true><<<B.ray3_fwd.count, 256, 0, L.stream>>>(L.inst, B.ray3_fwd, pred, x, y, ctr);
 		TG_CUDA(cudaGetLastError());
 	}
 }
@@ -260,6 +471,13 @@ void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel
 	}
 	gather(L, B.csc_adj, pred, 1, x, y);
 	gather(L, B.ray_adj, pred, 2, x, y);
+	if (B.ray_adj_staged.count > 0) {
+		k_ray_compact<<<B.ray_compact.count, 256, 0, L.stream>>>(L.inst, B.ray_compact, pred, x, ctr);
+		TG_CUDA(cudaGetLastError());
+		k_ray_adj_staged<<<B.ray_adj_staged.count, STAGED_THREADS, staged_smem_bytes(B.staged_ppb_max),
+		                   L.stream>>>(L.inst, B.ray_adj_staged, pred, y, ctr);
+		TG_CUDA(cudaGetLastError());
+	}
 }
 
 // ---------------------------------------------------------------------------

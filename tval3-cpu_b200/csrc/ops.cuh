@@ -17,9 +17,23 @@ struct OpBatch {
 	// its mean line length (4, 8, 16 or 32 lanes per line: class 0..3), so its
 	// summation order does not depend on the other instances of a batch.
 	TileMap csr_fwd[4], csc_adj[4], ray_adj[4];
-	// rays: warp per ray, on-the-fly Bresenham
-	TileMap ray_fwd;
+	// rays: on-the-fly Bresenham, 32 lanes per 2D ray (8 rays per block),
+	// 16 lanes per 3D ray (16 rays per block)
+	TileMap ray2_fwd, ray3_fwd;
+	TileMap ray2_transpose;   // 32x32 tiles of the image, for 2D ray operators with xT
+	// staged 2D ray adjoint: compaction of the input to traced rays, then one
+	// block per ppb pixels
+	TileMap ray_compact, ray_adj_staged;
+	int staged_ppb_max = 0;
 };
+
+// the staged 2D ray adjoint's index: 16-bit in-chunk ray offsets, every
+// pixel's segment of every chunk padded to 8 entries, and the per-pixel chunk
+// boundaries, from a pixel-major index of traced-ray ids.  Allocates the
+// index (recorded in `owned`) and returns its length.
+long long build_staged_index(cudaStream_t s, long long n, int nrays, const int *cptr, const int *cind,
+                             unsigned short **sidx, int *soff, std::vector<void *> &owned);
+int staged_smem_bytes(int ppb);
 
 // one-time builders (ops.cu)
 // exclusive scan of n int64 counts into out[0..n] (out[n] = total)

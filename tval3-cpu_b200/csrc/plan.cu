@@ -19,6 +19,7 @@ long long validate(const tval3g_problem &p, long long b_len, long long ut_len) {
 	TG_ARG(n < (1LL << 31), "Argument error: the image has more than 2^31-1 elements");
 	TG_ARG(ut_len == 0 || ut_len == n, "Argument error: U and Ut must have the same size!");
 	TG_ARG(b_len >= 1, "Argument error: b must not be empty");
+	TG_ARG(b_len < (1LL << 31), "Argument error: b has more than 2^31-1 elements");
 	switch (p.op_kind) {
 	case TVAL3G_OP_DENSE:
 	case TVAL3G_OP_CSR: {
@@ -211,6 +212,26 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		int *cptr = dalloc_op<int>(st, n + 1);
 		int *cind = dalloc_op<int>(st, total);
 		build_transpose(s, d.nrays, n, total, rptr, rind, nullptr, cptr, cind, nullptr);
+		const int nchunks = (d.nrays + RAY_CHUNK - 1) / RAY_CHUNK;
+		if (!is3 && d.nrays > 0 && nchunks <= RAY_MAX_CHUNKS) {
+			// staged adjoint: 16-bit in-chunk ray offsets (cind still holds ray ids)
+			unsigned short *sidx = nullptr;
+			int *soff = dalloc_op<int>(st, n * (nchunks + 1));
+			long long slen = build_staged_index(s, n, d.nrays, cptr, cind, &sidx, soff, st.owned);
+			st.bytes += slen * (long long)sizeof(unsigned short);
+			int *lo = dalloc_op<int>(st, d.nrays);
+			TG_CUDA(cudaMemcpyAsync(lo, st.ray_out.data(), sizeof(int) * d.nrays, cudaMemcpyHostToDevice, s));
+			d.ylive = dalloc_op<float>(st, (long long)nchunks * RAY_CHUNK);   // whole chunks
+			d.nchunks = nchunks;
+			d.sidx = sidx; d.soff = soff; d.live_out = lo;
+			long long ppb = (n + 147) / 148;   // one block per SM for a single image
+			ppb = (ppb + 31) / 32 * 32;
+			d.ppb = (int)std::max(64LL, std::min(512LL, ppb));
+		}
+		if (!is3 && n % p.ld == 0) {   // transposed image for the y-driven rays
+			d.xT = dalloc_op<float>(st, n);
+			d.tH = (int)(n / p.ld);
+		}
 		if (total > 0) k_map_out<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, drays, cind);
 		TG_CUDA(cudaGetLastError());
 		d.cptr = cptr; d.cind = cind; d.cval = nullptr;
@@ -321,7 +342,8 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 		tb.close(&ob.csc_adj[c]);
 		for (int i = 0; i < cnt; i++) {
 			const OpDev &d = inst[i].op;
-			if ((d.kind != TVAL3G_OP_RAY2D && d.kind != TVAL3G_OP_RAY3D) || cls((double)ops[i].nnz / inst[i].n) != c)
+			if ((d.kind != TVAL3G_OP_RAY2D && d.kind != TVAL3G_OP_RAY3D) || d.nchunks > 0 ||
+			    cls((double)ops[i].nnz / inst[i].n) != c)
 				continue;
 			long long lpb = 256 / widths[c];
 			tb.add(i, (inst[i].n + lpb - 1) / lpb);
@@ -330,10 +352,36 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 	}
 	for (int i = 0; i < cnt; i++) {
 		const OpDev &d = inst[i].op;
-		if (d.kind != TVAL3G_OP_RAY2D && d.kind != TVAL3G_OP_RAY3D) continue;
-		tb.add(i, (d.nrays + WARPS - 1) / WARPS);
+		if (d.kind != TVAL3G_OP_RAY2D) continue;
+		tb.add(i, (d.nrays + 7) / 8);
 	}
-	tb.close(&ob.ray_fwd);
+	tb.close(&ob.ray2_fwd);
+	for (int i = 0; i < cnt; i++) {
+		const OpDev &d = inst[i].op;
+		if (d.kind != TVAL3G_OP_RAY3D) continue;
+		tb.add(i, (d.nrays + 15) / 16);
+	}
+	tb.close(&ob.ray3_fwd);
+	for (int i = 0; i < cnt; i++) {
+		const OpDev &d = inst[i].op;
+		if (d.kind != TVAL3G_OP_RAY2D || !d.xT) continue;
+		tb.add(i, (long long)((d.rvx + 31) / 32) * ((d.tH + 31) / 32));
+	}
+	tb.close(&ob.ray2_transpose);
+	ob.staged_ppb_max = 0;
+	for (int i = 0; i < cnt; i++) {
+		const OpDev &d = inst[i].op;
+		if (d.nchunks <= 0) continue;
+		tb.add(i, (d.nrays + 255) / 256);
+	}
+	tb.close(&ob.ray_compact);
+	for (int i = 0; i < cnt; i++) {
+		const OpDev &d = inst[i].op;
+		if (d.nchunks <= 0) continue;
+		tb.add(i, (inst[i].n + d.ppb - 1) / d.ppb);
+		ob.staged_ppb_max = std::max(ob.staged_ppb_max, d.ppb);
+	}
+	tb.close(&ob.ray_adj_staged);
 	return dense_part;
 }
 
@@ -376,6 +424,8 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 			prepare_op(stream_, p, flags, ops_[i], false);
 			Inst &I = h_inst_[i];
 			I.dims = p.dims; I.p = p.dim_y; I.q = p.dim_x; I.r = p.dims == 3 ? p.dim_z : 1;
+			I.fq.init((unsigned)I.q);
+			I.fp.init((unsigned)I.p);
 			I.n = n; I.m = b_len;
 			I.ntn = (int)((n + TILE - 1) / TILE);
 			I.ntm = (int)((b_len + TILE - 1) / TILE);
@@ -409,9 +459,9 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 				trace_off_.push_back(recs);
 				recs += std::max(h_inst_[i].maxit, 1);
 			}
-			d_trace_ = (double *)dalloc(sizeof(double) * 5 * (size_t)recs);
-			TG_CUDA(cudaMemsetAsync(d_trace_, 0, sizeof(double) * 5 * (size_t)recs, stream_));
-			for (int i = 0; i < count; i++) h_inst_[i].trace = d_trace_ + 5 * trace_off_[i];
+			d_trace_ = (double *)dalloc(sizeof(tval3g_trace_record) * (size_t)recs);
+			TG_CUDA(cudaMemsetAsync(d_trace_, 0, sizeof(tval3g_trace_record) * (size_t)recs, stream_));
+			for (int i = 0; i < count; i++) h_inst_[i].trace = d_trace_ + TRACE_DOUBLES * trace_off_[i];
 		}
 		long long poff = 0;
 		for (int i = 0; i < count; i++) {
@@ -457,7 +507,8 @@ int Plan::trace(int index, tval3g_trace_record *out, int cap) const {
 	int n = index < (int)last_iters_.size() ? std::min(last_iters_[index], h_inst_[index].maxit) : 0;
 	n = std::min(n, cap);
 	if (n > 0)
-		TG_CUDA(cudaMemcpy(out, d_trace_ + 5 * trace_off_[index], sizeof(double) * 5 * n, cudaMemcpyDeviceToHost));
+		TG_CUDA(cudaMemcpy(out, d_trace_ + TRACE_DOUBLES * trace_off_[index], sizeof(tval3g_trace_record) * n,
+		                   cudaMemcpyDeviceToHost));
 	return n;
 }
 

@@ -41,6 +41,9 @@ public:
 	           cudaStream_t stream);
 	long long launches() const { return last_launches_; }
 	int trace(int index, tval3g_trace_record *out, int cap) const;
+	void set_target(double target) {
+		for (auto &I : h_inst_) I.target = target;
+	}
 	long long device_bytes() const { return device_bytes_; }
 
 private:

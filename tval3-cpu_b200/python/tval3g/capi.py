@@ -83,10 +83,12 @@ def lib():
         L.tval3g_plan_solve.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), I, vp]
         L.tval3g_plan_stats.argtypes = [vp, C.POINTER(ll), C.POINTER(ll)]
         L.tval3g_plan_trace.argtypes = [vp, i, C.POINTER(C.c_double), i, C.POINTER(i)]
+        L.tval3g_plan_set_target.argtypes = [vp, d]
         L.tval3g_plan_destroy.argtypes = [vp]
         L.tval3g_op_create.argtypes = [C.POINTER(vp), P, i]
         L.tval3g_op_shape.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(ll)]
         L.tval3g_op_apply.argtypes = [vp, i, vp, vp, vp]
+        L.tval3g_op_apply_n.argtypes = [vp, i, vp, vp, i, vp]
         L.tval3g_op_ray_csr.argtypes = [vp, C.POINTER(ll), _IP]
         L.tval3g_op_destroy.argtypes = [vp]
         L.tval3g_D.argtypes = [i, i, i, i, vp, vp, vp, vp, vp]
@@ -102,8 +104,9 @@ def _check(rc):
 
 
 EXPORTS = ("tval3g_last_error", "tval3g_version", "tval3g_solve", "tval3g_solve_batch", "tval3g_plan_create",
-           "tval3g_plan_solve", "tval3g_plan_stats", "tval3g_plan_trace", "tval3g_plan_destroy", "tval3g_op_create", "tval3g_op_shape",
-           "tval3g_op_apply", "tval3g_op_ray_csr", "tval3g_op_destroy", "tval3g_D", "tval3g_Dt", "tval3g_shrink")
+           "tval3g_plan_solve", "tval3g_plan_stats", "tval3g_plan_trace", "tval3g_plan_set_target",
+           "tval3g_plan_destroy", "tval3g_op_create", "tval3g_op_shape",
+           "tval3g_op_apply", "tval3g_op_apply_n", "tval3g_op_ray_csr", "tval3g_op_destroy", "tval3g_D", "tval3g_Dt", "tval3g_shrink")
 
 
 # --------------------------------------------------------------------------
@@ -266,12 +269,16 @@ class Plan:
         return {"kernel_launches": a.value, "device_bytes": b.value}
 
     def trace(self, index=0):
-        """Per inner iteration records (tau, f, relchg, backtracks, skipped)."""
+        """Per inner iteration records (tau, f, relchg, backtracks, skipped, relerr_ut)."""
         cap = max(self.maxit[index], 1)
-        buf = (C.c_double * (5 * cap))()
+        buf = (C.c_double * (6 * cap))()
         cnt = C.c_int()
         _check(lib().tval3g_plan_trace(self.h, index, buf, cap, C.byref(cnt)))
-        return np.array(buf[:5 * cnt.value]).reshape(cnt.value, 5)
+        return np.array(buf[:6 * cnt.value]).reshape(cnt.value, 6)
+
+    def set_target(self, target):
+        """Time-to-solution mode: also stop once |U - Ut| <= target |Ut|."""
+        _check(lib().tval3g_plan_set_target(self.h, float(target)))
 
     def close(self):
         if getattr(self, "h", None):
@@ -298,6 +305,11 @@ class Operator:
 
     def apply(self, x, y, trans=False, stream=None):
         _check(lib().tval3g_op_apply(self.h, int(trans), _dptr(x), _dptr(y), _dptr(stream)))
+        return y
+
+    def apply_n(self, x, y, reps, trans=False, stream=None):
+        """Enqueue `reps` back-to-back applications on `stream`; no wait."""
+        _check(lib().tval3g_op_apply_n(self.h, int(trans), _dptr(x), _dptr(y), int(reps), _dptr(stream)))
         return y
 
     def ray_csr(self):
