@@ -1,0 +1,80 @@
+// Shared pieces of the C++ drop-in libraries (libtval3_gpu_2d.so,
+// libtval3_gpu_3d.so): conversions between the reference's C++ types and the
+// C ABI, and the exception contract of the reference's driver
+// (2d/tval3_cpu_2d.cpp:878-884: tval3_exception passes through, any other
+// std::exception becomes "Internal error: ...").
+#ifndef TVAL3_DROPIN_COMMON_H_
+#define TVAL3_DROPIN_COMMON_H_
+
+#include <cstring>
+#include <string>
+
+#include "tval3/container.h"
+#include "tval3/tval3_types.h"
+#include "tval3g.h"
+
+namespace tval3g_dropin {
+
+template <class S>
+inline tval3g_options to_c(const tval3_options<S> &o) {
+	tval3g_options c;
+	std::memset(&c, 0, sizeof(c));
+	c.mu = o.mu; c.beta = o.beta; c.mu0 = o.mu0; c.beta0 = o.beta0; c.tol = o.tol; c.tol_inn = o.tol_inn;
+	c.c = o.c; c.gamma = o.gamma; c.gam = o.gam; c.rate_gam = o.rate_gam; c.rate_cnt = o.rate_cnt;
+	c.skipMulRatio = o.skipMulRatio; c.maxRelativeChange = o.maxRelativeChange;
+	c.maxit = o.maxit; c.maxcnt = o.maxcnt; c.nonneg = o.nonneg ? 1 : 0; c.isreal = o.isreal ? 1 : 0;
+	c.numInitIterations = (int)o.numInitIterations; c.tv_norm = o.tv_norm;
+	return c;
+}
+
+template <class S>
+inline tval3_info<S> from_c(const tval3g_info &i) {
+	tval3_info<S> r;
+	r.secs = i.secs;
+	r.outer_iters = i.outer_iters;
+	r.total_iters = i.total_iters;
+	r.rel_chg = (S)i.rel_chg;
+	r.rel_error = (S)i.rel_error;
+	return r;
+}
+
+inline tval3g_problem empty_problem() {
+	tval3g_problem p;
+	std::memset(&p, 0, sizeof(p));
+	p.layers = 1;
+	p.numMPs = 1;
+	return p;
+}
+
+// image shape of U: dim_z is used only by 3D problems
+inline void set_image(tval3g_problem &p, int dims, const mat<float> &U) {
+	p.dims = dims;
+	p.dim_y = U.dim_y;
+	p.dim_x = U.dim_x;
+	p.dim_z = dims == 3 ? U.dim_z : 1;
+}
+
+// run a solve; throws tval3_exception with the C ABI's message on failure
+template <class S>
+inline tval3_info<S> solve(const tval3g_problem &p, mat<float> &U, const mat<float> &b, const tval3_options<S> &opts,
+                           const mat<float> &Ut) {
+	tval3g_options o = to_c(opts);
+	tval3g_info info;
+	std::memset(&info, 0, sizeof(info));
+	int rc = tval3g_solve(&p, b.data(), b.len, &o, Ut.len > 0 ? Ut.data() : 0, Ut.len, U.data(), &info);
+	if (rc != TVAL3G_OK) {
+		std::string msg = tval3g_last_error();
+		if (rc == TVAL3G_ERR_ARGUMENT) throw tval3_exception(msg);
+		throw tval3_exception("Internal error: " + msg);
+	}
+	return from_c<S>(info);
+}
+
+inline void unsupported(const char *what) {
+	throw tval3_exception(std::string("Internal error: ") + what +
+	                      " data is not supported by the GPU build (float data is)");
+}
+
+}  // namespace tval3g_dropin
+
+#endif

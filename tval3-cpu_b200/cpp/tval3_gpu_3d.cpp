@@ -1,0 +1,130 @@
+// libtval3_gpu_3d.so: the reference's 3D C++ entry points on the GPU
+// (include/tval3_gpu_3d.h).  Argument checks follow check_params
+// (3d/tval3_cpu_3d.cpp:1028-1165) in order and wording; the size checks that
+// follow the format checks are made by tval3g_solve with the same messages.
+#include <vector>
+
+#include "../../include/tval3_gpu_3d.h"
+
+#include "dropin_common.h"
+
+using namespace tval3g_dropin;
+
+namespace {
+
+template <class S>
+tval3_info<S> dense3d(mat<float> &U, const mat<float> &A, const mat<float> &b, const tval3_options<S> &opts,
+                      const mat<float> &Ut) {
+	if (U.format != mat_row_major || Ut.format != mat_row_major || A.format != mat_row_major)
+		throw tval3_exception(std::string("Argument error: Matrices must be in row major format!"));
+	tval3g_problem p = empty_problem();
+	set_image(p, 3, U);
+	p.op_kind = TVAL3G_OP_DENSE;
+	p.m = A.dim_y;
+	p.n_cols = A.dim_x;
+	p.A = A.data();
+	return solve<S>(p, U, b, opts, Ut);
+}
+
+template <class S>
+tval3_info<S> sparse3d(mat<float> &U, const sparse_mat<float> &A, const mat<float> &b, const tval3_options<S> &opts,
+                       const mat<float> &Ut) {
+	if (U.format != mat_col_major || Ut.format != mat_col_major)
+		throw tval3_exception(std::string("Argument error: Matrices must be in row major format!"));
+	if (A.format != sparse_mat_both)
+		throw tval3_exception(std::string("Argument error: A must be available in csr and csc format!"));
+	tval3g_problem p = empty_problem();
+	set_image(p, 3, U);
+	p.op_kind = TVAL3G_OP_CSR;
+	p.m = A.dim_y;
+	p.n_cols = A.dim_x;
+	p.nnz = A.nnz;
+	p.csr_ptr = A.csr_ptr();
+	p.csr_ind = A.csr_ind();
+	p.csr_val = A.csr_val();
+	return solve<S>(p, U, b, opts, Ut);
+}
+
+template <class S>
+tval3_info<S> ray3d(mat<float> &U, const geometry &A, const mat<float> &b, const tval3_options<S> &opts,
+                    const mat<float> &Ut) {
+	if (U.format != mat_row_major || Ut.format != mat_row_major)
+		throw tval3_exception(std::string("Argument error: Matrices must be in row major format!"));
+	// per-measurement-position coordinate arrays, flattened [mp*E + e]
+	const int nmp = A.numMPs > 0 ? A.numMPs : 0, E = A.num_emitters, R = A.num_receivers;
+	std::vector<int> xe((size_t)nmp * E), ye(xe.size()), ze(xe.size()), xr((size_t)nmp * R), yr(xr.size()),
+		zr(xr.size());
+	for (int mp = 0; mp < nmp; mp++) {
+		for (int e = 0; e < E; e++) {
+			xe[(size_t)mp * E + e] = A.x_emitters[mp][e];
+			ye[(size_t)mp * E + e] = A.y_emitters[mp][e];
+			ze[(size_t)mp * E + e] = A.z_emitters[mp][e];
+		}
+		for (int r = 0; r < R; r++) {
+			xr[(size_t)mp * R + r] = A.x_receivers[mp][r];
+			yr[(size_t)mp * R + r] = A.y_receivers[mp][r];
+			zr[(size_t)mp * R + r] = A.z_receivers[mp][r];
+		}
+	}
+	tval3g_problem p = empty_problem();
+	set_image(p, 3, U);
+	p.op_kind = TVAL3G_OP_RAY3D;
+	p.numMPs = A.numMPs;
+	p.numPaths = A.numPaths;
+	p.num_emitters = E;
+	p.num_receivers = R;
+	p.use_path = A.use_path;
+	p.x_emitters = xe.data(); p.y_emitters = ye.data(); p.z_emitters = ze.data();
+	p.x_receivers = xr.data(); p.y_receivers = yr.data(); p.z_receivers = zr.data();
+	p.rv_x = A.rv_x; p.rv_y = A.rv_y; p.rv_z = A.rv_z;
+	p.scale_factor = A.scale_factor;
+	return solve<S>(p, U, b, opts, Ut);
+}
+
+}  // namespace
+
+#define UNSUPPORTED_3D(Ttype, Stype, OP, what)                                                                  \
+	const tval3_info<Stype> tval3_cpu_3d(mat<Ttype> &, const OP &, const mat<Ttype> &,                         \
+	                                     const tval3_options<Stype> &, const mat<Ttype> &, int, int) {         \
+		unsupported(what);                                                                                       \
+		return tval3_info<Stype>();                                                                              \
+	}
+
+typedef std::complex<float> cf;
+typedef std::complex<double> cd;
+
+const tval3_info<float> tval3_cpu_3d(mat<float> &U, const mat<float> &A, const mat<float> &b,
+                                     const tval3_options<float> &opts, const mat<float> &Ut, int, int) {
+	return dense3d<float>(U, A, b, opts, Ut);
+}
+const tval3_info<double> tval3_cpu_3d(mat<float> &U, const mat<float> &A, const mat<float> &b,
+                                      const tval3_options<double> &opts, const mat<float> &Ut, int, int) {
+	return dense3d<double>(U, A, b, opts, Ut);
+}
+UNSUPPORTED_3D(double, double, mat<double>, "double")
+UNSUPPORTED_3D(cf, float, mat<cf>, "complex")
+UNSUPPORTED_3D(cd, double, mat<cd>, "complex")
+
+const tval3_info<float> tval3_cpu_3d(mat<float> &U, const sparse_mat<float> &A, const mat<float> &b,
+                                     const tval3_options<float> &opts, const mat<float> &Ut, int, int) {
+	return sparse3d<float>(U, A, b, opts, Ut);
+}
+const tval3_info<double> tval3_cpu_3d(mat<float> &U, const sparse_mat<float> &A, const mat<float> &b,
+                                      const tval3_options<double> &opts, const mat<float> &Ut, int, int) {
+	return sparse3d<double>(U, A, b, opts, Ut);
+}
+UNSUPPORTED_3D(double, double, sparse_mat<double>, "double")
+UNSUPPORTED_3D(cf, float, sparse_mat<cf>, "complex")
+UNSUPPORTED_3D(cd, double, sparse_mat<cd>, "complex")
+
+const tval3_info<float> tval3_cpu_3d(mat<float> &U, const geometry &A, const mat<float> &b,
+                                     const tval3_options<float> &opts, const mat<float> &Ut, int, int) {
+	return ray3d<float>(U, A, b, opts, Ut);
+}
+const tval3_info<double> tval3_cpu_3d(mat<float> &U, const geometry &A, const mat<float> &b,
+                                      const tval3_options<double> &opts, const mat<float> &Ut, int, int) {
+	return ray3d<double>(U, A, b, opts, Ut);
+}
+UNSUPPORTED_3D(double, double, geometry, "double")
+UNSUPPORTED_3D(cf, float, geometry, "complex")
+UNSUPPORTED_3D(cd, double, geometry, "complex")
