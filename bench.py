@@ -1,24 +1,31 @@
 #!/usr/bin/env python
 """TVAL3 time-to-solution benchmark on B200 (one JSON line on rank 0).
 
-Workload (default): the 2D ultrasound-tomography ring - 256x256 image, 512
-transducers on the inscribed circle, each emitter firing at the 256 receivers
-on the opposite half (131072 rays, 2.72e7 Bresenham hits), isotropic TV,
-mu=2^10, beta=2^6, tol=1e-5, maxit=500 - on the on-the-fly Bresenham
-projector.  A step is one full reconstruction (scaleb, A^T b, the whole
+Default workload: the 2D ultrasound-tomography ring - 256x256
+image, 512 transducers on the inscribed circle, each emitter firing at the 256
+receivers on the opposite half (131072 rays, 2.72e7 Bresenham hits),
+isotropic TV, mu=2^10, beta=2^6, tol=1e-5, maxit=500 - on the on-the-fly
+Bresenham projector.  A step is one reconstruction (scaleb, A^T b, the
 continuation / inner loop, final scaling) through a device-resident plan whose
-iteration loop is one CUDA graph.
+iteration loop is one CUDA graph with conditional nodes, run until it is
+within 1e-3 (relative L2) of the FP64 solution (tests/golden, given as Ut) or
+the reference's own stopping rules end it.
 
   value   reconstructions/s with inputs resident in HBM (CUDA events around
           each solve on the launching stream; 256 MB L2 flush between solves)
-  e2e     the same through the host-buffer C ABI tval3g_solve (geometry and b
-          from host memory, U back to host; includes the per-call operator
-          preparation), host clock around the blocking call
-  roofline  the dominant kernel (ray adjoint gather) timed with CUDA events
+  e2e     the same problem through the host-buffer C ABI tval3g_solve
+          (geometry and b from host memory, U back to host, the per-call
+          operator preparation included, the reference's stopping rules);
+          host clock around the blocking call
+  roofline  the dominant kernel timed alone with CUDA events after an L2
+          flush, algorithmic bytes / time against the measured HBM copy rate
   cpu_baseline  the reference solver itself (oracle/_ref, compiled from its
-          own sources) on the CSR twin, on a bounded sample of iterations
+          own sources) on the CSR twin, a bounded sample of iterations
 
---impl reference runs only the reference CPU solver on the same workload.
+--workload dense2d | hemi3d | batch measures the plain dense 64x64 problem,
+the 128^3 hemisphere and the mixed batch of 64 independent 2D problems
+(batched graph vs plain one-instance-per-launch).
+--impl reference runs only the reference CPU solver on the default workload.
 Multi-GPU (torchrun): every rank solves its own replica (no collective in the
 data path); value = total reconstructions / max-over-ranks time.
 """
@@ -36,7 +43,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "tval3-cpu_b200", "python"))
 
 METRIC = "TVAL3 time-to-solution (relerr≤1e-3 vs FP64), batched vs plain, 1 B200; HBM %"
-FIXTURE = os.path.join(ROOT, "tests", "golden", "ring256_fp64.npz")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def args_():
@@ -45,6 +52,7 @@ def args_():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="tval3g", choices=["tval3g", "reference"])
+    p.add_argument("--workload", default="ring2d", choices=["ring2d", "dense2d", "hemi3d", "batch"])
     p.add_argument("--cpu-sample-iters", type=int, default=20)
     p.add_argument("--profile", action="store_true",
                    help="for ncu: build the plan, run --warmup + --steps solves, print nothing else")
@@ -55,22 +63,38 @@ def args_():
     return p.parse_args()
 
 
-def workload():
+def workload(name, forward3d=None):
     from tval3g import workloads as W
-    return W.ring2d(seed=1, side=256, T=512, tv_norm=1, maxit=500, tol=1e-5, normalize=True)
+    if name == "ring2d":
+        return W.ring2d(seed=1, side=256, T=512, tv_norm=1, maxit=500, tol=1e-5, normalize=True)
+    if name == "dense2d":
+        return W.dense2d(seed=0, side=64, sampling=0.3, tv_norm=1, maxit=300, tol=1e-4)
+    if name == "hemi3d":
+        return W.hemi3d(seed=2, side=128, T=2048, receivers=1024, tv_norm=0, maxit=400, tol=1e-5,
+                        forward=forward3d)
+    raise KeyError(name)
 
 
-def config_dict():
-    return {"workload": "2D ring 256x256, 512 transducers x 256 receivers (131072 rays, 2.72e7 hits), iso TV, "
-                        "mu 2^10, beta 2^6, tol 1e-5, maxit 500 (configs[1]); hit weight scale_factor = "
-                        "1/sigma_max(A) so that mu and beta act as in TVAL3",
-            "operator": "on-the-fly Bresenham projector (gather adjoint)", "instances": 1,
-            "l2": "256 MB write between timed solves"}
+CONFIGS = {
+    "ring2d": {"workload": "2D ring 256x256, 512 transducers x 256 receivers (131072 rays, 2.72e7 hits), iso TV, "
+                           "mu 2^10, beta 2^6, tol 1e-5, maxit 500; hit weight scale_factor = "
+                           "1/sigma_max(A) so that mu and beta act as in TVAL3",
+               "operator": "on-the-fly Bresenham projector, shared-memory staged adjoint"},
+    "dense2d": {"workload": "2D dense 64x64, A 1229x4096 N(0,1/m), iso TV, mu 2^8, beta 2^5, tol 1e-4, maxit 300",
+                "operator": "dense gemv pair"},
+    "hemi3d": {"workload": "3D 128^3, 2048 hemisphere transducers x 1024 random receivers (2.1M rays), aniso TV, "
+                           "mu 2^10, beta 2^6, tol 1e-5, maxit 400; hit weight 1/sigma_max(A)",
+               "operator": "on-the-fly 3D Bresenham projector, gather adjoint"},
+    "batch": {"workload": "64 independent 2D problems, sides {64..256}, dense Gaussian (25-40 % sampling) or ring "
+                          "Bresenham (128-512 transducers)",
+              "operator": "mixed dense / ray, one batched plan"},
+}
 
 
-def fp64_reference():
-    if os.path.exists(FIXTURE):
-        return dict(np.load(FIXTURE))
+def fp64_reference(name):
+    f = {"ring2d": "ring256_fp64.npz", "dense2d": "dense64_fp64.npz"}.get(name)
+    if f and os.path.exists(os.path.join(GOLDEN, f)):
+        return dict(np.load(os.path.join(GOLDEN, f)))
     return None
 
 
@@ -120,20 +144,25 @@ class Clocks:
 # --------------------------------------------------------------------------
 def reference_rate(w, sample_iters, full_iters):
     """Seconds per reconstruction of the reference's own solver (float data,
-    CSR twin, all host threads), from a bounded sample of iterations scaled to
-    the iteration count of a full solve."""
+    all host threads) from a bounded sample of iterations scaled to the
+    iteration count of a full solve.  Ray workloads run on their CSR twin (the
+    reference's 2D projector is commented out, 2d/mat_mult.h:111-193); the
+    reference has anisotropic TV only."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     if not O.ref_available(2):
         return None
-    A = w["csr"]
     o = dict(w["opts"])
     o["maxit"] = sample_iters
     o["tv_norm"] = 0
     cwd = os.getcwd()
     t0 = time.perf_counter()
-    r = O.ref_solve("csr", w["shape"], w["b"], o, dtype=0, csr=(A["m"], A["n"], A["rowptr"], A["colind"], A["val"]),
-                    vppc=1)
+    if w["kind"] == "dense":
+        r = O.ref_solve("dense", w["shape"], w["b"], o, dtype=0, A=w["A"], vppc=1)
+    else:
+        A = w["csr"]
+        r = O.ref_solve("csr", w["shape"], w["b"], o, dtype=0,
+                        csr=(A["m"], A["n"], A["rowptr"], A["colind"], A["val"]), vppc=1)
     os.chdir(cwd)
     secs = time.perf_counter() - t0
     per_iter = secs / max(r.total_iters, 1)
@@ -144,24 +173,25 @@ def reference_rate(w, sample_iters, full_iters):
 def run_reference(a, rank):
     if rank != 0:
         return
-    w = workload()
-    ref = fp64_reference()
+    w = workload("ring2d")
+    ref = fp64_reference("ring2d")
     full_iters = int(ref["iters"][1]) if ref is not None else int(w["opts"]["maxit"])
     for _ in range(a.warmup):
         reference_rate(w, a.cpu_sample_iters, full_iters)
     rates = []
+    r = None
     for _ in range(a.steps):
         r = reference_rate(w, a.cpu_sample_iters, full_iters)
         if r is None:
-            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources "
-                                                                  "absent when building)"}))
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (the reference "
+                                                                  "sources were absent when building)"}))
             return
         rates.append(r["secs_per_solve"])
     ms = float(np.mean(rates)) * 1000
     val = 1000.0 / ms
     line = {"metric": METRIC, "value": val, "unit": "reconstructions/s", "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic", "config": config_dict(), "impl": "reference",
+            "dtype": "f32", "data": "synthetic", "config": CONFIGS["ring2d"], "impl": "reference",
             "cpu_baseline": {"value": val, "unit": "reconstructions/s", "cores": r["cores"], "kind": "reference",
                              "sample": f"{r['sample_iters']} iterations of the reference solver (anisotropic TV: it "
                                        f"has no isotropic TV) on the CSR twin, scaled to {full_iters} iterations"},
@@ -172,6 +202,264 @@ def run_reference(a, rank):
 # --------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------
+class Ctx:
+    def __init__(self, torch, dev, stream, flush):
+        self.torch, self.dev, self.stream, self.flush = torch, dev, stream, flush
+
+    def event_time(self, fn, reps):
+        torch = self.torch
+        out, res = [], None
+        for _ in range(reps):
+            self.flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(self.stream)
+            res = fn()
+            e1.record(self.stream)
+            e1.synchronize()
+            out.append(e0.elapsed_time(e1))
+        return out, res
+
+
+def peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(p)) if os.path.exists(p) else {}
+    if "hbm_gbs" in peaks:
+        return float(peaks["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def profile_traffic(name):
+    prof = os.path.join(ROOT, "profiles", name)
+    if os.path.exists(prof):
+        for line in open(prof):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1].split()[0])
+    return None
+
+
+def kernel_roofline(cx, capi, spec, w, kind):
+    """Time the dominant operator kernel alone (per launch, after an L2 flush)."""
+    torch, dev, s = cx.torch, cx.dev, cx.stream.cuda_stream
+    op = capi.Operator(spec)
+    x = torch.rand(op.cols, device=dev)
+    y = torch.rand(op.rows, device=dev)
+    out_m = torch.empty(op.rows, device=dev)
+    out_n = torch.empty(op.cols, device=dev)
+    kt = {}
+    for name, (src, dst, tr) in {"forward": (x, out_m, False), "adjoint": (y, out_n, True)}.items():
+        op.apply_n(src, dst, 3, trans=tr, stream=s)
+        ts, _ = cx.event_time(lambda: op.apply_n(src, dst, 1, trans=tr, stream=s), 10)
+        kt[name] = float(np.mean(ts))
+    nnz, n, m = op.nnz, op.cols, op.rows
+    op.close()
+    peak, src = peak_hbm()
+    if kind == "ray2d":
+        nrays = int(np.count_nonzero(w["geom"]["use_path"]))
+        nchunks = -(-nrays // 32768)
+        # staged adjoint: measurement vector once, traced-ray vector written and
+        # read once, 16-bit pixel->ray index, per-pixel chunk offsets, image once
+        bytes_ = 4 * m + 8 * nrays + 2 * nnz + 4 * n * (nchunks + 1) + 4 * n
+        kname, prof, direction = "k_ray_compact + k_ray_adj_staged (ray adjoint)", "ray_adjoint_staged_ring256.md", "adjoint"
+    elif kind == "ray3d":
+        bytes_ = 4 * (n + 1) + 4 * nnz + 4 * m + 4 * n   # pixel pointers, ray ids, y once, image once
+        kname, prof, direction = "k_gather<ray adjoint>", "ray_adjoint_gather_hemi128.md", "adjoint"
+    else:
+        A = w["A"]
+        bytes_ = 4 * A.size + 4 * (A.shape[0] + A.shape[1])   # A once, x and y once
+        kname, prof, direction = "k_dense_fwd (A x)", "dense_gemv_64.md", "forward"
+    achieved = bytes_ / (kt[direction] * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": profile_traffic(prof), "algorithmic_bytes": int(bytes_),
+            "ms_per_launch": kt[direction], "peak_source": src,
+            "other_direction_ms_per_launch": kt["adjoint" if direction == "forward" else "forward"],
+            "timing": "one launch per CUDA-event pair, 256 MB L2 flush before each"}
+
+
+def run_single(a, cx, capi, name, world, rank, dist, clocks):
+    torch, dev, stream = cx.torch, cx.dev, cx.stream
+    fwd3d = None
+    if name == "hemi3d":   # data from the GPU operator (no host CSR twin at this size)
+        def fwd3d(g, u):
+            # hit weight 1/sigma_max(A), as for the ring (power iteration on A^T A)
+            op = capi.Operator(capi.ray3d_problem(u.shape, g))
+            x = torch.rand(op.cols, device=dev, generator=torch.Generator(device=dev).manual_seed(7))
+            y = torch.empty(op.rows, device=dev)
+            lam = 1.0
+            for _ in range(30):
+                x /= torch.linalg.vector_norm(x)
+                op.apply(x, y, stream=stream.cuda_stream)
+                op.apply(y, x, trans=True, stream=stream.cuda_stream)
+                lam = float(torch.linalg.vector_norm(x))
+            op.close()
+            g["scale"] = float(np.float32(1.0 / np.sqrt(lam)))
+            op = capi.Operator(capi.ray3d_problem(u.shape, g))
+            op.apply(torch.tensor(u.ravel().astype(np.float32), device=dev), y, stream=stream.cuda_stream)
+            op.close()
+            return y.cpu().numpy()
+    w = workload(name, fwd3d)
+    spec = capi.problem_from_workload(w)
+    opts = dict(w["opts"])
+    if a.maxit is not None:
+        opts["maxit"] = a.maxit
+    b_host = np.ascontiguousarray(w["b"], np.float32)
+    d_b = torch.tensor(b_host, device=dev)
+    d_U = torch.empty(spec.n, device=dev)
+    ref = fp64_reference(name)
+    d_ref = torch.tensor(ref["U"].ravel().astype(np.float32), device=dev) if ref is not None else None
+    target = 1e-3 if ref is not None else 0.0
+    uts = [d_ref] if d_ref is not None else None
+
+    plan = capi.Plan([spec], [opts], graph=not (a.profile and a.plain), trace=True)
+    plan.set_target(target)
+    solve = lambda p: p.solve([d_b], [d_U], d_Ut=uts, stream=stream.cuda_stream)  # noqa: E731
+    if a.profile:
+        cx.event_time(lambda: solve(plan), a.warmup + a.steps)
+        plan.close()
+        return None
+    cx.event_time(lambda: solve(plan), max(a.warmup, 3))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    times, launches, infos = [], 0, None
+    for _ in range(a.steps):
+        t1, infos = cx.event_time(lambda: solve(plan), 1)
+        times += t1
+        launches += plan.stats()["kernel_launches"]
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = float(np.mean(times))
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    iters = infos[0]["total_iters"]
+    relerr = float(infos[0]["rel_error"]) if ref is not None else None
+    curve = plan.trace(0)[:, 5] if ref is not None else []
+
+    plan.set_target(0.0)   # the full solve under the reference's stopping rules alone
+    full_t, full_info = cx.event_time(lambda: solve(plan), 2)
+    plan.close()
+
+    plan_plain = capi.Plan([spec], [opts], graph=False)   # host-driven loop, same kernels
+    plan_plain.set_target(target)
+    cx.event_time(lambda: solve(plan_plain), 1)
+    pt, _ = cx.event_time(lambda: solve(plan_plain), 2)
+    plan_plain.close()
+
+    et = []   # end to end through the host-buffer C ABI
+    for k in range(max(1, min(a.steps, 3)) + 1):
+        t0 = time.perf_counter()
+        capi.solve(spec, b_host, opts)
+        if k > 0:
+            et.append((time.perf_counter() - t0) * 1000)
+    e2e_ms = float(np.mean(et))
+    in_bytes = int(b_host.nbytes + sum(x.nbytes for x in spec.keep))
+
+    line = {"metric": METRIC, "value": world * 1000.0 / ms, "unit": "reconstructions/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom and operator, Gaussian noise)",
+            "config": dict(CONFIGS[name], instances=1, l2="256 MB write between timed solves"),
+            "iterations": iters, "time_to_solution_ms": ms, "relerr_vs_fp64": relerr,
+            "reached_target": bool(relerr is not None and relerr <= target), "target": target,
+            "relerr_curve_every_5": [round(float(x), 6) for x in curve[::5]],
+            "full_solve": {"ms": float(np.mean(full_t)), "iterations": full_info[0]["total_iters"],
+                           "relerr_vs_fp64": float(full_info[0]["rel_error"]) if ref is not None else None,
+                           "rule": "reference stopping rules (tol, tol_inn, maxit)"},
+            "plain": {"value": world * 1000.0 / float(np.mean(pt)), "unit": "reconstructions/s",
+                      "ms_per_step": float(np.mean(pt)), "form": "host-driven loop, one launch per kernel"},
+            "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "reconstructions/s", "h2d_bytes_per_step": in_bytes,
+                    "d2h_bytes_per_step": int(spec.n * 4)},
+            "roofline": kernel_roofline(cx, capi, spec, w, w["kind"]),
+            "clocks": clk, "gpu_launches": launches}
+    if rank == 0 and world == 1 and name != "hemi3d":
+        cb = reference_rate(w, a.cpu_sample_iters, iters)
+        if cb:
+            line["cpu_baseline"] = {"value": 1.0 / cb["secs_per_solve"], "unit": "reconstructions/s",
+                                    "cores": cb["cores"], "kind": "reference",
+                                    "sample": f"{cb['sample_iters']} iterations of the reference solver (anisotropic "
+                                              f"TV, float, {'CSR twin' if w['kind'] != 'dense' else 'dense'}) "
+                                              f"scaled to {iters} iterations"}
+    return line
+
+
+def batch_problems(capi, torch, dev):
+    """Materialise the mixed batch: dense A drawn on the device (seeded),
+    ring geometries and data on the host."""
+    from tval3g import workloads as W
+    specs, opts, bs, keep = [], [], [], []
+    for k, d in enumerate(W.batch_specs()):
+        side = d["side"]
+        n = side * side
+        rng = np.random.default_rng(d["seed"])
+        if d["kind"] == "dense":
+            m = int(round(d["sampling"] * n))
+            u = W.ellipse_phantom(side, side, rng, 5, 0.0, lambda r: r.uniform(0.2, 1.0), (side / 16, side / 3.2))
+            g = torch.Generator(device=dev)
+            g.manual_seed(d["seed"])
+            A = torch.randn(m, n, device=dev, generator=g).mul_(1.0 / np.sqrt(m))
+            y = (A @ torch.tensor(u.ravel(), dtype=torch.float32, device=dev)).double().cpu().numpy()
+            b = W.add_noise(y, 0.01, rng).astype(np.float32)
+            spec = capi.dense_problem((side, side), A, device_ptr=A.data_ptr())
+            keep.append(A)
+            o = W.options(2 ** 8, 2 ** 5, 1e-4, 300, tv_norm=1)
+        else:
+            w = W.ring2d(seed=d["seed"], side=side, T=d["T"], tv_norm=1, maxit=500, tol=1e-5, normalize=True)
+            spec, b, o = capi.ray2d_problem((side, side), w["geom"]), w["b"], w["opts"]
+        specs.append(spec)
+        bs.append(torch.tensor(np.ascontiguousarray(b, np.float32), device=dev))
+        opts.append(o)
+    return specs, opts, bs, keep
+
+
+def run_batch(a, cx, capi, world, dist, clocks):
+    torch, dev, stream = cx.torch, cx.dev, cx.stream
+    specs, opts, bs, keep = batch_problems(capi, torch, dev)
+    us = [torch.empty(s.n, device=dev) for s in specs]
+    nb = len(specs)
+    plan = capi.Plan(specs, opts, graph=True, device_inputs=True)
+    solve = lambda: plan.solve(bs, us, stream=stream.cuda_stream)  # noqa: E731
+    cx.event_time(solve, max(1, a.warmup))
+    if dist:
+        dist.barrier()
+    clocks.start()
+    tb, infos = cx.event_time(solve, a.steps)
+    launches = plan.stats()["kernel_launches"]
+    clk = clocks.stop()
+    ms_b = float(np.mean(tb))
+    device_bytes = plan.stats()["device_bytes"]
+    plan.close()
+    # plain: one instance per plan, host-driven loop, instances one after another
+    singles = [capi.Plan([s], [o], graph=False, device_inputs=True) for s, o in zip(specs, opts)]
+
+    def plain():
+        for p, b, u in zip(singles, bs, us):
+            p.solve([b], [u], stream=stream.cuda_stream)
+    cx.event_time(plain, 1)
+    tp, _ = cx.event_time(plain, 1)
+    for p in singles:
+        p.close()
+    ms_p = float(np.mean(tp))
+    if dist:
+        t = torch.tensor([ms_b, ms_p], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_b, ms_p = (float(x) for x in t.tolist())
+    iters = [i["total_iters"] for i in infos]
+    dense = sum(1 for s in specs if s.p.op_kind == capi.OP_DENSE)
+    dense_bytes = sum(4 * s.p.m * s.p.n_cols for s in specs if s.p.op_kind == capi.OP_DENSE)
+    return {"metric": METRIC, "value": world * nb * 1000.0 / ms_b, "unit": "reconstructions/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_b, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantoms and operators)",
+            "config": dict(CONFIGS["batch"], instances=nb, dense_instances=dense,
+                           dense_bytes=int(dense_bytes), plan_device_bytes=int(device_bytes)),
+            "plain": {"value": world * nb * 1000.0 / ms_p, "unit": "reconstructions/s", "ms_per_step": ms_p,
+                      "form": "one plan per instance, host-driven loop, instances in sequence"},
+            "batched_over_plain": ms_p / ms_b, "iterations_min_max": [min(iters), max(iters)],
+            "clocks": clk, "gpu_launches": launches}
+
+
 def main():
     a = args_()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -192,162 +480,17 @@ def main():
     from tval3g import capi
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    w = workload()
-    spec = capi.ray2d_problem(w["shape"], w["geom"])
-    opts = dict(w["opts"])
-    if a.maxit is not None:
-        opts["maxit"] = a.maxit
-    b_host = np.ascontiguousarray(w["b"], np.float32)
-    # a non-default stream: every kernel of the solve is launched on it and
-    # the CUDA events below are recorded on it
+    # a non-default stream: every kernel is launched on it and the CUDA
+    # events are recorded on it
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
-    d_b = torch.tensor(b_host, device=dev)
-    d_U = torch.empty(spec.n, device=dev)
-    flush = torch.empty(64 * 1024 * 1024, device=dev)
-    ref = fp64_reference()
-    # time-to-solution: stop at the first iteration within 1e-3 of the FP64
-    # solution (given as Ut), else by the reference's own stopping rules
-    d_ref = torch.tensor(ref["U"].ravel().astype(np.float32), device=dev) if ref is not None else None
-    target = 1e-3 if ref is not None else 0.0
-
-    plan = capi.Plan([spec], [opts], graph=not (a.profile and a.plain), trace=True)
-    plan.set_target(target)
-
-    def solve_timed(p, reps):
-        out, inf = [], None
-        for _ in range(reps):
-            flush.fill_(1.0)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            inf = p.solve([d_b], [d_U], d_Ut=[d_ref] if d_ref is not None else None, stream=stream.cuda_stream)
-            e1.record(stream)
-            e1.synchronize()
-            out.append(e0.elapsed_time(e1))
-        return out, inf
-
-    if a.profile:
-        solve_timed(plan, a.warmup + a.steps)
-        plan.close()
-        return
-    solve_timed(plan, max(a.warmup, 3))
-
+    cx = Ctx(torch, dev, stream, torch.empty(64 * 1024 * 1024, device=dev))
     clocks = Clocks(local)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    clocks.start()
-    times, launches, infos = [], 0, None
-    for _ in range(a.steps):
-        t1, infos = solve_timed(plan, 1)
-        times += t1
-        launches += plan.stats()["kernel_launches"]
-    torch.cuda.synchronize(dev)
-    if dist:
-        dist.barrier()
-    clk = clocks.stop()
-    ms = float(np.mean(times))
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * 1000.0 / ms
-    iters = infos[0]["total_iters"]
-    relerr = float(infos[0]["rel_error"]) if ref is not None else None
-    curve = plan.trace(0)[:, 5]
-
-    # the full solve under the reference's stopping rules alone
-    plan.set_target(0.0)
-    full_t, full_info = solve_timed(plan, 2)
-    full_relerr = float(full_info[0]["rel_error"]) if ref is not None else None
-
-    # the plain (host-driven, no graph) form of the same time-to-solution
-    plan_plain = capi.Plan([spec], [opts], graph=False)
-    plan_plain.set_target(target)
-    solve_timed(plan_plain, 1)
-    pt, _ = solve_timed(plan_plain, 2)
-    plan_plain.close()
-
-    # end to end through the host-buffer C ABI
-    et = []
-    for k in range(max(1, min(a.steps, 3)) + 1):
-        t0 = time.perf_counter()
-        Uh, info_h = capi.solve(spec, b_host, opts)
-        if k > 0:
-            et.append((time.perf_counter() - t0) * 1000)
-    geom_bytes = sum(np.asarray(w["geom"][k]).astype(np.int32).nbytes for k in ("use_path", "xe", "ye", "xr", "yr"))
-    e2e_ms = float(np.mean(et))
-
-    # dominant kernels, timed alone with CUDA events on their stream
-    op = capi.Operator(spec)
-    x = torch.rand(op.cols, device=dev)
-    y = torch.rand(op.rows, device=dev)
-    out_m = torch.empty(op.rows, device=dev)
-    out_n = torch.empty(op.cols, device=dev)
-    # each launch timed alone after an L2 flush, so its index comes from HBM
-    kt = {}
-    for name, (src, dst, tr) in {"ray_forward": (x, out_m, False), "ray_adjoint": (y, out_n, True)}.items():
-        op.apply_n(src, dst, 3, trans=tr, stream=stream.cuda_stream)
-        ts = []
-        for _ in range(10):
-            flush.fill_(1.0)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            op.apply_n(src, dst, 1, trans=tr, stream=stream.cuda_stream)
-            e1.record(stream)
-            e1.synchronize()
-            ts.append(e0.elapsed_time(e1))
-        kt[name] = float(np.mean(ts))
-    nnz, n, m = op.nnz, op.cols, op.rows
-    nrays = int(np.count_nonzero(w["geom"]["use_path"]))
-    nchunks = -(-nrays // 32768)
-    # algorithmic bytes of the staged adjoint (compaction + gather): the
-    # measurement vector read once, the traced-ray vector written and read
-    # once, the 16-bit pixel->ray index, the per-pixel chunk offsets, the image
-    # written once
-    adj_bytes = 4 * m + 8 * nrays + 2 * nnz + 4 * n * (nchunks + 1) + 4 * n
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = adj_bytes / (kt["ray_adjoint"] * 1e-3) / 1e9
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "ray_adjoint_staged_ring256.md")
-    if os.path.exists(prof):
-        for line in open(prof):
-            if line.startswith("traffic_bytes_per_launch:"):
-                traffic = float(line.split(":")[1].split()[0])
-
-    line = {"metric": METRIC, "value": value, "unit": "reconstructions/s", "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded ring phantom, 0.5% noise)", "config": config_dict(),
-            "iterations": iters, "time_to_solution_ms": ms, "relerr_vs_fp64": relerr,
-            "reached_target": bool(relerr is not None and relerr <= target), "target": target,
-            "relerr_curve_every_5": [round(float(x), 6) for x in curve[::5]],
-            "full_solve": {"ms": float(np.mean(full_t)), "iterations": full_info[0]["total_iters"],
-                           "relerr_vs_fp64": full_relerr, "rule": "reference stopping rules (tol, tol_inn, maxit)"},
-            "plain": {"value": world * 1000.0 / float(np.mean(pt)), "unit": "reconstructions/s",
-                      "ms_per_step": float(np.mean(pt)), "form": "host-driven loop, one launch per kernel"},
-            "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "reconstructions/s",
-                    "h2d_bytes_per_step": int(b_host.nbytes + geom_bytes), "d2h_bytes_per_step": int(spec.n * 4)},
-            "roofline": {"bound": "hbm", "kernel": "k_ray_compact + k_ray_adj_staged (ray adjoint)",
-                         "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "algorithmic_bytes": adj_bytes, "ms_per_launch": kt["ray_adjoint"],
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
-                         "forward_ms_per_launch": kt["ray_forward"], "hits": nnz},
-            "clocks": clk, "gpu_launches": launches}
-    if rank == 0 and world == 1:
-        full = ref["iters"][1] if ref is not None else iters
-        cb = reference_rate(w, a.cpu_sample_iters, iters)
-        if cb:
-            line["cpu_baseline"] = {"value": 1.0 / cb["secs_per_solve"], "unit": "reconstructions/s",
-                                    "cores": cb["cores"], "kind": "reference",
-                                    "sample": f"{cb['sample_iters']} iterations of the reference solver "
-                                              f"(anisotropic TV, CSR twin, float) scaled to {iters} iterations "
-                                              f"(FP64 oracle solve: {int(full)})"}
-    plan.close()
-    op.close()
-    if rank == 0:
+    if a.workload == "batch":
+        line = run_batch(a, cx, capi, world, dist, clocks)
+    else:
+        line = run_single(a, cx, capi, a.workload, world, rank, dist, clocks)
+    if rank == 0 and line is not None:
         print(json.dumps(line))
     if dist:
         dist.barrier()

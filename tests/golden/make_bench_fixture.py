@@ -45,6 +45,14 @@ def main():
         out["aniso_ref_f32_vs_fp64"] = np.array([d, rr.total_iters, r64.total_iters])
     np.savez_compressed(os.path.join(HERE, "ring256_fp64.npz"), **out)
 
+    # the plain dense 2D workload (64x64, 30 % sampling, isotropic TV)
+    w = W.dense2d(seed=0, side=64, sampling=0.3, tv_norm=1, maxit=300, tol=1e-4)
+    r = O.solve(O.Op.dense(w["A"].astype(np.float64)), w["b"].astype(np.float64), w["shape"], w["opts"],
+                Ut=w["u_true"])
+    print(f"dense 64x64 FP64 oracle: {r.total_iters} iterations, relerr to phantom {r.rel_error:.4f}")
+    np.savez_compressed(os.path.join(HERE, "dense64_fp64.npz"), U=r.U.astype(np.float32),
+                        iters=np.array([r.outer_iters, r.total_iters]))
+
 
 if __name__ == "__main__":
     main()

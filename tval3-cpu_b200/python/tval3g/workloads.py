@@ -334,16 +334,38 @@ def ring2d(seed=1, side=256, T=512, receivers=None, noise=0.005, tv_norm=1, maxi
     return out
 
 
+def batch_specs(seed=3, count=64, sides=(64, 96, 128, 192, 256)):
+    """The mixed batch of independent 2D problems: per instance a side drawn
+    from `sides`, and either a dense Gaussian A (sampling 25-40 %, drawn on
+    the device from the instance seed) or a ring geometry (128-512
+    transducers).  Returns descriptions; the caller materialises them."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        side = int(rng.choice(sides))
+        if rng.uniform() < 0.5:
+            out.append(dict(kind="dense", side=side, sampling=float(rng.uniform(0.25, 0.40)),
+                            seed=int(rng.integers(1 << 30))))
+        else:
+            T = int(rng.choice([128, 192, 256, 384, 512]))
+            out.append(dict(kind="ray2d", side=side, T=T, seed=int(rng.integers(1 << 30))))
+    return out
+
+
 def hemi3d(seed=2, side=128, T=2048, receivers=1024, noise=0.005, tv_norm=0, maxit=400, tol=1e-5,
-           n_ellipsoids=12, csr=False):
-    """3D hemisphere geometry (on-the-fly 3D Bresenham)."""
+           n_ellipsoids=12, csr=False, forward=None):
+    """3D hemisphere geometry (on-the-fly 3D Bresenham).
+
+    forward: optional callable (geometry, image) -> A image; by default the
+    data come from the CSR twin built here (which needs ~1 GB of host memory
+    per 1e8 hits at full size)."""
     rng = np.random.default_rng(seed)
     radius = (side - 1) / 2.0 - 0.5
     g = hemisphere_geometry(side, T, receivers, radius, rng)
     u = ellipsoid_phantom(side, rng, n_ellipsoids, 1.0, lambda r: 1.0 + r.uniform(-0.05, 0.05),
                           (side / 16, side / 5))
-    A = ray3d_csr(g)
-    y = csr_matvec(A, u.ravel())
+    A = ray3d_csr(g) if (csr or forward is None) else None
+    y = csr_matvec(A, u.ravel()) if forward is None else np.asarray(forward(g, u), np.float64)
     b = add_noise(y, noise, rng)
     out = dict(kind="ray3d", shape=(side, side, side), geom=g, b=b.astype(np.float32), u_true=u,
                opts=options(2 ** 10, 2 ** 6, tol, maxit, tv_norm=tv_norm))
