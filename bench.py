@@ -49,7 +49,7 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 def args_():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="tval3g", choices=["tval3g", "reference"])
     p.add_argument("--workload", default="ring2d", choices=["ring2d", "dense2d", "hemi3d", "batch"])
@@ -112,10 +112,13 @@ class Clocks:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()   # the first sample before the timed region starts
+            while not self.rows and time.time() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except FileNotFoundError:
             self.proc = None
 
@@ -126,6 +129,9 @@ class Clocks:
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        k, t0 = len(self.rows), time.time()   # and one taken after it ends
+        while len(self.rows) == k and time.time() - t0 < 1.0 and self.proc.poll() is None:
+            time.sleep(0.01)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)

@@ -43,7 +43,24 @@ __global__ void __launch_bounds__(256) k_dense_fwd(const Inst *tab, TileMap map,
 		const float4 *a4 = reinterpret_cast<const float4 *>(a);
 		const float4 *x4 = reinterpret_cast<const float4 *>(x);
 		const long long n4 = n >> 2;
-		for (long long j = lane; j < n4; j += 32) {
+		long long j = lane;
+		// four row segments in flight per lane; the FMA order is the plain loop's
+		for (; j + 96 < n4; j += 128) {
+			float4 av[4], xv[4];
+#pragma unroll
+			for (int u = 0; u < 4; u++) {
+				av[u] = __ldg(a4 + j + 32 * u);
+				xv[u] = __ldg(x4 + j + 32 * u);
+			}
+#pragma unroll
+			for (int u = 0; u < 4; u++) {
+				acc = fma((double)av[u].x, (double)xv[u].x, acc);
+				acc = fma((double)av[u].y, (double)xv[u].y, acc);
+				acc = fma((double)av[u].z, (double)xv[u].z, acc);
+				acc = fma((double)av[u].w, (double)xv[u].w, acc);
+			}
+		}
+		for (; j < n4; j += 32) {
 			float4 av = __ldg(a4 + j), xv = __ldg(x4 + j);
 			acc = fma((double)av.x, (double)xv.x, acc);
 			acc = fma((double)av.y, (double)xv.y, acc);
@@ -74,8 +91,26 @@ __global__ void __launch_bounds__(256) k_dense_adj(const Inst *tab, TileMap map,
 	const float *x = vsel(I, xs) + layer * m;
 	double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;   // FP64 accumulation
 	if ((n & 3) == 0 && (reinterpret_cast<uintptr_t>(op.A) & 15) == 0) {
-		if (c0 < n)
-			for (long long r = r0; r < r1; r++) {
+		if (c0 < n) {
+			long long r = r0;
+			// four rows in flight per thread; the FMA order is the plain loop's
+			for (; r + 3 < r1; r += 4) {
+				float xv[4];
+				float4 av[4];
+#pragma unroll
+				for (int u = 0; u < 4; u++) {
+					xv[u] = __ldg(x + r + u);
+					av[u] = __ldg(reinterpret_cast<const float4 *>(op.A + (r + u) * n + c0));
+				}
+#pragma unroll
+				for (int u = 0; u < 4; u++) {
+					acc0 = fma((double)av[u].x, (double)xv[u], acc0);
+					acc1 = fma((double)av[u].y, (double)xv[u], acc1);
+					acc2 = fma((double)av[u].z, (double)xv[u], acc2);
+					acc3 = fma((double)av[u].w, (double)xv[u], acc3);
+				}
+			}
+			for (; r < r1; r++) {
 				float xv = __ldg(x + r);
 				float4 av = __ldg(reinterpret_cast<const float4 *>(op.A + r * n + c0));
 				acc0 = fma((double)av.x, (double)xv, acc0);
@@ -83,6 +118,7 @@ __global__ void __launch_bounds__(256) k_dense_adj(const Inst *tab, TileMap map,
 				acc2 = fma((double)av.z, (double)xv, acc2);
 				acc3 = fma((double)av.w, (double)xv, acc3);
 			}
+		}
 	} else {
 		for (long long r = r0; r < r1; r++) {
 			float xv = __ldg(x + r);
@@ -100,22 +136,30 @@ __global__ void __launch_bounds__(256) k_dense_adj(const Inst *tab, TileMap map,
 	if (c0 + 3 < n) p[c0 + 3] = (float)acc3;
 }
 
+// y = sum of the K row-chunk partials, 32 columns per block: warp w adds the
+// partials k = w, w + 8, ... of its lane's column, then warp 0 adds the eight
+// warp sums in a fixed order (deterministic)
 __global__ void __launch_bounds__(256) k_dense_red(const Inst *tab, TileMap map, int pred, VecSel xs, VecSel ys,
                                                    const float *part, unsigned long long *launches) {
 	OPROLOGUE();
+	__shared__ double ws[8][32];
 	const OpDev &op = I.op;
 	const long long n = op.n;
 	const int K = op.dense_kchunks;
-	const long long ct_n = (n + 1023) / 1024;
+	const long long ct_n = (n + 31) / 32;
 	const long long layer = local / ct_n, ct = local - layer * ct_n;
-	float *y = vselw(I, ys) + layer * n;
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const long long c = ct * 32 + lane;
 	const float *p = part + op.dense_part + layer * K * n;
-	for (int e = 0; e < 4; e++) {
-		long long c = ct * 1024 + e * 256 + threadIdx.x;
-		if (c >= n) continue;
-		double s = 0.0;
-		for (int k = 0; k < K; k++) s += p[(long long)k * n + c];
-		y[c] = (float)s;
+	double s = 0.0;
+	if (c < n)
+		for (int k = warp; k < K; k += 8) s += p[(long long)k * n + c];
+	ws[warp][lane] = s;
+	__syncthreads();
+	if (warp == 0 && c < n) {
+		double t = ws[0][lane];
+		for (int w = 1; w < 8; w++) t += ws[w][lane];
+		vselw(I, ys)[layer * n + c] = (float)t;
 	}
 }
 

@@ -315,7 +315,7 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 	for (int i = 0; i < cnt; i++) {
 		OpDev &d = inst[i].op;
 		if (d.kind != TVAL3G_OP_DENSE) continue;
-		tb.add(i, d.layers * ((d.n + 1023) / 1024));
+		tb.add(i, d.layers * ((d.n + 31) / 32));
 	}
 	tb.close(&ob.dense_red);
 	// compressed gathers: each instance in the width class of its own mean
