@@ -54,6 +54,9 @@ extern "C" {
                                    conditional nodes (no host round trips) */
 #define TVAL3G_TRACE 4          /* record one tval3g_trace_record per inner
                                    iteration on the device (tval3g_plan_trace) */
+#define TVAL3G_NO_TENSOR 8      /* dense operators with 16, 32, 48 or 64 layers
+                                   use the FP64-accumulating gemv kernels instead
+                                   of the tcgen05 3xTF32 tensor-core path */
 
 /* Per inner iteration: step length, objective after update_W, relative
  * change, backtracking steps taken (6 = restart after five failures), whether

@@ -1,0 +1,80 @@
+"""The multi-right-hand-side dense operator on the tcgen05 tensor cores
+(3xTF32, `layers` in {16, 32, 48, 64}): products against FP64 and against the
+FP64-accumulating gemv kernels, determinism, and a layered solve against the
+FP64 oracle (the reference's joint multi-layer solve, 2d/mat_mult.h:15-36)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import relerr
+from tval3g import capi
+from tval3g import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+# (m, n, layers): ragged tile edges (300, 1000), long K (16384), wide N (64)
+SHAPES = [(256, 512, 16), (300, 1000, 32), (1024, 4096, 48), (4096, 2048, 64), (512, 16384, 32)]
+PRODUCT_TOL = 1e-5   # per layer, relative L2 against the FP64 product
+
+
+def _layer_err(got, ref):
+    return max(relerr(g, r) for g, r in zip(got, ref))
+
+
+@pytest.mark.parametrize("m,n,N", SHAPES)
+def test_products_match_fp64(m, n, N, torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(m * 7 + n * 3 + N)
+    A = (rng.standard_normal((m, n)) / np.sqrt(m)).astype(np.float32)
+    X = rng.standard_normal((N, n)).astype(np.float32)
+    R = rng.standard_normal((N, m)).astype(np.float32)
+    Y64 = X.astype(np.float64) @ A.T.astype(np.float64)
+    Z64 = R.astype(np.float64) @ A.astype(np.float64)
+    spec = capi.dense_problem((N, n), A, layers=N)
+    dx, dr = torch.tensor(X.ravel(), device="cuda"), torch.tensor(R.ravel(), device="cuda")
+    res = {}
+    for tensor in (True, False):
+        op = capi.Operator(spec, tensor=tensor)
+        y = torch.empty(N * m, device="cuda")
+        z = torch.empty(N * n, device="cuda")
+        op.apply(dx, y)
+        op.apply(dr, z, trans=True)
+        res[tensor] = (y.cpu().numpy().reshape(N, m), z.cpu().numpy().reshape(N, n))
+        if tensor:   # same inputs, same bits
+            y2 = torch.empty_like(y)
+            op.apply(dx, y2)
+            assert torch.equal(y, y2)
+        op.close()
+    ey, ez = _layer_err(res[True][0], Y64), _layer_err(res[True][1], Z64)
+    assert ey <= PRODUCT_TOL and ez <= PRODUCT_TOL, (ey, ez)
+    # the gemv path (FP64 accumulation) is the closer of the two
+    assert _layer_err(res[False][0], Y64) <= 1e-6 and _layer_err(res[False][1], Z64) <= 1e-6
+
+
+def _layered_case(side=16, layers=16, m=128, seed=5):
+    rng = np.random.default_rng(seed)
+    n = side * side
+    A = (rng.standard_normal((m, n)) / np.sqrt(m)).astype(np.float32)
+    us = [W.ellipse_phantom(side, side, rng, 3, 0.0, lambda r: r.uniform(0.2, 1.0), (2, 6)) for _ in range(layers)]
+    b = np.concatenate([A.astype(np.float64) @ u.ravel() for u in us])
+    b = W.add_noise(b, 0.01, rng).astype(np.float32)
+    opts = W.options(2 ** 8, 2 ** 5, 1e-12, 40, tv_norm=1)
+    return A, b, opts, (side * layers, side)
+
+
+def test_layered_solve_matches_oracle(torch_cuda):
+    A, b, opts, shape = _layered_case()
+    layers = shape[0] // shape[1]
+    ref = O.solve(O.Op.dense(A.astype(np.float64), layers=layers), b.astype(np.float64), shape, opts)
+    spec = capi.dense_problem(shape, A, layers=layers)
+    out = {}
+    for tensor in (True, False):
+        plan = capi.Plan([spec], [opts], graph=True, tensor=tensor)
+        d_b = torch_cuda.tensor(b, device="cuda")
+        d_U = torch_cuda.empty(spec.n, device="cuda")
+        info = plan.solve([d_b], [d_U])[0]
+        plan.close()
+        out[tensor] = (d_U.cpu().numpy(), info["total_iters"])
+    assert out[True][1] == out[False][1] == ref.total_iters
+    e_t, e_g = relerr(out[True][0], ref.U.ravel()), relerr(out[False][0], ref.U.ravel())
+    assert e_t <= 1e-3 and e_g <= 1e-3, (e_t, e_g)

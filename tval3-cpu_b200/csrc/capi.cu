@@ -212,6 +212,7 @@ int tval3g_op_create(tval3g_operator **out, const tval3g_problem *prob, int flag
 		std::vector<OpStore> ops(1);
 		ops[0].nnz = op->st.nnz;
 		ops[0].dev = op->st.dev;
+		ops[0].mrhs = op->st.mrhs;
 		long long dense_part = build_op_maps_upload(v, ops, op->ob, &op->d_tiles, op->s);
 		op->h = v[0];
 		if (dense_part > 0) {
@@ -243,6 +244,8 @@ int tval3g_op_apply(tval3g_operator *op, int trans, const float *d_x, float *d_y
 	if (rc != TVAL3G_OK) return rc;
 	CAPI_BEGIN
 	TG_CUDA(cudaStreamSynchronize(stream ? (cudaStream_t)stream : op->s));
+	if (op->st.mrhs && mrhs_take_error(stream ? (cudaStream_t)stream : op->s, *op->st.mrhs))
+		throw Error{TVAL3G_ERR_CUDA, "tensor-core operator: a bounded wait timed out (results invalid)"};
 	CAPI_END
 }
 

@@ -106,6 +106,7 @@ struct OpDev {
 	long long n;      // columns of one layer
 	// dense
 	const float *A;
+	int mrhs;              // layers on the tcgen05 3xTF32 path (mrhs.cu) instead of the gemv kernels
 	int dense_kchunks;     // row chunks of the transposed product
 	long long dense_part;  // offset of this instance in the dense partial buffer (floats)
 	// compressed gather operators: forward rows (CSR) and transpose (CSC)

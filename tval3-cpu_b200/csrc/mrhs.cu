@@ -1,0 +1,576 @@
+// Multi-right-hand-side dense operator on the tcgen05 tensor cores (3xTF32).
+//
+// For a dense A (m x n, row-major) and N right-hand sides stored layer-major
+// (x[l*K + k]), the forward y = A x and the adjoint y = A^T x are both one
+// contraction D[M x N] = P[M x K] Q[N x K]^T with P = A (forward: M = m,
+// K = n) or P = A^T (adjoint: a transposed copy made once, M = n, K = m).
+// Both operands are K-major, so one kernel serves both directions.
+//
+// Split precision (3xTF32): P = Ph + Pl and Q = Qh + Ql with Ph = P with its
+// low 13 mantissa bits cleared (exactly representable in TF32) and Pl = P - Ph
+// (exact in FP32, TF32 keeps its top 11 bits); D = Ph Qh + Ph Ql + Pl Qh,
+// accumulated in FP32 in tensor memory; the Pl Ql term (relative size 2^-22)
+// is dropped.  Q is split once per product into two global arrays (a few MB,
+// L2-resident); each P tile is split in shared memory by four converter warps
+// right after its TMA load, so A is read from HBM exactly once per product.
+//
+// Work split (stream-K): the tiles x K-steps iterations are cut into G equal
+// contiguous ranges, one per CTA, G = min(number of SMs, iterations) (one
+// 320-thread CTA per SM, up to 194 KB of shared memory).  For every tile segment in its range a CTA
+// writes a 128 x N FP32 partial; k_mrhs_red adds each tile's partials in CTA
+// order in FP64, so the result does not depend on timing.
+//
+// Warp roles: warp 0 issues the TMA loads (one elected lane), warp 1 owns the
+// tensor memory and issues the MMAs (one lane), warps 2-5 split P tiles, warps
+// 6-9 drain the accumulators (warp w reads TMEM lanes 32 (w % 4) .. +31).
+// Two accumulators alternate between tile segments, so draining one overlaps
+// the MMAs into the other.  Every mbarrier wait is bounded: a timeout sets the
+// operator's error flag and ends the CTA's loops; the producer then waits
+// (bounded) for its loads in flight and the MMA lane for its MMAs before the
+// tensor memory is released.
+#include "mrhs.cuh"
+
+#include <mutex>
+
+namespace tval3g {
+
+namespace {
+
+constexpr int BM = 128;           // rows per tile (MMA M = TMEM lanes)
+constexpr int BK = 32;            // K elements per stage: one 128-byte swizzle row of FP32
+constexpr int STAGES = 4;
+constexpr int THREADS = 320;
+constexpr unsigned WAIT_LIMIT = 1u << 22;
+constexpr unsigned TF32_MASK = 0xFFFFE000u;
+
+__host__ __device__ constexpr int p_tile_bytes() { return BM * BK * 4; }
+__host__ __device__ constexpr int q_tile_bytes(int N) { return N * BK * 4; }
+__host__ __device__ constexpr int stage_bytes(int N) { return 2 * p_tile_bytes() + 2 * q_tile_bytes(N); }
+__host__ __device__ constexpr int tmem_cols(int N) { return 2 * N <= 32 ? 32 : 2 * N <= 64 ? 64 : 128; }
+
+struct Bars {
+	unsigned long long full[STAGES], conv[STAGES], empty[STAGES], accf[2], acce[2], done;
+	unsigned tmem;
+	int abort;
+};
+
+size_t smem_bytes(int N) { return 1024 + (size_t)STAGES * stage_bytes(N) + sizeof(Bars); }
+
+// ---------------------------------------------------------------------------
+// PTX wrappers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+	return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned bar) {
+	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
+	unsigned ok;
+	asm volatile(
+	    "{\n\t.reg .pred p;\n\t"
+	    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+	    "selp.u32 %0, 1, 0, p;\n\t}"
+	    : "=r"(ok)
+	    : "r"(bar), "r"(parity)
+	    : "memory");
+	return ok != 0;
+}
+__device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap *map, int x, int y, unsigned bar) {
+	asm volatile(
+	    "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+	        dst),
+	    "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(bar)
+	    : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+	asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_alloc(unsigned dst_smem, unsigned ncols) {
+	asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem), "r"(ncols)
+	             : "memory");
+	asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols) {
+	asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+// D (tmem) (+)= A (smem, desc) * B (smem, desc)^T, kind::tf32, one thread
+__device__ __forceinline__ void mma_tf32(unsigned d, unsigned long long adesc, unsigned long long bdesc,
+                                         unsigned idesc, unsigned accumulate) {
+	asm volatile(
+	    "{\n\t.reg .pred p;\n\t"
+	    "setp.ne.b32 p, %4, 0;\n\t"
+	    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+	    "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+	    : "memory");
+}
+// arrive on `bar` once every tcgen05 operation issued so far by this thread is done
+__device__ __forceinline__ void mma_commit(unsigned bar) {
+	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+	             : "memory");
+}
+// 32 lanes x 16 consecutive FP32 columns: thread i gets lane (base + i)
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, float *v) {
+	unsigned r[16];
+	asm volatile(
+	    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+	    "%15}, [%16];"
+	    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+	      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+	    : "r"(taddr)
+	    : "memory");
+#pragma unroll
+	for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// shared-memory matrix descriptor: K-major operand in the 128-byte swizzle
+// layout written by TMA (rows of 128 bytes, 8-row groups 1024 bytes apart)
+__device__ __forceinline__ unsigned long long sdesc(unsigned addr) {
+	return (unsigned long long)((addr & 0x3FFFFu) >> 4)   // start address / 16
+	       | (1ull << 16)                                 // leading byte offset (unused when swizzled)
+	       | (64ull << 32)                                // stride byte offset: 1024 / 16
+	       | (1ull << 46)                                 // descriptor version of sm_100
+	       | (2ull << 61);                                // 128-byte swizzle
+}
+// instruction descriptor: D FP32, A and B TF32, both K-major, M = 128
+__host__ __device__ constexpr unsigned idesc_tf32(int N) {
+	return (1u << 4)                      // D format: F32
+	       | (2u << 7)                    // A format: TF32
+	       | (2u << 10)                   // B format: TF32
+	       | ((unsigned)(N >> 3) << 17)   // N / 8
+	       | ((unsigned)(BM >> 4) << 24); // M / 16
+}
+
+// bounded waits; false on timeout (which also raises the abort flag) or abort
+__device__ __forceinline__ bool wait1(unsigned bar, unsigned parity, volatile int *abort, int *err) {
+	for (unsigned i = 0; i < WAIT_LIMIT; i++) {
+		if (mbar_try(bar, parity)) return true;
+		if ((i & 255u) == 255u && *abort) return false;
+	}
+	*abort = 1;
+	atomicExch(err, 1);
+	return false;
+}
+// every lane of the warp polls; the warp leaves together
+__device__ __forceinline__ bool wait_warp(unsigned bar, unsigned parity, volatile int *abort, int *err) {
+	for (unsigned i = 0; i < WAIT_LIMIT; i++) {
+		if (__all_sync(0xffffffffu, mbar_try(bar, parity))) return true;
+		if ((i & 255u) == 255u && __any_sync(0xffffffffu, *abort != 0)) return false;
+	}
+	if ((threadIdx.x & 31) == 0) {
+		*abort = 1;
+		atomicExch(err, 1);
+	}
+	return false;
+}
+
+struct MrhsArgs {
+	const Inst *tab;
+	int inst, pred;
+	int M;          // rows of D
+	int ks;         // K steps of BK
+	int J;          // partial slots per CTA
+	long long T;    // tiles x ks
+	float *part;    // [G][J][N][BM]
+	int *err;
+	unsigned long long *launches;
+};
+
+template <int N>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_mrhs(const __grid_constant__ CUtensorMap tmP, const __grid_constant__ CUtensorMap tmQh,
+           const __grid_constant__ CUtensorMap tmQl, MrhsArgs a) {
+	if (!pred_ok(*a.tab[a.inst].ctrl, a.pred)) return;
+	if (a.launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(a.launches, 1ull);
+	extern __shared__ unsigned char smem_raw[];
+	const unsigned raw = smem_u32(smem_raw);
+	const unsigned base = (raw + 1023u) & ~1023u;   // swizzled tiles need 1024-byte alignment
+	constexpr int SB = stage_bytes(N);
+	constexpr unsigned TX = (unsigned)(p_tile_bytes() + 2 * q_tile_bytes(N));
+	constexpr unsigned NCOLS = tmem_cols(N);
+	Bars *bars = reinterpret_cast<Bars *>(smem_raw + (base - raw) + STAGES * SB);
+	volatile int *abort = &bars->abort;
+	auto st_p = [&](int s) { return base + s * SB; };
+	auto st_l = [&](int s) { return base + s * SB + p_tile_bytes(); };
+	auto st_qh = [&](int s) { return base + s * SB + 2 * p_tile_bytes(); };
+	auto st_ql = [&](int s) { return base + s * SB + 2 * p_tile_bytes() + q_tile_bytes(N); };
+	const unsigned b_full = smem_u32(&bars->full[0]), b_conv = smem_u32(&bars->conv[0]),
+	               b_empty = smem_u32(&bars->empty[0]), b_accf = smem_u32(&bars->accf[0]),
+	               b_acce = smem_u32(&bars->acce[0]), b_done = smem_u32(&bars->done);
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+	// this CTA's range of (tile, K step) iterations
+	const long long G = gridDim.x;
+	const long long it0 = (long long)blockIdx.x * a.T / G, it1 = ((long long)blockIdx.x + 1) * a.T / G;
+	const int tile0 = (int)(it0 / a.ks);
+	const int nseg = (int)((it1 - 1) / a.ks) - tile0 + 1;
+
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < STAGES; s++) {
+			mbar_init(b_full + 8 * s, 1);
+			mbar_init(b_conv + 8 * s, 4);
+			mbar_init(b_empty + 8 * s, 1);
+		}
+		for (int i = 0; i < 2; i++) {
+			mbar_init(b_accf + 8 * i, 1);
+			mbar_init(b_acce + 8 * i, 4);
+		}
+		mbar_init(b_done, 1);
+		bars->abort = 0;
+		fence_mbar_init();
+	}
+	if (warp == 1) tmem_alloc(smem_u32(&bars->tmem), NCOLS);
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const unsigned tmem = bars->tmem;
+
+	if (warp == 0) {
+		if (lane == 0) {   // TMA producer
+			unsigned it = 0;
+			for (long long g = it0; g < it1; g++, it++) {
+				const int s = it % STAGES;
+				if (!wait1(b_empty + 8 * s, ((it / STAGES) & 1) ^ 1, abort, a.err)) break;
+				const int tile = (int)(g / a.ks), k = (int)(g - (long long)tile * a.ks);
+				mbar_expect_tx(b_full + 8 * s, TX);
+				tma_load_2d(st_p(s), &tmP, k * BK, tile * BM, b_full + 8 * s);
+				tma_load_2d(st_qh(s), &tmQh, k * BK, 0, b_full + 8 * s);
+				tma_load_2d(st_ql(s), &tmQl, k * BK, 0, b_full + 8 * s);
+			}
+			// no load may still be writing shared memory when the CTA ends
+			const unsigned issued = it;
+			for (unsigned j = issued > STAGES ? issued - STAGES : 0; j < issued; j++) {
+				unsigned i = 0;
+				while (!mbar_try(b_full + 8 * (j % STAGES), (j / STAGES) & 1) && ++i < WAIT_LIMIT) {
+				}
+				if (i >= WAIT_LIMIT) atomicExch(a.err, 1);
+			}
+		}
+	} else if (warp == 1) {
+		if (lane == 0) {   // MMA issuer
+			constexpr unsigned ID = idesc_tf32(N);
+			unsigned it = 0;
+			bool ok = true;
+			for (int j = 0; j < nseg && ok; j++) {
+				const int acc = j & 1;
+				if (!wait1(b_acce + 8 * acc, ((j >> 1) & 1) ^ 1, abort, a.err)) break;
+				tc_fence_after();
+				const unsigned d = tmem + (unsigned)(acc * (NCOLS / 2));
+				const long long tb = (long long)(tile0 + j) * a.ks;
+				const long long gb = it0 > tb ? it0 : tb, ge = it1 < tb + a.ks ? it1 : tb + a.ks;
+				for (long long g = gb; g < ge; g++, it++) {
+					const int s = it % STAGES;
+					if (!wait1(b_conv + 8 * s, (it / STAGES) & 1, abort, a.err)) {
+						ok = false;
+						break;
+					}
+					tc_fence_after();
+#pragma unroll
+					for (int kk = 0; kk < BK / 8; kk++) {   // K = 8 per MMA: 32 bytes
+						const unsigned off = kk * 32;
+						const unsigned long long ph = sdesc(st_p(s) + off), pl = sdesc(st_l(s) + off);
+						const unsigned long long qh = sdesc(st_qh(s) + off), ql = sdesc(st_ql(s) + off);
+						mma_tf32(d, ph, qh, ID, (g > gb || kk > 0) ? 1u : 0u);
+						mma_tf32(d, ph, ql, ID, 1u);
+						mma_tf32(d, pl, qh, ID, 1u);
+					}
+					mma_commit(b_empty + 8 * s);
+				}
+				if (ok) mma_commit(b_accf + 8 * acc);
+			}
+			// every MMA issued has finished before the tensor memory is released
+			mma_commit(b_done);
+			unsigned i = 0;
+			while (!mbar_try(b_done, 0) && ++i < WAIT_LIMIT) {
+			}
+			if (i >= WAIT_LIMIT) atomicExch(a.err, 1);
+		}
+	} else if (warp < 6) {   // split P tiles into high and low parts
+		const int t = threadIdx.x - 64;
+		unsigned it = 0;
+		for (long long g = it0; g < it1; g++, it++) {
+			const int s = it % STAGES;
+			if (!wait_warp(b_full + 8 * s, (it / STAGES) & 1, abort, a.err)) break;
+			float4 *P = reinterpret_cast<float4 *>(smem_raw + (st_p(s) - raw));
+			float4 *L = reinterpret_cast<float4 *>(smem_raw + (st_l(s) - raw));
+#pragma unroll
+			for (int i = 0; i < p_tile_bytes() / 16 / 128; i++) {
+				const int idx = i * 128 + t;
+				const float4 v = P[idx];
+				float4 h;
+				h.x = __uint_as_float(__float_as_uint(v.x) & TF32_MASK);
+				h.y = __uint_as_float(__float_as_uint(v.y) & TF32_MASK);
+				h.z = __uint_as_float(__float_as_uint(v.z) & TF32_MASK);
+				h.w = __uint_as_float(__float_as_uint(v.w) & TF32_MASK);
+				P[idx] = h;
+				L[idx] = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+			}
+			fence_proxy_async_smem();   // generic-proxy writes, read next by the tensor cores
+			__syncwarp();
+			if (lane == 0) mbar_arrive(b_conv + 8 * s);
+		}
+	} else {   // epilogue: accumulator -> partial tile
+		const int q = warp & 3;
+		const int row = q * 32 + lane;
+		for (int j = 0; j < nseg; j++) {
+			const int acc = j & 1;
+			if (!wait_warp(b_accf + 8 * acc, (j >> 1) & 1, abort, a.err)) break;
+			tc_fence_after();
+			float v[N];
+#pragma unroll
+			for (int c = 0; c < N; c += 16)
+				tmem_ld16(tmem + ((unsigned)(q * 32) << 16) + (unsigned)(acc * (NCOLS / 2) + c), v + c);
+			tmem_wait_ld();
+			tc_fence_before();
+			__syncwarp();
+			if (lane == 0) mbar_arrive(b_acce + 8 * acc);
+			const int tile = tile0 + j;
+			if ((long long)tile * BM + row < a.M) {
+				float *dst = a.part + ((long long)blockIdx.x * a.J + j) * N * BM + row;
+#pragma unroll
+				for (int c = 0; c < N; c++) dst[c * BM] = v[c];
+			}
+		}
+	}
+
+	tc_fence_before();
+	__syncthreads();
+	if (warp == 1) {
+		__syncwarp();
+		tc_fence_after();
+		tmem_dealloc(tmem, NCOLS);
+	}
+}
+
+// D[r, l] = sum over the CTAs whose range meets tile r / BM of their partial
+__global__ void __launch_bounds__(256) k_mrhs_red(const Inst *tab, int inst, int pred, VecSel ys, const float *part,
+                                                  int M, int N, int ks, long long T, int G, int J,
+                                                  unsigned long long *launches) {
+	const Inst &I = tab[inst];
+	if (!pred_ok(*I.ctrl, pred)) return;
+	if (launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);
+	const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= (long long)N * M) return;
+	const int l = (int)(idx / M), r = (int)(idx - (long long)l * M);
+	const int t = r / BM, row = r - t * BM;
+	const long long i0 = (long long)t * ks, i1 = i0 + ks - 1;
+	const int c0 = (int)(((i0 + 1) * G - 1) / T), c1 = (int)(((i1 + 1) * G - 1) / T);
+	double s = 0.0;
+	for (int c = c0; c <= c1; c++) {
+		const long long beg = (long long)c * T / G;
+		const int j = t - (int)(beg / ks);
+		s += part[(((long long)c * J + j) * N + l) * BM + row];
+	}
+	float *y = ys.m ? I.vm[ys.idx] : I.vn[ys.idx];
+	y[(long long)l * M + r] = (float)s;
+}
+
+// right-hand sides -> high (TF32-exact) and low parts
+__global__ void __launch_bounds__(256) k_mrhs_split(const Inst *tab, int inst, int pred, VecSel xs, long long len,
+                                                    float *hi, float *lo, unsigned long long *launches) {
+	const Inst &I = tab[inst];
+	if (!pred_ok(*I.ctrl, pred)) return;
+	if (launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);
+	const float *x = xs.m ? I.vm[xs.idx] : I.vn[xs.idx];
+	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x) {
+		const float v = x[i];
+		const float h = __uint_as_float(__float_as_uint(v) & TF32_MASK);
+		hi[i] = h;
+		lo[i] = v - h;
+	}
+}
+
+__global__ void k_transpose(const float *A, long long m, long long n, float *At) {
+	__shared__ float tile[32][33];
+	const long long c0 = (long long)blockIdx.x * 32, r0 = (long long)blockIdx.y * 32;
+	for (int i = threadIdx.y; i < 32; i += 8) {
+		const long long r = r0 + i, c = c0 + threadIdx.x;
+		if (r < m && c < n) tile[i][threadIdx.x] = A[r * n + c];
+	}
+	__syncthreads();
+	for (int i = threadIdx.y; i < 32; i += 8) {
+		const long long c = c0 + i, r = r0 + threadIdx.x;
+		if (r < m && c < n) At[c * m + r] = tile[threadIdx.x][i];
+	}
+}
+
+// ---------------------------------------------------------------------------
+// host
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encoder() {
+	static std::once_flag once;
+	static EncodeTiled fn = nullptr;
+	std::call_once(once, [] {
+		void *p = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+		    q == cudaDriverEntryPointSuccess)
+			fn = reinterpret_cast<EncodeTiled>(p);
+	});
+	if (!fn) throw Error{TVAL3G_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver"};
+	return fn;
+}
+
+// row-major rows x inner FP32 matrix, box of box_rows x 32 elements, 128-byte swizzle
+CUtensorMap make_map(const float *ptr, long long inner, long long rows, int box_rows) {
+	CUtensorMap m;
+	const cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)rows};
+	const cuuint64_t strides[1] = {(cuuint64_t)inner * sizeof(float)};
+	const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+	const cuuint32_t estr[2] = {1, 1};
+	CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(ptr), dims, strides, box, estr,
+	                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+	                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	if (r != CUDA_SUCCESS)
+		throw Error{TVAL3G_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")"};
+	return m;
+}
+
+// stream-K plan of one direction: K steps, tiles, iterations, partial slots
+void plan_dir(long long M, long long K, int G, int &ks, int &tiles, long long &T, int &J) {
+	ks = (int)((K + BK - 1) / BK);
+	tiles = (int)((M + BM - 1) / BM);
+	T = (long long)tiles * ks;
+	J = 1;
+	for (long long c = 0; c < G; c++) {
+		const long long i0 = c * T / G, i1 = (c + 1) * T / G;
+		if (i1 > i0) J = std::max(J, (int)((i1 - 1) / ks - i0 / ks + 1));
+	}
+}
+
+template <int N>
+void set_smem_attr() {
+	static std::once_flag once;
+	static cudaError_t rc = cudaSuccess;
+	std::call_once(once, [] {
+		rc = cudaFuncSetAttribute(k_mrhs<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(N));
+	});
+	TG_CUDA(rc);
+}
+
+template <int N>
+void launch_mrhs(cudaStream_t s, int G, const CUtensorMap &p, const CUtensorMap &qh, const CUtensorMap &ql,
+                 const MrhsArgs &a) {
+	set_smem_attr<N>();
+	k_mrhs<N><<<G, THREADS, smem_bytes(N), s>>>(p, qh, ql, a);
+}
+
+}  // namespace
+
+MrhsOp::~MrhsOp() {
+	if (at) cudaFree(at);
+	if (xh) cudaFree(xh);
+	if (xl) cudaFree(xl);
+	if (part) cudaFree(part);
+	if (err) cudaFree(err);
+}
+
+bool mrhs_eligible(long long m, long long n, int layers) {
+	return (layers == 16 || layers == 32 || layers == 48 || layers == 64) && m >= BM && n >= BM && m % 4 == 0 &&
+	       n % 4 == 0 && m < (1LL << 31) / 64 && n < (1LL << 31) / 64 && (m + 31) / 32 < 65535;
+}
+
+std::shared_ptr<MrhsOp> mrhs_create(cudaStream_t s, const float *d_A, long long m, long long n, int layers) {
+	TG_ARG(mrhs_eligible(m, n, layers), "Internal error: operator not eligible for the tensor-core path");
+	TG_ARG((reinterpret_cast<uintptr_t>(d_A) & 15) == 0, "Argument error: A must be 16-byte aligned");
+	auto op = std::make_shared<MrhsOp>();
+	op->m = m;
+	op->n = n;
+	op->N = layers;
+	int dev = 0, sms = 0;
+	TG_CUDA(cudaGetDevice(&dev));
+	TG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+	// one CTA per SM, fewer when there are fewer (tile, K step) iterations
+	const long long tf = ((m + BM - 1) / BM) * ((n + BK - 1) / BK), ta = ((n + BM - 1) / BM) * ((m + BK - 1) / BK);
+	op->grid_f = (int)std::min<long long>(sms, tf);
+	op->grid_a = (int)std::min<long long>(sms, ta);
+	plan_dir(m, n, op->grid_f, op->ks_f, op->tiles_f, op->t_f, op->j_f);
+	plan_dir(n, m, op->grid_a, op->ks_a, op->tiles_a, op->t_a, op->j_a);
+	const long long kmax = std::max(m, n);
+	const long long part = std::max((long long)op->grid_f * op->j_f, (long long)op->grid_a * op->j_a) * layers * BM;
+	TG_CUDA(cudaMalloc(&op->at, sizeof(float) * (size_t)(m * n)));
+	TG_CUDA(cudaMalloc(&op->xh, sizeof(float) * (size_t)(kmax * layers)));
+	TG_CUDA(cudaMalloc(&op->xl, sizeof(float) * (size_t)(kmax * layers)));
+	TG_CUDA(cudaMalloc(&op->part, sizeof(float) * (size_t)part));
+	TG_CUDA(cudaMalloc(&op->err, sizeof(int)));
+	TG_CUDA(cudaMemsetAsync(op->err, 0, sizeof(int), s));
+	op->bytes = 4 * (m * n + 2 * kmax * layers + part) + 4;
+	dim3 tb(32, 8), tg((unsigned)((n + 31) / 32), (unsigned)((m + 31) / 32));
+	k_transpose<<<tg, tb, 0, s>>>(d_A, m, n, op->at);
+	TG_CUDA(cudaGetLastError());
+	op->tm_a = make_map(d_A, n, m, BM);
+	op->tm_at = make_map(op->at, m, n, BM);
+	op->tm_xh_f = make_map(op->xh, n, layers, layers);
+	op->tm_xl_f = make_map(op->xl, n, layers, layers);
+	op->tm_xh_a = make_map(op->xh, m, layers, layers);
+	op->tm_xl_a = make_map(op->xl, m, layers, layers);
+	return op;
+}
+
+void mrhs_apply(cudaStream_t s, const Inst *tab, int inst, int pred, const MrhsOp &op, bool trans, VecSel x,
+                VecSel y, unsigned long long *launches) {
+	const long long K = trans ? op.m : op.n, M = trans ? op.n : op.m;
+	const long long len = K * op.N;
+	const int G = trans ? op.grid_a : op.grid_f;
+	k_mrhs_split<<<(unsigned)std::min<long long>((len + 255) / 256, 4LL * G), 256, 0, s>>>(
+	    tab, inst, pred, x, len, op.xh, op.xl, launches);
+	TG_CUDA(cudaGetLastError());
+	MrhsArgs a;
+	a.tab = tab;
+	a.inst = inst;
+	a.pred = pred;
+	a.M = (int)M;
+	a.ks = trans ? op.ks_a : op.ks_f;
+	a.J = trans ? op.j_a : op.j_f;
+	a.T = trans ? op.t_a : op.t_f;
+	a.part = op.part;
+	a.err = op.err;
+	a.launches = launches;
+	const CUtensorMap &P = trans ? op.tm_at : op.tm_a;
+	const CUtensorMap &QH = trans ? op.tm_xh_a : op.tm_xh_f;
+	const CUtensorMap &QL = trans ? op.tm_xl_a : op.tm_xl_f;
+	switch (op.N) {
+	case 16: launch_mrhs<16>(s, G, P, QH, QL, a); break;
+	case 32: launch_mrhs<32>(s, G, P, QH, QL, a); break;
+	case 48: launch_mrhs<48>(s, G, P, QH, QL, a); break;
+	case 64: launch_mrhs<64>(s, G, P, QH, QL, a); break;
+	default: throw Error{TVAL3G_ERR_INTERNAL, "Internal error: unsupported right-hand-side count"};
+	}
+	TG_CUDA(cudaGetLastError());
+	const long long outs = M * op.N;
+	k_mrhs_red<<<(unsigned)((outs + 255) / 256), 256, 0, s>>>(tab, inst, pred, y, op.part, (int)M, op.N, a.ks, a.T, G,
+	                                                          a.J, launches);
+	TG_CUDA(cudaGetLastError());
+}
+
+int mrhs_take_error(cudaStream_t s, const MrhsOp &op) {
+	int h = 0;
+	TG_CUDA(cudaMemcpyAsync(&h, op.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+	TG_CUDA(cudaStreamSynchronize(s));
+	if (h) TG_CUDA(cudaMemsetAsync(op.err, 0, sizeof(int), s));
+	return h;
+}
+
+}  // namespace tval3g

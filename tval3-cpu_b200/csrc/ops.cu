@@ -486,6 +486,7 @@ static void gather(const LaunchCtx &L, const TileMap (&maps)[4], int pred, int k
 
 void op_forward(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y) {
 	auto *ctr = (unsigned long long *)L.launches;
+	for (const auto &e : B.mrhs) mrhs_apply(L.stream, L.inst, e.first, pred, *e.second, false, x, y, ctr);
 	if (B.dense_fwd.count > 0) {
 		k_dense_fwd<<<B.dense_fwd.count, 256, 0, L.stream>>>(L.inst, B.dense_fwd, pred, x, y, ctr);
 		TG_CUDA(cudaGetLastError());
@@ -507,6 +508,7 @@ void op_forward(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel
 
 void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y) {
 	auto *ctr = (unsigned long long *)L.launches;
+	for (const auto &e : B.mrhs) mrhs_apply(L.stream, L.inst, e.first, pred, *e.second, true, x, y, ctr);
 	if (B.dense_adj.count > 0) {
 		k_dense_adj<<<B.dense_adj.count, 256, 0, L.stream>>>(L.inst, B.dense_adj, pred, x, y, B.dense_part, ctr);
 		TG_CUDA(cudaGetLastError());

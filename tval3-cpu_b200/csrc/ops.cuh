@@ -1,7 +1,11 @@
 // Measurement operators of the TVAL3 solve (modk/tval3-cpu 2d/mat_mult.h,
 // 3d/mat_mult.h), batched over the instances of a plan.
 #pragma once
+#include <memory>
+#include <utility>
+
 #include "engine.cuh"
+#include "mrhs.cuh"
 
 namespace tval3g {
 
@@ -12,6 +16,9 @@ struct OpBatch {
 	// (column tile, row chunk) blocks into partials, then a column reduction
 	TileMap dense_fwd, dense_adj, dense_red;
 	float *dense_part = nullptr;
+	// dense operators with 16-64 layers: one launch sequence per instance on
+	// the tensor cores (mrhs.cu)
+	std::vector<std::pair<int, std::shared_ptr<MrhsOp>>> mrhs;
 	// compressed gathers: CSR rows (forward), CSC columns (adjoint of CSR and
 	// of the ray operators).  Each instance gets the sub-warp width that suits
 	// its mean line length (4, 8, 16 or 32 lanes per line: class 0..3), so its

@@ -138,6 +138,11 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		d.m = p.m; d.n = p.n_cols;
 		d.A = dcopy(s, st, p.A, (long long)p.m * p.n_cols, borrow);
 		st.b_len = (long long)p.m * d.layers;
+		if (!(flags & TVAL3G_NO_TENSOR) && mrhs_eligible(d.m, d.n, d.layers)) {
+			st.mrhs = mrhs_create(s, d.A, d.m, d.n, d.layers);
+			st.bytes += st.mrhs->bytes;
+			d.mrhs = 1;
+		}
 	} else if (p.op_kind == TVAL3G_OP_CSR) {
 		d.m = p.m; d.n = p.n_cols;
 		st.nnz = p.nnz;
@@ -250,6 +255,7 @@ void free_op(OpStore &st) {
 	for (void *q : st.owned)
 		if (q) cudaFree(q);
 	st.owned.clear();
+	st.mrhs.reset();
 }
 
 // ---------------------------------------------------------------------------
@@ -297,12 +303,16 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 	for (int i = 0; i < cnt; i++) {
 		OpDev &d = inst[i].op;
 		if (d.kind != TVAL3G_OP_DENSE) continue;
+		if (d.mrhs) {
+			ob.mrhs.emplace_back(i, ops[i].mrhs);
+			continue;
+		}
 		tb.add(i, d.layers * ((d.m + WARPS - 1) / WARPS));
 	}
 	tb.close(&ob.dense_fwd);
 	for (int i = 0; i < cnt; i++) {
 		OpDev &d = inst[i].op;
-		if (d.kind != TVAL3G_OP_DENSE) continue;
+		if (d.kind != TVAL3G_OP_DENSE || d.mrhs) continue;
 		long long ct = (d.n + 1023) / 1024;
 		long long K = (4 * 148 + d.layers * ct - 1) / (d.layers * ct);
 		K = std::max(1LL, std::min(K, d.m));
@@ -314,7 +324,7 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 	tb.close(&ob.dense_adj);
 	for (int i = 0; i < cnt; i++) {
 		OpDev &d = inst[i].op;
-		if (d.kind != TVAL3G_OP_DENSE) continue;
+		if (d.kind != TVAL3G_OP_DENSE || d.mrhs) continue;
 		tb.add(i, d.layers * ((d.n + 31) / 32));
 	}
 	tb.close(&ob.dense_red);
@@ -521,6 +531,7 @@ void Plan::release() {
 	if (stream_) cudaStreamSynchronize(stream_);
 	for (void *p : allocs_) cudaFree(p);
 	allocs_.clear();
+	ob_.mrhs.clear();
 	for (auto &o : ops_) free_op(o);
 	ops_.clear();
 	if (h_flag_) cudaFreeHost(h_flag_);
@@ -743,6 +754,9 @@ void Plan::solve(const float *const *d_b, const float *const *d_Ut, float *const
 	TG_CUDA(cudaMemcpyAsync(hc.data(), d_ctrl_, sizeof(Ctrl) * count_, cudaMemcpyDeviceToHost, cur_));
 	TG_CUDA(cudaMemcpyAsync(&nl, d_launches_, sizeof(nl), cudaMemcpyDeviceToHost, cur_));
 	TG_CUDA(cudaStreamSynchronize(cur_));
+	for (const auto &e : ob_.mrhs)
+		if (mrhs_take_error(cur_, *e.second))
+			throw Error{TVAL3G_ERR_CUDA, "tensor-core operator: a bounded wait timed out (results invalid)"};
 	last_launches_ = (long long)nl;
 	last_iters_.resize(count_);
 	for (int i = 0; i < count_; i++) last_iters_[i] = hc[i].count_total;

@@ -4,6 +4,7 @@
 #include <memory>
 
 #include "kernels.cuh"
+#include "mrhs.cuh"
 #include "ops.cuh"
 
 namespace tval3g {
@@ -12,6 +13,7 @@ namespace tval3g {
 struct OpStore {
 	OpDev dev{};
 	std::vector<void *> owned;   // device allocations to free
+	std::shared_ptr<MrhsOp> mrhs;   // multi-RHS dense operator on the tensor cores, or null
 	long long bytes = 0;         // device bytes allocated for the operator
 	long long nnz = 0;           // CSR nnz, or Bresenham hits of a ray operator
 	long long b_len = 0;

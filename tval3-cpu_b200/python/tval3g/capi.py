@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(PKG, "lib", "libtval3g.so")
 OK, ERR_ARGUMENT, ERR_CUDA, ERR_NO_DEVICE, ERR_NONFINITE, ERR_INTERNAL = 0, -1, -2, -3, -4, -5
 OP_DENSE, OP_CSR, OP_RAY2D, OP_RAY3D = 0, 1, 2, 3
 TV_ANISO, TV_ISO = 0, 1
-DEVICE_INPUTS, GRAPH, TRACE = 1, 2, 4
+DEVICE_INPUTS, GRAPH, TRACE, NO_TENSOR = 1, 2, 4, 8
 
 _OPT_D = ("mu", "beta", "mu0", "beta0", "tol", "tol_inn", "c", "gamma", "gam", "rate_gam", "rate_cnt",
           "skipMulRatio", "maxRelativeChange")
@@ -242,7 +242,7 @@ class Plan:
     """Device-resident solver state for a batch of problems (graph=True: the
     iteration loop is one CUDA graph with conditional nodes)."""
 
-    def __init__(self, specs, opts_list, graph=True, device_inputs=False, trace=False):
+    def __init__(self, specs, opts_list, graph=True, device_inputs=False, trace=False, tensor=True):
         n = len(specs)
         self.specs = specs
         self.count = n
@@ -250,7 +250,8 @@ class Plan:
         probs = (Problem * n)(*[s.p for s in specs])
         opts = (Options * n)(*[Options.from_dict(o) for o in opts_list])
         h = C.c_void_p()
-        flags = (GRAPH if graph else 0) | (DEVICE_INPUTS if device_inputs else 0) | (TRACE if trace else 0)
+        flags = (GRAPH if graph else 0) | (DEVICE_INPUTS if device_inputs else 0) | (TRACE if trace else 0) | \
+            (0 if tensor else NO_TENSOR)
         _check(lib().tval3g_plan_create(C.byref(h), n, probs, opts, flags))
         self.h = h
 
@@ -295,9 +296,10 @@ class Plan:
 class Operator:
     """A measurement operator on the device: apply(x, trans) with torch tensors."""
 
-    def __init__(self, spec: ProblemSpec):
+    def __init__(self, spec: ProblemSpec, tensor=True, device_inputs=False):
         h = C.c_void_p()
-        _check(lib().tval3g_op_create(C.byref(h), C.byref(spec.p), 0))
+        flags = (0 if tensor else NO_TENSOR) | (DEVICE_INPUTS if device_inputs else 0)
+        _check(lib().tval3g_op_create(C.byref(h), C.byref(spec.p), flags))
         self.h = h
         r, c, z = C.c_longlong(), C.c_longlong(), C.c_longlong()
         _check(lib().tval3g_op_shape(h, C.byref(r), C.byref(c), C.byref(z)))
