@@ -52,7 +52,7 @@ def args_():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="tval3g", choices=["tval3g", "reference"])
-    p.add_argument("--workload", default="ring2d", choices=["ring2d", "dense2d", "hemi3d", "batch"])
+    p.add_argument("--workload", default="ring2d", choices=["ring2d", "dense2d", "hemi3d", "batch", "mrhs"])
     p.add_argument("--cpu-sample-iters", type=int, default=20)
     p.add_argument("--profile", action="store_true",
                    help="for ncu: build the plan, run --warmup + --steps solves, print nothing else")
@@ -85,6 +85,9 @@ CONFIGS = {
     "hemi3d": {"workload": "3D 128^3, 2048 hemisphere transducers x 1024 random receivers (2.1M rays), aniso TV, "
                            "mu 2^10, beta 2^6, tol 1e-5, maxit 400; hit weight 1/sigma_max(A)",
                "operator": "on-the-fly 3D Bresenham projector, gather adjoint"},
+    "mrhs": {"workload": "dense A 4096 x 16384 N(0,1/m), 32 right-hand sides (128x128 phantoms) solved jointly as "
+                         "32 layers, iso TV, mu 2^8, beta 2^5, tol 1e-4, maxit 300",
+             "operator": "tcgen05 3xTF32 multi-RHS product (TMA, TMEM, stream-K over all SMs)"},
     "batch": {"workload": "64 independent 2D problems, sides {64..256}, dense Gaussian (25-40 % sampling) or ring "
                           "Bresenham (128-512 transducers)",
               "operator": "mixed dense / ray, one batched plan"},
@@ -92,7 +95,7 @@ CONFIGS = {
 
 
 def fp64_reference(name):
-    f = {"ring2d": "ring256_fp64.npz", "dense2d": "dense64_fp64.npz"}.get(name)
+    f = {"ring2d": "ring256_fp64.npz", "dense2d": "dense64_fp64.npz", "mrhs": "mrhs32_fp64.npz"}.get(name)
     if f and os.path.exists(os.path.join(GOLDEN, f)):
         return dict(np.load(os.path.join(GOLDEN, f)))
     return None
@@ -391,6 +394,89 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
     return line
 
 
+def run_mrhs(a, cx, capi, world, dist, clocks):
+    """Joint multi-RHS solve: the tensor-core product against the
+    FP64-accumulating gemv kernels, both as CUDA graphs."""
+    from tval3g import workloads as W
+    torch, dev, stream = cx.torch, cx.dev, cx.stream
+    w = W.mrhs()
+    N, (m, n) = w["layers"], w["A"].shape
+    d_A = torch.tensor(w["A"], device=dev)
+    spec = capi.dense_problem(w["shape"], w["A"], layers=N, device_ptr=d_A.data_ptr())
+    opts = dict(w["opts"])
+    d_b = torch.tensor(w["b"], device=dev)
+    d_U = torch.empty(spec.n, device=dev)
+    if a.maxit is not None:
+        opts["maxit"] = a.maxit
+    if a.profile:
+        plan = capi.Plan([spec], [opts], graph=not a.plain, device_inputs=True)
+        cx.event_time(lambda: plan.solve([d_b], [d_U], stream=stream.cuda_stream), a.warmup + a.steps)
+        plan.close()
+        return None
+    ref = fp64_reference("mrhs")
+    d_ref = torch.tensor(ref["U"].ravel(), device=dev) if ref is not None else None
+    target = 1e-3 if ref is not None else 0.0
+    res = {}
+    for tensor in (True, False):
+        plan = capi.Plan([spec], [opts], graph=True, device_inputs=True, tensor=tensor)
+        plan.set_target(target)
+        run = lambda: plan.solve([d_b], [d_U], d_Ut=[d_ref] if d_ref is not None else None,  # noqa: E731
+                                 stream=stream.cuda_stream)
+        cx.event_time(run, max(a.warmup, 3) if tensor else 1)
+        if tensor:
+            if dist:
+                dist.barrier()
+            clocks.start()
+        ts, infos = cx.event_time(run, a.steps if tensor else 2)
+        if tensor:
+            clk = clocks.stop()
+            launches = plan.stats()["kernel_launches"] * a.steps
+            U = d_U.cpu().numpy().reshape(N, -1)
+        res[tensor] = (float(np.mean(ts)), infos[0])
+        plan.close()
+    ms, info = res[True]
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    per_rhs = None
+    if ref is not None:
+        R = ref["U"].reshape(N, -1)
+        per_rhs = [float(np.linalg.norm(U[k] - R[k]) / np.linalg.norm(R[k])) for k in range(N)]
+    # the product alone: forward (split + tcgen05 kernel + reduce), L2 flushed
+    op = capi.Operator(spec, tensor=True, device_inputs=True)
+    x = torch.rand(op.cols, device=dev)
+    y = torch.empty(op.rows, device=dev)
+    op.apply_n(x, y, 3, stream=stream.cuda_stream)
+    kt, _ = cx.event_time(lambda: op.apply_n(x, y, 1, stream=stream.cuda_stream), 10)
+    zt, _ = cx.event_time(lambda: op.apply_n(y, x, 1, trans=True, stream=stream.cuda_stream), 10)
+    op.close()
+    k_ms = float(np.mean(kt))
+    bytes_ = 4 * m * n + 4 * N * (m + n)
+    peak, src = peak_hbm()
+    achieved = bytes_ / (k_ms * 1e-3) / 1e9
+    return {"metric": METRIC, "value": world * N * 1000.0 / ms, "unit": "reconstructions/s (right-hand sides)",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 data, 3xTF32 products",
+            "data": "synthetic (seeded A, phantoms, noise)",
+            "config": dict(CONFIGS["mrhs"], rhs=N, l2="256 MB write between timed solves"),
+            "iterations": info["total_iters"], "relerr_vs_fp64": float(info["rel_error"]) if ref is not None else None,
+            "relerr_per_rhs_max": max(per_rhs) if per_rhs else None,
+            "relerr_per_rhs": [round(e, 6) for e in per_rhs] if per_rhs else None,
+            "reached_target": bool(ref is not None and info["rel_error"] <= target), "target": target,
+            "gemv_path": {"ms_per_step": res[False][0], "iterations": res[False][1]["total_iters"],
+                          "relerr_vs_fp64": float(res[False][1]["rel_error"]) if ref is not None else None,
+                          "form": "same graph, FP64-accumulating gemv kernels, A read once per layer"},
+            "tensor_over_gemv": res[False][0] / ms,
+            "roofline": {"bound": "hbm", "kernel": "k_mrhs_split + k_mrhs<32> + k_mrhs_red (A X^T)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": profile_traffic("mrhs_tcgen05_4096x16384.md"), "algorithmic_bytes": bytes_,
+                         "ms_per_launch": k_ms, "adjoint_ms_per_launch": float(np.mean(zt)),
+                         "tensor_tflops": 3 * 2 * m * n * N / (k_ms * 1e-3) / 1e12, "peak_source": src,
+                         "timing": "one launch per CUDA-event pair, 256 MB L2 flush before each"},
+            "clocks": clk, "gpu_launches": launches}
+
+
 def batch_problems(capi, torch, dev):
     """Materialise the mixed batch: dense A drawn on the device (seeded),
     ring geometries and data on the host."""
@@ -494,6 +580,8 @@ def main():
     clocks = Clocks(local)
     if a.workload == "batch":
         line = run_batch(a, cx, capi, world, dist, clocks)
+    elif a.workload == "mrhs":
+        line = run_mrhs(a, cx, capi, world, dist, clocks)
     else:
         line = run_single(a, cx, capi, a.workload, world, rank, dist, clocks)
     if rank == 0 and line is not None:

@@ -1,12 +1,14 @@
-"""FP64 solution of the benchmark workload (bench.py), for its relerr check.
+"""FP64 solutions of the benchmark workloads (bench.py), for their relerr checks.
+
+    python tests/golden/make_bench_fixture.py [ring] [dense64] [mrhs]
 
 Solves the 256x256 ring workload (tval3g.workloads.ring2d with normalize=True,
 isotropic TV, maxit 500) with the FP64 oracle restatement and stores U and the
 iteration counts in tests/golden/ring256_fp64.npz.  Also records the
 reference's own float solver on the CSR twin of the same operator with
 anisotropic TV (the reference has no isotropic TV) for the drift statement.
-
-    python tests/golden/make_bench_fixture.py
+The dense 64x64 workload goes to dense64_fp64.npz and the joint 32-layer
+multi-RHS workload to mrhs32_fp64.npz.
 """
 import os
 import sys
@@ -45,7 +47,9 @@ def main():
         out["aniso_ref_f32_vs_fp64"] = np.array([d, rr.total_iters, r64.total_iters])
     np.savez_compressed(os.path.join(HERE, "ring256_fp64.npz"), **out)
 
-    # the plain dense 2D workload (64x64, 30 % sampling, isotropic TV)
+
+def dense64():
+    """The plain dense 2D workload (64x64, 30 % sampling, isotropic TV)."""
     w = W.dense2d(seed=0, side=64, sampling=0.3, tv_norm=1, maxit=300, tol=1e-4)
     r = O.solve(O.Op.dense(w["A"].astype(np.float64)), w["b"].astype(np.float64), w["shape"], w["opts"],
                 Ut=w["u_true"])
@@ -54,5 +58,24 @@ def main():
                         iters=np.array([r.outer_iters, r.total_iters]))
 
 
+def mrhs():
+    """The multi-right-hand-side workload (A 4096 x 16384, 32 phantoms of
+    128x128, solved jointly as 32 layers, isotropic TV)."""
+    w = W.mrhs()
+    t = time.time()
+    r = O.solve(O.Op.dense(w["A"].astype(np.float64), layers=w["layers"]), w["b"].astype(np.float64), w["shape"],
+                w["opts"], Ut=w["u_true"])
+    print(f"multi-RHS FP64 oracle: {r.total_iters} iterations, relerr to phantoms {r.rel_error:.4f}, "
+          f"{time.time() - t:.0f} s")
+    np.savez_compressed(os.path.join(HERE, "mrhs32_fp64.npz"), U=r.U.astype(np.float32),
+                        iters=np.array([r.outer_iters, r.total_iters]))
+
+
 if __name__ == "__main__":
-    main()
+    parts = sys.argv[1:] or ["ring", "dense64", "mrhs"]
+    if "ring" in parts:
+        main()
+    if "dense64" in parts:
+        dense64()
+    if "mrhs" in parts:
+        mrhs()

@@ -334,6 +334,22 @@ def ring2d(seed=1, side=256, T=512, receivers=None, noise=0.005, tv_norm=1, maxi
     return out
 
 
+def mrhs(seed=4, side=128, m=4096, rhs=32, noise=0.01, tv_norm=1, maxit=300, tol=1e-4):
+    """Multi-right-hand-side dense problem: one Gaussian A (m x side^2,
+    N(0, 1/m)) and `rhs` phantoms solved jointly as the reference's `layers`
+    (the layers stacked along y: image shape (side * rhs, side))."""
+    rng = np.random.default_rng(seed)
+    n = side * side
+    A = (rng.standard_normal((m, n), dtype=np.float32) / np.float32(math.sqrt(m))).astype(np.float32)
+    us = [ellipse_phantom(side, side, rng, 5, 0.0, lambda r: r.uniform(0.2, 1.0), (side / 16, side / 3.2))
+          for _ in range(rhs)]
+    U = np.stack([u.ravel() for u in us])                       # rhs x n
+    Y = (A.astype(np.float64) @ U.T).T                          # rhs x m
+    b = np.concatenate([add_noise(y, noise, rng) for y in Y])
+    return dict(kind="dense", shape=(side * rhs, side), A=A, b=b.astype(np.float32), u_true=U.reshape(side * rhs, side),
+                layers=rhs, opts=options(2 ** 8, 2 ** 5, tol, maxit, tv_norm=tv_norm))
+
+
 def batch_specs(seed=3, count=64, sides=(64, 96, 128, 192, 256)):
     """The mixed batch of independent 2D problems: per instance a side drawn
     from `sides`, and either a dense Gaussian A (sampling 25-40 %, drawn on
