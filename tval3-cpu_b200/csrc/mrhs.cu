@@ -16,13 +16,15 @@
 //
 // Work split (stream-K): the tiles x K-steps iterations are cut into G equal
 // contiguous ranges, one per CTA, G = min(number of SMs, iterations) (one
-// 320-thread CTA per SM, up to 194 KB of shared memory).  For every tile segment in its range a CTA
+// 448-thread CTA per SM, up to 226 KB of shared memory).  For every tile segment in its range a CTA
 // writes a 128 x N FP32 partial; k_mrhs_red adds each tile's partials in CTA
 // order in FP64, so the result does not depend on timing.
 //
 // Warp roles: warp 0 issues the TMA loads (one elected lane), warp 1 owns the
-// tensor memory and issues the MMAs (one lane), warps 2-5 split P tiles, warps
-// 6-9 drain the accumulators (warp w reads TMEM lanes 32 (w % 4) .. +31).
+// tensor memory and issues the MMAs (one lane), warps 2-9 split P tiles (the
+// high part in place, the low part into a ring of two buffers, so six TMA
+// stages stay in flight), warps 10-13 drain the accumulators (warp w reads
+// TMEM lanes 32 (w % 4) .. +31).
 // Two accumulators alternate between tile segments, so draining one overlaps
 // the MMAs into the other.  Every mbarrier wait is bounded: a timeout sets the
 // operator's error flag and ends the CTA's loops; the producer then waits
@@ -38,23 +40,27 @@ namespace {
 
 constexpr int BM = 128;           // rows per tile (MMA M = TMEM lanes)
 constexpr int BK = 32;            // K elements per stage: one 128-byte swizzle row of FP32
-constexpr int STAGES = 4;
-constexpr int THREADS = 320;
+constexpr int STAGES = 6;          // TMA stages (P tile + both Q tiles)
+constexpr int LO_BUFS = 2;         // ring of low-part P tiles
+constexpr int CONV_WARPS = 8;
+constexpr int THREADS = (2 + CONV_WARPS + 4) * 32;
 constexpr unsigned WAIT_LIMIT = 1u << 22;
 constexpr unsigned TF32_MASK = 0xFFFFE000u;
 
 __host__ __device__ constexpr int p_tile_bytes() { return BM * BK * 4; }
 __host__ __device__ constexpr int q_tile_bytes(int N) { return N * BK * 4; }
-__host__ __device__ constexpr int stage_bytes(int N) { return 2 * p_tile_bytes() + 2 * q_tile_bytes(N); }
+__host__ __device__ constexpr int stage_bytes(int N) { return p_tile_bytes() + 2 * q_tile_bytes(N); }
 __host__ __device__ constexpr int tmem_cols(int N) { return 2 * N <= 32 ? 32 : 2 * N <= 64 ? 64 : 128; }
 
 struct Bars {
-	unsigned long long full[STAGES], conv[STAGES], empty[STAGES], accf[2], acce[2], done;
+	unsigned long long full[STAGES], conv[STAGES], empty[STAGES], lofree[LO_BUFS], accf[2], acce[2], done;
 	unsigned tmem;
 	int abort;
 };
 
-size_t smem_bytes(int N) { return 1024 + (size_t)STAGES * stage_bytes(N) + sizeof(Bars); }
+size_t smem_bytes(int N) {
+	return 1024 + (size_t)STAGES * stage_bytes(N) + (size_t)LO_BUFS * p_tile_bytes() + sizeof(Bars);
+}
 
 // ---------------------------------------------------------------------------
 // PTX wrappers
@@ -206,15 +212,17 @@ __global__ void __launch_bounds__(THREADS, 1)
 	constexpr int SB = stage_bytes(N);
 	constexpr unsigned TX = (unsigned)(p_tile_bytes() + 2 * q_tile_bytes(N));
 	constexpr unsigned NCOLS = tmem_cols(N);
-	Bars *bars = reinterpret_cast<Bars *>(smem_raw + (base - raw) + STAGES * SB);
+	constexpr unsigned LO0 = STAGES * SB;   // low-part ring after the stages
+	Bars *bars = reinterpret_cast<Bars *>(smem_raw + (base - raw) + LO0 + LO_BUFS * p_tile_bytes());
 	volatile int *abort = &bars->abort;
 	auto st_p = [&](int s) { return base + s * SB; };
-	auto st_l = [&](int s) { return base + s * SB + p_tile_bytes(); };
-	auto st_qh = [&](int s) { return base + s * SB + 2 * p_tile_bytes(); };
-	auto st_ql = [&](int s) { return base + s * SB + 2 * p_tile_bytes() + q_tile_bytes(N); };
+	auto st_qh = [&](int s) { return base + s * SB + p_tile_bytes(); };
+	auto st_ql = [&](int s) { return base + s * SB + p_tile_bytes() + q_tile_bytes(N); };
+	auto lo_p = [&](int l) { return base + LO0 + l * p_tile_bytes(); };
 	const unsigned b_full = smem_u32(&bars->full[0]), b_conv = smem_u32(&bars->conv[0]),
-	               b_empty = smem_u32(&bars->empty[0]), b_accf = smem_u32(&bars->accf[0]),
-	               b_acce = smem_u32(&bars->acce[0]), b_done = smem_u32(&bars->done);
+	               b_empty = smem_u32(&bars->empty[0]), b_lofree = smem_u32(&bars->lofree[0]),
+	               b_accf = smem_u32(&bars->accf[0]), b_acce = smem_u32(&bars->acce[0]),
+	               b_done = smem_u32(&bars->done);
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
 	// this CTA's range of (tile, K step) iterations
@@ -226,9 +234,10 @@ __global__ void __launch_bounds__(THREADS, 1)
 	if (threadIdx.x == 0) {
 		for (int s = 0; s < STAGES; s++) {
 			mbar_init(b_full + 8 * s, 1);
-			mbar_init(b_conv + 8 * s, 4);
+			mbar_init(b_conv + 8 * s, CONV_WARPS);
 			mbar_init(b_empty + 8 * s, 1);
 		}
+		for (int l = 0; l < LO_BUFS; l++) mbar_init(b_lofree + 8 * l, 1);
 		for (int i = 0; i < 2; i++) {
 			mbar_init(b_accf + 8 * i, 1);
 			mbar_init(b_acce + 8 * i, 4);
@@ -283,16 +292,18 @@ __global__ void __launch_bounds__(THREADS, 1)
 						break;
 					}
 					tc_fence_after();
+					const int lb = it % LO_BUFS;
 #pragma unroll
 					for (int kk = 0; kk < BK / 8; kk++) {   // K = 8 per MMA: 32 bytes
 						const unsigned off = kk * 32;
-						const unsigned long long ph = sdesc(st_p(s) + off), pl = sdesc(st_l(s) + off);
+						const unsigned long long ph = sdesc(st_p(s) + off), pl = sdesc(lo_p(lb) + off);
 						const unsigned long long qh = sdesc(st_qh(s) + off), ql = sdesc(st_ql(s) + off);
 						mma_tf32(d, ph, qh, ID, (g > gb || kk > 0) ? 1u : 0u);
 						mma_tf32(d, ph, ql, ID, 1u);
 						mma_tf32(d, pl, qh, ID, 1u);
 					}
 					mma_commit(b_empty + 8 * s);
+					mma_commit(b_lofree + 8 * lb);
 				}
 				if (ok) mma_commit(b_accf + 8 * acc);
 			}
@@ -303,17 +314,18 @@ __global__ void __launch_bounds__(THREADS, 1)
 			}
 			if (i >= WAIT_LIMIT) atomicExch(a.err, 1);
 		}
-	} else if (warp < 6) {   // split P tiles into high and low parts
+	} else if (warp < 2 + CONV_WARPS) {   // split P tiles into high and low parts
 		const int t = threadIdx.x - 64;
 		unsigned it = 0;
 		for (long long g = it0; g < it1; g++, it++) {
-			const int s = it % STAGES;
+			const int s = it % STAGES, lb = it % LO_BUFS;
 			if (!wait_warp(b_full + 8 * s, (it / STAGES) & 1, abort, a.err)) break;
+			if (!wait_warp(b_lofree + 8 * lb, ((it / LO_BUFS) & 1) ^ 1, abort, a.err)) break;
 			float4 *P = reinterpret_cast<float4 *>(smem_raw + (st_p(s) - raw));
-			float4 *L = reinterpret_cast<float4 *>(smem_raw + (st_l(s) - raw));
+			float4 *L = reinterpret_cast<float4 *>(smem_raw + (lo_p(lb) - raw));
 #pragma unroll
-			for (int i = 0; i < p_tile_bytes() / 16 / 128; i++) {
-				const int idx = i * 128 + t;
+			for (int i = 0; i < p_tile_bytes() / 16 / (CONV_WARPS * 32); i++) {
+				const int idx = i * CONV_WARPS * 32 + t;
 				const float4 v = P[idx];
 				float4 h;
 				h.x = __uint_as_float(__float_as_uint(v.x) & TF32_MASK);
