@@ -12,8 +12,9 @@ from tval3g import workloads as W
 
 pytestmark = pytest.mark.gpu
 
-# (m, n, layers): ragged tile edges (300, 1000), long K (16384), wide N (64)
-SHAPES = [(256, 512, 16), (300, 1000, 32), (1024, 4096, 48), (4096, 2048, 64), (512, 16384, 32)]
+# (m, n, layers): ragged tile edges (300, 1000), long K (16384), wide N (64), and
+# the multi-RHS bench shape (4096 x 16384, 32 right-hand sides)
+SHAPES = [(256, 512, 16), (300, 1000, 32), (1024, 4096, 48), (4096, 2048, 64), (512, 16384, 32), (4096, 16384, 32)]
 PRODUCT_TOL = 1e-5   # per layer, relative L2 against the FP64 product
 
 

@@ -6,27 +6,33 @@
 // K = n) or P = A^T (adjoint: a transposed copy made once, M = n, K = m).
 // Both operands are K-major, so one kernel serves both directions.
 //
-// Split precision (3xTF32): P = Ph + Pl and Q = Qh + Ql with Ph = P with its
-// low 13 mantissa bits cleared (exactly representable in TF32) and Pl = P - Ph
-// (exact in FP32, TF32 keeps its top 11 bits); D = Ph Qh + Ph Ql + Pl Qh,
-// accumulated in FP32 in tensor memory; the Pl Ql term (relative size 2^-22)
-// is dropped.  Q is split once per product into two global arrays (a few MB,
-// L2-resident); each P tile is split in shared memory by four converter warps
+// Split precision (3xTF32): P = Ph + Pl and Q = Qh + Ql with Ph = P rounded
+// to the nearest TF32 value and Pl = P - Ph (exact in FP32, |Pl| <= 2^-11 |P|);
+// D = Ph Qh + Ph Ql + Pl Qh, the Pl Ql term (relative size 2^-22) dropped.
+// Qh and Ql are consecutive rows of one 2N-row operand, so each K slice takes
+// two MMAs: Ph [Qh; Ql] into 2N accumulator columns and Pl Qh into the first
+// N.  Q is split once per product into two global arrays (a few MB,
+// L2-resident); each P tile is split in shared memory by the converter warps
 // right after its TMA load, so A is read from HBM exactly once per product.
+//
+// Accumulation: the tensor cores' FP32 accumulation is not round-to-nearest,
+// and its error grows with the length of the MMA chain (2.5e-5 relative over
+// 110 stages at m = 4096, n = 16384, measured), so every stage (K = 32)
+// accumulates into a fresh TMEM buffer that the epilogue warps add into FP64
+// registers; two buffers alternate so the MMAs of stage i + 1 overlap the
+// drain of stage i.
 //
 // Work split (stream-K): the tiles x K-steps iterations are cut into G equal
 // contiguous ranges, one per CTA, G = min(number of SMs, iterations) (one
-// 448-thread CTA per SM, up to 226 KB of shared memory).  For every tile segment in its range a CTA
+// 320-thread CTA per SM, up to 226 KB of shared memory).  For every tile segment in its range a CTA
 // writes a 128 x N FP32 partial; k_mrhs_red adds each tile's partials in CTA
 // order in FP64, so the result does not depend on timing.
 //
 // Warp roles: warp 0 issues the TMA loads (one elected lane), warp 1 owns the
-// tensor memory and issues the MMAs (one lane), warps 2-9 split P tiles (the
+// tensor memory and issues the MMAs (one lane), warps 2-5 split P tiles (the
 // high part in place, the low part into a ring of two buffers, so six TMA
-// stages stay in flight), warps 10-13 drain the accumulators (warp w reads
-// TMEM lanes 32 (w % 4) .. +31).
-// Two accumulators alternate between tile segments, so draining one overlaps
-// the MMAs into the other.  Every mbarrier wait is bounded: a timeout sets the
+// stages stay in flight), warps 6-9 drain the accumulators (warp w reads
+// TMEM lanes 32 (w % 4) .. +31).  Every mbarrier wait is bounded: a timeout sets the
 // operator's error flag and ends the CTA's loops; the producer then waits
 // (bounded) for its loads in flight and the MMA lane for its MMAs before the
 // tensor memory is released.
@@ -42,7 +48,7 @@ constexpr int BM = 128;           // rows per tile (MMA M = TMEM lanes)
 constexpr int BK = 32;            // K elements per stage: one 128-byte swizzle row of FP32
 constexpr int STAGES = 6;          // TMA stages (P tile + both Q tiles)
 constexpr int LO_BUFS = 2;         // ring of low-part P tiles
-constexpr int CONV_WARPS = 8;
+constexpr int CONV_WARPS = 4;
 constexpr int THREADS = (2 + CONV_WARPS + 4) * 32;
 constexpr unsigned WAIT_LIMIT = 1u << 22;
 constexpr unsigned TF32_MASK = 0xFFFFE000u;
@@ -50,7 +56,8 @@ constexpr unsigned TF32_MASK = 0xFFFFE000u;
 __host__ __device__ constexpr int p_tile_bytes() { return BM * BK * 4; }
 __host__ __device__ constexpr int q_tile_bytes(int N) { return N * BK * 4; }
 __host__ __device__ constexpr int stage_bytes(int N) { return p_tile_bytes() + 2 * q_tile_bytes(N); }
-__host__ __device__ constexpr int tmem_cols(int N) { return 2 * N <= 32 ? 32 : 2 * N <= 64 ? 64 : 128; }
+// two accumulator buffers of 2N FP32 columns each, rounded up to a power of two
+__host__ __device__ constexpr int tmem_cols(int N) { return 4 * N <= 32 ? 32 : 4 * N <= 64 ? 64 : 4 * N <= 128 ? 128 : 256; }
 
 struct Bars {
 	unsigned long long full[STAGES], conv[STAGES], empty[STAGES], lofree[LO_BUFS], accf[2], acce[2], done;
@@ -147,6 +154,12 @@ __device__ __forceinline__ void tmem_wait_ld() {
 	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// nearest TF32 value (ties away from zero); exact in FP32, so P - tf32_rn(P)
+// is exact too and at most half a TF32 unit in the last place
+__device__ __forceinline__ float tf32_rn(float v) {
+	return __uint_as_float((__float_as_uint(v) + 0x1000u) & TF32_MASK);
+}
+
 // shared-memory matrix descriptor: K-major operand in the 128-byte swizzle
 // layout written by TMA (rows of 128 bytes, 8-row groups 1024 bytes apart)
 __device__ __forceinline__ unsigned long long sdesc(unsigned addr) {
@@ -229,7 +242,6 @@ __global__ void __launch_bounds__(THREADS, 1)
 	const long long G = gridDim.x;
 	const long long it0 = (long long)blockIdx.x * a.T / G, it1 = ((long long)blockIdx.x + 1) * a.T / G;
 	const int tile0 = (int)(it0 / a.ks);
-	const int nseg = (int)((it1 - 1) / a.ks) - tile0 + 1;
 
 	if (threadIdx.x == 0) {
 		for (int s = 0; s < STAGES; s++) {
@@ -274,38 +286,26 @@ __global__ void __launch_bounds__(THREADS, 1)
 			}
 		}
 	} else if (warp == 1) {
-		if (lane == 0) {   // MMA issuer
-			constexpr unsigned ID = idesc_tf32(N);
+		if (lane == 0) {   // MMA issuer: one stage into one accumulator buffer
+			constexpr unsigned ID2 = idesc_tf32(2 * N), ID1 = idesc_tf32(N);
 			unsigned it = 0;
-			bool ok = true;
-			for (int j = 0; j < nseg && ok; j++) {
-				const int acc = j & 1;
-				if (!wait1(b_acce + 8 * acc, ((j >> 1) & 1) ^ 1, abort, a.err)) break;
+			for (long long g = it0; g < it1; g++, it++) {
+				const int s = it % STAGES, lb = it % LO_BUFS, ab = it & 1;
+				if (!wait1(b_acce + 8 * ab, ((it >> 1) & 1) ^ 1, abort, a.err)) break;
+				if (!wait1(b_conv + 8 * s, (it / STAGES) & 1, abort, a.err)) break;
 				tc_fence_after();
-				const unsigned d = tmem + (unsigned)(acc * (NCOLS / 2));
-				const long long tb = (long long)(tile0 + j) * a.ks;
-				const long long gb = it0 > tb ? it0 : tb, ge = it1 < tb + a.ks ? it1 : tb + a.ks;
-				for (long long g = gb; g < ge; g++, it++) {
-					const int s = it % STAGES;
-					if (!wait1(b_conv + 8 * s, (it / STAGES) & 1, abort, a.err)) {
-						ok = false;
-						break;
-					}
-					tc_fence_after();
-					const int lb = it % LO_BUFS;
+				const unsigned d = tmem + (unsigned)(ab * 2 * N);
 #pragma unroll
-					for (int kk = 0; kk < BK / 8; kk++) {   // K = 8 per MMA: 32 bytes
-						const unsigned off = kk * 32;
-						const unsigned long long ph = sdesc(st_p(s) + off), pl = sdesc(lo_p(lb) + off);
-						const unsigned long long qh = sdesc(st_qh(s) + off), ql = sdesc(st_ql(s) + off);
-						mma_tf32(d, ph, qh, ID, (g > gb || kk > 0) ? 1u : 0u);
-						mma_tf32(d, ph, ql, ID, 1u);
-						mma_tf32(d, pl, qh, ID, 1u);
-					}
-					mma_commit(b_empty + 8 * s);
-					mma_commit(b_lofree + 8 * lb);
+				for (int kk = 0; kk < BK / 8; kk++) {   // K = 8 per MMA: 32 bytes
+					const unsigned off = kk * 32;
+					// columns [0, N): Ph Qh + Pl Qh; columns [N, 2N): Ph Ql (Qh and Ql
+					// are consecutive rows of one 2N-row operand)
+					mma_tf32(d, sdesc(st_p(s) + off), sdesc(st_qh(s) + off), ID2, kk > 0 ? 1u : 0u);
+					mma_tf32(d, sdesc(lo_p(lb) + off), sdesc(st_qh(s) + off), ID1, 1u);
 				}
-				if (ok) mma_commit(b_accf + 8 * acc);
+				mma_commit(b_empty + 8 * s);
+				mma_commit(b_lofree + 8 * lb);
+				mma_commit(b_accf + 8 * ab);
 			}
 			// every MMA issued has finished before the tensor memory is released
 			mma_commit(b_done);
@@ -327,11 +327,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 			for (int i = 0; i < p_tile_bytes() / 16 / (CONV_WARPS * 32); i++) {
 				const int idx = i * CONV_WARPS * 32 + t;
 				const float4 v = P[idx];
-				float4 h;
-				h.x = __uint_as_float(__float_as_uint(v.x) & TF32_MASK);
-				h.y = __uint_as_float(__float_as_uint(v.y) & TF32_MASK);
-				h.z = __uint_as_float(__float_as_uint(v.z) & TF32_MASK);
-				h.w = __uint_as_float(__float_as_uint(v.w) & TF32_MASK);
+				const float4 h = make_float4(tf32_rn(v.x), tf32_rn(v.y), tf32_rn(v.z), tf32_rn(v.w));
 				P[idx] = h;
 				L[idx] = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
 			}
@@ -339,26 +335,36 @@ __global__ void __launch_bounds__(THREADS, 1)
 			__syncwarp();
 			if (lane == 0) mbar_arrive(b_conv + 8 * s);
 		}
-	} else {   // epilogue: accumulator -> partial tile
+	} else {   // epilogue: every stage's accumulator is added in FP64 (short tensor-core chains)
 		const int q = warp & 3;
 		const int row = q * 32 + lane;
-		for (int j = 0; j < nseg; j++) {
-			const int acc = j & 1;
-			if (!wait_warp(b_accf + 8 * acc, (j >> 1) & 1, abort, a.err)) break;
-			tc_fence_after();
-			float v[N];
+		const unsigned lane_base = tmem + ((unsigned)(q * 32) << 16);
+		double acc[N];
+		unsigned it = 0;
+		for (long long g = it0; g < it1; g++, it++) {
+			const int tile = (int)(g / a.ks), k = (int)(g - (long long)tile * a.ks);
+			if (g == it0 || k == 0)
 #pragma unroll
-			for (int c = 0; c < N; c += 16)
-				tmem_ld16(tmem + ((unsigned)(q * 32) << 16) + (unsigned)(acc * (NCOLS / 2) + c), v + c);
-			tmem_wait_ld();
+				for (int c = 0; c < N; c++) acc[c] = 0.0;
+			const int ab = it & 1;
+			if (!wait_warp(b_accf + 8 * ab, (it >> 1) & 1, abort, a.err)) break;
+			tc_fence_after();
+#pragma unroll
+			for (int c = 0; c < N; c += 16) {
+				float lo[16], hi[16];
+				tmem_ld16(lane_base + (unsigned)(ab * 2 * N + c), lo);
+				tmem_ld16(lane_base + (unsigned)(ab * 2 * N + N + c), hi);
+				tmem_wait_ld();
+#pragma unroll
+				for (int e = 0; e < 16; e++) acc[c + e] += (double)lo[e] + (double)hi[e];
+			}
 			tc_fence_before();
 			__syncwarp();
-			if (lane == 0) mbar_arrive(b_acce + 8 * acc);
-			const int tile = tile0 + j;
-			if ((long long)tile * BM + row < a.M) {
-				float *dst = a.part + ((long long)blockIdx.x * a.J + j) * N * BM + row;
+			if (lane == 0) mbar_arrive(b_acce + 8 * ab);
+			if ((g == it1 - 1 || k == a.ks - 1) && (long long)tile * BM + row < a.M) {
+				float *dst = a.part + ((long long)blockIdx.x * a.J + (tile - tile0)) * N * BM + row;
 #pragma unroll
-				for (int c = 0; c < N; c++) dst[c * BM] = v[c];
+				for (int c = 0; c < N; c++) dst[c * BM] = (float)acc[c];
 			}
 		}
 	}
@@ -404,7 +410,7 @@ __global__ void __launch_bounds__(256) k_mrhs_split(const Inst *tab, int inst, i
 	const float *x = xs.m ? I.vm[xs.idx] : I.vn[xs.idx];
 	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x) {
 		const float v = x[i];
-		const float h = __uint_as_float(__float_as_uint(v) & TF32_MASK);
+		const float h = tf32_rn(v);
 		hi[i] = h;
 		lo[i] = v - h;
 	}
