@@ -19,20 +19,20 @@
 // and its error grows with the length of the MMA chain (2.5e-5 relative over
 // 110 stages at m = 4096, n = 16384, measured), so every stage (K = 32)
 // accumulates into a fresh TMEM buffer that the epilogue warps add into FP64
-// registers; two buffers alternate so the MMAs of stage i + 1 overlap the
-// drain of stage i.
+// registers; four buffers rotate so the MMAs of the next stages overlap the
+// drain of this one.
 //
 // Work split (stream-K): the tiles x K-steps iterations are cut into G equal
 // contiguous ranges, one per CTA, G = min(number of SMs, iterations) (one
-// 320-thread CTA per SM, up to 226 KB of shared memory).  For every tile segment in its range a CTA
+// 448-thread CTA per SM, up to 226 KB of shared memory).  For every tile segment in its range a CTA
 // writes a 128 x N FP32 partial; k_mrhs_red adds each tile's partials in CTA
 // order in FP64, so the result does not depend on timing.
 //
 // Warp roles: warp 0 issues the TMA loads (one elected lane), warp 1 owns the
 // tensor memory and issues the MMAs (one lane), warps 2-5 split P tiles (the
 // high part in place, the low part into a ring of two buffers, so six TMA
-// stages stay in flight), warps 6-9 drain the accumulators (warp w reads
-// TMEM lanes 32 (w % 4) .. +31).  Every mbarrier wait is bounded: a timeout sets the
+// stages stay in flight), warps 6-13 drain the accumulators (warp w reads
+// TMEM lanes 32 (w % 4) .. +31, half of the columns).  Every mbarrier wait is bounded: a timeout sets the
 // operator's error flag and ends the CTA's loops; the producer then waits
 // (bounded) for its loads in flight and the MMA lane for its MMAs before the
 // tensor memory is released.
@@ -49,18 +49,22 @@ constexpr int BK = 32;            // K elements per stage: one 128-byte swizzle 
 constexpr int STAGES = 6;          // TMA stages (P tile + both Q tiles)
 constexpr int LO_BUFS = 2;         // ring of low-part P tiles
 constexpr int CONV_WARPS = 4;
-constexpr int THREADS = (2 + CONV_WARPS + 4) * 32;
+constexpr int EPI_WARPS = 8;       // two per TMEM lane quarter, each half of the columns
+constexpr int ACC_BUFS = 4;        // TMEM accumulator buffers (one stage each)
+constexpr int THREADS = (2 + CONV_WARPS + EPI_WARPS) * 32;
 constexpr unsigned WAIT_LIMIT = 1u << 22;
 constexpr unsigned TF32_MASK = 0xFFFFE000u;
 
 __host__ __device__ constexpr int p_tile_bytes() { return BM * BK * 4; }
 __host__ __device__ constexpr int q_tile_bytes(int N) { return N * BK * 4; }
 __host__ __device__ constexpr int stage_bytes(int N) { return p_tile_bytes() + 2 * q_tile_bytes(N); }
-// two accumulator buffers of 2N FP32 columns each, rounded up to a power of two
-__host__ __device__ constexpr int tmem_cols(int N) { return 4 * N <= 32 ? 32 : 4 * N <= 64 ? 64 : 4 * N <= 128 ? 128 : 256; }
+// ACC_BUFS accumulator buffers of 2N FP32 columns each, rounded up to a power of two
+__host__ __device__ constexpr int tmem_cols(int N) {
+	return 2 * ACC_BUFS * N <= 128 ? 128 : 2 * ACC_BUFS * N <= 256 ? 256 : 512;
+}
 
 struct Bars {
-	unsigned long long full[STAGES], conv[STAGES], empty[STAGES], lofree[LO_BUFS], accf[2], acce[2], done;
+	unsigned long long full[STAGES], conv[STAGES], empty[STAGES], lofree[LO_BUFS], accf[ACC_BUFS], acce[ACC_BUFS], done;
 	unsigned tmem;
 	int abort;
 };
@@ -137,18 +141,15 @@ __device__ __forceinline__ void mma_commit(unsigned bar) {
 	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
 	             : "memory");
 }
-// 32 lanes x 16 consecutive FP32 columns: thread i gets lane (base + i)
-__device__ __forceinline__ void tmem_ld16(unsigned taddr, float *v) {
-	unsigned r[16];
-	asm volatile(
-	    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-	    "%15}, [%16];"
-	    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-	      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-	    : "r"(taddr)
-	    : "memory");
+// 32 lanes x 8 consecutive FP32 columns: thread i gets lane (base + i)
+__device__ __forceinline__ void tmem_ld8(unsigned taddr, float *v) {
+	unsigned r[8];
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+	             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+	             : "r"(taddr)
+	             : "memory");
 #pragma unroll
-	for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+	for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
 }
 __device__ __forceinline__ void tmem_wait_ld() {
 	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
@@ -250,9 +251,9 @@ __global__ void __launch_bounds__(THREADS, 1)
 			mbar_init(b_empty + 8 * s, 1);
 		}
 		for (int l = 0; l < LO_BUFS; l++) mbar_init(b_lofree + 8 * l, 1);
-		for (int i = 0; i < 2; i++) {
+		for (int i = 0; i < ACC_BUFS; i++) {
 			mbar_init(b_accf + 8 * i, 1);
-			mbar_init(b_acce + 8 * i, 4);
+			mbar_init(b_acce + 8 * i, EPI_WARPS);
 		}
 		mbar_init(b_done, 1);
 		bars->abort = 0;
@@ -290,8 +291,8 @@ __global__ void __launch_bounds__(THREADS, 1)
 			constexpr unsigned ID2 = idesc_tf32(2 * N), ID1 = idesc_tf32(N);
 			unsigned it = 0;
 			for (long long g = it0; g < it1; g++, it++) {
-				const int s = it % STAGES, lb = it % LO_BUFS, ab = it & 1;
-				if (!wait1(b_acce + 8 * ab, ((it >> 1) & 1) ^ 1, abort, a.err)) break;
+				const int s = it % STAGES, lb = it % LO_BUFS, ab = it % ACC_BUFS;
+				if (!wait1(b_acce + 8 * ab, ((it / ACC_BUFS) & 1) ^ 1, abort, a.err)) break;
 				if (!wait1(b_conv + 8 * s, (it / STAGES) & 1, abort, a.err)) break;
 				tc_fence_after();
 				const unsigned d = tmem + (unsigned)(ab * 2 * N);
@@ -336,35 +337,38 @@ __global__ void __launch_bounds__(THREADS, 1)
 			if (lane == 0) mbar_arrive(b_conv + 8 * s);
 		}
 	} else {   // epilogue: every stage's accumulator is added in FP64 (short tensor-core chains)
-		const int q = warp & 3;
+		constexpr int NH = N / 2;   // columns per epilogue warp
+		const int ew = warp - 2 - CONV_WARPS;
+		const int q = warp & 3, c0 = (ew >> 2) * NH;
 		const int row = q * 32 + lane;
 		const unsigned lane_base = tmem + ((unsigned)(q * 32) << 16);
-		double acc[N];
+		double acc[NH];
 		unsigned it = 0;
 		for (long long g = it0; g < it1; g++, it++) {
 			const int tile = (int)(g / a.ks), k = (int)(g - (long long)tile * a.ks);
 			if (g == it0 || k == 0)
 #pragma unroll
-				for (int c = 0; c < N; c++) acc[c] = 0.0;
-			const int ab = it & 1;
-			if (!wait_warp(b_accf + 8 * ab, (it >> 1) & 1, abort, a.err)) break;
+				for (int c = 0; c < NH; c++) acc[c] = 0.0;
+			const int ab = it % ACC_BUFS;
+			if (!wait_warp(b_accf + 8 * ab, (it / ACC_BUFS) & 1, abort, a.err)) break;
 			tc_fence_after();
 #pragma unroll
-			for (int c = 0; c < N; c += 16) {
-				float lo[16], hi[16];
-				tmem_ld16(lane_base + (unsigned)(ab * 2 * N + c), lo);
-				tmem_ld16(lane_base + (unsigned)(ab * 2 * N + N + c), hi);
+			for (int c = 0; c < NH; c += 8) {
+				float lo[8], hi[8];
+				tmem_ld8(lane_base + (unsigned)(ab * 2 * N + c0 + c), lo);
+				tmem_ld8(lane_base + (unsigned)(ab * 2 * N + N + c0 + c), hi);
 				tmem_wait_ld();
+				// Ph Ql (columns N..2N) is 2^-11 of the rest: one FP32 add, then FP64
 #pragma unroll
-				for (int e = 0; e < 16; e++) acc[c + e] += (double)lo[e] + (double)hi[e];
+				for (int e = 0; e < 8; e++) acc[c + e] += (double)(lo[e] + hi[e]);
 			}
 			tc_fence_before();
 			__syncwarp();
 			if (lane == 0) mbar_arrive(b_acce + 8 * ab);
 			if ((g == it1 - 1 || k == a.ks - 1) && (long long)tile * BM + row < a.M) {
-				float *dst = a.part + ((long long)blockIdx.x * a.J + (tile - tile0)) * N * BM + row;
+				float *dst = a.part + ((long long)blockIdx.x * a.J + (tile - tile0)) * N * BM + (long long)c0 * BM + row;
 #pragma unroll
-				for (int c = 0; c < N; c++) dst[c * BM] = (float)acc[c];
+				for (int c = 0; c < NH; c++) dst[c * BM] = (float)acc[c];
 			}
 		}
 	}
