@@ -12,6 +12,7 @@ namespace tval3g {
 
 struct MrhsOp {
 	// forward: D[m x N] = A[m x n] X[N x n]^T; adjoint: D[n x N] = At[n x m] R[N x m]^T
+	// (tm_a, tm_at: the tile-major copies as 2D arrays of 32 columns, one box per tile)
 	CUtensorMap tm_a, tm_at, tm_xh_f, tm_xl_f, tm_xh_a, tm_xl_a;
 	long long m = 0, n = 0;
 	int N = 0;                  // layers (right-hand sides)
@@ -20,7 +21,7 @@ struct MrhsOp {
 	int tiles_f = 0, tiles_a = 0;
 	int j_f = 0, j_a = 0;       // tile segments per CTA (partial slots)
 	long long t_f = 0, t_a = 0; // tiles x K steps
-	float *at = nullptr;        // A^T (n x m, row-major), owned
+	float *ta = nullptr, *tat = nullptr;   // A and A^T in tile-major order (128 x 32 tiles), owned
 	float *xh = nullptr, *xl = nullptr;   // split right-hand sides, N x max(m, n) each
 	float *part = nullptr;      // grid x J x N x 128 partial tiles
 	int *err = nullptr;         // device flag: a bounded wait timed out
