@@ -22,6 +22,8 @@
  *                       (2d/mat_mult.h:15-194, 3d/mat_mult.h:17-595)
  *   tval3g_D / _Dt      D / Dt (2d/tval3_cpu_2d.cpp:268-293, 3d/tval3_cpu_3d.cpp:365-425)
  *   tval3g_shrink       shrinkage (2d/tval3_cpu_2d.cpp:588-611, 3d/tval3_cpu_3d.cpp:834-871)
+ *   tval3g_unrolled_*   no reference counterpart: gradients of an unrolled K-iteration
+ *                       solve (2d/tval3_cpu_2d.cpp:752-853 with decisions held fixed)
  */
 #ifndef TVAL3G_H_
 #define TVAL3G_H_
@@ -60,10 +62,13 @@ extern "C" {
 
 /* Per inner iteration: step length, objective after update_W, relative
  * change, backtracking steps taken (6 = restart after five failures), whether
- * the A^T multiplication was skipped (skipMulRatio heuristic) and, when the
- * solve was given Ut, ||U/scl - Ut|| / ||Ut|| after the iteration (else 0). */
+ * the A^T multiplication was skipped (skipMulRatio heuristic), when the
+ * solve was given Ut, ||U/scl - Ut|| / ||Ut|| after the iteration (else 0),
+ * the step actually taken (U = U_prev - step * d: tau times the backtracking
+ * factor, or the restart's tau) and whether the multipliers were updated
+ * after the iteration (1) or not (0). */
 typedef struct tval3g_trace_record {
-	double tau, f, relchg, backtracks, skipped, relerr_ut;
+	double tau, f, relchg, backtracks, skipped, relerr_ut, step, outer;
 } tval3g_trace_record;
 
 /* Options; field meaning as tval3_options<T> (include/tval3/tval3_types.h). */
@@ -181,6 +186,29 @@ int tval3g_Dt(int dims, int dim_y, int dim_x, int dim_z, const float *X, const f
 int tval3g_shrink(int dims, long long n, int tv_norm, double beta, const float *Ux, const float *Uy,
                   const float *Uz, const float *sx, const float *sy, const float *sz, float *Wx,
                   float *Wy, float *Wz, double *lam1, void *stream);
+
+/* Differentiable unrolled solve (2D, one layer, no nonnegativity).  No
+ * counterpart in the reference.  `count` instances share the operator of
+ * `prob` and the options; the solve runs exactly K inner iterations with
+ * per-iteration (mu_k, beta_k) instead of the continuation.  The forward
+ * records, per instance and iteration, the step taken (BB step length times
+ * the Armijo backtracking factor) and whether the multipliers were updated,
+ * then replays the iteration map with those decisions held fixed, keeping a
+ * checkpoint every `ckpt` iterations; U = U_K / scl (DEVICE, count x n).
+ * The backward gives, for DEVICE cotangents gU (count x n), the gradients of
+ * sum_i <gU_i, U_i>: gb (DEVICE, count x m) and g_mu, g_beta (HOST, K each,
+ * summed over the instances), recomputing each segment from its checkpoint.
+ * d_b / d_U / d_gU / d_gb are arrays of `count` device pointers. */
+typedef struct tval3g_unrolled tval3g_unrolled;
+int tval3g_unrolled_create(tval3g_unrolled **h, const tval3g_problem *prob, int count,
+                           const tval3g_options *opts, int K, int ckpt);
+int tval3g_unrolled_forward(tval3g_unrolled *h, const float *const *d_b, const double *mu,
+                            const double *beta, float *const *d_U, void *stream);
+int tval3g_unrolled_backward(tval3g_unrolled *h, const float *const *d_gU, float *const *d_gb,
+                             double *g_mu, double *g_beta, void *stream);
+/* the recorded decisions of instance `index`: steps[K], outer[K], scl */
+int tval3g_unrolled_decisions(const tval3g_unrolled *h, int index, double *steps, int *outer, double *scl);
+int tval3g_unrolled_destroy(tval3g_unrolled *h);
 
 /* y = A^T x for a dense row-major m x n float matrix, with DEVICE pointers,
  * for callers that cannot allocate device memory at call time (for example

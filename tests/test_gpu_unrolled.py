@@ -1,0 +1,85 @@
+"""Differentiable unrolled solve on the GPU (tval3g_unrolled_*): the forward
+against the FP64 oracle with the recorded decisions, the hand-written CUDA
+adjoint against the oracle's adjoint and against FP64 central finite
+differences, and the torch.autograd binding."""
+import numpy as np
+import pytest
+
+import oracle as O
+import unrolled as UR
+from helpers import relerr
+from tval3g import capi
+from tval3g import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FWD_TOL = 1e-4      # U_K (FP32 replay) against the FP64 oracle, relative L2
+GRAD_TOL = 1e-3     # gradients (FP32 forward and adjoint) against the FP64 adjoint, relative L2
+FD_TOL = 1e-3       # directional derivatives against FP64 central differences
+
+
+def _batch(side, T, count, iso, seed=11):
+    ws = [W.ring2d(seed=seed + i, side=side, T=T, tv_norm=int(iso), normalize=True) for i in range(count)]
+    g = ws[0]["geom"]
+    b = np.stack([w["b"] for w in ws]).astype(np.float32)
+    u = np.stack([w["u_true"].ravel() for w in ws])
+    return g, b, u
+
+
+def _schedule(K):
+    k = np.arange(K)
+    return 2.0 ** 8 * (1 + 0.2 * np.sin(k)), 2.0 ** 5 * (1 + 0.2 * np.cos(k))
+
+
+@pytest.mark.parametrize("iso", [False, True])
+def test_unrolled_forward_and_adjoint(iso, torch_cuda):
+    torch = torch_cuda
+    from tval3g.autograd import unrolled_tval3
+    side, T, count, K = 32, 32, 3, 20
+    g, b, u = _batch(side, T, count, iso)
+    spec = capi.ray2d_problem((side, side), g)
+    opts = W.options(2 ** 8, 2 ** 5, 1e-4, K, tv_norm=int(iso))
+    h = capi.Unrolled(spec, count, opts, K, ckpt=6)
+    mu, beta = _schedule(K)
+    tb = torch.tensor(b, device="cuda", requires_grad=True)
+    tm = torch.tensor(mu, requires_grad=True)
+    tB = torch.tensor(beta, requires_grad=True)
+    U = unrolled_tval3(tb, tm, tB, h)
+    loss = 0.5 * ((U - torch.tensor(u, device="cuda", dtype=torch.float32)) ** 2).sum()
+    loss.backward()
+    Ug = U.detach().cpu().numpy()
+    gb = tb.grad.cpu().numpy()
+
+    op = O.Op.ray2d(g, side * side)
+    A, At = (lambda x: op.apply(x)), (lambda y: op.apply(y, True))
+    gmu_ref, gbeta_ref = np.zeros(K), np.zeros(K)
+    Fs = []
+    for i in range(count):
+        steps, outer, scl = h.decisions(i)
+        assert np.all(steps > 0) and not outer[-1]
+        F = UR.Unrolled(A, At, (side, side), steps, outer, scl, iso)
+        Fs.append(F)
+        U64 = F.forward(b[i], mu, beta)
+        assert relerr(Ug[i], U64) <= FWD_TOL
+        gb_i, gm_i, gB_i = F.backward(b[i], mu, beta, U64 - u[i])
+        assert relerr(gb[i], gb_i) <= GRAD_TOL
+        gmu_ref += gm_i
+        gbeta_ref += gB_i
+    assert relerr(tm.grad.numpy(), gmu_ref) <= GRAD_TOL
+    assert relerr(tB.grad.numpy(), gbeta_ref) <= GRAD_TOL
+
+    # directional derivatives against central differences of the FP64 map
+    rng = np.random.default_rng(5)
+
+    def L(db, fm, fB):
+        return sum(0.5 * np.sum((F.forward(b[i] + db[i], mu * fm, beta * fB) - u[i]) ** 2) for i, F in enumerate(Fs))
+
+    hstep, sb = 1e-6, np.abs(b).mean()
+    for _ in range(16):
+        vb = rng.standard_normal(b.shape)
+        vm, vB = rng.standard_normal(K), rng.standard_normal(K)
+        fd = (L(hstep * sb * vb, 1 + hstep * vm, 1 + hstep * vB) - L(-hstep * sb * vb, 1 - hstep * vm, 1 - hstep * vB)) \
+            / (2 * hstep)
+        an = sb * np.sum(gb * vb) + np.dot(tm.grad.numpy(), mu * vm) + np.dot(tB.grad.numpy(), beta * vB)
+        assert abs(fd - an) <= FD_TOL * abs(fd), (fd, an)
+    h.close()

@@ -62,6 +62,8 @@ struct Ctrl {
 	double currSkip;
 	double rel_error;
 	double relerr_ut;            // last |U/scl - Ut| / |Ut| (target mode)
+	double step;                 // step of the last descent: U = Up - step * d
+	double sched_ratio;          // schedule mode: beta of the last iteration / beta of this one
 	int currInit;
 	int count_outer, count_total;
 	int fst, active, need_bt, bt_cnt, restart, inner_break, need_mlp, need_Ad, skip_adj;
@@ -173,6 +175,7 @@ struct Inst {
 	double muf, betaf, mu0, beta0, tol, tol_inn, c, gamma, gam0, rate_gam, rate_cnt;
 	double skipRatio, maxRelChange;
 	double target;               // > 0: also stop once |U/scl - Ut| <= target |Ut|
+	const double *sched;         // schedule mode: mu_1..mu_maxit, beta_1..beta_maxit (device), or NULL
 	int maxit, maxcnt, nonneg, tv_norm, numInit, skip_enabled;
 	OpDev op;
 };

@@ -200,6 +200,8 @@ __global__ void __launch_bounds__(BLOCK) k_init(KArgs a) {
 			c.mu = I.mu0; c.beta = I.beta0;
 			if (c.mu > I.muf) c.mu = I.muf;
 			if (c.beta > I.betaf) c.beta = I.betaf;
+			if (I.sched) { c.mu = I.sched[0]; c.beta = I.sched[I.maxit]; }   // (mu_1, beta_1)
+			c.step = 0; c.sched_ratio = 1;
 			c.muDbeta = c.mu / c.beta;
 			c.gam = I.gam0; c.Q = 1; c.C = 0; c.f = 0;
 			c.lam1 = c.lam2 = c.lam3 = c.lam4 = c.lam5 = 0;
@@ -343,6 +345,7 @@ __global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
 	if (threadIdx.x != 0) return;
 	c.lam2 = tot[0]; c.lam4 = tot[1]; c.lam3 = tot[2]; c.lam5 = tot[3];
 	c.f = (c.lam1 + c.beta / 2 * c.lam2 + c.mu / 2 * c.lam3) - c.lam4 - c.lam5;
+	if (a.stage == ST_DESCEND || a.stage == ST_RESTART) c.step = c.tau;
 	if (a.stage == ST_DESCEND) {
 		c.alpha = 1;
 		c.c_armij = c.dd * c.tau * I.c * c.beta;
@@ -413,6 +416,7 @@ __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 		if (I.trace && c.count_total <= I.maxit) {
 			double *t = I.trace + (long long)(c.count_total - 1) * TRACE_DOUBLES;
 			t[0] = c.tau; t[1] = c.f; t[2] = c.relchg; t[3] = c.bt_cnt; t[4] = c.skip_adj; t[5] = c.relerr_ut;
+			t[6] = c.step; t[7] = 0;
 		}
 		c.bt_cnt = 0;
 		bool brk = (c.relchg < I.tol_inn) && !c.fst;
@@ -512,6 +516,7 @@ __global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
 	Ctrl &c = *I.ctrl;
 	const float ntau = (float)(-1 * c.tau);
 	const bool snap = a.stage == ST_DESCEND;
+	const float sratio = (float)c.sched_ratio;
 	if (local < I.ntn) {
 		float *__restrict__ U = I.vn[vU], *__restrict__ Up = I.vn[vUp];
 		const float *__restrict__ d = I.vn[vD];
@@ -525,6 +530,8 @@ __global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
 #pragma unroll
 				for (int cc = 0; cc < 3; cc++)
 					if (cc < I.dims) I.vn[vUxp + cc][i] = I.vn[vUx + cc][i];
+				// schedule mode: DtsAtd = -(Dt sigma + At delta) / beta for this iteration's beta
+				if (I.sched) I.vn[vDts][i] *= sratio;
 			} else {
 				u = Up[i];
 			}
@@ -589,6 +596,7 @@ __global__ void __launch_bounds__(BLOCK) k_lerp(KArgs a) {
 	if (!tile_reduce<4>(I, local, I.ntn + I.ntm, v, tot)) return;
 	if (threadIdx.x != 0) return;
 	c.alpha = alpha_new;
+	c.step = c.tau * alpha_new;
 	c.bt_cnt++;
 	c.lam2 = tot[0]; c.lam4 = tot[1]; c.lam3 = tot[2]; c.lam5 = tot[3];
 	c.f = c.lam1 + c.beta / 2 * c.lam2 + c.mu / 2 * c.lam3 - c.lam4 - c.lam5;
@@ -625,6 +633,8 @@ __global__ void __launch_bounds__(BLOCK) k_outer(KArgs a) {
 	// which no longer changes U; that step is skipped here
 	if (c.relchg_out < I.tol || c.count_outer >= I.maxcnt || c.count_total >= I.maxit) c.active = 0;
 	else c.need_mlp = 1;
+	if (I.trace && c.count_total >= 1 && c.count_total <= I.maxit)
+		I.trace[(long long)(c.count_total - 1) * TRACE_DOUBLES + 7] = c.need_mlp;
 }
 
 // update_mlp (2d:673-694) and the continuation step (2d:834-842)
@@ -659,10 +669,12 @@ __global__ void __launch_bounds__(BLOCK) k_mlp(KArgs a) {
 	c.lam4 = tot[0]; c.lam5 = tot[1];
 	c.f -= (c.lam4 + c.lam5);
 	c.beta0 = c.beta;
-	c.beta *= I.rate_cnt;
-	c.mu *= I.rate_cnt;
-	if (c.beta > I.betaf) c.beta = I.betaf;
-	if (c.mu > I.muf) c.mu = I.muf;
+	if (!I.sched) {   // schedule mode: mu and beta come from the schedule
+		c.beta *= I.rate_cnt;
+		c.mu *= I.rate_cnt;
+		if (c.beta > I.betaf) c.beta = I.betaf;
+		if (c.mu > I.muf) c.mu = I.muf;
+	}
 	c.muDbeta = c.mu / c.beta;
 	c.f = c.lam1 + c.beta / 2 * c.lam2 + c.mu / 2 * c.lam3 - c.lam4 - c.lam5;
 }
@@ -729,6 +741,24 @@ __global__ void k_cond(const Inst *tab, int count, int pred, int *flag, unsigned
 		*flag = any;
 		if (handle) cudaGraphSetConditional((cudaGraphConditionalHandle)handle, any ? 1u : 0u);
 	}
+}
+
+// schedule mode: the coming iteration's (mu_k, beta_k) from the schedule, and
+// the ratio by which DtsAtd = -(Dt sigma + At delta) / beta must be rescaled
+__global__ void k_sched(const Inst *tab, int count, unsigned long long *launches) {
+	if (launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= count) return;
+	const Inst &I = tab[i];
+	Ctrl &c = *I.ctrl;
+	if (!I.sched || !c.active) return;
+	const int k = c.count_total;   // iterations done: the coming one is k + 1
+	if (k >= I.maxit) return;
+	const double mu = I.sched[k], beta = I.sched[I.maxit + k];
+	c.sched_ratio = c.beta / beta;
+	c.mu = mu;
+	c.beta = beta;
+	c.muDbeta = mu / beta;
 }
 
 // ---------------------------------------------------------------------------
@@ -815,6 +845,11 @@ LAUNCHER(launch_mlp, k_mlp)
 LAUNCHER(launch_final, k_final)
 LAUNCHER(launch_skip_norms, k_skip_norms)
 LAUNCHER(launch_copy_lastau, k_copy_lastau)
+
+void launch_sched(cudaStream_t s, const Inst *tab, int count, unsigned long long *launches) {
+	k_sched<<<(count + 127) / 128, 128, 0, s>>>(tab, count, launches);
+	TG_CUDA(cudaGetLastError());
+}
 
 void launch_cond(cudaStream_t s, const Inst *tab, int count, int pred, int *flag, unsigned long long handle,
                  unsigned long long *launches) {

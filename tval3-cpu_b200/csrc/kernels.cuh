@@ -37,6 +37,8 @@ void launch_mlp(cudaStream_t s, const KArgs &a);
 void launch_final(cudaStream_t s, const KArgs &a);
 void launch_skip_norms(cudaStream_t s, const KArgs &a);
 void launch_copy_lastau(cudaStream_t s, const KArgs &a);
+// schedule mode: set (mu_k, beta_k) of the coming iteration (instances with a schedule)
+void launch_sched(cudaStream_t s, const Inst *tab, int count, unsigned long long *launches);
 // any instance with pred true -> *flag (device) and the graph conditional
 void launch_cond(cudaStream_t s, const Inst *tab, int count, int pred, int *flag,
                  unsigned long long handle, unsigned long long *launches);

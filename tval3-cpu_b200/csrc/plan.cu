@@ -463,6 +463,18 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 		d_part_ = (double *)dalloc(sizeof(double) * (size_t)parts);
 		d_ctrl_ = (Ctrl *)dalloc(sizeof(Ctrl) * count);
 		TG_CUDA(cudaMemsetAsync(d_ctrl_, 0, sizeof(Ctrl) * count, stream_));
+		if (flags & PLAN_SCHEDULE) {
+			const int K = h_inst_[0].maxit;
+			for (int i = 0; i < count; i++)
+				TG_ARG(h_inst_[i].maxit == K && K >= 1, "Argument error: a schedule needs one maxit >= 1");
+			sched_mode_ = true;
+			d_sched_ = (double *)dalloc(sizeof(double) * 2 * (size_t)K);
+			std::vector<double> def(2 * (size_t)K);
+			for (int k = 0; k < K; k++) { def[k] = h_inst_[0].mu0; def[K + k] = h_inst_[0].beta0; }
+			TG_CUDA(cudaMemcpyAsync(d_sched_, def.data(), sizeof(double) * def.size(), cudaMemcpyHostToDevice, stream_));
+			TG_CUDA(cudaStreamSynchronize(stream_));
+			for (int i = 0; i < count; i++) h_inst_[i].sched = d_sched_;
+		}
 		if (flags & TVAL3G_TRACE) {
 			long long recs = 0;
 			for (int i = 0; i < count; i++) {
@@ -670,9 +682,28 @@ void Plan::emit_program() {
 	launch_final(es(), kargs(MAP_N, P_ALL));
 }
 
+std::vector<Ctrl> Plan::ctrl() const {
+	std::vector<Ctrl> h(count_);
+	TG_CUDA(cudaMemcpy(h.data(), d_ctrl_, sizeof(Ctrl) * count_, cudaMemcpyDeviceToHost));
+	return h;
+}
+
+void Plan::set_schedule(const double *mu, const double *beta) {
+	TG_ARG(sched_mode_, "Internal error: the plan has no schedule");
+	const int K = h_inst_[0].maxit;
+	std::vector<double> h(2 * (size_t)K);
+	for (int k = 0; k < K; k++) {
+		TG_ARG(mu[k] > 0 && beta[k] > 0, "Argument error: mu_k and beta_k must be positive");
+		h[k] = mu[k];
+		h[K + k] = beta[k];
+	}
+	TG_CUDA(cudaMemcpy(d_sched_, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+}
+
 void Plan::emit_iteration() {
 	const LaunchCtx L = lctx();
 	cudaStream_t s = es();
+	if (sched_mode_) launch_sched(s, d_inst_, count_, d_launches_);
 	const VecSel U{false, vU}, G{false, vG}, D{false, vD};
 	const VecSel Au{true, vAu}, Ad{true, vAd};
 	// min_u (2d:526-576): step length

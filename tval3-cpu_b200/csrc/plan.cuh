@@ -35,6 +35,10 @@ void check_options(const tval3g_options &o);
 long long build_op_maps_upload(std::vector<Inst> &inst, const std::vector<OpStore> &ops, OpBatch &ob,
                                int2 **d_tiles, cudaStream_t s);
 
+// internal plan flag: per-iteration (mu_k, beta_k) from set_schedule instead of
+// the continuation (every instance must have the same maxit)
+constexpr int PLAN_SCHEDULE = 1 << 16;
+
 class Plan {
 public:
 	Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, int flags);
@@ -47,6 +51,11 @@ public:
 		for (auto &I : h_inst_) I.target = target;
 	}
 	long long device_bytes() const { return device_bytes_; }
+	// schedule mode: mu[0..maxit), beta[0..maxit) (host) for the next solves
+	void set_schedule(const double *mu, const double *beta);
+	int maxit() const { return h_inst_.empty() ? 0 : h_inst_[0].maxit; }
+	// the instances' scalar state after the last solve
+	std::vector<Ctrl> ctrl() const;
 
 private:
 	struct Frame {
@@ -57,6 +66,8 @@ private:
 	int flags_;
 	bool graph_mode_;
 	bool any_skip_ = false;
+	bool sched_mode_ = false;
+	double *d_sched_ = nullptr;
 	cudaStream_t stream_ = nullptr;   // the plan's own stream
 	cudaStream_t cur_ = nullptr;      // stream of the solve in progress
 	std::vector<OpStore> ops_;

@@ -94,6 +94,11 @@ def lib():
         L.tval3g_D.argtypes = [i, i, i, i, vp, vp, vp, vp, vp]
         L.tval3g_Dt.argtypes = [i, i, i, i, vp, vp, vp, vp, vp]
         L.tval3g_shrink.argtypes = [i, ll, i, d, vp, vp, vp, vp, vp, vp, vp, vp, vp, C.POINTER(d), vp]
+        L.tval3g_unrolled_create.argtypes = [C.POINTER(vp), P, i, O, i, i]
+        L.tval3g_unrolled_forward.argtypes = [vp, C.POINTER(vp), C.POINTER(d), C.POINTER(d), C.POINTER(vp), vp]
+        L.tval3g_unrolled_backward.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(d), C.POINTER(d), vp]
+        L.tval3g_unrolled_decisions.argtypes = [vp, i, C.POINTER(d), C.POINTER(i), C.POINTER(d)]
+        L.tval3g_unrolled_destroy.argtypes = [vp]
         _LIB = L
     return _LIB
 
@@ -106,7 +111,9 @@ def _check(rc):
 EXPORTS = ("tval3g_last_error", "tval3g_version", "tval3g_solve", "tval3g_solve_batch", "tval3g_plan_create",
            "tval3g_plan_solve", "tval3g_plan_stats", "tval3g_plan_trace", "tval3g_plan_set_target",
            "tval3g_plan_destroy", "tval3g_op_create", "tval3g_op_shape",
-           "tval3g_op_apply", "tval3g_op_apply_n", "tval3g_op_ray_csr", "tval3g_op_destroy", "tval3g_D", "tval3g_Dt", "tval3g_shrink")
+           "tval3g_op_apply", "tval3g_op_apply_n", "tval3g_op_ray_csr", "tval3g_op_destroy", "tval3g_D", "tval3g_Dt",
+           "tval3g_shrink", "tval3g_unrolled_create", "tval3g_unrolled_forward", "tval3g_unrolled_backward",
+           "tval3g_unrolled_decisions", "tval3g_unrolled_destroy")
 
 
 # --------------------------------------------------------------------------
@@ -270,12 +277,12 @@ class Plan:
         return {"kernel_launches": a.value, "device_bytes": b.value}
 
     def trace(self, index=0):
-        """Per inner iteration records (tau, f, relchg, backtracks, skipped, relerr_ut)."""
+        """Per inner iteration records (tau, f, relchg, backtracks, skipped, relerr_ut, step, outer)."""
         cap = max(self.maxit[index], 1)
-        buf = (C.c_double * (6 * cap))()
+        buf = (C.c_double * (8 * cap))()
         cnt = C.c_int()
         _check(lib().tval3g_plan_trace(self.h, index, buf, cap, C.byref(cnt)))
-        return np.array(buf[:6 * cnt.value]).reshape(cnt.value, 6)
+        return np.array(buf[:8 * cnt.value]).reshape(cnt.value, 8)
 
     def set_target(self, target):
         """Time-to-solution mode: also stop once |U - Ut| <= target |Ut|."""
@@ -349,3 +356,53 @@ def shrink(dims, n, tv_norm, beta, U, S, W):
     _check(lib().tval3g_shrink(dims, n, tv_norm, beta, _dptr(U[0]), _dptr(U[1]), _dptr(Uz), _dptr(S[0]),
                                _dptr(S[1]), _dptr(Sz), _dptr(W[0]), _dptr(W[1]), _dptr(Wz), C.byref(lam), None))
     return lam.value
+
+
+class Unrolled:
+    """Differentiable unrolled solve (tval3g_unrolled_*): `count` instances of
+    one 2D problem, K inner iterations with per-iteration (mu_k, beta_k)."""
+
+    def __init__(self, spec: ProblemSpec, count, opts: dict, K, ckpt=10):
+        h = C.c_void_p()
+        _check(lib().tval3g_unrolled_create(C.byref(h), C.byref(spec.p), int(count), C.byref(Options.from_dict(opts)),
+                                            int(K), int(ckpt)))
+        self.h, self.count, self.K, self.spec = h, int(count), int(K), spec
+
+    def forward(self, d_b, mu, beta, d_U, stream=None):
+        """d_b, d_U: sequences of `count` device tensors; mu, beta: K floats."""
+        n = self.count
+        mu = np.ascontiguousarray(mu, np.float64)
+        beta = np.ascontiguousarray(beta, np.float64)
+        bp = (C.c_void_p * n)(*[_dptr(x) for x in d_b])
+        up = (C.c_void_p * n)(*[_dptr(x) for x in d_U])
+        _check(lib().tval3g_unrolled_forward(self.h, bp, mu.ctypes.data_as(C.POINTER(C.c_double)),
+                                             beta.ctypes.data_as(C.POINTER(C.c_double)), up, _dptr(stream)))
+
+    def backward(self, d_gU, d_gb, stream=None):
+        """Returns (g_mu, g_beta) as numpy arrays; gb is written to d_gb."""
+        n = self.count
+        gp = (C.c_void_p * n)(*[_dptr(x) for x in d_gU])
+        bp = (C.c_void_p * n)(*[_dptr(x) for x in d_gb])
+        gmu, gbeta = np.zeros(self.K), np.zeros(self.K)
+        _check(lib().tval3g_unrolled_backward(self.h, gp, bp, gmu.ctypes.data_as(C.POINTER(C.c_double)),
+                                              gbeta.ctypes.data_as(C.POINTER(C.c_double)), _dptr(stream)))
+        return gmu, gbeta
+
+    def decisions(self, index):
+        steps = np.zeros(self.K)
+        outer = np.zeros(self.K, np.int32)
+        scl = C.c_double()
+        _check(lib().tval3g_unrolled_decisions(self.h, int(index), steps.ctypes.data_as(C.POINTER(C.c_double)),
+                                               outer.ctypes.data_as(C.POINTER(C.c_int)), C.byref(scl)))
+        return steps, outer.astype(bool), scl.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().tval3g_unrolled_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
