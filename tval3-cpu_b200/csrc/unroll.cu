@@ -249,6 +249,10 @@ private:
 	long long n_, m_;
 	Plan *plan_ = nullptr;
 	tval3g_operator *op_ = nullptr;
+	// used when the caller passes the legacy default stream: blocking, so it
+	// is ordered with that stream's work on both sides, and every launch
+	// here (and the operator's) goes to one stream
+	cudaStream_t own_ = nullptr;
 	std::vector<UnrolledInst> in_;
 	std::vector<double> mu_, beta_;
 	std::vector<float *> eng_u_;       // the engine's U (decisions only)
@@ -294,6 +298,7 @@ Unrolled::Unrolled(const tval3g_problem &p, int count, const tval3g_options &o, 
 	std::vector<tval3g_problem> probs(count, p);
 	std::vector<tval3g_options> opts(count, oo);
 	try {
+		TG_CUDA(cudaStreamCreate(&own_));
 		plan_ = new Plan(count, probs.data(), opts.data(), TVAL3G_GRAPH | TVAL3G_TRACE | PLAN_SCHEDULE);
 		int rc = tval3g_op_create(&op_, &p, 0);
 		if (rc != TVAL3G_OK) throw Error{rc, tval3g_last_error()};
@@ -344,6 +349,8 @@ void Unrolled::release() {
 	op_ = nullptr;
 	delete plan_;
 	plan_ = nullptr;
+	if (own_) cudaStreamDestroy(own_);
+	own_ = nullptr;
 }
 
 void Unrolled::apply(bool trans, const float *x, float *y, cudaStream_t s) {
@@ -403,6 +410,7 @@ void Unrolled::replay_from(int i, int k0, int k1, cudaStream_t s, bool store_seg
 
 void Unrolled::forward(const float *const *d_b, const double *mu, const double *beta, float *const *d_U,
                        cudaStream_t s) {
+	if (!s) s = own_;
 	mu_.assign(mu, mu + K_);
 	beta_.assign(beta, beta + K_);
 	// the solve that records the decisions
@@ -441,6 +449,7 @@ void Unrolled::forward(const float *const *d_b, const double *mu, const double *
 
 void Unrolled::backward(const float *const *d_gU, float *const *d_gb, double *g_mu, double *g_beta, cudaStream_t s) {
 	TG_ARG(!mu_.empty(), "Argument error: backward before forward");
+	if (!s) s = own_;
 	TG_CUDA(cudaMemsetAsync(gsc_, 0, sizeof(double) * 2 * (size_t)K_, s));
 	const size_t nb = sizeof(float) * (size_t)n_, mb = sizeof(float) * (size_t)m_;
 	for (int i = 0; i < count_; i++) {
