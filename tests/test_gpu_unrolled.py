@@ -31,16 +31,12 @@ def _schedule(K):
     return 2.0 ** 8 * (1 + 0.2 * np.sin(k)), 2.0 ** 5 * (1 + 0.2 * np.cos(k))
 
 
-@pytest.mark.parametrize("iso", [False, True])
-def test_unrolled_forward_and_adjoint(iso, torch_cuda):
-    torch = torch_cuda
+def _check(torch, side, T, count, K, ckpt, iso, n_dirs, mu, beta):
     from tval3g.autograd import unrolled_tval3
-    side, T, count, K = 32, 32, 3, 20
     g, b, u = _batch(side, T, count, iso)
     spec = capi.ray2d_problem((side, side), g)
     opts = W.options(2 ** 8, 2 ** 5, 1e-4, K, tv_norm=int(iso))
-    h = capi.Unrolled(spec, count, opts, K, ckpt=6)
-    mu, beta = _schedule(K)
+    h = capi.Unrolled(spec, count, opts, K, ckpt=ckpt)
     tb = torch.tensor(b, device="cuda", requires_grad=True)
     tm = torch.tensor(mu, requires_grad=True)
     tB = torch.tensor(beta, requires_grad=True)
@@ -54,19 +50,21 @@ def test_unrolled_forward_and_adjoint(iso, torch_cuda):
     A, At = (lambda x: op.apply(x)), (lambda y: op.apply(y, True))
     gmu_ref, gbeta_ref = np.zeros(K), np.zeros(K)
     Fs = []
+    errs = {"fwd": [], "gb": [], "fd": []}
     for i in range(count):
         steps, outer, scl = h.decisions(i)
         assert np.all(steps > 0) and not outer[-1]
         F = UR.Unrolled(A, At, (side, side), steps, outer, scl, iso)
         Fs.append(F)
         U64 = F.forward(b[i], mu, beta)
-        assert relerr(Ug[i], U64) <= FWD_TOL
+        errs["fwd"].append(relerr(Ug[i], U64))
         gb_i, gm_i, gB_i = F.backward(b[i], mu, beta, U64 - u[i])
-        assert relerr(gb[i], gb_i) <= GRAD_TOL
+        errs["gb"].append(relerr(gb[i], gb_i))
+        assert errs["fwd"][-1] <= FWD_TOL and errs["gb"][-1] <= GRAD_TOL
         gmu_ref += gm_i
         gbeta_ref += gB_i
-    assert relerr(tm.grad.numpy(), gmu_ref) <= GRAD_TOL
-    assert relerr(tB.grad.numpy(), gbeta_ref) <= GRAD_TOL
+    errs["gmu"], errs["gbeta"] = relerr(tm.grad.numpy(), gmu_ref), relerr(tB.grad.numpy(), gbeta_ref)
+    assert errs["gmu"] <= GRAD_TOL and errs["gbeta"] <= GRAD_TOL
 
     # directional derivatives against central differences of the FP64 map
     rng = np.random.default_rng(5)
@@ -75,11 +73,26 @@ def test_unrolled_forward_and_adjoint(iso, torch_cuda):
         return sum(0.5 * np.sum((F.forward(b[i] + db[i], mu * fm, beta * fB) - u[i]) ** 2) for i, F in enumerate(Fs))
 
     hstep, sb = 1e-6, np.abs(b).mean()
-    for _ in range(16):
+    for _ in range(n_dirs):
         vb = rng.standard_normal(b.shape)
         vm, vB = rng.standard_normal(K), rng.standard_normal(K)
         fd = (L(hstep * sb * vb, 1 + hstep * vm, 1 + hstep * vB) - L(-hstep * sb * vb, 1 - hstep * vm, 1 - hstep * vB)) \
             / (2 * hstep)
         an = sb * np.sum(gb * vb) + np.dot(tm.grad.numpy(), mu * vm) + np.dot(tB.grad.numpy(), beta * vB)
-        assert abs(fd - an) <= FD_TOL * abs(fd), (fd, an)
+        errs["fd"].append(abs(fd - an) / abs(fd))
+        assert errs["fd"][-1] <= FD_TOL, (fd, an)
     h.close()
+    return errs
+
+
+@pytest.mark.parametrize("iso", [False, True])
+def test_unrolled_forward_and_adjoint(iso, torch_cuda):
+    """32x32 ring, 3 instances, K = 20, varying (mu_k, beta_k), 64 directions."""
+    mu, beta = _schedule(20)
+    _check(torch_cuda, 32, 32, 3, 20, 6, iso, 64, mu, beta)
+
+
+def test_unrolled_differentiation_config(torch_cuda):
+    """128x128 ring, 256 transducers x 128 receivers (m = 32768), 8 instances,
+    K = 50 with a checkpoint every 10, (mu_k, beta_k) = (2^8, 2^5), 16 directions."""
+    _check(torch_cuda, 128, 256, 8, 50, 10, True, 16, np.full(50, 2.0 ** 8), np.full(50, 2.0 ** 5))
