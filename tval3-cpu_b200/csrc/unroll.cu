@@ -2,8 +2,8 @@
 // per-iteration (mu_k, beta_k), gradients of <gU, U_K / scl> with respect to
 // b, mu_k and beta_k by a hand-written adjoint.
 //
-// Forward.  A plan in schedule mode runs the real solve for exactly K inner
-// iterations (tol = 0, no A^T skipping) and records, per instance and
+// Forward.  A plan in schedule mode runs the real FP32 solve for exactly K
+// inner iterations (tol = 0, no A^T skipping) and records, per instance and
 // iteration, the step actually taken (tau times the Armijo backtracking
 // factor, or the restart's tau; 2d/tval3_cpu_2d.cpp:425-453,526-576) and
 // whether the multipliers were updated after it (2d:673-694,820-842).  These
@@ -18,15 +18,20 @@
 //             if outer_k: sigma_k = sigma_{k-1} - beta_k E, delta_k = delta_{k-1} - mu_k r
 //             d_k = D^T (E - sigma_k / beta_k) + A^T ((mu_k r - delta_k) / beta_k)
 //
-// F is replayed on the device in FP32 (the projector, stencil and shrinkage
-// kernels), with a checkpoint of (U, sigma, delta, d) every `ckpt`
-// iterations; its U_K / scl is the forward output.
+// F is replayed on the device in FP64, with a checkpoint of (U, sigma,
+// delta, d) every `ckpt` iterations; its U_K / scl is the forward output.
+// FP64, because F is only piecewise smooth (the shrinkage switches pixels on
+// and off at |Z| = 1/beta): rounding the trajectory's states to FP32 moves
+// the exact gradient by up to 8e-4 relative at 128x128 with K = 50 (measured
+// on the FP64 restatement), far above the FP32 forward's 2e-6.
 //
 // Backward.  Segment by segment from the last, the states of the segment are
 // recomputed from its checkpoint and the adjoint runs back through them:
-// per iteration one forward and one adjoint projector application, D and D^T,
-// the shrinkage's Jacobian-transpose, and FP64 inner products (block partials
-// summed in a fixed order) for the mu_k and beta_k gradients.
+// per iteration one forward and one adjoint projector application (FP64
+// gathers over the operator's CSR and its device-built CSC; for ray
+// operators the traced Bresenham lists), D and D^T, the shrinkage's
+// Jacobian-transpose, and FP64 inner products (block partials summed in a
+// fixed order) for the mu_k and beta_k gradients.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -40,39 +45,42 @@ constexpr int EW_BLOCKS = 296;   // grid-stride elementwise kernels: 2 blocks pe
 constexpr int EW_THREADS = 256;
 constexpr int NPIX = 4, NMEAS = 3;   // inner products per reverse step
 
-__device__ __forceinline__ void shrink2(float zx, float zy, float t, bool iso, float &wx, float &wy) {
+#define GRID_STRIDE(i, n) \
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+__device__ __forceinline__ void shrink2(double zx, double zy, double t, bool iso, double &wx, double &wy) {
 	if (iso) {
-		const float nrm = sqrtf(zx * zx + zy * zy);
-		const float s = nrm > t ? (nrm - t) / nrm : 0.f;
+		const double nrm = sqrt(zx * zx + zy * zy);
+		const double s = nrm > t ? (nrm - t) / nrm : 0.0;
 		wx = s * zx;
 		wy = s * zy;
 	} else {
-		const float ax = fabsf(zx) - t, ay = fabsf(zy) - t;
-		wx = ax > 0.f ? (zx >= 0.f ? ax : -ax) : 0.f;
-		wy = ay > 0.f ? (zy >= 0.f ? ay : -ay) : 0.f;
+		const double ax = fabs(zx) - t, ay = fabs(zy) - t;
+		wx = ax > 0.0 ? (zx >= 0.0 ? ax : -ax) : 0.0;
+		wy = ay > 0.0 ? (zy >= 0.0 ? ay : -ay) : 0.0;
 	}
 }
 
 // Z-cotangent and the t-derivative term of W = S(Z, t) for the W-cotangent (wbx, wby)
-__device__ __forceinline__ void shrink2_vjp(float zx, float zy, float t, bool iso, float wbx, float wby,
-                                            float &zbx, float &zby, double &tbar) {
+__device__ __forceinline__ void shrink2_vjp(double zx, double zy, double t, bool iso, double wbx, double wby,
+                                            double &zbx, double &zby, double &tbar) {
 	if (iso) {
-		const float nrm = sqrtf(zx * zx + zy * zy);
+		const double nrm = sqrt(zx * zx + zy * zy);
 		if (nrm > t) {
-			const float zw = (zx * wbx + zy * wby) / nrm;
-			const float a = 1.f - t / nrm, c = t / (nrm * nrm);
+			const double zw = (zx * wbx + zy * wby) / nrm;
+			const double a = 1.0 - t / nrm, c = t / (nrm * nrm);
 			zbx = a * wbx + c * zx * zw;
 			zby = a * wby + c * zy * zw;
-			tbar += -(double)zw;
+			tbar += -zw;
 		} else {
-			zbx = zby = 0.f;
+			zbx = zby = 0.0;
 		}
 	} else {
-		const bool onx = fabsf(zx) > t, ony = fabsf(zy) > t;
-		zbx = onx ? wbx : 0.f;
-		zby = ony ? wby : 0.f;
-		if (onx) tbar += (zx >= 0.f ? -1.0 : 1.0) * wbx;
-		if (ony) tbar += (zy >= 0.f ? -1.0 : 1.0) * wby;
+		const bool onx = fabs(zx) > t, ony = fabs(zy) > t;
+		zbx = onx ? wbx : 0.0;
+		zby = ony ? wby : 0.0;
+		if (onx) tbar += (zx >= 0.0 ? -1.0 : 1.0) * wbx;
+		if (ony) tbar += (zy >= 0.0 ? -1.0 : 1.0) * wby;
 	}
 }
 
@@ -93,35 +101,60 @@ __device__ __forceinline__ void block_partials(double (&v)[NS], double *part) {
 	}
 }
 
-// y += a x
-__global__ void k_axpy(long long n, float a, const float *x, float *y) {
-	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-		y[i] = fmaf(a, x[i], y[i]);
+// y = A x over a CSR (rows of `ptr`), warp per row, FP64; val NULL = every
+// weight w (ray operators: the scale factor)
+__global__ void __launch_bounds__(256) k_spmv64(long long rows, const int *ptr, const int *ind, const float *val,
+                                                double w, const double *x, double *y) {
+	const long long row = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if (row >= rows) return;
+	double acc = 0.0;
+	for (int k = ptr[row] + lane; k < ptr[row + 1]; k += 32) acc += (val ? (double)val[k] : w) * x[ind[k]];
+	acc = warp_sum(acc);
+	if (lane == 0) y[row] = acc;
 }
-// y = a x
-__global__ void k_scale(long long n, float a, const float *x, float *y) {
-	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-		y[i] = a * x[i];
+
+// periodic forward differences / their adjoint on a p x q image (2d:268-293)
+__global__ void k_D64(int p, int q, const double *U, double *ux, double *uy) {
+	GRID_STRIDE(i, (long long)p * q) {
+		const int y = (int)(i / q), x = (int)(i - (long long)y * q);
+		ux[i] = (x < q - 1 ? U[i + 1] : U[i - (q - 1)]) - U[i];
+		uy[i] = (y < p - 1 ? U[i + q] : U[i - (long long)(p - 1) * q]) - U[i];
+	}
 }
-// out = x + y
-__global__ void k_add(long long n, const float *x, const float *y, float *out) {
-	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-		out[i] = x[i] + y[i];
+__global__ void k_Dt64(int p, int q, const double *X, const double *Y, double *res) {
+	GRID_STRIDE(i, (long long)p * q) {
+		const int y = (int)(i / q), x = (int)(i - (long long)y * q);
+		res[i] = ((x > 0 ? X[i - 1] : X[i + q - 1]) - X[i]) +
+		         ((y > 0 ? Y[i - q] : Y[i + (long long)(p - 1) * q]) - Y[i]);
+	}
+}
+
+__global__ void k_axpy(long long n, double a, const double *x, double *y) {
+	GRID_STRIDE(i, n) y[i] = fma(a, x[i], y[i]);
+}
+__global__ void k_add(long long n, const double *x, const double *y, double *out) {
+	GRID_STRIDE(i, n) out[i] = x[i] + y[i];
+}
+__global__ void k_to64(long long n, double a, const float *x, double *y) {
+	GRID_STRIDE(i, n) y[i] = a * (double)x[i];
+}
+__global__ void k_to32(long long n, double a, const double *x, float *y) {
+	GRID_STRIDE(i, n) y[i] = (float)(a * x[i]);
 }
 
 // forward state, pixels: shrinkage, multiplier update of sigma, G = E - sigma_k / beta
-__global__ void k_state_pix(long long n, const float *vx, const float *vy, float *sx, float *sy, float beta,
-                            int outer, int iso, float *gx, float *gy) {
-	const float t = 1.f / beta;
-	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-		const float Vx = vx[i], Vy = vy[i];
-		float s_x = sx[i], s_y = sy[i];
-		float wx, wy;
+__global__ void k_state_pix(long long n, const double *vx, const double *vy, double *sx, double *sy, double beta,
+                            int outer, int iso, double *gx, double *gy) {
+	const double t = 1.0 / beta;
+	GRID_STRIDE(i, n) {
+		const double Vx = vx[i], Vy = vy[i];
+		double s_x = sx[i], s_y = sy[i], wx, wy;
 		shrink2(Vx - s_x / beta, Vy - s_y / beta, t, iso, wx, wy);
-		const float ex = Vx - wx, ey = Vy - wy;
+		const double ex = Vx - wx, ey = Vy - wy;
 		if (outer) {
-			s_x = fmaf(-beta, ex, s_x);
-			s_y = fmaf(-beta, ey, s_y);
+			s_x -= beta * ex;
+			s_y -= beta * ey;
 			sx[i] = s_x;
 			sy[i] = s_y;
 		}
@@ -131,13 +164,13 @@ __global__ void k_state_pix(long long n, const float *vx, const float *vy, float
 }
 
 // forward state, measurements: r = Au - bs, multiplier update of delta, q = (mu r - delta) / beta
-__global__ void k_state_meas(long long m, const float *au, const float *bs, float *r, float *dl, float mu,
-                             float beta, int outer, float *q) {
-	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
-		const float rr = au[i] - bs[i];
-		float d = dl[i];
+__global__ void k_state_meas(long long m, const double *au, const double *bs, double *r, double *dl, double mu,
+                             double beta, int outer, double *q) {
+	GRID_STRIDE(i, m) {
+		const double rr = au[i] - bs[i];
+		double d = dl[i];
 		if (outer) {
-			d = fmaf(-mu, rr, d);
+			d -= mu * rr;
 			dl[i] = d;
 		}
 		r[i] = rr;
@@ -145,32 +178,32 @@ __global__ void k_state_meas(long long m, const float *au, const float *bs, floa
 	}
 }
 
-// reverse step, pixels (see the file comment); partials: <Dd, sigma_k>,
-// <sigma_k-bar, E>, sum of the shrinkage's t-derivative term, <Zbar, sigma_{k-1}>
-__global__ void __launch_bounds__(EW_THREADS) k_rev_pix(long long n, const float *ddx, const float *ddy,
-                                                        const float *vx, const float *vy, const float *s0x,
-                                                        const float *s0y, const float *s1x, const float *s1y,
-                                                        float *sbx, float *sby, float beta, int outer, int iso,
-                                                        float *vbx, float *vby, double *part) {
-	const float t = 1.f / beta;
+// reverse step, pixels; partials: <Dd, sigma_k>, <sigma_k-bar, E>, the
+// shrinkage's t-derivative term, <Zbar, sigma_{k-1}>
+__global__ void __launch_bounds__(EW_THREADS) k_rev_pix(long long n, const double *ddx, const double *ddy,
+                                                        const double *vx, const double *vy, const double *s0x,
+                                                        const double *s0y, const double *s1x, const double *s1y,
+                                                        double *sbx, double *sby, double beta, int outer, int iso,
+                                                        double *vbx, double *vby, double *part) {
+	const double t = 1.0 / beta;
 	double acc[NPIX] = {0, 0, 0, 0};
-	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-		const float zx = vx[i] - s0x[i] / beta, zy = vy[i] - s0y[i] / beta;
-		float wx, wy;
+	GRID_STRIDE(i, n) {
+		const double zx = vx[i] - s0x[i] / beta, zy = vy[i] - s0y[i] / beta;
+		double wx, wy;
 		shrink2(zx, zy, t, iso, wx, wy);
-		const float ex = vx[i] - wx, ey = vy[i] - wy;
-		const float dx = ddx ? ddx[i] : 0.f, dy = ddy ? ddy[i] : 0.f;
-		float sx = sbx[i] - dx / beta, sy = sby[i] - dy / beta;   // cotangent of sigma_k
-		float ebx = dx, eby = dy;
-		acc[0] += (double)dx * s1x[i] + (double)dy * s1y[i];
+		const double ex = vx[i] - wx, ey = vy[i] - wy;
+		const double dx = ddx ? ddx[i] : 0.0, dy = ddy ? ddy[i] : 0.0;
+		const double sx = sbx[i] - dx / beta, sy = sby[i] - dy / beta;   // cotangent of sigma_k
+		double ebx = dx, eby = dy;
+		acc[0] += dx * s1x[i] + dy * s1y[i];
 		if (outer) {
-			ebx = fmaf(-beta, sx, ebx);
-			eby = fmaf(-beta, sy, eby);
-			acc[1] += (double)sx * ex + (double)sy * ey;
+			ebx -= beta * sx;
+			eby -= beta * sy;
+			acc[1] += sx * ex + sy * ey;
 		}
-		float zbx, zby;
+		double zbx, zby;
 		shrink2_vjp(zx, zy, t, iso, -ebx, -eby, zbx, zby, acc[2]);
-		acc[3] += (double)zbx * s0x[i] + (double)zby * s0y[i];
+		acc[3] += zbx * s0x[i] + zby * s0y[i];
 		vbx[i] = ebx + zbx;
 		vby[i] = eby + zby;
 		sbx[i] = sx - zbx / beta;   // cotangent of sigma_{k-1}
@@ -180,19 +213,19 @@ __global__ void __launch_bounds__(EW_THREADS) k_rev_pix(long long n, const float
 }
 
 // reverse step, measurements; partials: <Ad, r>, <Ad, delta - mu r>, <delta_k-bar, r>
-__global__ void __launch_bounds__(EW_THREADS) k_rev_meas(long long m, const float *ad, const float *r, const float *dl,
-                                                         float *dlb, float *bsb, float mu, float beta, int outer,
-                                                         float *rb, double *part) {
+__global__ void __launch_bounds__(EW_THREADS) k_rev_meas(long long m, const double *ad, const double *r,
+                                                         const double *dl, double *dlb, double *bsb, double mu,
+                                                         double beta, int outer, double *rb, double *part) {
 	double acc[NMEAS] = {0, 0, 0};
-	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
-		const float a = ad ? ad[i] : 0.f, rr = r[i];
-		const float db = dlb[i] - a / beta;   // cotangent of delta_k
-		float rbv = (mu / beta) * a;
-		acc[0] += (double)a * rr;
-		acc[1] += (double)a * (dl[i] - mu * rr);
+	GRID_STRIDE(i, m) {
+		const double a = ad ? ad[i] : 0.0, rr = r[i];
+		const double db = dlb[i] - a / beta;   // cotangent of delta_k
+		double rbv = (mu / beta) * a;
+		acc[0] += a * rr;
+		acc[1] += a * (dl[i] - mu * rr);
 		if (outer) {
-			rbv = fmaf(-mu, db, rbv);
-			acc[2] += (double)db * rr;
+			rbv -= mu * db;
+			acc[2] += db * rr;
 		}
 		dlb[i] = db;
 		rb[i] = rbv;
@@ -202,9 +235,9 @@ __global__ void __launch_bounds__(EW_THREADS) k_rev_meas(long long m, const floa
 }
 
 // Ubar += t1 + t2; dd = -step Ubar
-__global__ void k_rev_u(long long n, const float *t1, const float *t2, float *ub, float nstep, float *dd) {
-	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-		const float u = ub[i] + t1[i] + t2[i];
+__global__ void k_rev_u(long long n, const double *t1, const double *t2, double *ub, double nstep, double *dd) {
+	GRID_STRIDE(i, n) {
+		const double u = ub[i] + t1[i] + t2[i];
 		ub[i] = u;
 		if (dd) dd[i] = nstep * u;
 	}
@@ -226,12 +259,11 @@ __global__ void k_rev_scalars(const double *pp, const double *pm, int nb, double
 
 }  // namespace
 
-// one instance's device buffers for the replay and the adjoint
 struct UnrolledInst {
 	std::vector<double> steps;
 	std::vector<int> outer;
 	double scl = 1;
-	float *bs = nullptr;   // scl * b
+	double *bs = nullptr;   // scl * b (FP64)
 };
 
 class Unrolled {
@@ -246,45 +278,48 @@ public:
 
 private:
 	int count_, K_, C_, p_, q_, iso_;
-	long long n_, m_;
+	long long n_, m_, nnz_ = 0;
 	Plan *plan_ = nullptr;
-	tval3g_operator *op_ = nullptr;
 	// used when the caller passes the legacy default stream: blocking, so it
-	// is ordered with that stream's work on both sides, and every launch
-	// here (and the operator's) goes to one stream
+	// is ordered with that stream's work on both sides
 	cudaStream_t own_ = nullptr;
+	// the operator as a CSR over measurements and its CSC over pixels
+	int *rptr_ = nullptr, *rind_ = nullptr, *cptr_ = nullptr, *cind_ = nullptr;
+	float *rval_ = nullptr, *cval_ = nullptr;
+	double w_ = 1.0;
 	std::vector<UnrolledInst> in_;
 	std::vector<double> mu_, beta_;
-	std::vector<float *> eng_u_;       // the engine's U (decisions only)
+	std::vector<float *> eng_u_;       // the FP32 solve's U (decisions only)
 	std::vector<void *> allocs_;
 	// checkpoints: [instance][c] -> U, sx, sy, delta, d
-	std::vector<std::vector<float *>> ck_;
+	std::vector<std::vector<double *>> ck_;
 	// segment states, j = 0..C: U, sx, sy, delta, r
-	std::vector<float *> segU_, segSx_, segSy_, segDl_, segR_;
+	std::vector<double *> segU_, segSx_, segSy_, segDl_, segR_;
 	// scratch
-	float *vx_, *vy_, *gx_, *gy_, *t1_, *t2_, *d_, *U_, *sx_, *sy_, *au_, *qv_, *dl_, *r_;
-	float *ub_, *sbx_, *sby_, *dlb_, *bsb_, *dd_, *ddx_, *ddy_, *ad_, *rb_, *vbx_, *vby_;
+	double *vx_, *vy_, *gx_, *gy_, *t1_, *t2_, *d_, *U_, *sx_, *sy_, *au_, *qv_, *dl_, *r_;
+	double *ub_, *sbx_, *sby_, *dlb_, *bsb_, *dd_, *ddx_, *ddy_, *ad_, *rb_, *vbx_, *vby_, *zero_;
 	double *pp_, *pm_, *gsc_;   // partials, gradient scalars (2K)
-	float *fa(long long count);
+	void *dmalloc(size_t bytes);
+	double *da(long long count) { return static_cast<double *>(dmalloc(sizeof(double) * (size_t)std::max(count, 1LL))); }
 	void release();
-	void apply(bool trans, const float *x, float *y, cudaStream_t s);
-	void state(int k, const float *bs, float *U, float *sx, float *sy, float *dl, float *r, float *d, int o,
+	void apply(bool trans, const double *x, double *y, cudaStream_t s);
+	void state(int k, const double *bs, double *U, double *sx, double *sy, double *dl, double *r, double *d, int o,
 	           cudaStream_t s);
 	void replay_from(int i, int k0, int k1, cudaStream_t s, bool store_seg, bool ckpt);
 };
 
-float *Unrolled::fa(long long count) {
+void *Unrolled::dmalloc(size_t bytes) {
 	void *p = nullptr;
-	TG_CUDA(cudaMalloc(&p, sizeof(float) * (size_t)std::max(count, 1LL)));
+	TG_CUDA(cudaMalloc(&p, std::max(bytes, (size_t)8)));
 	allocs_.push_back(p);
-	return static_cast<float *>(p);
+	return p;
 }
 
 Unrolled::Unrolled(const tval3g_problem &p, int count, const tval3g_options &o, int K, int ckpt)
 	: count_(count), K_(K), C_(ckpt) {
 	TG_ARG(count >= 1 && K >= 1 && ckpt >= 1, "Argument error: count, K and the checkpoint interval must be >= 1");
 	TG_ARG(p.dims == 2 && (p.op_kind == TVAL3G_OP_RAY2D || p.op_kind == TVAL3G_OP_CSR ||
-	                       (p.op_kind == TVAL3G_OP_DENSE && p.layers <= 1)),
+	                       (p.op_kind == TVAL3G_OP_DENSE && p.layers <= 1)) && p.layers <= 1,
 	       "Argument error: the unrolled solve is 2D with one layer");
 	TG_ARG(!o.nonneg, "Argument error: the unrolled solve has no nonnegativity projection");
 	p_ = p.dim_y;
@@ -297,43 +332,87 @@ Unrolled::Unrolled(const tval3g_problem &p, int count, const tval3g_options &o, 
 	oo.skipMulRatio = 0;        // g = A^T (A U - b) every iteration
 	std::vector<tval3g_problem> probs(count, p);
 	std::vector<tval3g_options> opts(count, oo);
+	tval3g_operator *op = nullptr;
 	try {
 		TG_CUDA(cudaStreamCreate(&own_));
 		plan_ = new Plan(count, probs.data(), opts.data(), TVAL3G_GRAPH | TVAL3G_TRACE | PLAN_SCHEDULE);
-		int rc = tval3g_op_create(&op_, &p, 0);
-		if (rc != TVAL3G_OK) throw Error{rc, tval3g_last_error()};
-		long long rows = 0, cols = 0, nnz = 0;
-		tval3g_op_shape(op_, &rows, &cols, &nnz);
-		m_ = rows;
-		n_ = cols;
+		// the operator's CSR on the host: the traced rays, the caller's CSR, or the dense rows
+		std::vector<long long> hp;
+		std::vector<int> hi;
+		std::vector<float> hv;
+		if (p.op_kind == TVAL3G_OP_RAY2D) {
+			int rc = tval3g_op_create(&op, &p, 0);
+			if (rc != TVAL3G_OK) throw Error{rc, tval3g_last_error()};
+			long long rows = 0, cols = 0, nnz = 0;
+			tval3g_op_shape(op, &rows, &cols, &nnz);
+			m_ = rows;
+			n_ = cols;
+			hp.resize(m_ + 1);
+			hi.resize(std::max(nnz, 1LL));
+			rc = tval3g_op_ray_csr(op, hp.data(), hi.data());
+			if (rc != TVAL3G_OK) throw Error{rc, tval3g_last_error()};
+			tval3g_op_destroy(op);
+			op = nullptr;
+			w_ = p.scale_factor;
+		} else if (p.op_kind == TVAL3G_OP_CSR) {
+			m_ = p.m;
+			n_ = p.n_cols;
+			hp.assign(p.csr_ptr, p.csr_ptr + m_ + 1);
+			hi.assign(p.csr_ind, p.csr_ind + p.nnz);
+			hv.assign(p.csr_val, p.csr_val + p.nnz);
+		} else {
+			m_ = p.m;
+			n_ = p.n_cols;
+			hp.resize(m_ + 1);
+			for (long long r = 0; r <= m_; r++) hp[r] = r * n_;
+			hi.resize(m_ * n_);
+			for (long long k = 0; k < m_ * n_; k++) hi[k] = (int)(k % n_);
+			hv.assign(p.A, p.A + m_ * n_);
+		}
+		TG_ARG(n_ == (long long)p_ * q_, "Argument error: the operator does not match the image");
+		nnz_ = hp[m_];
+		TG_ARG(nnz_ < (1LL << 31), "Argument error: too many operator entries");
+		std::vector<int> hp32(hp.begin(), hp.end());
+		rptr_ = static_cast<int *>(dmalloc(sizeof(int) * (m_ + 1)));
+		rind_ = static_cast<int *>(dmalloc(sizeof(int) * (size_t)nnz_));
+		cptr_ = static_cast<int *>(dmalloc(sizeof(int) * (n_ + 1)));
+		cind_ = static_cast<int *>(dmalloc(sizeof(int) * (size_t)nnz_));
+		TG_CUDA(cudaMemcpy(rptr_, hp32.data(), sizeof(int) * (m_ + 1), cudaMemcpyHostToDevice));
+		TG_CUDA(cudaMemcpy(rind_, hi.data(), sizeof(int) * (size_t)nnz_, cudaMemcpyHostToDevice));
+		if (!hv.empty()) {
+			rval_ = static_cast<float *>(dmalloc(sizeof(float) * (size_t)nnz_));
+			cval_ = static_cast<float *>(dmalloc(sizeof(float) * (size_t)nnz_));
+			TG_CUDA(cudaMemcpy(rval_, hv.data(), sizeof(float) * (size_t)nnz_, cudaMemcpyHostToDevice));
+		}
+		build_transpose(own_, m_, n_, nnz_, rptr_, rind_, rval_, cptr_, cind_, cval_);
+		TG_CUDA(cudaStreamSynchronize(own_));
 		in_.resize(count);
 		for (int i = 0; i < count; i++) {
-			in_[i].bs = fa(m_);
-			eng_u_.push_back(fa(n_));
+			in_[i].bs = da(m_);
+			eng_u_.push_back(static_cast<float *>(dmalloc(sizeof(float) * (size_t)n_)));
 		}
 		const int nck = K / C_ + 1;
 		ck_.resize(count);
 		for (int i = 0; i < count; i++)
 			for (int c = 0; c < nck; c++)
-				for (int v = 0; v < 5; v++) ck_[i].push_back(fa(v == 3 ? m_ : n_));
+				for (int v = 0; v < 5; v++) ck_[i].push_back(da(v == 3 ? m_ : n_));
 		for (int j = 0; j <= C_; j++) {
-			segU_.push_back(fa(n_));
-			segSx_.push_back(fa(n_));
-			segSy_.push_back(fa(n_));
-			segDl_.push_back(fa(m_));
-			segR_.push_back(fa(m_));
+			segU_.push_back(da(n_));
+			segSx_.push_back(da(n_));
+			segSy_.push_back(da(n_));
+			segDl_.push_back(da(m_));
+			segR_.push_back(da(m_));
 		}
-		for (float **v : {&vx_, &vy_, &gx_, &gy_, &t1_, &t2_, &d_, &U_, &sx_, &sy_, &ub_, &sbx_, &sby_, &dd_, &ddx_,
-		                  &ddy_, &vbx_, &vby_})
-			*v = fa(n_);
-		for (float **v : {&au_, &qv_, &dl_, &r_, &dlb_, &bsb_, &ad_, &rb_}) *v = fa(m_);
-		void *pp = nullptr;
-		TG_CUDA(cudaMalloc(&pp, sizeof(double) * (size_t)(EW_BLOCKS * (NPIX + NMEAS) + 2 * K)));
-		allocs_.push_back(pp);
-		pp_ = static_cast<double *>(pp);
+		for (double **v : {&vx_, &vy_, &gx_, &gy_, &t1_, &t2_, &d_, &U_, &sx_, &sy_, &ub_, &sbx_, &sby_, &dd_, &ddx_,
+		                   &ddy_, &vbx_, &vby_, &zero_})
+			*v = da(n_);
+		for (double **v : {&au_, &qv_, &dl_, &r_, &dlb_, &bsb_, &ad_, &rb_}) *v = da(m_);
+		TG_CUDA(cudaMemset(zero_, 0, sizeof(double) * (size_t)n_));
+		pp_ = da(EW_BLOCKS * (NPIX + NMEAS) + 2 * (long long)K);
 		pm_ = pp_ + EW_BLOCKS * NPIX;
 		gsc_ = pm_ + EW_BLOCKS * NMEAS;
 	} catch (...) {
+		if (op) tval3g_op_destroy(op);
 		release();
 		throw;
 	}
@@ -345,17 +424,10 @@ void Unrolled::release() {
 	cudaDeviceSynchronize();
 	for (void *p : allocs_) cudaFree(p);
 	allocs_.clear();
-	if (op_) tval3g_op_destroy(op_);
-	op_ = nullptr;
 	delete plan_;
 	plan_ = nullptr;
 	if (own_) cudaStreamDestroy(own_);
 	own_ = nullptr;
-}
-
-void Unrolled::apply(bool trans, const float *x, float *y, cudaStream_t s) {
-	int rc = tval3g_op_apply_n(op_, trans ? 1 : 0, x, y, 1, s);
-	if (rc != TVAL3G_OK) throw Error{rc, tval3g_last_error()};
 }
 
 #define EW(kern, ...)                                                     \
@@ -364,17 +436,25 @@ void Unrolled::apply(bool trans, const float *x, float *y, cudaStream_t s) {
 		TG_CUDA(cudaGetLastError());                                      \
 	} while (0)
 
+// y = A x (trans = false) or A^T x, FP64
+void Unrolled::apply(bool trans, const double *x, double *y, cudaStream_t s) {
+	const long long rows = trans ? n_ : m_;
+	k_spmv64<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(rows, trans ? cptr_ : rptr_, trans ? cind_ : rind_,
+	                                                            trans ? cval_ : rval_, w_, x, y);
+	TG_CUDA(cudaGetLastError());
+}
+
 // state(k) from U (in place: sigma, delta updated when o); d written
-void Unrolled::state(int k, const float *bs, float *U, float *sx, float *sy, float *dl, float *r, float *d, int o,
-                     cudaStream_t s) {
+void Unrolled::state(int k, const double *bs, double *U, double *sx, double *sy, double *dl, double *r, double *d,
+                     int o, cudaStream_t s) {
 	const int j = std::max(k, 1) - 1;
-	const float mu = (float)mu_[j], beta = (float)beta_[j];
-	launch_D_plain(s, 2, p_, q_, 1, U, vx_, vy_, nullptr);
+	const double mu = mu_[j], beta = beta_[j];
+	EW(k_D64, p_, q_, U, vx_, vy_);
 	EW(k_state_pix, n_, vx_, vy_, sx, sy, beta, o, iso_, gx_, gy_);
 	apply(false, U, au_, s);
 	EW(k_state_meas, m_, au_, bs, r, dl, mu, beta, o, qv_);
 	apply(true, qv_, t1_, s);
-	launch_Dt_plain(s, 2, p_, q_, 1, gx_, gy_, nullptr, t2_);
+	EW(k_Dt64, p_, q_, gx_, gy_, t2_);
 	EW(k_add, n_, t1_, t2_, d);
 }
 
@@ -382,7 +462,7 @@ void Unrolled::state(int k, const float *bs, float *U, float *sx, float *sy, flo
 // sx_, sy_, dl_, d_ = iteration k0); store_seg: keep every state (j = k - k0)
 void Unrolled::replay_from(int i, int k0, int k1, cudaStream_t s, bool store_seg, bool ckpt) {
 	const UnrolledInst &I = in_[i];
-	const size_t nb = sizeof(float) * (size_t)n_, mb = sizeof(float) * (size_t)m_;
+	const size_t nb = sizeof(double) * (size_t)n_, mb = sizeof(double) * (size_t)m_;
 	auto save_seg = [&](int j) {
 		TG_CUDA(cudaMemcpyAsync(segU_[j], U_, nb, cudaMemcpyDeviceToDevice, s));
 		TG_CUDA(cudaMemcpyAsync(segSx_[j], sx_, nb, cudaMemcpyDeviceToDevice, s));
@@ -391,7 +471,7 @@ void Unrolled::replay_from(int i, int k0, int k1, cudaStream_t s, bool store_seg
 		TG_CUDA(cudaMemcpyAsync(segR_[j], r_, mb, cudaMemcpyDeviceToDevice, s));
 	};
 	auto save_ck = [&](int k) {
-		float *const *c = &ck_[i][(size_t)(k / C_) * 5];
+		double *const *c = &ck_[i][(size_t)(k / C_) * 5];
 		TG_CUDA(cudaMemcpyAsync(c[0], U_, nb, cudaMemcpyDeviceToDevice, s));
 		TG_CUDA(cudaMemcpyAsync(c[1], sx_, nb, cudaMemcpyDeviceToDevice, s));
 		TG_CUDA(cudaMemcpyAsync(c[2], sy_, nb, cudaMemcpyDeviceToDevice, s));
@@ -401,7 +481,7 @@ void Unrolled::replay_from(int i, int k0, int k1, cudaStream_t s, bool store_seg
 	if (store_seg) save_seg(0);
 	if (ckpt && k0 % C_ == 0) save_ck(k0);
 	for (int k = k0 + 1; k <= k1; k++) {
-		EW(k_axpy, n_, (float)(-I.steps[k - 1]), d_, U_);
+		EW(k_axpy, n_, -I.steps[k - 1], d_, U_);
 		state(k, I.bs, U_, sx_, sy_, dl_, r_, d_, I.outer[k - 1], s);
 		if (store_seg) save_seg(k - k0);
 		if (ckpt && k % C_ == 0) save_ck(k);
@@ -413,7 +493,7 @@ void Unrolled::forward(const float *const *d_b, const double *mu, const double *
 	if (!s) s = own_;
 	mu_.assign(mu, mu + K_);
 	beta_.assign(beta, beta + K_);
-	// the solve that records the decisions
+	// the FP32 solve that records the decisions
 	plan_->set_schedule(mu, beta);
 	std::vector<tval3g_info> info(count_);
 	plan_->solve(d_b, nullptr, eng_u_.data(), info.data(), s);
@@ -432,17 +512,18 @@ void Unrolled::forward(const float *const *d_b, const double *mu, const double *
 		}
 		I.scl = c[i].scl;
 	}
-	// replay F with checkpoints
+	// replay F in FP64 with checkpoints
+	const size_t nb = sizeof(double) * (size_t)n_, mb = sizeof(double) * (size_t)m_;
 	for (int i = 0; i < count_; i++) {
 		UnrolledInst &I = in_[i];
-		EW(k_scale, m_, (float)I.scl, d_b[i], I.bs);
+		EW(k_to64, m_, I.scl, d_b[i], I.bs);
 		apply(true, I.bs, U_, s);
-		TG_CUDA(cudaMemsetAsync(sx_, 0, sizeof(float) * (size_t)n_, s));
-		TG_CUDA(cudaMemsetAsync(sy_, 0, sizeof(float) * (size_t)n_, s));
-		TG_CUDA(cudaMemsetAsync(dl_, 0, sizeof(float) * (size_t)m_, s));
+		TG_CUDA(cudaMemsetAsync(sx_, 0, nb, s));
+		TG_CUDA(cudaMemsetAsync(sy_, 0, nb, s));
+		TG_CUDA(cudaMemsetAsync(dl_, 0, mb, s));
 		state(0, I.bs, U_, sx_, sy_, dl_, r_, d_, 0, s);
 		replay_from(i, 0, K_, s, false, true);
-		EW(k_scale, n_, (float)(1.0 / I.scl), U_, d_U[i]);
+		EW(k_to32, n_, 1.0 / I.scl, U_, d_U[i]);
 	}
 	TG_CUDA(cudaStreamSynchronize(s));
 }
@@ -451,58 +532,52 @@ void Unrolled::backward(const float *const *d_gU, float *const *d_gb, double *g_
 	TG_ARG(!mu_.empty(), "Argument error: backward before forward");
 	if (!s) s = own_;
 	TG_CUDA(cudaMemsetAsync(gsc_, 0, sizeof(double) * 2 * (size_t)K_, s));
-	const size_t nb = sizeof(float) * (size_t)n_, mb = sizeof(float) * (size_t)m_;
+	const size_t nb = sizeof(double) * (size_t)n_, mb = sizeof(double) * (size_t)m_;
 	for (int i = 0; i < count_; i++) {
 		const UnrolledInst &I = in_[i];
-		EW(k_scale, n_, (float)(1.0 / I.scl), d_gU[i], ub_);
-		for (float *v : {sbx_, sby_}) TG_CUDA(cudaMemsetAsync(v, 0, nb, s));
-		for (float *v : {dlb_, bsb_}) TG_CUDA(cudaMemsetAsync(v, 0, mb, s));
+		EW(k_to64, n_, 1.0 / I.scl, d_gU[i], ub_);
+		for (double *v : {sbx_, sby_}) TG_CUDA(cudaMemsetAsync(v, 0, nb, s));
+		for (double *v : {dlb_, bsb_}) TG_CUDA(cudaMemsetAsync(v, 0, mb, s));
 		bool has_d = false;
 		for (int c = K_ / C_; c >= 0; c--) {
 			const int k0 = c * C_, k1 = std::min(k0 + C_, K_);
-			if (k0 > K_ || (k0 == K_ && K_ > 0 && c > 0 && k1 == k0)) continue;
+			if (c > 0 && k0 >= K_) continue;   // a segment without iterations
 			// the checkpoint state of iteration k0, r of iteration k0, then the segment
-			float *const *ck = &ck_[i][(size_t)c * 5];
+			double *const *ck = &ck_[i][(size_t)c * 5];
 			TG_CUDA(cudaMemcpyAsync(U_, ck[0], nb, cudaMemcpyDeviceToDevice, s));
 			TG_CUDA(cudaMemcpyAsync(sx_, ck[1], nb, cudaMemcpyDeviceToDevice, s));
 			TG_CUDA(cudaMemcpyAsync(sy_, ck[2], nb, cudaMemcpyDeviceToDevice, s));
 			TG_CUDA(cudaMemcpyAsync(dl_, ck[3], mb, cudaMemcpyDeviceToDevice, s));
 			TG_CUDA(cudaMemcpyAsync(d_, ck[4], nb, cudaMemcpyDeviceToDevice, s));
 			apply(false, U_, au_, s);
-			EW(k_state_meas, m_, au_, I.bs, r_, dl_, 1.f, 1.f, 0, qv_);   // r only (q unused)
+			EW(k_state_meas, m_, au_, I.bs, r_, dl_, 1.0, 1.0, 0, qv_);   // r only (q unused)
 			replay_from(i, k0, k1, s, true, false);
 			const int klo = c == 0 ? 0 : k0 + 1;
 			for (int k = k1; k >= klo; k--) {
 				const int jj = k - k0, j = std::max(k, 1) - 1;
-				const float mu = (float)mu_[j], beta = (float)beta_[j];
+				const double mu = mu_[j], beta = beta_[j];
 				const int o = k >= 1 ? I.outer[k - 1] : 0;
-				const float *s0x = k >= 1 ? segSx_[jj - 1] : nullptr, *s0y = k >= 1 ? segSy_[jj - 1] : nullptr;
-				if (k == 0) {   // sigma_{-1} = 0
-					TG_CUDA(cudaMemsetAsync(gx_, 0, nb, s));
-					TG_CUDA(cudaMemsetAsync(gy_, 0, nb, s));
-					s0x = gx_;
-					s0y = gy_;
-				}
+				const double *s0x = k >= 1 ? segSx_[jj - 1] : zero_, *s0y = k >= 1 ? segSy_[jj - 1] : zero_;
 				if (has_d) {
-					launch_D_plain(s, 2, p_, q_, 1, dd_, ddx_, ddy_, nullptr);
+					EW(k_D64, p_, q_, dd_, ddx_, ddy_);
 					apply(false, dd_, ad_, s);
 				}
-				launch_D_plain(s, 2, p_, q_, 1, segU_[jj], vx_, vy_, nullptr);
+				EW(k_D64, p_, q_, segU_[jj], vx_, vy_);
 				EW(k_rev_pix, n_, has_d ? ddx_ : nullptr, has_d ? ddy_ : nullptr, vx_, vy_, s0x, s0y, segSx_[jj],
 				   segSy_[jj], sbx_, sby_, beta, o, iso_, vbx_, vby_, pp_);
 				EW(k_rev_meas, m_, has_d ? ad_ : nullptr, segR_[jj], segDl_[jj], dlb_, bsb_, mu, beta, o, rb_, pm_);
-				k_rev_scalars<<<1, 32, 0, s>>>(pp_, pm_, EW_BLOCKS, mu_[j], beta_[j], gsc_ + j, gsc_ + K_ + j);
+				k_rev_scalars<<<1, 32, 0, s>>>(pp_, pm_, EW_BLOCKS, mu, beta, gsc_ + j, gsc_ + K_ + j);
 				TG_CUDA(cudaGetLastError());
 				apply(true, rb_, t1_, s);
-				launch_Dt_plain(s, 2, p_, q_, 1, vbx_, vby_, nullptr, t2_);
-				EW(k_rev_u, n_, t1_, t2_, ub_, k >= 1 ? (float)(-I.steps[k - 1]) : 0.f, k >= 1 ? dd_ : nullptr);
+				EW(k_Dt64, p_, q_, vbx_, vby_, t2_);
+				EW(k_rev_u, n_, t1_, t2_, ub_, k >= 1 ? -I.steps[k - 1] : 0.0, k >= 1 ? dd_ : nullptr);
 				has_d = k >= 1;
 			}
 		}
 		// U_0 = A^T bs: bsbar += A Ubar; gb = scl bsbar
 		apply(false, ub_, au_, s);
 		EW(k_add, m_, bsb_, au_, bsb_);
-		EW(k_scale, m_, (float)I.scl, bsb_, d_gb[i]);
+		EW(k_to32, m_, I.scl, bsb_, d_gb[i]);
 	}
 	std::vector<double> h(2 * (size_t)K_);
 	TG_CUDA(cudaMemcpyAsync(h.data(), gsc_, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s));
