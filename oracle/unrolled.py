@@ -22,6 +22,13 @@ updated after it (2d:673-694, 2d:820-842).  With the scaled data bs = scl b:
 S is the shrinkage (anisotropic 2d:588-611, or isotropic).  The adjoint
 below is derived by hand from these lines; tests check it against central
 finite differences of `forward` and against torch autograd.
+
+F is piecewise smooth: S has a kink where |Z| = 1/beta.  The adjoint is the
+derivative of the piece active at the point.  On large problems a central
+difference with step 1e-6 crosses some of the millions of kinks on its way
+(one crossing moves the quotient by up to 1e-2), so `forward(kinks=...)`
+can hold every shrinkage on the branches of a recorded point, as the step
+lengths and multiplier updates already are.
 """
 from __future__ import annotations
 
@@ -44,6 +51,24 @@ def shrink(Zx, Zy, t, iso):
         s = np.where(nrm > 0, np.maximum(nrm - t, 0.0) / np.where(nrm > 0, nrm, 1.0), 0.0)
         return s * Zx, s * Zy
     return (np.sign(Zx) * np.maximum(np.abs(Zx) - t, 0.0), np.sign(Zy) * np.maximum(np.abs(Zy) - t, 0.0))
+
+
+def shrink_on(Zx, Zy, t, iso):
+    """Where the shrinkage is off its zero branch (iso: one mask; aniso: one per component)."""
+    if iso:
+        return (np.sqrt(Zx * Zx + Zy * Zy) > t,)
+    return np.abs(Zx) > t, np.abs(Zy) > t
+
+
+def shrink_fixed(Zx, Zy, t, iso, on):
+    """The shrinkage with its branch held at `on` (from shrink_on at another
+    point): the smooth piece of S that is active there."""
+    if iso:
+        nrm = np.sqrt(Zx * Zx + Zy * Zy)
+        s = np.where(on[0], (nrm - t) / np.where(on[0], nrm, 1.0), 0.0)
+        return s * Zx, s * Zy
+    return (np.where(on[0], np.sign(Zx) * (np.abs(Zx) - t), 0.0),
+            np.where(on[1], np.sign(Zy) * (np.abs(Zy) - t), 0.0))
 
 
 def shrink_vjp(Zx, Zy, t, iso, Wbx, Wby):
@@ -79,11 +104,17 @@ class Unrolled:
         self.iso = bool(iso)
         self.K = len(self.steps)
 
-    def _state(self, U, sx, sy, dl, bs, mu, beta, o):
+    def _state(self, U, sx, sy, dl, bs, mu, beta, o, kinks=None, k=0):
         p, q = self.p, self.q
         Vx, Vy = D2(U, p, q)
         Zx, Zy = Vx - sx / beta, Vy - sy / beta
-        Wx, Wy = shrink(Zx, Zy, 1.0 / beta, self.iso)
+        if kinks is None:
+            Wx, Wy = shrink(Zx, Zy, 1.0 / beta, self.iso)
+        elif len(kinks) == k:      # recording
+            kinks.append(shrink_on(Zx, Zy, 1.0 / beta, self.iso))
+            Wx, Wy = shrink(Zx, Zy, 1.0 / beta, self.iso)
+        else:
+            Wx, Wy = shrink_fixed(Zx, Zy, 1.0 / beta, self.iso, kinks[k])
         Ex, Ey = Vx - Wx, Vy - Wy
         r = self.A(U) - bs
         if o:
@@ -91,18 +122,23 @@ class Unrolled:
         d = Dt2(Ex - sx / beta, Ey - sy / beta, p, q) + self.At((mu * r - dl) / beta)
         return sx, sy, dl, d, r
 
-    def forward(self, b, mu, beta, trajectory=False):
+    def forward(self, b, mu, beta, trajectory=False, kinks=None):
+        """U_K / scl.  kinks: None, or an empty list that this call fills with
+        the shrinkage branches it takes, or such a filled list, which then
+        holds every shrinkage on those branches (the map's smooth piece at the
+        point that recorded them, for finite differences that must not cross
+        a kink)."""
         bs = self.scl * np.asarray(b, np.float64)
         n = self.p * self.q
         U = self.At(bs)
         sx, sy, dl = np.zeros(n), np.zeros(n), np.zeros(bs.size)
         traj = []
-        sx, sy, dl, d, r = self._state(U, sx, sy, dl, bs, mu[0], beta[0], False)
+        sx, sy, dl, d, r = self._state(U, sx, sy, dl, bs, mu[0], beta[0], False, kinks, 0)
         traj.append((U, np.zeros(n), np.zeros(n), sx, sy, dl, r))
         for k in range(1, self.K + 1):
             U = U - self.steps[k - 1] * d
             s0x, s0y = sx, sy
-            sx, sy, dl, d, r = self._state(U, sx, sy, dl, bs, mu[k - 1], beta[k - 1], self.outer[k - 1])
+            sx, sy, dl, d, r = self._state(U, sx, sy, dl, bs, mu[k - 1], beta[k - 1], self.outer[k - 1], kinks, k)
             traj.append((U, s0x, s0y, sx, sy, dl, r))
         out = U / self.scl
         return (out, traj) if trajectory else out

@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 
 FWD_TOL = 1e-4      # U_K (FP32 replay) against the FP64 oracle, relative L2
 GRAD_TOL = 1e-3     # gradients (FP32 forward and adjoint) against the FP64 adjoint, relative L2
-FD_TOL = 1e-3       # directional derivatives against FP64 central differences
+FD_TOL = 1e-4       # directional derivatives against FP64 central differences (step 1e-6 relative)
 
 
 def _batch(side, T, count, iso, seed=11):
@@ -66,11 +66,21 @@ def _check(torch, side, T, count, K, ckpt, iso, n_dirs, mu, beta):
     errs["gmu"], errs["gbeta"] = relerr(tm.grad.numpy(), gmu_ref), relerr(tB.grad.numpy(), gbeta_ref)
     assert errs["gmu"] <= GRAD_TOL and errs["gbeta"] <= GRAD_TOL
 
-    # directional derivatives against central differences of the FP64 map
+    # directional derivatives against central differences of the FP64 map.
+    # The map is piecewise smooth (shrinkage kinks at |Z| = 1/beta); with
+    # 10^5-10^7 shrinkage evaluations a step of 1e-6 crosses a few kinks in
+    # some directions, so the differences run on the smooth piece of the
+    # unperturbed point: every shrinkage held on the branch it took there, as
+    # the step lengths and multiplier updates are.
     rng = np.random.default_rng(5)
+    kinks = []
+    for i, F in enumerate(Fs):
+        kinks.append([])
+        F.forward(b[i], mu, beta, kinks=kinks[i])
 
     def L(db, fm, fB):
-        return sum(0.5 * np.sum((F.forward(b[i] + db[i], mu * fm, beta * fB) - u[i]) ** 2) for i, F in enumerate(Fs))
+        return sum(0.5 * np.sum((F.forward(b[i] + db[i], mu * fm, beta * fB, kinks=kinks[i]) - u[i]) ** 2)
+                   for i, F in enumerate(Fs))
 
     hstep, sb = 1e-6, np.abs(b).mean()
     for _ in range(n_dirs):
@@ -89,10 +99,12 @@ def _check(torch, side, T, count, K, ckpt, iso, n_dirs, mu, beta):
 def test_unrolled_forward_and_adjoint(iso, torch_cuda):
     """32x32 ring, 3 instances, K = 20, varying (mu_k, beta_k), 64 directions."""
     mu, beta = _schedule(20)
-    _check(torch_cuda, 32, 32, 3, 20, 6, iso, 64, mu, beta)
+    errs = _check(torch_cuda, 32, 32, 3, 20, 6, iso, 64, mu, beta)
+    print("unrolled 32x32 iso=%d" % iso, {k: float(np.max(v)) for k, v in errs.items()})
 
 
 def test_unrolled_differentiation_config(torch_cuda):
     """128x128 ring, 256 transducers x 128 receivers (m = 32768), 8 instances,
-    K = 50 with a checkpoint every 10, (mu_k, beta_k) = (2^8, 2^5), 16 directions."""
-    _check(torch_cuda, 128, 256, 8, 50, 10, True, 16, np.full(50, 2.0 ** 8), np.full(50, 2.0 ** 5))
+    K = 50 with a checkpoint every 10, (mu_k, beta_k) = (2^8, 2^5), 64 directions."""
+    errs = _check(torch_cuda, 128, 256, 8, 50, 10, True, 64, np.full(50, 2.0 ** 8), np.full(50, 2.0 ** 5))
+    print("unrolled 128x128 K=50", {k: float(np.max(v)) for k, v in errs.items()})

@@ -105,3 +105,44 @@ def test_adjoint_matches_torch_autograd(iso):
     for got, ref in ((gb, tb.grad), (gmu, tm.grad), (gbeta, tB.grad)):
         ref = ref.numpy()
         assert np.linalg.norm(got - ref) <= AUTOGRAD_TOL * np.linalg.norm(ref)
+
+
+def test_kinks_held_fixed_on_a_large_case():
+    """128x128 ring (256 transducers x 128 receivers), K = 50 with the step
+    lengths of an oracle solve: a central difference with step 1e-6 crosses
+    shrinkage kinks in some directions; on the smooth piece of the point
+    (kinks held fixed) it matches the adjoint, and without a kink crossing
+    (step 1e-8) it matches as well."""
+    import oracle as O
+    from tval3g import workloads as W
+    side, K = 128, 50
+    w = W.ring2d(seed=11, side=side, T=256, tv_norm=1, normalize=True)
+    g, b, u = w["geom"], w["b"].astype(np.float64), w["u_true"].ravel()
+    op = O.Op.ray2d(g, side * side)
+    opts = W.options(2 ** 8, 2 ** 5, 1e-4, K, tv_norm=1)
+    r = O.solve(op, b, (side, side), opts, record=True)
+    steps = np.array([it[0] * opts["gamma"] ** it[3] for it in r.iters])[:K]
+    F = UR.Unrolled(lambda x: op.apply(x), lambda y: op.apply(y, True), (side, side), steps, np.zeros(K, bool),
+                    1.0, True)
+    mu, beta = np.full(K, 2.0 ** 8), np.full(K, 2.0 ** 5)
+    kinks = []
+    U = F.forward(b, mu, beta, kinks=kinks)
+    assert len(kinks) == K + 1
+    gb, gmu, gbeta = F.backward(b, mu, beta, U - u)
+    rng = np.random.default_rng(5)
+    sb = np.abs(b).mean()
+
+    def fd(h, vb, vm, vB, kk):
+        L = lambda s_: 0.5 * np.sum((F.forward(b + s_ * h * sb * vb, mu * (1 + s_ * h * vm), beta * (1 + s_ * h * vB),
+                                               kinks=kk) - u) ** 2)  # noqa: E731
+        return (L(1) - L(-1)) / (2 * h)
+
+    plain_1e6 = []
+    for _ in range(4):
+        vb, vm, vB = rng.standard_normal(b.size), rng.standard_normal(K), rng.standard_normal(K)
+        an = sb * np.dot(gb, vb) + np.dot(gmu, mu * vm) + np.dot(gbeta, beta * vB)
+        assert abs(fd(1e-6, vb, vm, vB, kinks) - an) <= 1e-6 * abs(an)
+        assert abs(fd(1e-8, vb, vm, vB, None) - an) <= 1e-5 * abs(an)
+        plain_1e6.append(abs(fd(1e-6, vb, vm, vB, None) - an) / abs(an))
+    # at least one of these directions crosses a kink with step 1e-6
+    assert max(plain_1e6) > 1e-4, plain_1e6
