@@ -79,9 +79,9 @@ CONFIGS = {
     "ring2d": {"workload": "2D ring 256x256, 512 transducers x 256 receivers (131072 rays, 2.72e7 hits), iso TV, "
                            "mu 2^10, beta 2^6, tol 1e-5, maxit 500; hit weight scale_factor = "
                            "1/sigma_max(A) so that mu and beta act as in TVAL3",
-               "operator": "on-the-fly Bresenham projector, shared-memory staged adjoint"},
+               "operator": "on-the-fly Bresenham projector, tiled pixel-major adjoint"},
     "dense2d": {"workload": "2D dense 64x64, A 1229x4096 N(0,1/m), iso TV, mu 2^8, beta 2^5, tol 1e-4, maxit 300",
-                "operator": "dense gemv pair"},
+                "operator": "dense normal product in one pass over A"},
     "hemi3d": {"workload": "3D 128^3, 2048 hemisphere transducers x 1024 random receivers (2.1M rays), aniso TV, "
                            "mu 2^10, beta 2^6, tol 1e-5, maxit 400; hit weight 1/sigma_max(A)",
                "operator": "on-the-fly 3D Bresenham projector, gather adjoint"},
@@ -255,32 +255,35 @@ def kernel_roofline(cx, capi, spec, w, kind):
     out_m = torch.empty(op.rows, device=dev)
     out_n = torch.empty(op.cols, device=dev)
     kt = {}
-    for name, (src, dst, tr) in {"forward": (x, out_m, False), "adjoint": (y, out_n, True)}.items():
+    dirs = {"forward": (x, out_m, 0), "adjoint": (y, out_n, 1)}
+    if kind == "dense":
+        dirs["normal"] = (x, out_n, 2)
+    for name, (src, dst, tr) in dirs.items():
         op.apply_n(src, dst, 3, trans=tr, stream=s)
         ts, _ = cx.event_time(lambda: op.apply_n(src, dst, 1, trans=tr, stream=s), 10)
         kt[name] = float(np.mean(ts))
-    nnz, n, m = op.nnz, op.cols, op.rows
+    nnz, n, m, index = op.nnz, op.cols, op.rows, op.adjoint_index_bytes
     op.close()
     peak, src = peak_hbm()
     if kind == "ray2d":
-        nrays = int(np.count_nonzero(w["geom"]["use_path"]))
-        nchunks = -(-nrays // 32768)
-        # staged adjoint: measurement vector once, traced-ray vector written and
-        # read once, 16-bit pixel->ray index, per-pixel chunk offsets, image once
-        bytes_ = 4 * m + 8 * nrays + 2 * nnz + 4 * n * (nchunks + 1) + 4 * n
-        kname, prof, direction = "k_ray_compact + k_ray_adj_staged (ray adjoint)", "ray_adjoint_staged_ring256.md", "adjoint"
+        # tiled adjoint: its index once (tile lists, 16-bit positions, offsets),
+        # the measurement vector once, the image once
+        bytes_ = index + 4 * m + 4 * n
+        kname, prof, direction = "k_ray_adj_tiled (ray adjoint)", "ray_adjoint_tiled_ring256.md", "adjoint"
     elif kind == "ray3d":
-        bytes_ = 4 * (n + 1) + 4 * nnz + 4 * m + 4 * n   # pixel pointers, ray ids, y once, image once
+        bytes_ = index + 4 * m + 4 * n   # pixel pointers and ray ids, y once, image once
         kname, prof, direction = "k_gather<ray adjoint>", "ray_adjoint_gather_hemi128.md", "adjoint"
     else:
         A = w["A"]
-        bytes_ = 4 * A.size + 4 * (A.shape[0] + A.shape[1])   # A once, x and y once
-        kname, prof, direction = "k_dense_fwd (A x)", "dense_gemv_64.md", "forward"
+        # the solve's normal product A^T (A u): A once, u read, Au written and
+        # read back, g written
+        bytes_ = 4 * A.size + 4 * (2 * A.shape[1] + 2 * A.shape[0])
+        kname, prof, direction = "k_dense_normal (A^T A u, A read once)", "dense_normal_64.md", "normal"
     achieved = bytes_ / (kt[direction] * 1e-3) / 1e9
     return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": profile_traffic(prof), "algorithmic_bytes": int(bytes_),
             "ms_per_launch": kt[direction], "peak_source": src,
-            "other_direction_ms_per_launch": kt["adjoint" if direction == "forward" else "forward"],
+            "ms_per_launch_by_direction": kt,
             "timing": "one launch per CUDA-event pair, 256 MB L2 flush before each"}
 
 

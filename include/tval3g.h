@@ -159,8 +159,11 @@ int tval3g_plan_set_target(tval3g_plan *plan, double target);
 int tval3g_plan_trace(const tval3g_plan *plan, int index, tval3g_trace_record *out, int cap, int *count);
 int tval3g_plan_destroy(tval3g_plan *plan);
 
-/* Operators alone.  tval3g_op_apply: y = A x (trans = 0) or y = A^T x
- * (trans = 1) with DEVICE x, y (lengths rows/cols as reported). */
+/* Operators alone.  tval3g_op_apply: y = A x (trans = 0), y = A^T x
+ * (trans = 1) or the normal product y = A^T (A x) of the solve's get_g_mult
+ * (trans = 2; a one-layer dense operator reads A once, as the reference's
+ * cache-blocked dense path, 2d/tval3_cpu_2d.cpp:361-394) with DEVICE x, y
+ * (lengths rows/cols as reported; both cols for trans = 2). */
 typedef struct tval3g_operator tval3g_operator;
 int tval3g_op_create(tval3g_operator **op, const tval3g_problem *prob, int flags);
 int tval3g_op_shape(const tval3g_operator *op, long long *rows, long long *cols, long long *nnz);
@@ -173,6 +176,12 @@ int tval3g_op_apply_n(tval3g_operator *op, int trans, const float *d_x, float *d
  * the Bresenham rasterisation, copied to HOST arrays rowptr [rows+1] and
  * colind [nnz]; with colind == NULL only rowptr is written. */
 int tval3g_op_ray_csr(const tval3g_operator *op, long long *rowptr, int *colind);
+/* Bytes of the index that one adjoint application (y = A^T x) reads besides
+ * x and y: the device-built CSC of a sparse operator, the pixel-major ray
+ * index of a ray operator (for 2D rays: the tile lists, the per-pixel 16-bit
+ * positions and their offsets), 0 for a dense operator.  No counterpart in
+ * the reference (its operators keep no derived index). */
+int tval3g_op_adjoint_index_bytes(const tval3g_operator *op, long long *bytes);
 int tval3g_op_destroy(tval3g_operator *op);
 
 /* Stencils on DEVICE arrays of an image dim_y x dim_x (x dim_z for dims 3).

@@ -126,6 +126,70 @@ def test_full_ring_operator_properties(torch_cuda):
     assert relerr(dx2.cpu().numpy(), dx.cpu().numpy()) < 1e-6
 
 
+@pytest.mark.parametrize("m, shape", [
+    (1229, (64, 64)),      # one band
+    (3000, (200, 200)),    # 21 bands of one row per CTA, A 480 MB
+    (100, (16, 20)),       # fewer rows than CTAs
+    (500, (31, 33)),       # n not a multiple of 4: scalar loads
+])
+def test_dense_normal_product(m, shape, torch_cuda):
+    """y = A^T (A x) in one pass over A (trans = 2) against the FP64 product
+    and against the two separate products; deterministic."""
+    torch = torch_cuda
+    rng = np.random.default_rng(m)
+    n = shape[0] * shape[1]
+    A = (rng.standard_normal((m, n), dtype=np.float32) / np.float32(np.sqrt(m)))
+    op = capi.Operator(capi.dense_problem(shape, A))
+    x = rng.standard_normal(n).astype(np.float32)
+    dx = _dev(torch, x)
+    y = torch.empty(n, device="cuda")
+    op.apply(dx, y, trans=2)
+    A64 = A.astype(np.float64)
+    ref = A64.T @ (A64 @ x.astype(np.float64))
+    assert relerr(y.cpu().numpy(), ref) < 1e-5
+    au = torch.empty(m, device="cuda")
+    y2 = torch.empty(n, device="cuda")
+    op.apply(dx, au)
+    op.apply(au, y2, trans=True)
+    assert relerr(y.cpu().numpy(), y2.cpu().numpy()) < 1e-5
+    y3 = torch.empty(n, device="cuda")
+    op.apply(dx, y3, trans=2)
+    assert torch.equal(y, y3)
+
+
+def _random_rays(rng, H, ld, E, R, frac):
+    return dict(use_path=(rng.uniform(size=E * R) < frac).astype(np.int32),
+                xe=rng.integers(0, ld, E), ye=rng.integers(0, H, E),
+                xr=rng.integers(0, ld, R), yr=rng.integers(0, H, R), ld=ld, scale=0.75)
+
+
+@pytest.mark.parametrize("H, ld, E, R, frac", [
+    (50, 37, 40, 30, 0.7),      # tiles cut by both image edges
+    (17, 300, 25, 40, 0.5),     # one tile row and a partial one
+    (40, 40, 640, 480, 0.9),    # 276480 traced rays: beyond the tiled index, pixel-major gather
+])
+def test_ray2d_adjoint_ragged_and_large(H, ld, E, R, frac, torch_cuda):
+    """The 2D ray adjoint on images that the 16x16 pixel tiles do not divide,
+    and past the tiled index's ray limit, against the FP64 oracle."""
+    torch = torch_cuda
+    rng = np.random.default_rng(H * ld + E)
+    g = _random_rays(rng, H, ld, E, R, frac)
+    op = capi.Operator(capi.ray2d_problem((H, ld), g))
+    ref_op = O.Op.ray2d(g, H * ld)
+    y = rng.standard_normal(op.rows).astype(np.float32)
+    dx = torch.empty(op.cols, device="cuda")
+    op.apply(_dev(torch, y), dx, trans=True)
+    assert relerr(dx.cpu().numpy(), ref_op.apply(y.astype(np.float64), trans=True)) < 1e-5
+    x = rng.standard_normal(op.cols).astype(np.float32)
+    dy = torch.empty(op.rows, device="cuda")
+    op.apply(_dev(torch, x), dy)
+    assert relerr(dy.cpu().numpy(), ref_op.apply(x.astype(np.float64))) < 1e-5
+    dx2 = torch.empty(op.cols, device="cuda")
+    op.apply(_dev(torch, y), dx2, trans=True)
+    assert torch.equal(dx, dx2)
+    assert op.adjoint_index_bytes > 0
+
+
 @pytest.mark.parametrize("shape", [(5, 7), (16, 16), (3, 4, 5), (8, 6, 4)])
 def test_stencils_match_oracle(shape, torch_cuda):
     torch = torch_cuda

@@ -24,6 +24,8 @@ struct tval3g_operator {
 	Ctrl *d_ctrl = nullptr;
 	int2 *d_tiles = nullptr;
 	float *d_part = nullptr;
+	int *d_fused = nullptr;   // band flags and error word of the one-pass dense normal product
+	float *d_au = nullptr;    // A x of a normal product (trans = 2)
 	cudaStream_t s = nullptr;
 	long long rows = 0, cols = 0;
 };
@@ -219,6 +221,12 @@ int tval3g_op_create(tval3g_operator **out, const tval3g_problem *prob, int flag
 			TG_CUDA(cudaMalloc(&op->d_part, sizeof(float) * dense_part));
 			op->ob.dense_part = op->d_part;
 		}
+		if (op->ob.fused_words > 0) {
+			TG_CUDA(cudaMalloc(&op->d_fused, sizeof(int) * op->ob.fused_words));
+			TG_CUDA(cudaMemsetAsync(op->d_fused, 0, sizeof(int) * op->ob.fused_words, op->s));
+			op->ob.fused_flags = op->d_fused;
+		}
+		TG_CUDA(cudaMalloc(&op->d_au, sizeof(float) * std::max<long long>(op->rows, 1)));
 		TG_CUDA(cudaMalloc(&op->d_inst, sizeof(Inst)));
 		TG_CUDA(cudaStreamSynchronize(op->s));
 	} catch (...) {
@@ -239,6 +247,13 @@ int tval3g_op_shape(const tval3g_operator *op, long long *rows, long long *cols,
 	CAPI_END
 }
 
+int tval3g_op_adjoint_index_bytes(const tval3g_operator *op, long long *bytes) {
+	CAPI_BEGIN
+	TG_ARG(op && bytes, "Argument error: NULL argument");
+	*bytes = op->st.adj_index_bytes;
+	CAPI_END
+}
+
 int tval3g_op_apply(tval3g_operator *op, int trans, const float *d_x, float *d_y, void *stream) {
 	int rc = tval3g_op_apply_n(op, trans, d_x, d_y, 1, stream);
 	if (rc != TVAL3G_OK) return rc;
@@ -254,8 +269,36 @@ int tval3g_op_apply_n(tval3g_operator *op, int trans, const float *d_x, float *d
 	TG_ARG(op && d_x && d_y && reps >= 1, "Argument error: NULL argument or reps < 1");
 	cudaStream_t s = stream ? (cudaStream_t)stream : op->s;
 	Inst I = op->h;
+	TG_ARG(trans >= 0 && trans <= 2, "Argument error: trans must be 0, 1 or 2");
 	// x lives in the bank of its length: image vectors vn, measurement vectors vm
 	VecSel xs, ys;
+	if (trans == 2) {   // y = A^T (A x): vn[0] = x, vm[0] = A x, vn[1] = y
+		I.vn[0] = const_cast<float *>(d_x); I.vm[0] = op->d_au; I.vn[1] = d_y;
+		if (op->st.dev.kind == TVAL3G_OP_RAY2D || op->st.dev.kind == TVAL3G_OP_RAY3D)
+			TG_CUDA(cudaMemsetAsync(op->d_au, 0, sizeof(float) * op->rows, s));
+		TG_CUDA(cudaMemcpyAsync(op->d_inst, &I, sizeof(Inst), cudaMemcpyHostToDevice, s));
+		LaunchCtx L{s, op->d_inst, nullptr};
+		// the one-pass dense kernel reads x as float4: a misaligned x takes the two products
+		const bool aligned = (reinterpret_cast<uintptr_t>(d_x) & 15) == 0;
+		for (int r = 0; r < reps; r++) {
+			if (aligned) {
+				op_normal(L, op->ob, P_ALL, VecSel{false, 0}, VecSel{true, 0}, VecSel{false, 1});
+			} else {
+				op_forward(L, op->ob, P_ALL, VecSel{false, 0}, VecSel{true, 0});
+				op_adjoint(L, op->ob, P_ALL, VecSel{true, 0}, VecSel{false, 1});
+			}
+		}
+		if (op->ob.fused_flags) {
+			int e = 0;
+			TG_CUDA(cudaMemcpyAsync(&e, op->d_fused + op->ob.fused_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+			TG_CUDA(cudaStreamSynchronize(s));
+			if (e) {
+				TG_CUDA(cudaMemsetAsync(op->d_fused + op->ob.fused_err, 0, sizeof(int), s));
+				throw Error{TVAL3G_ERR_CUDA, "dense normal product: a bounded wait timed out (results invalid)"};
+			}
+		}
+		return TVAL3G_OK;
+	}
 	if (!trans) {
 		I.vn[0] = const_cast<float *>(d_x); I.vm[0] = d_y;
 		xs = VecSel{false, 0}; ys = VecSel{true, 0};
@@ -304,6 +347,8 @@ int tval3g_op_destroy(tval3g_operator *op) {
 		cudaFree(op->d_ctrl);
 		cudaFree(op->d_tiles);
 		cudaFree(op->d_part);
+		cudaFree(op->d_fused);
+		cudaFree(op->d_au);
 		if (op->s) cudaStreamDestroy(op->s);
 		delete op;
 	}

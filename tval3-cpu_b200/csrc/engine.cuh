@@ -110,6 +110,8 @@ struct OpDev {
 	const float *A;
 	int mrhs;              // layers on the tcgen05 3xTF32 path (mrhs.cu) instead of the gemv kernels
 	int dense_kchunks;     // row chunks of the transposed product
+	int fused_rpc;         // rows per CTA per band of the one-pass normal product (0: not used)
+	int fused_slab;        // its column slab per CTA
 	long long dense_part;  // offset of this instance in the dense partial buffer (floats)
 	// compressed gather operators: forward rows (CSR) and transpose (CSC)
 	const int *rptr, *rind;
@@ -121,24 +123,30 @@ struct OpDev {
 	int nrays;
 	const int4 *rays;
 	int rvx, rvy;           // index = x + y*rvx + z*rvx*rvy (2D: rvx = ld)
-	// 2D ray adjoint staged through shared memory (nchunks > 0): the traced
-	// rays are cut into chunks of RAY_CHUNK; for pixel p and chunk c the hits
-	// are sidx[soff[p*(nchunks+1)+c] .. soff[p*(nchunks+1)+c+1]) as 16-bit
-	// offsets of the ray within the chunk, in ray order
-	int nchunks;
-	int ppb;                // pixels per block of the staged adjoint
-	const unsigned short *sidx;
-	const int *soff;
-	const int *live_out;    // measurement index of each traced ray
-	float *ylive;           // scratch: the adjoint's input compacted to traced rays
+	// 2D ray adjoint over pixel tiles (tiled != 0): the image is cut into
+	// RAYT x RAYT tiles, ntx per row; tile t lists the measurement indices of
+	// the rays that cross it, tmeas[tptr[t] .. tptr[t+1]), in traced order,
+	// and each pixel lists its hits as 16-bit 1-based positions in its tile's
+	// list (0: a pad entry), eight to a 16-byte word.  Thread r of tile t's
+	// block takes pixel tperm[256 t + r] (row-major in the tile; pixels by
+	// decreasing list length); the words of warp w's 32 pixels (tile t's
+	// warps are 8t .. 8t+7) are interleaved: word v of lane l is
+	// sidx[woff[w] + 32 v + l]
+	int tiled;
+	int ntx;
+	int tmax;               // longest tile list
+	const int *tptr, *tmeas, *woff;
+	const uint4 *sidx;
+	const unsigned char *tperm;
 	// 2D forward: y-driven rays read a transposed copy of the image (rows of
 	// length tH = n / ld), in which their steps are contiguous; NULL = off
 	float *xT;
 	int tH;
 };
 
-constexpr int RAY_CHUNK = 32768;       // rays per shared-memory chunk (128 KB)
-constexpr int RAY_MAX_CHUNKS = 8;      // staged adjoint up to 262144 traced rays
+constexpr int RAYT = 16;                // tile side of the tiled 2D ray adjoint
+constexpr int RAYT_MAX_RAYS = 1 << 18;  // its index builder keeps a bitmap of the traced rays in shared memory
+constexpr int RAYT_MAX_LIST = 57344;    // rays per tile: 16-bit positions, 224 KB of shared memory
 
 // Unsigned 32-bit division by a run-time constant with one multiply-high
 // (Granlund & Montgomery, "Division by invariant integers using
@@ -180,9 +188,14 @@ struct Inst {
 	OpDev op;
 };
 
-constexpr int TILE = 512;        // elements per tile (256 threads x 2)
+// Tiles: image vectors one element per thread (a 256^2 image is 256 blocks),
+// measurement vectors four (their kernels do little per element, and fewer
+// tiles contend less for the instance's reduction ticket)
+constexpr int TILE = 256;
+constexpr int TILE_M = 1024;
 constexpr int BLOCK = 256;
 constexpr int EPT = TILE / BLOCK;
+constexpr int EPT_M = TILE_M / BLOCK;
 constexpr int NSUM = 6;          // partial sums per tile
 constexpr int TRACE_DOUBLES = (int)(sizeof(tval3g_trace_record) / sizeof(double));
 
@@ -193,6 +206,35 @@ struct TileMap {
 	const int2 *tiles = nullptr;  // (instance, local tile); local >= ntn means an m tile (MAP_NM)
 	int count = 0;
 };
+
+// ---------------------------------------------------------------------------
+// programmatic dependent launch.  The solve's kernels are launched with
+// programmatic stream serialisation (launch_pdl): each lets the next kernel
+// of its stream launch as soon as all of its blocks are running
+// (pdl_launch_next, first thing), and the next kernel's blocks load their
+// tile and instance descriptors meanwhile, then wait in pdl_wait_prev - in
+// every block, before the first read of anything an earlier kernel wrote and
+// before any early return - for the previous kernel to finish and its writes
+// to be visible.  Without the launch attribute both are no-ops.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_launch_next() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait_prev() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KParams, typename... Args>
+inline void launch_pdl(void (*kern)(KParams...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args... args) {
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = grid;
+	cfg.blockDim = block;
+	cfg.dynamicSmemBytes = smem;
+	cfg.stream = s;
+	cudaLaunchAttribute at[1];
+	at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	at[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = at;
+	cfg.numAttrs = 1;
+	TG_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KParams>(args)...));
+}
 
 // ---------------------------------------------------------------------------
 // device helpers
@@ -280,7 +322,11 @@ struct VecSel {
 };
 
 struct OpBatch;   // per-kind launch data, built by the plan
-void op_forward(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y);
-void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y);
+// unfused: leave out the dense instances of the one-pass normal product;
+// xT_ready: the 2D ray operators' transposed image already holds x (k_descend
+// wrote it), so the forward skips its transpose
+void op_forward(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y, bool unfused = false,
+                bool xT_ready = false);
+void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y, bool unfused = false);
 
 }  // namespace tval3g

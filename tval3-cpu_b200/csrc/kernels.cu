@@ -14,15 +14,21 @@ namespace tval3g {
 // prologue / image geometry
 // ---------------------------------------------------------------------------
 #define KPROLOGUE(a)                                                                        \
+	pdl_launch_next();                                                                      \
 	if ((a).launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd((a).launches, 1ull); \
 	const int2 tl_ = (a).map.tiles[blockIdx.x];                                             \
 	const Inst I = (a).tab[tl_.x];                                                          \
 	const int local = tl_.y;                                                                \
+	pdl_wait_prev();                                                                        \
 	if (!pred_ok(*I.ctrl, (a).pred)) return;
 
-// element k of this thread in a tile starting at i0
+// element k of this thread in a tile of image elements starting at i0
 #define FOR_TILE(i0, len, i)                                  \
 	_Pragma("unroll") for (int k_ = 0; k_ < EPT; k_++)        \
+		if (const int i = (i0) + (int)threadIdx.x + k_ * BLOCK; i < (len))
+// the same over a tile of measurement elements (TILE_M = BLOCK x EPT_M)
+#define FOR_TILE_M(i0, len, i)                                \
+	_Pragma("unroll") for (int k_ = 0; k_ < EPT_M; k_++)      \
 		if (const int i = (i0) + (int)threadIdx.x + k_ * BLOCK; i < (len))
 
 struct Geo {
@@ -70,21 +76,26 @@ __device__ __forceinline__ float dt_at(const Geo &g, int i, int x, int y, int z,
 
 // shrinkage of one pixel: anisotropic 2d:588-611 / 3d:834-871; isotropic:
 // W = max(|Ubar|_2 - 1/beta, 0) * Ubar / |Ubar|_2 (no reference counterpart)
+//
+// sigma / beta is formed as sigma * (1 / beta): identical to the reference's
+// division whenever beta is a power of two (beta0 = 2^k and rate_cnt = 2
+// keep it one), within one rounding otherwise.
 struct Shrink {
-	float beta, thr;
+	float rbeta, thr;
 	int iso, dims;
 	__device__ Shrink(const Inst &I, double beta_d)
-		: beta((float)beta_d), thr((float)(1.0 / beta_d)), iso(I.tv_norm), dims(I.dims) {}
+		: rbeta((float)(1.0 / beta_d)), thr((float)(1.0 / beta_d)), iso(I.tv_norm), dims(I.dims) {}
 	__device__ __forceinline__ float apply(const float (&u)[3], const float (&s)[3], float (&w)[3]) const {
 		float ub[3];
 #pragma unroll
-		for (int c = 0; c < 3; c++) ub[c] = (c < dims) ? u[c] - s[c] / beta : 0.f;
+		for (int c = 0; c < 3; c++) ub[c] = (c < dims) ? u[c] - s[c] * rbeta : 0.f;
 		if (iso) {
 			float nrm = sqrtf(ub[0] * ub[0] + ub[1] * ub[1] + ub[2] * ub[2]);
 			float t = nrm - thr;
 			t = t >= 0.f ? t : 0.f;
+			const float sc = nrm > 0.f ? t / nrm : 0.f;
 #pragma unroll
-			for (int c = 0; c < 3; c++) w[c] = nrm > 0.f ? t * ub[c] / nrm : 0.f;
+			for (int c = 0; c < 3; c++) w[c] = sc * ub[c];
 			return t;
 		}
 		float lam = 0.f;
@@ -96,24 +107,6 @@ struct Shrink {
 			w[c] = ub[c] >= 0.f ? t : -t;
 		}
 		return lam;
-	}
-	// component c (compile-time after inlining) of W at j, from U_c, sigma_c
-	__device__ __forceinline__ float comp(const float *const (&U)[3], const float *const (&S)[3], int j,
-	                                      int c) const {
-		if (iso) {
-			float u[3], s[3], w[3];
-#pragma unroll
-			for (int cc = 0; cc < 3; cc++) {
-				u[cc] = cc < dims ? U[cc][j] : 0.f;
-				s[cc] = cc < dims ? S[cc][j] : 0.f;
-			}
-			apply(u, s, w);
-			return w[c];
-		}
-		float ub = U[c][j] - S[c][j] / beta;
-		float t = fabsf(ub) - thr;
-		t = t >= 0.f ? t : 0.f;
-		return ub >= 0.f ? t : -t;
 	}
 };
 
@@ -131,10 +124,10 @@ __device__ __forceinline__ void better_max(float &a, int &ia, float b, int ib) {
 
 __global__ void __launch_bounds__(BLOCK) k_scaleb(KArgs a) {
 	KPROLOGUE(a);
-	const int m = (int)I.m, i0 = local * TILE;
+	const int m = (int)I.m, i0 = local * TILE_M;
 	float mn = INFINITY, mx = -INFINITY;
 	int imn = INT_MAX, imx = INT_MAX;
-	FOR_TILE(i0, m, i) {
+	FOR_TILE_M(i0, m, i) {
 		float v = fabsf(I.b_user[i]);
 		better_min(mn, imn, v, i);
 		better_max(mx, imx, v, i);
@@ -213,7 +206,7 @@ __global__ void __launch_bounds__(BLOCK) k_init(KArgs a) {
 		}
 	} else {
 		const float scl = (float)c.scl;
-		FOR_TILE((local - I.ntn) * TILE, (int)I.m, i) {
+		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) {
 #pragma unroll
 			for (int v = 0; v < NVM; v++) I.vm[v][i] = 0.f;
 			I.vm[vB][i] = scl != 1.f ? I.b_user[i] * scl : I.b_user[i];
@@ -247,39 +240,28 @@ __global__ void __launch_bounds__(BLOCK) k_D(KArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// update_W (2d:651-671): shrinkage, then g2 = Dt(DU - W), lam1, lam2, lam4.
-// The neighbours' W needed by Dt are recomputed from their U and sigma.
+// update_W (2d:651-671), first part: shrinkage W, lam1, lam2, lam4.  The
+// second part, g2 = Dt(DU - W), needs the neighbours' W and runs in k_grad,
+// the next kernel of the iteration, from the stored W.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(BLOCK) k_shrink_g2(KArgs a) {
+__global__ void __launch_bounds__(BLOCK) k_shrink(KArgs a) {
 	KPROLOGUE(a);
-	Geo g(I);
 	Ctrl &c = *I.ctrl;
 	Shrink sh(I, c.beta);
-	const float *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
-	const float *const Sc[3] = {I.vn[vSx], I.vn[vSy], I.vn[vSz]};
-	float *const Wc[3] = {I.vn[vWx], I.vn[vWy], I.vn[vWz]};
-	float *__restrict__ g2 = I.vn[vG2];
+	const int n = (int)I.n, dims = I.dims;
 	double v[3] = {0, 0, 0};   // lam1, lam2, lam4
-	FOR_TILE(local * TILE, g.n, i) {
-		int x, y, z;
-		g.coords(i, x, y, z);
+	FOR_TILE(local * TILE, n, i) {
 		float u[3], s[3], w[3];
 #pragma unroll
 		for (int cc = 0; cc < 3; cc++) {
-			u[cc] = cc < g.dims ? Uc[cc][i] : 0.f;
-			s[cc] = cc < g.dims ? Sc[cc][i] : 0.f;
+			u[cc] = cc < dims ? I.vn[vUx + cc][i] : 0.f;
+			s[cc] = cc < dims ? I.vn[vSx + cc][i] : 0.f;
 		}
 		v[0] += sh.apply(u, s, w);
 #pragma unroll
 		for (int cc = 0; cc < 3; cc++)
-			if (cc < g.dims) Wc[cc][i] = w[cc];
-		auto V = [&](int cc) {
-			return [&, cc](int j) { return j == i ? u[cc] - w[cc] : Uc[cc][j] - sh.comp(Uc, Sc, j, cc); };
-		};
-		g2[i] = dt_at(g, i, x, y, z, V(0), V(1), V(2));
-#pragma unroll
-		for (int cc = 0; cc < 3; cc++)
-			if (cc < g.dims) {
+			if (cc < dims) {
+				I.vn[vWx + cc][i] = w[cc];
 				float vv = u[cc] - w[cc];
 				v[1] += (double)vv * vv;
 				v[2] += (double)s[cc] * vv;
@@ -301,10 +283,34 @@ __global__ void __launch_bounds__(BLOCK) k_shrink_g2(KArgs a) {
 	}
 }
 
+// component cc of D U at j, from U (2d:268-278, 3d:365-389)
+__device__ __forceinline__ float du_at(const float *__restrict__ U, const Geo &g, int j, int cc) {
+	int x, y, z;
+	g.coords(j, x, y, z);
+	return cc == 0 ? dxf(U, g, j, x) : cc == 1 ? dyf(U, g, j, y) : dzf(U, g, j, z);
+}
+
+// g2 at i: Dt(DU - W) with D U formed from U here (2d:280-293)
+__device__ __forceinline__ float g2_at_u(const Inst &I, const Geo &g, int i, int x, int y, int z) {
+	const float *__restrict__ U = I.vn[vU];
+	const float *const Wc[3] = {I.vn[vWx], I.vn[vWy], I.vn[vWz]};
+	auto V = [&](int cc) { return [&, cc](int j) { return du_at(U, g, j, cc) - Wc[cc][j]; }; };
+	return dt_at(g, i, x, y, z, V(0), V(1), V(2));
+}
+
+// g2 at i: Dt(DU - W) from the stored gradient components and W (2d:280-293)
+__device__ __forceinline__ float g2_at(const Inst &I, const Geo &g, int i, int x, int y, int z) {
+	const float *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
+	const float *const Wc[3] = {I.vn[vWx], I.vn[vWy], I.vn[vWz]};
+	auto V = [&](int cc) { return [&, cc](int j) { return Uc[cc][j] - Wc[cc][j]; }; };
+	return dt_at(g, i, x, y, z, V(0), V(1), V(2));
+}
+
 // ---------------------------------------------------------------------------
 // get_g epilogue (2d:396-423): g -= Atb; V = DU - W; g2 = Dt V; lam2, lam4;
 // Aub = Au - b; lam3, lam5; f.  Descent stage also runs the Armijo test
-// (2d:543-548).
+// (2d:543-548).  The gradient components (Ux, Uy[, Uz]) = D U of the new U
+// (the end of descend, 2d:481-493) are formed here and stored.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
 	KPROLOGUE(a);
@@ -312,7 +318,8 @@ __global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
 	double v[4] = {0, 0, 0, 0};   // lam2, lam4, lam3, lam5
 	if (local < I.ntn) {
 		Geo g(I);
-		const float *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
+		const float *__restrict__ U = I.vn[vU];
+		float *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
 		const float *const Wc[3] = {I.vn[vWx], I.vn[vWy], I.vn[vWz]};
 		const float *const Sc[3] = {I.vn[vSx], I.vn[vSy], I.vn[vSz]};
 		float *__restrict__ gv = I.vn[vG];
@@ -322,19 +329,20 @@ __global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
 			int x, y, z;
 			g.coords(i, x, y, z);
 			gv[i] = gv[i] - atb[i];
-			auto V = [&](int cc) { return [&, cc](int j) { return Uc[cc][j] - Wc[cc][j]; }; };
-			g2[i] = dt_at(g, i, x, y, z, V(0), V(1), V(2));
+			g2[i] = g2_at_u(I, g, i, x, y, z);
+			float du[3] = {dxf(U, g, i, x), dyf(U, g, i, y), g.dims == 3 ? dzf(U, g, i, z) : 0.f};
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++)
 				if (cc < g.dims) {
-					float vv = Uc[cc][i] - Wc[cc][i];
+					Uc[cc][i] = du[cc];
+					float vv = du[cc] - Wc[cc][i];
 					v[0] += (double)vv * vv;
 					v[1] += (double)Sc[cc][i] * vv;
 				}
 		}
 	} else {
 		const float *__restrict__ au = I.vm[vAu], *__restrict__ bb = I.vm[vB], *__restrict__ dl = I.vm[vDelta];
-		FOR_TILE((local - I.ntn) * TILE, (int)I.m, i) {
+		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) {
 			float r = au[i] - bb[i];
 			v[2] += (double)r * r;
 			v[3] += (double)dl[i] * r;
@@ -364,7 +372,8 @@ __global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
 
 // ---------------------------------------------------------------------------
 // get_gradient (2d:578-585) and the inner stopping test (2d:803-817)
-//   ST_LOOP:  uup = U - Up; d = DtsAtd + g2 + muDbeta*g; RelChg
+//   ST_LOOP:  g2 = Dt(DU - W) (the end of update_W, 2d:651-671);
+//             uup = U - Up; d = DtsAtd + g2 + muDbeta*g; RelChg
 //   ST_INIT:  d = DtsAtd + g2 + muDbeta*g (DtsAtd = 0); Q = 1, C = f
 //   ST_OUTER: DtsAtd = (beta0/beta) d; d = ... (2d:844-852)
 // ---------------------------------------------------------------------------
@@ -380,7 +389,17 @@ __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 	const bool ut = a.stage == ST_LOOP && I.ut_user && (I.trace || I.target > 0);
 	const float scl = (float)c.scl;
 	double v[5] = {0, 0, 0, 0, 0};   // |d|^2, |Up|^2, |uup|^2, |U/scl - Ut|^2, |Ut|^2
+	Geo geo(I);
 	FOR_TILE(local * TILE, (int)I.n, i) {
+		float g2i;
+		if (a.stage == ST_LOOP) {
+			int x, y, z;
+			geo.coords(i, x, y, z);
+			g2i = g2_at(I, geo, i, x, y, z);
+			I.vn[vG2][i] = g2i;
+		} else {
+			g2i = g2[i];
+		}
 		if (ut) {
 			float t = I.ut_user[i];
 			float e = U[i] / scl - t;
@@ -392,7 +411,7 @@ __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 			t = d[i] * bscale;
 			dts[i] = t;
 		}
-		float dv = t + g2[i];
+		float dv = t + g2i;
 		dv = fmaf(mdb, gv[i], dv);
 		d[i] = dv;
 		v[0] += (double)dv * dv;
@@ -493,7 +512,7 @@ __global__ void __launch_bounds__(BLOCK) k_tau_first(KArgs a) {
 	Ctrl &c = *I.ctrl;
 	double v[1] = {0};
 	const float *__restrict__ ad = I.vm[vAd];
-	FOR_TILE(local * TILE, (int)I.m, i) {
+	FOR_TILE_M(local * TILE_M, (int)I.m, i) {
 		float t = ad[i];
 		v[0] += (double)t * t;
 	}
@@ -506,7 +525,9 @@ __global__ void __launch_bounds__(BLOCK) k_tau_first(KArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// descend (2d:481-493) with the snapshot of min_u (2d:536-537):
+// descend (2d:481-493) with the snapshot of min_u (2d:536-537); for a 2D ray
+// operator it also writes the new U transposed (OpDev::xT), which the
+// forward projection that follows reads for its y-driven rays:
 //   ST_DESCEND: Up=U, gp=g, g2p=g2, U[xyz]p=U[xyz], Aup=Au; U = U - tau d
 //   ST_RESTART: U = Up - tau d (2d:565-566)
 // then nonneg (2d:455-465)
@@ -520,6 +541,8 @@ __global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
 	if (local < I.ntn) {
 		float *__restrict__ U = I.vn[vU], *__restrict__ Up = I.vn[vUp];
 		const float *__restrict__ d = I.vn[vD];
+		float *__restrict__ xT = I.op.xT;   // 2D ray operators: the new U transposed for the forward
+		const int ld = I.op.rvx, tH = I.op.tH;   // the geometry's row length (its ld)
 		FOR_TILE(local * TILE, (int)I.n, i) {
 			float u;
 			if (snap) {
@@ -538,9 +561,13 @@ __global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
 			u = fmaf(ntau, d[i], u);
 			if (I.nonneg) u = u < 0.f ? 0.f : u;
 			U[i] = u;
+			if (xT) {
+				const int row = i / ld;
+				xT[row + (i - row * ld) * tH] = u;
+			}
 		}
 	} else if (snap) {
-		FOR_TILE((local - I.ntn) * TILE, (int)I.m, i) I.vm[vAup][i] = I.vm[vAu][i];
+		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) I.vm[vAup][i] = I.vm[vAu][i];
 	}
 }
 
@@ -557,7 +584,7 @@ __global__ void __launch_bounds__(BLOCK) k_bt_diff(KArgs a) {
 				if (cc < I.dims) I.vn[vdUx + cc][i] = I.vn[vUx + cc][i] - I.vn[vUxp + cc][i];
 		}
 	} else {
-		FOR_TILE((local - I.ntn) * TILE, (int)I.m, i) I.vm[vdAu][i] = I.vm[vAu][i] - I.vm[vAup][i];
+		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) I.vm[vdAu][i] = I.vm[vAu][i] - I.vm[vAup][i];
 	}
 }
 
@@ -584,7 +611,7 @@ __global__ void __launch_bounds__(BLOCK) k_lerp(KArgs a) {
 				}
 		}
 	} else {
-		FOR_TILE((local - I.ntn) * TILE, (int)I.m, i) {
+		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) {
 			float au = fmaf(al, I.vm[vdAu][i], I.vm[vAup][i]);
 			I.vm[vAu][i] = au;
 			float r = au - I.vm[vB][i];
@@ -655,7 +682,7 @@ __global__ void __launch_bounds__(BLOCK) k_mlp(KArgs a) {
 				}
 		}
 	} else {
-		FOR_TILE((local - I.ntn) * TILE, (int)I.m, i) {
+		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) {
 			float r = I.vm[vAu][i] - I.vm[vB][i];
 			float dl = fmaf(nmu, r, I.vm[vDelta][i]);
 			I.vm[vDelta][i] = dl;
@@ -707,7 +734,7 @@ __global__ void __launch_bounds__(BLOCK) k_skip_norms(KArgs a) {
 	if (!I.skip_enabled) return;
 	Ctrl &c = *I.ctrl;
 	double v[2] = {0, 0};
-	FOR_TILE(local * TILE, (int)I.m, i) {
+	FOR_TILE_M(local * TILE_M, (int)I.m, i) {
 		float au = I.vm[vAu][i];
 		float dl = au - I.vm[vLastAu][i];
 		v[0] += (double)dl * dl;
@@ -728,12 +755,14 @@ __global__ void __launch_bounds__(BLOCK) k_skip_norms(KArgs a) {
 __global__ void __launch_bounds__(BLOCK) k_copy_lastau(KArgs a) {
 	KPROLOGUE(a);
 	if (!I.skip_enabled) return;
-	FOR_TILE(local * TILE, (int)I.m, i) I.vm[vLastAu][i] = I.vm[vAu][i];
+	FOR_TILE_M(local * TILE_M, (int)I.m, i) I.vm[vLastAu][i] = I.vm[vAu][i];
 }
 
 __global__ void k_cond(const Inst *tab, int count, int pred, int *flag, unsigned long long handle,
                        unsigned long long *launches) {
+	pdl_launch_next();
 	if (launches && threadIdx.x == 0) atomicAdd(launches, 1ull);
+	pdl_wait_prev();
 	int any = 0;
 	for (int i = threadIdx.x; i < count; i += blockDim.x) any |= pred_ok(*tab[i].ctrl, pred) ? 1 : 0;
 	any = __syncthreads_or(any);
@@ -746,7 +775,9 @@ __global__ void k_cond(const Inst *tab, int count, int pred, int *flag, unsigned
 // schedule mode: the coming iteration's (mu_k, beta_k) from the schedule, and
 // the ratio by which DtsAtd = -(Dt sigma + At delta) / beta must be rescaled
 __global__ void k_sched(const Inst *tab, int count, unsigned long long *launches) {
+	pdl_launch_next();
 	if (launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);
+	pdl_wait_prev();
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= count) return;
 	const Inst &I = tab[i];
@@ -825,14 +856,13 @@ __global__ void k_shrink_plain(int dims, long long n, int iso, double beta, cons
 #define LAUNCHER(name, kern)                                                  \
 	void name(cudaStream_t s, const KArgs &a) {                               \
 		if (a.map.count <= 0) return;                                         \
-		kern<<<a.map.count, BLOCK, 0, s>>>(a);                                \
-		TG_CUDA(cudaGetLastError());                                          \
+		launch_pdl(kern, a.map.count, BLOCK, 0, s, a);                        \
 	}
 LAUNCHER(launch_scaleb, k_scaleb)
 LAUNCHER(launch_init, k_init)
 LAUNCHER(launch_init_u, k_init_u)
 LAUNCHER(launch_D, k_D)
-LAUNCHER(launch_shrink_g2, k_shrink_g2)
+LAUNCHER(launch_shrink, k_shrink)
 LAUNCHER(launch_getg, k_getg)
 LAUNCHER(launch_grad, k_grad)
 LAUNCHER(launch_tau_prep, k_tau_prep)
@@ -847,14 +877,12 @@ LAUNCHER(launch_skip_norms, k_skip_norms)
 LAUNCHER(launch_copy_lastau, k_copy_lastau)
 
 void launch_sched(cudaStream_t s, const Inst *tab, int count, unsigned long long *launches) {
-	k_sched<<<(count + 127) / 128, 128, 0, s>>>(tab, count, launches);
-	TG_CUDA(cudaGetLastError());
+	launch_pdl(k_sched, (count + 127) / 128, 128, 0, s, tab, count, launches);
 }
 
 void launch_cond(cudaStream_t s, const Inst *tab, int count, int pred, int *flag, unsigned long long handle,
                  unsigned long long *launches) {
-	k_cond<<<1, 128, 0, s>>>(tab, count, pred, flag, handle, launches);
-	TG_CUDA(cudaGetLastError());
+	launch_pdl(k_cond, 1, 128, 0, s, tab, count, pred, flag, handle, launches);
 }
 
 static int grid_for(long long n) {

@@ -24,7 +24,7 @@ void launch_scaleb(cudaStream_t s, const KArgs &a);
 void launch_init(cudaStream_t s, const KArgs &a);
 void launch_init_u(cudaStream_t s, const KArgs &a);
 void launch_D(cudaStream_t s, const KArgs &a);
-void launch_shrink_g2(cudaStream_t s, const KArgs &a);
+void launch_shrink(cudaStream_t s, const KArgs &a);
 void launch_getg(cudaStream_t s, const KArgs &a);
 void launch_grad(cudaStream_t s, const KArgs &a);
 void launch_tau_prep(cudaStream_t s, const KArgs &a);

@@ -8,7 +8,8 @@
 //   rays      forward: warp per ray, lanes take strided Bresenham steps in
 //             closed form (2d/mat_mult.h:145-181, 3d/mat_mult.h:241-359);
 //             adjoint: pixel-major gather over the ray->pixel index transposed
-//             once on the device (deterministic, no atomics in the solve)
+//             once on the device (deterministic, no atomics in the solve); in
+//             2D per pixel tile, through shared memory
 #include "ops.cuh"
 
 namespace tval3g {
@@ -17,10 +18,12 @@ __device__ __forceinline__ const float *vsel(const Inst &I, VecSel s) { return s
 __device__ __forceinline__ float *vselw(const Inst &I, VecSel s) { return s.m ? I.vm[s.idx] : I.vn[s.idx]; }
 
 #define OPROLOGUE()                                                                   \
+	pdl_launch_next();                                                                \
 	if (launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);   \
 	const int2 tl_ = map.tiles[blockIdx.x];                                           \
 	const Inst &I = tab[tl_.x];                                                       \
 	const long long local = tl_.y;                                                    \
+	pdl_wait_prev();                                                                  \
 	if (!pred_ok(*I.ctrl, pred)) return;
 
 // ---------------------------------------------------------------------------
@@ -161,6 +164,223 @@ __global__ void __launch_bounds__(256) k_dense_red(const Inst *tab, TileMap map,
 		for (int w = 1; w < 8; w++) t += ws[w][lane];
 		vselw(I, ys)[layer * n + c] = (float)t;
 	}
+}
+
+// ---------------------------------------------------------------------------
+// dense normal product, A read once (get_g_mult's cache-blocked dense path,
+// 2d/tval3_cpu_2d.cpp:361-394): Au = A u and g = A^T Au in one pass over A.
+// A is cut into bands of R = grid x rpc rows; CTA c owns rows c rpc ..
+// c rpc + rpc - 1 of every band and the column slab [c S, c S + S) of g.
+// Each CTA's warps split in two roles that run concurrently:
+//   streamers (warps 0-7): band after band, the CTA's rows of Au (whole-row
+//     dot products, A streamed from HBM), published with a release
+//     increment of flags[band];
+//   reducers (warps 8-15): band after band, once all rows of the band are
+//     published, the slab of A_band^T Au_band added into FP64 accumulators
+//     kept for the whole launch - the band is read again from L2, where the
+//     streamers just brought it.
+// The streamers start band b only when their CTA's reducers have finished
+// band b - 2, so two bands at most are in L2.  All CTAs must be co-resident
+// (cooperative launch); every wait is bounded and sets *err when it gives
+// up.  Every product is accumulated in FP64 (as the gemv kernels do) in a
+// fixed order: deterministic.
+// ---------------------------------------------------------------------------
+constexpr int FUSED_THREADS = 512;
+constexpr int FUSED_ROLE = 256;                     // threads per role
+constexpr int FUSED_RPC_MAX = 16;                   // rows per CTA per band
+constexpr int FUSED_GRID_MAX = 160;
+constexpr long long FUSED_BAND_BYTES = 24LL << 20;  // target band size
+constexpr long long FUSED_L2_BYTES = 96LL << 20;    // two bands must stay in L2
+constexpr unsigned FUSED_SPIN_MAX = 1u << 21;       // bounded waits (~0.2 s)
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+	int v;
+	asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+	return v;
+}
+__device__ __forceinline__ void role_sync(int id) {   // named barrier of one role's 256 threads
+	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(FUSED_ROLE) : "memory");
+}
+
+template <bool V4>
+__global__ void __launch_bounds__(FUSED_THREADS, 1) k_dense_normal(const Inst *tab, int inst, int pred, VecSel us,
+                                                                   VecSel aus, VecSel gs, int *flags, int *err,
+                                                                   unsigned long long *launches) {
+	if (launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);
+	const Inst &I = tab[inst];
+	if (!pred_ok(*I.ctrl, pred)) return;   // the same in every CTA: ctrl is not written here
+	constexpr int V = V4 ? 4 : 1;
+	__shared__ double sau[FUSED_GRID_MAX * FUSED_RPC_MAX];   // the band's Au (reducers)
+	__shared__ double spart[8 * FUSED_RPC_MAX];              // row-segment partials (streamers)
+	__shared__ volatile int s_done, s_abort;                 // bands reduced; a wait gave up
+	const OpDev &op = I.op;
+	const int m = (int)op.m, n = (int)op.n;
+	const int G = gridDim.x, c = blockIdx.x, rpc = op.fused_rpc, R = G * rpc;
+	const int nb = (m + R - 1) / R;
+	const float *A = op.A;
+	const int S = op.fused_slab;   // slab width, a multiple of V
+	const int c0 = min(n, c * S), c1 = min(n, c0 + S);
+	if (threadIdx.x == 0) { s_done = 0; s_abort = 0; }
+	__syncthreads();
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	if (warp < 8) {
+		// ---- streamers ----
+		const float *u = vsel(I, us);
+		float *au = vselw(I, aus);
+		const int nseg = rpc >= 8 ? 1 : 8 / rpc;      // warps per row
+		const int L = n / V;                           // row length in loads
+		for (int b = 0; b < nb; b++) {
+			if (threadIdx.x == 0 && !s_abort) {
+				unsigned it = 0;
+				while (s_done < b - 1) {
+					if (++it > FUSED_SPIN_MAX) { atomicExch(err, 1); s_abort = 1; break; }
+					__nanosleep(32);
+				}
+			}
+			role_sync(1);
+			const int r0 = b * R + c * rpc;
+			for (int pr = warp; pr < rpc * nseg; pr += 8) {
+				const int j = pr / nseg, sg = pr - j * nseg, r = r0 + j;
+				double acc = 0.0;
+				if (r < m) {
+					const int k0 = (int)((long long)L * sg / nseg), k1 = (int)((long long)L * (sg + 1) / nseg);
+					if (V4) {
+						const float4 *a4 = reinterpret_cast<const float4 *>(A + (long long)r * n);
+						const float4 *u4 = reinterpret_cast<const float4 *>(u);
+#pragma unroll 8
+						for (int k = k0 + lane; k < k1; k += 32) {
+							const float4 av = a4[k], uv = __ldg(u4 + k);
+							acc = fma((double)av.x, (double)uv.x, acc);
+							acc = fma((double)av.y, (double)uv.y, acc);
+							acc = fma((double)av.z, (double)uv.z, acc);
+							acc = fma((double)av.w, (double)uv.w, acc);
+						}
+					} else {
+						const float *a = A + (long long)r * n;
+#pragma unroll 8
+						for (int k = k0 + lane; k < k1; k += 32) acc = fma((double)a[k], (double)__ldg(u + k), acc);
+					}
+				}
+				acc = warp_sum(acc);
+				if (lane == 0) spart[pr] = acc;
+			}
+			role_sync(1);
+			if (threadIdx.x < rpc && r0 + (int)threadIdx.x < m) {
+				double t = 0.0;
+				for (int sg = 0; sg < nseg; sg++) t += spart[threadIdx.x * nseg + sg];
+				au[r0 + threadIdx.x] = (float)t;
+			}
+			role_sync(1);
+			if (threadIdx.x == 0 && r0 < m) {
+				__threadfence();
+				atomicAdd(&flags[b], 1);
+			}
+		}
+	} else {
+		// ---- reducers ----
+		const int t = threadIdx.x - FUSED_ROLE;
+		const float *au = vsel(I, aus);
+		const int SV = S / V;                              // loads per slab row
+		const int Q = SV >= FUSED_ROLE ? 1 : FUSED_ROLE / SV;   // row groups
+		const int j = t % SV, q = t / SV;
+		const bool act = q < Q && c0 + V * j < c1;
+		double acc[V];
+#pragma unroll
+		for (int e = 0; e < V; e++) acc[e] = 0.0;
+		for (int b = 0; b < nb; b++) {
+			const int r0 = b * R, rows = min(R, m - r0);
+			const int expect = min(G, (rows + rpc - 1) / rpc);
+			if (t == 0 && !s_abort) {
+				unsigned it = 0;
+				while (ld_acquire(flags + b) < expect) {
+					if (++it > FUSED_SPIN_MAX) { atomicExch(err, 1); s_abort = 1; break; }
+					__nanosleep(32);
+				}
+			}
+			role_sync(2);
+			for (int k = t; k < rows; k += FUSED_ROLE) sau[k] = (double)__ldcg(au + r0 + k);
+			role_sync(2);
+			if (act) {
+				const float *a = A + (long long)r0 * n + c0 + V * j;
+				int r = q;
+				for (; r + 7 * Q < rows; r += 8 * Q) {
+					if (V4) {
+						float4 v[8];
+#pragma unroll
+						for (int e = 0; e < 8; e++) v[e] = *reinterpret_cast<const float4 *>(a + (long long)(r + e * Q) * n);
+#pragma unroll
+						for (int e = 0; e < 8; e++) {
+							const double w = sau[r + e * Q];
+							acc[0] = fma((double)v[e].x, w, acc[0]);
+							acc[V > 1 ? 1 : 0] = fma((double)v[e].y, w, acc[V > 1 ? 1 : 0]);
+							acc[V > 2 ? 2 : 0] = fma((double)v[e].z, w, acc[V > 2 ? 2 : 0]);
+							acc[V > 3 ? 3 : 0] = fma((double)v[e].w, w, acc[V > 3 ? 3 : 0]);
+						}
+					} else {
+						float v[8];
+#pragma unroll
+						for (int e = 0; e < 8; e++) v[e] = a[(long long)(r + e * Q) * n];
+#pragma unroll
+						for (int e = 0; e < 8; e++) acc[0] = fma((double)v[e], sau[r + e * Q], acc[0]);
+					}
+				}
+				for (; r < rows; r += Q) {
+					const double w = sau[r];
+					if (V4) {
+						const float4 v = *reinterpret_cast<const float4 *>(a + (long long)r * n);
+						acc[0] = fma((double)v.x, w, acc[0]);
+						acc[V > 1 ? 1 : 0] = fma((double)v.y, w, acc[V > 1 ? 1 : 0]);
+						acc[V > 2 ? 2 : 0] = fma((double)v.z, w, acc[V > 2 ? 2 : 0]);
+						acc[V > 3 ? 3 : 0] = fma((double)v.w, w, acc[V > 3 ? 3 : 0]);
+					} else {
+						acc[0] = fma((double)a[(long long)r * n], w, acc[0]);
+					}
+				}
+			}
+			role_sync(2);
+			if (t == 0) {
+				__threadfence_block();
+				s_done = b + 1;
+			}
+		}
+		// the row groups' sums of each column, in group order
+		double *sred = sau;   // Q x S doubles (Q S <= V x 256)
+		if (act)
+#pragma unroll
+			for (int e = 0; e < V; e++) sred[q * S + V * j + e] = acc[e];
+		role_sync(2);
+		float *gv = vselw(I, gs);
+		for (int col = t; col < c1 - c0; col += FUSED_ROLE) {
+			double tot = 0.0;
+			for (int qq = 0; qq < Q; qq++) tot += sred[qq * S + col];
+			gv[c0 + col] = (float)tot;
+		}
+	}
+}
+
+int fused_grid() {
+	int dev = 0, sms = 0;
+	TG_CUDA(cudaGetDevice(&dev));
+	TG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+	return std::max(1, std::min(sms, FUSED_GRID_MAX));
+}
+
+int fused_rows_per_cta(long long m, long long n, int grid, const float *A, int *slab, bool *v4) {
+	if (m < 1 || n < 1 || m >= (1LL << 31)) return 0;
+	const int V = (n % 4 == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0) ? 4 : 1;
+	long long S = (n + grid - 1) / grid;   // slab width, a multiple of V
+	S = (S + V - 1) / V * V;
+	const long long SV = S / V;
+	if (SV > FUSED_ROLE) return 0;        // one load per reducer thread and slab row
+	const long long Q = FUSED_ROLE / SV;  // row groups
+	if (Q * S > (long long)FUSED_GRID_MAX * FUSED_RPC_MAX) return 0;   // their sums reuse the band buffer
+	const long long row = 4 * n;
+	long long rpc = FUSED_BAND_BYTES / (grid * row);
+	rpc = std::max(1LL, std::min<long long>(rpc, FUSED_RPC_MAX));
+	if (2 * grid * rpc * row > FUSED_L2_BYTES) return 0;
+	*slab = (int)S;
+	*v4 = V == 4;
+	return (int)rpc;
 }
 
 // ---------------------------------------------------------------------------
@@ -340,132 +560,254 @@ __global__ void __launch_bounds__(256) k_transpose2d(const Inst *tab, TileMap ma
 }
 
 // ---------------------------------------------------------------------------
-// staged 2D ray adjoint
+// tiled 2D ray adjoint
 // ---------------------------------------------------------------------------
-// ylive[k] = y[measurement index of traced ray k]
-__global__ void __launch_bounds__(256) k_ray_compact(const Inst *tab, TileMap map, int pred, VecSel xs,
-                                                     unsigned long long *launches) {
-	OPROLOGUE();
-	const OpDev &op = I.op;
-	const int k = (int)local * 256 + threadIdx.x;
-	if (k < op.nrays) op.ylive[k] = vsel(I, xs)[op.live_out[k]];
+__global__ void k_to_int(const long long *in, int *out, long long n);
+
+constexpr int RAYT_THREADS = RAYT * RAYT;   // one thread per pixel of a tile
+constexpr int RAYT_WARPS = RAYT_THREADS / 32;
+
+int tiled_smem_bytes(int tmax) { return (int)sizeof(float) * (tmax + 1); }
+
+// the eight entries of a 16-byte index word, summed in a fixed tree
+__device__ __forceinline__ float word_sum(const float *yt, uint4 q) {
+	return ((yt[q.x & 0xffff] + yt[q.x >> 16]) + (yt[q.y & 0xffff] + yt[q.y >> 16])) +
+	       ((yt[q.z & 0xffff] + yt[q.z >> 16]) + (yt[q.w & 0xffff] + yt[q.w >> 16]));
 }
 
-constexpr int STAGED_THREADS = 512;   // one pixel per thread: ppb <= 512
-constexpr int STAGED_PAD = 8;         // per-chunk segments padded to 8 entries (16 bytes)
-constexpr unsigned short STAGED_SENTINEL = RAY_CHUNK;   // pad entry: reads the zero slot
-
-int staged_smem_bytes(int) { return (int)sizeof(float) * (RAY_CHUNK + STAGED_PAD); }
-
-// g[p] = scale * sum over the rays through p of ylive[ray]: chunk by chunk,
-// the chunk of ylive is copied to shared memory (slot RAY_CHUNK holds 0 for
-// the pad entries) and each thread sums its pixel's entries of the chunk in
-// ray order, reading them eight at a time with 16-byte loads
-__global__ void __launch_bounds__(STAGED_THREADS) k_ray_adj_staged(const Inst *tab, TileMap map, int pred,
-                                                                   VecSel ys, unsigned long long *launches) {
+// g[p] = scale * sum over the rays through p of y[ray] (the transposed
+// projection of 2d/mat_mult.h:145-181).  Block per RAYT x RAYT tile: the
+// measurements of the rays crossing the tile are gathered into shared memory
+// (slot 0 holds the zero that pad entries read), then every thread sums its
+// pixel's entries in ray order - eight per 16-byte word in FP32, the words in
+// FP64 - reading its lane's column of the warp's interleaved words, so each
+// warp load is 512 contiguous bytes.  Threads take the tile's pixels in order
+// of decreasing hit count (OpDev::tperm), so a warp's pixels have lists of
+// nearly one length and its words carry little padding.  Deterministic, no
+// atomics.
+__global__ void __launch_bounds__(RAYT_THREADS) k_ray_adj_tiled(const Inst *tab, TileMap map, int pred, VecSel xs,
+                                                                VecSel ys, unsigned long long *launches) {
 	OPROLOGUE();
-	extern __shared__ float smem[];
-	float *chunk = smem;
+	extern __shared__ float yt[];
 	const OpDev &op = I.op;
-	const int n = (int)I.n, NC = op.nchunks;
-	const int p = (int)local * op.ppb + threadIdx.x;
-	const bool own = threadIdx.x < op.ppb && p < n;
-	constexpr int V4 = RAY_CHUNK / 4 / STAGED_THREADS;   // float4 per thread per chunk
-	if (threadIdx.x < STAGED_PAD) chunk[RAY_CHUNK + threadIdx.x] = 0.f;
-	const int *so = op.soff + (long long)(own ? p : 0) * (NC + 1);
-	// eight interleaved FP64 partial sums (one per index slot), added by a
-	// fixed tree at the end: deterministic
-	double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-	for (int c = 0; c < NC; c++) {
-		const int c0 = c * RAY_CHUNK, cl = min(RAY_CHUNK, op.nrays - c0);
-		__syncthreads();
-		// all loads of the chunk in flight at once (ylive holds whole chunks)
-		const float4 *src = reinterpret_cast<const float4 *>(op.ylive + c0);
-		float4 r[V4];
+	const int t = (int)local;
+	const int k0 = __ldg(op.tptr + t), len = __ldg(op.tptr + t + 1) - k0;
+	const float *y = vsel(I, xs);
+	if (threadIdx.x == 0) yt[0] = 0.f;
+	{   // eight list entries, then their eight measurements, in flight per thread
+		constexpr int U8 = 8;
+		int k = threadIdx.x;
+		for (; k + (U8 - 1) * RAYT_THREADS < len; k += U8 * RAYT_THREADS) {
+			int mi[U8];
 #pragma unroll
-		for (int u = 0; u < V4; u++) {
-			const int t4 = threadIdx.x + u * STAGED_THREADS;
-			r[u] = (4 * t4 < cl) ? __ldcg(src + t4) : make_float4(0.f, 0.f, 0.f, 0.f);
+			for (int u = 0; u < U8; u++) mi[u] = __ldg(op.tmeas + k0 + k + u * RAYT_THREADS);
+			float yv[U8];
+#pragma unroll
+			for (int u = 0; u < U8; u++) yv[u] = y[mi[u]];
+#pragma unroll
+			for (int u = 0; u < U8; u++) yt[1 + k + u * RAYT_THREADS] = yv[u];
 		}
+		for (; k < len; k += RAYT_THREADS) yt[1 + k] = y[__ldg(op.tmeas + k0 + k)];
+	}
+	__syncthreads();
+	const int lane = threadIdx.x & 31, wl = t * RAYT_WARPS + (threadIdx.x >> 5);
+	const int w0 = __ldg(op.woff + wl), nv = (__ldg(op.woff + wl + 1) - w0) >> 5;
+	const uint4 *ix = op.sidx + w0 + lane;
+	double acc = 0.0;
+	int v = 0;
+	for (; v + 4 <= nv; v += 4) {   // four words in flight
+		uint4 q[4];
 #pragma unroll
-		for (int u = 0; u < V4; u++) reinterpret_cast<float4 *>(chunk)[threadIdx.x + u * STAGED_THREADS] = r[u];
-		__syncthreads();
-		if (own) {
-			const int k0 = __ldg(so + c), k1 = __ldg(so + c + 1);
-			const uint4 *ix = reinterpret_cast<const uint4 *>(op.sidx + k0);
-			const int nv = (k1 - k0) / STAGED_PAD;
-#pragma unroll 4
-			for (int v = 0; v < nv; v++) {
-				const uint4 w = __ldg(ix + v);
-				acc[0] += chunk[w.x & 0xffff]; acc[1] += chunk[w.x >> 16];
-				acc[2] += chunk[w.y & 0xffff]; acc[3] += chunk[w.y >> 16];
-				acc[4] += chunk[w.z & 0xffff]; acc[5] += chunk[w.z >> 16];
-				acc[6] += chunk[w.w & 0xffff]; acc[7] += chunk[w.w >> 16];
+		for (int u = 0; u < 4; u++) q[u] = __ldg(ix + 32 * (v + u));
+#pragma unroll
+		for (int u = 0; u < 4; u++) acc += (double)word_sum(yt, q[u]);
+	}
+	for (; v < nv; v++) acc += (double)word_sum(yt, __ldg(ix + 32 * v));
+	const int px = __ldg(op.tperm + (long long)t * RAYT_THREADS + threadIdx.x);   // this thread's pixel of the tile
+	const int x = (t % op.ntx) * RAYT + (px % RAYT), row = (t / op.ntx) * RAYT + (px / RAYT);
+	if (x < op.rvx && row < op.tH) vselw(I, ys)[x + row * op.rvx] = (float)(acc * op.scale);
+}
+
+// --- index builder (once per operator) ---------------------------------------
+// The rays crossing tile t, as a bitmap over traced-ray ids in shared memory,
+// from the pixel-major lists of traced-ray ids (cptr, cind).
+// image index of pixel px (0 .. RAYT^2 - 1, row-major) of tile t, or -1 outside the image
+__device__ __forceinline__ int tile_pixel(int t, int px, int ntx, int ld, int H) {
+	const int x = (t % ntx) * RAYT + px % RAYT, y = (t / ntx) * RAYT + px / RAYT;
+	return (x < ld && y < H) ? x + y * ld : -1;
+}
+
+__device__ void tile_bitmap(unsigned *bm, int nwords, int p, const int *cptr, const int *cind) {
+	for (int w = threadIdx.x; w < nwords; w += blockDim.x) bm[w] = 0u;
+	__syncthreads();
+	if (p >= 0)
+		for (int k = cptr[p]; k < cptr[p + 1]; k++) {
+			const int r = cind[k];
+			atomicOr(&bm[r >> 5], 1u << (r & 31));
+		}
+	__syncthreads();
+}
+
+// rays per tile; the tile's pixels in order of decreasing list length, ties
+// by position (perm[rank] = pixel); per warp of ranks its word count: 32 x
+// the longest of its pixels' lists, in 16-byte words
+__global__ void __launch_bounds__(RAYT_THREADS) k_tile_count(int ld, int H, int ntx, int nrays, const int *cptr,
+                                                             const int *cind, long long *tlen, long long *wlen,
+                                                             unsigned char *perm) {
+	extern __shared__ unsigned bm[];
+	__shared__ int ws[RAYT_WARPS];
+	__shared__ int cnt[RAYT_THREADS];
+	__shared__ int byrank[RAYT_THREADS];
+	const int t = blockIdx.x, nwords = (nrays + 31) >> 5;
+	const int p = tile_pixel(t, threadIdx.x, ntx, ld, H);
+	tile_bitmap(bm, nwords, p, cptr, cind);
+	int c = 0;
+	for (int w = threadIdx.x; w < nwords; w += blockDim.x) c += __popc(bm[w]);
+	c = __reduce_add_sync(0xffffffffu, c);
+	const int mine = p >= 0 ? cptr[p + 1] - cptr[p] : 0;
+	cnt[threadIdx.x] = mine;
+	if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+	__syncthreads();
+	int rank = 0;
+	for (int q = 0; q < RAYT_THREADS; q++) {
+		const int o = cnt[q];
+		rank += (o > mine || (o == mine && q < (int)threadIdx.x)) ? 1 : 0;
+	}
+	perm[(long long)t * RAYT_THREADS + rank] = (unsigned char)threadIdx.x;
+	byrank[rank] = mine;
+	__syncthreads();
+	const int nv = __reduce_max_sync(0xffffffffu, (byrank[threadIdx.x] + 7) >> 3);
+	if ((threadIdx.x & 31) == 0) wlen[(long long)t * RAYT_WARPS + (threadIdx.x >> 5)] = 32LL * nv;
+	if (threadIdx.x == 0) {
+		long long tot = 0;
+		for (int i = 0; i < RAYT_WARPS; i++) tot += ws[i];
+		tlen[t] = tot;
+	}
+}
+
+// the tile's list (measurement indices in traced order) and its pixels'
+// 1-based positions in it, padded with 0 to the warp's word count
+__global__ void __launch_bounds__(RAYT_THREADS) k_tile_fill(int ld, int H, int ntx, int nrays, const int *cptr,
+                                                            const int *cind, const int *live_out,
+                                                            const long long *tptr, const long long *woff,
+                                                            const unsigned char *perm, int *tmeas, uint4 *sidx) {
+	extern __shared__ unsigned bm[];   // nwords bits, then nwords exclusive prefix counts
+	__shared__ int ws[RAYT_WARPS];
+	const int t = blockIdx.x, nwords = (nrays + 31) >> 5;
+	int *pre = reinterpret_cast<int *>(bm + nwords);
+	// thread = rank: its pixel in the order of decreasing list length
+	const int p = tile_pixel(t, perm[(long long)t * RAYT_THREADS + threadIdx.x], ntx, ld, H);
+	tile_bitmap(bm, nwords, p, cptr, cind);
+	// exclusive prefix of the words' popcounts: thread i scans a contiguous run
+	const int per = (nwords + RAYT_THREADS - 1) / RAYT_THREADS;
+	const int w0 = min(nwords, (int)threadIdx.x * per), w1 = min(nwords, w0 + per);
+	int c = 0;
+	for (int w = w0; w < w1; w++) c += __popc(bm[w]);
+	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	int inc = c;
+	for (int o = 1; o < 32; o <<= 1) {
+		const int u = __shfl_up_sync(0xffffffffu, inc, o);
+		if (lane >= o) inc += u;
+	}
+	if (lane == 31) ws[wid] = inc;
+	__syncthreads();
+	int run = inc - c;
+	for (int i = 0; i < wid; i++) run += ws[i];
+	for (int w = w0; w < w1; w++) {
+		pre[w] = run;
+		run += __popc(bm[w]);
+	}
+	__syncthreads();
+	const long long base = tptr[t];
+	for (int w = w0; w < w1; w++) {
+		unsigned b = bm[w];
+		int r = pre[w];
+		while (b) {
+			const int bit = __ffs(b) - 1;
+			b &= b - 1;
+			tmeas[base + r++] = live_out[w * 32 + bit];
+		}
+	}
+	const long long wl = (long long)t * RAYT_WARPS + wid;
+	const long long v0 = woff[wl];
+	const int nv = (int)((woff[wl + 1] - v0) >> 5);
+	int k = p >= 0 ? cptr[p] : 0;
+	const int k1 = p >= 0 ? cptr[p + 1] : 0;
+	for (int v = 0; v < nv; v++) {
+		unsigned e[8];
+#pragma unroll
+		for (int j = 0; j < 8; j++) {
+			unsigned pos = 0;
+			if (k < k1) {
+				const int r = cind[k++];
+				pos = 1u + (unsigned)pre[r >> 5] + __popc(bm[r >> 5] & ((1u << (r & 31)) - 1u));
 			}
+			e[j] = pos;
 		}
+		sidx[v0 + 32LL * v + lane] = make_uint4(e[0] | (e[1] << 16), e[2] | (e[3] << 16), e[4] | (e[5] << 16),
+		                                        e[6] | (e[7] << 16));
 	}
-	const double sum = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
-	if (own) vselw(I, ys)[p] = (float)(sum * op.scale);
 }
 
-// padded length of every pixel's list (each chunk segment rounded up to 8)
-__global__ void k_stage_count(long long n, int nchunks, const int *cptr, const int *cind, long long *plen) {
-	const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-	if (p >= n) return;
-	long long len = 0;
-	int k = cptr[p];
-	const int k1 = cptr[p + 1];
-	for (int c = 0; c < nchunks; c++) {
-		int cnt = 0;
-		while (k < k1 && cind[k] < (c + 1) * RAY_CHUNK) { k++; cnt++; }
-		len += (cnt + STAGED_PAD - 1) / STAGED_PAD * STAGED_PAD;
-	}
-	plen[p] = len;
-}
-
-// write the padded 16-bit lists and the per-pixel chunk boundaries
-__global__ void k_stage_fill(long long n, int nchunks, const int *cptr, const int *cind, const long long *pbase,
-                             unsigned short *sidx, int *soff) {
-	const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-	if (p >= n) return;
-	int k = cptr[p];
-	const int k1 = cptr[p + 1];
-	int *so = soff + p * (nchunks + 1);
-	long long w = pbase[p];
-	for (int c = 0; c < nchunks; c++) {
-		so[c] = (int)w;
-		int cnt = 0;
-		while (k < k1 && cind[k] < (c + 1) * RAY_CHUNK) {
-			sidx[w++] = (unsigned short)(cind[k] - c * RAY_CHUNK);
-			k++; cnt++;
-		}
-		while (cnt % STAGED_PAD) { sidx[w++] = STAGED_SENTINEL; cnt++; }
-	}
-	so[nchunks] = (int)w;
-}
-
-long long build_staged_index(cudaStream_t s, long long n, int nrays, const int *cptr, const int *cind,
-                             unsigned short **sidx_out, int *soff, std::vector<void *> &owned) {
-	const int nchunks = (nrays + RAY_CHUNK - 1) / RAY_CHUNK;
-	long long *plen = nullptr, *pbase = nullptr;
-	TG_CUDA(cudaMallocAsync(&plen, sizeof(long long) * (n + 1), s));
-	TG_CUDA(cudaMallocAsync(&pbase, sizeof(long long) * (n + 1), s));
-	k_stage_count<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, nchunks, cptr, cind, plen);
-	scan_counts(s, plen, pbase, n);
-	long long total = 0;
-	TG_CUDA(cudaMemcpyAsync(&total, pbase + n, sizeof(long long), cudaMemcpyDeviceToHost, s));
-	TG_CUDA(cudaStreamSynchronize(s));
-	unsigned short *sidx = nullptr;
-	TG_CUDA(cudaMalloc(&sidx, sizeof(unsigned short) * (size_t)std::max(total, 8LL)));
-	owned.push_back(sidx);
-	k_stage_fill<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, nchunks, cptr, cind, pbase, sidx, soff);
+bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr, const int *cind,
+                       const int *live_out, OpDev &d, long long *bytes, std::vector<void *> &owned) {
+	if (nrays <= 0 || nrays > RAYT_MAX_RAYS) return false;
+	const int ntx = (ld + RAYT - 1) / RAYT, nty = (H + RAYT - 1) / RAYT, nt = ntx * nty;
+	const long long nw = (long long)nt * RAYT_WARPS;
+	const int nwords = (nrays + 31) / 32;
+	const int smem_count = (int)sizeof(unsigned) * nwords, smem_fill = 2 * smem_count;
+	TG_CUDA(cudaFuncSetAttribute(k_tile_count, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_count));
+	TG_CUDA(cudaFuncSetAttribute(k_tile_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_fill));
+	long long *tlen = nullptr, *tptr = nullptr, *wlen = nullptr, *woff = nullptr;
+	TG_CUDA(cudaMallocAsync(&tlen, sizeof(long long) * (nt + 1), s));
+	TG_CUDA(cudaMallocAsync(&tptr, sizeof(long long) * (nt + 1), s));
+	TG_CUDA(cudaMallocAsync(&wlen, sizeof(long long) * (nw + 1), s));
+	TG_CUDA(cudaMallocAsync(&woff, sizeof(long long) * (nw + 1), s));
+	unsigned char *perm = nullptr;
+	TG_CUDA(cudaMalloc(&perm, (size_t)nt * RAYT_THREADS));
+	k_tile_count<<<nt, RAYT_THREADS, smem_count, s>>>(ld, H, ntx, nrays, cptr, cind, tlen, wlen, perm);
 	TG_CUDA(cudaGetLastError());
-	TG_CUDA(cudaFreeAsync(plen, s));
-	TG_CUDA(cudaFreeAsync(pbase, s));
-	TG_CUDA(cudaFuncSetAttribute(k_ray_adj_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
-	                             staged_smem_bytes(0)));
-	*sidx_out = sidx;
-	return total;
+	scan_counts(s, tlen, tptr, nt);
+	scan_counts(s, wlen, woff, nw);
+	std::vector<long long> h_tptr(nt + 1);
+	long long words = 0;
+	TG_CUDA(cudaMemcpyAsync(h_tptr.data(), tptr, sizeof(long long) * (nt + 1), cudaMemcpyDeviceToHost, s));
+	TG_CUDA(cudaMemcpyAsync(&words, woff + nw, sizeof(long long), cudaMemcpyDeviceToHost, s));
+	TG_CUDA(cudaStreamSynchronize(s));
+	long long tmax = 0;
+	for (int t = 0; t < nt; t++) tmax = std::max(tmax, h_tptr[t + 1] - h_tptr[t]);
+	const bool ok = tmax <= RAYT_MAX_LIST && words < (1LL << 31) && h_tptr[nt] < (1LL << 31);
+	if (ok) {
+		int *tmeas = nullptr, *tptr32 = nullptr, *woff32 = nullptr;
+		uint4 *sidx = nullptr;
+		TG_CUDA(cudaMalloc(&tmeas, sizeof(int) * (size_t)std::max(h_tptr[nt], 1LL)));
+		TG_CUDA(cudaMalloc(&sidx, sizeof(uint4) * (size_t)std::max(words, 1LL)));
+		TG_CUDA(cudaMalloc(&tptr32, sizeof(int) * (nt + 1)));
+		TG_CUDA(cudaMalloc(&woff32, sizeof(int) * (nw + 1)));
+		owned.push_back(tmeas); owned.push_back(sidx); owned.push_back(tptr32); owned.push_back(woff32);
+		k_tile_fill<<<nt, RAYT_THREADS, smem_fill, s>>>(ld, H, ntx, nrays, cptr, cind, live_out, tptr, woff, perm,
+		                                                tmeas, sidx);
+		TG_CUDA(cudaGetLastError());
+		k_to_int<<<(unsigned)((nt + 1 + 255) / 256), 256, 0, s>>>(tptr, tptr32, nt + 1);
+		k_to_int<<<(unsigned)((nw + 1 + 255) / 256), 256, 0, s>>>(woff, woff32, nw + 1);
+		TG_CUDA(cudaGetLastError());
+		TG_CUDA(cudaFuncSetAttribute(k_ray_adj_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                             tiled_smem_bytes(RAYT_MAX_LIST)));
+		d.tiled = 1;
+		d.ntx = ntx;
+		d.tmax = (int)tmax;
+		d.tptr = tptr32; d.tmeas = tmeas; d.woff = woff32; d.sidx = sidx; d.tperm = perm;
+		owned.push_back(perm);
+		*bytes = (long long)sizeof(uint4) * words + (long long)sizeof(int) * (h_tptr[nt] + nt + nw + 2) +
+		         (long long)nt * RAYT_THREADS;
+	} else {
+		TG_CUDA(cudaFree(perm));
+	}
+	TG_CUDA(cudaFreeAsync(tlen, s));
+	TG_CUDA(cudaFreeAsync(tptr, s));
+	TG_CUDA(cudaFreeAsync(wlen, s));
+	TG_CUDA(cudaFreeAsync(woff, s));
+	return ok;
 }
 
 // ---------------------------------------------------------------------------
@@ -474,7 +816,7 @@ long long build_staged_index(cudaStream_t s, long long n, int nrays, const int *
 template <int W>
 static void gather_w(cudaStream_t s, const LaunchCtx &L, const TileMap &map, int pred, int kind, VecSel x,
                      VecSel y) {
-	k_gather<W><<<map.count, 256, 0, s>>>(L.inst, map, pred, kind, x, y, (unsigned long long *)L.launches);
+	launch_pdl(k_gather<W>, map.count, 256, 0, s, L.inst, map, pred, kind, x, y, (unsigned long long *)L.launches);
 }
 static void gather(const LaunchCtx &L, const TileMap (&maps)[4], int pred, int kind, VecSel x, VecSel y) {
 	if (maps[0].count > 0) gather_w<4>(L.stream, L, maps[0], pred, kind, x, y);
@@ -484,46 +826,59 @@ static void gather(const LaunchCtx &L, const TileMap (&maps)[4], int pred, int k
 	TG_CUDA(cudaGetLastError());
 }
 
-void op_forward(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y) {
+void op_forward(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y, bool unfused, bool xT_ready) {
 	auto *ctr = (unsigned long long *)L.launches;
 	for (const auto &e : B.mrhs) mrhs_apply(L.stream, L.inst, e.first, pred, *e.second, false, x, y, ctr);
-	if (B.dense_fwd.count > 0) {
-		k_dense_fwd<<<B.dense_fwd.count, 256, 0, L.stream>>>(L.inst, B.dense_fwd, pred, x, y, ctr);
-		TG_CUDA(cudaGetLastError());
+	const TileMap &df = unfused ? B.dense_fwd_nf : B.dense_fwd;
+	if (df.count > 0) {
+		launch_pdl(k_dense_fwd, df.count, 256, 0, L.stream, L.inst, df, pred, x, y, ctr);
 	}
 	gather(L, B.csr_fwd, pred, 0, x, y);
-	if (B.ray2_transpose.count > 0) {
-		k_transpose2d<<<B.ray2_transpose.count, 256, 0, L.stream>>>(L.inst, B.ray2_transpose, pred, x, ctr);
-		TG_CUDA(cudaGetLastError());
+	if (B.ray2_transpose.count > 0 && !xT_ready) {
+		launch_pdl(k_transpose2d, B.ray2_transpose.count, 256, 0, L.stream, L.inst, B.ray2_transpose, pred, x, ctr);
 	}
 	if (B.ray2_fwd.count > 0) {
-		k_ray_fwd<32, false><<<B.ray2_fwd.count, 256, 0, L.stream>>>(L.inst, B.ray2_fwd, pred, x, y, ctr);
-		TG_CUDA(cudaGetLastError());
+		launch_pdl(k_ray_fwd<RAY_SUBW, false>, B.ray2_fwd.count, 256, 0, L.stream, L.inst, B.ray2_fwd, pred, x, y, ctr);
 	}
 	if (B.ray3_fwd.count > 0) {
-		k_ray_fwd<16, true><<<B.ray3_fwd.count, 256, 0, L.stream>>>(L.inst, B.ray3_fwd, pred, x, y, ctr);
-		TG_CUDA(cudaGetLastError());
+		launch_pdl(k_ray_fwd<RAY_SUBW, true>, B.ray3_fwd.count, 256, 0, L.stream, L.inst, B.ray3_fwd, pred, x, y, ctr);
 	}
 }
 
-void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y) {
+void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y, bool unfused) {
 	auto *ctr = (unsigned long long *)L.launches;
 	for (const auto &e : B.mrhs) mrhs_apply(L.stream, L.inst, e.first, pred, *e.second, true, x, y, ctr);
-	if (B.dense_adj.count > 0) {
-		k_dense_adj<<<B.dense_adj.count, 256, 0, L.stream>>>(L.inst, B.dense_adj, pred, x, y, B.dense_part, ctr);
-		TG_CUDA(cudaGetLastError());
-		k_dense_red<<<B.dense_red.count, 256, 0, L.stream>>>(L.inst, B.dense_red, pred, x, y, B.dense_part, ctr);
-		TG_CUDA(cudaGetLastError());
+	const TileMap &da = unfused ? B.dense_adj_nf : B.dense_adj, &dr = unfused ? B.dense_red_nf : B.dense_red;
+	if (da.count > 0) {
+		launch_pdl(k_dense_adj, da.count, 256, 0, L.stream, L.inst, da, pred, x, y, B.dense_part, ctr);
+		launch_pdl(k_dense_red, dr.count, 256, 0, L.stream, L.inst, dr, pred, x, y, (const float *)B.dense_part, ctr);
 	}
 	gather(L, B.csc_adj, pred, 1, x, y);
 	gather(L, B.ray_adj, pred, 2, x, y);
-	if (B.ray_adj_staged.count > 0) {
-		k_ray_compact<<<B.ray_compact.count, 256, 0, L.stream>>>(L.inst, B.ray_compact, pred, x, ctr);
-		TG_CUDA(cudaGetLastError());
-		k_ray_adj_staged<<<B.ray_adj_staged.count, STAGED_THREADS, staged_smem_bytes(B.staged_ppb_max),
-		                   L.stream>>>(L.inst, B.ray_adj_staged, pred, y, ctr);
-		TG_CUDA(cudaGetLastError());
+	if (B.ray_adj_tiled.count > 0) {
+		launch_pdl(k_ray_adj_tiled, B.ray_adj_tiled.count, RAYT_THREADS, tiled_smem_bytes(B.tiled_tmax), L.stream,
+		           L.inst, B.ray_adj_tiled, pred, x, y, ctr);
 	}
+}
+
+void op_fused_normal(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y, VecSel z) {
+	auto *ctr = (unsigned long long *)L.launches;
+	for (const auto &f : B.fused) {
+		int *flags = B.fused_flags + f.off, *err = B.fused_flags + B.fused_err;
+		TG_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * f.bands, L.stream));
+		int inst = f.inst;
+		const Inst *tab = L.inst;
+		void *args[] = {(void *)&tab, (void *)&inst, (void *)&pred, (void *)&x, (void *)&y, (void *)&z,
+		                (void *)&flags, (void *)&err, (void *)&ctr};
+		const void *kern = f.v4 ? (const void *)k_dense_normal<true> : (const void *)k_dense_normal<false>;
+		TG_CUDA(cudaLaunchCooperativeKernel(kern, dim3(B.fused_grid), dim3(FUSED_THREADS), args, 0, L.stream));
+	}
+}
+
+void op_normal(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y, VecSel z) {
+	op_fused_normal(L, B, pred, x, y, z);
+	op_forward(L, B, pred, x, y, true, false);
+	op_adjoint(L, B, pred, y, z, true);
 }
 
 // ---------------------------------------------------------------------------

@@ -10,12 +10,33 @@
 namespace tval3g {
 
 constexpr int WARPS = 8;   // warps per block in the operator kernels
+// lanes per ray of the on-the-fly forward projectors: a warp traces
+// 32 / RAY_SUBW rays at once, which spreads the per-ray set-up (unpacking,
+// the closed-form start of every lane, the final shuffle sum) over several
+// rays; 2D rays of 100-400 hits and 3D rays of ~60 hits keep 8 lanes busy
+constexpr int RAY_SUBW = 8;
+constexpr int RAYS_PER_BLOCK = 256 / RAY_SUBW;
 
 struct OpBatch {
 	// dense (2d/mat_mult.h:15-36): forward warp-per-row gemv; adjoint over
 	// (column tile, row chunk) blocks into partials, then a column reduction
 	TileMap dense_fwd, dense_adj, dense_red;
 	float *dense_part = nullptr;
+	// dense operators whose normal product A^T (A u) reads A once
+	// (k_dense_normal, one cooperative launch per instance); the gemv maps
+	// without them serve the rest of a normal product
+	struct Fused {
+		int inst;
+		int bands;
+		long long off;   // of its band flags in fused_flags
+		bool v4;         // float4 loads (n % 4 == 0, A 16-byte aligned)
+	};
+	std::vector<Fused> fused;
+	TileMap dense_fwd_nf, dense_adj_nf, dense_red_nf;
+	int fused_grid = 0;
+	long long fused_words = 0;   // band flags of all fused instances, then one error word
+	long long fused_err = 0;
+	int *fused_flags = nullptr;
 	// dense operators with 16-64 layers: one launch sequence per instance on
 	// the tensor cores (mrhs.cu)
 	std::vector<std::pair<int, std::shared_ptr<MrhsOp>>> mrhs;
@@ -24,23 +45,35 @@ struct OpBatch {
 	// its mean line length (4, 8, 16 or 32 lanes per line: class 0..3), so its
 	// summation order does not depend on the other instances of a batch.
 	TileMap csr_fwd[4], csc_adj[4], ray_adj[4];
-	// rays: on-the-fly Bresenham, 32 lanes per 2D ray (8 rays per block),
-	// 16 lanes per 3D ray (16 rays per block)
+	// rays: on-the-fly Bresenham, RAY_SUBW lanes per ray (2D and 3D)
 	TileMap ray2_fwd, ray3_fwd;
 	TileMap ray2_transpose;   // 32x32 tiles of the image, for 2D ray operators with xT
-	// staged 2D ray adjoint: compaction of the input to traced rays, then one
-	// block per ppb pixels
-	TileMap ray_compact, ray_adj_staged;
-	int staged_ppb_max = 0;
+	// tiled 2D ray adjoint: one block per RAYT x RAYT pixel tile; dynamic
+	// shared memory for the longest tile list of the batch
+	TileMap ray_adj_tiled;
+	int tiled_tmax = 0;
 };
 
-// the staged 2D ray adjoint's index: 16-bit in-chunk ray offsets, every
-// pixel's segment of every chunk padded to 8 entries, and the per-pixel chunk
-// boundaries, from a pixel-major index of traced-ray ids.  Allocates the
-// index (recorded in `owned`) and returns its length.
-long long build_staged_index(cudaStream_t s, long long n, int nrays, const int *cptr, const int *cind,
-                             unsigned short **sidx, int *soff, std::vector<void *> &owned);
-int staged_smem_bytes(int ppb);
+// the tiled 2D ray adjoint's index (OpDev::tiled) for an ld x H image, from
+// the pixel-major lists of traced-ray ids (cptr, cind; sorted by ray) and the
+// measurement index of every traced ray.  Fills d's tiled fields, allocates
+// the index (recorded in `owned`, its size stored in *bytes) and returns true;
+// returns false, allocating nothing, when there are more than RAYT_MAX_RAYS
+// traced rays or a tile list would exceed RAYT_MAX_LIST.
+bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr, const int *cind,
+                       const int *live_out, OpDev &d, long long *bytes, std::vector<void *> &owned);
+int tiled_smem_bytes(int tmax);
+// the dense normal product's launch: CTAs (one per SM), and rows per CTA per
+// band for an m x n operator A (0: the operator does not suit it - its slab
+// or two bands do not fit), with the slab width and whether the rows are
+// read as float4
+int fused_grid();
+int fused_rows_per_cta(long long m, long long n, int grid, const float *A, int *slab, bool *v4);
+// Au = A u and g = A^T Au for the fused dense instances (A read once)
+void op_fused_normal(const LaunchCtx &L, const OpBatch &B, int pred, VecSel u, VecSel au, VecSel g);
+// the normal product of every instance: fused dense instances in one pass,
+// the others as op_forward then op_adjoint
+void op_normal(const LaunchCtx &L, const OpBatch &B, int pred, VecSel u, VecSel au, VecSel g);
 
 // one-time builders (ops.cu)
 // exclusive scan of n int64 counts into out[0..n] (out[n] = total)

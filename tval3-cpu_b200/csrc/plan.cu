@@ -161,6 +161,7 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		float *cval = dalloc_op<float>(st, p.nnz);
 		build_transpose(s, d.m, d.n, p.nnz, d.rptr, d.rind, d.rval, cptr, cind, cval);
 		d.cptr = cptr; d.cind = cind; d.cval = cval;
+		st.adj_index_bytes = (long long)sizeof(int) * (d.n + 1) + 8LL * p.nnz;
 		st.b_len = (long long)p.m * d.layers;
 	} else {
 		// traced rays in the reference's loop order (mp, emitter, receiver)
@@ -217,26 +218,21 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		int *cptr = dalloc_op<int>(st, n + 1);
 		int *cind = dalloc_op<int>(st, total);
 		build_transpose(s, d.nrays, n, total, rptr, rind, nullptr, cptr, cind, nullptr);
-		const int nchunks = (d.nrays + RAY_CHUNK - 1) / RAY_CHUNK;
-		if (!is3 && d.nrays > 0 && nchunks <= RAY_MAX_CHUNKS) {
-			// staged adjoint: 16-bit in-chunk ray offsets (cind still holds ray ids)
-			unsigned short *sidx = nullptr;
-			int *soff = dalloc_op<int>(st, n * (nchunks + 1));
-			long long slen = build_staged_index(s, n, d.nrays, cptr, cind, &sidx, soff, st.owned);
-			st.bytes += slen * (long long)sizeof(unsigned short);
-			int *lo = dalloc_op<int>(st, d.nrays);
-			TG_CUDA(cudaMemcpyAsync(lo, st.ray_out.data(), sizeof(int) * d.nrays, cudaMemcpyHostToDevice, s));
-			d.ylive = dalloc_op<float>(st, (long long)nchunks * RAY_CHUNK);   // whole chunks
-			d.nchunks = nchunks;
-			d.sidx = sidx; d.soff = soff; d.live_out = lo;
-			long long ppb = (n + 147) / 148;   // one block per SM for a single image
-			ppb = (ppb + 31) / 32 * 32;
-			d.ppb = (int)std::max(64LL, std::min(512LL, ppb));
-		}
 		if (!is3 && n % p.ld == 0) {   // transposed image for the y-driven rays
 			d.xT = dalloc_op<float>(st, n);
 			d.tH = (int)(n / p.ld);
 		}
+		if (!is3 && n % p.ld == 0 && d.nrays > 0 && d.nrays <= RAYT_MAX_RAYS) {
+			// tiled adjoint (cind still holds traced-ray ids)
+			int *lo = dalloc_op<int>(st, d.nrays);
+			TG_CUDA(cudaMemcpyAsync(lo, st.ray_out.data(), sizeof(int) * d.nrays, cudaMemcpyHostToDevice, s));
+			long long ib = 0;
+			if (build_tiled_index(s, (int)p.ld, (int)(n / p.ld), d.nrays, cptr, cind, lo, d, &ib, st.owned)) {
+				st.bytes += ib;
+				st.adj_index_bytes = ib;
+			}
+		}
+		if (!d.tiled) st.adj_index_bytes = (long long)sizeof(int) * (n + 1 + total);   // pixel-major gather
 		if (total > 0) k_map_out<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, drays, cind);
 		TG_CUDA(cudaGetLastError());
 		d.cptr = cptr; d.cind = cind; d.cval = nullptr;
@@ -299,7 +295,33 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
                                OpBatch &ob) {
 	const int cnt = (int)inst.size();
 	long long dense_part = 0;
-	// dense
+	// dense operators of one layer: the normal product reads A once
+	ob.fused.clear();
+	ob.fused_grid = fused_grid();
+	ob.fused_words = 0;
+	for (int i = 0; i < cnt; i++) {
+		OpDev &d = inst[i].op;
+		d.fused_rpc = 0;
+		if (d.kind != TVAL3G_OP_DENSE || d.mrhs || d.layers != 1) continue;
+		bool v4 = false;
+		d.fused_rpc = fused_rows_per_cta(d.m, d.n, ob.fused_grid, d.A, &d.fused_slab, &v4);
+		if (d.fused_rpc <= 0) continue;
+		const long long R = (long long)ob.fused_grid * d.fused_rpc;
+		const int bands = (int)((d.m + R - 1) / R);
+		ob.fused.push_back({i, bands, ob.fused_words, v4});
+		ob.fused_words += bands;
+	}
+	ob.fused_err = ob.fused_words;
+	if (!ob.fused.empty()) ob.fused_words += 1;
+	// dense gemv maps: all dense instances, then those outside the fused set
+	for (int nf = 0; nf < 2; nf++) {
+		for (int i = 0; i < cnt; i++) {
+			OpDev &d = inst[i].op;
+			if (d.kind != TVAL3G_OP_DENSE || d.mrhs || (nf && d.fused_rpc)) continue;
+			tb.add(i, d.layers * ((d.m + WARPS - 1) / WARPS));
+		}
+		tb.close(nf ? &ob.dense_fwd_nf : &ob.dense_fwd);
+	}
 	for (int i = 0; i < cnt; i++) {
 		OpDev &d = inst[i].op;
 		if (d.kind != TVAL3G_OP_DENSE) continue;
@@ -307,27 +329,27 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 			ob.mrhs.emplace_back(i, ops[i].mrhs);
 			continue;
 		}
-		tb.add(i, d.layers * ((d.m + WARPS - 1) / WARPS));
-	}
-	tb.close(&ob.dense_fwd);
-	for (int i = 0; i < cnt; i++) {
-		OpDev &d = inst[i].op;
-		if (d.kind != TVAL3G_OP_DENSE || d.mrhs) continue;
 		long long ct = (d.n + 1023) / 1024;
 		long long K = (4 * 148 + d.layers * ct - 1) / (d.layers * ct);
 		K = std::max(1LL, std::min(K, d.m));
 		d.dense_kchunks = (int)K;
 		d.dense_part = dense_part;
 		dense_part += d.layers * K * d.n;
-		tb.add(i, d.layers * ct * K);
 	}
-	tb.close(&ob.dense_adj);
-	for (int i = 0; i < cnt; i++) {
-		OpDev &d = inst[i].op;
-		if (d.kind != TVAL3G_OP_DENSE || d.mrhs) continue;
-		tb.add(i, d.layers * ((d.n + 31) / 32));
+	for (int nf = 0; nf < 2; nf++) {
+		for (int i = 0; i < cnt; i++) {
+			const OpDev &d = inst[i].op;
+			if (d.kind != TVAL3G_OP_DENSE || d.mrhs || (nf && d.fused_rpc)) continue;
+			tb.add(i, d.layers * ((d.n + 1023) / 1024) * d.dense_kchunks);
+		}
+		tb.close(nf ? &ob.dense_adj_nf : &ob.dense_adj);
+		for (int i = 0; i < cnt; i++) {
+			const OpDev &d = inst[i].op;
+			if (d.kind != TVAL3G_OP_DENSE || d.mrhs || (nf && d.fused_rpc)) continue;
+			tb.add(i, d.layers * ((d.n + 31) / 32));
+		}
+		tb.close(nf ? &ob.dense_red_nf : &ob.dense_red);
 	}
-	tb.close(&ob.dense_red);
 	// compressed gathers: each instance in the width class of its own mean
 	// line length (lines per block = 256 / width)
 	static const int widths[4] = {4, 8, 16, 32};
@@ -352,7 +374,7 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 		tb.close(&ob.csc_adj[c]);
 		for (int i = 0; i < cnt; i++) {
 			const OpDev &d = inst[i].op;
-			if ((d.kind != TVAL3G_OP_RAY2D && d.kind != TVAL3G_OP_RAY3D) || d.nchunks > 0 ||
+			if ((d.kind != TVAL3G_OP_RAY2D && d.kind != TVAL3G_OP_RAY3D) || d.tiled ||
 			    cls((double)ops[i].nnz / inst[i].n) != c)
 				continue;
 			long long lpb = 256 / widths[c];
@@ -363,13 +385,13 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 	for (int i = 0; i < cnt; i++) {
 		const OpDev &d = inst[i].op;
 		if (d.kind != TVAL3G_OP_RAY2D) continue;
-		tb.add(i, (d.nrays + 7) / 8);
+		tb.add(i, (d.nrays + RAYS_PER_BLOCK - 1) / RAYS_PER_BLOCK);
 	}
 	tb.close(&ob.ray2_fwd);
 	for (int i = 0; i < cnt; i++) {
 		const OpDev &d = inst[i].op;
 		if (d.kind != TVAL3G_OP_RAY3D) continue;
-		tb.add(i, (d.nrays + 15) / 16);
+		tb.add(i, (d.nrays + RAYS_PER_BLOCK - 1) / RAYS_PER_BLOCK);
 	}
 	tb.close(&ob.ray3_fwd);
 	for (int i = 0; i < cnt; i++) {
@@ -378,20 +400,14 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 		tb.add(i, (long long)((d.rvx + 31) / 32) * ((d.tH + 31) / 32));
 	}
 	tb.close(&ob.ray2_transpose);
-	ob.staged_ppb_max = 0;
+	ob.tiled_tmax = 0;
 	for (int i = 0; i < cnt; i++) {
 		const OpDev &d = inst[i].op;
-		if (d.nchunks <= 0) continue;
-		tb.add(i, (d.nrays + 255) / 256);
+		if (!d.tiled) continue;
+		tb.add(i, (long long)d.ntx * ((d.tH + RAYT - 1) / RAYT));
+		ob.tiled_tmax = std::max(ob.tiled_tmax, d.tmax);
 	}
-	tb.close(&ob.ray_compact);
-	for (int i = 0; i < cnt; i++) {
-		const OpDev &d = inst[i].op;
-		if (d.nchunks <= 0) continue;
-		tb.add(i, (inst[i].n + d.ppb - 1) / d.ppb);
-		ob.staged_ppb_max = std::max(ob.staged_ppb_max, d.ppb);
-	}
-	tb.close(&ob.ray_adj_staged);
+	tb.close(&ob.ray_adj_tiled);
 	return dense_part;
 }
 
@@ -438,7 +454,7 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 			I.fp.init((unsigned)I.p);
 			I.n = n; I.m = b_len;
 			I.ntn = (int)((n + TILE - 1) / TILE);
-			I.ntm = (int)((b_len + TILE - 1) / TILE);
+			I.ntm = (int)((b_len + TILE_M - 1) / TILE_M);
 			const tval3g_options &o = opts[i];
 			I.muf = o.mu; I.betaf = o.beta; I.mu0 = o.mu0; I.beta0 = o.beta0; I.tol = o.tol; I.tol_inn = o.tol_inn;
 			I.c = o.c; I.gamma = o.gamma; I.gam0 = o.gam; I.rate_gam = o.rate_gam; I.rate_cnt = o.rate_cnt;
@@ -508,6 +524,10 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 		d_tiles_ = tb.upload(stream_);
 		allocs_.push_back(d_tiles_);
 		if (dense_part > 0) ob_.dense_part = (float *)dalloc(sizeof(float) * (size_t)dense_part);
+		if (ob_.fused_words > 0) {
+			ob_.fused_flags = (int *)dalloc(sizeof(int) * (size_t)ob_.fused_words);
+			TG_CUDA(cudaMemsetAsync(ob_.fused_flags, 0, sizeof(int) * (size_t)ob_.fused_words, stream_));
+		}
 		d_inst_ = (Inst *)dalloc(sizeof(Inst) * count);
 		TG_CUDA(cudaMemcpyAsync(d_inst_, h_inst_.data(), sizeof(Inst) * count, cudaMemcpyHostToDevice, stream_));
 		d_flag_ = (int *)dalloc(sizeof(int));
@@ -671,10 +691,11 @@ void Plan::emit_program() {
 	op_adjoint(L, ob_, P_ALL, B, Atb);
 	launch_init_u(s, kargs(MAP_N, P_ALL));
 	launch_D(s, kargs(MAP_N, P_ALL));
-	launch_shrink_g2(s, kargs(MAP_N, P_ALL, ST_INIT));
-	op_forward(L, ob_, P_ALL, U, Au);
+	launch_shrink(s, kargs(MAP_N, P_ALL, ST_INIT));
+	op_fused_normal(L, ob_, P_ALL, U, Au, G);
+	op_forward(L, ob_, P_ALL, U, Au, true);
 	if (any_skip_) launch_copy_lastau(s, kargs(MAP_M, P_ALL));
-	op_adjoint(L, ob_, P_ALL, Au, G);
+	op_adjoint(L, ob_, P_ALL, Au, G, true);
 	launch_getg(s, kargs(MAP_NM, P_ALL, ST_INIT));
 	launch_grad(s, kargs(MAP_N, P_ALL, ST_INIT));
 	(void)D; (void)Ad;
@@ -713,14 +734,15 @@ void Plan::emit_iteration() {
 		launch_tau_first(es(), kargs(MAP_M, P_NEED_AD));
 	});
 	// descent step and get_g
-	launch_descend(es(), kargs(MAP_NM, P_ACTIVE, ST_DESCEND));
-	launch_D(es(), kargs(MAP_N, P_ACTIVE));
-	op_forward(lctx(), ob_, P_ACTIVE, U, Au);
+	launch_descend(es(), kargs(MAP_NM, P_ACTIVE, ST_DESCEND));   // D U: in k_getg
+	// get_g_mult: dense instances in one pass over A (they never skip)
+	op_fused_normal(lctx(), ob_, P_ACTIVE, U, Au, G);
+	op_forward(lctx(), ob_, P_ACTIVE, U, Au, true, true);
 	if (any_skip_) {
 		launch_skip_norms(es(), kargs(MAP_M, P_ACTIVE));
 		launch_copy_lastau(es(), kargs(MAP_M, P_ACTIVE_MUL));
 	}
-	op_adjoint(lctx(), ob_, P_ACTIVE_MUL, Au, G);
+	op_adjoint(lctx(), ob_, P_ACTIVE_MUL, Au, G, true);
 	launch_getg(es(), kargs(MAP_NM, P_ACTIVE, ST_DESCEND));
 	// nonmonotone Armijo backtracking, restart after five failures
 	if_(P_NEED_BT, [&] {
@@ -731,15 +753,15 @@ void Plan::emit_iteration() {
 			op_forward(lctx(), ob_, P_NEED_AD, D, Ad);
 			launch_tau_first(es(), kargs(MAP_M, P_NEED_AD));
 			launch_descend(es(), kargs(MAP_NM, P_RESTART, ST_RESTART));
-			launch_D(es(), kargs(MAP_N, P_RESTART));
-			op_forward(lctx(), ob_, P_RESTART, U, Au);
+			op_fused_normal(lctx(), ob_, P_RESTART, U, Au, G);
+			op_forward(lctx(), ob_, P_RESTART, U, Au, true, true);
 			if (any_skip_) launch_copy_lastau(es(), kargs(MAP_M, P_RESTART));
-			op_adjoint(lctx(), ob_, P_RESTART, Au, G);
+			op_adjoint(lctx(), ob_, P_RESTART, Au, G, true);
 			launch_getg(es(), kargs(MAP_NM, P_RESTART, ST_RESTART));
 		});
 	});
 	// update_W, reference values, gradient, inner stopping test
-	launch_shrink_g2(es(), kargs(MAP_N, P_ACTIVE, ST_LOOP));
+	launch_shrink(es(), kargs(MAP_N, P_ACTIVE, ST_LOOP));
 	launch_grad(es(), kargs(MAP_N, P_ACTIVE, ST_LOOP));
 	// outer step: stopping test, multipliers, continuation
 	if_(P_INNER_BREAK, [&] {
@@ -784,10 +806,17 @@ void Plan::solve(const float *const *d_b, const float *const *d_Ut, float *const
 	unsigned long long nl = 0;
 	TG_CUDA(cudaMemcpyAsync(hc.data(), d_ctrl_, sizeof(Ctrl) * count_, cudaMemcpyDeviceToHost, cur_));
 	TG_CUDA(cudaMemcpyAsync(&nl, d_launches_, sizeof(nl), cudaMemcpyDeviceToHost, cur_));
+	int fused_err = 0;
+	if (ob_.fused_flags)
+		TG_CUDA(cudaMemcpyAsync(&fused_err, ob_.fused_flags + ob_.fused_err, sizeof(int), cudaMemcpyDeviceToHost, cur_));
 	TG_CUDA(cudaStreamSynchronize(cur_));
 	for (const auto &e : ob_.mrhs)
 		if (mrhs_take_error(cur_, *e.second))
 			throw Error{TVAL3G_ERR_CUDA, "tensor-core operator: a bounded wait timed out (results invalid)"};
+	if (fused_err) {
+		TG_CUDA(cudaMemsetAsync(ob_.fused_flags + ob_.fused_err, 0, sizeof(int), cur_));
+		throw Error{TVAL3G_ERR_CUDA, "dense normal product: a bounded wait timed out (results invalid)"};
+	}
 	last_launches_ = (long long)nl;
 	last_iters_.resize(count_);
 	for (int i = 0; i < count_; i++) last_iters_[i] = hc[i].count_total;

@@ -15,6 +15,7 @@ struct OpStore {
 	std::vector<void *> owned;   // device allocations to free
 	std::shared_ptr<MrhsOp> mrhs;   // multi-RHS dense operator on the tensor cores, or null
 	long long bytes = 0;         // device bytes allocated for the operator
+	long long adj_index_bytes = 0;   // index read by one adjoint application (besides x and y)
 	long long nnz = 0;           // CSR nnz, or Bresenham hits of a ray operator
 	long long b_len = 0;
 	// ray operators: forward CSR over traced rays (kept on request) and the

@@ -90,6 +90,7 @@ def lib():
         L.tval3g_op_apply.argtypes = [vp, i, vp, vp, vp]
         L.tval3g_op_apply_n.argtypes = [vp, i, vp, vp, i, vp]
         L.tval3g_op_ray_csr.argtypes = [vp, C.POINTER(ll), _IP]
+        L.tval3g_op_adjoint_index_bytes.argtypes = [vp, C.POINTER(ll)]
         L.tval3g_op_destroy.argtypes = [vp]
         L.tval3g_D.argtypes = [i, i, i, i, vp, vp, vp, vp, vp]
         L.tval3g_Dt.argtypes = [i, i, i, i, vp, vp, vp, vp, vp]
@@ -111,7 +112,8 @@ def _check(rc):
 EXPORTS = ("tval3g_last_error", "tval3g_version", "tval3g_solve", "tval3g_solve_batch", "tval3g_plan_create",
            "tval3g_plan_solve", "tval3g_plan_stats", "tval3g_plan_trace", "tval3g_plan_set_target",
            "tval3g_plan_destroy", "tval3g_op_create", "tval3g_op_shape",
-           "tval3g_op_apply", "tval3g_op_apply_n", "tval3g_op_ray_csr", "tval3g_op_destroy", "tval3g_D", "tval3g_Dt",
+           "tval3g_op_apply", "tval3g_op_apply_n", "tval3g_op_ray_csr", "tval3g_op_adjoint_index_bytes",
+           "tval3g_op_destroy", "tval3g_D", "tval3g_Dt",
            "tval3g_shrink", "tval3g_unrolled_create", "tval3g_unrolled_forward", "tval3g_unrolled_backward",
            "tval3g_unrolled_decisions", "tval3g_unrolled_destroy")
 
@@ -311,6 +313,9 @@ class Operator:
         r, c, z = C.c_longlong(), C.c_longlong(), C.c_longlong()
         _check(lib().tval3g_op_shape(h, C.byref(r), C.byref(c), C.byref(z)))
         self.rows, self.cols, self.nnz = r.value, c.value, z.value
+        ib = C.c_longlong()
+        _check(lib().tval3g_op_adjoint_index_bytes(h, C.byref(ib)))
+        self.adjoint_index_bytes = ib.value
 
     def apply(self, x, y, trans=False, stream=None):
         _check(lib().tval3g_op_apply(self.h, int(trans), _dptr(x), _dptr(y), _dptr(stream)))
