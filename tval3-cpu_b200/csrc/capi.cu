@@ -24,7 +24,8 @@ struct tval3g_operator {
 	Ctrl *d_ctrl = nullptr;
 	int2 *d_tiles = nullptr;
 	float *d_part = nullptr;
-	int *d_fused = nullptr;   // band flags and error word of the one-pass dense normal product
+	int *d_fused = nullptr;   // band flags of the one-pass dense normal product
+	int *d_err = nullptr;     // set by a kernel whose bounded wait gave up
 	float *d_au = nullptr;    // A x of a normal product (trans = 2)
 	cudaStream_t s = nullptr;
 	long long rows = 0, cols = 0;
@@ -226,6 +227,9 @@ int tval3g_op_create(tval3g_operator **out, const tval3g_problem *prob, int flag
 			TG_CUDA(cudaMemsetAsync(op->d_fused, 0, sizeof(int) * op->ob.fused_words, op->s));
 			op->ob.fused_flags = op->d_fused;
 		}
+		TG_CUDA(cudaMalloc(&op->d_err, sizeof(int)));
+		TG_CUDA(cudaMemsetAsync(op->d_err, 0, sizeof(int), op->s));
+		op->ob.err = op->d_err;
 		TG_CUDA(cudaMalloc(&op->d_au, sizeof(float) * std::max<long long>(op->rows, 1)));
 		TG_CUDA(cudaMalloc(&op->d_inst, sizeof(Inst)));
 		TG_CUDA(cudaStreamSynchronize(op->s));
@@ -258,9 +262,17 @@ int tval3g_op_apply(tval3g_operator *op, int trans, const float *d_x, float *d_y
 	int rc = tval3g_op_apply_n(op, trans, d_x, d_y, 1, stream);
 	if (rc != TVAL3G_OK) return rc;
 	CAPI_BEGIN
-	TG_CUDA(cudaStreamSynchronize(stream ? (cudaStream_t)stream : op->s));
-	if (op->st.mrhs && mrhs_take_error(stream ? (cudaStream_t)stream : op->s, *op->st.mrhs))
+	cudaStream_t s = stream ? (cudaStream_t)stream : op->s;
+	int e = 0;
+	TG_CUDA(cudaMemcpyAsync(&e, op->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+	TG_CUDA(cudaStreamSynchronize(s));
+	if (op->st.mrhs && mrhs_take_error(s, *op->st.mrhs))
 		throw Error{TVAL3G_ERR_CUDA, "tensor-core operator: a bounded wait timed out (results invalid)"};
+	if (e) {
+		TG_CUDA(cudaMemsetAsync(op->d_err, 0, sizeof(int), s));
+		TG_CUDA(cudaStreamSynchronize(s));
+		throw Error{TVAL3G_ERR_CUDA, "operator: a bounded wait timed out (results invalid)"};
+	}
 	CAPI_END
 }
 
@@ -286,15 +298,6 @@ int tval3g_op_apply_n(tval3g_operator *op, int trans, const float *d_x, float *d
 			} else {
 				op_forward(L, op->ob, P_ALL, VecSel{false, 0}, VecSel{true, 0});
 				op_adjoint(L, op->ob, P_ALL, VecSel{true, 0}, VecSel{false, 1});
-			}
-		}
-		if (op->ob.fused_flags) {
-			int e = 0;
-			TG_CUDA(cudaMemcpyAsync(&e, op->d_fused + op->ob.fused_err, sizeof(int), cudaMemcpyDeviceToHost, s));
-			TG_CUDA(cudaStreamSynchronize(s));
-			if (e) {
-				TG_CUDA(cudaMemsetAsync(op->d_fused + op->ob.fused_err, 0, sizeof(int), s));
-				throw Error{TVAL3G_ERR_CUDA, "dense normal product: a bounded wait timed out (results invalid)"};
 			}
 		}
 		return TVAL3G_OK;
@@ -348,6 +351,7 @@ int tval3g_op_destroy(tval3g_operator *op) {
 		cudaFree(op->d_tiles);
 		cudaFree(op->d_part);
 		cudaFree(op->d_fused);
+		cudaFree(op->d_err);
 		cudaFree(op->d_au);
 		if (op->s) cudaStreamDestroy(op->s);
 		delete op;

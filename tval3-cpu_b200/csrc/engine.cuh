@@ -146,7 +146,7 @@ struct OpDev {
 
 constexpr int RAYT = 16;                // tile side of the tiled 2D ray adjoint
 constexpr int RAYT_MAX_RAYS = 1 << 18;  // its index builder keeps a bitmap of the traced rays in shared memory
-constexpr int RAYT_MAX_LIST = 57344;    // rays per tile: 16-bit positions, 224 KB of shared memory
+constexpr int RAYT_MAX_LIST = 40960;    // rays per tile (16-bit positions; 160 KB of shared memory beside the index rings)
 
 // Unsigned 32-bit division by a run-time constant with one multiply-high
 // (Granlund & Montgomery, "Division by invariant integers using

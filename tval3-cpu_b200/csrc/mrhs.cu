@@ -44,6 +44,8 @@
 
 #include <mutex>
 
+#include "async.cuh"
+
 namespace tval3g {
 
 namespace {
@@ -80,41 +82,12 @@ size_t smem_bytes(int N) {
 // ---------------------------------------------------------------------------
 // PTX wrappers
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned smem_u32(const void *p) {
-	return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
-	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
-	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(unsigned bar) {
-	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
-	unsigned ok;
-	asm volatile(
-	    "{\n\t.reg .pred p;\n\t"
-	    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-	    "selp.u32 %0, 1, 0, p;\n\t}"
-	    : "=r"(ok)
-	    : "r"(bar), "r"(parity)
-	    : "memory");
-	return ok != 0;
-}
 __device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap *map, int x, int y, unsigned bar) {
 	asm volatile(
 	    "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
 	        dst),
 	    "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(bar)
 	    : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async_smem() {
-	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() {
-	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 __device__ __forceinline__ void tc_fence_before() {
 	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

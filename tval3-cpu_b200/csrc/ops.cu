@@ -12,6 +12,8 @@
 //             2D per pixel tile, through shared memory
 #include "ops.cuh"
 
+#include "async.cuh"
+
 namespace tval3g {
 
 __device__ __forceinline__ const float *vsel(const Inst &I, VecSel s) { return s.m ? I.vm[s.idx] : I.vn[s.idx]; }
@@ -171,24 +173,35 @@ __global__ void __launch_bounds__(256) k_dense_red(const Inst *tab, TileMap map,
 // 2d/tval3_cpu_2d.cpp:361-394): Au = A u and g = A^T Au in one pass over A.
 // A is cut into bands of R = grid x rpc rows; CTA c owns rows c rpc ..
 // c rpc + rpc - 1 of every band and the column slab [c S, c S + S) of g.
-// Each CTA's warps split in two roles that run concurrently:
-//   streamers (warps 0-7): band after band, the CTA's rows of Au (whole-row
-//     dot products, A streamed from HBM), published with a release
-//     increment of flags[band];
+// Each CTA's warps take three roles that run concurrently:
+//   producer (warp 0): streams the CTA's rows, chunk by chunk, with the
+//     matching chunk of u, into a ring of shared-memory stages by bulk
+//     asynchronous copies (full / empty barriers per stage);
+//   consumers (warps 1-7): the rows' dot products from the stages; thread 0
+//     of the role writes each row of Au and, after the band's rows, publishes
+//     them with a release increment of flags[band];
 //   reducers (warps 8-15): band after band, once all rows of the band are
 //     published, the slab of A_band^T Au_band added into FP64 accumulators
 //     kept for the whole launch - the band is read again from L2, where the
-//     streamers just brought it.
-// The streamers start band b only when their CTA's reducers have finished
-// band b - 2, so two bands at most are in L2.  All CTAs must be co-resident
-// (cooperative launch); every wait is bounded and sets *err when it gives
-// up.  Every product is accumulated in FP64 (as the gemv kernels do) in a
-// fixed order: deterministic.
+//     producer just brought it.
+// The producer starts band b only when its CTA's reducers have finished band
+// b - 2, so two bands at most are in L2.  All CTAs must be co-resident
+// (cooperative launch).  Every wait is bounded: one that gives up sets *err
+// and the CTA's abort flag, after which no role waits again (every named
+// barrier is still passed the same number of times) and the producer lets
+// its copies in flight land before the CTA exits.  Every product is
+// accumulated in FP64 (as the gemv kernels do) in a fixed order:
+// deterministic.
 // ---------------------------------------------------------------------------
 constexpr int FUSED_THREADS = 512;
-constexpr int FUSED_ROLE = 256;                     // threads per role
+constexpr int FUSED_ROLE = 256;                     // reducer threads
+constexpr int FUSED_CONS = 224;                     // consumer threads (warps 1-7)
 constexpr int FUSED_RPC_MAX = 16;                   // rows per CTA per band
 constexpr int FUSED_GRID_MAX = 160;
+constexpr int FUSED_NS = 4;                         // ring stages
+constexpr int FUSED_CH = 4096;                      // floats per chunk (16 KB of A, 16 KB of u)
+constexpr int FUSED_STAGE_BYTES = 2 * FUSED_CH * 4;
+constexpr int FUSED_DYN_BYTES = FUSED_NS * FUSED_STAGE_BYTES + 2 * FUSED_NS * 8;
 constexpr long long FUSED_BAND_BYTES = 24LL << 20;  // target band size
 constexpr long long FUSED_L2_BYTES = 96LL << 20;    // two bands must stay in L2
 constexpr unsigned FUSED_SPIN_MAX = 1u << 21;       // bounded waits (~0.2 s)
@@ -198,80 +211,116 @@ __device__ __forceinline__ int ld_acquire(const int *p) {
 	asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
 	return v;
 }
-__device__ __forceinline__ void role_sync(int id) {   // named barrier of one role's 256 threads
-	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(FUSED_ROLE) : "memory");
+__device__ __forceinline__ void named_sync(int id, int threads) {   // barrier of one role's threads
+	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+// one thread polls a stage barrier; false (err raised) if it gives up
+__device__ __forceinline__ bool mbar_wait1(unsigned bar, unsigned parity, int *err) {
+	for (unsigned i = 0; i < ASYNC_WAIT_LIMIT; i++)
+		if (mbar_try(bar, parity)) return true;
+	atomicExch(err, 1);
+	return false;
 }
 
-template <bool V4>
 __global__ void __launch_bounds__(FUSED_THREADS, 1) k_dense_normal(const Inst *tab, int inst, int pred, VecSel us,
                                                                    VecSel aus, VecSel gs, int *flags, int *err,
                                                                    unsigned long long *launches) {
 	if (launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);
 	const Inst &I = tab[inst];
 	if (!pred_ok(*I.ctrl, pred)) return;   // the same in every CTA: ctrl is not written here
-	constexpr int V = V4 ? 4 : 1;
+	extern __shared__ __align__(128) unsigned char dsm[];
 	__shared__ double sau[FUSED_GRID_MAX * FUSED_RPC_MAX];   // the band's Au (reducers)
-	__shared__ double spart[8 * FUSED_RPC_MAX];              // row-segment partials (streamers)
+	__shared__ double spart[2][8];                           // consumer warps' row partials
 	__shared__ volatile int s_done, s_abort;                 // bands reduced; a wait gave up
 	const OpDev &op = I.op;
 	const int m = (int)op.m, n = (int)op.n;
 	const int G = gridDim.x, c = blockIdx.x, rpc = op.fused_rpc, R = G * rpc;
-	const int nb = (m + R - 1) / R;
+	const int nb = (m + R - 1) / R, nch = (n + FUSED_CH - 1) / FUSED_CH;
 	const float *A = op.A;
-	const int S = op.fused_slab;   // slab width, a multiple of V
+	const int S = op.fused_slab;   // slab width, a multiple of 4
 	const int c0 = min(n, c * S), c1 = min(n, c0 + S);
-	if (threadIdx.x == 0) { s_done = 0; s_abort = 0; }
+	const unsigned full0 = smem_u32(dsm + FUSED_NS * FUSED_STAGE_BYTES), empty0 = full0 + 8u * FUSED_NS;
+	auto stage_a = [&](int st) { return reinterpret_cast<float4 *>(dsm + st * FUSED_STAGE_BYTES); };
+	auto stage_u = [&](int st) { return reinterpret_cast<float4 *>(dsm + st * FUSED_STAGE_BYTES + FUSED_CH * 4); };
+	if (threadIdx.x == 0) {
+		s_done = 0;
+		s_abort = 0;
+		for (int st = 0; st < FUSED_NS; st++) {
+			mbar_init(full0 + 8u * st, 1);
+			mbar_init(empty0 + 8u * st, FUSED_CONS / 32);
+		}
+		fence_mbar_init();
+	}
 	__syncthreads();
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	if (warp < 8) {
-		// ---- streamers ----
-		const float *u = vsel(I, us);
-		float *au = vselw(I, aus);
-		const int nseg = rpc >= 8 ? 1 : 8 / rpc;      // warps per row
-		const int L = n / V;                           // row length in loads
-		for (int b = 0; b < nb; b++) {
-			if (threadIdx.x == 0 && !s_abort) {
-				unsigned it = 0;
-				while (s_done < b - 1) {
-					if (++it > FUSED_SPIN_MAX) { atomicExch(err, 1); s_abort = 1; break; }
+	if (warp == 0) {
+		// ---- producer ----
+		if (lane == 0) {
+			const float *u = vsel(I, us);
+			long long it = 0;
+			for (int b = 0; b < nb && !s_abort; b++) {
+				for (unsigned sp = 0; s_done < b - 1 && !s_abort; sp++) {
+					if (sp > FUSED_SPIN_MAX) { atomicExch(err, 1); s_abort = 1; }
 					__nanosleep(32);
 				}
+				const int r0 = b * R + c * rpc;
+				for (int j = 0; j < rpc && r0 + j < m && !s_abort; j++)
+					for (int ch = 0; ch < nch && !s_abort; ch++, it++) {
+						const int st = (int)(it % FUSED_NS);
+						const long long ph = it / FUSED_NS;
+						if (ph > 0 && !mbar_wait1(empty0 + 8u * st, (unsigned)(ph - 1) & 1u, err)) {
+							s_abort = 1;
+							break;
+						}
+						const int cnt = min(FUSED_CH, n - ch * FUSED_CH);
+						mbar_expect_tx(full0 + 8u * st, 8u * cnt);
+						bulk_g2s(smem_u32(stage_a(st)), A + (long long)(r0 + j) * n + (long long)ch * FUSED_CH, 4u * cnt,
+						         full0 + 8u * st);
+						bulk_g2s(smem_u32(stage_u(st)), u + (long long)ch * FUSED_CH, 4u * cnt, full0 + 8u * st);
+					}
 			}
-			role_sync(1);
+			if (s_abort)   // let the copies in flight land before the CTA exits (bounded)
+				for (long long k = it > FUSED_NS ? it - FUSED_NS : 0; k < it; k++)
+					mbar_wait1(full0 + 8u * (int)(k % FUSED_NS), (unsigned)(k / FUSED_NS) & 1u, err);
+		}
+	} else if (warp < 8) {
+		// ---- consumers ----
+		const int ct = threadIdx.x - 32, cw = warp - 1;
+		float *au = vselw(I, aus);
+		long long it = 0;
+		int rowc = 0;
+		for (int b = 0; b < nb; b++) {
 			const int r0 = b * R + c * rpc;
-			for (int pr = warp; pr < rpc * nseg; pr += 8) {
-				const int j = pr / nseg, sg = pr - j * nseg, r = r0 + j;
+			for (int j = 0; j < rpc && r0 + j < m; j++, rowc++) {
 				double acc = 0.0;
-				if (r < m) {
-					const int k0 = (int)((long long)L * sg / nseg), k1 = (int)((long long)L * (sg + 1) / nseg);
-					if (V4) {
-						const float4 *a4 = reinterpret_cast<const float4 *>(A + (long long)r * n);
-						const float4 *u4 = reinterpret_cast<const float4 *>(u);
-#pragma unroll 8
-						for (int k = k0 + lane; k < k1; k += 32) {
-							const float4 av = a4[k], uv = __ldg(u4 + k);
+				for (int ch = 0; ch < nch; ch++, it++) {
+					const int st = (int)(it % FUSED_NS);
+					if (!s_abort && !mbar_wait_warp(full0 + 8u * st, (unsigned)(it / FUSED_NS) & 1u, err))
+						if (lane == 0) s_abort = 1;
+					if (!s_abort) {
+						const int cnt4 = min(FUSED_CH, n - ch * FUSED_CH) >> 2;
+						const float4 *sa = stage_a(st), *su = stage_u(st);
+						for (int k = ct; k < cnt4; k += FUSED_CONS) {
+							const float4 av = sa[k], uv = su[k];
 							acc = fma((double)av.x, (double)uv.x, acc);
 							acc = fma((double)av.y, (double)uv.y, acc);
 							acc = fma((double)av.z, (double)uv.z, acc);
 							acc = fma((double)av.w, (double)uv.w, acc);
 						}
-					} else {
-						const float *a = A + (long long)r * n;
-#pragma unroll 8
-						for (int k = k0 + lane; k < k1; k += 32) acc = fma((double)a[k], (double)__ldg(u + k), acc);
 					}
+					__syncwarp();
+					if (lane == 0) mbar_arrive(empty0 + 8u * st);
 				}
 				acc = warp_sum(acc);
-				if (lane == 0) spart[pr] = acc;
+				if (lane == 0) spart[rowc & 1][cw] = acc;
+				named_sync(1, FUSED_CONS);
+				if (ct == 0) {
+					double t = 0.0;
+					for (int w = 0; w < FUSED_CONS / 32; w++) t += spart[rowc & 1][w];
+					au[r0 + j] = (float)t;
+				}
 			}
-			role_sync(1);
-			if (threadIdx.x < rpc && r0 + (int)threadIdx.x < m) {
-				double t = 0.0;
-				for (int sg = 0; sg < nseg; sg++) t += spart[threadIdx.x * nseg + sg];
-				au[r0 + threadIdx.x] = (float)t;
-			}
-			role_sync(1);
-			if (threadIdx.x == 0 && r0 < m) {
+			if (ct == 0 && r0 < m) {
 				__threadfence();
 				atomicAdd(&flags[b], 1);
 			}
@@ -280,75 +329,61 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_dense_normal(const Inst *t
 		// ---- reducers ----
 		const int t = threadIdx.x - FUSED_ROLE;
 		const float *au = vsel(I, aus);
-		const int SV = S / V;                              // loads per slab row
+		const int SV = S / 4;                                   // float4 per slab row
 		const int Q = SV >= FUSED_ROLE ? 1 : FUSED_ROLE / SV;   // row groups
 		const int j = t % SV, q = t / SV;
-		const bool act = q < Q && c0 + V * j < c1;
-		double acc[V];
-#pragma unroll
-		for (int e = 0; e < V; e++) acc[e] = 0.0;
+		const bool act = q < Q && c0 + 4 * j < c1;
+		double acc[4] = {0.0, 0.0, 0.0, 0.0};
 		for (int b = 0; b < nb; b++) {
 			const int r0 = b * R, rows = min(R, m - r0);
 			const int expect = min(G, (rows + rpc - 1) / rpc);
 			if (t == 0 && !s_abort) {
-				unsigned it = 0;
+				unsigned sp = 0;
 				while (ld_acquire(flags + b) < expect) {
-					if (++it > FUSED_SPIN_MAX) { atomicExch(err, 1); s_abort = 1; break; }
+					if (++sp > FUSED_SPIN_MAX) { atomicExch(err, 1); s_abort = 1; break; }
 					__nanosleep(32);
 				}
 			}
-			role_sync(2);
+			named_sync(2, FUSED_ROLE);
 			for (int k = t; k < rows; k += FUSED_ROLE) sau[k] = (double)__ldcg(au + r0 + k);
-			role_sync(2);
-			if (act) {
-				const float *a = A + (long long)r0 * n + c0 + V * j;
+			named_sync(2, FUSED_ROLE);
+			if (act && !s_abort) {
+				const float *a = A + (long long)r0 * n + c0 + 4 * j;
 				int r = q;
 				for (; r + 7 * Q < rows; r += 8 * Q) {
-					if (V4) {
-						float4 v[8];
+					float4 v[8];
 #pragma unroll
-						for (int e = 0; e < 8; e++) v[e] = *reinterpret_cast<const float4 *>(a + (long long)(r + e * Q) * n);
+					for (int e = 0; e < 8; e++) v[e] = *reinterpret_cast<const float4 *>(a + (long long)(r + e * Q) * n);
 #pragma unroll
-						for (int e = 0; e < 8; e++) {
-							const double w = sau[r + e * Q];
-							acc[0] = fma((double)v[e].x, w, acc[0]);
-							acc[V > 1 ? 1 : 0] = fma((double)v[e].y, w, acc[V > 1 ? 1 : 0]);
-							acc[V > 2 ? 2 : 0] = fma((double)v[e].z, w, acc[V > 2 ? 2 : 0]);
-							acc[V > 3 ? 3 : 0] = fma((double)v[e].w, w, acc[V > 3 ? 3 : 0]);
-						}
-					} else {
-						float v[8];
-#pragma unroll
-						for (int e = 0; e < 8; e++) v[e] = a[(long long)(r + e * Q) * n];
-#pragma unroll
-						for (int e = 0; e < 8; e++) acc[0] = fma((double)v[e], sau[r + e * Q], acc[0]);
+					for (int e = 0; e < 8; e++) {
+						const double w = sau[r + e * Q];
+						acc[0] = fma((double)v[e].x, w, acc[0]);
+						acc[1] = fma((double)v[e].y, w, acc[1]);
+						acc[2] = fma((double)v[e].z, w, acc[2]);
+						acc[3] = fma((double)v[e].w, w, acc[3]);
 					}
 				}
 				for (; r < rows; r += Q) {
 					const double w = sau[r];
-					if (V4) {
-						const float4 v = *reinterpret_cast<const float4 *>(a + (long long)r * n);
-						acc[0] = fma((double)v.x, w, acc[0]);
-						acc[V > 1 ? 1 : 0] = fma((double)v.y, w, acc[V > 1 ? 1 : 0]);
-						acc[V > 2 ? 2 : 0] = fma((double)v.z, w, acc[V > 2 ? 2 : 0]);
-						acc[V > 3 ? 3 : 0] = fma((double)v.w, w, acc[V > 3 ? 3 : 0]);
-					} else {
-						acc[0] = fma((double)a[(long long)r * n], w, acc[0]);
-					}
+					const float4 v = *reinterpret_cast<const float4 *>(a + (long long)r * n);
+					acc[0] = fma((double)v.x, w, acc[0]);
+					acc[1] = fma((double)v.y, w, acc[1]);
+					acc[2] = fma((double)v.z, w, acc[2]);
+					acc[3] = fma((double)v.w, w, acc[3]);
 				}
 			}
-			role_sync(2);
+			named_sync(2, FUSED_ROLE);
 			if (t == 0) {
 				__threadfence_block();
 				s_done = b + 1;
 			}
 		}
 		// the row groups' sums of each column, in group order
-		double *sred = sau;   // Q x S doubles (Q S <= V x 256)
+		double *sred = sau;   // Q x S doubles (Q S <= 4 x 256)
 		if (act)
 #pragma unroll
-			for (int e = 0; e < V; e++) sred[q * S + V * j + e] = acc[e];
-		role_sync(2);
+			for (int e = 0; e < 4; e++) sred[q * S + 4 * j + e] = acc[e];
+		named_sync(2, FUSED_ROLE);
 		float *gv = vselw(I, gs);
 		for (int col = t; col < c1 - c0; col += FUSED_ROLE) {
 			double tot = 0.0;
@@ -362,16 +397,17 @@ int fused_grid() {
 	int dev = 0, sms = 0;
 	TG_CUDA(cudaGetDevice(&dev));
 	TG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+	TG_CUDA(cudaFuncSetAttribute(k_dense_normal, cudaFuncAttributeMaxDynamicSharedMemorySize, FUSED_DYN_BYTES));
 	return std::max(1, std::min(sms, FUSED_GRID_MAX));
 }
 
-int fused_rows_per_cta(long long m, long long n, int grid, const float *A, int *slab, bool *v4) {
-	if (m < 1 || n < 1 || m >= (1LL << 31)) return 0;
-	const int V = (n % 4 == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0) ? 4 : 1;
-	long long S = (n + grid - 1) / grid;   // slab width, a multiple of V
-	S = (S + V - 1) / V * V;
-	const long long SV = S / V;
-	if (SV > FUSED_ROLE) return 0;        // one load per reducer thread and slab row
+int fused_rows_per_cta(long long m, long long n, int grid, const float *A, int *slab) {
+	// rows are streamed by 16-byte bulk copies: n % 4 == 0 and A 16-byte aligned
+	if (m < 1 || n < 1 || m >= (1LL << 31) || n % 4 != 0 || (reinterpret_cast<uintptr_t>(A) & 15) != 0) return 0;
+	long long S = (n + grid - 1) / grid;   // slab width, a multiple of 4
+	S = (S + 3) / 4 * 4;
+	const long long SV = S / 4;
+	if (SV > FUSED_ROLE) return 0;        // one float4 per reducer thread and slab row
 	const long long Q = FUSED_ROLE / SV;  // row groups
 	if (Q * S > (long long)FUSED_GRID_MAX * FUSED_RPC_MAX) return 0;   // their sums reuse the band buffer
 	const long long row = 4 * n;
@@ -379,7 +415,6 @@ int fused_rows_per_cta(long long m, long long n, int grid, const float *A, int *
 	rpc = std::max(1LL, std::min<long long>(rpc, FUSED_RPC_MAX));
 	if (2 * grid * rpc * row > FUSED_L2_BYTES) return 0;
 	*slab = (int)S;
-	*v4 = V == 4;
 	return (int)rpc;
 }
 
@@ -567,7 +602,23 @@ __global__ void k_to_int(const long long *in, int *out, long long n);
 constexpr int RAYT_THREADS = RAYT * RAYT;   // one thread per pixel of a tile
 constexpr int RAYT_WARPS = RAYT_THREADS / 32;
 
-int tiled_smem_bytes(int tmax) { return (int)sizeof(float) * (tmax + 1); }
+// Each warp streams its own words through a ring of RAYT_STAGES shared-memory
+// stages of RAYT_CW words per lane (1 KB), filled by bulk asynchronous copies
+// that lane 0 issues ahead of use, so two blocks per SM keep 64 KB of index
+// in flight without holding it in registers.
+constexpr int RAYT_STAGES = 4;
+constexpr int RAYT_CW = 2;                               // 16-byte words per lane per stage
+constexpr int RAYT_STAGE_WORDS = RAYT_CW * 32;           // per warp
+constexpr int RAYT_RING_BYTES = RAYT_WARPS * RAYT_STAGES * RAYT_STAGE_WORDS * 16;
+constexpr int RAYT_BAR_BYTES = (RAYT_WARPS * RAYT_STAGES + 2) * 8;   // the rings' barriers, the list's
+constexpr int RAYT_LIST_CHUNK = 8192;                    // list entries per bulk copy
+
+// ring, barriers, then the tile's measurements: slot 0 (the zero pad entries
+// read) sits 12 bytes past a 16-byte boundary so that slots 1.. are aligned
+// for the bulk copy of the list
+int tiled_smem_bytes(int tmax) {
+	return RAYT_RING_BYTES + RAYT_BAR_BYTES + 12 + (int)sizeof(float) * (tmax + 1);
+}
 
 // the eight entries of a 16-byte index word, summed in a fixed tree
 __device__ __forceinline__ float word_sum(const float *yt, uint4 q) {
@@ -580,49 +631,94 @@ __device__ __forceinline__ float word_sum(const float *yt, uint4 q) {
 // measurements of the rays crossing the tile are gathered into shared memory
 // (slot 0 holds the zero that pad entries read), then every thread sums its
 // pixel's entries in ray order - eight per 16-byte word in FP32, the words in
-// FP64 - reading its lane's column of the warp's interleaved words, so each
-// warp load is 512 contiguous bytes.  Threads take the tile's pixels in order
-// of decreasing hit count (OpDev::tperm), so a warp's pixels have lists of
-// nearly one length and its words carry little padding.  Deterministic, no
-// atomics.
+// FP64 - from its lane's column of the warp's interleaved words, which reach
+// shared memory through the warp's ring of bulk copies (issued before the
+// gather, so the first stages arrive meanwhile).  Threads take the tile's
+// pixels in order of decreasing hit count (OpDev::tperm), so a warp's pixels
+// have lists of nearly one length and its words carry little padding.
+// Deterministic, no atomics.
 __global__ void __launch_bounds__(RAYT_THREADS) k_ray_adj_tiled(const Inst *tab, TileMap map, int pred, VecSel xs,
-                                                                VecSel ys, unsigned long long *launches) {
+                                                                VecSel ys, int *err, unsigned long long *launches) {
 	OPROLOGUE();
-	extern __shared__ float yt[];
+	extern __shared__ __align__(128) unsigned char smem[];
 	const OpDev &op = I.op;
 	const int t = (int)local;
+	const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	uint4 *ring = reinterpret_cast<uint4 *>(smem) + wid * RAYT_STAGES * RAYT_STAGE_WORDS;
+	const unsigned bar0 = smem_u32(smem + RAYT_RING_BYTES) + 8u * (wid * RAYT_STAGES);
+	const unsigned bar_list = smem_u32(smem + RAYT_RING_BYTES) + 8u * (RAYT_WARPS * RAYT_STAGES);
+	float *yt = reinterpret_cast<float *>(smem + RAYT_RING_BYTES + RAYT_BAR_BYTES + 12);
+	const int wl = t * RAYT_WARPS + wid;
+	const int w0 = __ldg(op.woff + wl), nv = (__ldg(op.woff + wl + 1) - w0) >> 5;   // words per lane
+	const int nch = (nv + RAYT_CW - 1) / RAYT_CW;
+	const uint4 *src = op.sidx + w0;
+	auto issue = [&](int k) {   // lane 0: chunk k of this warp's words into stage k % RAYT_STAGES
+		const int st = k % RAYT_STAGES, words = min(RAYT_CW, nv - k * RAYT_CW);
+		const unsigned bytes = (unsigned)words * 32u * 16u;
+		mbar_expect_tx(bar0 + 8u * st, bytes);
+		bulk_g2s(smem_u32(ring + st * RAYT_STAGE_WORDS), src + (long long)k * RAYT_STAGE_WORDS, bytes, bar0 + 8u * st);
+	};
+	// the tile's list (a multiple of 4 entries from a 16-byte boundary) is
+	// bulk-copied into the measurement slots 1..len, then each slot's
+	// measurement index is replaced by its value
 	const int k0 = __ldg(op.tptr + t), len = __ldg(op.tptr + t + 1) - k0;
+	if (threadIdx.x == 0) {
+		mbar_init(bar_list, 1);
+		fence_mbar_init();
+		mbar_expect_tx(bar_list, (unsigned)len * 4u);
+		for (int c0 = 0; c0 < len; c0 += RAYT_LIST_CHUNK)
+			bulk_g2s(smem_u32(yt + 1 + c0), op.tmeas + k0 + c0, (unsigned)min(RAYT_LIST_CHUNK, len - c0) * 4u, bar_list);
+		yt[0] = 0.f;
+	}
+	if (lane == 0) {
+		for (int st = 0; st < RAYT_STAGES; st++) mbar_init(bar0 + 8u * st, 1);
+		fence_mbar_init();
+		for (int k = 0; k < min(RAYT_STAGES, nch); k++) issue(k);
+	}
+	__syncthreads();   // barrier initialisation seen by every thread
 	const float *y = vsel(I, xs);
-	if (threadIdx.x == 0) yt[0] = 0.f;
-	{   // eight list entries, then their eight measurements, in flight per thread
-		constexpr int U8 = 8;
+	bool ok = mbar_wait_warp(bar_list, 0u, err);
+	if (ok) {   // sixteen independent gathers in flight per thread
+		constexpr int U16 = 16;
 		int k = threadIdx.x;
-		for (; k + (U8 - 1) * RAYT_THREADS < len; k += U8 * RAYT_THREADS) {
-			int mi[U8];
+		for (; k + (U16 - 1) * RAYT_THREADS < len; k += U16 * RAYT_THREADS) {
+			float yv[U16];
 #pragma unroll
-			for (int u = 0; u < U8; u++) mi[u] = __ldg(op.tmeas + k0 + k + u * RAYT_THREADS);
-			float yv[U8];
+			for (int u = 0; u < U16; u++) yv[u] = y[__float_as_int(yt[1 + k + u * RAYT_THREADS])];
 #pragma unroll
-			for (int u = 0; u < U8; u++) yv[u] = y[mi[u]];
-#pragma unroll
-			for (int u = 0; u < U8; u++) yt[1 + k + u * RAYT_THREADS] = yv[u];
+			for (int u = 0; u < U16; u++) yt[1 + k + u * RAYT_THREADS] = yv[u];
 		}
-		for (; k < len; k += RAYT_THREADS) yt[1 + k] = y[__ldg(op.tmeas + k0 + k)];
+		for (; k < len; k += RAYT_THREADS) yt[1 + k] = y[__float_as_int(yt[1 + k])];
 	}
 	__syncthreads();
-	const int lane = threadIdx.x & 31, wl = t * RAYT_WARPS + (threadIdx.x >> 5);
-	const int w0 = __ldg(op.woff + wl), nv = (__ldg(op.woff + wl + 1) - w0) >> 5;
-	const uint4 *ix = op.sidx + w0 + lane;
 	double acc = 0.0;
-	int v = 0;
-	for (; v + 4 <= nv; v += 4) {   // four words in flight
-		uint4 q[4];
+	int k = 0;
+	for (; ok && k < nch; k++) {
+		const int st = k % RAYT_STAGES;
+		if (!mbar_wait_warp(bar0 + 8u * st, (unsigned)(k / RAYT_STAGES) & 1u, err)) break;
+		const uint4 *buf = ring + st * RAYT_STAGE_WORDS + lane;
+		const int words = min(RAYT_CW, nv - k * RAYT_CW);
+		if (words == RAYT_CW) {
+			uint4 q[RAYT_CW];
 #pragma unroll
-		for (int u = 0; u < 4; u++) q[u] = __ldg(ix + 32 * (v + u));
+			for (int j = 0; j < RAYT_CW; j++) q[j] = buf[32 * j];
 #pragma unroll
-		for (int u = 0; u < 4; u++) acc += (double)word_sum(yt, q[u]);
+			for (int j = 0; j < RAYT_CW; j++) acc += (double)word_sum(yt, q[j]);
+		} else {
+			for (int j = 0; j < words; j++) acc += (double)word_sum(yt, buf[32 * j]);
+		}
+		__syncwarp();
+		if (lane == 0 && k + RAYT_STAGES < nch) {
+			fence_proxy_async_smem();   // the stage was read: now the bulk copy may refill it
+			issue(k + RAYT_STAGES);
+		}
 	}
-	for (; v < nv; v++) acc += (double)word_sum(yt, __ldg(ix + 32 * v));
+	if (!ok || k < nch) {   // a wait gave up: let the copies in flight land (bounded) before the block exits
+		if (!ok) mbar_wait_warp(bar_list, 0u, err);
+		for (int kk = k; kk < min(nch, k + RAYT_STAGES); kk++)
+			mbar_wait_warp(bar0 + 8u * (kk % RAYT_STAGES), (unsigned)(kk / RAYT_STAGES) & 1u, err);
+		return;
+	}
 	const int px = __ldg(op.tperm + (long long)t * RAYT_THREADS + threadIdx.x);   // this thread's pixel of the tile
 	const int x = (t % op.ntx) * RAYT + (px % RAYT), row = (t / op.ntx) * RAYT + (px / RAYT);
 	if (x < op.rvx && row < op.tH) vselw(I, ys)[x + row * op.rvx] = (float)(acc * op.scale);
@@ -648,7 +744,9 @@ __device__ void tile_bitmap(unsigned *bm, int nwords, int p, const int *cptr, co
 	__syncthreads();
 }
 
-// rays per tile; the tile's pixels in order of decreasing list length, ties
+// rays per tile (rounded up to a multiple of 4: the pad entries stay 0, a
+// valid measurement index that no position refers to); the tile's pixels in
+// order of decreasing list length, ties
 // by position (perm[rank] = pixel); per warp of ranks its word count: 32 x
 // the longest of its pixels' lists, in 16-byte words
 __global__ void __launch_bounds__(RAYT_THREADS) k_tile_count(int ld, int H, int ntx, int nrays, const int *cptr,
@@ -681,7 +779,7 @@ __global__ void __launch_bounds__(RAYT_THREADS) k_tile_count(int ld, int H, int 
 	if (threadIdx.x == 0) {
 		long long tot = 0;
 		for (int i = 0; i < RAYT_WARPS; i++) tot += ws[i];
-		tlen[t] = tot;
+		tlen[t] = (tot + 3) / 4 * 4;   // lists start on 16-byte boundaries (bulk copies)
 	}
 }
 
@@ -780,7 +878,8 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 	if (ok) {
 		int *tmeas = nullptr, *tptr32 = nullptr, *woff32 = nullptr;
 		uint4 *sidx = nullptr;
-		TG_CUDA(cudaMalloc(&tmeas, sizeof(int) * (size_t)std::max(h_tptr[nt], 1LL)));
+		TG_CUDA(cudaMalloc(&tmeas, sizeof(int) * (size_t)std::max(h_tptr[nt], 4LL)));
+		TG_CUDA(cudaMemsetAsync(tmeas, 0, sizeof(int) * (size_t)std::max(h_tptr[nt], 4LL), s));
 		TG_CUDA(cudaMalloc(&sidx, sizeof(uint4) * (size_t)std::max(words, 1LL)));
 		TG_CUDA(cudaMalloc(&tptr32, sizeof(int) * (nt + 1)));
 		TG_CUDA(cudaMalloc(&woff32, sizeof(int) * (nw + 1)));
@@ -857,21 +956,21 @@ void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel
 	gather(L, B.ray_adj, pred, 2, x, y);
 	if (B.ray_adj_tiled.count > 0) {
 		launch_pdl(k_ray_adj_tiled, B.ray_adj_tiled.count, RAYT_THREADS, tiled_smem_bytes(B.tiled_tmax), L.stream,
-		           L.inst, B.ray_adj_tiled, pred, x, y, ctr);
+		           L.inst, B.ray_adj_tiled, pred, x, y, B.err, ctr);
 	}
 }
 
 void op_fused_normal(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y, VecSel z) {
 	auto *ctr = (unsigned long long *)L.launches;
 	for (const auto &f : B.fused) {
-		int *flags = B.fused_flags + f.off, *err = B.fused_flags + B.fused_err;
+		int *flags = B.fused_flags + f.off, *err = B.err;
 		TG_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * f.bands, L.stream));
 		int inst = f.inst;
 		const Inst *tab = L.inst;
 		void *args[] = {(void *)&tab, (void *)&inst, (void *)&pred, (void *)&x, (void *)&y, (void *)&z,
 		                (void *)&flags, (void *)&err, (void *)&ctr};
-		const void *kern = f.v4 ? (const void *)k_dense_normal<true> : (const void *)k_dense_normal<false>;
-		TG_CUDA(cudaLaunchCooperativeKernel(kern, dim3(B.fused_grid), dim3(FUSED_THREADS), args, 0, L.stream));
+		TG_CUDA(cudaLaunchCooperativeKernel((const void *)k_dense_normal, dim3(B.fused_grid), dim3(FUSED_THREADS),
+		                                    args, FUSED_DYN_BYTES, L.stream));
 	}
 }
 

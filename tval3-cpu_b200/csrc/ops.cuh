@@ -29,14 +29,15 @@ struct OpBatch {
 		int inst;
 		int bands;
 		long long off;   // of its band flags in fused_flags
-		bool v4;         // float4 loads (n % 4 == 0, A 16-byte aligned)
 	};
 	std::vector<Fused> fused;
 	TileMap dense_fwd_nf, dense_adj_nf, dense_red_nf;
 	int fused_grid = 0;
-	long long fused_words = 0;   // band flags of all fused instances, then one error word
-	long long fused_err = 0;
+	long long fused_words = 0;   // band flags of all fused instances
 	int *fused_flags = nullptr;
+	// set (to nonzero) by a kernel whose bounded wait gave up: its results
+	// are invalid; the owner checks and clears it after each solve or product
+	int *err = nullptr;
 	// dense operators with 16-64 layers: one launch sequence per instance on
 	// the tensor cores (mrhs.cu)
 	std::vector<std::pair<int, std::shared_ptr<MrhsOp>>> mrhs;
@@ -64,11 +65,11 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
                        const int *live_out, OpDev &d, long long *bytes, std::vector<void *> &owned);
 int tiled_smem_bytes(int tmax);
 // the dense normal product's launch: CTAs (one per SM), and rows per CTA per
-// band for an m x n operator A (0: the operator does not suit it - its slab
-// or two bands do not fit), with the slab width and whether the rows are
-// read as float4
+// band for an m x n operator A (0: the operator does not suit it - n not a
+// multiple of 4, A not 16-byte aligned, its slab or two bands do not fit),
+// with the slab width
 int fused_grid();
-int fused_rows_per_cta(long long m, long long n, int grid, const float *A, int *slab, bool *v4);
+int fused_rows_per_cta(long long m, long long n, int grid, const float *A, int *slab);
 // Au = A u and g = A^T Au for the fused dense instances (A read once)
 void op_fused_normal(const LaunchCtx &L, const OpBatch &B, int pred, VecSel u, VecSel au, VecSel g);
 // the normal product of every instance: fused dense instances in one pass,

@@ -303,16 +303,13 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 		OpDev &d = inst[i].op;
 		d.fused_rpc = 0;
 		if (d.kind != TVAL3G_OP_DENSE || d.mrhs || d.layers != 1) continue;
-		bool v4 = false;
-		d.fused_rpc = fused_rows_per_cta(d.m, d.n, ob.fused_grid, d.A, &d.fused_slab, &v4);
+		d.fused_rpc = fused_rows_per_cta(d.m, d.n, ob.fused_grid, d.A, &d.fused_slab);
 		if (d.fused_rpc <= 0) continue;
 		const long long R = (long long)ob.fused_grid * d.fused_rpc;
 		const int bands = (int)((d.m + R - 1) / R);
-		ob.fused.push_back({i, bands, ob.fused_words, v4});
+		ob.fused.push_back({i, bands, ob.fused_words});
 		ob.fused_words += bands;
 	}
-	ob.fused_err = ob.fused_words;
-	if (!ob.fused.empty()) ob.fused_words += 1;
 	// dense gemv maps: all dense instances, then those outside the fused set
 	for (int nf = 0; nf < 2; nf++) {
 		for (int i = 0; i < cnt; i++) {
@@ -528,6 +525,8 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 			ob_.fused_flags = (int *)dalloc(sizeof(int) * (size_t)ob_.fused_words);
 			TG_CUDA(cudaMemsetAsync(ob_.fused_flags, 0, sizeof(int) * (size_t)ob_.fused_words, stream_));
 		}
+		ob_.err = (int *)dalloc(sizeof(int));
+		TG_CUDA(cudaMemsetAsync(ob_.err, 0, sizeof(int), stream_));
 		d_inst_ = (Inst *)dalloc(sizeof(Inst) * count);
 		TG_CUDA(cudaMemcpyAsync(d_inst_, h_inst_.data(), sizeof(Inst) * count, cudaMemcpyHostToDevice, stream_));
 		d_flag_ = (int *)dalloc(sizeof(int));
@@ -806,16 +805,15 @@ void Plan::solve(const float *const *d_b, const float *const *d_Ut, float *const
 	unsigned long long nl = 0;
 	TG_CUDA(cudaMemcpyAsync(hc.data(), d_ctrl_, sizeof(Ctrl) * count_, cudaMemcpyDeviceToHost, cur_));
 	TG_CUDA(cudaMemcpyAsync(&nl, d_launches_, sizeof(nl), cudaMemcpyDeviceToHost, cur_));
-	int fused_err = 0;
-	if (ob_.fused_flags)
-		TG_CUDA(cudaMemcpyAsync(&fused_err, ob_.fused_flags + ob_.fused_err, sizeof(int), cudaMemcpyDeviceToHost, cur_));
+	int op_err = 0;
+	TG_CUDA(cudaMemcpyAsync(&op_err, ob_.err, sizeof(int), cudaMemcpyDeviceToHost, cur_));
 	TG_CUDA(cudaStreamSynchronize(cur_));
 	for (const auto &e : ob_.mrhs)
 		if (mrhs_take_error(cur_, *e.second))
 			throw Error{TVAL3G_ERR_CUDA, "tensor-core operator: a bounded wait timed out (results invalid)"};
-	if (fused_err) {
-		TG_CUDA(cudaMemsetAsync(ob_.fused_flags + ob_.fused_err, 0, sizeof(int), cur_));
-		throw Error{TVAL3G_ERR_CUDA, "dense normal product: a bounded wait timed out (results invalid)"};
+	if (op_err) {
+		TG_CUDA(cudaMemsetAsync(ob_.err, 0, sizeof(int), cur_));
+		throw Error{TVAL3G_ERR_CUDA, "operator: a bounded wait timed out (results invalid)"};
 	}
 	last_launches_ = (long long)nl;
 	last_iters_.resize(count_);
