@@ -13,6 +13,16 @@ namespace tval3g {
 // ---------------------------------------------------------------------------
 // prologue / image geometry
 // ---------------------------------------------------------------------------
+// the graph conditionals this launch sets (single-instance plans only), from
+// the instance's state
+__device__ __forceinline__ void set_conds(const CondSet &cs, const Ctrl &c) {
+#pragma unroll
+	for (int k = 0; k < 2; k++)
+		if (cs.h[k]) cudaGraphSetConditional((cudaGraphConditionalHandle)cs.h[k], pred_ok(c, cs.p[k]) ? 1u : 0u);
+}
+
+// A launch whose instance is excluded by its predicate still sets its
+// conditionals (block 0), from the state it leaves unchanged.
 #define KPROLOGUE(a)                                                                        \
 	pdl_launch_next();                                                                      \
 	if ((a).launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd((a).launches, 1ull); \
@@ -20,7 +30,10 @@ namespace tval3g {
 	const Inst I = (a).tab[tl_.x];                                                          \
 	const int local = tl_.y;                                                                \
 	pdl_wait_prev();                                                                        \
-	if (!pred_ok(*I.ctrl, (a).pred)) return;
+	if (!pred_ok(*I.ctrl, (a).pred)) {                                                      \
+		if (blockIdx.x == 0 && threadIdx.x == 0) set_conds((a).cs, *I.ctrl);                \
+		return;                                                                             \
+	}
 
 // element k of this thread in a tile of image elements starting at i0
 #define FOR_TILE(i0, len, i)                                  \
@@ -368,6 +381,7 @@ __global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
 	} else if (a.stage == ST_INIT) {
 		if (I.skip_enabled) c.currSkip = 0;
 	}
+	set_conds(a.cs, c);
 }
 
 // ---------------------------------------------------------------------------
@@ -455,6 +469,7 @@ __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 		c.need_mlp = 0; c.fst = 1; c.inner_break = 0;
 		c.gam = I.gam0; c.Q = 1; c.C = c.f;
 	}
+	set_conds(a.cs, c);
 }
 
 // ---------------------------------------------------------------------------
@@ -504,6 +519,7 @@ __global__ void __launch_bounds__(BLOCK) k_tau_prep(KArgs a) {
 		c.tau = fabs(tot[0] / tot[1]);
 		if (bad(c.tau)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; }
 	}
+	set_conds(a.cs, c);
 }
 
 // first-iteration step: tau = |dd / (dDd + muDbeta * |A d|^2)| (2d:430-442)
@@ -574,6 +590,7 @@ __global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
 // backtracking differences (2d:544,550-554)
 __global__ void __launch_bounds__(BLOCK) k_bt_diff(KArgs a) {
 	KPROLOGUE(a);
+	if (blockIdx.x == 0 && threadIdx.x == 0) set_conds(a.cs, *I.ctrl);   // state unchanged here
 	if (local < I.ntn) {
 		FOR_TILE(local * TILE, (int)I.n, i) {
 			I.vn[vdU][i] = I.vn[vU][i] - I.vn[vUp][i];
@@ -635,6 +652,7 @@ __global__ void __launch_bounds__(BLOCK) k_lerp(KArgs a) {
 		c.restart = 1;
 	}
 	if (bad(c.f)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; c.need_bt = 0; c.restart = 0; }
+	set_conds(a.cs, c);
 }
 
 // outer stopping test (2d:820-828): RelChgOut = |U - rcdU| / nrmup; rcdU = U

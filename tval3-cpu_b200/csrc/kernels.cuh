@@ -12,12 +12,32 @@ namespace tval3g {
 enum Stage { ST_INIT = 0, ST_LOOP, ST_DESCEND, ST_RESTART, ST_OUTER };
 enum TauMode { TAU_ACTIVE = 0, TAU_RESTART };
 
+// Graph conditionals that the kernel itself sets (single-instance graph
+// plans): after its scalar step, handle h[k] (nonzero) gets pred_ok(ctrl,
+// p[k]) - in place of a separate condition kernel before the node
+struct CondSet {
+	unsigned long long h[2] = {0ull, 0ull};
+	int p[2] = {0, 0};
+	CondSet &add(unsigned long long hh, int pp) {   // hh = 0: none (plans that evaluate conditions apart)
+		if (!hh) return *this;
+		const int k = h[0] ? 1 : 0;
+		h[k] = hh;
+		p[k] = pp;
+		return *this;
+	}
+};
+
 struct KArgs {
 	const Inst *tab;
 	TileMap map;
 	int pred;
 	int stage;
 	unsigned long long *launches;
+	CondSet cs;
+	KArgs &cond(unsigned long long h, int p) {
+		cs.add(h, p);
+		return *this;
+	}
 };
 
 void launch_scaleb(cudaStream_t s, const KArgs &a);

@@ -515,7 +515,7 @@ __global__ void __launch_bounds__(256) k_ray_fwd(const Inst *tab, TileMap map, i
 	const int gl = threadIdx.x % SUBW;
 	const long long ray = local * RPB + threadIdx.x / SUBW;
 	const float *x = vsel(I, xs);
-	double acc = 0.0;   // FP64 accumulation along the ray
+	double acc = 0.0;   // FP64 accumulation along the ray (of FP32 sums of four hits)
 	int out = -1;
 	if (ray < op.nrays) {
 		int x0, y0, z0, dx, dy, dz;
@@ -552,9 +552,7 @@ __global__ void __launch_bounds__(256) k_ray_fwd(const Inst *tab, TileMap map, i
 			}
 		}
 		const int dstep = SUBW * sd + qa1 * s1 + (D3 ? qa2 * s2 : 0);
-#pragma unroll 4
-		for (int j = gl; j <= M; j += SUBW) {
-			acc += __ldg(x + idx);
+		auto step = [&]() {
 			idx += dstep;
 			r1 += ra1;
 			if (r1 >= twoM) { r1 -= twoM; idx += s1; }
@@ -562,7 +560,25 @@ __global__ void __launch_bounds__(256) k_ray_fwd(const Inst *tab, TileMap map, i
 				r2 += ra2;
 				if (r2 >= twoM) { r2 -= twoM; idx += s2; }
 			}
+		};
+		// four of the lane's hits summed in FP32, those sums in FP64 (one
+		// conversion per four hits)
+		int j = gl;
+		for (; j + 3 * SUBW <= M; j += 4 * SUBW) {
+			float v[4];
+#pragma unroll
+			for (int u = 0; u < 4; u++) {
+				v[u] = __ldg(x + idx);
+				step();
+			}
+			acc += (double)((v[0] + v[1]) + (v[2] + v[3]));
 		}
+		float rest = 0.f;
+		for (; j <= M; j += SUBW) {
+			rest += __ldg(x + idx);
+			step();
+		}
+		acc += (double)rest;
 	}
 #pragma unroll
 	for (int o = SUBW / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);

@@ -610,7 +610,15 @@ void Plan::seg_end() {
 	capturing_ = false;
 }
 
-void Plan::if_(int pred, const std::function<void()> &body) {
+unsigned long long Plan::cond_handle() {
+	// single-instance graph plans: the deciding kernel sets the condition
+	if (!graph_mode_ || count_ != 1) return 0ull;
+	cudaGraphConditionalHandle h;
+	TG_CUDA(cudaGraphConditionalHandleCreate(&h, frames_.back().g, 0, cudaGraphCondAssignDefault));
+	return (unsigned long long)h;
+}
+
+void Plan::if_(int pred, const std::function<void()> &body, unsigned long long hset) {
 	if (!graph_mode_) {
 		launch_cond(cur_, d_inst_, count_, pred, d_flag_, 0, d_launches_);
 		TG_CUDA(cudaMemcpyAsync(h_flag_, d_flag_, sizeof(int), cudaMemcpyDeviceToHost, cur_));
@@ -618,9 +626,11 @@ void Plan::if_(int pred, const std::function<void()> &body) {
 		if (*h_flag_) body();
 		return;
 	}
-	cudaGraphConditionalHandle h;
-	TG_CUDA(cudaGraphConditionalHandleCreate(&h, frames_.back().g, 0, cudaGraphCondAssignDefault));
-	launch_cond(cap_, d_inst_, count_, pred, d_flag_, (unsigned long long)h, d_launches_);
+	cudaGraphConditionalHandle h = (cudaGraphConditionalHandle)hset;
+	if (!hset) {
+		TG_CUDA(cudaGraphConditionalHandleCreate(&h, frames_.back().g, 0, cudaGraphCondAssignDefault));
+		launch_cond(cap_, d_inst_, count_, pred, d_flag_, (unsigned long long)h, d_launches_);
+	}
 	seg_end();
 	alignas(cudaGraphNodeParams) unsigned char np_raw[sizeof(cudaGraphNodeParams)] = {};
 	cudaGraphNodeParams &np = *reinterpret_cast<cudaGraphNodeParams *>(np_raw);
@@ -642,7 +652,7 @@ void Plan::if_(int pred, const std::function<void()> &body) {
 	seg_begin();
 }
 
-void Plan::while_(int pred, const std::function<void()> &body) {
+void Plan::while_(int pred, const std::function<void()> &body, unsigned long long hset) {
 	if (!graph_mode_) {
 		for (;;) {
 			launch_cond(cur_, d_inst_, count_, pred, d_flag_, 0, d_launches_);
@@ -653,9 +663,11 @@ void Plan::while_(int pred, const std::function<void()> &body) {
 		}
 		return;
 	}
-	cudaGraphConditionalHandle h;
-	TG_CUDA(cudaGraphConditionalHandleCreate(&h, frames_.back().g, 0, cudaGraphCondAssignDefault));
-	launch_cond(cap_, d_inst_, count_, pred, d_flag_, (unsigned long long)h, d_launches_);
+	cudaGraphConditionalHandle h = (cudaGraphConditionalHandle)hset;
+	if (!hset) {
+		TG_CUDA(cudaGraphConditionalHandleCreate(&h, frames_.back().g, 0, cudaGraphCondAssignDefault));
+		launch_cond(cap_, d_inst_, count_, pred, d_flag_, (unsigned long long)h, d_launches_);
+	}
 	seg_end();
 	alignas(cudaGraphNodeParams) unsigned char np_raw[sizeof(cudaGraphNodeParams)] = {};
 	cudaGraphNodeParams &np = *reinterpret_cast<cudaGraphNodeParams *>(np_raw);
@@ -671,7 +683,7 @@ void Plan::while_(int pred, const std::function<void()> &body) {
 	frames_.push_back(Frame{np.conditional.phGraph_out[0], {}});
 	seg_begin();
 	body();
-	launch_cond(cap_, d_inst_, count_, pred, d_flag_, (unsigned long long)h, d_launches_);
+	if (!hset) launch_cond(cap_, d_inst_, count_, pred, d_flag_, (unsigned long long)h, d_launches_);
 	seg_end();
 	frames_.pop_back();
 	frames_.back().deps.assign(1, node);
@@ -696,9 +708,10 @@ void Plan::emit_program() {
 	if (any_skip_) launch_copy_lastau(s, kargs(MAP_M, P_ALL));
 	op_adjoint(L, ob_, P_ALL, Au, G, true);
 	launch_getg(s, kargs(MAP_NM, P_ALL, ST_INIT));
-	launch_grad(s, kargs(MAP_N, P_ALL, ST_INIT));
+	const unsigned long long h_act = cond_handle();
+	launch_grad(s, kargs(MAP_N, P_ALL, ST_INIT).cond(h_act, P_ACTIVE));
 	(void)D; (void)Ad;
-	while_(P_ACTIVE, [&] { emit_iteration(); });
+	while_(P_ACTIVE, [&] { emit_iteration(h_act); }, h_act);
 	launch_final(es(), kargs(MAP_N, P_ALL));
 }
 
@@ -720,18 +733,21 @@ void Plan::set_schedule(const double *mu, const double *beta) {
 	TG_CUDA(cudaMemcpy(d_sched_, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
 }
 
-void Plan::emit_iteration() {
+// h_active: the loop's condition handle when the iteration's last kernel sets
+// it (0: a condition kernel evaluates it)
+void Plan::emit_iteration(unsigned long long h_active) {
 	const LaunchCtx L = lctx();
 	cudaStream_t s = es();
 	if (sched_mode_) launch_sched(s, d_inst_, count_, d_launches_);
 	const VecSel U{false, vU}, G{false, vG}, D{false, vD};
 	const VecSel Au{true, vAu}, Ad{true, vAd};
 	// min_u (2d:526-576): step length
-	launch_tau_prep(s, kargs(MAP_N, P_ACTIVE));
+	const unsigned long long h_ad = cond_handle();
+	launch_tau_prep(s, kargs(MAP_N, P_ACTIVE).cond(h_ad, P_NEED_AD));
 	if_(P_NEED_AD, [&] {
 		op_forward(lctx(), ob_, P_NEED_AD, D, Ad);
 		launch_tau_first(es(), kargs(MAP_M, P_NEED_AD));
-	});
+	}, h_ad);
 	// descent step and get_g
 	launch_descend(es(), kargs(MAP_NM, P_ACTIVE, ST_DESCEND));   // D U: in k_getg
 	// get_g_mult: dense instances in one pass over A (they never skip)
@@ -742,11 +758,15 @@ void Plan::emit_iteration() {
 		launch_copy_lastau(es(), kargs(MAP_M, P_ACTIVE_MUL));
 	}
 	op_adjoint(lctx(), ob_, P_ACTIVE_MUL, Au, G, true);
-	launch_getg(es(), kargs(MAP_NM, P_ACTIVE, ST_DESCEND));
+	const unsigned long long h_bt = cond_handle();
+	launch_getg(es(), kargs(MAP_NM, P_ACTIVE, ST_DESCEND).cond(h_bt, P_NEED_BT));
 	// nonmonotone Armijo backtracking, restart after five failures
 	if_(P_NEED_BT, [&] {
-		launch_bt_diff(es(), kargs(MAP_NM, P_NEED_BT));
-		while_(P_NEED_BT, [&] { launch_lerp(es(), kargs(MAP_NM, P_NEED_BT)); });
+		const unsigned long long h_loop = cond_handle(), h_restart = cond_handle();
+		launch_bt_diff(es(), kargs(MAP_NM, P_NEED_BT).cond(h_loop, P_NEED_BT));
+		while_(P_NEED_BT, [&] {
+			launch_lerp(es(), kargs(MAP_NM, P_NEED_BT).cond(h_loop, P_NEED_BT).cond(h_restart, P_RESTART));
+		}, h_loop);
 		if_(P_RESTART, [&] {
 			launch_tau_prep(es(), kargs(MAP_N, P_RESTART));
 			op_forward(lctx(), ob_, P_NEED_AD, D, Ad);
@@ -757,17 +777,18 @@ void Plan::emit_iteration() {
 			if (any_skip_) launch_copy_lastau(es(), kargs(MAP_M, P_RESTART));
 			op_adjoint(lctx(), ob_, P_RESTART, Au, G, true);
 			launch_getg(es(), kargs(MAP_NM, P_RESTART, ST_RESTART));
-		});
-	});
+		}, h_restart);
+	}, h_bt);
 	// update_W, reference values, gradient, inner stopping test
 	launch_shrink(es(), kargs(MAP_N, P_ACTIVE, ST_LOOP));
-	launch_grad(es(), kargs(MAP_N, P_ACTIVE, ST_LOOP));
+	const unsigned long long h_brk = cond_handle();
+	launch_grad(es(), kargs(MAP_N, P_ACTIVE, ST_LOOP).cond(h_brk, P_INNER_BREAK).cond(h_active, P_ACTIVE));
 	// outer step: stopping test, multipliers, continuation
 	if_(P_INNER_BREAK, [&] {
 		launch_outer(es(), kargs(MAP_N, P_INNER_BREAK));
 		launch_mlp(es(), kargs(MAP_NM, P_NEED_MLP));
-		launch_grad(es(), kargs(MAP_N, P_NEED_MLP, ST_OUTER));
-	});
+		launch_grad(es(), kargs(MAP_N, P_NEED_MLP, ST_OUTER).cond(h_active, P_ACTIVE));
+	}, h_brk);
 	(void)L; (void)s;
 }
 

@@ -101,10 +101,14 @@ private:
 	KArgs kargs(MapKind mk, int pred, int stage = 0) const;
 	LaunchCtx lctx() const;
 	void emit_program();
-	void emit_iteration();
+	void emit_iteration(unsigned long long h_active);
 	// control flow: direct execution or graph construction
-	void if_(int pred, const std::function<void()> &body);
-	void while_(int pred, const std::function<void()> &body);
+	// Conditional regions.  With a handle from cond_handle() the kernel launched
+	// just before (and, for while_, the body's last kernel) sets the condition;
+	// with h = 0 a condition kernel evaluates it (batches, host-driven plans).
+	unsigned long long cond_handle();
+	void if_(int pred, const std::function<void()> &body, unsigned long long h = 0);
+	void while_(int pred, const std::function<void()> &body, unsigned long long h = 0);
 	void seg_begin();
 	void seg_end();
 	cudaStream_t es() const { return graph_mode_ ? cap_ : cur_; }
