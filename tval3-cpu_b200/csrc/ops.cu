@@ -442,12 +442,38 @@ __global__ void __launch_bounds__(256) k_gather(const Inst *tab, TileMap map, in
 	const float *x = vsel(I, xs) + layer * xlen;
 	double acc = 0.0;   // FP64 accumulation of FP32 products
 	if (line < lines) {
+		// four of the lane's entries per step: their indices, then the four
+		// gathers, in flight together; summed in the lane's entry order
 		const int k0 = ptr[line], k1 = ptr[line + 1];
-		if (val)
-			for (int k = k0 + gl; k < k1; k += W)
-				acc = fma((double)__ldg(val + k), (double)__ldg(x + __ldg(ind + k)), acc);
-		else
-			for (int k = k0 + gl; k < k1; k += W) acc += __ldg(x + __ldg(ind + k));
+		int k = k0 + gl;
+		if (val) {
+			for (; k + 3 * W < k1; k += 4 * W) {
+				int ii[4];
+				float vv[4], xx[4];
+#pragma unroll
+				for (int u = 0; u < 4; u++) {
+					ii[u] = __ldg(ind + k + u * W);
+					vv[u] = __ldg(val + k + u * W);
+				}
+#pragma unroll
+				for (int u = 0; u < 4; u++) xx[u] = __ldg(x + ii[u]);
+#pragma unroll
+				for (int u = 0; u < 4; u++) acc = fma((double)vv[u], (double)xx[u], acc);
+			}
+			for (; k < k1; k += W) acc = fma((double)__ldg(val + k), (double)__ldg(x + __ldg(ind + k)), acc);
+		} else {
+			for (; k + 3 * W < k1; k += 4 * W) {
+				int ii[4];
+				float xx[4];
+#pragma unroll
+				for (int u = 0; u < 4; u++) ii[u] = __ldg(ind + k + u * W);
+#pragma unroll
+				for (int u = 0; u < 4; u++) xx[u] = __ldg(x + ii[u]);
+#pragma unroll
+				for (int u = 0; u < 4; u++) acc += xx[u];
+			}
+			for (; k < k1; k += W) acc += __ldg(x + __ldg(ind + k));
+		}
 	}
 #pragma unroll
 	for (int o = W / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -618,22 +644,27 @@ __global__ void k_to_int(const long long *in, int *out, long long n);
 constexpr int RAYT_THREADS = RAYT * RAYT;   // one thread per pixel of a tile
 constexpr int RAYT_WARPS = RAYT_THREADS / 32;
 
-// Each warp streams its own words through a ring of RAYT_STAGES shared-memory
-// stages of RAYT_CW words per lane (1 KB), filled by bulk asynchronous copies
-// that lane 0 issues ahead of use, so two blocks per SM keep 64 KB of index
-// in flight without holding it in registers.
-constexpr int RAYT_STAGES = 4;
+// Two threads per pixel: warp w and warp w + 8 of a block take the first and
+// the second half of the words of pixel-warp w (its 32 pixels), and each
+// warp streams its half through a ring of RAYT_STAGES shared-memory stages of
+// RAYT_CW words per lane (1 KB), filled by bulk asynchronous copies that lane
+// 0 issues ahead of use - two blocks per SM keep 64 KB of index in flight
+// without holding it in registers.
+constexpr int RAYT_ADJ_THREADS = 2 * RAYT_THREADS;      // two threads per pixel
+constexpr int RAYT_ADJ_WARPS = RAYT_ADJ_THREADS / 32;
+constexpr int RAYT_STAGES = 2;
 constexpr int RAYT_CW = 2;                               // 16-byte words per lane per stage
 constexpr int RAYT_STAGE_WORDS = RAYT_CW * 32;           // per warp
-constexpr int RAYT_RING_BYTES = RAYT_WARPS * RAYT_STAGES * RAYT_STAGE_WORDS * 16;
-constexpr int RAYT_BAR_BYTES = (RAYT_WARPS * RAYT_STAGES + 2) * 8;   // the rings' barriers, the list's
+constexpr int RAYT_RING_BYTES = RAYT_ADJ_WARPS * RAYT_STAGES * RAYT_STAGE_WORDS * 16;
+constexpr int RAYT_BAR_BYTES = (RAYT_ADJ_WARPS * RAYT_STAGES + 2) * 8;   // the rings' barriers, the list's
+constexpr int RAYT_SACC_BYTES = RAYT_THREADS * 8;        // the second halves' sums
 constexpr int RAYT_LIST_CHUNK = 8192;                    // list entries per bulk copy
 
-// ring, barriers, then the tile's measurements: slot 0 (the zero pad entries
-// read) sits 12 bytes past a 16-byte boundary so that slots 1.. are aligned
-// for the bulk copy of the list
+// ring, barriers, second-half sums, then the tile's measurements: slot 0
+// (the zero pad entries read) sits 12 bytes past a 16-byte boundary so that
+// slots 1.. are aligned for the bulk copy of the list
 int tiled_smem_bytes(int tmax) {
-	return RAYT_RING_BYTES + RAYT_BAR_BYTES + 12 + (int)sizeof(float) * (tmax + 1);
+	return RAYT_RING_BYTES + RAYT_BAR_BYTES + RAYT_SACC_BYTES + 12 + (int)sizeof(float) * (tmax + 1);
 }
 
 // the eight entries of a 16-byte index word, summed in a fixed tree
@@ -653,21 +684,26 @@ __device__ __forceinline__ float word_sum(const float *yt, uint4 q) {
 // pixels in order of decreasing hit count (OpDev::tperm), so a warp's pixels
 // have lists of nearly one length and its words carry little padding.
 // Deterministic, no atomics.
-__global__ void __launch_bounds__(RAYT_THREADS) k_ray_adj_tiled(const Inst *tab, TileMap map, int pred, VecSel xs,
-                                                                VecSel ys, int *err, unsigned long long *launches) {
+__global__ void __launch_bounds__(RAYT_ADJ_THREADS) k_ray_adj_tiled(const Inst *tab, TileMap map, int pred,
+                                                                    VecSel xs, VecSel ys, int *err,
+                                                                    unsigned long long *launches) {
 	OPROLOGUE();
 	extern __shared__ __align__(128) unsigned char smem[];
 	const OpDev &op = I.op;
 	const int t = (int)local;
 	const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int pw = wid % RAYT_WARPS, half = wid / RAYT_WARPS;   // pixel-warp, which half of its words
 	uint4 *ring = reinterpret_cast<uint4 *>(smem) + wid * RAYT_STAGES * RAYT_STAGE_WORDS;
 	const unsigned bar0 = smem_u32(smem + RAYT_RING_BYTES) + 8u * (wid * RAYT_STAGES);
-	const unsigned bar_list = smem_u32(smem + RAYT_RING_BYTES) + 8u * (RAYT_WARPS * RAYT_STAGES);
-	float *yt = reinterpret_cast<float *>(smem + RAYT_RING_BYTES + RAYT_BAR_BYTES + 12);
-	const int wl = t * RAYT_WARPS + wid;
-	const int w0 = __ldg(op.woff + wl), nv = (__ldg(op.woff + wl + 1) - w0) >> 5;   // words per lane
+	const unsigned bar_list = smem_u32(smem + RAYT_RING_BYTES) + 8u * (RAYT_ADJ_WARPS * RAYT_STAGES);
+	double *sacc = reinterpret_cast<double *>(smem + RAYT_RING_BYTES + RAYT_BAR_BYTES);
+	float *yt = reinterpret_cast<float *>(smem + RAYT_RING_BYTES + RAYT_BAR_BYTES + RAYT_SACC_BYTES + 12);
+	const int wl = t * RAYT_WARPS + pw;
+	const int w0 = __ldg(op.woff + wl), nvall = (__ldg(op.woff + wl + 1) - w0) >> 5;   // words per lane
+	const int nfirst = (nvall + 1) / 2;
+	const int v0 = half ? nfirst : 0, nv = half ? nvall - nfirst : nfirst;
 	const int nch = (nv + RAYT_CW - 1) / RAYT_CW;
-	const uint4 *src = op.sidx + w0;
+	const uint4 *src = op.sidx + w0 + 32LL * v0;
 	auto issue = [&](int k) {   // lane 0: chunk k of this warp's words into stage k % RAYT_STAGES
 		const int st = k % RAYT_STAGES, words = min(RAYT_CW, nv - k * RAYT_CW);
 		const unsigned bytes = (unsigned)words * 32u * 16u;
@@ -694,17 +730,17 @@ __global__ void __launch_bounds__(RAYT_THREADS) k_ray_adj_tiled(const Inst *tab,
 	__syncthreads();   // barrier initialisation seen by every thread
 	const float *y = vsel(I, xs);
 	bool ok = mbar_wait_warp(bar_list, 0u, err);
-	if (ok) {   // sixteen independent gathers in flight per thread
-		constexpr int U16 = 16;
+	if (ok) {   // eight independent gathers in flight per thread
+		constexpr int U8 = 8;
 		int k = threadIdx.x;
-		for (; k + (U16 - 1) * RAYT_THREADS < len; k += U16 * RAYT_THREADS) {
-			float yv[U16];
+		for (; k + (U8 - 1) * RAYT_ADJ_THREADS < len; k += U8 * RAYT_ADJ_THREADS) {
+			float yv[U8];
 #pragma unroll
-			for (int u = 0; u < U16; u++) yv[u] = y[__float_as_int(yt[1 + k + u * RAYT_THREADS])];
+			for (int u = 0; u < U8; u++) yv[u] = y[__float_as_int(yt[1 + k + u * RAYT_ADJ_THREADS])];
 #pragma unroll
-			for (int u = 0; u < U16; u++) yt[1 + k + u * RAYT_THREADS] = yv[u];
+			for (int u = 0; u < U8; u++) yt[1 + k + u * RAYT_ADJ_THREADS] = yv[u];
 		}
-		for (; k < len; k += RAYT_THREADS) yt[1 + k] = y[__float_as_int(yt[1 + k])];
+		for (; k < len; k += RAYT_ADJ_THREADS) yt[1 + k] = y[__float_as_int(yt[1 + k])];
 	}
 	__syncthreads();
 	double acc = 0.0;
@@ -729,12 +765,16 @@ __global__ void __launch_bounds__(RAYT_THREADS) k_ray_adj_tiled(const Inst *tab,
 			issue(k + RAYT_STAGES);
 		}
 	}
-	if (!ok || k < nch) {   // a wait gave up: let the copies in flight land (bounded) before the block exits
+	const bool good = ok && k >= nch;
+	if (!good) {   // a wait gave up: let the copies in flight land (bounded) before the block exits
 		if (!ok) mbar_wait_warp(bar_list, 0u, err);
 		for (int kk = k; kk < min(nch, k + RAYT_STAGES); kk++)
 			mbar_wait_warp(bar0 + 8u * (kk % RAYT_STAGES), (unsigned)(kk / RAYT_STAGES) & 1u, err);
-		return;
 	}
+	if (half) sacc[pw * 32 + lane] = acc;
+	__syncthreads();
+	if (half || !good) return;
+	acc += sacc[pw * 32 + lane];   // first half + second half
 	const int px = __ldg(op.tperm + (long long)t * RAYT_THREADS + threadIdx.x);   // this thread's pixel of the tile
 	const int x = (t % op.ntx) * RAYT + (px % RAYT), row = (t / op.ntx) * RAYT + (px / RAYT);
 	if (x < op.rvx && row < op.tH) vselw(I, ys)[x + row * op.rvx] = (float)(acc * op.scale);
@@ -971,7 +1011,7 @@ void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel
 	gather(L, B.csc_adj, pred, 1, x, y);
 	gather(L, B.ray_adj, pred, 2, x, y);
 	if (B.ray_adj_tiled.count > 0) {
-		launch_pdl(k_ray_adj_tiled, B.ray_adj_tiled.count, RAYT_THREADS, tiled_smem_bytes(B.tiled_tmax), L.stream,
+		launch_pdl(k_ray_adj_tiled, B.ray_adj_tiled.count, RAYT_ADJ_THREADS, tiled_smem_bytes(B.tiled_tmax), L.stream,
 		           L.inst, B.ray_adj_tiled, pred, x, y, B.err, ctr);
 	}
 }
