@@ -7,6 +7,7 @@
 //                        tval3_cpu_2d, each compared with tval3g_solve on the
 //                        same inputs; prints "<case> <max |diff|> <iters>"
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -64,10 +65,14 @@ static void e_geom_layers() {
 	geometry g = {2, 2, use, xe, ye, xr, yr, 8, 1.0f};
 	tval3_cpu_2d(U, g, b, opts(), Ut);
 }
-static void e_double() {
-	mat<double> U(8, 8, mat_col_major), A(20, 64, mat_row_major), b(20), Ut(0, mat_col_major);
+static void e_double() {   // double data: the same argument checks
+	mat<double> U(8, 8, mat_row_major), A(20, 64, mat_row_major), b(20), Ut(0, mat_col_major);
 	tval3_options<double> o;
 	tval3_cpu_2d(U, A, b, o, Ut);
+}
+static void e_complex() {
+	mat<std::complex<float> > U(8, 8, mat_col_major), A(20, 64, mat_row_major), b(20), Ut(0, mat_col_major);
+	tval3_cpu_2d(U, A, b, opts(), Ut);
 }
 
 static double maxdiff(const float *a, const float *b, int n) {
@@ -103,6 +108,19 @@ static void solve_cases() {
 	tval3g_info ci;
 	int rc = tval3g_solve(&pr, b.data(), m, &co, 0, 0, U2.data(), &ci);
 	std::printf("dense %d %.3e %d %d\n", rc, maxdiff(U.data(), U2.data(), n), info.total_iters, ci.total_iters);
+	{   // double data through the double overload: FP32 copies of the same values, the same solve
+		mat<double> Ad(m, n, mat_row_major), Ud(p, q, mat_col_major), bd(m), Utd(0, mat_col_major);
+		for (int i = 0; i < m * n; i++) Ad[i] = A[i];
+		for (int r = 0; r < m; r++) bd[r] = b[r];
+		tval3_options<double> od;
+		od.mu = o.mu; od.beta = o.beta; od.mu0 = o.mu0; od.beta0 = o.beta0; od.tol = o.tol; od.tol_inn = o.tol_inn;
+		od.maxit = o.maxit; od.maxcnt = o.maxcnt;
+		od.c = o.c; od.gamma = o.gamma; od.gam = o.gam; od.rate_gam = o.rate_gam; od.rate_cnt = o.rate_cnt;
+		tval3_info<double> infod = tval3_cpu_2d(Ud, Ad, bd, od, Utd);
+		double d = 0;
+		for (int i = 0; i < n; i++) d = std::fmax(d, std::fabs(Ud[i] - (double)U2[i]));
+		std::printf("dense_f64 0 %.3e %d %d\n", d, infod.total_iters, ci.total_iters);
+	}
 	// CSR twin of A restricted to |a| > 0.2
 	std::vector<int> ptr(1, 0), ind;
 	std::vector<float> val;
@@ -149,6 +167,7 @@ int main(int argc, char **argv) {
 		err("csc", e_csc);
 		err("geom_layers_or_blen", e_geom_layers);
 		err("double", e_double);
+		err("complex", e_complex);
 		return 0;
 	}
 	try {

@@ -70,6 +70,32 @@ inline tval3_info<S> solve(const tval3g_problem &p, mat<float> &U, const mat<flo
 	return from_c<S>(info);
 }
 
+// Double data (the reference's double overloads, 2d/tval3_cpu_2d.cpp:905,
+// 948,991 and 3d/tval3_cpu_3d.cpp:1408,1475,1542) runs through the FP32
+// engine: FP32 copies of the arrays (shape and format kept), the FP32 solve
+// with its FP64 reductions, the solution widened into the caller's U.  The
+// result therefore carries FP32 storage error, not double precision.
+inline mat<float> narrow(const mat<double> &a) {
+	mat<float> f(a.dim_y, a.dim_x, a.dim_z, a.format);
+	for (int i = 0; i < a.len; i++) f[i] = (float)a[i];
+	return f;
+}
+inline void narrow(const sparse_mat<double> &a, sparse_mat<float> &f) {   // f: sized as a
+	std::memcpy(f.csr_ptr(), a.csr_ptr(), sizeof(int) * ((size_t)a.dim_y + 1));
+	std::memcpy(f.csc_ptr(), a.csc_ptr(), sizeof(int) * ((size_t)a.dim_x + 1));
+	if (a.nnz > 0) {
+		std::memcpy(f.csr_ind(), a.csr_ind(), sizeof(int) * (size_t)a.nnz);
+		std::memcpy(f.csc_ind(), a.csc_ind(), sizeof(int) * (size_t)a.nnz);
+	}
+	for (int k = 0; k < a.nnz; k++) {
+		f.csr_val()[k] = (float)a.csr_val()[k];
+		f.csc_val()[k] = (float)a.csc_val()[k];
+	}
+}
+inline void widen(const mat<float> &f, mat<double> &a) {
+	for (int i = 0; i < a.len && i < f.len; i++) a[i] = (double)f[i];
+}
+
 inline void unsupported(const char *what) {
 	throw tval3_exception(std::string("Internal error: ") + what +
 	                      " data is not supported by the GPU build (float data is)");

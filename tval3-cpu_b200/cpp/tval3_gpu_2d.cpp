@@ -76,10 +76,13 @@ const tval3_info<double> tval3_cpu_2d(mat<float> &U, const mat<float> &A, const 
                                       const tval3_options<double> &opts, const mat<float> &Ut, int, int) {
 	return dense2d<double>(U, A, b, opts, Ut);
 }
-const tval3_info<double> tval3_cpu_2d(mat<double> &, const mat<double> &, const mat<double> &,
-                                      const tval3_options<double> &, const mat<double> &, int, int) {
-	unsupported("double");
-	return tval3_info<double>();
+const tval3_info<double> tval3_cpu_2d(mat<double> &U, const mat<double> &A, const mat<double> &b,
+                                      const tval3_options<double> &opts, const mat<double> &Ut, int, int) {
+	mat<float> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
+	mat<float> Af = narrow(A);
+	const tval3_info<double> r = dense2d<double>(Uf, Af, bf, opts, Utf);
+	widen(Uf, U);
+	return r;
 }
 const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &, const mat<std::complex<float> > &,
                                      const mat<std::complex<float> > &, const tval3_options<float> &,
@@ -103,10 +106,14 @@ const tval3_info<double> tval3_cpu_2d(mat<float> &U, const sparse_mat<float> &A,
                                       const tval3_options<double> &opts, const mat<float> &Ut, int, int) {
 	return sparse2d<double>(U, A, b, opts, Ut);
 }
-const tval3_info<double> tval3_cpu_2d(mat<double> &, const sparse_mat<double> &, const mat<double> &,
-                                      const tval3_options<double> &, const mat<double> &, int, int) {
-	unsupported("double");
-	return tval3_info<double>();
+const tval3_info<double> tval3_cpu_2d(mat<double> &U, const sparse_mat<double> &A, const mat<double> &b,
+                                      const tval3_options<double> &opts, const mat<double> &Ut, int, int) {
+	mat<float> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
+	sparse_mat<float> Af(A.dim_y, A.dim_x, A.nnz, A.format);
+	narrow(A, Af);
+	const tval3_info<double> r = sparse2d<double>(Uf, Af, bf, opts, Utf);
+	widen(Uf, U);
+	return r;
 }
 const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &, const sparse_mat<std::complex<float> > &,
                                      const mat<std::complex<float> > &, const tval3_options<float> &,
@@ -130,10 +137,12 @@ const tval3_info<double> tval3_cpu_2d(mat<float> &U, const geometry &A, const ma
                                       const tval3_options<double> &opts, const mat<float> &Ut, int, int) {
 	return ray2d<double>(U, A, b, opts, Ut);
 }
-const tval3_info<double> tval3_cpu_2d(mat<double> &, const geometry &, const mat<double> &,
-                                      const tval3_options<double> &, const mat<double> &, int, int) {
-	unsupported("double");
-	return tval3_info<double>();
+const tval3_info<double> tval3_cpu_2d(mat<double> &U, const geometry &A, const mat<double> &b,
+                                      const tval3_options<double> &opts, const mat<double> &Ut, int, int) {
+	mat<float> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
+	const tval3_info<double> r = ray2d<double>(Uf, A, bf, opts, Utf);
+	widen(Uf, U);
+	return r;
 }
 const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &, const geometry &,
                                      const mat<std::complex<float> > &, const tval3_options<float> &,

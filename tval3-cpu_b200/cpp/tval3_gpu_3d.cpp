@@ -101,7 +101,14 @@ const tval3_info<double> tval3_cpu_3d(mat<float> &U, const mat<float> &A, const 
                                       const tval3_options<double> &opts, const mat<float> &Ut, int, int) {
 	return dense3d<double>(U, A, b, opts, Ut);
 }
-UNSUPPORTED_3D(double, double, mat<double>, "double")
+const tval3_info<double> tval3_cpu_3d(mat<double> &U, const mat<double> &A, const mat<double> &b,
+                                      const tval3_options<double> &opts, const mat<double> &Ut, int, int) {
+	mat<float> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
+	mat<float> Af = narrow(A);
+	const tval3_info<double> r = dense3d<double>(Uf, Af, bf, opts, Utf);
+	widen(Uf, U);
+	return r;
+}
 UNSUPPORTED_3D(cf, float, mat<cf>, "complex")
 UNSUPPORTED_3D(cd, double, mat<cd>, "complex")
 
@@ -113,7 +120,15 @@ const tval3_info<double> tval3_cpu_3d(mat<float> &U, const sparse_mat<float> &A,
                                       const tval3_options<double> &opts, const mat<float> &Ut, int, int) {
 	return sparse3d<double>(U, A, b, opts, Ut);
 }
-UNSUPPORTED_3D(double, double, sparse_mat<double>, "double")
+const tval3_info<double> tval3_cpu_3d(mat<double> &U, const sparse_mat<double> &A, const mat<double> &b,
+                                      const tval3_options<double> &opts, const mat<double> &Ut, int, int) {
+	mat<float> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
+	sparse_mat<float> Af(A.dim_y, A.dim_x, A.nnz, A.format);
+	narrow(A, Af);
+	const tval3_info<double> r = sparse3d<double>(Uf, Af, bf, opts, Utf);
+	widen(Uf, U);
+	return r;
+}
 UNSUPPORTED_3D(cf, float, sparse_mat<cf>, "complex")
 UNSUPPORTED_3D(cd, double, sparse_mat<cd>, "complex")
 
@@ -125,6 +140,12 @@ const tval3_info<double> tval3_cpu_3d(mat<float> &U, const geometry &A, const ma
                                       const tval3_options<double> &opts, const mat<float> &Ut, int, int) {
 	return ray3d<double>(U, A, b, opts, Ut);
 }
-UNSUPPORTED_3D(double, double, geometry, "double")
+const tval3_info<double> tval3_cpu_3d(mat<double> &U, const geometry &A, const mat<double> &b,
+                                      const tval3_options<double> &opts, const mat<double> &Ut, int, int) {
+	mat<float> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
+	const tval3_info<double> r = ray3d<double>(Uf, A, bf, opts, Utf);
+	widen(Uf, U);
+	return r;
+}
 UNSUPPORTED_3D(cf, float, geometry, "complex")
 UNSUPPORTED_3D(cd, double, geometry, "complex")

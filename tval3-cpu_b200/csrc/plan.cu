@@ -283,10 +283,13 @@ struct TileBuilder {
 	}
 };
 
+// lanes per line of the compressed gathers: about eight entries per lane, so
+// that the gather's four-deep unrolled steps run (a 3D voxel's ~60 hits: 8
+// lanes; a CSR row of ~200: 16)
 static int subwarp_for(double avg) {
-	if (avg >= 48) return 32;
-	if (avg >= 20) return 16;
-	if (avg >= 8) return 8;
+	if (avg >= 256) return 32;
+	if (avg >= 128) return 16;
+	if (avg >= 32) return 8;
 	return 4;
 }
 
