@@ -544,6 +544,31 @@ def run_batch(a, cx, capi, world, dist, clocks):
     iters = [i["total_iters"] for i in infos]
     dense = sum(1 for s in specs if s.p.op_kind == capi.OP_DENSE)
     dense_bytes = sum(4 * s.p.m * s.p.n_cols for s in specs if s.p.op_kind == capi.OP_DENSE)
+    # HBM floor of the dense instances: A read once per iteration (the
+    # one-pass normal product) plus the initial A^T b, at the measured copy rate
+    peak, _ = peak_hbm()
+    floor_ms = sum(4.0 * s.p.m * s.p.n_cols * (it + 1) for s, it in zip(specs, iters)
+                   if s.p.op_kind == capi.OP_DENSE) / (peak * 1e9) * 1e3
+    # the ray instances alone: where batching removes launch and latency cost
+    rays = [k for k, s in enumerate(specs) if s.p.op_kind != capi.OP_DENSE]
+    sub = {}
+    if rays:
+        rplan = capi.Plan([specs[k] for k in rays], [opts[k] for k in rays], graph=True, device_inputs=True)
+        rsolve = lambda: rplan.solve([bs[k] for k in rays], [us[k] for k in rays], stream=stream.cuda_stream)  # noqa: E731
+        cx.event_time(rsolve, 1)
+        trb, _ = cx.event_time(rsolve, 2)
+        rplan.close()
+        rsingles = [capi.Plan([specs[k]], [opts[k]], graph=False, device_inputs=True) for k in rays]
+
+        def rplain():
+            for p, k in zip(rsingles, rays):
+                p.solve([bs[k]], [us[k]], stream=stream.cuda_stream)
+        cx.event_time(rplain, 1)
+        trp, _ = cx.event_time(rplain, 1)
+        for p in rsingles:
+            p.close()
+        sub = {"instances": len(rays), "batched_ms": float(np.mean(trb)), "plain_ms": float(np.mean(trp)),
+               "batched_over_plain": float(np.mean(trp)) / float(np.mean(trb))}
     return {"metric": METRIC, "value": world * nb * 1000.0 / ms_b, "unit": "reconstructions/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_b, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantoms and operators)",
@@ -552,6 +577,7 @@ def run_batch(a, cx, capi, world, dist, clocks):
             "plain": {"value": world * nb * 1000.0 / ms_p, "unit": "reconstructions/s", "ms_per_step": ms_p,
                       "form": "one plan per instance, host-driven loop, instances in sequence"},
             "batched_over_plain": ms_p / ms_b, "iterations_min_max": [min(iters), max(iters)],
+            "dense_hbm_floor_ms": floor_ms, "ray_instances_only": sub,
             "clocks": clk, "gpu_launches": launches}
 
 

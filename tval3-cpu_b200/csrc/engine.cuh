@@ -83,6 +83,7 @@ enum Pred {
 	P_NEED_MLP,     // multiplier update and continuation
 	P_ACTIVE_MUL,   // active and the A^T multiplication is not skipped
 	P_RESTART_MUL,  // restarting (the restart always multiplies)
+	P_FIRST,        // active and the step length needs the first-iteration form (or a restart)
 };
 
 __device__ __forceinline__ bool pred_ok(const Ctrl &c, int p) {
@@ -96,6 +97,7 @@ __device__ __forceinline__ bool pred_ok(const Ctrl &c, int p) {
 	case P_NEED_MLP: return c.need_mlp != 0;
 	case P_ACTIVE_MUL: return c.active != 0 && c.skip_adj == 0;
 	case P_RESTART_MUL: return c.restart != 0;
+	case P_FIRST: return c.active != 0 && (c.fst != 0 || c.restart != 0);
 	}
 	return false;
 }
@@ -196,7 +198,7 @@ constexpr int TILE_M = 1024;
 constexpr int BLOCK = 256;
 constexpr int EPT = TILE / BLOCK;
 constexpr int EPT_M = TILE_M / BLOCK;
-constexpr int NSUM = 6;          // partial sums per tile
+constexpr int NSUM = 10;         // partial sums per tile
 constexpr int TRACE_DOUBLES = (int)(sizeof(tval3g_trace_record) / sizeof(double));
 
 // tile maps

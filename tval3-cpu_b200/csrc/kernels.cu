@@ -253,9 +253,9 @@ __global__ void __launch_bounds__(BLOCK) k_D(KArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// update_W (2d:651-671), first part: shrinkage W, lam1, lam2, lam4.  The
-// second part, g2 = Dt(DU - W), needs the neighbours' W and runs in k_grad,
-// the next kernel of the iteration, from the stored W.
+// update_W (2d:651-671) at initialisation: shrinkage W, lambda1, lambda2,
+// lambda4 (g2 follows in k_getg).  In the inner loop update_W runs inside
+// k_shrink_grad.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(BLOCK) k_shrink(KArgs a) {
 	KPROLOGUE(a);
@@ -283,17 +283,8 @@ __global__ void __launch_bounds__(BLOCK) k_shrink(KArgs a) {
 	double tot[3];
 	if (!tile_reduce<3>(I, local, I.ntn, v, tot)) return;
 	if (threadIdx.x != 0) return;
-	if (a.stage == ST_LOOP) {
-		c.f -= (c.lam1 + c.beta / 2 * c.lam2 - c.lam4);
-		c.lam1 = tot[0]; c.lam2 = tot[1]; c.lam4 = tot[2];
-		c.f += (c.lam1 + c.beta / 2 * c.lam2 - c.lam4);
-		// nonmonotone reference values (2d:802)
-		double Qp = c.Q;
-		c.Q = c.gam * Qp + 1;
-		c.C = (c.gam * Qp * c.C + c.f) / c.Q;
-	} else {
-		c.lam1 = tot[0]; c.lam2 = tot[1]; c.lam4 = tot[2];
-	}
+	c.lam1 = tot[0]; c.lam2 = tot[1]; c.lam4 = tot[2];
+	set_conds(a.cs, c);
 }
 
 // component cc of D U at j, from U (2d:268-278, 3d:365-389)
@@ -308,14 +299,6 @@ __device__ __forceinline__ float g2_at_u(const Inst &I, const Geo &g, int i, int
 	const float *__restrict__ U = I.vn[vU];
 	const float *const Wc[3] = {I.vn[vWx], I.vn[vWy], I.vn[vWz]};
 	auto V = [&](int cc) { return [&, cc](int j) { return du_at(U, g, j, cc) - Wc[cc][j]; }; };
-	return dt_at(g, i, x, y, z, V(0), V(1), V(2));
-}
-
-// g2 at i: Dt(DU - W) from the stored gradient components and W (2d:280-293)
-__device__ __forceinline__ float g2_at(const Inst &I, const Geo &g, int i, int x, int y, int z) {
-	const float *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
-	const float *const Wc[3] = {I.vn[vWx], I.vn[vWy], I.vn[vWz]};
-	auto V = [&](int cc) { return [&, cc](int j) { return Uc[cc][j] - Wc[cc][j]; }; };
 	return dt_at(g, i, x, y, z, V(0), V(1), V(2));
 }
 
@@ -385,9 +368,7 @@ __global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// get_gradient (2d:578-585) and the inner stopping test (2d:803-817)
-//   ST_LOOP:  g2 = Dt(DU - W) (the end of update_W, 2d:651-671);
-//             uup = U - Up; d = DtsAtd + g2 + muDbeta*g; RelChg
+// get_gradient (2d:578-585) outside the inner loop:
 //   ST_INIT:  d = DtsAtd + g2 + muDbeta*g (DtsAtd = 0); Q = 1, C = f
 //   ST_OUTER: DtsAtd = (beta0/beta) d; d = ... (2d:844-852)
 // ---------------------------------------------------------------------------
@@ -396,71 +377,25 @@ __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 	Ctrl &c = *I.ctrl;
 	const float mdb = (float)c.muDbeta;
 	const float bscale = a.stage == ST_OUTER ? (float)(c.beta0 / c.beta) : 1.f;
-	float *__restrict__ dts = I.vn[vDts], *__restrict__ d = I.vn[vD], *__restrict__ uup = I.vn[vUUP];
+	float *__restrict__ dts = I.vn[vDts], *__restrict__ d = I.vn[vD];
 	const float *__restrict__ g2 = I.vn[vG2], *__restrict__ gv = I.vn[vG];
-	const float *__restrict__ U = I.vn[vU], *__restrict__ Up = I.vn[vUp];
-	// distance to Ut after the iteration (trace / time-to-solution target)
-	const bool ut = a.stage == ST_LOOP && I.ut_user && (I.trace || I.target > 0);
-	const float scl = (float)c.scl;
-	double v[5] = {0, 0, 0, 0, 0};   // |d|^2, |Up|^2, |uup|^2, |U/scl - Ut|^2, |Ut|^2
-	Geo geo(I);
+	double v[1] = {0};   // |d|^2
 	FOR_TILE(local * TILE, (int)I.n, i) {
-		float g2i;
-		if (a.stage == ST_LOOP) {
-			int x, y, z;
-			geo.coords(i, x, y, z);
-			g2i = g2_at(I, geo, i, x, y, z);
-			I.vn[vG2][i] = g2i;
-		} else {
-			g2i = g2[i];
-		}
-		if (ut) {
-			float t = I.ut_user[i];
-			float e = U[i] / scl - t;
-			v[3] += (double)e * e;
-			v[4] += (double)t * t;
-		}
 		float t = dts[i];
 		if (a.stage == ST_OUTER) {
 			t = d[i] * bscale;
 			dts[i] = t;
 		}
-		float dv = t + g2i;
+		float dv = t + g2[i];
 		dv = fmaf(mdb, gv[i], dv);
 		d[i] = dv;
 		v[0] += (double)dv * dv;
-		if (a.stage == ST_LOOP) {
-			float up = Up[i];
-			float uu = U[i] - up;
-			uup[i] = uu;
-			v[1] += (double)up * up;
-			v[2] += (double)uu * uu;
-		}
 	}
-	double tot[5];
-	if (!tile_reduce<5>(I, local, I.ntn, v, tot)) return;
+	double tot[1];
+	if (!tile_reduce<1>(I, local, I.ntn, v, tot)) return;
 	if (threadIdx.x != 0) return;
 	c.dd = tot[0];
-	if (a.stage == ST_LOOP) {
-		c.count_total++;
-		c.nrmup = sqrt(tot[1]);
-		c.relchg = sqrt(tot[2]) / c.nrmup;
-		c.relerr_ut = ut ? sqrt(tot[3]) / sqrt(tot[4]) : 0.0;
-		if (I.trace && c.count_total <= I.maxit) {
-			double *t = I.trace + (long long)(c.count_total - 1) * TRACE_DOUBLES;
-			t[0] = c.tau; t[1] = c.f; t[2] = c.relchg; t[3] = c.bt_cnt; t[4] = c.skip_adj; t[5] = c.relerr_ut;
-			t[6] = c.step; t[7] = 0;
-		}
-		c.bt_cnt = 0;
-		bool brk = (c.relchg < I.tol_inn) && !c.fst;
-		c.inner_break = brk || c.count_total >= I.maxit;
-		if (!brk) c.fst = 0;
-		if (ut && I.target > 0 && c.relerr_ut <= I.target) {   // time-to-solution target reached
-			c.active = 0;
-			c.inner_break = 0;
-		}
-		if (bad(c.dd)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; c.inner_break = 0; }
-	} else if (a.stage == ST_INIT) {
+	if (a.stage == ST_INIT) {
 		c.Q = 1; c.C = c.f;
 		c.count_outer = 0; c.count_total = 0; c.fst = 1;
 		c.active = (I.maxcnt > 0 && I.maxit > 0);
@@ -468,6 +403,128 @@ __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 	} else {   // ST_OUTER
 		c.need_mlp = 0; c.fst = 1; c.inner_break = 0;
 		c.gam = I.gam0; c.Q = 1; c.C = c.f;
+	}
+	set_conds(a.cs, c);
+}
+
+// ---------------------------------------------------------------------------
+// The inner loop's update_W (2d:651-671) and get_gradient with the inner
+// stopping test (2d:578-585, 803-817) in one pass over the image:
+//   W = shrink(U_c - sigma_c / beta) at the pixel, stored, and recomputed
+//   from their U_c and sigma_c at the pixels Dt reads; g2 = Dt(DU - W);
+//   d = DtsAtd + g2 + muDbeta*g; uup = U - Up; the sums of both steps.
+// The last tile runs update_W's scalar step (f, the nonmonotone reference
+// values Q and C, 2d:802) and then the inner loop's (RelChg, stopping test,
+// trace, time-to-solution target).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(BLOCK) k_shrink_grad(KArgs a) {
+	KPROLOGUE(a);
+	Ctrl &c = *I.ctrl;
+	Geo g(I);
+	Shrink sh(I, c.beta);
+	const int dims = I.dims;
+	const float *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
+	const float *const Sc[3] = {I.vn[vSx], I.vn[vSy], I.vn[vSz]};
+	const float mdb = (float)c.muDbeta;
+	float *__restrict__ d = I.vn[vD], *__restrict__ uup = I.vn[vUUP];
+	const float *__restrict__ dts = I.vn[vDts], *__restrict__ gv = I.vn[vG];
+	const float *__restrict__ U = I.vn[vU], *__restrict__ Up = I.vn[vUp];
+	// distance to Ut after the iteration (trace / time-to-solution target)
+	const bool ut = I.ut_user && (I.trace || I.target > 0);
+	const float rscl = (float)(1.0 / c.scl);
+	// the next iteration's Barzilai-Borwein step (get_tau, 2d:444-451) from
+	// this iteration's uup, g - gp, g2 - g2p (schedule mode: k_tau_prep, as
+	// mu and beta change before that step)
+	const bool bb = !I.sched;
+	const float *__restrict__ gp = I.vn[vGp], *__restrict__ g2p = I.vn[vG2p];
+	// lam1, lam2, lam4, |d|^2, |Up|^2, |uup|^2, |U/scl - Ut|^2, |Ut|^2, <uup, dg2 + muDbeta dg>
+	double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+	FOR_TILE(local * TILE, g.n, i) {
+		int x, y, z;
+		g.coords(i, x, y, z);
+		float u[3], s[3], w[3];
+#pragma unroll
+		for (int cc = 0; cc < 3; cc++) {
+			u[cc] = cc < dims ? Uc[cc][i] : 0.f;
+			s[cc] = cc < dims ? Sc[cc][i] : 0.f;
+		}
+		v[0] += sh.apply(u, s, w);
+#pragma unroll
+		for (int cc = 0; cc < 3; cc++)
+			if (cc < dims) {
+				I.vn[vWx + cc][i] = w[cc];
+				const float vv = u[cc] - w[cc];
+				v[1] += (double)vv * vv;
+				v[2] += (double)s[cc] * vv;
+			}
+		// component cc of DU - W at j (the neighbours' W recomputed)
+		auto V = [&](int cc) {
+			return [&, cc](int j) -> float {
+				if (j == i) return u[cc] - w[cc];
+				float uj[3], sj[3], wj[3];
+#pragma unroll
+				for (int k = 0; k < 3; k++) {
+					uj[k] = k < dims ? Uc[k][j] : 0.f;
+					sj[k] = k < dims ? Sc[k][j] : 0.f;
+				}
+				sh.apply(uj, sj, wj);
+				return uj[cc] - wj[cc];
+			};
+		};
+		const float g2i = dt_at(g, i, x, y, z, V(0), V(1), V(2));
+		I.vn[vG2][i] = g2i;
+		float dv = dts[i] + g2i;
+		dv = fmaf(mdb, gv[i], dv);
+		d[i] = dv;
+		v[3] += (double)dv * dv;
+		const float up = Up[i], uu = U[i] - up;
+		uup[i] = uu;
+		v[4] += (double)up * up;
+		v[5] += (double)uu * uu;
+		if (bb) {
+			const float tmp = fmaf(mdb, gv[i] - gp[i], g2i - g2p[i]);
+			v[8] += (double)uu * tmp;
+		}
+		if (ut) {
+			const float t = I.ut_user[i], e = U[i] * rscl - t;
+			v[6] += (double)e * e;
+			v[7] += (double)t * t;
+		}
+	}
+	double tot[9];
+	if (!tile_reduce<9>(I, local, I.ntn, v, tot)) return;
+	if (threadIdx.x != 0) return;
+	// update_W: objective and nonmonotone reference values
+	c.f -= (c.lam1 + c.beta / 2 * c.lam2 - c.lam4);
+	c.lam1 = tot[0]; c.lam2 = tot[1]; c.lam4 = tot[2];
+	c.f += (c.lam1 + c.beta / 2 * c.lam2 - c.lam4);
+	const double Qp = c.Q;
+	c.Q = c.gam * Qp + 1;
+	c.C = (c.gam * Qp * c.C + c.f) / c.Q;
+	// get_gradient and the inner stopping test
+	c.dd = tot[3];
+	c.count_total++;
+	c.nrmup = sqrt(tot[4]);
+	c.relchg = sqrt(tot[5]) / c.nrmup;
+	c.relerr_ut = ut ? sqrt(tot[6]) / sqrt(tot[7]) : 0.0;
+	if (I.trace && c.count_total <= I.maxit) {
+		double *t = I.trace + (long long)(c.count_total - 1) * TRACE_DOUBLES;
+		t[0] = c.tau; t[1] = c.f; t[2] = c.relchg; t[3] = c.bt_cnt; t[4] = c.skip_adj; t[5] = c.relerr_ut;
+		t[6] = c.step; t[7] = 0;
+	}
+	c.bt_cnt = 0;
+	const bool brk = (c.relchg < I.tol_inn) && !c.fst;
+	c.inner_break = brk || c.count_total >= I.maxit;
+	if (!brk) c.fst = 0;
+	if (ut && I.target > 0 && c.relerr_ut <= I.target) {   // time-to-solution target reached
+		c.active = 0;
+		c.inner_break = 0;
+	}
+	if (bad(c.dd)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; c.inner_break = 0; }
+	// the next iteration's step length when it takes the Barzilai-Borwein form
+	if (bb && c.active && !c.inner_break && !c.fst) {
+		c.tau = fabs(tot[5] / tot[8]);
+		if (bad(c.tau)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; }
 	}
 	set_conds(a.cs, c);
 }
@@ -883,6 +940,7 @@ LAUNCHER(launch_D, k_D)
 LAUNCHER(launch_shrink, k_shrink)
 LAUNCHER(launch_getg, k_getg)
 LAUNCHER(launch_grad, k_grad)
+LAUNCHER(launch_shrink_grad, k_shrink_grad)
 LAUNCHER(launch_tau_prep, k_tau_prep)
 LAUNCHER(launch_tau_first, k_tau_first)
 LAUNCHER(launch_descend, k_descend)

@@ -47,6 +47,7 @@ void launch_D(cudaStream_t s, const KArgs &a);
 void launch_shrink(cudaStream_t s, const KArgs &a);
 void launch_getg(cudaStream_t s, const KArgs &a);
 void launch_grad(cudaStream_t s, const KArgs &a);
+void launch_shrink_grad(cudaStream_t s, const KArgs &a);
 void launch_tau_prep(cudaStream_t s, const KArgs &a);
 void launch_tau_first(cudaStream_t s, const KArgs &a);
 void launch_descend(cudaStream_t s, const KArgs &a);

@@ -745,8 +745,10 @@ void Plan::emit_iteration(unsigned long long h_active) {
 	const VecSel U{false, vU}, G{false, vG}, D{false, vD};
 	const VecSel Au{true, vAu}, Ad{true, vAd};
 	// min_u (2d:526-576): step length
+	// (the Barzilai-Borwein form comes from the previous k_shrink_grad, except
+	// in schedule mode, where mu and beta change at the iteration's start)
 	const unsigned long long h_ad = cond_handle();
-	launch_tau_prep(s, kargs(MAP_N, P_ACTIVE).cond(h_ad, P_NEED_AD));
+	launch_tau_prep(s, kargs(MAP_N, sched_mode_ ? P_ACTIVE : P_FIRST).cond(h_ad, P_NEED_AD));
 	if_(P_NEED_AD, [&] {
 		op_forward(lctx(), ob_, P_NEED_AD, D, Ad);
 		launch_tau_first(es(), kargs(MAP_M, P_NEED_AD));
@@ -783,9 +785,8 @@ void Plan::emit_iteration(unsigned long long h_active) {
 		}, h_restart);
 	}, h_bt);
 	// update_W, reference values, gradient, inner stopping test
-	launch_shrink(es(), kargs(MAP_N, P_ACTIVE, ST_LOOP));
 	const unsigned long long h_brk = cond_handle();
-	launch_grad(es(), kargs(MAP_N, P_ACTIVE, ST_LOOP).cond(h_brk, P_INNER_BREAK).cond(h_active, P_ACTIVE));
+	launch_shrink_grad(es(), kargs(MAP_N, P_ACTIVE, ST_LOOP).cond(h_brk, P_INNER_BREAK).cond(h_active, P_ACTIVE));
 	// outer step: stopping test, multipliers, continuation
 	if_(P_INNER_BREAK, [&] {
 		launch_outer(es(), kargs(MAP_N, P_INNER_BREAK));
