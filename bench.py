@@ -229,6 +229,17 @@ class Ctx:
         return out, res
 
 
+def max_over_ranks(dist, values, device):
+    """Each value's maximum over the ranks (the job's time is its slowest
+    rank's); the values unchanged without a process group."""
+    if not dist:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
 def peak_hbm():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peaks = json.load(open(p)) if os.path.exists(p) else {}
@@ -342,11 +353,7 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
     if dist:
         dist.barrier()
     clk = clocks.stop()
-    ms = float(np.mean(times))
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(dist, [float(np.mean(times))], dev)[0]
     iters = infos[0]["total_iters"]
     relerr = float(infos[0]["rel_error"]) if ref is not None else None
     curve = plan.trace(0)[:, 5] if ref is not None else []
@@ -438,10 +445,7 @@ def run_mrhs(a, cx, capi, world, dist, clocks):
         res[tensor] = (float(np.mean(ts)), infos[0])
         plan.close()
     ms, info = res[True]
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(dist, [ms], dev)[0]
     per_rhs = None
     if ref is not None:
         R = ref["U"].reshape(N, -1)
@@ -536,11 +540,7 @@ def run_batch(a, cx, capi, world, dist, clocks):
     tp, _ = cx.event_time(plain, 1)
     for p in singles:
         p.close()
-    ms_p = float(np.mean(tp))
-    if dist:
-        t = torch.tensor([ms_b, ms_p], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_b, ms_p = (float(x) for x in t.tolist())
+    ms_b, ms_p = max_over_ranks(dist, [ms_b, float(np.mean(tp))], dev)
     iters = [i["total_iters"] for i in infos]
     dense = sum(1 for s in specs if s.p.op_kind == capi.OP_DENSE)
     dense_bytes = sum(4 * s.p.m * s.p.n_cols for s in specs if s.p.op_kind == capi.OP_DENSE)

@@ -83,8 +83,7 @@ int tval3g_solve_batch(int count, const tval3g_problem *probs, const float *cons
 		~Guard() {
 			cudaStreamSynchronize(s);
 			for (auto *v : {a, b, c})
-				for (float *p : *v)
-					if (p) cudaFree(p);
+				for (float *p : *v) dev_free(p, s);
 			cudaStreamDestroy(s);
 		}
 	} guard{&db, &du, &dut, s};
@@ -92,11 +91,11 @@ int tval3g_solve_batch(int count, const tval3g_problem *probs, const float *cons
 		const tval3g_problem &p = probs[i];
 		long long n = (long long)p.dim_x * p.dim_y * (p.dims == 3 ? p.dim_z : 1), bl = b_len_of(p);
 		ns[i] = n;
-		TG_CUDA(cudaMalloc(&db[i], sizeof(float) * bl));
-		TG_CUDA(cudaMalloc(&du[i], sizeof(float) * n));
+		db[i] = (float *)dev_alloc(sizeof(float) * bl, s);
+		du[i] = (float *)dev_alloc(sizeof(float) * n, s);
 		TG_CUDA(cudaMemcpyAsync(db[i], b[i], sizeof(float) * bl, cudaMemcpyHostToDevice, s));
 		if (Ut && Ut[i]) {
-			TG_CUDA(cudaMalloc(&dut[i], sizeof(float) * n));
+			dut[i] = (float *)dev_alloc(sizeof(float) * n, s);
 			TG_CUDA(cudaMemcpyAsync(dut[i], Ut[i], sizeof(float) * n, cudaMemcpyHostToDevice, s));
 		}
 	}
@@ -234,7 +233,7 @@ int tval3g_op_create(tval3g_operator **out, const tval3g_problem *prob, int flag
 		TG_CUDA(cudaMalloc(&op->d_inst, sizeof(Inst)));
 		TG_CUDA(cudaStreamSynchronize(op->s));
 	} catch (...) {
-		free_op(op->st);
+		free_op(op->st, op->s);
 		delete op;
 		throw;
 	}
@@ -345,7 +344,7 @@ int tval3g_op_destroy(tval3g_operator *op) {
 	CAPI_BEGIN
 	if (op) {
 		if (op->s) cudaStreamSynchronize(op->s);
-		free_op(op->st);
+		free_op(op->st, op->s);
 		cudaFree(op->d_inst);
 		cudaFree(op->d_ctrl);
 		cudaFree(op->d_tiles);

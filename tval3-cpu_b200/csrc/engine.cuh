@@ -38,6 +38,14 @@ struct Error {
 		if (e_ != cudaSuccess)                                                                      \
 			throw ::tval3g::Error{TVAL3G_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
 	} while (0)
+// Device memory of plans, operators and host-buffer solves: stream-ordered
+// allocations from a per-device pool of this library that keeps freed blocks
+// for reuse (unlimited release threshold), so repeated solves do not go back
+// to the driver for their buffers and no free synchronises the device.  A
+// block may be freed only when no queued work still uses it.
+void *dev_alloc(size_t bytes, cudaStream_t s);
+void dev_free(void *p, cudaStream_t s);
+
 #define TG_ARG(cond, msg)                                                                           \
 	do {                                                                                            \
 		if (!(cond)) throw ::tval3g::Error{TVAL3G_ERR_ARGUMENT, (msg)};                             \

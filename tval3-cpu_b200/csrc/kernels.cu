@@ -595,6 +595,7 @@ __global__ void __launch_bounds__(BLOCK) k_tau_first(KArgs a) {
 	c.tau = fabs(c.dd / (c.dDd + c.muDbeta * tot[0]));
 	c.need_Ad = 0;
 	if (bad(c.tau)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; c.restart = 0; c.need_bt = 0; }
+	set_conds(a.cs, c);
 }
 
 // ---------------------------------------------------------------------------

@@ -917,8 +917,7 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 	TG_CUDA(cudaMallocAsync(&tptr, sizeof(long long) * (nt + 1), s));
 	TG_CUDA(cudaMallocAsync(&wlen, sizeof(long long) * (nw + 1), s));
 	TG_CUDA(cudaMallocAsync(&woff, sizeof(long long) * (nw + 1), s));
-	unsigned char *perm = nullptr;
-	TG_CUDA(cudaMalloc(&perm, (size_t)nt * RAYT_THREADS));
+	unsigned char *perm = (unsigned char *)dev_alloc((size_t)nt * RAYT_THREADS, s);
 	k_tile_count<<<nt, RAYT_THREADS, smem_count, s>>>(ld, H, ntx, nrays, cptr, cind, tlen, wlen, perm);
 	TG_CUDA(cudaGetLastError());
 	scan_counts(s, tlen, tptr, nt);
@@ -932,13 +931,11 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 	for (int t = 0; t < nt; t++) tmax = std::max(tmax, h_tptr[t + 1] - h_tptr[t]);
 	const bool ok = tmax <= RAYT_MAX_LIST && words < (1LL << 31) && h_tptr[nt] < (1LL << 31);
 	if (ok) {
-		int *tmeas = nullptr, *tptr32 = nullptr, *woff32 = nullptr;
-		uint4 *sidx = nullptr;
-		TG_CUDA(cudaMalloc(&tmeas, sizeof(int) * (size_t)std::max(h_tptr[nt], 4LL)));
+		int *tmeas = (int *)dev_alloc(sizeof(int) * (size_t)std::max(h_tptr[nt], 4LL), s);
 		TG_CUDA(cudaMemsetAsync(tmeas, 0, sizeof(int) * (size_t)std::max(h_tptr[nt], 4LL), s));
-		TG_CUDA(cudaMalloc(&sidx, sizeof(uint4) * (size_t)std::max(words, 1LL)));
-		TG_CUDA(cudaMalloc(&tptr32, sizeof(int) * (nt + 1)));
-		TG_CUDA(cudaMalloc(&woff32, sizeof(int) * (nw + 1)));
+		uint4 *sidx = (uint4 *)dev_alloc(sizeof(uint4) * (size_t)std::max(words, 1LL), s);
+		int *tptr32 = (int *)dev_alloc(sizeof(int) * (nt + 1), s);
+		int *woff32 = (int *)dev_alloc(sizeof(int) * (nw + 1), s);
 		owned.push_back(tmeas); owned.push_back(sidx); owned.push_back(tptr32); owned.push_back(woff32);
 		k_tile_fill<<<nt, RAYT_THREADS, smem_fill, s>>>(ld, H, ntx, nrays, cptr, cind, live_out, tptr, woff, perm,
 		                                                tmeas, sidx);
@@ -956,7 +953,7 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 		*bytes = (long long)sizeof(uint4) * words + (long long)sizeof(int) * (h_tptr[nt] + nt + nw + 2) +
 		         (long long)nt * RAYT_THREADS;
 	} else {
-		TG_CUDA(cudaFree(perm));
+		dev_free(perm, s);
 	}
 	TG_CUDA(cudaFreeAsync(tlen, s));
 	TG_CUDA(cudaFreeAsync(tptr, s));

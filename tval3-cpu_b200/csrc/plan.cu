@@ -6,7 +6,42 @@
 
 #include "plan.cuh"
 
+#include <map>
+#include <mutex>
+
 namespace tval3g {
+
+cudaMemPool_t library_pool() {
+	static std::mutex mu;
+	static std::map<int, cudaMemPool_t> pools;
+	int dev = 0;
+	TG_CUDA(cudaGetDevice(&dev));
+	std::lock_guard<std::mutex> lock(mu);
+	auto it = pools.find(dev);
+	if (it != pools.end()) return it->second;
+	cudaMemPoolProps props;
+	std::memset(&props, 0, sizeof(props));
+	props.allocType = cudaMemAllocationTypePinned;
+	props.location.type = cudaMemLocationTypeDevice;
+	props.location.id = dev;
+	cudaMemPool_t pool;
+	TG_CUDA(cudaMemPoolCreate(&pool, &props));
+	unsigned long long keep = ~0ull;
+	TG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+	pools[dev] = pool;
+	return pool;
+}
+
+void *dev_alloc(size_t bytes, cudaStream_t s) {
+	void *p = nullptr;
+	TG_CUDA(cudaMallocFromPoolAsync(&p, std::max<size_t>(bytes, 16), library_pool(), s));
+	return p;
+}
+
+void dev_free(void *p, cudaStream_t s) {
+	if (p) cudaFreeAsync(p, s);
+}
+
 
 // ---------------------------------------------------------------------------
 // validation (2d/tval3_cpu_2d.cpp:696-750, 3d/tval3_cpu_3d.cpp:1028-1165)
@@ -104,18 +139,16 @@ void check_options(const tval3g_options &o) {
 template <class T>
 static T *dcopy(cudaStream_t s, OpStore &st, const T *src, long long count, bool borrow) {
 	if (borrow) return const_cast<T *>(src);
-	T *d = nullptr;
 	size_t bytes = sizeof(T) * (size_t)std::max(count, 1LL);
-	TG_CUDA(cudaMalloc(&d, bytes));
+	T *d = (T *)dev_alloc(bytes, s);
 	st.owned.push_back(d);
 	st.bytes += (long long)bytes;
 	if (count > 0) TG_CUDA(cudaMemcpyAsync(d, src, sizeof(T) * (size_t)count, cudaMemcpyHostToDevice, s));
 	return d;
 }
 template <class T>
-static T *dalloc_op(OpStore &st, long long count) {
-	T *d = nullptr;
-	TG_CUDA(cudaMalloc(&d, sizeof(T) * (size_t)std::max(count, 1LL)));
+static T *dalloc_op(cudaStream_t s, OpStore &st, long long count) {
+	T *d = (T *)dev_alloc(sizeof(T) * (size_t)std::max(count, 1LL), s);
 	st.owned.push_back(d);
 	st.bytes += (long long)(sizeof(T) * (size_t)std::max(count, 1LL));
 	return d;
@@ -156,9 +189,9 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		d.rptr = dcopy(s, st, p.csr_ptr, (long long)p.m + 1, borrow);
 		d.rind = dcopy(s, st, p.csr_ind, p.nnz, borrow);
 		d.rval = dcopy(s, st, p.csr_val, p.nnz, borrow);
-		int *cptr = dalloc_op<int>(st, d.n + 1);
-		int *cind = dalloc_op<int>(st, p.nnz);
-		float *cval = dalloc_op<float>(st, p.nnz);
+		int *cptr = dalloc_op<int>(s, st, d.n + 1);
+		int *cind = dalloc_op<int>(s, st, p.nnz);
+		float *cval = dalloc_op<float>(s, st, p.nnz);
 		build_transpose(s, d.m, d.n, p.nnz, d.rptr, d.rind, d.rval, cptr, cind, cval);
 		d.cptr = cptr; d.cind = cind; d.cval = cval;
 		st.adj_index_bytes = (long long)sizeof(int) * (d.n + 1) + 8LL * p.nnz;
@@ -203,28 +236,28 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		d.rvx = is3 ? p.rv_x : p.ld;
 		d.rvy = is3 ? p.rv_y : 1;
 		d.scale = p.scale_factor;
-		int4 *drays = dalloc_op<int4>(st, d.nrays);
+		int4 *drays = dalloc_op<int4>(s, st, d.nrays);
 		if (d.nrays > 0)
 			TG_CUDA(cudaMemcpyAsync(drays, rays.data(), sizeof(int4) * rays.size(), cudaMemcpyHostToDevice, s));
 		d.rays = drays;
 		// forward CSR over traced rays, then its transpose: the pixel-major
 		// index of the adjoint, entries = measurement indices sorted by ray
-		int *rptr = dalloc_op<int>(st, (long long)d.nrays + 1);
+		int *rptr = dalloc_op<int>(s, st, (long long)d.nrays + 1);
 		long long total = 0;
 		trace_rays(s, d.nrays, drays, d.rvx, d.rvy, rptr, nullptr, &total);
-		int *rind = dalloc_op<int>(st, total);
+		int *rind = dalloc_op<int>(s, st, total);
 		trace_rays(s, d.nrays, drays, d.rvx, d.rvy, rptr, rind, &total);
 		st.nnz = total;
-		int *cptr = dalloc_op<int>(st, n + 1);
-		int *cind = dalloc_op<int>(st, total);
+		int *cptr = dalloc_op<int>(s, st, n + 1);
+		int *cind = dalloc_op<int>(s, st, total);
 		build_transpose(s, d.nrays, n, total, rptr, rind, nullptr, cptr, cind, nullptr);
 		if (!is3 && n % p.ld == 0) {   // transposed image for the y-driven rays
-			d.xT = dalloc_op<float>(st, n);
+			d.xT = dalloc_op<float>(s, st, n);
 			d.tH = (int)(n / p.ld);
 		}
 		if (!is3 && n % p.ld == 0 && d.nrays > 0 && d.nrays <= RAYT_MAX_RAYS) {
 			// tiled adjoint (cind still holds traced-ray ids)
-			int *lo = dalloc_op<int>(st, d.nrays);
+			int *lo = dalloc_op<int>(s, st, d.nrays);
 			TG_CUDA(cudaMemcpyAsync(lo, st.ray_out.data(), sizeof(int) * d.nrays, cudaMemcpyHostToDevice, s));
 			long long ib = 0;
 			if (build_tiled_index(s, (int)p.ld, (int)(n / p.ld), d.nrays, cptr, cind, lo, d, &ib, st.owned)) {
@@ -241,15 +274,14 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		if (!keep_ray_csr) {
 			TG_CUDA(cudaStreamSynchronize(s));
 			for (void *&q : st.owned)
-				if (q == rptr || q == rind) { cudaFree(q); q = nullptr; }
+				if (q == rptr || q == rind) { dev_free(q, s); q = nullptr; }
 			st.ray_rptr = st.ray_rind = nullptr;
 		}
 	}
 }
 
-void free_op(OpStore &st) {
-	for (void *q : st.owned)
-		if (q) cudaFree(q);
+void free_op(OpStore &st, cudaStream_t s) {
+	for (void *q : st.owned) dev_free(q, s);
 	st.owned.clear();
 	st.mrhs.reset();
 }
@@ -271,8 +303,7 @@ struct TileBuilder {
 		cur.clear();
 	}
 	int2 *upload(cudaStream_t s) {
-		int2 *d = nullptr;
-		TG_CUDA(cudaMalloc(&d, sizeof(int2) * std::max<size_t>(all.size(), 1)));
+		int2 *d = (int2 *)dev_alloc(sizeof(int2) * std::max<size_t>(all.size(), 1), s);
 		if (!all.empty())
 			TG_CUDA(cudaMemcpyAsync(d, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, s));
 		for (auto &p : pend) {
@@ -423,8 +454,7 @@ long long build_op_maps_upload(std::vector<Inst> &inst, const std::vector<OpStor
 // Plan
 // ---------------------------------------------------------------------------
 void *Plan::dalloc(size_t bytes) {
-	void *p = nullptr;
-	TG_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+	void *p = dev_alloc(bytes, stream_);
 	allocs_.push_back(p);
 	device_bytes_ += (long long)bytes;
 	return p;
@@ -534,7 +564,6 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 		TG_CUDA(cudaMemcpyAsync(d_inst_, h_inst_.data(), sizeof(Inst) * count, cudaMemcpyHostToDevice, stream_));
 		d_flag_ = (int *)dalloc(sizeof(int));
 		d_launches_ = (unsigned long long *)dalloc(sizeof(unsigned long long));
-		TG_CUDA(cudaMallocHost(&h_flag_, sizeof(int)));
 		for (auto &o : ops_) device_bytes_ += o.bytes;
 		TG_CUDA(cudaStreamSynchronize(stream_));
 	} catch (...) {
@@ -563,13 +592,11 @@ void Plan::release() {
 	if (cap_) cudaStreamDestroy(cap_);
 	cap_ = nullptr;
 	if (stream_) cudaStreamSynchronize(stream_);
-	for (void *p : allocs_) cudaFree(p);
+	for (void *p : allocs_) dev_free(p, stream_);
 	allocs_.clear();
 	ob_.mrhs.clear();
-	for (auto &o : ops_) free_op(o);
+	for (auto &o : ops_) free_op(o, stream_);
 	ops_.clear();
-	if (h_flag_) cudaFreeHost(h_flag_);
-	h_flag_ = nullptr;
 	if (stream_) cudaStreamDestroy(stream_);
 	stream_ = nullptr;
 }
@@ -624,9 +651,9 @@ unsigned long long Plan::cond_handle() {
 void Plan::if_(int pred, const std::function<void()> &body, unsigned long long hset) {
 	if (!graph_mode_) {
 		launch_cond(cur_, d_inst_, count_, pred, d_flag_, 0, d_launches_);
-		TG_CUDA(cudaMemcpyAsync(h_flag_, d_flag_, sizeof(int), cudaMemcpyDeviceToHost, cur_));
+		TG_CUDA(cudaMemcpyAsync(&h_flag_, d_flag_, sizeof(int), cudaMemcpyDeviceToHost, cur_));
 		TG_CUDA(cudaStreamSynchronize(cur_));
-		if (*h_flag_) body();
+		if (h_flag_) body();
 		return;
 	}
 	cudaGraphConditionalHandle h = (cudaGraphConditionalHandle)hset;
@@ -659,9 +686,9 @@ void Plan::while_(int pred, const std::function<void()> &body, unsigned long lon
 	if (!graph_mode_) {
 		for (;;) {
 			launch_cond(cur_, d_inst_, count_, pred, d_flag_, 0, d_launches_);
-			TG_CUDA(cudaMemcpyAsync(h_flag_, d_flag_, sizeof(int), cudaMemcpyDeviceToHost, cur_));
+			TG_CUDA(cudaMemcpyAsync(&h_flag_, d_flag_, sizeof(int), cudaMemcpyDeviceToHost, cur_));
 			TG_CUDA(cudaStreamSynchronize(cur_));
-			if (!*h_flag_) break;
+			if (!h_flag_) break;
 			body();
 		}
 		return;
@@ -713,6 +740,7 @@ void Plan::emit_program() {
 	launch_getg(s, kargs(MAP_NM, P_ALL, ST_INIT));
 	const unsigned long long h_act = cond_handle();
 	launch_grad(s, kargs(MAP_N, P_ALL, ST_INIT).cond(h_act, P_ACTIVE));
+	if (!sched_mode_) emit_first_tau(h_act);
 	(void)D; (void)Ad;
 	while_(P_ACTIVE, [&] { emit_iteration(h_act); }, h_act);
 	launch_final(es(), kargs(MAP_N, P_ALL));
@@ -736,6 +764,21 @@ void Plan::set_schedule(const double *mu, const double *beta) {
 	TG_CUDA(cudaMemcpy(d_sched_, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
 }
 
+// The first-iteration step length (get_tau, 2d:430-442) of an inner loop:
+// |D d|^2, then A d and tau.  Outside schedule mode it runs where an inner
+// loop begins - after the initialisation and after each outer step - and the
+// Barzilai-Borwein form of the other iterations comes from k_shrink_grad.
+// Its kernels also set the loop's condition (h_active).
+void Plan::emit_first_tau(unsigned long long h_active) {
+	const VecSel D{false, vD}, Ad{true, vAd};
+	const unsigned long long h_ad = cond_handle();
+	launch_tau_prep(es(), kargs(MAP_N, P_FIRST).cond(h_ad, P_NEED_AD).cond(h_active, P_ACTIVE));
+	if_(P_NEED_AD, [&] {
+		op_forward(lctx(), ob_, P_NEED_AD, D, Ad);
+		launch_tau_first(es(), kargs(MAP_M, P_NEED_AD).cond(h_active, P_ACTIVE));
+	}, h_ad);
+}
+
 // h_active: the loop's condition handle when the iteration's last kernel sets
 // it (0: a condition kernel evaluates it)
 void Plan::emit_iteration(unsigned long long h_active) {
@@ -745,14 +788,16 @@ void Plan::emit_iteration(unsigned long long h_active) {
 	const VecSel U{false, vU}, G{false, vG}, D{false, vD};
 	const VecSel Au{true, vAu}, Ad{true, vAd};
 	// min_u (2d:526-576): step length
-	// (the Barzilai-Borwein form comes from the previous k_shrink_grad, except
-	// in schedule mode, where mu and beta change at the iteration's start)
-	const unsigned long long h_ad = cond_handle();
-	launch_tau_prep(s, kargs(MAP_N, sched_mode_ ? P_ACTIVE : P_FIRST).cond(h_ad, P_NEED_AD));
-	if_(P_NEED_AD, [&] {
-		op_forward(lctx(), ob_, P_NEED_AD, D, Ad);
-		launch_tau_first(es(), kargs(MAP_M, P_NEED_AD));
-	}, h_ad);
+	// (outside schedule mode, where mu and beta change at the iteration's
+	// start, tau is ready: emit_first_tau or the previous k_shrink_grad)
+	if (sched_mode_) {
+		const unsigned long long h_ad = cond_handle();
+		launch_tau_prep(s, kargs(MAP_N, P_ACTIVE).cond(h_ad, P_NEED_AD));
+		if_(P_NEED_AD, [&] {
+			op_forward(lctx(), ob_, P_NEED_AD, D, Ad);
+			launch_tau_first(es(), kargs(MAP_M, P_NEED_AD));
+		}, h_ad);
+	}
 	// descent step and get_g
 	launch_descend(es(), kargs(MAP_NM, P_ACTIVE, ST_DESCEND));   // D U: in k_getg
 	// get_g_mult: dense instances in one pass over A (they never skip)
@@ -792,6 +837,7 @@ void Plan::emit_iteration(unsigned long long h_active) {
 		launch_outer(es(), kargs(MAP_N, P_INNER_BREAK));
 		launch_mlp(es(), kargs(MAP_NM, P_NEED_MLP));
 		launch_grad(es(), kargs(MAP_N, P_NEED_MLP, ST_OUTER).cond(h_active, P_ACTIVE));
+		if (!sched_mode_) emit_first_tau(h_active);
 	}, h_brk);
 	(void)L; (void)s;
 }

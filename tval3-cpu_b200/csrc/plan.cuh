@@ -29,7 +29,7 @@ struct OpStore {
 long long validate(const tval3g_problem &p, long long b_len, long long ut_len);
 // prepare the device operator of a problem (flags: TVAL3G_DEVICE_INPUTS)
 void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st, bool keep_ray_csr);
-void free_op(OpStore &st);
+void free_op(OpStore &st, cudaStream_t s);
 void check_options(const tval3g_options &o);
 // operator tile maps of a batch, uploaded to *d_tiles; returns the dense
 // partial-buffer size in floats
@@ -79,7 +79,7 @@ private:
 	float *d_arena_ = nullptr;
 	int2 *d_tiles_ = nullptr;
 	int *d_flag_ = nullptr;
-	int *h_flag_ = nullptr;
+	int h_flag_ = 0;                  // host copy of d_flag_ (host-driven plans)
 	unsigned long long *d_launches_ = nullptr;
 	TileMap maps_[NMAPS];
 	OpBatch ob_;
@@ -102,6 +102,7 @@ private:
 	LaunchCtx lctx() const;
 	void emit_program();
 	void emit_iteration(unsigned long long h_active);
+	void emit_first_tau(unsigned long long h_active);
 	// control flow: direct execution or graph construction
 	// Conditional regions.  With a handle from cond_handle() the kernel launched
 	// just before (and, for while_, the body's last kernel) sets the condition;
