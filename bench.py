@@ -368,12 +368,13 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
     pt, _ = cx.event_time(lambda: solve(plan_plain), 2)
     plan_plain.close()
 
-    et = []   # end to end through the host-buffer C ABI
+    et, ec = [], []   # end to end through the host-buffer C ABI
     for k in range(max(1, min(a.steps, 3)) + 1):
         t0 = time.perf_counter()
-        capi.solve(spec, b_host, opts)
+        _, e_info = capi.solve(spec, b_host, opts)
         if k > 0:
             et.append((time.perf_counter() - t0) * 1000)
+            ec.append(e_info["secs"] * 1000)
     e2e_ms = float(np.mean(et))
     in_bytes = int(b_host.nbytes + sum(x.nbytes for x in spec.keep))
 
@@ -390,7 +391,8 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
             "plain": {"value": world * 1000.0 / float(np.mean(pt)), "unit": "reconstructions/s",
                       "ms_per_step": float(np.mean(pt)), "form": "host-driven loop, one launch per kernel"},
             "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "reconstructions/s", "h2d_bytes_per_step": in_bytes,
-                    "d2h_bytes_per_step": int(spec.n * 4)},
+                    "d2h_bytes_per_step": int(spec.n * 4), "ms_each": [round(x, 3) for x in et],
+                    "ms_inside_library": [round(x, 3) for x in ec]},
             "roofline": kernel_roofline(cx, capi, spec, w, w["kind"]),
             "clocks": clk, "gpu_launches": launches}
     if rank == 0 and world == 1 and name != "hemi3d":

@@ -55,10 +55,10 @@ void dev_free(void *p, cudaStream_t s);
 // per-instance vectors
 // ---------------------------------------------------------------------------
 enum VecN {
-	vU, vUp, vdU, vUUP, vUx, vUy, vUz, vUxp, vUyp, vUzp, vdUx, vdUy, vdUz, vWx, vWy, vWz,
-	vSx, vSy, vSz, vAtb, vD, vG, vGp, vdG, vG2, vG2p, vdG2, vDts, vRcd, NVN
+	vU, vUp, vUUP, vUx, vUy, vUz, vUxp, vUyp, vUzp, vWx, vWy, vWz,
+	vSx, vSy, vSz, vAtb, vD, vG, vGp, vG2, vG2p, vDts, vRcd, NVN
 };
-enum VecM { vB, vAu, vAup, vdAu, vDelta, vLastAu, vAd, NVM };
+enum VecM { vB, vAu, vAup, vDelta, vLastAu, vAd, NVM };
 
 // scalar state of one instance (the reference's tval3_data scalars and the
 // locals of its driver, 2d/tval3_cpu_2d.cpp:99-196,752-853)
@@ -99,7 +99,7 @@ __device__ __forceinline__ bool pred_ok(const Ctrl &c, int p) {
 	case P_ALL: return true;
 	case P_ACTIVE: return c.active != 0;
 	case P_NEED_AD: return c.need_Ad != 0;
-	case P_NEED_BT: return c.need_bt != 0 && c.restart == 0;
+	case P_NEED_BT: return c.active != 0 && c.need_bt != 0 && c.restart == 0;
 	case P_RESTART: return c.restart != 0;
 	case P_INNER_BREAK: return c.inner_break != 0;
 	case P_NEED_MLP: return c.need_mlp != 0;

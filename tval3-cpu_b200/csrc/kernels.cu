@@ -325,7 +325,9 @@ __global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
 			int x, y, z;
 			g.coords(i, x, y, z);
 			gv[i] = gv[i] - atb[i];
-			g2[i] = g2_at_u(I, g, i, x, y, z);
+			// in the inner loop k_shrink_grad forms g2 again from the new W
+			// before anything reads it, so only the initialisation needs it
+			if (a.stage == ST_INIT) g2[i] = g2_at_u(I, g, i, x, y, z);
 			float du[3] = {dxf(U, g, i, x), dyf(U, g, i, y), g.dims == 3 ? dzf(U, g, i, z) : 0.f};
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++)
@@ -513,6 +515,7 @@ __global__ void __launch_bounds__(BLOCK) k_shrink_grad(KArgs a) {
 		t[6] = c.step; t[7] = 0;
 	}
 	c.bt_cnt = 0;
+	c.need_bt = 0;   // an accepted backtracking step leaves it set for k_lerp
 	const bool brk = (c.relchg < I.tol_inn) && !c.fst;
 	c.inner_break = brk || c.count_total >= I.maxit;
 	if (!brk) c.fst = 0;
@@ -554,12 +557,9 @@ __global__ void __launch_bounds__(BLOCK) k_tau_prep(KArgs a) {
 	} else {
 		const float *__restrict__ gv = I.vn[vG], *__restrict__ gp = I.vn[vGp];
 		const float *__restrict__ g2 = I.vn[vG2], *__restrict__ g2p = I.vn[vG2p], *__restrict__ uup = I.vn[vUUP];
-		float *__restrict__ dgv = I.vn[vdG], *__restrict__ dg2v = I.vn[vdG2];
 		FOR_TILE(local * TILE, g.n, i) {
 			float dg = gv[i] - gp[i];
 			float dg2 = g2[i] - g2p[i];
-			dgv[i] = dg;
-			dg2v[i] = dg2;
 			float uu = uup[i];
 			float tmp = fmaf(mdb, dg, dg2);
 			v[0] += (double)uu * uu;
@@ -645,72 +645,102 @@ __global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
 	}
 }
 
-// backtracking differences (2d:544,550-554)
-__global__ void __launch_bounds__(BLOCK) k_bt_diff(KArgs a) {
-	KPROLOGUE(a);
-	if (blockIdx.x == 0 && threadIdx.x == 0) set_conds(a.cs, *I.ctrl);   // state unchanged here
-	if (local < I.ntn) {
-		FOR_TILE(local * TILE, (int)I.n, i) {
-			I.vn[vdU][i] = I.vn[vU][i] - I.vn[vUp][i];
-			I.vn[vdG][i] = I.vn[vG][i] - I.vn[vGp][i];
-			I.vn[vdG2][i] = I.vn[vG2][i] - I.vn[vG2p][i];
-#pragma unroll
-			for (int cc = 0; cc < 3; cc++)
-				if (cc < I.dims) I.vn[vdUx + cc][i] = I.vn[vUx + cc][i] - I.vn[vUxp + cc][i];
-		}
-	} else {
-		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) I.vm[vdAu][i] = I.vm[vAu][i] - I.vm[vAup][i];
-	}
-}
-
-// one backtracking step: alpha *= gamma; update_g (2d:495-524,558-574)
-__global__ void __launch_bounds__(BLOCK) k_lerp(KArgs a) {
+// Nonmonotone Armijo backtracking (2d:544-574) in one pass over the vectors.
+// The reference's loop sets alpha *= gamma and evaluates f at
+//   U(alpha) = Up + alpha (U - Up),  likewise g, g2, Ux, Uy (, Uz), Au
+// (update_g, 2d:495-524), up to five times, then restarts.  Every term of
+// f is a polynomial in alpha over these interpolants:
+//   lam2(a) = |E0 + a dU'|^2,  lam4(a) = <S, E0> + a <S, dU'>      (E0 = U'p - W, dU' = U' - U'p)
+//   lam3(a) = |R0 + a dAu|^2,  lam5(a) = <delta, R0> + a <delta, dAu>   (R0 = Aup - b)
+// so k_bt_search forms their coefficients once (lam4(1), lam5(1) come from
+// k_getg) and its last block runs the loop on them; k_lerp then moves the
+// vectors to the accepted alpha once, with the reference's float arithmetic
+// (fmaf(alpha, U - Up, Up)).  When all five steps fail the vectors are not
+// moved: the restart (2d:561-567) recomputes every one of them from Up.
+__global__ void __launch_bounds__(BLOCK) k_bt_search(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
-	const double alpha_new = c.alpha * I.gamma;
-	const float al = (float)alpha_new;
-	double v[4] = {0, 0, 0, 0};   // lam2, lam4, lam3, lam5
+	// |E0|^2, <E0, dU'>, |dU'|^2, <S, E0>; |R0|^2, <R0, dAu>, |dAu|^2, <delta, R0>
+	double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 	if (local < I.ntn) {
 		FOR_TILE(local * TILE, (int)I.n, i) {
-			I.vn[vG][i] = fmaf(al, I.vn[vdG][i], I.vn[vGp][i]);
-			I.vn[vG2][i] = fmaf(al, I.vn[vdG2][i], I.vn[vG2p][i]);
-			I.vn[vU][i] = fmaf(al, I.vn[vdU][i], I.vn[vUp][i]);
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++)
 				if (cc < I.dims) {
-					float ux = fmaf(al, I.vn[vdUx + cc][i], I.vn[vUxp + cc][i]);
-					I.vn[vUx + cc][i] = ux;
-					float vv = ux - I.vn[vWx + cc][i];
-					v[0] += (double)vv * vv;
-					v[1] += (double)I.vn[vSx + cc][i] * vv;
+					const float up = I.vn[vUxp + cc][i];
+					const float du = I.vn[vUx + cc][i] - up;
+					const float e0 = up - I.vn[vWx + cc][i];
+					v[0] += (double)e0 * e0;
+					v[1] += (double)e0 * du;
+					v[2] += (double)du * du;
+					v[3] += (double)I.vn[vSx + cc][i] * e0;
 				}
 		}
 	} else {
 		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) {
-			float au = fmaf(al, I.vm[vdAu][i], I.vm[vAup][i]);
-			I.vm[vAu][i] = au;
-			float r = au - I.vm[vB][i];
-			v[2] += (double)r * r;
-			v[3] += (double)I.vm[vDelta][i] * r;
+			const float ap = I.vm[vAup][i];
+			const float da = I.vm[vAu][i] - ap;
+			const float r0 = ap - I.vm[vB][i];
+			v[4] += (double)r0 * r0;
+			v[5] += (double)r0 * da;
+			v[6] += (double)da * da;
+			v[7] += (double)I.vm[vDelta][i] * r0;
 		}
 	}
-	double tot[4];
-	if (!tile_reduce<4>(I, local, I.ntn + I.ntm, v, tot)) return;
+	double t[8];
+	if (!tile_reduce<8>(I, local, I.ntn + I.ntm, v, t)) return;
 	if (threadIdx.x != 0) return;
-	c.alpha = alpha_new;
-	c.step = c.tau * alpha_new;
-	c.bt_cnt++;
-	c.lam2 = tot[0]; c.lam4 = tot[1]; c.lam3 = tot[2]; c.lam5 = tot[3];
-	c.f = c.lam1 + c.beta / 2 * c.lam2 + c.mu / 2 * c.lam3 - c.lam4 - c.lam5;
-	bool still = fabs(c.f) > fabs(c.C - c.alpha * c.c_armij);
-	if (!still) {
-		c.need_bt = 0;
-	} else if (c.bt_cnt == 5) {   // backtracking not successful (2d:561-567)
-		c.gam *= I.rate_gam;
-		c.restart = 1;
+	const double s4 = c.lam4 - t[3], s5 = c.lam5 - t[7];   // slopes of the linear terms
+	double al = c.alpha;
+	int cnt = c.bt_cnt;
+	for (;;) {
+		if (cnt == 5) {   // backtracking not successful: restart
+			c.gam *= I.rate_gam;
+			c.restart = 1;
+			break;
+		}
+		al *= I.gamma;
+		cnt++;
+		c.lam2 = t[0] + al * (2 * t[1] + al * t[2]);
+		c.lam4 = t[3] + al * s4;
+		c.lam3 = t[4] + al * (2 * t[5] + al * t[6]);
+		c.lam5 = t[7] + al * s5;
+		c.f = c.lam1 + c.beta / 2 * c.lam2 + c.mu / 2 * c.lam3 - c.lam4 - c.lam5;
+		if (bad(c.f)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; c.need_bt = 0; c.restart = 0; break; }
+		if (!(fabs(c.f) > fabs(c.C - al * c.c_armij))) break;   // accepted: need_bt stays set for k_lerp
 	}
-	if (bad(c.f)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; c.need_bt = 0; c.restart = 0; }
+	c.alpha = al;
+	c.step = c.tau * al;
+	c.bt_cnt = cnt;
 	set_conds(a.cs, c);
+}
+
+// the accepted backtracking step: U' = U'p + alpha (U' - U'p) for U, g, Ux,
+// Uy (, Uz) and Au (g2 is formed again by k_shrink_grad, which follows)
+__global__ void __launch_bounds__(BLOCK) k_lerp(KArgs a) {
+	KPROLOGUE(a);
+	const float al = (float)I.ctrl->alpha;
+	if (local < I.ntn) {
+		FOR_TILE(local * TILE, (int)I.n, i) {
+			float *__restrict__ g = I.vn[vG];
+			float *__restrict__ u = I.vn[vU];
+			g[i] = fmaf(al, g[i] - I.vn[vGp][i], I.vn[vGp][i]);
+			u[i] = fmaf(al, u[i] - I.vn[vUp][i], I.vn[vUp][i]);
+#pragma unroll
+			for (int cc = 0; cc < 3; cc++)
+				if (cc < I.dims) {
+					float *__restrict__ ux = I.vn[vUx + cc];
+					const float p = I.vn[vUxp + cc][i];
+					ux[i] = fmaf(al, ux[i] - p, p);
+				}
+		}
+	} else {
+		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) {
+			float *__restrict__ au = I.vm[vAu];
+			const float p = I.vm[vAup][i];
+			au[i] = fmaf(al, au[i] - p, p);
+		}
+	}
 }
 
 // outer stopping test (2d:820-828): RelChgOut = |U - rcdU| / nrmup; rcdU = U
@@ -945,7 +975,7 @@ LAUNCHER(launch_shrink_grad, k_shrink_grad)
 LAUNCHER(launch_tau_prep, k_tau_prep)
 LAUNCHER(launch_tau_first, k_tau_first)
 LAUNCHER(launch_descend, k_descend)
-LAUNCHER(launch_bt_diff, k_bt_diff)
+LAUNCHER(launch_bt_search, k_bt_search)
 LAUNCHER(launch_lerp, k_lerp)
 LAUNCHER(launch_outer, k_outer)
 LAUNCHER(launch_mlp, k_mlp)

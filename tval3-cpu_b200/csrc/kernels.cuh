@@ -51,7 +51,7 @@ void launch_shrink_grad(cudaStream_t s, const KArgs &a);
 void launch_tau_prep(cudaStream_t s, const KArgs &a);
 void launch_tau_first(cudaStream_t s, const KArgs &a);
 void launch_descend(cudaStream_t s, const KArgs &a);
-void launch_bt_diff(cudaStream_t s, const KArgs &a);
+void launch_bt_search(cudaStream_t s, const KArgs &a);
 void launch_lerp(cudaStream_t s, const KArgs &a);
 void launch_outer(cudaStream_t s, const KArgs &a);
 void launch_mlp(cudaStream_t s, const KArgs &a);

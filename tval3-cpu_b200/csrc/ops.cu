@@ -1111,92 +1111,142 @@ __global__ void k_count_cols(const int *rind, long long nnz, long long *cnt) {
 		atomicAdd((unsigned long long *)&cnt[rind[k]], 1ull);
 }
 
-// warp per row: place every entry at the next free slot of its column
-__global__ void k_scatter_cols(long long rows, const int *rptr, const int *rind, const float *rval, int *cursor,
-                               int *cind, float *cval) {
+// The transpose is a stable least-significant-digit radix sort of the CSR
+// entries by column, 8 bits per pass: the entries arrive in row order, so
+// each column's rows come out ascending, with no per-column sort and no
+// atomics that would make the order depend on timing.
+constexpr int RADIX_T = 256, RADIX_ITEMS = 16, RADIX_TILE = RADIX_T * RADIX_ITEMS;
+constexpr int RADIX_WARPS = RADIX_T / 32;
+
+// the row of every entry (warp per row)
+__global__ void k_entry_rows(long long rows, const int *rptr, int *row_of) {
 	long long row = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	int lane = threadIdx.x & 31;
 	if (row >= rows) return;
-	for (int k = rptr[row] + lane; k < rptr[row + 1]; k += 32) {
-		int pos = atomicAdd(&cursor[rind[k]], 1);
-		cind[pos] = (int)row;
-		if (cval) cval[pos] = rval[k];
-	}
+	for (int k = rptr[row] + lane; k < rptr[row + 1]; k += 32) row_of[k] = (int)row;
 }
 
-// block per column: sort its (row, value) entries by row (bitonic in shared
-// memory; long columns fall back to an insertion sort in global memory)
-constexpr int SEG_CAP = 4096;
-__global__ void k_sort_cols(long long cols, const int *cptr, int *cind, float *cval) {
-	__shared__ int key[SEG_CAP];
-	__shared__ float val[SEG_CAP];
-	for (long long col = blockIdx.x; col < cols; col += gridDim.x) {
-		const int k0 = cptr[col], len = cptr[col + 1] - k0;
-		if (len <= 1) continue;
-		if (len > SEG_CAP) {
-			if (threadIdx.x == 0)
-				for (int a = 1; a < len; a++) {
-					int kk = cind[k0 + a];
-					float vv = cval ? cval[k0 + a] : 0.f;
-					int b = a - 1;
-					while (b >= 0 && cind[k0 + b] > kk) {
-						cind[k0 + b + 1] = cind[k0 + b];
-						if (cval) cval[k0 + b + 1] = cval[k0 + b];
-						b--;
-					}
-					cind[k0 + b + 1] = kk;
-					if (cval) cval[k0 + b + 1] = vv;
-				}
-			__syncthreads();
-			continue;
-		}
-		int P = 1;
-		while (P < len) P <<= 1;
-		for (int t = threadIdx.x; t < P; t += blockDim.x) {
-			key[t] = t < len ? cind[k0 + t] : INT_MAX;
-			val[t] = (t < len && cval) ? cval[k0 + t] : 0.f;
-		}
+// digit counts of one tile of entries: hist[digit * tiles + tile]
+__global__ void __launch_bounds__(RADIX_T) k_radix_hist(const int *key, long long nnz, int shift,
+                                                        long long *hist) {
+	__shared__ int cnt[256];
+	cnt[threadIdx.x] = 0;
+	__syncthreads();
+	const long long base = (long long)blockIdx.x * RADIX_TILE;
+#pragma unroll 4
+	for (int j = 0; j < RADIX_ITEMS; j++) {
+		long long k = base + j * RADIX_T + threadIdx.x;
+		if (k < nnz) atomicAdd(&cnt[(key[k] >> shift) & 255], 1);
+	}
+	__syncthreads();
+	hist[(long long)threadIdx.x * gridDim.x + blockIdx.x] = cnt[threadIdx.x];
+}
+
+// stable scatter of one tile by its digit: within the tile an entry's rank
+// among the entries of its digit follows the input order (round j holds
+// entries j*256 + t; a warp ranks its lanes with __match_any_sync, and the
+// per-digit pass over the warps orders the warps)
+__global__ void __launch_bounds__(RADIX_T) k_radix_scatter(const int *key, const int *val, const float *fval,
+                                                           long long nnz, int shift, const long long *off,
+                                                           int *key_out, int *val_out, float *fval_out) {
+	__shared__ int wcnt[RADIX_WARPS][256];
+	__shared__ int wbase[RADIX_WARPS][256];
+	__shared__ long long tile_off[256];
+	const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+	tile_off[t] = off[(long long)t * gridDim.x + blockIdx.x];
+	int running = 0;   // entries of digit t in the earlier rounds
+	const long long base = (long long)blockIdx.x * RADIX_TILE;
+	for (int j = 0; j < RADIX_ITEMS; j++) {
+#pragma unroll
+		for (int q = 0; q < RADIX_WARPS; q++) wcnt[q][t] = 0;
 		__syncthreads();
-		for (int size = 2; size <= P; size <<= 1)
-			for (int stride = size >> 1; stride > 0; stride >>= 1) {
-				for (int t = threadIdx.x; t < P; t += blockDim.x) {
-					int o = t ^ stride;
-					if (o > t) {
-						bool up = (t & size) == 0;
-						if ((key[t] > key[o]) == up) {
-							int tk = key[t]; key[t] = key[o]; key[o] = tk;
-							float tv = val[t]; val[t] = val[o]; val[o] = tv;
-						}
-					}
-				}
-				__syncthreads();
+		const long long k = base + j * RADIX_T + t;
+		const bool ok = k < nnz;
+		int kv = 0, vv = 0;
+		float fv = 0.f;
+		if (ok) {
+			kv = key[k];
+			vv = val[k];
+			if (fval) fv = fval[k];
+		}
+		const int d = ok ? (kv >> shift) & 255 : 256;
+		const unsigned peers = __match_any_sync(0xffffffffu, d);
+		const int rank = __popc(peers & ((1u << lane) - 1u));
+		if (ok && rank == 0) wcnt[w][d] = __popc(peers);
+		__syncthreads();
+		{
+			int run = running;
+#pragma unroll
+			for (int q = 0; q < RADIX_WARPS; q++) {
+				wbase[q][t] = run;
+				run += wcnt[q][t];
 			}
-		for (int t = threadIdx.x; t < len; t += blockDim.x) {
-			cind[k0 + t] = key[t];
-			if (cval) cval[k0 + t] = val[t];
+			running = run;
 		}
 		__syncthreads();
+		if (ok) {
+			const long long pos = tile_off[d] + wbase[w][d] + rank;
+			if (key_out) key_out[pos] = kv;
+			val_out[pos] = vv;
+			if (fval_out) fval_out[pos] = fv;
+		}
 	}
 }
 
 void build_transpose(cudaStream_t s, long long rows, long long cols, long long nnz, const int *rptr,
                      const int *rind, const float *rval, int *cptr, int *cind, float *cval) {
 	long long *cnt = nullptr, *off = nullptr;
-	int *cursor = nullptr;
 	TG_CUDA(cudaMallocAsync(&cnt, sizeof(long long) * (cols + 1), s));
 	TG_CUDA(cudaMallocAsync(&off, sizeof(long long) * (cols + 1), s));
 	TG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(long long) * (cols + 1), s));
 	if (nnz > 0) k_count_cols<<<(unsigned)min(4096LL, (nnz + 255) / 256), 256, 0, s>>>(rind, nnz, cnt);
 	scan_counts(s, cnt, off, cols);
 	k_to_int<<<(unsigned)((cols + 1 + 255) / 256), 256, 0, s>>>(off, cptr, cols + 1);
-	TG_CUDA(cudaMallocAsync(&cursor, sizeof(int) * (cols + 1), s));
-	TG_CUDA(cudaMemcpyAsync(cursor, cptr, sizeof(int) * (cols + 1), cudaMemcpyDeviceToDevice, s));
-	if (rows > 0) k_scatter_cols<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(rows, rptr, rind, rval, cursor, cind, cval);
-	if (cols > 0) k_sort_cols<<<(unsigned)min(cols, 148LL * 64), 256, 0, s>>>(cols, cptr, cind, cval);
 	TG_CUDA(cudaGetLastError());
 	TG_CUDA(cudaFreeAsync(cnt, s));
 	TG_CUDA(cudaFreeAsync(off, s));
-	TG_CUDA(cudaFreeAsync(cursor, s));
+	if (nnz <= 0 || rows <= 0) return;
+	int bits = 1;
+	while (bits < 31 && (1LL << bits) < cols) bits++;
+	const int passes = (bits + 7) / 8;
+	const long long tiles = (nnz + RADIX_TILE - 1) / RADIX_TILE;
+	int *k0 = nullptr, *k1 = nullptr, *v0 = nullptr, *v1 = nullptr;
+	float *f0 = nullptr, *f1 = nullptr;
+	long long *hist = nullptr, *hoff = nullptr;
+	TG_CUDA(cudaMallocAsync(&hist, sizeof(long long) * (256 * tiles + 1), s));
+	TG_CUDA(cudaMallocAsync(&hoff, sizeof(long long) * (256 * tiles + 1), s));
+	TG_CUDA(cudaMallocAsync(&v0, sizeof(int) * nnz, s));
+	if (passes > 1) {
+		TG_CUDA(cudaMallocAsync(&k0, sizeof(int) * nnz, s));
+		TG_CUDA(cudaMallocAsync(&k1, sizeof(int) * nnz, s));
+		TG_CUDA(cudaMallocAsync(&v1, sizeof(int) * nnz, s));
+		if (rval) {
+			TG_CUDA(cudaMallocAsync(&f0, sizeof(float) * nnz, s));
+			TG_CUDA(cudaMallocAsync(&f1, sizeof(float) * nnz, s));
+		}
+	}
+	k_entry_rows<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(rows, rptr, v0);
+	// pass p reads (key, row, value) from the previous pass (the CSR itself
+	// first) and writes the next pair of buffers; the last pass writes cind
+	// and cval and drops the keys
+	const int *kin = rind, *vin = v0;
+	const float *fin = rval;
+	for (int p = 0; p < passes; p++) {
+		const bool last = p == passes - 1;
+		int *kout = last ? nullptr : (p % 2 == 0 ? k0 : k1);
+		int *vout = last ? cind : (p % 2 == 0 ? v1 : v0);
+		float *fout = !rval ? nullptr : last ? cval : (p % 2 == 0 ? f0 : f1);
+		k_radix_hist<<<(unsigned)tiles, RADIX_T, 0, s>>>(kin, nnz, 8 * p, hist);
+		scan_counts(s, hist, hoff, 256 * tiles);
+		k_radix_scatter<<<(unsigned)tiles, RADIX_T, 0, s>>>(kin, vin, fin, nnz, 8 * p, hoff, kout, vout, fout);
+		kin = kout;
+		vin = vout;
+		fin = fout;
+	}
+	TG_CUDA(cudaGetLastError());
+	for (void *ptr : {(void *)hist, (void *)hoff, (void *)v0, (void *)v1, (void *)k0, (void *)k1, (void *)f0,
+	                  (void *)f1})
+		if (ptr) TG_CUDA(cudaFreeAsync(ptr, s));
 }
 
 __global__ void k_ray_len(int nrays, const int4 *rays, long long *len) {

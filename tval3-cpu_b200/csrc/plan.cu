@@ -812,11 +812,9 @@ void Plan::emit_iteration(unsigned long long h_active) {
 	launch_getg(es(), kargs(MAP_NM, P_ACTIVE, ST_DESCEND).cond(h_bt, P_NEED_BT));
 	// nonmonotone Armijo backtracking, restart after five failures
 	if_(P_NEED_BT, [&] {
-		const unsigned long long h_loop = cond_handle(), h_restart = cond_handle();
-		launch_bt_diff(es(), kargs(MAP_NM, P_NEED_BT).cond(h_loop, P_NEED_BT));
-		while_(P_NEED_BT, [&] {
-			launch_lerp(es(), kargs(MAP_NM, P_NEED_BT).cond(h_loop, P_NEED_BT).cond(h_restart, P_RESTART));
-		}, h_loop);
+		const unsigned long long h_lerp = cond_handle(), h_restart = cond_handle();
+		launch_bt_search(es(), kargs(MAP_NM, P_NEED_BT).cond(h_lerp, P_NEED_BT).cond(h_restart, P_RESTART));
+		if_(P_NEED_BT, [&] { launch_lerp(es(), kargs(MAP_NM, P_NEED_BT)); }, h_lerp);
 		if_(P_RESTART, [&] {
 			launch_tau_prep(es(), kargs(MAP_N, P_RESTART));
 			op_forward(lctx(), ob_, P_NEED_AD, D, Ad);
