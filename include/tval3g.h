@@ -159,6 +159,13 @@ int tval3g_plan_set_target(tval3g_plan *plan, double target);
 int tval3g_plan_trace(const tval3g_plan *plan, int index, tval3g_trace_record *out, int cap, int *count);
 int tval3g_plan_destroy(tval3g_plan *plan);
 
+/* Device memory of plans, operators and their one-time builders comes from a
+ * stream-ordered pool of the library (one per device), which keeps freed
+ * blocks for the next solve.  tval3g_trim_memory returns the current device's
+ * cached blocks beyond keep_bytes to the driver.  No counterpart in the
+ * reference (it allocates host memory per call). */
+int tval3g_trim_memory(long long keep_bytes);
+
 /* Operators alone.  tval3g_op_apply: y = A x (trans = 0), y = A^T x
  * (trans = 1) or the normal product y = A^T (A x) of the solve's get_g_mult
  * (trans = 2; a one-layer dense operator reads A once, as the reference's

@@ -146,3 +146,16 @@ def test_plan_reuse_is_deterministic(torch_cuda):
     plan.close()
     np.testing.assert_array_equal(outs[0], outs[1])
     np.testing.assert_array_equal(outs[0], outs[2])
+
+
+def test_trim_memory_between_solves(torch_cuda):
+    """Returning the pool's cached blocks to the driver between two solves
+    changes nothing in the second solve."""
+    c = build_case("ring2d_s64_conv")
+    spec = api_problem(c, capi)
+    U1, _ = capi.solve(spec, c["b"], c["opts"])
+    capi.trim_memory(0)
+    U2, _ = capi.solve(spec, c["b"], c["opts"])
+    np.testing.assert_array_equal(U1, U2)
+    with pytest.raises(capi.TVAL3Error):
+        capi.trim_memory(-1)

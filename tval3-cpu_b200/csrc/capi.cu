@@ -130,6 +130,15 @@ int tval3g_solve(const tval3g_problem *prob, const float *b, int b_len, const tv
 	CAPI_END
 }
 
+int tval3g_trim_memory(long long keep_bytes) {
+	CAPI_BEGIN
+	TG_ARG(keep_bytes >= 0, "Argument error: keep_bytes must not be negative");
+	need_device();
+	TG_CUDA(cudaDeviceSynchronize());
+	TG_CUDA(cudaMemPoolTrimTo(library_pool(), (size_t)keep_bytes));
+	CAPI_END
+}
+
 int tval3g_plan_create(tval3g_plan **plan, int count, const tval3g_problem *probs, const tval3g_options *opts,
                        int flags) {
 	CAPI_BEGIN
@@ -390,12 +399,12 @@ int tval3g_shrink(int dims, long long n, int tv_norm, double beta, const float *
 	       "Argument error: bad shrinkage arguments");
 	double *d = nullptr;
 	cudaStream_t s = (cudaStream_t)stream;
-	TG_CUDA(cudaMallocAsync(&d, sizeof(double), s));
+	d = (decltype(d))dev_alloc(sizeof(double), s);
 	TG_CUDA(cudaMemsetAsync(d, 0, sizeof(double), s));
 	launch_shrink_plain(s, dims, n, tv_norm, beta, Ux, Uy, Uz, sx, sy, sz, Wx, Wy, Wz, d);
 	double h = 0;
 	TG_CUDA(cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, s));
-	TG_CUDA(cudaFreeAsync(d, s));
+	dev_free(d, s);
 	TG_CUDA(cudaStreamSynchronize(s));
 	if (lam1) *lam1 = h;
 	CAPI_END

@@ -45,6 +45,7 @@ struct Error {
 // block may be freed only when no queued work still uses it.
 void *dev_alloc(size_t bytes, cudaStream_t s);
 void dev_free(void *p, cudaStream_t s);
+cudaMemPool_t library_pool();   // the current device's pool
 
 #define TG_ARG(cond, msg)                                                                           \
 	do {                                                                                            \
@@ -138,23 +139,29 @@ struct OpDev {
 	// the rays that cross it, tmeas[tptr[t] .. tptr[t+1]), in traced order,
 	// and each pixel lists its hits as 16-bit 1-based positions in its tile's
 	// list (0: a pad entry), eight to a 16-byte word.  Thread r of tile t's
-	// block takes pixel tperm[256 t + r] (row-major in the tile; pixels by
+	// block takes pixel tperm[RAYT^2 t + r] (row-major in the tile; pixels by
 	// decreasing list length); the words of warp w's 32 pixels (tile t's
-	// warps are 8t .. 8t+7) are interleaved: word v of lane l is
-	// sidx[woff[w] + 32 v + l]
+	// warps are RAYT^2/32 t + 0, 1, ...) are interleaved: word v of lane l is
+	// sidx[woff[w] + 32 v + l].  Block b of a launch takes tile torder[b]:
+	// tiles by decreasing list length, so the longest start first and the
+	// short ones fill the SMs that finish early.
 	int tiled;
 	int ntx;
 	int tmax;               // longest tile list
 	const int *tptr, *tmeas, *woff;
 	const uint4 *sidx;
 	const unsigned char *tperm;
+	const int *torder;
 	// 2D forward: y-driven rays read a transposed copy of the image (rows of
 	// length tH = n / ld), in which their steps are contiguous; NULL = off
 	float *xT;
 	int tH;
 };
 
-constexpr int RAYT = 16;                // tile side of the tiled 2D ray adjoint
+#ifndef TVAL3G_RAYT
+#define TVAL3G_RAYT 16
+#endif
+constexpr int RAYT = TVAL3G_RAYT;       // tile side of the tiled 2D ray adjoint
 constexpr int RAYT_MAX_RAYS = 1 << 18;  // its index builder keeps a bitmap of the traced rays in shared memory
 constexpr int RAYT_MAX_LIST = 40960;    // rays per tile (16-bit positions; 160 KB of shared memory beside the index rings)
 

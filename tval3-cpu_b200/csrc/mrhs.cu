@@ -538,13 +538,13 @@ std::shared_ptr<MrhsOp> mrhs_create(cudaStream_t s, const float *d_A, long long 
 	// A and A^T re-laid tile by tile (a snapshot of A, like the CSC transpose of
 	// a sparse operator): every TMA stage then reads 16 KB contiguous
 	float *at = nullptr;
-	TG_CUDA(cudaMallocAsync(&at, sizeof(float) * (size_t)(m * n), s));
+	at = (decltype(at))dev_alloc(sizeof(float) * (size_t)(m * n), s);
 	dim3 tb(32, 8), tg((unsigned)((n + 31) / 32), (unsigned)((m + 31) / 32));
 	k_transpose<<<tg, tb, 0, s>>>(d_A, m, n, at);
 	k_tile_major<<<4 * sms, 256, 0, s>>>(d_A, m, n, op->ks_f, sz_f, op->ta);
 	k_tile_major<<<4 * sms, 256, 0, s>>>(at, n, m, op->ks_a, sz_a, op->tat);
 	TG_CUDA(cudaGetLastError());
-	TG_CUDA(cudaFreeAsync(at, s));
+	dev_free(at, s);
 	op->tm_a = make_map(op->ta, BK, sz_f / BK, BM);
 	op->tm_at = make_map(op->tat, BK, sz_a / BK, BM);
 	op->tm_xh_f = make_map(op->xh, n, layers, layers);

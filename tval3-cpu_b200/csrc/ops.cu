@@ -12,6 +12,9 @@
 //             2D per pixel tile, through shared memory
 #include "ops.cuh"
 
+#include <algorithm>
+#include <vector>
+
 #include "async.cuh"
 
 namespace tval3g {
@@ -690,7 +693,7 @@ __global__ void __launch_bounds__(RAYT_ADJ_THREADS) k_ray_adj_tiled(const Inst *
 	OPROLOGUE();
 	extern __shared__ __align__(128) unsigned char smem[];
 	const OpDev &op = I.op;
-	const int t = (int)local;
+	const int t = __ldg(op.torder + local);
 	const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int pw = wid % RAYT_WARPS, half = wid / RAYT_WARPS;   // pixel-warp, which half of its words
 	uint4 *ring = reinterpret_cast<uint4 *>(smem) + wid * RAYT_STAGES * RAYT_STAGE_WORDS;
@@ -913,10 +916,10 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 	TG_CUDA(cudaFuncSetAttribute(k_tile_count, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_count));
 	TG_CUDA(cudaFuncSetAttribute(k_tile_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_fill));
 	long long *tlen = nullptr, *tptr = nullptr, *wlen = nullptr, *woff = nullptr;
-	TG_CUDA(cudaMallocAsync(&tlen, sizeof(long long) * (nt + 1), s));
-	TG_CUDA(cudaMallocAsync(&tptr, sizeof(long long) * (nt + 1), s));
-	TG_CUDA(cudaMallocAsync(&wlen, sizeof(long long) * (nw + 1), s));
-	TG_CUDA(cudaMallocAsync(&woff, sizeof(long long) * (nw + 1), s));
+	tlen = (decltype(tlen))dev_alloc(sizeof(long long) * (nt + 1), s);
+	tptr = (decltype(tptr))dev_alloc(sizeof(long long) * (nt + 1), s);
+	wlen = (decltype(wlen))dev_alloc(sizeof(long long) * (nw + 1), s);
+	woff = (decltype(woff))dev_alloc(sizeof(long long) * (nw + 1), s);
 	unsigned char *perm = (unsigned char *)dev_alloc((size_t)nt * RAYT_THREADS, s);
 	k_tile_count<<<nt, RAYT_THREADS, smem_count, s>>>(ld, H, ntx, nrays, cptr, cind, tlen, wlen, perm);
 	TG_CUDA(cudaGetLastError());
@@ -931,6 +934,16 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 	for (int t = 0; t < nt; t++) tmax = std::max(tmax, h_tptr[t + 1] - h_tptr[t]);
 	const bool ok = tmax <= RAYT_MAX_LIST && words < (1LL << 31) && h_tptr[nt] < (1LL << 31);
 	if (ok) {
+		// launch order: tiles by decreasing list length (ties by index)
+		std::vector<int> order(nt);
+		for (int t = 0; t < nt; t++) order[t] = t;
+		std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+			return h_tptr[a + 1] - h_tptr[a] > h_tptr[b + 1] - h_tptr[b];
+		});
+		int *torder = (int *)dev_alloc(sizeof(int) * nt, s);
+		owned.push_back(torder);
+		TG_CUDA(cudaMemcpyAsync(torder, order.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, s));
+		d.torder = torder;
 		int *tmeas = (int *)dev_alloc(sizeof(int) * (size_t)std::max(h_tptr[nt], 4LL), s);
 		TG_CUDA(cudaMemsetAsync(tmeas, 0, sizeof(int) * (size_t)std::max(h_tptr[nt], 4LL), s));
 		uint4 *sidx = (uint4 *)dev_alloc(sizeof(uint4) * (size_t)std::max(words, 1LL), s);
@@ -950,15 +963,15 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 		d.tmax = (int)tmax;
 		d.tptr = tptr32; d.tmeas = tmeas; d.woff = woff32; d.sidx = sidx; d.tperm = perm;
 		owned.push_back(perm);
-		*bytes = (long long)sizeof(uint4) * words + (long long)sizeof(int) * (h_tptr[nt] + nt + nw + 2) +
+		*bytes = (long long)sizeof(uint4) * words + (long long)sizeof(int) * (h_tptr[nt] + 2 * nt + nw + 2) +
 		         (long long)nt * RAYT_THREADS;
 	} else {
 		dev_free(perm, s);
 	}
-	TG_CUDA(cudaFreeAsync(tlen, s));
-	TG_CUDA(cudaFreeAsync(tptr, s));
-	TG_CUDA(cudaFreeAsync(wlen, s));
-	TG_CUDA(cudaFreeAsync(woff, s));
+	dev_free(tlen, s);
+	dev_free(tptr, s);
+	dev_free(wlen, s);
+	dev_free(woff, s);
 	return ok;
 }
 
@@ -1093,12 +1106,12 @@ void scan_counts(cudaStream_t s, const long long *cnt, long long *out, long long
 	long long nb = (n + SCAN_TILE - 1) / SCAN_TILE;
 	if (nb < 1) nb = 1;
 	long long *tot = nullptr;
-	TG_CUDA(cudaMallocAsync(&tot, sizeof(long long) * nb, s));
+	tot = (decltype(tot))dev_alloc(sizeof(long long) * nb, s);
 	k_scan_tiles<<<(unsigned)nb, SCAN_T, 0, s>>>(cnt, out, n, tot);
 	k_scan_totals<<<1, 32, 0, s>>>(tot, (int)nb, out, n);
 	if (n > 0) k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, n, tot);
 	TG_CUDA(cudaGetLastError());
-	TG_CUDA(cudaFreeAsync(tot, s));
+	dev_free(tot, s);
 }
 
 __global__ void k_to_int(const long long *in, int *out, long long n) {
@@ -1196,15 +1209,15 @@ __global__ void __launch_bounds__(RADIX_T) k_radix_scatter(const int *key, const
 void build_transpose(cudaStream_t s, long long rows, long long cols, long long nnz, const int *rptr,
                      const int *rind, const float *rval, int *cptr, int *cind, float *cval) {
 	long long *cnt = nullptr, *off = nullptr;
-	TG_CUDA(cudaMallocAsync(&cnt, sizeof(long long) * (cols + 1), s));
-	TG_CUDA(cudaMallocAsync(&off, sizeof(long long) * (cols + 1), s));
+	cnt = (decltype(cnt))dev_alloc(sizeof(long long) * (cols + 1), s);
+	off = (decltype(off))dev_alloc(sizeof(long long) * (cols + 1), s);
 	TG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(long long) * (cols + 1), s));
 	if (nnz > 0) k_count_cols<<<(unsigned)min(4096LL, (nnz + 255) / 256), 256, 0, s>>>(rind, nnz, cnt);
 	scan_counts(s, cnt, off, cols);
 	k_to_int<<<(unsigned)((cols + 1 + 255) / 256), 256, 0, s>>>(off, cptr, cols + 1);
 	TG_CUDA(cudaGetLastError());
-	TG_CUDA(cudaFreeAsync(cnt, s));
-	TG_CUDA(cudaFreeAsync(off, s));
+	dev_free(cnt, s);
+	dev_free(off, s);
 	if (nnz <= 0 || rows <= 0) return;
 	int bits = 1;
 	while (bits < 31 && (1LL << bits) < cols) bits++;
@@ -1213,16 +1226,16 @@ void build_transpose(cudaStream_t s, long long rows, long long cols, long long n
 	int *k0 = nullptr, *k1 = nullptr, *v0 = nullptr, *v1 = nullptr;
 	float *f0 = nullptr, *f1 = nullptr;
 	long long *hist = nullptr, *hoff = nullptr;
-	TG_CUDA(cudaMallocAsync(&hist, sizeof(long long) * (256 * tiles + 1), s));
-	TG_CUDA(cudaMallocAsync(&hoff, sizeof(long long) * (256 * tiles + 1), s));
-	TG_CUDA(cudaMallocAsync(&v0, sizeof(int) * nnz, s));
+	hist = (decltype(hist))dev_alloc(sizeof(long long) * (256 * tiles + 1), s);
+	hoff = (decltype(hoff))dev_alloc(sizeof(long long) * (256 * tiles + 1), s);
+	v0 = (decltype(v0))dev_alloc(sizeof(int) * nnz, s);
 	if (passes > 1) {
-		TG_CUDA(cudaMallocAsync(&k0, sizeof(int) * nnz, s));
-		TG_CUDA(cudaMallocAsync(&k1, sizeof(int) * nnz, s));
-		TG_CUDA(cudaMallocAsync(&v1, sizeof(int) * nnz, s));
+		k0 = (decltype(k0))dev_alloc(sizeof(int) * nnz, s);
+		k1 = (decltype(k1))dev_alloc(sizeof(int) * nnz, s);
+		v1 = (decltype(v1))dev_alloc(sizeof(int) * nnz, s);
 		if (rval) {
-			TG_CUDA(cudaMallocAsync(&f0, sizeof(float) * nnz, s));
-			TG_CUDA(cudaMallocAsync(&f1, sizeof(float) * nnz, s));
+			f0 = (decltype(f0))dev_alloc(sizeof(float) * nnz, s);
+			f1 = (decltype(f1))dev_alloc(sizeof(float) * nnz, s);
 		}
 	}
 	k_entry_rows<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(rows, rptr, v0);
@@ -1246,7 +1259,7 @@ void build_transpose(cudaStream_t s, long long rows, long long cols, long long n
 	TG_CUDA(cudaGetLastError());
 	for (void *ptr : {(void *)hist, (void *)hoff, (void *)v0, (void *)v1, (void *)k0, (void *)k1, (void *)f0,
 	                  (void *)f1})
-		if (ptr) TG_CUDA(cudaFreeAsync(ptr, s));
+		if (ptr) dev_free(ptr, s);
 }
 
 __global__ void k_ray_len(int nrays, const int4 *rays, long long *len) {
@@ -1274,8 +1287,8 @@ __global__ void k_ray_trace(int nrays, const int4 *rays, int rvx, int rvy, const
 void trace_rays(cudaStream_t s, int nrays, const int4 *rays, int rvx, int rvy, int *rptr, int *rind,
                 long long *total_out) {
 	long long *len = nullptr, *off = nullptr;
-	TG_CUDA(cudaMallocAsync(&len, sizeof(long long) * (nrays + 1), s));
-	TG_CUDA(cudaMallocAsync(&off, sizeof(long long) * (nrays + 1), s));
+	len = (decltype(len))dev_alloc(sizeof(long long) * (nrays + 1), s);
+	off = (decltype(off))dev_alloc(sizeof(long long) * (nrays + 1), s);
 	if (nrays > 0) k_ray_len<<<(nrays + 255) / 256, 256, 0, s>>>(nrays, rays, len);
 	scan_counts(s, len, off, nrays);
 	long long total = 0;
@@ -1283,15 +1296,15 @@ void trace_rays(cudaStream_t s, int nrays, const int4 *rays, int rvx, int rvy, i
 	TG_CUDA(cudaStreamSynchronize(s));
 	*total_out = total;
 	if (total >= (1LL << 31) - 1) {
-		cudaFreeAsync(len, s);
-		cudaFreeAsync(off, s);
+		dev_free(len, s);
+		dev_free(off, s);
 		throw Error{TVAL3G_ERR_ARGUMENT, "Argument error: the ray operator has more than 2^31-1 hits"};
 	}
 	k_to_int<<<(unsigned)((nrays + 1 + 255) / 256), 256, 0, s>>>(off, rptr, nrays + 1);
 	if (rind && nrays > 0) k_ray_trace<<<(unsigned)(((long long)nrays * 32 + 255) / 256), 256, 0, s>>>(nrays, rays, rvx, rvy, rptr, rind);
 	TG_CUDA(cudaGetLastError());
-	TG_CUDA(cudaFreeAsync(len, s));
-	TG_CUDA(cudaFreeAsync(off, s));
+	dev_free(len, s);
+	dev_free(off, s);
 }
 
 }  // namespace tval3g

@@ -85,6 +85,7 @@ def lib():
         L.tval3g_plan_trace.argtypes = [vp, i, C.POINTER(C.c_double), i, C.POINTER(i)]
         L.tval3g_plan_set_target.argtypes = [vp, d]
         L.tval3g_plan_destroy.argtypes = [vp]
+        L.tval3g_trim_memory.argtypes = [ll]
         L.tval3g_op_create.argtypes = [C.POINTER(vp), P, i]
         L.tval3g_op_shape.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(ll)]
         L.tval3g_op_apply.argtypes = [vp, i, vp, vp, vp]
@@ -109,9 +110,14 @@ def _check(rc):
         raise TVAL3Error(rc, lib().tval3g_last_error().decode())
 
 
+def trim_memory(keep_bytes=0):
+    """Return the library pool's cached device memory beyond keep_bytes."""
+    _check(lib().tval3g_trim_memory(int(keep_bytes)))
+
+
 EXPORTS = ("tval3g_last_error", "tval3g_version", "tval3g_solve", "tval3g_solve_batch", "tval3g_plan_create",
            "tval3g_plan_solve", "tval3g_plan_stats", "tval3g_plan_trace", "tval3g_plan_set_target",
-           "tval3g_plan_destroy", "tval3g_op_create", "tval3g_op_shape",
+           "tval3g_plan_destroy", "tval3g_trim_memory", "tval3g_op_create", "tval3g_op_shape",
            "tval3g_op_apply", "tval3g_op_apply_n", "tval3g_op_ray_csr", "tval3g_op_adjoint_index_bytes",
            "tval3g_op_destroy", "tval3g_D", "tval3g_Dt",
            "tval3g_shrink", "tval3g_unrolled_create", "tval3g_unrolled_forward", "tval3g_unrolled_backward",
