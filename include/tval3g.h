@@ -119,6 +119,12 @@ typedef struct tval3g_problem {
 	int ld;                         /* RAY2D row stride of the image */
 	int rv_x, rv_y, rv_z;           /* RAY3D volume extent */
 	float scale_factor;             /* RAY2D / RAY3D weight of one hit */
+	/* 1: complex data (the reference's complex<float> overloads,
+	 * 2d/tval3_cpu_2d.cpp:913-929 and the sparse / geometry ones): b, Ut and
+	 * U hold interleaved (re, im) float pairs (b_len, ut_len and n count
+	 * complex elements), as do DENSE A and CSR csr_val; the adjoint is the
+	 * conjugate transpose.  2D only, one layer, host operator arrays. */
+	int complex_data;
 } tval3g_problem;
 
 const char *tval3g_last_error(void);

@@ -268,7 +268,7 @@ def ref_lib(dims):
     return _REF[dims]
 
 
-_DT = {0: np.float32, 1: np.float32, 2: np.float64}
+_DT = {0: np.float32, 1: np.float32, 2: np.float64, 3: np.complex64, 4: np.complex128}
 
 
 def _vp(a):
@@ -280,7 +280,9 @@ def ref_solve(kind: str, shape, b, opts: dict, dtype: int = 0, A=None, csr=None,
     """Run the reference's own tval3_cpu_2d / tval3_cpu_3d.
 
     kind: 'dense' (A: m x n), 'csr' (csr=(m, n, rowptr, colind, val)) or 'ray3d'
-    (geom dict).  dtype 0 = float/float opts, 1 = float/double opts, 2 = double.
+    (geom dict).  dtype 0 = float/float opts, 1 = float/double opts, 2 = double,
+    3 = complex<float>/float opts, 4 = complex<double>/double opts (2D dense
+    and CSR).
     formats = (U, A, Ut) mat_format codes (0 row major, 1 col major); default is
     what the reference requires for the operator kind (2d:700-702,719,739;
     3d:1038-1039,1086-1087,1140-1141).  Raises ReferenceError with the

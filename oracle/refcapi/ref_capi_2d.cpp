@@ -4,6 +4,7 @@
  * overloads are re-declared here exactly as the reference declares them and
  * resolved at link time against the reference's own object file.
  */
+#include <complex>
 #include <cstring>
 #include <string>
 #include "container.h"
@@ -22,6 +23,16 @@ extern const tval3_info<double> tval3_cpu_2d(mat<float> &U, const sparse_mat<flo
 		const tval3_options<double> &opts, const mat<float> &Ut, int submat_mb, int vppc) throw(tval3_exception);
 extern const tval3_info<double> tval3_cpu_2d(mat<double> &U, const sparse_mat<double> &A, const mat<double> &b,
 		const tval3_options<double> &opts, const mat<double> &Ut, int submat_mb, int vppc) throw(tval3_exception);
+typedef std::complex<float> cf;
+typedef std::complex<double> cd;
+extern const tval3_info<float> tval3_cpu_2d(mat<cf> &U, const mat<cf> &A, const mat<cf> &b,
+		const tval3_options<float> &opts, const mat<cf> &Ut, int submat_mb, int vppc) throw(tval3_exception);
+extern const tval3_info<double> tval3_cpu_2d(mat<cd> &U, const mat<cd> &A, const mat<cd> &b,
+		const tval3_options<double> &opts, const mat<cd> &Ut, int submat_mb, int vppc) throw(tval3_exception);
+extern const tval3_info<float> tval3_cpu_2d(mat<cf> &U, const sparse_mat<cf> &A, const mat<cf> &b,
+		const tval3_options<float> &opts, const mat<cf> &Ut, int submat_mb, int vppc) throw(tval3_exception);
+extern const tval3_info<double> tval3_cpu_2d(mat<cd> &U, const sparse_mat<cd> &A, const mat<cd> &b,
+		const tval3_options<double> &opts, const mat<cd> &Ut, int submat_mb, int vppc) throw(tval3_exception);
 
 template <class T, class S, class OP>
 static int run(void *U_, int dim_y, int dim_x, int ufmt, const OP &A, const void *b_, int blen,
@@ -76,6 +87,8 @@ int ref2d_dense(int dtype, void *U, int dim_y, int dim_x, int ufmt, const void *
                 int vppc, ref_info *info, char *err, int errlen) {
 	if (dtype == 0) return dense<float, float>(U, dim_y, dim_x, ufmt, A, m, n, afmt, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
 	if (dtype == 1) return dense<float, double>(U, dim_y, dim_x, ufmt, A, m, n, afmt, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
+	if (dtype == 3) return dense<cf, float>(U, dim_y, dim_x, ufmt, A, m, n, afmt, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
+	if (dtype == 4) return dense<cd, double>(U, dim_y, dim_x, ufmt, A, m, n, afmt, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
 	return dense<double, double>(U, dim_y, dim_x, ufmt, A, m, n, afmt, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
 }
 
@@ -85,6 +98,8 @@ int ref2d_csr(int dtype, void *U, int dim_y, int dim_x, int ufmt, int m, int n, 
               int utfmt, int submat_mb, int vppc, ref_info *info, char *err, int errlen) {
 	if (dtype == 0) return sparse<float, float>(U, dim_y, dim_x, ufmt, m, n, nnz, afmt, rptr, rind, rval, cptr, cind, cval, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
 	if (dtype == 1) return sparse<float, double>(U, dim_y, dim_x, ufmt, m, n, nnz, afmt, rptr, rind, rval, cptr, cind, cval, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
+	if (dtype == 3) return sparse<cf, float>(U, dim_y, dim_x, ufmt, m, n, nnz, afmt, rptr, rind, rval, cptr, cind, cval, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
+	if (dtype == 4) return sparse<cd, double>(U, dim_y, dim_x, ufmt, m, n, nnz, afmt, rptr, rind, rval, cptr, cind, cval, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
 	return sparse<double, double>(U, dim_y, dim_x, ufmt, m, n, nnz, afmt, rptr, rind, rval, cptr, cind, cval, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
 }
 

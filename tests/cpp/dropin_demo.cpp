@@ -70,9 +70,14 @@ static void e_double() {   // double data: the same argument checks
 	tval3_options<double> o;
 	tval3_cpu_2d(U, A, b, o, Ut);
 }
-static void e_complex() {
-	mat<std::complex<float> > U(8, 8, mat_col_major), A(20, 64, mat_row_major), b(20), Ut(0, mat_col_major);
+static void e_complex() {   // complex data: one layer only
+	mat<std::complex<float> > U(8, 16, mat_col_major), A(20, 64, mat_row_major), b(40), Ut(0, mat_col_major);
 	tval3_cpu_2d(U, A, b, opts(), Ut);
+}
+static void e_complex_format() {   // complex data: the same argument checks
+	mat<std::complex<double> > U(8, 8, mat_row_major), A(20, 64, mat_row_major), b(20), Ut(0, mat_col_major);
+	tval3_options<double> o;
+	tval3_cpu_2d(U, A, b, o, Ut);
 }
 
 static double maxdiff(const float *a, const float *b, int n) {
@@ -155,6 +160,28 @@ static void solve_cases() {
 	pr.x_emitters = xs; pr.y_emitters = ys; pr.x_receivers = xs; pr.y_receivers = ys; pr.ld = q; pr.scale_factor = 1.f;
 	rc = tval3g_solve(&pr, br.data(), T * T, &co, 0, 0, U2.data(), &ci);
 	std::printf("ray2d %d %.3e %d %d\n", rc, maxdiff(Ur.data(), U2.data(), n), info.total_iters, ci.total_iters);
+	{   // complex data through the complex<float> overload and through the C ABI
+		mat<std::complex<float> > Ac(m, n, mat_row_major), Uc(p, q, mat_col_major), bc(m), Utc(0, mat_col_major);
+		for (int i = 0; i < m * n; i++) Ac[i] = std::complex<float>(A[i], frand() / std::sqrt((float)m));
+		for (int r = 0; r < m; r++) {
+			std::complex<double> s = 0;
+			for (int c = 0; c < n; c++) s += std::complex<double>(Ac[r * n + c]) * (double)u0[c];
+			bc[r] = std::complex<float>(s);
+		}
+		info = tval3_cpu_2d(Uc, Ac, bc, opts(), Utc);
+		tval3g_problem pc;
+		std::memset(&pc, 0, sizeof(pc));
+		pc.dims = 2; pc.dim_y = p; pc.dim_x = q; pc.dim_z = 1; pc.op_kind = TVAL3G_OP_DENSE;
+		pc.m = m; pc.n_cols = n; pc.layers = 1; pc.A = reinterpret_cast<const float *>(Ac.data());
+		pc.complex_data = 1;
+		std::vector<std::complex<float> > Uc2(n);
+		rc = tval3g_solve(&pc, reinterpret_cast<const float *>(bc.data()), m, &co, 0, 0,
+		                  reinterpret_cast<float *>(Uc2.data()), &ci);
+		std::printf("cdense %d %.3e %d %d\n", rc,
+		            maxdiff(reinterpret_cast<const float *>(Uc.data()), reinterpret_cast<const float *>(Uc2.data()),
+		                    2 * n),
+		            info.total_iters, ci.total_iters);
+	}
 }
 
 int main(int argc, char **argv) {
@@ -168,6 +195,7 @@ int main(int argc, char **argv) {
 		err("geom_layers_or_blen", e_geom_layers);
 		err("double", e_double);
 		err("complex", e_complex);
+		err("complex_format", e_complex_format);
 		return 0;
 	}
 	try {

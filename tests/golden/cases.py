@@ -18,6 +18,28 @@ CASES = [
     "ring2d_s64_iso", "ring2d_s64_nonneg", "ring2d_s64_skip", "hemi3d_s16_it20", "hemi3d_s16_conv",
     "csr3d_s16", "dense3d_s8",
 ]
+# complex data (the reference's complex<float> / complex<double> overloads):
+# the FP64 anchor is the reference's own complex<double> build
+COMPLEX_CASES = ["cdense2d_s32", "ccsr2d_s32", "cring2d_s64"]
+
+
+def _complex_phantom(side, rng):
+    ur = W.ellipse_phantom(side, side, rng, 4, 0.0, lambda r: r.uniform(0.2, 1.0), (side / 10, side / 3))
+    ui = W.ellipse_phantom(side, side, rng, 3, 0.0, lambda r: r.uniform(-0.6, 0.6), (side / 10, side / 3))
+    return ur + 1j * ui
+
+
+def _complex_noise(y, rel, rng):
+    e = rng.standard_normal(y.shape) + 1j * rng.standard_normal(y.shape)
+    return y + e * (rel * np.linalg.norm(y) / np.linalg.norm(e))
+
+
+def _csr_apply(csr, x):
+    m, rowptr, colind, val = csr["m"], csr["rowptr"], csr["colind"], csr["val"]
+    rows = np.repeat(np.arange(m), np.diff(rowptr))
+    y = np.zeros(m, np.complex128)
+    np.add.at(y, rows, val.astype(np.complex128) * x[colind])
+    return y
 
 
 def _csr_tuple(A):
@@ -84,6 +106,39 @@ def build_case(name):
         c.update(shape=(s, s, s), A=A, b=b, u_true=u, ref_kind="dense", api="dense", layers=1,
                  opts=W.options(2 ** 8, 2 ** 5, 1e-4, 40, tv_norm=0))
         c["oracle_op"] = O.Op.dense(A.astype(np.float64))
+    elif name == "cdense2d_s32":
+        rng = np.random.default_rng(11)
+        side = 32
+        n = side * side
+        m = int(0.4 * n)
+        u = _complex_phantom(side, rng)
+        A = ((rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))) / math.sqrt(2 * m)).astype(np.complex64)
+        b = _complex_noise(A.astype(np.complex128) @ u.ravel(), 0.01, rng).astype(np.complex64)
+        c.update(shape=(side, side), A=A, b=b, u_true=u.astype(np.complex64), ref_kind="dense", api="dense",
+                 layers=1, opts=W.options(2 ** 8, 2 ** 5, 1e-4, 300, tv_norm=0))
+    elif name == "ccsr2d_s32":
+        rng = np.random.default_rng(12)
+        side = 32
+        n = side * side
+        m = int(0.5 * n)
+        k = 40   # entries per row
+        colind = np.concatenate([np.sort(rng.choice(n, k, replace=False)) for _ in range(m)]).astype(np.int32)
+        rowptr = (np.arange(m + 1) * k).astype(np.int32)
+        val = ((rng.standard_normal(m * k) + 1j * rng.standard_normal(m * k)) / math.sqrt(2 * k)).astype(np.complex64)
+        csr = {"m": m, "n": n, "rowptr": rowptr, "colind": colind, "val": val}
+        u = _complex_phantom(side, rng)
+        b = _complex_noise(_csr_apply(csr, u.ravel()), 0.01, rng).astype(np.complex64)
+        c.update(shape=(side, side), b=b, u_true=u.astype(np.complex64), csr=csr, csr_tuple=_csr_tuple(csr),
+                 ref_kind="csr", api="csr", layers=1, opts=W.options(2 ** 8, 2 ** 5, 1e-4, 300, tv_norm=0))
+    elif name == "cring2d_s64":
+        w = W.ring2d(seed=13, side=64, T=64, tv_norm=0, maxit=300, tol=1e-5)
+        rng = np.random.default_rng(13)
+        u = _complex_phantom(64, rng)
+        csr = dict(w["csr"])
+        csr["val"] = csr["val"].astype(np.complex64)
+        b = _complex_noise(_csr_apply(csr, u.ravel()), 0.005, rng).astype(np.complex64)
+        c.update(shape=w["shape"], b=b, u_true=u.astype(np.complex64), opts=w["opts"], geom=w["geom"], csr=csr,
+                 csr_tuple=_csr_tuple(csr), ref_kind="csr", api="ray2d_complex", layers=1)
     else:
         raise KeyError(name)
     return c
@@ -98,4 +153,6 @@ def api_problem(c, capi):
         return capi.csr_problem(c["shape"], A["m"], A["n"], A["rowptr"], A["colind"], A["val"], c.get("layers", 1))
     if c["api"] == "ray2d":
         return capi.ray2d_problem(c["shape"], c["geom"])
+    if c["api"] == "ray2d_complex":
+        return capi.ray2d_problem(c["shape"], c["geom"], complex_data=True)
     return capi.ray3d_problem(c["shape"], c["geom"])

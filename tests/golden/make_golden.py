@@ -6,7 +6,7 @@ restatement on small seeded problems from tval3g.workloads, and stores their
 outputs with checksums of the inputs (the inputs are regenerated from the same
 seeds at test time).  Must run where the reference sources are available:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
 
 The 3D reference prints to stdout and writes profile.txt into the current
 directory (3d/tval3_cpu_3d.cpp:1228,1328-1335), so it runs in a temporary
@@ -26,7 +26,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle as O  # noqa: E402
 from tval3g import workloads as W  # noqa: E402
 
-from cases import CASES, build_case  # noqa: E402
+from cases import CASES, COMPLEX_CASES, build_case  # noqa: E402
 
 
 def checksum(a):
@@ -34,11 +34,40 @@ def checksum(a):
     return np.array([a.size, a.sum(), np.abs(a).sum(), (a * np.arange(a.size) % 7.0).sum()])
 
 
+def complex_case(name, tmp):
+    """Complex data: the reference's complex<float> (dtype 3) and
+    complex<double> (dtype 4) builds; the latter is the FP64 anchor."""
+    c = build_case(name)
+    out = {"b_sum": checksum(np.concatenate([c["b"].real, c["b"].imag]))}
+    if "A" in c:
+        out["A_sum"] = checksum(np.concatenate([c["A"].real.ravel(), c["A"].imag.ravel()]))
+    cwd = os.getcwd()
+    os.chdir(tmp)
+    try:
+        for dtype in (3, 4):
+            rr = O.ref_solve(c["ref_kind"], c["shape"], c["b"], c["opts"], dtype=dtype, A=c.get("A"),
+                             csr=c.get("csr_tuple"), Ut=c["u_true"])
+            out[f"ref{dtype}_U"] = rr.U.astype(np.complex128)
+            out[f"ref{dtype}_iters"] = np.array([rr.outer_iters, rr.total_iters])
+            out[f"ref{dtype}_relerr"] = np.array([rr.rel_error, rr.rel_chg])
+    finally:
+        os.chdir(cwd)
+    out["oracle_U"] = out["ref4_U"]
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(name, {k: v.shape for k, v in out.items()})
+
+
 def main():
     O.build(reference=True)
     cwd = os.getcwd()
     tmp = tempfile.mkdtemp()
+    only = set(sys.argv[1:])
+    for name in COMPLEX_CASES:
+        if not only or name in only:
+            complex_case(name, tmp)
     for name in CASES:
+        if only and name not in only:
+            continue
         c = build_case(name)
         out = {"b_sum": checksum(c["b"])}
         if "A" in c:

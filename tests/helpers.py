@@ -8,8 +8,9 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def relerr(a, b):
-    a = np.asarray(a, np.float64).ravel()
-    b = np.asarray(b, np.float64).ravel()
+    dt = np.complex128 if np.iscomplexobj(a) or np.iscomplexobj(b) else np.float64
+    a = np.asarray(a, dt).ravel()
+    b = np.asarray(b, dt).ravel()
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 

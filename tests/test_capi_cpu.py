@@ -96,3 +96,21 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(capi.TVAL3Error) as e:
         capi.solve(spec, np.zeros(5, np.float32), _opts())
     assert e.value.code in (capi.ERR_NO_DEVICE, capi.ERR_CUDA)
+
+
+def test_complex_argument_errors():
+    """Complex data: 2D, one layer; the reference's size checks first."""
+    A = np.zeros((5, 16), np.complex64)
+    spec = capi.dense_problem((4, 4), A)
+    assert spec.p.complex_data == 1
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve(spec, np.zeros(6, np.complex64), _opts())
+    assert str(e.value) == "Argument error: b.len must be equal to A.dim_y * layers!"
+    spec = capi.dense_problem((4, 8), A, layers=2)
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve(spec, np.zeros(10, np.complex64), _opts())
+    assert str(e.value) == "Argument error: complex data with more than one layer is not supported"
+    spec = capi.dense_problem((2, 2, 4), A)
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve(spec, np.zeros(5, np.complex64), _opts())
+    assert str(e.value) == "Argument error: complex data is supported for 2D problems only"

@@ -48,7 +48,8 @@ def test_argument_errors_match_reference(demo):
     assert got["csc"] == "Argument error: A must be available in CSR and CSC format!"
     assert got["geom_layers_or_blen"] == "Argument error: b.len must be equal to A.num_emitters * A.num_receivers!"
     assert got["double"] == "Argument error: Matrices must be in row major format!"   # checked as for float
-    assert got["complex"].startswith("Internal error: complex data is not supported")
+    assert got["complex"] == "Argument error: complex data with more than one layer is not supported"
+    assert got["complex_format"] == "Argument error: Matrices must be in row major format!"
     if O.ref_available(2):   # the reference itself, same arguments
         opts = dict(mu=256.0, beta=32.0, mu0=256.0, beta0=32.0, tol=1e-4, tol_inn=1e-3, c=1e-5, gamma=0.6,
                     gam=0.9995, rate_gam=0.9, rate_cnt=2.0, maxit=30, maxcnt=10)
@@ -63,6 +64,6 @@ def test_argument_errors_match_reference(demo):
 def test_dropin_solves_equal_c_abi(demo, torch_cuda):
     out = subprocess.run([demo, "solve"], capture_output=True, text=True, check=True).stdout.strip().splitlines()
     rows = {line.split()[0]: line.split()[1:] for line in out}
-    for case in ("dense", "dense_f64", "csr", "ray2d"):
+    for case in ("dense", "dense_f64", "csr", "ray2d", "cdense"):
         rc, diff, it1, it2 = rows[case]
         assert rc == "0" and float(diff) == 0.0 and it1 == it2, (case, rows[case])

@@ -1,0 +1,102 @@
+"""Complex data on the GPU (the reference's complex<float> overloads,
+2d/tval3_cpu_2d.cpp:913-929 and the sparse and geometry ones).
+
+The FP64 anchor is the reference's own complex<double> build; the bar for the
+FP32 GPU solution is the one of the real cases,
+
+    |U_gpu - U_ref_cdouble| <= max(1e-3, 2 * |U_ref_cfloat - U_ref_cdouble|).
+
+The engine solves the real form of the problem on planar vectors (real plane,
+imaginary plane) with the complex shrinkage coupling the planes; the
+operator tests check that real form against numpy's complex products.
+"""
+import numpy as np
+import pytest
+
+from golden.cases import COMPLEX_CASES, api_problem, build_case
+from helpers import golden, relerr
+from tval3g import capi
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", COMPLEX_CASES)
+def test_complex_solve_matches_reference(name, torch_cuda):
+    c = build_case(name)
+    g = golden(f"{name}.npz")
+    U, info = capi.solve(api_problem(c, capi), c["b"], c["opts"], Ut=c["u_true"])
+    assert U.dtype == np.complex64 and info["status"] == 0
+    bar = max(1e-3, 2 * relerr(g["ref3_U"], g["ref4_U"]))
+    e = relerr(U, g["ref4_U"])
+    print(name, "relerr vs complex<double> reference", e, "bar", bar, "iterations", info["total_iters"],
+          "reference", tuple(g["ref4_iters"]))
+    assert e < bar, (name, e, bar)
+    assert abs(info["rel_error"] - relerr(U, c["u_true"])) < 1e-5
+
+
+def _planar(x):
+    return np.concatenate([x.real, x.imag]).astype(np.float32)
+
+
+@pytest.mark.parametrize("name", COMPLEX_CASES)
+def test_complex_operator_is_the_real_form(name, torch_cuda):
+    """Operator on planar vectors: [Re A x; Im A x] and [Re A^H y; Im A^H y]."""
+    torch = torch_cuda
+    c = build_case(name)
+    op = capi.Operator(api_problem(c, capi))
+    rng = np.random.default_rng(3)
+    n, m = op.cols // 2, op.rows // 2
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    y = rng.standard_normal(m) + 1j * rng.standard_normal(m)
+    if "A" in c:
+        A = c["A"].astype(np.complex128)
+        Ax, Ahy = A @ x, A.conj().T @ y
+    else:
+        csr = c["csr"]
+        rows = np.repeat(np.arange(csr["m"]), np.diff(csr["rowptr"]))
+        v = csr["val"].astype(np.complex128)
+        Ax = np.zeros(m, complex)
+        np.add.at(Ax, rows, v * x[csr["colind"]])
+        Ahy = np.zeros(n, complex)
+        np.add.at(Ahy, csr["colind"], v.conj() * y[rows])
+    dx = torch.tensor(_planar(x), device="cuda")
+    dy = torch.tensor(_planar(y), device="cuda")
+    out_m = torch.empty(2 * m, device="cuda")
+    out_n = torch.empty(2 * n, device="cuda")
+    op.apply(dx, out_m)
+    op.apply(dy, out_n, trans=True)
+    torch.cuda.synchronize()
+    got_m, got_n = out_m.cpu().numpy(), out_n.cpu().numpy()
+    op.close()
+    assert relerr(got_m[:m] + 1j * got_m[m:], Ax) < 1e-6
+    assert relerr(got_n[:n] + 1j * got_n[n:], Ahy) < 1e-6
+
+
+def test_complex_data_with_real_values_is_the_real_solve(torch_cuda):
+    """Complex data whose imaginary parts are 0 stay real: the solution's
+    imaginary part is exactly 0 and its real part is the real solve's."""
+    c = build_case("dense2d_s32_it20")
+    Ur, ir = capi.solve(capi.dense_problem(c["shape"], c["A"]), c["b"], c["opts"])
+    Uc, ic = capi.solve(capi.dense_problem(c["shape"], c["A"].astype(np.complex64)), c["b"].astype(np.complex64),
+                        c["opts"])
+    assert np.all(Uc.imag == 0)
+    assert ic["total_iters"] == ir["total_iters"]
+    assert relerr(Uc.real, Ur) < 1e-4
+
+
+def test_complex_batch_equals_single_bitwise(torch_cuda):
+    names = ["cdense2d_s32", "ccsr2d_s32", "dense2d_s32_it20", "cring2d_s64"]
+    cases = [build_case(n) for n in names]
+    specs = [api_problem(c, capi) for c in cases]
+    ub, ib = capi.solve_batch(specs, [c["b"] for c in cases], [c["opts"] for c in cases])
+    for k, c in enumerate(cases):
+        us, is_ = capi.solve_batch([specs[k]], [c["b"]], [c["opts"]])
+        np.testing.assert_array_equal(ub[k], us[0])
+        assert ib[k]["total_iters"] == is_[0]["total_iters"]
+
+
+def test_complex_operator_needs_host_arrays(torch_cuda):
+    c = build_case("cdense2d_s32")
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.Plan([api_problem(c, capi)], [c["opts"]], device_inputs=True)
+    assert str(e.value) == "Argument error: complex operators must be given in host memory"

@@ -14,7 +14,7 @@ import oracle as O
 from helpers import golden, relerr
 from tval3g import workloads as W
 
-from golden.cases import CASES, build_case  # noqa: E402
+from golden.cases import CASES, COMPLEX_CASES, build_case  # noqa: E402
 
 
 def _checksum(a):
@@ -49,6 +49,35 @@ def test_reference_float_build_drift_documented():
     assert relerr(g["ref0_U"], g["ref2_U"]) < 1e-3
     g = golden("dense2d_s32_conv.npz")
     assert relerr(g["ref0_U"], g["ref2_U"]) < 2e-2
+
+
+@pytest.mark.parametrize("name", COMPLEX_CASES)
+def test_complex_inputs_regenerate_bit_identically(name):
+    c = build_case(name)
+    g = golden(f"{name}.npz")
+    np.testing.assert_array_equal(_checksum(np.concatenate([c["b"].real, c["b"].imag])), g["b_sum"])
+    if "A" in c:
+        np.testing.assert_array_equal(_checksum(np.concatenate([c["A"].real.ravel(), c["A"].imag.ravel()])),
+                                      g["A_sum"])
+
+
+def test_complex_reference_float_drift_documented():
+    """The reference's complex<float> build against its complex<double>
+    build (the FP64 anchor of the complex cases): the GPU bar is twice this."""
+    drift = {n: relerr(golden(f"{n}.npz")["ref3_U"], golden(f"{n}.npz")["ref4_U"]) for n in COMPLEX_CASES}
+    assert drift["cdense2d_s32"] < 2e-2 and drift["ccsr2d_s32"] < 1e-3 and drift["cring2d_s64"] < 5e-2, drift
+    for n in COMPLEX_CASES:   # the anchor is the complex<double> solution, complex-valued
+        g = golden(f"{n}.npz")
+        assert np.iscomplexobj(g["oracle_U"]) and np.abs(g["oracle_U"].imag).max() > 0.05
+
+
+@pytest.mark.skipif(not O.ref_available(2), reason="reference not built here")
+def test_complex_reference_live_matches_fixture(tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)
+    c = build_case("ccsr2d_s32")
+    g = golden("ccsr2d_s32.npz")
+    r = O.ref_solve("csr", c["shape"], c["b"], c["opts"], dtype=4, csr=c["csr_tuple"], Ut=c["u_true"])
+    np.testing.assert_array_equal(r.U, g["ref4_U"])
 
 
 @pytest.mark.skipif(not O.ref_available(2), reason="reference not built here")

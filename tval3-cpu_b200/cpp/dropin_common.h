@@ -6,6 +6,7 @@
 #ifndef TVAL3_DROPIN_COMMON_H_
 #define TVAL3_DROPIN_COMMON_H_
 
+#include <complex>
 #include <cstring>
 #include <string>
 
@@ -47,21 +48,29 @@ inline tval3g_problem empty_problem() {
 }
 
 // image shape of U: dim_z is used only by 3D problems
-inline void set_image(tval3g_problem &p, int dims, const mat<float> &U) {
+template <class T>
+inline void set_image(tval3g_problem &p, int dims, const mat<T> &U) {
 	p.dims = dims;
 	p.dim_y = U.dim_y;
 	p.dim_x = U.dim_x;
 	p.dim_z = dims == 3 ? U.dim_z : 1;
 }
 
-// run a solve; throws tval3_exception with the C ABI's message on failure
-template <class S>
-inline tval3_info<S> solve(const tval3g_problem &p, mat<float> &U, const mat<float> &b, const tval3_options<S> &opts,
-                           const mat<float> &Ut) {
+// the float view of float or complex<float> data (interleaved re, im)
+inline const float *fdata(const mat<float> &a) { return a.data(); }
+inline float *fdata(mat<float> &a) { return a.data(); }
+inline const float *fdata(const mat<std::complex<float> > &a) { return reinterpret_cast<const float *>(a.data()); }
+inline float *fdata(mat<std::complex<float> > &a) { return reinterpret_cast<float *>(a.data()); }
+
+// run a solve (T = float, or complex<float> with p.complex_data = 1); throws
+// tval3_exception with the C ABI's message on failure
+template <class S, class T>
+inline tval3_info<S> solve(const tval3g_problem &p, mat<T> &U, const mat<T> &b, const tval3_options<S> &opts,
+                           const mat<T> &Ut) {
 	tval3g_options o = to_c(opts);
 	tval3g_info info;
 	std::memset(&info, 0, sizeof(info));
-	int rc = tval3g_solve(&p, b.data(), b.len, &o, Ut.len > 0 ? Ut.data() : 0, Ut.len, U.data(), &info);
+	int rc = tval3g_solve(&p, fdata(b), b.len, &o, Ut.len > 0 ? fdata(Ut) : 0, Ut.len, fdata(U), &info);
 	if (rc != TVAL3G_OK) {
 		std::string msg = tval3g_last_error();
 		if (rc == TVAL3G_ERR_ARGUMENT) throw tval3_exception(msg);
@@ -94,6 +103,28 @@ inline void narrow(const sparse_mat<double> &a, sparse_mat<float> &f) {   // f: 
 }
 inline void widen(const mat<float> &f, mat<double> &a) {
 	for (int i = 0; i < a.len && i < f.len; i++) a[i] = (double)f[i];
+}
+// complex<double> data (the reference's complex<double> overloads) likewise
+// through complex<float>
+inline mat<std::complex<float> > narrow(const mat<std::complex<double> > &a) {
+	mat<std::complex<float> > f(a.dim_y, a.dim_x, a.dim_z, a.format);
+	for (int i = 0; i < a.len; i++) f[i] = std::complex<float>((float)a[i].real(), (float)a[i].imag());
+	return f;
+}
+inline void narrow(const sparse_mat<std::complex<double> > &a, sparse_mat<std::complex<float> > &f) {
+	std::memcpy(f.csr_ptr(), a.csr_ptr(), sizeof(int) * ((size_t)a.dim_y + 1));
+	std::memcpy(f.csc_ptr(), a.csc_ptr(), sizeof(int) * ((size_t)a.dim_x + 1));
+	if (a.nnz > 0) {
+		std::memcpy(f.csr_ind(), a.csr_ind(), sizeof(int) * (size_t)a.nnz);
+		std::memcpy(f.csc_ind(), a.csc_ind(), sizeof(int) * (size_t)a.nnz);
+	}
+	for (int k = 0; k < a.nnz; k++) {
+		f.csr_val()[k] = std::complex<float>((float)a.csr_val()[k].real(), (float)a.csr_val()[k].imag());
+		f.csc_val()[k] = std::complex<float>((float)a.csc_val()[k].real(), (float)a.csc_val()[k].imag());
+	}
+}
+inline void widen(const mat<std::complex<float> > &f, mat<std::complex<double> > &a) {
+	for (int i = 0; i < a.len && i < f.len; i++) a[i] = std::complex<double>(f[i].real(), f[i].imag());
 }
 
 inline void unsupported(const char *what) {

@@ -10,9 +10,11 @@ using namespace tval3g_dropin;
 
 namespace {
 
-template <class S>
-tval3_info<S> dense2d(mat<float> &U, const mat<float> &A, const mat<float> &b, const tval3_options<S> &opts,
-                      const mat<float> &Ut) {
+template <class T> struct is_cplx { static const int value = 0; };
+template <class T> struct is_cplx<std::complex<T> > { static const int value = 1; };
+
+template <class S, class T>
+tval3_info<S> dense2d(mat<T> &U, const mat<T> &A, const mat<T> &b, const tval3_options<S> &opts, const mat<T> &Ut) {
 	if (U.format != mat_col_major || Ut.format != mat_col_major || A.format != mat_row_major)
 		throw tval3_exception(std::string("Argument error: Matrices must be in row major format!"));
 	tval3g_problem p = empty_problem();
@@ -21,13 +23,14 @@ tval3_info<S> dense2d(mat<float> &U, const mat<float> &A, const mat<float> &b, c
 	p.m = A.dim_y;
 	p.n_cols = A.dim_x;
 	p.layers = A.dim_y > 0 ? b.len / A.dim_y : 0;   // 2d/tval3_cpu_2d.cpp:894
-	p.A = A.data();
+	p.A = fdata(A);
+	p.complex_data = is_cplx<T>::value;
 	return solve<S>(p, U, b, opts, Ut);
 }
 
-template <class S>
-tval3_info<S> sparse2d(mat<float> &U, const sparse_mat<float> &A, const mat<float> &b, const tval3_options<S> &opts,
-                       const mat<float> &Ut) {
+template <class S, class T>
+tval3_info<S> sparse2d(mat<T> &U, const sparse_mat<T> &A, const mat<T> &b, const tval3_options<S> &opts,
+                       const mat<T> &Ut) {
 	if (U.format != mat_col_major || Ut.format != mat_col_major)
 		throw tval3_exception(std::string("Argument error: Matrices must be in row major format!"));
 	if (A.format != sparse_mat_both)
@@ -41,13 +44,13 @@ tval3_info<S> sparse2d(mat<float> &U, const sparse_mat<float> &A, const mat<floa
 	p.nnz = A.nnz;
 	p.csr_ptr = A.csr_ptr();
 	p.csr_ind = A.csr_ind();
-	p.csr_val = A.csr_val();
+	p.csr_val = reinterpret_cast<const float *>(A.csr_val());
+	p.complex_data = is_cplx<T>::value;
 	return solve<S>(p, U, b, opts, Ut);
 }
 
-template <class S>
-tval3_info<S> ray2d(mat<float> &U, const geometry &A, const mat<float> &b, const tval3_options<S> &opts,
-                    const mat<float> &Ut) {
+template <class S, class T>
+tval3_info<S> ray2d(mat<T> &U, const geometry &A, const mat<T> &b, const tval3_options<S> &opts, const mat<T> &Ut) {
 	if (U.format != mat_row_major || Ut.format != mat_row_major)
 		throw tval3_exception(std::string("Argument error: Matrices must be in row major format!"));
 	tval3g_problem p = empty_problem();
@@ -62,6 +65,7 @@ tval3_info<S> ray2d(mat<float> &U, const geometry &A, const mat<float> &b, const
 	p.y_receivers = A.y_receivers;
 	p.ld = A.ld;
 	p.scale_factor = A.scale_factor;
+	p.complex_data = is_cplx<T>::value;
 	return solve<S>(p, U, b, opts, Ut);
 }
 
@@ -84,17 +88,18 @@ const tval3_info<double> tval3_cpu_2d(mat<double> &U, const mat<double> &A, cons
 	widen(Uf, U);
 	return r;
 }
-const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &, const mat<std::complex<float> > &,
-                                     const mat<std::complex<float> > &, const tval3_options<float> &,
-                                     const mat<std::complex<float> > &, int, int) {
-	unsupported("complex");
-	return tval3_info<float>();
+const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &U, const mat<std::complex<float> > &A,
+                                     const mat<std::complex<float> > &b, const tval3_options<float> &opts,
+                                     const mat<std::complex<float> > &Ut, int, int) {
+	return dense2d<float>(U, A, b, opts, Ut);
 }
-const tval3_info<double> tval3_cpu_2d(mat<std::complex<double> > &, const mat<std::complex<double> > &,
-                                      const mat<std::complex<double> > &, const tval3_options<double> &,
-                                      const mat<std::complex<double> > &, int, int) {
-	unsupported("complex");
-	return tval3_info<double>();
+const tval3_info<double> tval3_cpu_2d(mat<std::complex<double> > &U, const mat<std::complex<double> > &A,
+                                      const mat<std::complex<double> > &b, const tval3_options<double> &opts,
+                                      const mat<std::complex<double> > &Ut, int, int) {
+	mat<std::complex<float> > Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut), Af = narrow(A);
+	const tval3_info<double> r = dense2d<double>(Uf, Af, bf, opts, Utf);
+	widen(Uf, U);
+	return r;
 }
 
 // ---- sparse ----------------------------------------------------------------
@@ -115,17 +120,20 @@ const tval3_info<double> tval3_cpu_2d(mat<double> &U, const sparse_mat<double> &
 	widen(Uf, U);
 	return r;
 }
-const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &, const sparse_mat<std::complex<float> > &,
-                                     const mat<std::complex<float> > &, const tval3_options<float> &,
-                                     const mat<std::complex<float> > &, int, int) {
-	unsupported("complex");
-	return tval3_info<float>();
+const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &U, const sparse_mat<std::complex<float> > &A,
+                                     const mat<std::complex<float> > &b, const tval3_options<float> &opts,
+                                     const mat<std::complex<float> > &Ut, int, int) {
+	return sparse2d<float>(U, A, b, opts, Ut);
 }
-const tval3_info<double> tval3_cpu_2d(mat<std::complex<double> > &, const sparse_mat<std::complex<double> > &,
-                                      const mat<std::complex<double> > &, const tval3_options<double> &,
-                                      const mat<std::complex<double> > &, int, int) {
-	unsupported("complex");
-	return tval3_info<double>();
+const tval3_info<double> tval3_cpu_2d(mat<std::complex<double> > &U, const sparse_mat<std::complex<double> > &A,
+                                      const mat<std::complex<double> > &b, const tval3_options<double> &opts,
+                                      const mat<std::complex<double> > &Ut, int, int) {
+	mat<std::complex<float> > Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
+	sparse_mat<std::complex<float> > Af(A.dim_y, A.dim_x, A.nnz, A.format);
+	narrow(A, Af);
+	const tval3_info<double> r = sparse2d<double>(Uf, Af, bf, opts, Utf);
+	widen(Uf, U);
+	return r;
 }
 
 // ---- geometry --------------------------------------------------------------
@@ -144,15 +152,16 @@ const tval3_info<double> tval3_cpu_2d(mat<double> &U, const geometry &A, const m
 	widen(Uf, U);
 	return r;
 }
-const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &, const geometry &,
-                                     const mat<std::complex<float> > &, const tval3_options<float> &,
-                                     const mat<std::complex<float> > &, int, int) {
-	unsupported("complex");
-	return tval3_info<float>();
+const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &U, const geometry &A,
+                                     const mat<std::complex<float> > &b, const tval3_options<float> &opts,
+                                     const mat<std::complex<float> > &Ut, int, int) {
+	return ray2d<float>(U, A, b, opts, Ut);
 }
-const tval3_info<double> tval3_cpu_2d(mat<std::complex<double> > &, const geometry &,
-                                      const mat<std::complex<double> > &, const tval3_options<double> &,
-                                      const mat<std::complex<double> > &, int, int) {
-	unsupported("complex");
-	return tval3_info<double>();
+const tval3_info<double> tval3_cpu_2d(mat<std::complex<double> > &U, const geometry &A,
+                                      const mat<std::complex<double> > &b, const tval3_options<double> &opts,
+                                      const mat<std::complex<double> > &Ut, int, int) {
+	mat<std::complex<float> > Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
+	const tval3_info<double> r = ray2d<double>(Uf, A, bf, opts, Utf);
+	widen(Uf, U);
+	return r;
 }

@@ -89,7 +89,8 @@ int tval3g_solve_batch(int count, const tval3g_problem *probs, const float *cons
 	} guard{&db, &du, &dut, s};
 	for (int i = 0; i < count; i++) {
 		const tval3g_problem &p = probs[i];
-		long long n = (long long)p.dim_x * p.dim_y * (p.dims == 3 ? p.dim_z : 1), bl = b_len_of(p);
+		const int planes = p.complex_data ? 2 : 1;   // complex data: interleaved (re, im) floats
+		long long n = (long long)p.dim_x * p.dim_y * (p.dims == 3 ? p.dim_z : 1) * planes, bl = b_len_of(p) * planes;
 		ns[i] = n;
 		db[i] = (float *)dev_alloc(sizeof(float) * bl, s);
 		du[i] = (float *)dev_alloc(sizeof(float) * n, s);
@@ -209,9 +210,11 @@ int tval3g_op_create(tval3g_operator **out, const tval3g_problem *prob, int flag
 		prepare_op(op->s, *prob, flags, op->st, true);
 		const tval3g_problem &p = *prob;
 		Inst &I = op->h;
-		I.dims = p.dims; I.p = p.dim_y; I.q = p.dim_x; I.r = p.dims == 3 ? p.dim_z : 1;
+		const int planes = p.complex_data ? 2 : 1;   // complex: the real form on planar vectors
+		I.dims = p.dims; I.p = p.dim_y; I.q = p.dim_x; I.r = p.dims == 3 ? p.dim_z : planes;
 		I.n = (long long)p.dim_x * p.dim_y * I.r;
 		I.m = op->st.b_len;
+		I.cplx = p.complex_data != 0;
 		I.op = op->st.dev;
 		op->rows = I.m;
 		op->cols = I.n;

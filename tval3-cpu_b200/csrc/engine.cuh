@@ -202,8 +202,22 @@ struct Inst {
 	double target;               // > 0: also stop once |U/scl - Ut| <= target |Ut|
 	const double *sched;         // schedule mode: mu_1..mu_maxit, beta_1..beta_maxit (device), or NULL
 	int maxit, maxcnt, nonneg, tv_norm, numInit, skip_enabled;
+	// complex data (2D): the image vectors hold the real plane (z = 0) and
+	// the imaginary plane (z = 1) of the complex image, the measurement
+	// vectors Re b then Im b, and the operator is the real form
+	// [[Re A, -Im A], [Im A, Re A]]; the caller's b, Ut and U stay
+	// interleaved (re, im) pairs (cplx_index)
+	int cplx;
 	OpDev op;
 };
+
+// position in the caller's interleaved complex array of element i of a
+// planar vector of length len (two planes of len / 2); i itself for real data
+__device__ __forceinline__ long long cplx_index(const Inst &I, long long i, long long len) {
+	if (!I.cplx) return i;
+	const long long h = len >> 1;
+	return i < h ? 2 * i : 2 * (i - h) + 1;
+}
 
 // Tiles: image vectors one element per thread (a 256^2 image is 256 blocks),
 // measurement vectors four (their kernels do little per element, and fewer

@@ -121,7 +121,70 @@ struct Shrink {
 		}
 		return lam;
 	}
+	// complex data: (u, s) of this plane and (up, sp) of the other plane at
+	// the same pixel; anisotropic: each component's Ubar = (re, im) shrinks
+	// by its modulus, W = max(|Ubar| - 1/beta, 0) Ubar / |Ubar| (2d:614-649);
+	// isotropic: by the modulus over all components.  Returns this plane's
+	// share of lambda1 (the real plane carries it, the imaginary plane 0).
+	__device__ __forceinline__ float apply_c(const float (&u)[3], const float (&s)[3], const float (&up)[3],
+	                                         const float (&sp)[3], bool imag, float (&w)[3]) const {
+		float re[3], im[3];
+#pragma unroll
+		for (int c = 0; c < 3; c++) {
+			const float a = (c < dims) ? u[c] - s[c] * rbeta : 0.f;
+			const float b = (c < dims) ? up[c] - sp[c] * rbeta : 0.f;
+			re[c] = imag ? b : a;
+			im[c] = imag ? a : b;
+		}
+		if (iso) {
+			float nrm2 = 0.f;
+#pragma unroll
+			for (int c = 0; c < 3; c++) nrm2 += re[c] * re[c] + im[c] * im[c];
+			const float nrm = sqrtf(nrm2);
+			float t = nrm - thr;
+			t = t >= 0.f ? t : 0.f;
+			const float sc = nrm > 0.f ? t / nrm : 0.f;
+#pragma unroll
+			for (int c = 0; c < 3; c++) w[c] = sc * (imag ? im[c] : re[c]);
+			return imag ? 0.f : t;
+		}
+		float lam = 0.f;
+#pragma unroll
+		for (int c = 0; c < 3; c++) {
+			const float ab = sqrtf(re[c] * re[c] + im[c] * im[c]);
+			float t = ab - thr;
+			t = t >= 0.f ? t : 0.f;
+			if (c < dims) lam += t;
+			w[c] = ab > 0.f ? t * (imag ? im[c] : re[c]) / ab : 0.f;
+		}
+		return imag ? 0.f : lam;
+	}
 };
+
+// shrinkage at image element j: loads its gradient components u and
+// multipliers s (and, for complex data, the other plane's) and returns the
+// lambda1 share
+__device__ __forceinline__ float shrink_at(const Inst &I, const Shrink &sh, int j, const float *const (&Uc)[3],
+                                           const float *const (&Sc)[3], float (&u)[3], float (&s)[3],
+                                           float (&w)[3]) {
+	const int dims = I.dims;
+#pragma unroll
+	for (int c = 0; c < 3; c++) {
+		u[c] = c < dims ? Uc[c][j] : 0.f;
+		s[c] = c < dims ? Sc[c][j] : 0.f;
+	}
+	if (!I.cplx) return sh.apply(u, s, w);
+	const int h = (int)(I.n >> 1);
+	const bool imag = j >= h;
+	const int jp = imag ? j - h : j + h;
+	float up[3], sp[3];
+#pragma unroll
+	for (int c = 0; c < 3; c++) {
+		up[c] = c < dims ? Uc[c][jp] : 0.f;
+		sp[c] = c < dims ? Sc[c][jp] : 0.f;
+	}
+	return sh.apply_c(u, s, up, sp, imag, w);
+}
 
 __device__ __forceinline__ bool bad(double v) { return !isfinite(v); }
 
@@ -137,11 +200,12 @@ __device__ __forceinline__ void better_max(float &a, int &ia, float b, int ib) {
 
 __global__ void __launch_bounds__(BLOCK) k_scaleb(KArgs a) {
 	KPROLOGUE(a);
-	const int m = (int)I.m, i0 = local * TILE_M;
+	// complex data: over the m / 2 complex entries, |b| their modulus
+	const int m = I.cplx ? (int)(I.m >> 1) : (int)I.m, i0 = local * TILE_M;
 	float mn = INFINITY, mx = -INFINITY;
 	int imn = INT_MAX, imx = INT_MAX;
 	FOR_TILE_M(i0, m, i) {
-		float v = fabsf(I.b_user[i]);
+		float v = I.cplx ? hypotf(I.b_user[2 * i], I.b_user[2 * i + 1]) : fabsf(I.b_user[i]);
 		better_min(mn, imn, v, i);
 		better_max(mx, imx, v, i);
 	}
@@ -183,7 +247,10 @@ __global__ void __launch_bounds__(BLOCK) k_scaleb(KArgs a) {
 	Ctrl &c = *I.ctrl;
 	double scl = 1.0;
 	if (gimn < m && gimx < m) {   // (all-NaN data leaves no index: no scaling)
-		double dif = fabs((double)I.b_user[gimx] - (double)I.b_user[gimn]);
+		// |bmax - bmin|; complex: the modulus of the float difference
+		double dif = I.cplx ? (double)hypotf(I.b_user[2 * gimx] - I.b_user[2 * gimn],
+		                                     I.b_user[2 * gimx + 1] - I.b_user[2 * gimn + 1])
+		                    : fabs((double)I.b_user[gimx] - (double)I.b_user[gimn]);
 		if (dif < 0.5) scl = 0.5 / dif;
 		else if (dif > 1.5) scl = 1.5 / dif;
 	}
@@ -222,7 +289,8 @@ __global__ void __launch_bounds__(BLOCK) k_init(KArgs a) {
 		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) {
 #pragma unroll
 			for (int v = 0; v < NVM; v++) I.vm[v][i] = 0.f;
-			I.vm[vB][i] = scl != 1.f ? I.b_user[i] * scl : I.b_user[i];
+			const float bu = I.b_user[cplx_index(I, i, I.m)];
+			I.vm[vB][i] = scl != 1.f ? bu * scl : bu;
 		}
 	}
 }
@@ -262,15 +330,12 @@ __global__ void __launch_bounds__(BLOCK) k_shrink(KArgs a) {
 	Ctrl &c = *I.ctrl;
 	Shrink sh(I, c.beta);
 	const int n = (int)I.n, dims = I.dims;
+	const float *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
+	const float *const Sc[3] = {I.vn[vSx], I.vn[vSy], I.vn[vSz]};
 	double v[3] = {0, 0, 0};   // lam1, lam2, lam4
 	FOR_TILE(local * TILE, n, i) {
 		float u[3], s[3], w[3];
-#pragma unroll
-		for (int cc = 0; cc < 3; cc++) {
-			u[cc] = cc < dims ? I.vn[vUx + cc][i] : 0.f;
-			s[cc] = cc < dims ? I.vn[vSx + cc][i] : 0.f;
-		}
-		v[0] += sh.apply(u, s, w);
+		v[0] += shrink_at(I, sh, i, Uc, Sc, u, s, w);
 #pragma unroll
 		for (int cc = 0; cc < 3; cc++)
 			if (cc < dims) {
@@ -445,12 +510,7 @@ __global__ void __launch_bounds__(BLOCK) k_shrink_grad(KArgs a) {
 		int x, y, z;
 		g.coords(i, x, y, z);
 		float u[3], s[3], w[3];
-#pragma unroll
-		for (int cc = 0; cc < 3; cc++) {
-			u[cc] = cc < dims ? Uc[cc][i] : 0.f;
-			s[cc] = cc < dims ? Sc[cc][i] : 0.f;
-		}
-		v[0] += sh.apply(u, s, w);
+		v[0] += shrink_at(I, sh, i, Uc, Sc, u, s, w);
 #pragma unroll
 		for (int cc = 0; cc < 3; cc++)
 			if (cc < dims) {
@@ -464,12 +524,7 @@ __global__ void __launch_bounds__(BLOCK) k_shrink_grad(KArgs a) {
 			return [&, cc](int j) -> float {
 				if (j == i) return u[cc] - w[cc];
 				float uj[3], sj[3], wj[3];
-#pragma unroll
-				for (int k = 0; k < 3; k++) {
-					uj[k] = k < dims ? Uc[k][j] : 0.f;
-					sj[k] = k < dims ? Sc[k][j] : 0.f;
-				}
-				sh.apply(uj, sj, wj);
+				shrink_at(I, sh, j, Uc, Sc, uj, sj, wj);
 				return uj[cc] - wj[cc];
 			};
 		};
@@ -488,7 +543,7 @@ __global__ void __launch_bounds__(BLOCK) k_shrink_grad(KArgs a) {
 			v[8] += (double)uu * tmp;
 		}
 		if (ut) {
-			const float t = I.ut_user[i], e = U[i] * rscl - t;
+			const float t = I.ut_user[cplx_index(I, i, I.n)], e = U[i] * rscl - t;
 			v[6] += (double)e * e;
 			v[7] += (double)t * t;
 		}
@@ -633,7 +688,7 @@ __global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
 				u = Up[i];
 			}
 			u = fmaf(ntau, d[i], u);
-			if (I.nonneg) u = u < 0.f ? 0.f : u;
+			if (I.nonneg) u = (I.cplx && i >= (int)(I.n >> 1)) ? 0.f : (u < 0.f ? 0.f : u);   // complex: Re >= 0, Im = 0 (2d:467-479)
 			U[i] = u;
 			if (xT) {
 				const int row = i / ld;
@@ -820,9 +875,10 @@ __global__ void __launch_bounds__(BLOCK) k_final(KArgs a) {
 	double v[2] = {0, 0};
 	FOR_TILE(local * TILE, (int)I.n, i) {
 		float u = I.vn[vU][i] / scl;
-		I.u_user[i] = u;
+		const long long ui = cplx_index(I, i, I.n);
+		I.u_user[ui] = u;
 		if (I.ut_user) {
-			float t = I.ut_user[i];
+			float t = I.ut_user[ui];
 			float dlt = t - u;
 			v[0] += (double)dlt * dlt;
 			v[1] += (double)t * t;

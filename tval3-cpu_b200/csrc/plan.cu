@@ -98,6 +98,12 @@ long long validate(const tval3g_problem &p, long long b_len, long long ut_len) {
 	default:
 		throw Error{TVAL3G_ERR_ARGUMENT, "Argument error: unknown operator kind"};
 	}
+	if (p.complex_data) {
+		TG_ARG(p.dims == 2 && p.op_kind != TVAL3G_OP_RAY3D,
+		       "Argument error: complex data is supported for 2D problems only");
+		TG_ARG(p.op_kind == TVAL3G_OP_RAY2D || p.layers == 1,
+		       "Argument error: complex data with more than one layer is not supported");
+	}
 	if (p.op_kind == TVAL3G_OP_RAY2D || p.op_kind == TVAL3G_OP_RAY3D) {
 		// every traced ray must stay inside the image (Bresenham stays inside
 		// the bounding box of its endpoints); the reference does not check
@@ -159,7 +165,101 @@ __global__ void k_map_out(long long nnz, const int4 *rays, int *cind) {
 	if (k < nnz) cind[k] = rays[cind[k]].w;
 }
 
+// Complex data (2D): the operator becomes its real form on planar vectors
+// [Re x; Im x] -> [Re A x; Im A x], i.e. [[Re A, -Im A], [Im A, Re A]], whose
+// transpose gives [Re A^H y; Im A^H y] - the reference's conjugate-transposed
+// products (2d/mat_mult.h:15-91, CblasConjTrans / 'c').  Dense A and CSR
+// values arrive as interleaved (re, im) floats; a ray geometry (real
+// weights) becomes the CSR form of diag(A, A) over its traced rays.
+static void prepare_complex_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
+                               bool keep_ray_csr) {
+	TG_ARG(!(flags & TVAL3G_DEVICE_INPUTS), "Argument error: complex operators must be given in host memory");
+	tval3g_problem q = p;
+	q.complex_data = 0;
+	q.layers = 1;
+	if (p.op_kind == TVAL3G_OP_DENSE) {
+		const long long m = p.m, nc = p.n_cols;
+		std::vector<float> R((size_t)(4 * m * nc));
+		for (long long r = 0; r < m; r++)
+			for (long long c = 0; c < nc; c++) {
+				const float ar = p.A[2 * (r * nc + c)], ai = p.A[2 * (r * nc + c) + 1];
+				R[(size_t)(r * 2 * nc + c)] = ar;
+				R[(size_t)(r * 2 * nc + nc + c)] = -ai;
+				R[(size_t)((m + r) * 2 * nc + c)] = ai;
+				R[(size_t)((m + r) * 2 * nc + nc + c)] = ar;
+			}
+		q.m = (int)(2 * m);
+		q.n_cols = (int)(2 * nc);
+		q.A = R.data();
+		prepare_op(s, q, flags, st, keep_ray_csr);   // copies R before it returns
+		return;
+	}
+	// CSR rows of the real form from (row pointers, columns, complex values)
+	auto expand = [&](long long m, long long nc, const std::vector<int> &ptr, const std::vector<int> &ind,
+	                  const float *re, const float *im, int re_stride) {
+		const long long nnz = ptr[m];
+		std::vector<int> rp((size_t)(2 * m + 1)), ri((size_t)(4 * nnz));
+		std::vector<float> rv((size_t)(4 * nnz));
+		long long o = 0;
+		for (int half = 0; half < 2; half++)
+			for (long long r = 0; r < m; r++) {
+				rp[(size_t)(half * m + r)] = (int)o;
+				for (int part = 0; part < 2; part++)   // columns of Re x, then of Im x
+					for (long long k = ptr[r]; k < ptr[r + 1]; k++) {
+						const float vr = re[k * re_stride], vi = im ? im[k * re_stride] : 0.f;
+						ri[(size_t)o] = ind[(size_t)k] + (part ? (int)nc : 0);
+						// [[Re A, -Im A], [Im A, Re A]]
+						rv[(size_t)o++] = half == 0 ? (part == 0 ? vr : -vi) : (part == 0 ? vi : vr);
+					}
+			}
+		rp[(size_t)(2 * m)] = (int)o;
+		tval3g_problem c = p;
+		c.complex_data = 0;
+		c.layers = 1;
+		c.op_kind = TVAL3G_OP_CSR;
+		c.m = (int)(2 * m);
+		c.n_cols = (int)(2 * nc);
+		c.nnz = o;
+		c.csr_ptr = rp.data();
+		c.csr_ind = ri.data();
+		c.csr_val = rv.data();
+		prepare_op(s, c, flags, st, keep_ray_csr);
+		TG_CUDA(cudaStreamSynchronize(s));
+	};
+	if (p.op_kind == TVAL3G_OP_CSR) {
+		std::vector<int> ptr(p.csr_ptr, p.csr_ptr + p.m + 1), ind(p.csr_ind, p.csr_ind + p.nnz);
+		expand(p.m, p.n_cols, ptr, ind, p.csr_val, p.csr_val + 1, 2);
+		return;
+	}
+	// 2D rays: trace on the device, then the CSR over all E x R measurements
+	OpStore tmp;
+	q.complex_data = 0;
+	prepare_op(s, q, flags, tmp, true);
+	const long long m = (long long)p.num_emitters * p.num_receivers;
+	const long long n = (long long)p.dim_x * p.dim_y;
+	const int nr = tmp.dev.nrays;
+	std::vector<int> trp((size_t)nr + 1), tri((size_t)std::max(tmp.nnz, 1LL));
+	TG_CUDA(cudaMemcpyAsync(trp.data(), tmp.ray_rptr, sizeof(int) * ((size_t)nr + 1), cudaMemcpyDeviceToHost, s));
+	if (tmp.nnz > 0)
+		TG_CUDA(cudaMemcpyAsync(tri.data(), tmp.ray_rind, sizeof(int) * (size_t)tmp.nnz, cudaMemcpyDeviceToHost, s));
+	TG_CUDA(cudaStreamSynchronize(s));
+	const float scale = tmp.dev.scale;
+	free_op(tmp, s);
+	std::vector<int> ptr((size_t)m + 1, 0), ind((size_t)std::max(tmp.nnz, 1LL));
+	for (int k = 0; k < nr; k++) ptr[(size_t)tmp.ray_out[k] + 1] = trp[(size_t)k + 1] - trp[(size_t)k];
+	for (long long r = 0; r < m; r++) ptr[(size_t)r + 1] += ptr[(size_t)r];
+	for (int k = 0; k < nr; k++)
+		std::copy(tri.begin() + trp[(size_t)k], tri.begin() + trp[(size_t)k + 1],
+		          ind.begin() + ptr[(size_t)tmp.ray_out[k]]);
+	std::vector<float> val((size_t)std::max(tmp.nnz, 1LL), scale);
+	expand(m, n, ptr, ind, val.data(), nullptr, 1);
+}
+
 void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st, bool keep_ray_csr) {
+	if (p.complex_data) {
+		prepare_complex_op(s, p, flags, st, keep_ray_csr);
+		return;
+	}
 	OpDev &d = st.dev;
 	d = OpDev{};
 	d.kind = p.op_kind;
@@ -479,10 +579,14 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 			long long n = validate(p, b_len, 0);
 			prepare_op(stream_, p, flags, ops_[i], false);
 			Inst &I = h_inst_[i];
-			I.dims = p.dims; I.p = p.dim_y; I.q = p.dim_x; I.r = p.dims == 3 ? p.dim_z : 1;
+			const int planes = p.complex_data ? 2 : 1;   // complex: real and imaginary planes
+			I.dims = p.dims; I.p = p.dim_y; I.q = p.dim_x; I.r = p.dims == 3 ? p.dim_z : planes;
 			I.fq.init((unsigned)I.q);
 			I.fp.init((unsigned)I.p);
-			I.n = n; I.m = b_len;
+			I.n = n * planes; I.m = b_len * planes;
+			I.cplx = p.complex_data != 0;
+			n = I.n;
+			b_len = I.m;
 			I.ntn = (int)((n + TILE - 1) / TILE);
 			I.ntm = (int)((b_len + TILE_M - 1) / TILE_M);
 			const tval3g_options &o = opts[i];

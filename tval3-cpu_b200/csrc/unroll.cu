@@ -613,6 +613,7 @@ extern "C" int tval3g_unrolled_create(tval3g_unrolled **h, const tval3g_problem 
                                       const tval3g_options *opts, int K, int ckpt) {
 	UNR_BEGIN
 	TG_ARG(h && prob && opts, "Argument error: NULL argument");
+	TG_ARG(!prob->complex_data, "Argument error: the unrolled solve takes real data");
 	*h = nullptr;
 	auto *u = new tval3g_unrolled{nullptr};
 	try {

@@ -56,7 +56,8 @@ class Problem(C.Structure):
                 ("num_emitters", C.c_int), ("num_receivers", C.c_int), ("numMPs", C.c_int), ("numPaths", C.c_int),
                 ("use_path", _IP), ("x_emitters", _IP), ("y_emitters", _IP), ("z_emitters", _IP),
                 ("x_receivers", _IP), ("y_receivers", _IP), ("z_receivers", _IP), ("ld", C.c_int),
-                ("rv_x", C.c_int), ("rv_y", C.c_int), ("rv_z", C.c_int), ("scale_factor", C.c_float)]
+                ("rv_x", C.c_int), ("rv_y", C.c_int), ("rv_z", C.c_int), ("scale_factor", C.c_float),
+                ("complex_data", C.c_int)]
 
 
 class TVAL3Error(RuntimeError):
@@ -165,28 +166,43 @@ def _ptr(a, ct):
     return a.ctypes.data_as(C.POINTER(ct))
 
 
+def _values(a):
+    """float32 array of a real array, or the interleaved (re, im) float32
+    view of a complex one; and whether it is complex"""
+    if np.iscomplexobj(a):
+        return _arr(a, np.complex64).view(np.float32), 1
+    return _arr(a, np.float32), 0
+
+
 def dense_problem(shape, A, layers=1, device_ptr=None):
-    """A: (m, n_cols) float32 host array (or device_ptr with A's shape)."""
+    """A: (m, n_cols) float32 or complex64 host array (or device_ptr with A's
+    shape, real).  A complex A makes a complex-data problem (b, Ut, U complex)."""
     m, ncols = A.shape
     if device_ptr is not None:
         return ProblemSpec(shape, OP_DENSE, [A], m=m, n_cols=ncols, layers=layers,
                            A=C.cast(C.c_void_p(device_ptr), _FP))
-    A = _arr(A, np.float32)
-    return ProblemSpec(shape, OP_DENSE, [A], m=m, n_cols=ncols, layers=layers, A=_ptr(A, C.c_float))
+    A, cplx = _values(A)
+    return ProblemSpec(shape, OP_DENSE, [A], m=m, n_cols=ncols, layers=layers, A=_ptr(A, C.c_float),
+                       complex_data=cplx)
 
 
 def csr_problem(shape, m, ncols, rowptr, colind, val, layers=1):
-    rowptr, colind, val = _arr(rowptr, np.int32), _arr(colind, np.int32), _arr(val, np.float32)
+    """val: float32 or complex64 (a complex-data problem)."""
+    rowptr, colind = _arr(rowptr, np.int32), _arr(colind, np.int32)
+    val, cplx = _values(val)
     return ProblemSpec(shape, OP_CSR, [rowptr, colind, val], m=m, n_cols=ncols, layers=layers, nnz=len(colind),
-                       csr_ptr=_ptr(rowptr, C.c_int), csr_ind=_ptr(colind, C.c_int), csr_val=_ptr(val, C.c_float))
+                       csr_ptr=_ptr(rowptr, C.c_int), csr_ind=_ptr(colind, C.c_int), csr_val=_ptr(val, C.c_float),
+                       complex_data=cplx)
 
 
-def ray2d_problem(shape, g):
+def ray2d_problem(shape, g, complex_data=False):
+    """complex_data: b, Ut and U are complex (the geometry is real)."""
     a = {k: _arr(g[k], np.int32) for k in ("use_path", "xe", "ye", "xr", "yr")}
     return ProblemSpec(shape, OP_RAY2D, list(a.values()), num_emitters=len(a["xe"]), num_receivers=len(a["xr"]),
                        numMPs=1, use_path=_ptr(a["use_path"], C.c_int), x_emitters=_ptr(a["xe"], C.c_int),
                        y_emitters=_ptr(a["ye"], C.c_int), x_receivers=_ptr(a["xr"], C.c_int),
-                       y_receivers=_ptr(a["yr"], C.c_int), ld=int(g["ld"]), scale_factor=float(g["scale"]))
+                       y_receivers=_ptr(a["yr"], C.c_int), ld=int(g["ld"]), scale_factor=float(g["scale"]),
+                       complex_data=int(bool(complex_data)))
 
 
 def ray3d_problem(shape, g):
@@ -217,10 +233,12 @@ def problem_from_workload(w, use_csr=False):
 # calls
 # --------------------------------------------------------------------------
 def solve(spec: ProblemSpec, b, opts: dict, Ut=None):
-    """One solve with host buffers; returns (U as spec.shape float32, info dict)."""
-    b = _arr(b, np.float32)
-    U = np.zeros(spec.n, np.float32)
-    Utv = _arr(Ut, np.float32).ravel() if Ut is not None else None
+    """One solve with host buffers; returns (U as spec.shape, float32 or -
+    for a complex-data problem - complex64, info dict)."""
+    dt = np.complex64 if spec.p.complex_data else np.float32
+    b = _arr(b, dt).ravel()
+    U = np.zeros(spec.n, dt)
+    Utv = _arr(Ut, dt).ravel() if Ut is not None else None
     info = Info()
     o = Options.from_dict(opts)
     rc = lib().tval3g_solve(C.byref(spec.p), b.ctypes.data, len(b), C.byref(o),
@@ -234,9 +252,10 @@ def solve_batch(specs, bs, opts_list, Uts=None, graph=True):
     n = len(specs)
     probs = (Problem * n)(*[s.p for s in specs])
     opts = (Options * n)(*[Options.from_dict(o) for o in opts_list])
-    barr = [_arr(b, np.float32) for b in bs]
-    uarr = [np.zeros(s.n, np.float32) for s in specs]
-    utarr = [(_arr(u, np.float32).ravel() if u is not None else None) for u in (Uts or [None] * n)]
+    dts = [np.complex64 if s.p.complex_data else np.float32 for s in specs]
+    barr = [_arr(b, dt).ravel() for b, dt in zip(bs, dts)]
+    uarr = [np.zeros(s.n, dt) for s, dt in zip(specs, dts)]
+    utarr = [(_arr(u, dt).ravel() if u is not None else None) for u, dt in zip(Uts or [None] * n, dts)]
     bp = (C.c_void_p * n)(*[b.ctypes.data for b in barr])
     up = (C.c_void_p * n)(*[u.ctypes.data for u in uarr])
     utp = (C.c_void_p * n)(*[(u.ctypes.data if u is not None else None) for u in utarr])
