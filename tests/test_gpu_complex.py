@@ -21,15 +21,40 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("name", COMPLEX_CASES)
+def test_complex_fixed_iterations_match_reference(name, torch_cuda):
+    """20 iterations (no stopping decision involved): within max(1e-4, 2 x
+    the reference's complex<float> drift) of its complex<double> build."""
+    c = build_case(name)
+    g = golden(f"{name}.npz")
+    U, info = capi.solve(api_problem(c, capi), c["b"], dict(c["opts"], maxit=20))
+    assert U.dtype == np.complex64 and info["status"] == 0 and info["total_iters"] == 20
+    bar = max(1e-4, 2 * relerr(g["ref3_U_it20"], g["ref4_U_it20"]))
+    e = relerr(U, g["ref4_U_it20"])
+    print(name, "20 iterations: relerr vs complex<double> reference", e, "bar", bar)
+    assert e < bar, (name, e, bar)
+
+
+@pytest.mark.parametrize("name", COMPLEX_CASES)
 def test_complex_solve_matches_reference(name, torch_cuda):
+    """The full solve under the reference's stopping rules.  Where the inner
+    stopping test (relative change below tol_inn) is decided a few
+    iterations apart by FP32 rounding - the reference's own float build can
+    do the same - the solutions differ by those iterations' progress: the bar
+    is then 1e-2 and the counts stay within 5 % or within the spread of the
+    reference's own float and double builds."""
     c = build_case(name)
     g = golden(f"{name}.npz")
     U, info = capi.solve(api_problem(c, capi), c["b"], c["opts"], Ut=c["u_true"])
     assert U.dtype == np.complex64 and info["status"] == 0
     bar = max(1e-3, 2 * relerr(g["ref3_U"], g["ref4_U"]))
+    ref_iters = int(g["ref4_iters"][1])
+    if info["total_iters"] != ref_iters:   # within 5 %, or the reference's own float-vs-double spread
+        spread = max(0.05 * ref_iters, abs(int(g["ref3_iters"][1]) - ref_iters))
+        assert abs(info["total_iters"] - ref_iters) <= spread, (info["total_iters"], ref_iters, spread)
+        bar = max(bar, 1e-2)
     e = relerr(U, g["ref4_U"])
     print(name, "relerr vs complex<double> reference", e, "bar", bar, "iterations", info["total_iters"],
-          "reference", tuple(g["ref4_iters"]))
+          "reference", ref_iters)
     assert e < bar, (name, e, bar)
     assert abs(info["rel_error"] - relerr(U, c["u_true"])) < 1e-5
 
