@@ -59,6 +59,14 @@ extern "C" {
 #define TVAL3G_NO_TENSOR 8      /* dense operators with 16, 32, 48 or 64 layers
                                    use the FP64-accumulating gemv kernels instead
                                    of the tcgen05 3xTF32 tensor-core path */
+#define TVAL3G_TUNE 16          /* time each operator's launch-shape candidates
+                                   once (lanes per ray of the ray forward,
+                                   sub-warp width of the compressed gathers)
+                                   and keep the fastest; cached per operator
+                                   signature in memory and, if the environment
+                                   variable TVAL3G_TUNE_CACHE names a file, on
+                                   disk.  Results then equal the untuned ones
+                                   within rounding (other summation order). */
 
 /* Per inner iteration: step length, objective after update_W, relative
  * change, backtracking steps taken (6 = restart after five failures), whether
@@ -136,7 +144,7 @@ int tval3g_solve(const tval3g_problem *prob, const float *b, int b_len, const tv
                  const float *Ut, int ut_len, float *U, tval3g_info *info);
 
 /* count independent solves with host buffers, run as one batch (flags:
- * TVAL3G_GRAPH).  Arrays are indexed by problem; Ut may be NULL. */
+ * TVAL3G_GRAPH, TVAL3G_TUNE).  Arrays are indexed by problem; Ut may be NULL. */
 int tval3g_solve_batch(int count, const tval3g_problem *probs, const float *const *b,
                        const tval3g_options *opts, const float *const *Ut, float *const *U,
                        tval3g_info *info, int flags);
@@ -172,6 +180,10 @@ int tval3g_plan_destroy(tval3g_plan *plan);
  * reference (it allocates host memory per call). */
 int tval3g_trim_memory(long long keep_bytes);
 
+/* Autotuner (TVAL3G_TUNE): operators timed, and choices taken from the cache,
+ * in this process so far.  No counterpart in the reference. */
+int tval3g_tune_stats(long long *measured, long long *cached);
+
 /* Operators alone.  tval3g_op_apply: y = A x (trans = 0), y = A^T x
  * (trans = 1) or the normal product y = A^T (A x) of the solve's get_g_mult
  * (trans = 2; a one-layer dense operator reads A once, as the reference's
@@ -195,6 +207,11 @@ int tval3g_op_ray_csr(const tval3g_operator *op, long long *rowptr, int *colind)
  * positions and their offsets), 0 for a dense operator.  No counterpart in
  * the reference (its operators keep no derived index). */
 int tval3g_op_adjoint_index_bytes(const tval3g_operator *op, long long *bytes);
+/* The operator's launch shapes (tval3g_op_create with TVAL3G_TUNE): lanes per
+ * ray of the ray forward and 1 + the width class (4, 8, 16, 32 lanes per
+ * line) of the forward and adjoint gathers; 0 = the built-in choice.  No
+ * counterpart in the reference. */
+int tval3g_op_launch_shape(const tval3g_operator *op, int *fwd_lanes, int *gather_fwd, int *gather_adj);
 int tval3g_op_destroy(tval3g_operator *op);
 
 /* Stencils on DEVICE arrays of an image dim_y x dim_x (x dim_z for dims 3).

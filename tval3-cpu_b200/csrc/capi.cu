@@ -72,7 +72,7 @@ int tval3g_solve_batch(int count, const tval3g_problem *probs, const float *cons
 	auto t0 = std::chrono::steady_clock::now();
 	for (int i = 0; i < count; i++) validate(probs[i], b_len_of(probs[i]), 0);
 	need_device();
-	Plan plan(count, probs, opts, flags & TVAL3G_GRAPH);
+	Plan plan(count, probs, opts, flags & (TVAL3G_GRAPH | TVAL3G_TUNE));
 	std::vector<float *> db(count), du(count), dut(count, nullptr);
 	std::vector<long long> ns(count);
 	cudaStream_t s;
@@ -122,12 +122,27 @@ int tval3g_solve(const tval3g_problem *prob, const float *b, int b_len, const tv
                  const float *Ut, int ut_len, float *U, tval3g_info *info) {
 	CAPI_BEGIN
 	TG_ARG(prob && b && opts && U, "Argument error: NULL argument");
-	validate(*prob, b_len, Ut ? ut_len : 0);
+	validate(*prob, b_len, Ut ? ut_len : 0, false);   // tval3g_solve_batch checks the rays
 	const float *bb[1] = {b};
 	const float *uu[1] = {Ut && ut_len > 0 ? Ut : nullptr};
 	float *out[1] = {U};
 	int rc = tval3g_solve_batch(1, prob, bb, opts, uu, out, info, TVAL3G_GRAPH);
 	return rc;
+	CAPI_END
+}
+
+int tval3g_tune_stats(long long *measured, long long *cached) {
+	CAPI_BEGIN
+	autotune_stats(measured, cached);
+	CAPI_END
+}
+
+int tval3g_op_launch_shape(const tval3g_operator *op, int *fwd_lanes, int *gather_fwd, int *gather_adj) {
+	CAPI_BEGIN
+	TG_ARG(op, "Argument error: NULL operator");
+	if (fwd_lanes) *fwd_lanes = op->st.dev.fwd_lanes;
+	if (gather_fwd) *gather_fwd = op->st.dev.gcls_fwd;
+	if (gather_adj) *gather_adj = op->st.dev.gcls_adj;
 	CAPI_END
 }
 
@@ -215,6 +230,7 @@ int tval3g_op_create(tval3g_operator **out, const tval3g_problem *prob, int flag
 		I.n = (long long)p.dim_x * p.dim_y * I.r;
 		I.m = op->st.b_len;
 		I.cplx = p.complex_data != 0;
+		if (flags & TVAL3G_TUNE) autotune_operator(op->s, op->st, I);
 		I.op = op->st.dev;
 		op->rows = I.m;
 		op->cols = I.n;

@@ -156,6 +156,12 @@ struct OpDev {
 	// length tH = n / ld), in which their steps are contiguous; NULL = off
 	float *xT;
 	int tH;
+	// launch shapes chosen by the autotuner (tune.cu); 0 = the built-in
+	// choice: lanes per ray of the ray forward (4, 8 or 16), and 1 + the
+	// width class (4, 8, 16, 32 lanes per line) of the compressed gathers of
+	// the forward (CSR rows) and of the adjoint (CSC columns, 3D ray index)
+	int fwd_lanes;
+	int gcls_fwd, gcls_adj;
 };
 
 #ifndef TVAL3G_RAYT

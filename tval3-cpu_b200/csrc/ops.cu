@@ -1002,12 +1002,18 @@ void op_forward(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel
 	if (B.ray2_transpose.count > 0 && !xT_ready) {
 		launch_pdl(k_transpose2d, B.ray2_transpose.count, 256, 0, L.stream, L.inst, B.ray2_transpose, pred, x, ctr);
 	}
-	if (B.ray2_fwd.count > 0) {
-		launch_pdl(k_ray_fwd<RAY_SUBW, false>, B.ray2_fwd.count, 256, 0, L.stream, L.inst, B.ray2_fwd, pred, x, y, ctr);
-	}
-	if (B.ray3_fwd.count > 0) {
-		launch_pdl(k_ray_fwd<RAY_SUBW, true>, B.ray3_fwd.count, 256, 0, L.stream, L.inst, B.ray3_fwd, pred, x, y, ctr);
-	}
+	if (B.ray2_fwd[0].count > 0)
+		launch_pdl(k_ray_fwd<4, false>, B.ray2_fwd[0].count, 256, 0, L.stream, L.inst, B.ray2_fwd[0], pred, x, y, ctr);
+	if (B.ray2_fwd[1].count > 0)
+		launch_pdl(k_ray_fwd<8, false>, B.ray2_fwd[1].count, 256, 0, L.stream, L.inst, B.ray2_fwd[1], pred, x, y, ctr);
+	if (B.ray2_fwd[2].count > 0)
+		launch_pdl(k_ray_fwd<16, false>, B.ray2_fwd[2].count, 256, 0, L.stream, L.inst, B.ray2_fwd[2], pred, x, y, ctr);
+	if (B.ray3_fwd[0].count > 0)
+		launch_pdl(k_ray_fwd<4, true>, B.ray3_fwd[0].count, 256, 0, L.stream, L.inst, B.ray3_fwd[0], pred, x, y, ctr);
+	if (B.ray3_fwd[1].count > 0)
+		launch_pdl(k_ray_fwd<8, true>, B.ray3_fwd[1].count, 256, 0, L.stream, L.inst, B.ray3_fwd[1], pred, x, y, ctr);
+	if (B.ray3_fwd[2].count > 0)
+		launch_pdl(k_ray_fwd<16, true>, B.ray3_fwd[2].count, 256, 0, L.stream, L.inst, B.ray3_fwd[2], pred, x, y, ctr);
 }
 
 void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y, bool unfused) {

@@ -16,6 +16,7 @@ constexpr int WARPS = 8;   // warps per block in the operator kernels
 // rays; 2D rays of 100-400 hits and 3D rays of ~60 hits keep 8 lanes busy
 constexpr int RAY_SUBW = 8;
 constexpr int RAYS_PER_BLOCK = 256 / RAY_SUBW;
+constexpr int RAY_LANES[3] = {4, 8, 16};   // lanes-per-ray classes of the forward
 
 struct OpBatch {
 	// dense (2d/mat_mult.h:15-36): forward warp-per-row gemv; adjoint over
@@ -46,8 +47,9 @@ struct OpBatch {
 	// its mean line length (4, 8, 16 or 32 lanes per line: class 0..3), so its
 	// summation order does not depend on the other instances of a batch.
 	TileMap csr_fwd[4], csc_adj[4], ray_adj[4];
-	// rays: on-the-fly Bresenham, RAY_SUBW lanes per ray (2D and 3D)
-	TileMap ray2_fwd, ray3_fwd;
+	// rays: on-the-fly Bresenham, 4, 8 or 16 lanes per ray (class 0..2;
+	// RAY_SUBW = 8 unless the autotuner chose otherwise), 2D and 3D
+	TileMap ray2_fwd[3], ray3_fwd[3];
 	TileMap ray2_transpose;   // 32x32 tiles of the image, for 2D ray operators with xT
 	// tiled 2D ray adjoint: one block per RAYT x RAYT pixel tile; dynamic
 	// shared memory for the longest tile list of the batch

@@ -46,7 +46,7 @@ void dev_free(void *p, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // validation (2d/tval3_cpu_2d.cpp:696-750, 3d/tval3_cpu_3d.cpp:1028-1165)
 // ---------------------------------------------------------------------------
-long long validate(const tval3g_problem &p, long long b_len, long long ut_len) {
+long long validate(const tval3g_problem &p, long long b_len, long long ut_len, bool rays) {
 	TG_ARG(p.dims == 2 || p.dims == 3, "Argument error: dims must be 2 or 3");
 	TG_ARG(p.dim_x >= 1 && p.dim_y >= 1 && (p.dims == 2 || p.dim_z >= 1),
 	       "Argument error: image dimensions must be positive");
@@ -104,7 +104,7 @@ long long validate(const tval3g_problem &p, long long b_len, long long ut_len) {
 		TG_ARG(p.op_kind == TVAL3G_OP_RAY2D || p.layers == 1,
 		       "Argument error: complex data with more than one layer is not supported");
 	}
-	if (p.op_kind == TVAL3G_OP_RAY2D || p.op_kind == TVAL3G_OP_RAY3D) {
+	if (rays && (p.op_kind == TVAL3G_OP_RAY2D || p.op_kind == TVAL3G_OP_RAY3D)) {
 		// every traced ray must stay inside the image (Bresenham stays inside
 		// the bounding box of its endpoints); the reference does not check
 		const bool is3 = p.op_kind == TVAL3G_OP_RAY3D;
@@ -299,6 +299,8 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 	} else {
 		// traced rays in the reference's loop order (mp, emitter, receiver)
 		std::vector<int4> rays;
+		rays.reserve((size_t)((p.op_kind == TVAL3G_OP_RAY3D ? p.numMPs : 1) * (long long)p.num_emitters * p.num_receivers));
+		st.ray_out.reserve(rays.capacity());
 		const bool is3 = p.op_kind == TVAL3G_OP_RAY3D;
 		const int E = p.num_emitters, R = p.num_receivers, nmp = is3 ? p.numMPs : 1;
 		const long long mtot = is3 ? (long long)p.numPaths * p.numMPs : (long long)E * R;
@@ -483,22 +485,24 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 	}
 	// compressed gathers: each instance in the width class of its own mean
 	// line length (lines per block = 256 / width)
+	// (or in the class the autotuner measured fastest, OpDev::gcls_*)
 	static const int widths[4] = {4, 8, 16, 32};
-	auto cls = [](double avg) {
+	auto cls = [](double avg, int tuned) {
+		if (tuned > 0) return tuned - 1;
 		int w = subwarp_for(avg);
 		return w == 4 ? 0 : w == 8 ? 1 : w == 16 ? 2 : 3;
 	};
 	for (int c = 0; c < 4; c++) {
 		for (int i = 0; i < cnt; i++) {
 			const OpDev &d = inst[i].op;
-			if (d.kind != TVAL3G_OP_CSR || cls((double)ops[i].nnz / d.m) != c) continue;
+			if (d.kind != TVAL3G_OP_CSR || cls((double)ops[i].nnz / d.m, d.gcls_fwd) != c) continue;
 			long long lpb = 256 / widths[c];
 			tb.add(i, d.layers * ((d.m + lpb - 1) / lpb));
 		}
 		tb.close(&ob.csr_fwd[c]);
 		for (int i = 0; i < cnt; i++) {
 			const OpDev &d = inst[i].op;
-			if (d.kind != TVAL3G_OP_CSR || cls((double)ops[i].nnz / d.n) != c) continue;
+			if (d.kind != TVAL3G_OP_CSR || cls((double)ops[i].nnz / d.n, d.gcls_adj) != c) continue;
 			long long lpb = 256 / widths[c];
 			tb.add(i, d.layers * ((d.n + lpb - 1) / lpb));
 		}
@@ -506,25 +510,26 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 		for (int i = 0; i < cnt; i++) {
 			const OpDev &d = inst[i].op;
 			if ((d.kind != TVAL3G_OP_RAY2D && d.kind != TVAL3G_OP_RAY3D) || d.tiled ||
-			    cls((double)ops[i].nnz / inst[i].n) != c)
+			    cls((double)ops[i].nnz / inst[i].n, d.gcls_adj) != c)
 				continue;
 			long long lpb = 256 / widths[c];
 			tb.add(i, (inst[i].n + lpb - 1) / lpb);
 		}
 		tb.close(&ob.ray_adj[c]);
 	}
-	for (int i = 0; i < cnt; i++) {
-		const OpDev &d = inst[i].op;
-		if (d.kind != TVAL3G_OP_RAY2D) continue;
-		tb.add(i, (d.nrays + RAYS_PER_BLOCK - 1) / RAYS_PER_BLOCK);
-	}
-	tb.close(&ob.ray2_fwd);
-	for (int i = 0; i < cnt; i++) {
-		const OpDev &d = inst[i].op;
-		if (d.kind != TVAL3G_OP_RAY3D) continue;
-		tb.add(i, (d.nrays + RAYS_PER_BLOCK - 1) / RAYS_PER_BLOCK);
-	}
-	tb.close(&ob.ray3_fwd);
+	// ray forwards by lanes per ray (RAY_SUBW unless tuned)
+	for (int dim3 = 0; dim3 < 2; dim3++)
+		for (int c = 0; c < 3; c++) {
+			for (int i = 0; i < cnt; i++) {
+				const OpDev &d = inst[i].op;
+				if (d.kind != (dim3 ? TVAL3G_OP_RAY3D : TVAL3G_OP_RAY2D)) continue;
+				const int lanes = d.fwd_lanes > 0 ? d.fwd_lanes : RAY_SUBW;
+				if (lanes != RAY_LANES[c]) continue;
+				const int rpb = 256 / lanes;
+				tb.add(i, (d.nrays + rpb - 1) / rpb);
+			}
+			tb.close(dim3 ? &ob.ray3_fwd[c] : &ob.ray2_fwd[c]);
+		}
 	for (int i = 0; i < cnt; i++) {
 		const OpDev &d = inst[i].op;
 		if (d.kind != TVAL3G_OP_RAY2D || !d.xT) continue;
@@ -576,7 +581,7 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 			long long b_len = (p.op_kind == TVAL3G_OP_RAY2D) ? (long long)p.num_emitters * p.num_receivers
 			                  : (p.op_kind == TVAL3G_OP_RAY3D) ? (long long)p.numPaths * p.numMPs
 			                  : (long long)p.m * (p.dims == 3 ? 1 : p.layers);
-			long long n = validate(p, b_len, 0);
+			long long n = validate(p, b_len, 0, false);   // the callers validated p
 			prepare_op(stream_, p, flags, ops_[i], false);
 			Inst &I = h_inst_[i];
 			const int planes = p.complex_data ? 2 : 1;   // complex: real and imaginary planes
@@ -597,6 +602,7 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 			I.numInit = o.numInitIterations;
 			I.skip_enabled = (o.skipMulRatio != 0 && p.op_kind != TVAL3G_OP_DENSE);
 			any_skip_ |= I.skip_enabled != 0;
+			if (flags & TVAL3G_TUNE) autotune_operator(stream_, ops_[i], I);
 			I.op = ops_[i].dev;
 		}
 		// vectors: one arena, every vector 256-byte aligned

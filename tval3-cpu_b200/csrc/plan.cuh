@@ -25,12 +25,19 @@ struct OpStore {
 };
 
 // validate a problem against (b_len, ut_len) with the reference's messages;
-// returns n (image length)
-long long validate(const tval3g_problem &p, long long b_len, long long ut_len);
+// returns n (image length).  rays = false leaves out the per-ray endpoint
+// check, for callers that validated the same problem already (the operator
+// builder checks every endpoint again while it packs the rays)
+long long validate(const tval3g_problem &p, long long b_len, long long ut_len, bool rays = true);
 // prepare the device operator of a problem (flags: TVAL3G_DEVICE_INPUTS)
 void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st, bool keep_ray_csr);
 void free_op(OpStore &st, cudaStream_t s);
 void check_options(const tval3g_options &o);
+// TVAL3G_TUNE: time the operator's launch-shape candidates on its own data
+// (or take the cached choice of its signature) and store the fastest in
+// st.dev; shape gives the instance's image and vector sizes (tune.cu)
+void autotune_operator(cudaStream_t s, OpStore &st, const Inst &shape);
+void autotune_stats(long long *measured, long long *cached);
 // operator tile maps of a batch, uploaded to *d_tiles; returns the dense
 // partial-buffer size in floats
 long long build_op_maps_upload(std::vector<Inst> &inst, const std::vector<OpStore> &ops, OpBatch &ob,

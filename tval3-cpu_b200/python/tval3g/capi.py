@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(PKG, "lib", "libtval3g.so")
 OK, ERR_ARGUMENT, ERR_CUDA, ERR_NO_DEVICE, ERR_NONFINITE, ERR_INTERNAL = 0, -1, -2, -3, -4, -5
 OP_DENSE, OP_CSR, OP_RAY2D, OP_RAY3D = 0, 1, 2, 3
 TV_ANISO, TV_ISO = 0, 1
-DEVICE_INPUTS, GRAPH, TRACE, NO_TENSOR = 1, 2, 4, 8
+DEVICE_INPUTS, GRAPH, TRACE, NO_TENSOR, TUNE = 1, 2, 4, 8, 16
 
 _OPT_D = ("mu", "beta", "mu0", "beta0", "tol", "tol_inn", "c", "gamma", "gam", "rate_gam", "rate_cnt",
           "skipMulRatio", "maxRelativeChange")
@@ -87,6 +87,8 @@ def lib():
         L.tval3g_plan_set_target.argtypes = [vp, d]
         L.tval3g_plan_destroy.argtypes = [vp]
         L.tval3g_trim_memory.argtypes = [ll]
+        L.tval3g_tune_stats.argtypes = [C.POINTER(ll), C.POINTER(ll)]
+        L.tval3g_op_launch_shape.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         L.tval3g_op_create.argtypes = [C.POINTER(vp), P, i]
         L.tval3g_op_shape.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(ll)]
         L.tval3g_op_apply.argtypes = [vp, i, vp, vp, vp]
@@ -116,9 +118,18 @@ def trim_memory(keep_bytes=0):
     _check(lib().tval3g_trim_memory(int(keep_bytes)))
 
 
+def tune_stats():
+    """(operators timed, choices taken from the cache) of the autotuner in
+    this process (TVAL3G_TUNE)."""
+    m, c = C.c_longlong(), C.c_longlong()
+    _check(lib().tval3g_tune_stats(C.byref(m), C.byref(c)))
+    return m.value, c.value
+
+
 EXPORTS = ("tval3g_last_error", "tval3g_version", "tval3g_solve", "tval3g_solve_batch", "tval3g_plan_create",
            "tval3g_plan_solve", "tval3g_plan_stats", "tval3g_plan_trace", "tval3g_plan_set_target",
-           "tval3g_plan_destroy", "tval3g_trim_memory", "tval3g_op_create", "tval3g_op_shape",
+           "tval3g_plan_destroy", "tval3g_trim_memory", "tval3g_tune_stats", "tval3g_op_launch_shape",
+           "tval3g_op_create", "tval3g_op_shape",
            "tval3g_op_apply", "tval3g_op_apply_n", "tval3g_op_ray_csr", "tval3g_op_adjoint_index_bytes",
            "tval3g_op_destroy", "tval3g_D", "tval3g_Dt",
            "tval3g_shrink", "tval3g_unrolled_create", "tval3g_unrolled_forward", "tval3g_unrolled_backward",
@@ -248,7 +259,7 @@ def solve(spec: ProblemSpec, b, opts: dict, Ut=None):
     return U.reshape(spec.shape), info.as_dict()
 
 
-def solve_batch(specs, bs, opts_list, Uts=None, graph=True):
+def solve_batch(specs, bs, opts_list, Uts=None, graph=True, tune=False):
     n = len(specs)
     probs = (Problem * n)(*[s.p for s in specs])
     opts = (Options * n)(*[Options.from_dict(o) for o in opts_list])
@@ -260,7 +271,7 @@ def solve_batch(specs, bs, opts_list, Uts=None, graph=True):
     up = (C.c_void_p * n)(*[u.ctypes.data for u in uarr])
     utp = (C.c_void_p * n)(*[(u.ctypes.data if u is not None else None) for u in utarr])
     infos = (Info * n)()
-    _check(lib().tval3g_solve_batch(n, probs, bp, opts, utp, up, infos, GRAPH if graph else 0))
+    _check(lib().tval3g_solve_batch(n, probs, bp, opts, utp, up, infos, (GRAPH if graph else 0) | (TUNE if tune else 0)))
     return [u.reshape(s.shape) for u, s in zip(uarr, specs)], [i.as_dict() for i in infos]
 
 
@@ -276,7 +287,7 @@ class Plan:
     """Device-resident solver state for a batch of problems (graph=True: the
     iteration loop is one CUDA graph with conditional nodes)."""
 
-    def __init__(self, specs, opts_list, graph=True, device_inputs=False, trace=False, tensor=True):
+    def __init__(self, specs, opts_list, graph=True, device_inputs=False, trace=False, tensor=True, tune=False):
         n = len(specs)
         self.specs = specs
         self.count = n
@@ -285,7 +296,7 @@ class Plan:
         opts = (Options * n)(*[Options.from_dict(o) for o in opts_list])
         h = C.c_void_p()
         flags = (GRAPH if graph else 0) | (DEVICE_INPUTS if device_inputs else 0) | (TRACE if trace else 0) | \
-            (0 if tensor else NO_TENSOR)
+            (0 if tensor else NO_TENSOR) | (TUNE if tune else 0)
         _check(lib().tval3g_plan_create(C.byref(h), n, probs, opts, flags))
         self.h = h
 
@@ -330,9 +341,9 @@ class Plan:
 class Operator:
     """A measurement operator on the device: apply(x, trans) with torch tensors."""
 
-    def __init__(self, spec: ProblemSpec, tensor=True, device_inputs=False):
+    def __init__(self, spec: ProblemSpec, tensor=True, device_inputs=False, tune=False):
         h = C.c_void_p()
-        flags = (0 if tensor else NO_TENSOR) | (DEVICE_INPUTS if device_inputs else 0)
+        flags = (0 if tensor else NO_TENSOR) | (DEVICE_INPUTS if device_inputs else 0) | (TUNE if tune else 0)
         _check(lib().tval3g_op_create(C.byref(h), C.byref(spec.p), flags))
         self.h = h
         r, c, z = C.c_longlong(), C.c_longlong(), C.c_longlong()
@@ -345,6 +356,13 @@ class Operator:
     def apply(self, x, y, trans=False, stream=None):
         _check(lib().tval3g_op_apply(self.h, int(trans), _dptr(x), _dptr(y), _dptr(stream)))
         return y
+
+    def launch_shape(self):
+        """(lanes per ray of the ray forward, 1 + gather width class of the
+        forward, of the adjoint); 0 = the built-in choice."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().tval3g_op_launch_shape(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
 
     def apply_n(self, x, y, reps, trans=False, stream=None):
         """Enqueue `reps` back-to-back applications on `stream`; no wait."""
