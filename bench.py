@@ -57,6 +57,8 @@ def args_():
     p.add_argument("--profile", action="store_true",
                    help="for ncu: build the plan, run --warmup + --steps solves, print nothing else")
     p.add_argument("--maxit", type=int, default=None, help="override maxit (profiling a short solve)")
+    p.add_argument("--tune", action="store_true",
+                   help="single-instance workloads: operators built with the launch-shape autotuner")
     p.add_argument("--plain", action="store_true",
                    help="with --profile: run the host-driven loop (same kernels, same order) instead of the "
                         "CUDA graph, whose conditional nodes ncu cannot profile kernel by kernel")
@@ -298,6 +300,16 @@ def kernel_roofline(cx, capi, spec, w, kind):
             "timing": "one launch per CUDA-event pair, 256 MB L2 flush before each"}
 
 
+def launch_shape(capi, spec):
+    """The autotuner's choice for spec's operator (from its cache, filled by
+    the plan): lanes per ray of the ray forward, forward / adjoint gather
+    width classes (0 = built-in)."""
+    op = capi.Operator(spec, tune=True)
+    s = op.launch_shape()
+    op.close()
+    return {"forward_lanes_per_ray": s[0], "forward_gather_class": s[1], "adjoint_gather_class": s[2]}
+
+
 def run_single(a, cx, capi, name, world, rank, dist, clocks):
     torch, dev, stream = cx.torch, cx.dev, cx.stream
     fwd3d = None
@@ -332,7 +344,7 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
     target = 1e-3 if ref is not None else 0.0
     uts = [d_ref] if d_ref is not None else None
 
-    plan = capi.Plan([spec], [opts], graph=not (a.profile and a.plain), trace=True)
+    plan = capi.Plan([spec], [opts], graph=not (a.profile and a.plain), trace=True, tune=a.tune)
     plan.set_target(target)
     solve = lambda p: p.solve([d_b], [d_U], d_Ut=uts, stream=stream.cuda_stream)  # noqa: E731
     if a.profile:
@@ -362,7 +374,7 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
     full_t, full_info = cx.event_time(lambda: solve(plan), 2)
     plan.close()
 
-    plan_plain = capi.Plan([spec], [opts], graph=False)   # host-driven loop, same kernels
+    plan_plain = capi.Plan([spec], [opts], graph=False, tune=a.tune)   # host-driven loop, same kernels
     plan_plain.set_target(target)
     cx.event_time(lambda: solve(plan_plain), 1)
     pt, _ = cx.event_time(lambda: solve(plan_plain), 2)
@@ -371,7 +383,11 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
     et, ec = [], []   # end to end through the host-buffer C ABI (two untimed calls first)
     for k in range(max(1, min(a.steps, 3)) + 2):
         t0 = time.perf_counter()
-        _, e_info = capi.solve(spec, b_host, opts)
+        if a.tune:   # the batch entry point takes the flags (one instance)
+            _, e_infos = capi.solve_batch([spec], [b_host], [opts], tune=True)
+            e_info = e_infos[0]
+        else:
+            _, e_info = capi.solve(spec, b_host, opts)
         if k > 1:
             et.append((time.perf_counter() - t0) * 1000)
             ec.append(e_info["secs"] * 1000)
@@ -381,7 +397,8 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
     line = {"metric": METRIC, "value": world * 1000.0 / ms, "unit": "reconstructions/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom and operator, Gaussian noise)",
-            "config": dict(CONFIGS[name], instances=1, l2="256 MB write between timed solves"),
+            "config": dict(CONFIGS[name], instances=1, l2="256 MB write between timed solves",
+                           launch_shape=launch_shape(capi, spec) if a.tune else "built-in"),
             "iterations": iters, "time_to_solution_ms": ms, "relerr_vs_fp64": relerr,
             "reached_target": bool(relerr is not None and relerr <= target), "target": target,
             "relerr_curve_every_5": [round(float(x), 6) for x in curve[::5]],

@@ -68,16 +68,27 @@ void store_cache(const std::string &key, const Choice &c) {
 	if (f) f << key << '\t' << c.fwd_lanes << ' ' << c.gcls_fwd << ' ' << c.gcls_adj << '\n';
 }
 
-std::string signature(const OpStore &st, long long rows, long long cols) {
+// the device part of a signature, looked up once per device
+std::string device_tag() {
+	static std::mutex mu;
+	static std::map<int, std::string> tags;
 	int dev = 0;
 	TG_CUDA(cudaGetDevice(&dev));
+	std::lock_guard<std::mutex> lock(mu);
+	auto it = tags.find(dev);
+	if (it != tags.end()) return it->second;
 	cudaDeviceProp prop;
 	TG_CUDA(cudaGetDeviceProperties(&prop, dev));
+	std::ostringstream k;
+	k << "sm=" << prop.multiProcessorCount << " dev=" << prop.name;
+	return tags[dev] = k.str();
+}
+
+std::string signature(const OpStore &st, long long rows, long long cols) {
 	const OpDev &d = st.dev;
 	std::ostringstream k;
 	k << "v1 kind=" << d.kind << " rows=" << rows << " cols=" << cols << " layers=" << d.layers
-	  << " nnz=" << st.nnz << " rays=" << d.nrays << " tiled=" << d.tiled << " sm=" << prop.multiProcessorCount
-	  << " dev=" << prop.name;
+	  << " nnz=" << st.nnz << " rays=" << d.nrays << " tiled=" << d.tiled << " " << device_tag();
 	std::string s = k.str();
 	for (char &ch : s)
 		if (ch == '\t' || ch == '\n') ch = ' ';
