@@ -16,7 +16,7 @@ from tval3g import workloads as W
 CASES = [
     "dense2d_s32_it20", "dense2d_s32_conv", "dense2d_layers", "ring2d_s64_it20", "ring2d_s64_conv",
     "ring2d_s64_iso", "ring2d_s64_nonneg", "ring2d_s64_skip", "hemi3d_s16_it20", "hemi3d_s16_conv",
-    "csr3d_s16", "dense3d_s8",
+    "csr3d_s16", "dense3d_s8", "hemi3d_mp2_s16", "csr2d_layers",
 ]
 # complex data (the reference's complex<float> / complex<double> overloads):
 # the FP64 anchor is the reference's own complex<double> build
@@ -106,6 +106,42 @@ def build_case(name):
         c.update(shape=(s, s, s), A=A, b=b, u_true=u, ref_kind="dense", api="dense", layers=1,
                  opts=W.options(2 ** 8, 2 ** 5, 1e-4, 40, tv_norm=0))
         c["oracle_op"] = O.Op.dense(A.astype(np.float64))
+    elif name == "hemi3d_mp2_s16":
+        # two measurement positions (numMPs = 2, 3d/mat_mult.h:183): the same
+        # hemisphere, and the hemisphere turned a quarter about z
+        w = W.hemi3d(seed=2, side=16, T=64, receivers=16, maxit=20, tol=1e-5, csr=True)
+        g = dict(w["geom"])
+        s_ = 15
+        for a, b_ in (("xe", "ye"), ("xr", "yr")):
+            x, y = g[a], g[b_]
+            g[a] = np.concatenate([x, s_ - y]).astype(np.int32)
+            g[b_] = np.concatenate([y, x]).astype(np.int32)
+        for a in ("ze", "zr"):
+            g[a] = np.concatenate([g[a], g[a]]).astype(np.int32)
+        g["numMPs"] = 2
+        rng = np.random.default_rng(21)
+        A = W.ray3d_csr(g)
+        b = W.add_noise(W.csr_matvec(A, w["u_true"].ravel()), 0.005, rng).astype(np.float32)
+        c.update(shape=w["shape"], b=b, u_true=w["u_true"], opts=w["opts"], geom=g, csr=A, csr_tuple=_csr_tuple(A),
+                 layers=1, ref_kind="ray3d", api="ray3d")
+        c["oracle_op"] = O.Op.ray3d(g)
+    elif name == "csr2d_layers":
+        # 2D sparse operator with three layers (the reference's cscmm path,
+        # 2d/mat_mult.h:68-90)
+        rng = np.random.default_rng(6)
+        side, layers, k = 16, 3, 24
+        n = side * side
+        m = int(0.4 * n)
+        colind = np.concatenate([np.sort(rng.choice(n, k, replace=False)) for _ in range(m)]).astype(np.int32)
+        rowptr = (np.arange(m + 1) * k).astype(np.int32)
+        val = (rng.standard_normal(m * k) / math.sqrt(k)).astype(np.float32)
+        csr = {"m": m, "n": n, "rowptr": rowptr, "colind": colind, "val": val}
+        us = [W.ellipse_phantom(side, side, rng, 3, 0.0, lambda r: r.uniform(0.2, 1.0), (2, 6)) for _ in range(layers)]
+        b = np.concatenate([W.add_noise(W.csr_matvec(csr, u.ravel()), 0.01, rng) for u in us]).astype(np.float32)
+        u_true = np.concatenate([u.ravel() for u in us]).reshape(side * layers, side)
+        c.update(shape=(side * layers, side), b=b, u_true=u_true, csr=csr, csr_tuple=_csr_tuple(csr),
+                 ref_kind="csr", api="csr", layers=layers, opts=W.options(2 ** 8, 2 ** 5, 1e-4, 30, tv_norm=0))
+        c["oracle_op"] = O.Op.csr(m, n, rowptr, colind, val, layers=layers)
     elif name == "cdense2d_s32":
         rng = np.random.default_rng(11)
         side = 32

@@ -14,7 +14,7 @@ from tval3g import capi, workloads as W
 pytestmark = pytest.mark.gpu
 
 OP_CASES = ["dense2d_s32_it20", "dense2d_layers", "ring2d_s64_it20", "ring2d_s64_skip", "hemi3d_s16_it20",
-            "csr3d_s16", "dense3d_s8"]
+            "csr3d_s16", "dense3d_s8", "hemi3d_mp2_s16", "csr2d_layers"]
 
 
 def _dev(torch, a):
