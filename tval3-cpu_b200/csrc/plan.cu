@@ -367,10 +367,21 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 				st.adj_index_bytes = ib;
 			}
 		}
-		if (!d.tiled) st.adj_index_bytes = (long long)sizeof(int) * (n + 1 + total);   // pixel-major gather
-		if (total > 0) k_map_out<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, drays, cind);
-		TG_CUDA(cudaGetLastError());
-		d.cptr = cptr; d.cind = cind; d.cval = nullptr;
+		if (!d.tiled) {   // pixel-major gather over measurement indices
+			st.adj_index_bytes = (long long)sizeof(int) * (n + 1 + total);
+			if (total > 0) k_map_out<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, drays, cind);
+			TG_CUDA(cudaGetLastError());
+			d.cptr = cptr; d.cind = cind;
+		} else {          // the tiled index replaces the pixel-major one
+			for (void *&q : st.owned)
+				if (q == cptr || q == cind) {
+					st.bytes -= q == cptr ? (long long)sizeof(int) * (n + 1) : (long long)sizeof(int) * std::max(total, 1LL);
+					dev_free(q, s);
+					q = nullptr;
+				}
+			d.cptr = nullptr; d.cind = nullptr;
+		}
+		d.cval = nullptr;
 		st.ray_rptr = rptr; st.ray_rind = rind;
 		st.b_len = mtot;
 		if (!keep_ray_csr) {
