@@ -8,9 +8,10 @@
  * changes.  Each forwards to tval3g_solve (include/tval3g.h).
  *
  * Differences from the reference:
- *   - float data (mat<float>, with tval3_options<float> or <double>) runs on
- *     the GPU; double and complex data throw tval3_exception("Internal error:
- *     ...") - those overloads are part of the interface but not yet built;
+ *   - float data (mat<float>, with tval3_options<float> or <double>) and
+ *     complex<float> data run on the GPU; double and complex<double> data
+ *     run through float / complex<float> copies (FP32 storage with FP64
+ *     reductions: float accuracy, not double); 2D complex data takes one layer;
  *   - submat_mb and virtual_procs_per_core are accepted and ignored (they
  *     tune the reference's CPU cache blocking and thread count);
  *   - the 2D ray geometry works (the reference's projector body is commented

@@ -282,7 +282,7 @@ def ref_solve(kind: str, shape, b, opts: dict, dtype: int = 0, A=None, csr=None,
     kind: 'dense' (A: m x n), 'csr' (csr=(m, n, rowptr, colind, val)) or 'ray3d'
     (geom dict).  dtype 0 = float/float opts, 1 = float/double opts, 2 = double,
     3 = complex<float>/float opts, 4 = complex<double>/double opts (2D dense
-    and CSR).
+    and CSR, 3D dense, CSR and rays).
     formats = (U, A, Ut) mat_format codes (0 row major, 1 col major); default is
     what the reference requires for the operator kind (2d:700-702,719,739;
     3d:1038-1039,1086-1087,1140-1141).  Raises ReferenceError with the

@@ -7,7 +7,8 @@
  * dtype: 0 = float data + tval3_options<float>, 1 = float data +
  *        tval3_options<double>, 2 = double data + tval3_options<double>,
  *        3 = complex<float> data + tval3_options<float>, 4 = complex<double>
- *        data + tval3_options<double> (2D dense and CSR).
+ *        data + tval3_options<double> (2D dense and CSR; 3D dense, CSR
+ *        and geometry).
  * Returns 0, or 1 with the exception's message in err (the reference throws
  * tval3_exception, 2d/tval3_cpu_2d.cpp:878-884).
  */

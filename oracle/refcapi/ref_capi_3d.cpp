@@ -5,6 +5,7 @@
  * The reference prints "count_outer = ..." to stdout and writes profile.txt to
  * the current directory on every call (3d/tval3_cpu_3d.cpp:1228,1328-1349).
  */
+#include <complex>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -24,6 +25,14 @@ DECL(double, double, sparse_mat<double>)
 DECL(float, float, geometry)
 DECL(float, double, geometry)
 DECL(double, double, geometry)
+typedef std::complex<float> cf;
+typedef std::complex<double> cd;
+DECL(cf, float, mat<cf>)
+DECL(cd, double, mat<cd>)
+DECL(cf, float, sparse_mat<cf>)
+DECL(cd, double, sparse_mat<cd>)
+DECL(cf, float, geometry)
+DECL(cd, double, geometry)
 #undef DECL
 
 template <class T, class S, class OP>
@@ -65,6 +74,16 @@ extern "C" {
 int ref3d_dense(int dtype, void *U, int dim_y, int dim_x, int dim_z, int ufmt, const void *A_, int m, int n,
                 int afmt, const void *b, int blen, const ref_opts *o, const void *Ut, int utlen, int utfmt,
                 int submat_mb, int vppc, ref_info *info, char *err, int errlen) {
+	if (dtype == 3 || dtype == 4) {   // complex<float> / complex<double> data
+		if (dtype == 3) {
+			mat<cf> A(m, n, (mat_format)afmt);
+			fill(A, A_);
+			return run<cf, float>(U, dim_y, dim_x, dim_z, ufmt, A, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
+		}
+		mat<cd> A(m, n, (mat_format)afmt);
+		fill(A, A_);
+		return run<cd, double>(U, dim_y, dim_x, dim_z, ufmt, A, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
+	}
 	if (dtype == 2) {
 		mat<double> A(m, n, (mat_format)afmt);
 		fill(A, A_);
@@ -81,6 +100,16 @@ int ref3d_csr(int dtype, void *U, int dim_y, int dim_x, int dim_z, int ufmt, int
               const int *rptr, const int *rind, const void *rval, const int *cptr, const int *cind,
               const void *cval, const void *b, int blen, const ref_opts *o, const void *Ut, int utlen,
               int utfmt, int submat_mb, int vppc, ref_info *info, char *err, int errlen) {
+	if (dtype == 3) {
+		sparse_mat<cf> A(m, n, nnz, (sparse_mat_format)afmt);
+		fill_sparse(A, rptr, rind, rval, cptr, cind, cval);
+		return run<cf, float>(U, dim_y, dim_x, dim_z, ufmt, A, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
+	}
+	if (dtype == 4) {
+		sparse_mat<cd> A(m, n, nnz, (sparse_mat_format)afmt);
+		fill_sparse(A, rptr, rind, rval, cptr, cind, cval);
+		return run<cd, double>(U, dim_y, dim_x, dim_z, ufmt, A, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
+	}
 	if (dtype == 2) {
 		sparse_mat<double> A(m, n, nnz, (sparse_mat_format)afmt);
 		fill_sparse(A, rptr, rind, rval, cptr, cind, cval);
@@ -114,6 +143,10 @@ int ref3d_ray(int dtype, void *U, int dim_y, int dim_x, int dim_z, int ufmt, int
 		return run<float, float>(U, dim_y, dim_x, dim_z, ufmt, g, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
 	if (dtype == 1)
 		return run<float, double>(U, dim_y, dim_x, dim_z, ufmt, g, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
+	if (dtype == 3)
+		return run<cf, float>(U, dim_y, dim_x, dim_z, ufmt, g, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
+	if (dtype == 4)
+		return run<cd, double>(U, dim_y, dim_x, dim_z, ufmt, g, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
 	return run<double, double>(U, dim_y, dim_x, dim_z, ufmt, g, b, blen, o, Ut, utlen, utfmt, submat_mb, vppc, info, err, errlen);
 }
 

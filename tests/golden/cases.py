@@ -20,7 +20,7 @@ CASES = [
 ]
 # complex data (the reference's complex<float> / complex<double> overloads):
 # the FP64 anchor is the reference's own complex<double> build
-COMPLEX_CASES = ["cdense2d_s32", "ccsr2d_s32", "cring2d_s64"]
+COMPLEX_CASES = ["cdense2d_s32", "ccsr2d_s32", "cring2d_s64", "cdense3d_s8", "chemi3d_s16"]
 
 
 def _complex_phantom(side, rng):
@@ -166,6 +166,29 @@ def build_case(name):
         b = _complex_noise(_csr_apply(csr, u.ravel()), 0.01, rng).astype(np.complex64)
         c.update(shape=(side, side), b=b, u_true=u.astype(np.complex64), csr=csr, csr_tuple=_csr_tuple(csr),
                  ref_kind="csr", api="csr", layers=1, opts=W.options(2 ** 8, 2 ** 5, 1e-4, 300, tv_norm=0))
+    elif name == "cdense3d_s8":
+        rng = np.random.default_rng(14)
+        sd = 8
+        n = sd ** 3
+        m = int(0.4 * n)
+        ur = W.ellipsoid_phantom(sd, rng, 3, 0.0, lambda r: r.uniform(0.2, 1.0), (1.5, 3.5))
+        ui = W.ellipsoid_phantom(sd, rng, 2, 0.0, lambda r: r.uniform(-0.6, 0.6), (1.5, 3.5))
+        u = ur + 1j * ui
+        A = ((rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))) / math.sqrt(2 * m)).astype(np.complex64)
+        b = _complex_noise(A.astype(np.complex128) @ u.ravel(), 0.01, rng).astype(np.complex64)
+        c.update(shape=(sd, sd, sd), A=A, b=b, u_true=u.astype(np.complex64), ref_kind="dense", api="dense",
+                 layers=1, opts=W.options(2 ** 8, 2 ** 5, 1e-4, 200, tv_norm=0))
+    elif name == "chemi3d_s16":
+        # complex data on the 3D hemisphere geometry (the reference runs its
+        # own 3D projector on complex vectors)
+        w = W.hemi3d(seed=15, side=16, T=64, receivers=16, maxit=200, tol=1e-5, csr=True)
+        rng = np.random.default_rng(15)
+        u = w["u_true"] * np.exp(1j * np.linspace(0, 1.5, w["u_true"].size)).reshape(w["u_true"].shape)
+        csr = dict(w["csr"])
+        csr["val"] = csr["val"].astype(np.complex64)
+        b = _complex_noise(_csr_apply(csr, u.ravel()), 0.005, rng).astype(np.complex64)
+        c.update(shape=w["shape"], b=b, u_true=u.astype(np.complex64), opts=w["opts"], geom=w["geom"], csr=csr,
+                 ref_kind="ray3d", api="ray3d_complex", layers=1)
     elif name == "cring2d_s64":
         w = W.ring2d(seed=13, side=64, T=64, tv_norm=0, maxit=300, tol=1e-5)
         rng = np.random.default_rng(13)
@@ -191,4 +214,6 @@ def api_problem(c, capi):
         return capi.ray2d_problem(c["shape"], c["geom"])
     if c["api"] == "ray2d_complex":
         return capi.ray2d_problem(c["shape"], c["geom"], complex_data=True)
+    if c["api"] == "ray3d_complex":
+        return capi.ray3d_problem(c["shape"], c["geom"], complex_data=True)
     return capi.ray3d_problem(c["shape"], c["geom"])

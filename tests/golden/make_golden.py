@@ -46,14 +46,14 @@ def complex_case(name, tmp):
     try:
         for dtype in (3, 4):
             rr = O.ref_solve(c["ref_kind"], c["shape"], c["b"], c["opts"], dtype=dtype, A=c.get("A"),
-                             csr=c.get("csr_tuple"), Ut=c["u_true"])
+                             csr=c.get("csr_tuple"), geom=c.get("geom"), Ut=c["u_true"])
             out[f"ref{dtype}_U"] = rr.U.astype(np.complex128)
             out[f"ref{dtype}_iters"] = np.array([rr.outer_iters, rr.total_iters])
             out[f"ref{dtype}_relerr"] = np.array([rr.rel_error, rr.rel_chg])
         o20 = dict(c["opts"], maxit=20)   # a fixed count: no stopping decision involved
         for dtype in (3, 4):
             rr = O.ref_solve(c["ref_kind"], c["shape"], c["b"], o20, dtype=dtype, A=c.get("A"),
-                             csr=c.get("csr_tuple"), Ut=c["u_true"])
+                             csr=c.get("csr_tuple"), geom=c.get("geom"), Ut=c["u_true"])
             out[f"ref{dtype}_U_it20"] = rr.U.astype(np.complex128)
     finally:
         os.chdir(cwd)

@@ -127,10 +127,6 @@ inline void widen(const mat<std::complex<float> > &f, mat<std::complex<double> >
 	for (int i = 0; i < a.len && i < f.len; i++) a[i] = std::complex<double>(f[i].real(), f[i].imag());
 }
 
-inline void unsupported(const char *what) {
-	throw tval3_exception(std::string("Internal error: ") + what +
-	                      " data is not supported by the GPU build (float data is)");
-}
 
 }  // namespace tval3g_dropin
 

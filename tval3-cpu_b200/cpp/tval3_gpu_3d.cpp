@@ -12,9 +12,11 @@ using namespace tval3g_dropin;
 
 namespace {
 
-template <class S>
-tval3_info<S> dense3d(mat<float> &U, const mat<float> &A, const mat<float> &b, const tval3_options<S> &opts,
-                      const mat<float> &Ut) {
+template <class T> struct is_cplx { static const int value = 0; };
+template <class T> struct is_cplx<std::complex<T> > { static const int value = 1; };
+
+template <class S, class T>
+tval3_info<S> dense3d(mat<T> &U, const mat<T> &A, const mat<T> &b, const tval3_options<S> &opts, const mat<T> &Ut) {
 	if (U.format != mat_row_major || Ut.format != mat_row_major || A.format != mat_row_major)
 		throw tval3_exception(std::string("Argument error: Matrices must be in row major format!"));
 	tval3g_problem p = empty_problem();
@@ -22,13 +24,14 @@ tval3_info<S> dense3d(mat<float> &U, const mat<float> &A, const mat<float> &b, c
 	p.op_kind = TVAL3G_OP_DENSE;
 	p.m = A.dim_y;
 	p.n_cols = A.dim_x;
-	p.A = A.data();
+	p.A = fdata(A);
+	p.complex_data = is_cplx<T>::value;
 	return solve<S>(p, U, b, opts, Ut);
 }
 
-template <class S>
-tval3_info<S> sparse3d(mat<float> &U, const sparse_mat<float> &A, const mat<float> &b, const tval3_options<S> &opts,
-                       const mat<float> &Ut) {
+template <class S, class T>
+tval3_info<S> sparse3d(mat<T> &U, const sparse_mat<T> &A, const mat<T> &b, const tval3_options<S> &opts,
+                       const mat<T> &Ut) {
 	if (U.format != mat_col_major || Ut.format != mat_col_major)
 		throw tval3_exception(std::string("Argument error: Matrices must be in row major format!"));
 	if (A.format != sparse_mat_both)
@@ -41,13 +44,13 @@ tval3_info<S> sparse3d(mat<float> &U, const sparse_mat<float> &A, const mat<floa
 	p.nnz = A.nnz;
 	p.csr_ptr = A.csr_ptr();
 	p.csr_ind = A.csr_ind();
-	p.csr_val = A.csr_val();
+	p.csr_val = reinterpret_cast<const float *>(A.csr_val());
+	p.complex_data = is_cplx<T>::value;
 	return solve<S>(p, U, b, opts, Ut);
 }
 
-template <class S>
-tval3_info<S> ray3d(mat<float> &U, const geometry &A, const mat<float> &b, const tval3_options<S> &opts,
-                    const mat<float> &Ut) {
+template <class S, class T>
+tval3_info<S> ray3d(mat<T> &U, const geometry &A, const mat<T> &b, const tval3_options<S> &opts, const mat<T> &Ut) {
 	if (U.format != mat_row_major || Ut.format != mat_row_major)
 		throw tval3_exception(std::string("Argument error: Matrices must be in row major format!"));
 	// per-measurement-position coordinate arrays, flattened [mp*E + e]
@@ -78,17 +81,11 @@ tval3_info<S> ray3d(mat<float> &U, const geometry &A, const mat<float> &b, const
 	p.x_receivers = xr.data(); p.y_receivers = yr.data(); p.z_receivers = zr.data();
 	p.rv_x = A.rv_x; p.rv_y = A.rv_y; p.rv_z = A.rv_z;
 	p.scale_factor = A.scale_factor;
+	p.complex_data = is_cplx<T>::value;
 	return solve<S>(p, U, b, opts, Ut);
 }
 
 }  // namespace
-
-#define UNSUPPORTED_3D(Ttype, Stype, OP, what)                                                                  \
-	const tval3_info<Stype> tval3_cpu_3d(mat<Ttype> &, const OP &, const mat<Ttype> &,                         \
-	                                     const tval3_options<Stype> &, const mat<Ttype> &, int, int) {         \
-		unsupported(what);                                                                                       \
-		return tval3_info<Stype>();                                                                              \
-	}
 
 typedef std::complex<float> cf;
 typedef std::complex<double> cd;
@@ -109,8 +106,18 @@ const tval3_info<double> tval3_cpu_3d(mat<double> &U, const mat<double> &A, cons
 	widen(Uf, U);
 	return r;
 }
-UNSUPPORTED_3D(cf, float, mat<cf>, "complex")
-UNSUPPORTED_3D(cd, double, mat<cd>, "complex")
+const tval3_info<float> tval3_cpu_3d(mat<cf> &U, const mat<cf> &A, const mat<cf> &b,
+                                     const tval3_options<float> &opts, const mat<cf> &Ut, int, int) {
+	return dense3d<float>(U, A, b, opts, Ut);
+}
+const tval3_info<double> tval3_cpu_3d(mat<cd> &U, const mat<cd> &A, const mat<cd> &b,
+                                      const tval3_options<double> &opts, const mat<cd> &Ut, int, int) {
+	mat<cf> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
+	mat<cf> Af = narrow(A);
+	const tval3_info<double> r = dense3d<double>(Uf, Af, bf, opts, Utf);
+	widen(Uf, U);
+	return r;
+}
 
 const tval3_info<float> tval3_cpu_3d(mat<float> &U, const sparse_mat<float> &A, const mat<float> &b,
                                      const tval3_options<float> &opts, const mat<float> &Ut, int, int) {
@@ -129,8 +136,19 @@ const tval3_info<double> tval3_cpu_3d(mat<double> &U, const sparse_mat<double> &
 	widen(Uf, U);
 	return r;
 }
-UNSUPPORTED_3D(cf, float, sparse_mat<cf>, "complex")
-UNSUPPORTED_3D(cd, double, sparse_mat<cd>, "complex")
+const tval3_info<float> tval3_cpu_3d(mat<cf> &U, const sparse_mat<cf> &A, const mat<cf> &b,
+                                     const tval3_options<float> &opts, const mat<cf> &Ut, int, int) {
+	return sparse3d<float>(U, A, b, opts, Ut);
+}
+const tval3_info<double> tval3_cpu_3d(mat<cd> &U, const sparse_mat<cd> &A, const mat<cd> &b,
+                                      const tval3_options<double> &opts, const mat<cd> &Ut, int, int) {
+	mat<cf> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
+	sparse_mat<cf> Af(A.dim_y, A.dim_x, A.nnz, A.format);
+	narrow(A, Af);
+	const tval3_info<double> r = sparse3d<double>(Uf, Af, bf, opts, Utf);
+	widen(Uf, U);
+	return r;
+}
 
 const tval3_info<float> tval3_cpu_3d(mat<float> &U, const geometry &A, const mat<float> &b,
                                      const tval3_options<float> &opts, const mat<float> &Ut, int, int) {
@@ -147,5 +165,14 @@ const tval3_info<double> tval3_cpu_3d(mat<double> &U, const geometry &A, const m
 	widen(Uf, U);
 	return r;
 }
-UNSUPPORTED_3D(cf, float, geometry, "complex")
-UNSUPPORTED_3D(cd, double, geometry, "complex")
+const tval3_info<float> tval3_cpu_3d(mat<cf> &U, const geometry &A, const mat<cf> &b,
+                                     const tval3_options<float> &opts, const mat<cf> &Ut, int, int) {
+	return ray3d<float>(U, A, b, opts, Ut);
+}
+const tval3_info<double> tval3_cpu_3d(mat<cd> &U, const geometry &A, const mat<cd> &b,
+                                      const tval3_options<double> &opts, const mat<cd> &Ut, int, int) {
+	mat<cf> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
+	const tval3_info<double> r = ray3d<double>(Uf, A, bf, opts, Utf);
+	widen(Uf, U);
+	return r;
+}

@@ -227,7 +227,7 @@ int tval3g_op_create(tval3g_operator **out, const tval3g_problem *prob, int flag
 		Inst &I = op->h;
 		const int planes = p.complex_data ? 2 : 1;   // complex: the real form on planar vectors
 		I.dims = p.dims; I.p = p.dim_y; I.q = p.dim_x; I.r = p.dims == 3 ? p.dim_z : planes;
-		I.n = (long long)p.dim_x * p.dim_y * I.r;
+		I.n = (long long)p.dim_x * p.dim_y * (p.dims == 3 ? p.dim_z : 1) * planes;
 		I.m = op->st.b_len;
 		I.cplx = p.complex_data != 0;
 		if (flags & TVAL3G_TUNE) autotune_operator(op->s, op->st, I);

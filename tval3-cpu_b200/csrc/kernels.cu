@@ -55,6 +55,7 @@ struct Geo {
 		const unsigned zz = fp.div(row);
 		z = (int)zz;
 		y = (int)row - (int)zz * p;
+		if (z >= r) z -= r;   // complex data: the imaginary plane repeats the real plane's z
 	}
 };
 
@@ -155,7 +156,11 @@ struct Shrink {
 			float t = ab - thr;
 			t = t >= 0.f ? t : 0.f;
 			if (c < dims) lam += t;
-			w[c] = ab > 0.f ? t * (imag ? im[c] : re[c]) / ab : 0.f;
+			// the reference's 3D complex shrinkage scales the z component's
+			// modulus by the y component's direction (3d/tval3_cpu_3d.cpp:934-937);
+			// kept, as its 3D Dt quirk is
+			const int dc = (dims == 3 && c == 2) ? 1 : c;
+			w[c] = ab > 0.f ? t * (imag ? im[dc] : re[dc]) / ab : 0.f;
 		}
 		return imag ? 0.f : lam;
 	}

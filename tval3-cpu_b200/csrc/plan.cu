@@ -98,12 +98,9 @@ long long validate(const tval3g_problem &p, long long b_len, long long ut_len, b
 	default:
 		throw Error{TVAL3G_ERR_ARGUMENT, "Argument error: unknown operator kind"};
 	}
-	if (p.complex_data) {
-		TG_ARG(p.dims == 2 && p.op_kind != TVAL3G_OP_RAY3D,
-		       "Argument error: complex data is supported for 2D problems only");
-		TG_ARG(p.op_kind == TVAL3G_OP_RAY2D || p.layers == 1,
+	if (p.complex_data)
+		TG_ARG(p.dims == 3 || p.op_kind == TVAL3G_OP_RAY2D || p.layers == 1,
 		       "Argument error: complex data with more than one layer is not supported");
-	}
 	if (rays && (p.op_kind == TVAL3G_OP_RAY2D || p.op_kind == TVAL3G_OP_RAY3D)) {
 		// every traced ray must stay inside the image (Bresenham stays inside
 		// the bounding box of its endpoints); the reference does not check
@@ -170,7 +167,7 @@ __global__ void k_map_out(long long nnz, const int4 *rays, int *cind) {
 // transpose gives [Re A^H y; Im A^H y] - the reference's conjugate-transposed
 // products (2d/mat_mult.h:15-91, CblasConjTrans / 'c').  Dense A and CSR
 // values arrive as interleaved (re, im) floats; a ray geometry (real
-// weights) becomes the CSR form of diag(A, A) over its traced rays.
+// weights, 2D or 3D) becomes the CSR form of diag(A, A) over its traced rays.
 static void prepare_complex_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
                                bool keep_ray_csr) {
 	TG_ARG(!(flags & TVAL3G_DEVICE_INPUTS), "Argument error: complex operators must be given in host memory");
@@ -231,12 +228,14 @@ static void prepare_complex_op(cudaStream_t s, const tval3g_problem &p, int flag
 		expand(p.m, p.n_cols, ptr, ind, p.csr_val, p.csr_val + 1, 2);
 		return;
 	}
-	// 2D rays: trace on the device, then the CSR over all E x R measurements
+	// rays: trace on the device, then the CSR over all measurements (2D: E x
+	// R; 3D: numPaths x numMPs, the compact index)
 	OpStore tmp;
 	q.complex_data = 0;
 	prepare_op(s, q, flags, tmp, true);
-	const long long m = (long long)p.num_emitters * p.num_receivers;
-	const long long n = (long long)p.dim_x * p.dim_y;
+	const bool is3 = p.op_kind == TVAL3G_OP_RAY3D;
+	const long long m = is3 ? (long long)p.numPaths * p.numMPs : (long long)p.num_emitters * p.num_receivers;
+	const long long n = (long long)p.dim_x * p.dim_y * (is3 ? p.dim_z : 1);
 	const int nr = tmp.dev.nrays;
 	std::vector<int> trp((size_t)nr + 1), tri((size_t)std::max(tmp.nnz, 1LL));
 	TG_CUDA(cudaMemcpyAsync(trp.data(), tmp.ray_rptr, sizeof(int) * ((size_t)nr + 1), cudaMemcpyDeviceToHost, s));

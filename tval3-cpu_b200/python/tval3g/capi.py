@@ -216,7 +216,8 @@ def ray2d_problem(shape, g, complex_data=False):
                        complex_data=int(bool(complex_data)))
 
 
-def ray3d_problem(shape, g):
+def ray3d_problem(shape, g, complex_data=False):
+    """complex_data: b, Ut and U are complex (the geometry is real)."""
     a = {k: _arr(g[k], np.int32) for k in ("use_path", "xe", "ye", "ze", "xr", "yr", "zr")}
     return ProblemSpec(shape, OP_RAY3D, list(a.values()), num_emitters=int(g["E"]), num_receivers=int(g["R"]),
                        numMPs=int(g["numMPs"]), numPaths=int(g["numPaths"]),
@@ -224,7 +225,7 @@ def ray3d_problem(shape, g):
                        y_emitters=_ptr(a["ye"], C.c_int), z_emitters=_ptr(a["ze"], C.c_int),
                        x_receivers=_ptr(a["xr"], C.c_int), y_receivers=_ptr(a["yr"], C.c_int),
                        z_receivers=_ptr(a["zr"], C.c_int), rv_x=int(g["rv_x"]), rv_y=int(g["rv_y"]),
-                       rv_z=int(g["rv_z"]), scale_factor=float(g["scale"]))
+                       rv_z=int(g["rv_z"]), scale_factor=float(g["scale"]), complex_data=int(bool(complex_data)))
 
 
 def problem_from_workload(w, use_csr=False):
