@@ -125,3 +125,16 @@ def test_complex_operator_needs_host_arrays(torch_cuda):
     with pytest.raises(capi.TVAL3Error) as e:
         capi.Plan([api_problem(c, capi)], [c["opts"]], device_inputs=True)
     assert str(e.value) == "Argument error: complex operators must be given in host memory"
+
+
+def test_complex_isreal_keeps_the_real_part(torch_cuda):
+    """isreal (2d:855-859): the solve is the same, the returned U is the real
+    part of the complex solution (then scaled), rel_error measured on it."""
+    c = build_case("cdense2d_s32")
+    spec = api_problem(c, capi)
+    o = dict(c["opts"], maxit=20)
+    U, _ = capi.solve(spec, c["b"], o)
+    Ur, info = capi.solve(spec, c["b"], dict(o, isreal=1), Ut=c["u_true"])
+    assert np.all(Ur.imag == 0)
+    np.testing.assert_array_equal(Ur.real, U.real)
+    assert abs(info["rel_error"] - relerr(Ur, c["u_true"])) < 1e-5

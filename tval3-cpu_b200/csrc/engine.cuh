@@ -214,6 +214,7 @@ struct Inst {
 	// [[Re A, -Im A], [Im A, Re A]]; the caller's b, Ut and U stay
 	// interleaved (re, im) pairs (cplx_index)
 	int cplx;
+	int isreal;                  // complex data: keep the real part of the final U (2d:855-859)
 	OpDev op;
 };
 

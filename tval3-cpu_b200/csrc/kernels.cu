@@ -879,7 +879,9 @@ __global__ void __launch_bounds__(BLOCK) k_final(KArgs a) {
 	const float scl = (float)c.scl;
 	double v[2] = {0, 0};
 	FOR_TILE(local * TILE, (int)I.n, i) {
-		float u = I.vn[vU][i] / scl;
+		float u = I.vn[vU][i];
+		if (I.cplx && I.isreal && i >= (int)(I.n >> 1)) u = 0.f;   // isreal: U = real(U) before scaling
+		u = u / scl;
 		const long long ui = cplx_index(I, i, I.n);
 		I.u_user[ui] = u;
 		if (I.ut_user) {

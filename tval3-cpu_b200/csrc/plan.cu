@@ -609,6 +609,7 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 			I.c = o.c; I.gamma = o.gamma; I.gam0 = o.gam; I.rate_gam = o.rate_gam; I.rate_cnt = o.rate_cnt;
 			I.skipRatio = o.skipMulRatio; I.maxRelChange = o.maxRelativeChange;
 			I.maxit = o.maxit; I.maxcnt = o.maxcnt; I.nonneg = o.nonneg != 0; I.tv_norm = o.tv_norm;
+			I.isreal = o.isreal != 0;
 			I.numInit = o.numInitIterations;
 			I.skip_enabled = (o.skipMulRatio != 0 && p.op_kind != TVAL3G_OP_DENSE);
 			any_skip_ |= I.skip_enabled != 0;
