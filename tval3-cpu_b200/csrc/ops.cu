@@ -1091,16 +1091,39 @@ __global__ void k_scan_tiles(const long long *in, long long *out, long long n, l
 	if (threadIdx.x == SCAN_T - 1) tot[blockIdx.x] = sh[wid] + incl;
 }
 
-__global__ void k_scan_totals(long long *tot, int nb, long long *out, long long n) {
-	// one thread: nb is small (n / 1024)
-	if (threadIdx.x != 0 || blockIdx.x != 0) return;
-	long long run = 0;
-	for (int b = 0; b < nb; b++) {
-		long long t = tot[b];
-		tot[b] = run;
-		run += t;
+// exclusive scan of the nb tile totals in place, by one block of 1024
+// threads (each a contiguous run of totals); out[n] = the grand total
+__global__ void __launch_bounds__(1024) k_scan_totals(long long *tot, int nb, long long *out, long long n) {
+	__shared__ long long sh[32];
+	const int t = threadIdx.x, per = (nb + 1023) / 1024;
+	const int b0 = min(nb, t * per), b1 = min(nb, b0 + per);
+	long long s = 0;
+	for (int b = b0; b < b1; b++) s += tot[b];
+	const int lane = t & 31, wid = t >> 5;
+	long long incl = s;
+	for (int o = 1; o < 32; o <<= 1) {
+		const long long u = __shfl_up_sync(0xffffffffu, incl, o);
+		if (lane >= o) incl += u;
 	}
-	out[n] = run;
+	if (lane == 31) sh[wid] = incl;
+	__syncthreads();
+	if (wid == 0) {
+		const long long v = sh[lane];
+		long long vi = v;
+		for (int o = 1; o < 32; o <<= 1) {
+			const long long u = __shfl_up_sync(0xffffffffu, vi, o);
+			if (lane >= o) vi += u;
+		}
+		sh[lane] = vi - v;
+	}
+	__syncthreads();
+	long long run = sh[wid] + incl - s;
+	for (int b = b0; b < b1; b++) {
+		const long long v = tot[b];
+		tot[b] = run;
+		run += v;
+	}
+	if (t == 1023) out[n] = sh[wid] + incl;
 }
 
 __global__ void k_scan_add(long long *out, long long n, const long long *tot) {
@@ -1114,7 +1137,7 @@ void scan_counts(cudaStream_t s, const long long *cnt, long long *out, long long
 	long long *tot = nullptr;
 	tot = (decltype(tot))dev_alloc(sizeof(long long) * nb, s);
 	k_scan_tiles<<<(unsigned)nb, SCAN_T, 0, s>>>(cnt, out, n, tot);
-	k_scan_totals<<<1, 32, 0, s>>>(tot, (int)nb, out, n);
+	k_scan_totals<<<1, 1024, 0, s>>>(tot, (int)nb, out, n);
 	if (n > 0) k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, n, tot);
 	TG_CUDA(cudaGetLastError());
 	dev_free(tot, s);
