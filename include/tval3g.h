@@ -139,7 +139,9 @@ const char *tval3g_last_error(void);
 int tval3g_version(void);
 
 /* One solve with host buffers (the drop-in path): U (n floats, output),
- * b (b_len floats), Ut (ut_len floats: 0 or n; may be NULL). */
+ * b (b_len floats), Ut (ut_len floats: 0 or n; may be NULL).  With the
+ * environment variable TVAL3G_TUNE=1 its operator is built with the
+ * autotuner (TVAL3G_TUNE). */
 int tval3g_solve(const tval3g_problem *prob, const float *b, int b_len, const tval3g_options *opts,
                  const float *Ut, int ut_len, float *U, tval3g_info *info);
 

@@ -89,3 +89,27 @@ def test_tuner_caches_per_signature_in_memory_and_on_disk(tmp_path, torch_cuda):
     assert second["stats"] == [0, 2]    # found in the file both times
     assert first["shapes"][0] == first["shapes"][1] == second["shapes"][0] == second["shapes"][1]
     assert len(cache.read_text().strip().splitlines()) == 1
+
+
+_CHILD_SOLVE = r"""
+import json, sys
+sys.path[:0] = [sys.argv[1], sys.argv[2], sys.argv[3]]
+from golden.cases import api_problem, build_case
+from tval3g import capi
+c = build_case("csr3d_s16")
+U, info = capi.solve(api_problem(c, capi), c["b"], c["opts"])
+print(json.dumps({"stats": capi.tune_stats(), "status": info["status"]}))
+"""
+
+
+def test_drop_in_path_tunes_when_asked_by_the_environment(torch_cuda):
+    """tval3g_solve (the path of the C++ overloads) takes no flags: the
+    environment variable TVAL3G_TUNE=1 turns the autotuner on for it."""
+    args = [sys.executable, "-c", _CHILD_SOLVE, os.path.join(ROOT, "tests"),
+            os.path.join(ROOT, "tval3-cpu_b200", "python"), os.path.join(ROOT, "oracle")]
+    for value, measured in (("1", 1), ("0", 0)):
+        env = dict(os.environ, TVAL3G_TUNE=value)
+        env.pop("TVAL3G_TUNE_CACHE", None)
+        out = subprocess.run(args, env=env, capture_output=True, text=True, check=True).stdout.strip().splitlines()
+        got = json.loads(out[-1])
+        assert got["status"] == 0 and got["stats"][0] == measured, (value, got)

@@ -1,5 +1,6 @@
 // C ABI of libtval3g.so (include/tval3g.h).
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 
 #include "plan.cuh"
@@ -126,7 +127,11 @@ int tval3g_solve(const tval3g_problem *prob, const float *b, int b_len, const tv
 	const float *bb[1] = {b};
 	const float *uu[1] = {Ut && ut_len > 0 ? Ut : nullptr};
 	float *out[1] = {U};
-	int rc = tval3g_solve_batch(1, prob, bb, opts, uu, out, info, TVAL3G_GRAPH);
+	// the drop-in path takes no flags: TVAL3G_TUNE=1 in the environment turns
+	// the autotuner on for it
+	const char *tune = std::getenv("TVAL3G_TUNE");
+	const int flags = TVAL3G_GRAPH | (tune && std::atoi(tune) != 0 ? TVAL3G_TUNE : 0);
+	int rc = tval3g_solve_batch(1, prob, bb, opts, uu, out, info, flags);
 	return rc;
 	CAPI_END
 }
