@@ -1,0 +1,95 @@
+"""Degenerate and ragged problems through the C ABI against the FP64 oracle:
+a one-pixel image, images whose sides are not multiples of any tile, CSR
+rows without entries, rays of length zero and unused paths, a 2x2x2 volume."""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import relerr
+from tval3g import capi, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _opts(maxit=10):
+    return W.options(2 ** 8, 2 ** 5, 1e-4, maxit, tv_norm=0)
+
+
+def _check(spec, op, b, shape, opts, bar=1e-3):
+    U, info = capi.solve(spec, b, opts)
+    r = O.solve(op, np.asarray(b, np.float64), shape, opts)
+    assert info["status"] == 0
+    assert info["total_iters"] == r.total_iters, (info, r.total_iters)
+    scale = max(np.linalg.norm(r.U), 1e-30)
+    assert np.linalg.norm(U.astype(np.float64) - r.U) <= bar * scale, relerr(U, r.U)
+    return U
+
+
+def test_one_pixel_is_reported_not_returned_as_nan(torch_cuda):
+    """On a 1x1 image the first step length is 0/0: the reference (and the
+    oracle) return NaN; the C ABI stops with TVAL3G_ERR_NONFINITE instead."""
+    A = np.array([[0.7]], np.float32)
+    b = np.array([0.35], np.float32)
+    r = O.solve(O.Op.dense(A.astype(np.float64)), b.astype(np.float64), (1, 1), _opts())
+    assert np.isnan(r.U).all()
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve(capi.dense_problem((1, 1), A), b, _opts())
+    assert e.value.code == capi.ERR_NONFINITE
+
+
+@pytest.mark.parametrize("shape,m", [((2, 3), 4), ((3, 5), 7), ((17, 9), 40)])
+def test_dense_tiny_and_ragged(shape, m, torch_cuda):
+    rng = np.random.default_rng(sum(shape) + m)
+    n = shape[0] * shape[1]
+    A = (rng.standard_normal((m, n)) / np.sqrt(m)).astype(np.float32)
+    b = (A.astype(np.float64) @ rng.uniform(0, 1, n)).astype(np.float32)
+    _check(capi.dense_problem(shape, A), O.Op.dense(A.astype(np.float64)), b, shape, _opts())
+
+
+def test_csr_with_empty_rows(torch_cuda):
+    rng = np.random.default_rng(3)
+    shape, m = (6, 7), 20
+    n = shape[0] * shape[1]
+    lens = rng.integers(0, 5, m)
+    lens[[0, 5, 19]] = 0                       # rows without entries
+    rowptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    colind = np.concatenate([np.sort(rng.choice(n, k, replace=False)) for k in lens]).astype(np.int32)
+    val = rng.standard_normal(len(colind)).astype(np.float32)
+    x = rng.uniform(0, 1, n)
+    y = np.zeros(m)
+    rows = np.repeat(np.arange(m), lens)
+    np.add.at(y, rows, val * x[colind])
+    b = y.astype(np.float32)
+    b[[0, 5, 19]] = 0.1                        # data no operator row explains
+    _check(capi.csr_problem(shape, m, n, rowptr, colind, val),
+           O.Op.csr(m, n, rowptr, colind, val.astype(np.float64)), b, shape, _opts())
+
+
+def test_rays_of_length_zero_and_unused_paths(torch_cuda):
+    side = 5
+    xs = np.array([0, 4, 2, 0, 4], np.int32)
+    ys = np.array([0, 0, 4, 2, 4], np.int32)
+    T = len(xs)
+    use = np.ones((T, T), np.int32)
+    use[1, 3] = use[3, 1] = 0                  # unused paths
+    # emitter == receiver on the diagonal: one-pixel rays
+    g = dict(use_path=use.ravel(), xe=xs, ye=ys, xr=xs, yr=ys, ld=side, scale=0.25)
+    rng = np.random.default_rng(4)
+    b = rng.uniform(0.5, 1.5, T * T).astype(np.float32) * use.ravel()
+    _check(capi.ray2d_problem((side, side), g), O.Op.ray2d(g, side * side), b, (side, side), _opts())
+
+
+def test_two_by_two_by_two_volume(torch_cuda):
+    N = 4
+    pts = np.array([[0, 0, 0], [1, 1, 1], [1, 0, 1], [0, 1, 0]], np.int32)
+    use = np.zeros((N, N), np.int32)
+    k = 1
+    for e in range(N):
+        for r in range(N):
+            if e != r:
+                use[e, r] = k
+                k += 1
+    g = dict(numMPs=1, numPaths=k - 1, E=N, R=N, use_path=use.ravel(), xe=pts[:, 0], ye=pts[:, 1], ze=pts[:, 2],
+             xr=pts[:, 0], yr=pts[:, 1], zr=pts[:, 2], rv_x=2, rv_y=2, rv_z=2, scale=0.5)
+    b = np.random.default_rng(5).uniform(0.5, 1.5, k - 1).astype(np.float32)
+    _check(capi.ray3d_problem((2, 2, 2), g), O.Op.ray3d(g), b, (2, 2, 2), _opts())
