@@ -138,3 +138,15 @@ def test_complex_isreal_keeps_the_real_part(torch_cuda):
     assert np.all(Ur.imag == 0)
     np.testing.assert_array_equal(Ur.real, U.real)
     assert abs(info["rel_error"] - relerr(Ur, c["u_true"])) < 1e-5
+
+
+def test_complex_isotropic_tv_with_real_values_is_the_real_solve(torch_cuda):
+    """Isotropic TV (no reference counterpart) on complex data shrinks by the
+    modulus over both components and both planes; with imaginary parts 0 it
+    is the real isotropic solve."""
+    c = build_case("dense2d_s32_it20")
+    o = dict(c["opts"], tv_norm=1)
+    Ur, ir = capi.solve(capi.dense_problem(c["shape"], c["A"]), c["b"], o)
+    Uc, ic = capi.solve(capi.dense_problem(c["shape"], c["A"].astype(np.complex64)), c["b"].astype(np.complex64), o)
+    assert np.all(Uc.imag == 0) and ic["total_iters"] == ir["total_iters"]
+    assert relerr(Uc.real, Ur) < 1e-4
