@@ -11,7 +11,7 @@
  *   - float data (mat<float>, with tval3_options<float> or <double>) and
  *     complex<float> data run on the GPU; double and complex<double> data
  *     run through float / complex<float> copies (FP32 storage with FP64
- *     reductions: float accuracy, not double); 2D complex data takes one layer;
+ *     reductions: float accuracy, not double);
  *   - submat_mb and virtual_procs_per_core are accepted and ignored (they
  *     tune the reference's CPU cache blocking and thread count);
  *   - the 2D ray geometry works (the reference's projector body is commented

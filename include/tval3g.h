@@ -131,7 +131,7 @@ typedef struct tval3g_problem {
 	 * 2d/tval3_cpu_2d.cpp:913-929 and the sparse / geometry ones): b, Ut and
 	 * U hold interleaved (re, im) float pairs (b_len, ut_len and n count
 	 * complex elements), as do DENSE A and CSR csr_val; the adjoint is the
-	 * conjugate transpose.  2D and 3D; in 2D one layer; host operator arrays. */
+	 * conjugate transpose.  2D (layers too) and 3D; host operator arrays. */
 	int complex_data;
 } tval3g_problem;
 

@@ -70,8 +70,8 @@ static void e_double() {   // double data: the same argument checks
 	tval3_options<double> o;
 	tval3_cpu_2d(U, A, b, o, Ut);
 }
-static void e_complex() {   // complex data: one layer only
-	mat<std::complex<float> > U(8, 16, mat_col_major), A(20, 64, mat_row_major), b(40), Ut(0, mat_col_major);
+static void e_complex() {   // complex data: the layered size check
+	mat<std::complex<float> > U(8, 16, mat_col_major), A(20, 64, mat_row_major), b(41), Ut(0, mat_col_major);
 	tval3_cpu_2d(U, A, b, opts(), Ut);
 }
 static void e_complex_format() {   // complex data: the same argument checks

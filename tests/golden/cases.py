@@ -20,7 +20,8 @@ CASES = [
 ]
 # complex data (the reference's complex<float> / complex<double> overloads):
 # the FP64 anchor is the reference's own complex<double> build
-COMPLEX_CASES = ["cdense2d_s32", "ccsr2d_s32", "cring2d_s64", "cdense3d_s8", "chemi3d_s16"]
+COMPLEX_CASES = ["cdense2d_s32", "ccsr2d_s32", "cring2d_s64", "cdense3d_s8", "chemi3d_s16", "cdense2d_layers",
+                 "ccsr2d_layers"]
 
 
 def _complex_phantom(side, rng):
@@ -166,6 +167,29 @@ def build_case(name):
         b = _complex_noise(_csr_apply(csr, u.ravel()), 0.01, rng).astype(np.complex64)
         c.update(shape=(side, side), b=b, u_true=u.astype(np.complex64), csr=csr, csr_tuple=_csr_tuple(csr),
                  ref_kind="csr", api="csr", layers=1, opts=W.options(2 ** 8, 2 ** 5, 1e-4, 300, tv_norm=0))
+    elif name in ("cdense2d_layers", "ccsr2d_layers"):
+        # complex data with three stacked layers (2d/tval3_cpu_2d.cpp:894)
+        rng = np.random.default_rng(16)
+        side, layers = 16, 3
+        n = side * side
+        m = int(0.4 * n)
+        us = [_complex_phantom(side, rng) for _ in range(layers)]
+        u_true = np.concatenate([u.ravel() for u in us]).reshape(side * layers, side).astype(np.complex64)
+        if name == "cdense2d_layers":
+            A = ((rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))) / math.sqrt(2 * m)).astype(np.complex64)
+            ys = [A.astype(np.complex128) @ u.ravel() for u in us]
+            c.update(A=A, ref_kind="dense", api="dense")
+        else:
+            k = 32
+            colind = np.concatenate([np.sort(rng.choice(n, k, replace=False)) for _ in range(m)]).astype(np.int32)
+            rowptr = (np.arange(m + 1) * k).astype(np.int32)
+            val = ((rng.standard_normal(m * k) + 1j * rng.standard_normal(m * k)) / math.sqrt(2 * k)).astype(np.complex64)
+            csr = {"m": m, "n": n, "rowptr": rowptr, "colind": colind, "val": val}
+            ys = [_csr_apply(csr, u.ravel()) for u in us]
+            c.update(csr=csr, csr_tuple=_csr_tuple(csr), ref_kind="csr", api="csr")
+        b = np.concatenate([_complex_noise(y, 0.01, rng) for y in ys]).astype(np.complex64)
+        c.update(shape=(side * layers, side), b=b, u_true=u_true, layers=layers,
+                 opts=W.options(2 ** 8, 2 ** 5, 1e-4, 300, tv_norm=0))
     elif name == "cdense3d_s8":
         rng = np.random.default_rng(14)
         sd = 8

@@ -99,17 +99,17 @@ def test_no_device_is_an_error_not_a_fallback():
 
 
 def test_complex_argument_errors():
-    """Complex data: one layer in 2D; the reference's size checks first."""
+    """Complex data: the reference's size checks, layers included."""
     A = np.zeros((5, 16), np.complex64)
     spec = capi.dense_problem((4, 4), A)
     assert spec.p.complex_data == 1
     with pytest.raises(capi.TVAL3Error) as e:
         capi.solve(spec, np.zeros(6, np.complex64), _opts())
     assert str(e.value) == "Argument error: b.len must be equal to A.dim_y * layers!"
-    spec = capi.dense_problem((4, 8), A, layers=2)
+    spec = capi.dense_problem((4, 8), A, layers=2)   # layers: b.len = A.dim_y * layers
     with pytest.raises(capi.TVAL3Error) as e:
-        capi.solve(spec, np.zeros(10, np.complex64), _opts())
-    assert str(e.value) == "Argument error: complex data with more than one layer is not supported"
+        capi.solve(spec, np.zeros(11, np.complex64), _opts())
+    assert str(e.value) == "Argument error: b.len must be equal to A.dim_y * layers!"
     spec = capi.dense_problem((2, 2, 4), A)   # 3D: the reference's 3D size message
     with pytest.raises(capi.TVAL3Error) as e:
         capi.solve(spec, np.zeros(6, np.complex64), _opts())

@@ -48,7 +48,7 @@ def test_argument_errors_match_reference(demo):
     assert got["csc"] == "Argument error: A must be available in CSR and CSC format!"
     assert got["geom_layers_or_blen"] == "Argument error: b.len must be equal to A.num_emitters * A.num_receivers!"
     assert got["double"] == "Argument error: Matrices must be in row major format!"   # checked as for float
-    assert got["complex"] == "Argument error: complex data with more than one layer is not supported"
+    assert got["complex"] == "Argument error: b.len must be equal to A.dim_y * layers!"
     assert got["complex_format"] == "Argument error: Matrices must be in row major format!"
     if O.ref_available(2):   # the reference itself, same arguments
         opts = dict(mu=256.0, beta=32.0, mu0=256.0, beta0=32.0, tol=1e-4, tol_inn=1e-3, c=1e-5, gamma=0.6,

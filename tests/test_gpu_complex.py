@@ -70,20 +70,30 @@ def test_complex_operator_is_the_real_form(name, torch_cuda):
     c = build_case(name)
     op = capi.Operator(api_problem(c, capi))
     rng = np.random.default_rng(3)
-    n, m = op.cols // 2, op.rows // 2
+    n, m = op.cols // 2, op.rows // 2       # complex lengths, all layers
+    L = c.get("layers", 1)
     x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
     y = rng.standard_normal(m) + 1j * rng.standard_normal(m)
     if "A" in c:
         A = c["A"].astype(np.complex128)
-        Ax, Ahy = A @ x, A.conj().T @ y
+        fwd = lambda v: A @ v            # noqa: E731
+        adj = lambda v: A.conj().T @ v   # noqa: E731
     else:
         csr = c["csr"]
         rows = np.repeat(np.arange(csr["m"]), np.diff(csr["rowptr"]))
-        v = csr["val"].astype(np.complex128)
-        Ax = np.zeros(m, complex)
-        np.add.at(Ax, rows, v * x[csr["colind"]])
-        Ahy = np.zeros(n, complex)
-        np.add.at(Ahy, csr["colind"], v.conj() * y[rows])
+        val = csr["val"].astype(np.complex128)
+
+        def fwd(v):
+            out = np.zeros(csr["m"], complex)
+            np.add.at(out, rows, val * v[csr["colind"]])
+            return out
+
+        def adj(v):
+            out = np.zeros(csr["n"], complex)
+            np.add.at(out, csr["colind"], val.conj() * v[rows])
+            return out
+    Ax = np.concatenate([fwd(xl) for xl in x.reshape(L, -1)])      # layer by layer
+    Ahy = np.concatenate([adj(yl) for yl in y.reshape(L, -1)])
     dx = torch.tensor(_planar(x), device="cuda")
     dy = torch.tensor(_planar(y), device="cuda")
     out_m = torch.empty(2 * m, device="cuda")

@@ -98,9 +98,6 @@ long long validate(const tval3g_problem &p, long long b_len, long long ut_len, b
 	default:
 		throw Error{TVAL3G_ERR_ARGUMENT, "Argument error: unknown operator kind"};
 	}
-	if (p.complex_data)
-		TG_ARG(p.dims == 3 || p.op_kind == TVAL3G_OP_RAY2D || p.layers == 1,
-		       "Argument error: complex data with more than one layer is not supported");
 	if (rays && (p.op_kind == TVAL3G_OP_RAY2D || p.op_kind == TVAL3G_OP_RAY3D)) {
 		// every traced ray must stay inside the image (Bresenham stays inside
 		// the bounding box of its endpoints); the reference does not check
@@ -174,7 +171,8 @@ static void prepare_complex_op(cudaStream_t s, const tval3g_problem &p, int flag
 	tval3g_problem q = p;
 	q.complex_data = 0;
 	q.layers = 1;
-	if (p.op_kind == TVAL3G_OP_DENSE) {
+	const long long L = p.dims == 2 && p.op_kind != TVAL3G_OP_RAY2D ? std::max(p.layers, 1) : 1;
+	if (p.op_kind == TVAL3G_OP_DENSE && L == 1) {
 		const long long m = p.m, nc = p.n_cols;
 		std::vector<float> R((size_t)(4 * m * nc));
 		for (long long r = 0; r < m; r++)
@@ -191,31 +189,36 @@ static void prepare_complex_op(cudaStream_t s, const tval3g_problem &p, int flag
 		prepare_op(s, q, flags, st, keep_ray_csr);   // copies R before it returns
 		return;
 	}
-	// CSR rows of the real form from (row pointers, columns, complex values)
+	// CSR rows of the real form from (row pointers, columns, complex values).
+	// With L layers (2D, the reference's stacked layers) the planar vectors
+	// hold all layers' real parts, then all imaginary parts, so layer l's
+	// block maps columns l nc (+ L nc for Im x) to rows l m (+ L m for Im y).
 	auto expand = [&](long long m, long long nc, const std::vector<int> &ptr, const std::vector<int> &ind,
 	                  const float *re, const float *im, int re_stride) {
-		const long long nnz = ptr[m];
-		std::vector<int> rp((size_t)(2 * m + 1)), ri((size_t)(4 * nnz));
-		std::vector<float> rv((size_t)(4 * nnz));
+		const long long nnz = ptr[m], P = L * nc;
+		TG_ARG(4 * nnz * L < (1LL << 31), "Argument error: the complex operator has too many entries");
+		std::vector<int> rp((size_t)(2 * m * L + 1)), ri((size_t)(4 * nnz * L));
+		std::vector<float> rv((size_t)(4 * nnz * L));
 		long long o = 0;
 		for (int half = 0; half < 2; half++)
-			for (long long r = 0; r < m; r++) {
-				rp[(size_t)(half * m + r)] = (int)o;
-				for (int part = 0; part < 2; part++)   // columns of Re x, then of Im x
-					for (long long k = ptr[r]; k < ptr[r + 1]; k++) {
-						const float vr = re[k * re_stride], vi = im ? im[k * re_stride] : 0.f;
-						ri[(size_t)o] = ind[(size_t)k] + (part ? (int)nc : 0);
-						// [[Re A, -Im A], [Im A, Re A]]
-						rv[(size_t)o++] = half == 0 ? (part == 0 ? vr : -vi) : (part == 0 ? vi : vr);
-					}
-			}
-		rp[(size_t)(2 * m)] = (int)o;
+			for (long long l = 0; l < L; l++)
+				for (long long r = 0; r < m; r++) {
+					rp[(size_t)(half * m * L + l * m + r)] = (int)o;
+					for (int part = 0; part < 2; part++)   // columns of Re x, then of Im x
+						for (long long k = ptr[r]; k < ptr[r + 1]; k++) {
+							const float vr = re[k * re_stride], vi = im ? im[k * re_stride] : 0.f;
+							ri[(size_t)o] = (int)(ind[(size_t)k] + l * nc + (part ? P : 0));
+							// [[Re A, -Im A], [Im A, Re A]]
+							rv[(size_t)o++] = half == 0 ? (part == 0 ? vr : -vi) : (part == 0 ? vi : vr);
+						}
+				}
+		rp[(size_t)(2 * m * L)] = (int)o;
 		tval3g_problem c = p;
 		c.complex_data = 0;
 		c.layers = 1;
 		c.op_kind = TVAL3G_OP_CSR;
-		c.m = (int)(2 * m);
-		c.n_cols = (int)(2 * nc);
+		c.m = (int)(2 * m * L);
+		c.n_cols = (int)(2 * nc * L);
 		c.nnz = o;
 		c.csr_ptr = rp.data();
 		c.csr_ind = ri.data();
@@ -226,6 +229,13 @@ static void prepare_complex_op(cudaStream_t s, const tval3g_problem &p, int flag
 	if (p.op_kind == TVAL3G_OP_CSR) {
 		std::vector<int> ptr(p.csr_ptr, p.csr_ptr + p.m + 1), ind(p.csr_ind, p.csr_ind + p.nnz);
 		expand(p.m, p.n_cols, ptr, ind, p.csr_val, p.csr_val + 1, 2);
+		return;
+	}
+	if (p.op_kind == TVAL3G_OP_DENSE) {   // layered: every entry of A as a CSR entry
+		std::vector<int> ptr((size_t)p.m + 1), ind((size_t)p.m * p.n_cols);
+		for (long long r = 0; r <= p.m; r++) ptr[(size_t)r] = (int)(r * p.n_cols);
+		for (long long k = 0; k < (long long)p.m * p.n_cols; k++) ind[(size_t)k] = (int)(k % p.n_cols);
+		expand(p.m, p.n_cols, ptr, ind, p.A, p.A + 1, 2);
 		return;
 	}
 	// rays: trace on the device, then the CSR over all measurements (2D: E x
