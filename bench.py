@@ -53,7 +53,6 @@ def args_():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="tval3g", choices=["tval3g", "reference"])
     p.add_argument("--workload", default="ring2d", choices=["ring2d", "dense2d", "hemi3d", "batch", "mrhs"])
-    p.add_argument("--cpu-sample-iters", type=int, default=20)
     p.add_argument("--profile", action="store_true",
                    help="for ncu: build the plan, run --warmup + --steps solves, print nothing else")
     p.add_argument("--maxit", type=int, default=None, help="override maxit (profiling a short solve)")
@@ -153,18 +152,19 @@ class Clocks:
 # --------------------------------------------------------------------------
 # reference arm / CPU baseline
 # --------------------------------------------------------------------------
-def reference_rate(w, sample_iters, full_iters):
-    """Seconds per reconstruction of the reference's own solver (float data,
-    all host threads) from a bounded sample of iterations scaled to the
-    iteration count of a full solve.  Ray workloads run on their CSR twin (the
+def reference_solve(w):
+    """One complete solve of the reference's own solver (float data, all host
+    threads, its own stopping rules: maxit, tol, tol_inn), timed by the host
+    clock around the call (its info.secs covers the same span,
+    2d/tval3_cpu_2d.cpp:760,862).  Ray workloads run on their CSR twin (the
     reference's 2D projector is commented out, 2d/mat_mult.h:111-193); the
-    reference has anisotropic TV only."""
+    reference has anisotropic TV only.  Returns (seconds, result) or None
+    when oracle/_ref was not built."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     if not O.ref_available(2):
         return None
     o = dict(w["opts"])
-    o["maxit"] = sample_iters
     o["tv_norm"] = 0
     cwd = os.getcwd()
     t0 = time.perf_counter()
@@ -174,11 +174,20 @@ def reference_rate(w, sample_iters, full_iters):
         A = w["csr"]
         r = O.ref_solve("csr", w["shape"], w["b"], o, dtype=0,
                         csr=(A["m"], A["n"], A["rowptr"], A["colind"], A["val"]), vppc=1)
-    os.chdir(cwd)
     secs = time.perf_counter() - t0
-    per_iter = secs / max(r.total_iters, 1)
-    return {"secs_per_iter": per_iter, "secs_per_solve": per_iter * full_iters, "sample_iters": r.total_iters,
-            "cores": os.cpu_count()}
+    os.chdir(cwd)
+    return secs, r
+
+
+def relerr(a, b):
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+# the reference arm times complete solves: at most this many (and one
+# warm-up), so that the arm ends within a few minutes whatever --steps asks
+REF_MAX_STEPS, REF_MAX_WARMUP = 3, 1
 
 
 def run_reference(a, rank):
@@ -186,26 +195,34 @@ def run_reference(a, rank):
         return
     w = workload("ring2d")
     ref = fp64_reference("ring2d")
-    full_iters = int(ref["iters"][1]) if ref is not None else int(w["opts"]["maxit"])
-    for _ in range(a.warmup):
-        reference_rate(w, a.cpu_sample_iters, full_iters)
-    rates = []
-    r = None
-    for _ in range(a.steps):
-        r = reference_rate(w, a.cpu_sample_iters, full_iters)
-        if r is None:
+    steps, warm = max(1, min(a.steps, REF_MAX_STEPS)), min(a.warmup, REF_MAX_WARMUP)
+    for _ in range(warm):
+        if reference_solve(w) is None:
+            break
+    secs, r = [], None
+    for _ in range(steps):
+        out = reference_solve(w)
+        if out is None:
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (the reference "
                                                                   "sources were absent when building)"}))
             return
-        rates.append(r["secs_per_solve"])
-    ms = float(np.mean(rates)) * 1000
+        secs.append(out[0])
+        r = out[1]
+    ms = float(np.mean(secs)) * 1000
     val = 1000.0 / ms
-    line = {"metric": METRIC, "value": val, "unit": "reconstructions/s", "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+    err = relerr(r.U, ref["U_aniso"]) if ref is not None and "U_aniso" in ref else None
+    sample = (f"complete solves of the reference solver (float data, anisotropic TV: it has no isotropic TV) "
+              f"on the CSR twin of the ring operator, its own stopping rules: {r.total_iters} iterations, "
+              f"relerr vs the FP64 anisotropic solution {err:.2e}" if err is not None else
+              f"complete solves of the reference solver ({r.total_iters} iterations)")
+    line = {"metric": METRIC, "value": val, "unit": "reconstructions/s", "n_gpus": a.gpus, "steps": steps,
+            "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic", "config": CONFIGS["ring2d"], "impl": "reference",
-            "cpu_baseline": {"value": val, "unit": "reconstructions/s", "cores": r["cores"], "kind": "reference",
-                             "sample": f"{r['sample_iters']} iterations of the reference solver (anisotropic TV: it "
-                                       f"has no isotropic TV) on the CSR twin, scaled to {full_iters} iterations"},
+            "requested": {"steps": a.steps, "warmup": a.warmup,
+                          "note": f"at most {REF_MAX_STEPS} timed complete solves and {REF_MAX_WARMUP} warm-up"},
+            "iterations": r.total_iters, "relerr_vs_fp64_aniso": err, "tv": "anisotropic",
+            "cpu_baseline": {"value": val, "unit": "reconstructions/s", "cores": os.cpu_count(), "kind": "reference",
+                             "sample": sample},
             "e2e": {"value": val, "unit": "reconstructions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -394,6 +411,8 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
     e2e_ms = float(np.mean(et))
     in_bytes = int(b_host.nbytes + sum(x.nbytes for x in spec.keep))
 
+    extra = ring_variants(a, cx, capi, ref) if name == "ring2d" else {}
+
     line = {"metric": METRIC, "value": world * 1000.0 / ms, "unit": "reconstructions/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom and operator, Gaussian noise)",
@@ -412,15 +431,67 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
                     "ms_inside_library": [round(x, 3) for x in ec]},
             "roofline": kernel_roofline(cx, capi, spec, w, w["kind"]),
             "clocks": clk, "gpu_launches": launches}
+    line.update(extra)
     if rank == 0 and world == 1 and name != "hemi3d":
-        cb = reference_rate(w, a.cpu_sample_iters, iters)
-        if cb:
-            line["cpu_baseline"] = {"value": 1.0 / cb["secs_per_solve"], "unit": "reconstructions/s",
-                                    "cores": cb["cores"], "kind": "reference",
-                                    "sample": f"{cb['sample_iters']} iterations of the reference solver (anisotropic "
-                                              f"TV, float, {'CSR twin' if w['kind'] != 'dense' else 'dense'}) "
-                                              f"scaled to {iters} iterations"}
+        out = reference_solve(w)
+        if out:
+            secs, r = out
+            err = relerr(r.U, ref["U_aniso"]) if ref is not None and "U_aniso" in ref else None
+            line["cpu_baseline"] = {"value": 1.0 / secs, "unit": "reconstructions/s", "cores": os.cpu_count(),
+                                    "kind": "reference",
+                                    "sample": f"one complete solve of the reference solver (anisotropic TV, float, "
+                                              f"{'CSR twin' if w['kind'] != 'dense' else 'dense'}, its own stopping "
+                                              f"rules): {r.total_iters} iterations"
+                                              + (f", relerr vs the FP64 anisotropic solution {err:.2e}"
+                                                 if err is not None else "")}
     return line
+
+
+def timed_plan(cx, capi, spec, opts, b, Ut=None, target=0.0, reps=3):
+    """Mean CUDA-event time of `reps` solves of a one-instance graph plan
+    (after one untimed solve), with the last solve's info."""
+    torch, dev, s = cx.torch, cx.dev, cx.stream.cuda_stream
+    d_b = torch.tensor(np.ascontiguousarray(b, np.float32), device=dev)
+    d_U = torch.empty(spec.n, device=dev)
+    uts = [torch.tensor(np.ascontiguousarray(Ut, np.float32).ravel(), device=dev)] if Ut is not None else None
+    plan = capi.Plan([spec], [opts], graph=True, trace=Ut is not None)
+    plan.set_target(target)
+    run = lambda: plan.solve([d_b], [d_U], d_Ut=uts, stream=s)  # noqa: E731
+    cx.event_time(run, 1)
+    ts, infos = cx.event_time(run, reps)
+    plan.close()
+    return float(np.mean(ts)), infos[0], d_U.cpu().numpy()
+
+
+def ring_variants(a, cx, capi, ref):
+    """Sub-records of the ring workload: the anisotropic problem (the one the
+    reference solves: it has no isotropic TV) and the literal unit-weight
+    configuration for a fixed 20 iterations."""
+    from tval3g import workloads as W
+    out = {}
+    if ref is None:
+        return out
+    w = W.ring2d(seed=1, side=256, T=512, tv_norm=0, maxit=500, tol=1e-5, normalize=True)
+    spec = capi.problem_from_workload(w)
+    t_ms, t_info, _ = timed_plan(cx, capi, spec, w["opts"], w["b"], Ut=ref["U_aniso"], target=1e-3)
+    f_ms, f_info, U = timed_plan(cx, capi, spec, w["opts"], w["b"])
+    out["aniso"] = {"time_to_solution_ms": t_ms, "iterations_to_target": t_info["total_iters"],
+                    "relerr_at_target": float(t_info["rel_error"]),
+                    "reached_target": bool(t_info["rel_error"] <= 1e-3),
+                    "full_solve_ms": f_ms, "full_solve_iterations": f_info["total_iters"],
+                    "full_solve_relerr_vs_fp64": relerr(U, ref["U_aniso"]),
+                    "fp64_iterations": int(ref["iters_aniso"][1]),
+                    "value": 1000.0 / t_ms, "unit": "reconstructions/s",
+                    "what": "the same ring workload with anisotropic TV (the reference arm's problem), "
+                            "time to relerr <= 1e-3 vs the FP64 anisotropic solution and the full solve"}
+    wu = W.ring2d(seed=1, side=256, T=512, tv_norm=1, maxit=20, tol=1e-5, normalize=False)
+    spec = capi.problem_from_workload(wu)
+    u_ms, u_info, U = timed_plan(cx, capi, spec, wu["opts"], wu["b"])
+    out["unit_weight"] = {"ms_20_iterations": u_ms, "iterations": u_info["total_iters"],
+                          "relerr_vs_fp64_20_iterations": relerr(U, ref["U_unit20"]),
+                          "what": "the literal configuration (weight 1 per hit), a fixed 20 iterations, against "
+                                  "the FP64 oracle's first 20 iterations"}
+    return out
 
 
 def run_mrhs(a, cx, capi, world, dist, clocks):

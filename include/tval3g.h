@@ -257,9 +257,17 @@ int tval3g_unrolled_destroy(tval3g_unrolled *h);
  * cudaMalloc's synchronisation is not acceptable).  It allocates nothing: its
  * partial-sum scratch is a fixed 4 MiB array compiled into the library, so n
  * may be at most 1048576 (larger n is rejected with TVAL3G_ERR_ARGUMENT).
- * The first call on each device looks up that array's device address; make it
+ * A device holds that array once the library's device code is loaded onto
+ * it: under CUDA's default lazy module loading that is this entry point's
+ * first call on the device, which therefore takes the 4 MiB (and the code)
+ * from the device - make that first call at start-up, before another
+ * allocator reserves the memory, or set CUDA_MODULE_LOADING=EAGER.  The first
+ * call on each device also looks up the array's device address; make it
  * before any stream capture begins.  All calls share the array: calls whose
- * work overlaps on the GPU race.  Returns after the product is complete.
+ * work overlaps on the GPU race.  Stream-ordered: the call returns once the
+ * work is enqueued on `stream` (NULL: the legacy default stream), and y is
+ * complete when the stream reaches that point.  Same arithmetic as
+ * tval3g_op_apply's dense adjoint (FP64 accumulation).
  * No counterpart in the reference (it has no device code). */
 int tval3g_dense_adjoint_static(const float *d_A, int m, int n, const float *d_x, float *d_y, void *stream);
 

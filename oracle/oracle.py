@@ -29,10 +29,8 @@ def build(reference: bool = False) -> None:
     """Compile the restatement (and, when asked and the reference sources are
     present, the reference itself) with oracle/Makefile."""
     subprocess.run(["make", "-s", "-C", HERE, "restate"], check=True)
-    if reference:
-        ref = os.environ.get("TVAL3_REFERENCE", "/root/reference")
-        if os.path.isdir(ref):
-            subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
+    if reference:   # the Makefile builds nothing when the sources are absent
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
 
 
 def ref_available(dims: int = 2) -> bool:
@@ -59,9 +57,14 @@ class Info(C.Structure):
                 ("outer_iters", C.c_int), ("total_iters", C.c_int)]
 
 
+class Replay(C.Structure):
+    _fields_ = [("count", C.c_int), ("backtracks", C.POINTER(C.c_int)), ("skipped", C.POINTER(C.c_int)),
+                ("inner_end", C.POINTER(C.c_int))]
+
+
 class Iter(C.Structure):
     _fields_ = [("tau", C.c_double), ("f", C.c_double), ("relchg", C.c_double), ("backtracks", C.c_int),
-                ("skipped", C.c_int)]
+                ("skipped", C.c_int), ("inner_end", C.c_int), ("pad", C.c_int)]
 
 
 def _fill(struct, opts: dict):
@@ -103,6 +106,8 @@ def lib():
         L.orc_shrink.argtypes = [i, i, i, d] + [dp] * 9
         L.orc_solve.argtypes = [i, i, i, i, vp, dp, i, C.POINTER(OrcOpts), dp, dp, C.POINTER(Info),
                                 C.POINTER(Iter)]
+        L.orc_solve_replay.argtypes = [i, i, i, i, vp, dp, i, C.POINTER(OrcOpts), dp, dp, C.POINTER(Info),
+                                       C.POINTER(Iter), C.POINTER(Replay)]
         _LIB = L
     return _LIB
 
@@ -217,8 +222,26 @@ class Result:
     iters: list | None = None
 
 
-def solve(op: Op, b, shape, opts: dict, Ut=None, record=False) -> Result:
-    """FP64 oracle solve; shape = (dim_y, dim_x) or (dim_z, dim_y, dim_x)."""
+def replay_from_trace(trace):
+    """Decisions of a recorded solve, from its per-iteration trace rows
+    (tau, f, relchg, backtracks, skipped, relerr_ut, step, outer), as the
+    tval3g plan trace gives them: backtracks, skipped and whether the inner
+    loop ended after the iteration (the multipliers were updated, or it was
+    the last iteration)."""
+    tr = np.asarray(trace, np.float64)
+    k = len(tr)
+    inner_end = (tr[:, 7] != 0).astype(np.int32)
+    inner_end[k - 1] = 1 if tr[k - 1, 7] != 0 else 0
+    return {"count": k, "backtracks": tr[:, 3].astype(np.int32), "skipped": tr[:, 4].astype(np.int32),
+            "inner_end": inner_end}
+
+
+def solve(op: Op, b, shape, opts: dict, Ut=None, record=False, replay=None) -> Result:
+    """FP64 oracle solve; shape = (dim_y, dim_x) or (dim_z, dim_y, dim_x).
+
+    replay: decisions of another solve (replay_from_trace) to follow instead
+    of taking its own Armijo, skip and stopping decisions: the FP64 solution
+    at the same iteration count and discrete path."""
     b = _f64(b)
     dims = len(shape)
     if dims == 2:
@@ -230,15 +253,26 @@ def solve(op: Op, b, shape, opts: dict, Ut=None, record=False) -> Result:
     info = Info()
     its = (Iter * max(int(opts["maxit"]), 1))() if record else None
     Utp = _f64(Ut).ravel() if Ut is not None else None
-    rc = lib().orc_solve(dims, dy, dx, dz, op.h, _p(b), len(b), C.byref(o), _p(Utp), _p(U), C.byref(info), its)
+    if replay is None:
+        rc = lib().orc_solve(dims, dy, dx, dz, op.h, _p(b), len(b), C.byref(o), _p(Utp), _p(U), C.byref(info),
+                             its)
+    else:
+        arrs = [np.ascontiguousarray(replay[k], np.int32) for k in ("backtracks", "skipped", "inner_end")]
+        rp = Replay(int(replay["count"]), *[_p(a, C.c_int) for a in arrs])
+        rc = lib().orc_solve_replay(dims, dy, dx, dz, op.h, _p(b), len(b), C.byref(o), _p(Utp), _p(U),
+                                    C.byref(info), its, C.byref(rp))
     if rc != 0:
         raise ValueError(f"oracle solve rejected its arguments ({rc})")
     rec = None
     if record:
         rec = [(its[k].tau, its[k].f, its[k].relchg, its[k].backtracks, its[k].skipped)
                for k in range(info.total_iters)]
-    return Result(U.reshape(shape), info.secs, info.outer_iters, info.total_iters, info.rel_chg,
-                  info.rel_error, rec)
+        rec_end = [its[k].inner_end for k in range(info.total_iters)]
+    res = Result(U.reshape(shape), info.secs, info.outer_iters, info.total_iters, info.rel_chg,
+                 info.rel_error, rec)
+    if record:
+        res.inner_end = rec_end
+    return res
 
 
 # --------------------------------------------------------------------------
@@ -269,6 +303,37 @@ def ref_lib(dims):
 
 
 _DT = {0: np.float32, 1: np.float32, 2: np.float64, 3: np.complex64, 4: np.complex128}
+_PROJ = None
+
+
+def ref_project3d(g, x, trans=False):
+    """The reference's own 3D Bresenham projector (3d/mat_mult.h:148-595,
+    compiled from its sources into oracle/_ref/libref_proj_3d.so) applied in
+    double precision: y = A x (x over voxels) or y = A^T x (x over rays)."""
+    global _PROJ
+    if _PROJ is None:
+        path = os.path.join(HERE, "_ref", "libref_proj_3d.so")
+        if not os.path.exists(path):
+            build(reference=True)
+        L = C.CDLL(path)
+        ip, i = C.POINTER(C.c_int), C.c_int
+        L.ref3d_project.argtypes = [i, i, i, i, i, ip, ip, ip, ip, ip, ip, ip, i, i, i, C.c_float,
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        _PROJ = L
+    a = [_i32(g[k]) for k in ("use_path", "xe", "ye", "ze", "xr", "yr", "zr")]
+    nvox = int(g["rv_x"]) * int(g["rv_y"]) * int(g["rv_z"])
+    nray = int(g["numMPs"]) * int(g["numPaths"])
+    x = _f64(x)
+    assert x.size == (nray if trans else nvox)
+    y = np.zeros(nvox if trans else nray)
+    _PROJ.ref3d_project(int(trans), int(g["numMPs"]), int(g["numPaths"]), int(g["E"]), int(g["R"]),
+                        *[_p(v, C.c_int) for v in a], int(g["rv_x"]), int(g["rv_y"]), int(g["rv_z"]),
+                        float(g["scale"]), _p(x), _p(y))
+    return y
+
+
+def ref_available_proj3d() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_proj_3d.so"))
 
 
 def _vp(a):

@@ -418,6 +418,7 @@ typedef struct {
 	double *last_Au;
 	double *V[3];   /* scratch for Ux - Wx etc. */
 	int last_skip;  /* the last get_g_mult skipped A^T (trace only) */
+	int force_skip; /* replay: -1 own decision, 0 multiply, 1 skip (next get_g_mult only) */
 	double *tmp_n, *tmp_m;
 	const orc_op *op;
 	int tv_norm;
@@ -442,6 +443,8 @@ static void Dst(st_t *s, const double *U, double *Ux, double *Uy, double *Uz) {
 /* get_g_mult: generic with the A^T-skip heuristic 2d:300-357 / 3d:433-493;
  * dense always multiplies (2d:361-394 / 3d:498-529). */
 static void get_g_mult(st_t *s, const double *U, int force) {
+	int want = s->force_skip;
+	s->force_skip = -1;
 	s->last_skip = 0;
 	orc_apply(s->op, 0, U, s->Au);
 	if (s->op->kind == ORC_DENSE || s->skipRatio == 0) {
@@ -452,11 +455,14 @@ static void get_g_mult(st_t *s, const double *U, int force) {
 	double rel = nrm2(s->m, s->tmp_m) / nrm2(s->m, s->Au);
 	if (force) {
 		cpy(s->m, s->Au, s->last_Au); orc_apply(s->op, 1, s->Au, s->g); s->currSkip = 0;
+	} else if (want == 1) {   /* replayed skip */
+		s->currSkip -= 1;
+		s->last_skip = 1;
 	} else if (s->currInit < s->numInit) {
 		cpy(s->m, s->Au, s->last_Au); orc_apply(s->op, 1, s->Au, s->g); s->currInit++; s->currSkip = 0;
 	} else if (s->currSkip < 1) {
 		cpy(s->m, s->Au, s->last_Au); orc_apply(s->op, 1, s->Au, s->g); s->currSkip += s->skipRatio;
-	} else if (rel > s->maxRelChange) {
+	} else if (rel > s->maxRelChange || want == 0) {
 		cpy(s->m, s->Au, s->last_Au); orc_apply(s->op, 1, s->Au, s->g);
 	} else {
 		s->currSkip -= 1;
@@ -544,9 +550,11 @@ static void update_g(st_t *s, double alpha, double *U, const double *b) {
 	s->f = s->lam1 + s->beta / 2 * s->lam2 + s->mu / 2 * s->lam3 - s->lam4 - s->lam5;
 }
 
-/* min_u 2d:526-576 / 3d:750-814; returns the backtracking count (6 = restart) */
+/* min_u 2d:526-576 / 3d:750-814; returns the backtracking count (6 = restart).
+ * force_bt >= 0 (replay): take exactly that many backtracking steps (6: five,
+ * then the restart) instead of testing the Armijo condition. */
 static int min_u(st_t *s, double *U, double *gam, const double *b, const orc_opts *o, double C,
-                 int fst, double *tau_out) {
+                 int fst, double *tau_out, int force_bt) {
 	double tau = get_tau(s, fst);
 	cpy(s->n, U, s->Up); cpy(s->n, s->g, s->gp); cpy(s->n, s->g2, s->g2p);
 	cpy(s->m, s->Au, s->Aup); cpy(s->n, s->Ux, s->Uxp); cpy(s->n, s->Uy, s->Uyp);
@@ -556,14 +564,14 @@ static int min_u(st_t *s, double *U, double *gam, const double *b, const orc_opt
 	vadd(s->n, U, -1, s->Up, s->dU);
 	double c_armij = dot(s->n, s->d, s->d) * tau * o->c * s->beta;
 	int cnt = 0;
-	if (fabs(s->f) > fabs(C - alpha * c_armij)) {
+	if (force_bt >= 0 ? force_bt > 0 : fabs(s->f) > fabs(C - alpha * c_armij)) {
 		vadd(s->n, s->g, -1, s->gp, s->dg);
 		vadd(s->n, s->g2, -1, s->g2p, s->dg2);
 		vadd(s->m, s->Au, -1, s->Aup, s->dAu);
 		vadd(s->n, s->Ux, -1, s->Uxp, s->dUx);
 		vadd(s->n, s->Uy, -1, s->Uyp, s->dUy);
 		if (s->dims == 3) vadd(s->n, s->Uz, -1, s->Uzp, s->dUz);
-		while (fabs(s->f) > fabs(C - alpha * c_armij)) {
+		while (force_bt >= 0 ? cnt < force_bt : fabs(s->f) > fabs(C - alpha * c_armij)) {
 			if (cnt == 5) {
 				*gam *= o->rate_gam;
 				tau = get_tau(s, 1);
@@ -641,9 +649,10 @@ static double now(void) {
 	return tv.tv_sec + tv.tv_usec / 1e6;
 }
 
-/* the driver, 2d:752-886 / 3d:1172-1378 */
-int orc_solve(int dims, int dim_y, int dim_x, int dim_z, const orc_op *op, const double *b_in, int blen,
-              const orc_opts *o, const double *Ut, double *U, orc_info *info, orc_iter *iters) {
+/* the driver, 2d:752-886 / 3d:1172-1378; rp != NULL replays recorded decisions */
+static int solve_impl(int dims, int dim_y, int dim_x, int dim_z, const orc_op *op, const double *b_in, int blen,
+                      const orc_opts *o, const double *Ut, double *U, orc_info *info, orc_iter *iters,
+                      const orc_replay *rp) {
 	double t0 = now();
 	st_t S, *s = &S;
 	memset(s, 0, sizeof(S));
@@ -664,6 +673,7 @@ int orc_solve(int dims, int dim_y, int dim_x, int dim_z, const orc_op *op, const
 	s->mu = o->mu0; s->beta = o->beta0;
 	s->numInit = (unsigned)o->numInitIterations; s->skipRatio = o->skipMulRatio;
 	s->maxRelChange = o->maxRelativeChange;
+	s->force_skip = -1;
 
 	double *bs = zeros(m);
 	cpy(m, b_in, bs);
@@ -686,10 +696,12 @@ int orc_solve(int dims, int dim_y, int dim_x, int dim_z, const orc_op *op, const
 	double RelChg, RelChgOut = 0, nrmup = 0;
 
 	while (count_outer < o->maxcnt && count_total < o->maxit) {
+		if (rp && count_total >= rp->count) break;
 		fst = 1;
 		while (count_total < o->maxit) {
 			double tau;
-			int bt = min_u(s, U, &gam, bs, o, C, fst, &tau);
+			if (rp) s->force_skip = rp->skipped[count_total];
+			int bt = min_u(s, U, &gam, bs, o, C, fst, &tau, rp ? rp->backtracks[count_total] : -1);
 			update_W(s);
 			Qp = Q; Q = gam * Qp + 1; C = (gam * Qp * C + s->f) / Q;
 			vadd(n, U, -1, s->Up, s->uup);
@@ -700,16 +712,19 @@ int orc_solve(int dims, int dim_y, int dim_x, int dim_z, const orc_op *op, const
 				iters[count_total].tau = tau; iters[count_total].f = s->f;
 				iters[count_total].relchg = RelChg; iters[count_total].backtracks = bt;
 				iters[count_total].skipped = s->last_skip;
+				iters[count_total].inner_end = 0;
 			}
 			count_total++;
-			if (RelChg < o->tol_inn && !fst) break;
+			int end = rp ? rp->inner_end[count_total - 1] || count_total >= rp->count : RelChg < o->tol_inn && !fst;
+			if (iters) iters[count_total - 1].inner_end = end || count_total >= o->maxit;
+			if (end) break;
 			fst = 0;
 		}
 		count_outer++;
 		vadd(n, U, -1, rcdU, UrcdU);
 		RelChgOut = nrm2(n, UrcdU) / nrmup;
 		cpy(n, U, rcdU);
-		if (RelChgOut < o->tol) break;
+		if (rp ? count_total >= rp->count && !rp->inner_end[count_total - 1] : RelChgOut < o->tol) break;
 		update_mlp(s, bs);
 		beta0 = s->beta;
 		s->beta *= o->rate_cnt;
@@ -739,4 +754,16 @@ int orc_solve(int dims, int dim_y, int dim_x, int dim_z, const orc_op *op, const
 	for (size_t i = 0; i < sizeof(mv) / sizeof(mv[0]); i++) free(*mv[i]);
 	free(bs); free(DtsAtd); free(rcdU); free(UrcdU);
 	return 0;
+}
+
+int orc_solve(int dims, int dim_y, int dim_x, int dim_z, const orc_op *op, const double *b, int blen,
+              const orc_opts *opts, const double *Ut, double *U, orc_info *info, orc_iter *iters) {
+	return solve_impl(dims, dim_y, dim_x, dim_z, op, b, blen, opts, Ut, U, info, iters, NULL);
+}
+
+int orc_solve_replay(int dims, int dim_y, int dim_x, int dim_z, const orc_op *op, const double *b, int blen,
+                     const orc_opts *opts, const double *Ut, double *U, orc_info *info, orc_iter *iters,
+                     const orc_replay *replay) {
+	if (!replay || replay->count < 1 || !replay->backtracks || !replay->skipped || !replay->inner_end) return -3;
+	return solve_impl(dims, dim_y, dim_x, dim_z, op, b, blen, opts, Ut, U, info, iters, replay);
 }

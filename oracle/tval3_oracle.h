@@ -36,12 +36,15 @@ typedef struct {
 } orc_info;
 
 /* Per inner iteration record (optional): tau, f after update_W, RelChg, the
- * number of backtracking steps (6 = restart after 5 failures) and whether the
- * descent step skipped the A^T multiplication. */
+ * number of backtracking steps (6 = restart after 5 failures), whether the
+ * descent step skipped the A^T multiplication and whether the inner loop
+ * ended after the iteration. */
 typedef struct {
 	double tau, f, relchg;
 	int backtracks;
 	int skipped;
+	int inner_end;
+	int pad;
 } orc_iter;
 
 /* Operators (all arrays are copied). */
@@ -84,6 +87,29 @@ double orc_shrink(int dims, int n, int tv_norm, double beta, const double *Ux, c
  * records.  Returns 0, or a negative code for argument errors. */
 int orc_solve(int dims, int dim_y, int dim_x, int dim_z, const orc_op *op, const double *b, int blen,
               const orc_opts *opts, const double *Ut, double *U, orc_info *info, orc_iter *iters);
+
+/* Decisions recorded by another solver (for example the GPU's per-iteration
+ * trace), replayed by orc_solve_replay so that the FP64 solve takes the same
+ * discrete path: per iteration k < count, the backtracking steps (0-5, or 6 =
+ * five and the restart), whether the descent skipped the A^T multiplication
+ * (-1: the heuristic decides) and whether the inner loop ended after it
+ * (inner_end[k] = 1: multipliers and continuation updated next).  The solve
+ * stops after `count` iterations; it then also updates the multipliers if
+ * inner_end[count - 1] says so.  This replaces the Armijo test, the skip
+ * heuristic and the inner / outer stopping tests of 2d:790-853; everything
+ * continuous (step lengths, objective, vectors) is computed in FP64 as in
+ * orc_solve.  A test-only device: it lets an FP32 solve be compared with the
+ * FP64 one at the same iteration count and decisions. */
+typedef struct {
+	int count;
+	const int *backtracks;
+	const int *skipped;
+	const int *inner_end;
+} orc_replay;
+
+int orc_solve_replay(int dims, int dim_y, int dim_x, int dim_z, const orc_op *op, const double *b, int blen,
+                     const orc_opts *opts, const double *Ut, double *U, orc_info *info, orc_iter *iters,
+                     const orc_replay *replay);
 
 #ifdef __cplusplus
 }

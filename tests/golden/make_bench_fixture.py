@@ -4,9 +4,12 @@
 
 Solves the 256x256 ring workload (tval3g.workloads.ring2d with normalize=True,
 isotropic TV, maxit 500) with the FP64 oracle restatement and stores U and the
-iteration counts in tests/golden/ring256_fp64.npz.  Also records the
-reference's own float solver on the CSR twin of the same operator with
-anisotropic TV (the reference has no isotropic TV) for the drift statement.
+iteration counts in tests/golden/ring256_fp64.npz, together with the
+anisotropic FP64 solution of the same problem (U_aniso: what the reference,
+which has no isotropic TV, solves) and the first 20 iterations of the literal
+unit-weight ring (normalize=False, U_unit20).  Also records the reference's
+own float solver on the CSR twin of the same operator with anisotropic TV for
+the drift statement.
 The dense 64x64 workload goes to dense64_fp64.npz and the joint 32-layer
 multi-RHS workload to mrhs32_fp64.npz.
 """
@@ -34,17 +37,25 @@ def main():
           f"{time.time() - t:.1f} s")
     out = {"U": r.U.astype(np.float32), "iters": np.array([r.outer_iters, r.total_iters]),
            "scale": np.array([w["geom"]["scale"]]), "b_sum": np.array([float(np.sum(w["b"], dtype=np.float64))])}
+    o = dict(w["opts"])
+    o["tv_norm"] = 0
+    r64 = O.solve(op, w["b"].astype(np.float64), w["shape"], o)
+    print(f"FP64 oracle, anisotropic: {r64.total_iters} iterations")
+    out["U_aniso"] = r64.U.astype(np.float32)
+    out["iters_aniso"] = np.array([r64.outer_iters, r64.total_iters])
     if O.ref_available(2):
-        o = dict(w["opts"])
-        o["tv_norm"] = 0
         A = w["csr"]
-        r64 = O.solve(op, w["b"].astype(np.float64), w["shape"], o)
         cwd = os.getcwd()
         rr = O.ref_solve("csr", w["shape"], w["b"], o, dtype=0, csr=(A["m"], A["n"], A["rowptr"], A["colind"], A["val"]))
         os.chdir(cwd)
         d = float(np.linalg.norm(rr.U.ravel() - r64.U.ravel()) / np.linalg.norm(r64.U))
         print(f"aniso: reference float {rr.total_iters} it vs FP64 oracle {r64.total_iters} it, relerr {d:.2e}")
         out["aniso_ref_f32_vs_fp64"] = np.array([d, rr.total_iters, r64.total_iters])
+    # the literal configuration: unit weight per hit, 20 iterations
+    wu = W.ring2d(seed=1, side=256, T=512, tv_norm=1, maxit=20, tol=1e-5, normalize=False)
+    ru = O.solve(O.Op.ray2d(wu["geom"], 256 * 256), wu["b"].astype(np.float64), wu["shape"], wu["opts"])
+    out["U_unit20"] = ru.U.astype(np.float32)
+    out["iters_unit20"] = np.array([ru.outer_iters, ru.total_iters])
     np.savez_compressed(os.path.join(HERE, "ring256_fp64.npz"), **out)
 
 

@@ -47,7 +47,7 @@ def test_max_over_ranks_gloo():
 def test_reference_arm_under_torchrun():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
            "--master-addr", "127.0.0.1", "--master-port", str(_port()), os.path.join(ROOT, "bench.py"),
-           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--cpu-sample-iters", "2"]
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0"]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [json.loads(line) for line in r.stdout.splitlines() if line.startswith("{")]
@@ -55,3 +55,4 @@ def test_reference_arm_under_torchrun():
     line = lines[0]
     assert line["impl"] == "reference" and line["value"] > 0 and line["cpu_baseline"]["kind"] == "reference"
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+    assert line["steps"] == 1 and line["iterations"] > 1

@@ -195,3 +195,141 @@ def test_shrink_edges():
     n4 = np.hypot(ux[4], uy[4])
     assert abs(ix[4] - (n4 - 0.25) * ux[4] / n4) < 1e-15
     assert ix[2] == 0 and iy[2] == 0
+
+
+@pytest.mark.parametrize("name", ["dense2d_s32_conv", "ring2d_s64_skip", "hemi3d_s16_conv", "dense2d_layers"])
+def test_replay_of_own_decisions_is_identical(name):
+    """The replay mode (the checker for equal-iteration-count parity) follows
+    recorded decisions exactly: replaying the oracle's own decisions gives
+    the same iterations, backtracking steps, skips and bits."""
+    c = build_case(name)
+    b = c["b"].astype(np.float64)
+    r = O.solve(c["oracle_op"], b, c["shape"], c["opts"], record=True)
+    rp = {"count": r.total_iters, "backtracks": [x[3] for x in r.iters], "skipped": [x[4] for x in r.iters],
+          "inner_end": r.inner_end}
+    r2 = O.solve(c["oracle_op"], b, c["shape"], c["opts"], record=True, replay=rp)
+    assert r2.total_iters == r.total_iters and r2.outer_iters == r.outer_iters
+    assert r2.iters == r.iters
+    np.testing.assert_array_equal(r2.U, r.U)
+
+
+def test_replay_takes_the_given_path():
+    """Replayed decisions that differ from the oracle's own (one extra
+    backtracking step, the inner loop ended one iteration early) are taken:
+    the iteration records show them, and the image moves away from the
+    unforced solve."""
+    c = build_case("dense2d_s32_it20")
+    b = c["b"].astype(np.float64)
+    r = O.solve(c["oracle_op"], b, c["shape"], c["opts"], record=True)
+    bt = [x[3] for x in r.iters]
+    end = list(r.inner_end)
+    k = next(i for i in range(2, len(bt)) if bt[i] == 0)
+    bt[k] = 1
+    end[3] = 1
+    r2 = O.solve(c["oracle_op"], b, c["shape"], c["opts"], record=True,
+                 replay={"count": r.total_iters, "backtracks": bt, "skipped": [0] * len(bt), "inner_end": end})
+    assert [x[3] for x in r2.iters] == bt
+    assert r2.inner_end[3] == 1 and r2.total_iters == r.total_iters
+    assert r2.outer_iters > r.outer_iters
+    assert relerr(r2.U, r.U) > 1e-6
+
+
+def test_replay_from_gpu_trace_rows():
+    """replay_from_trace reads the plan trace's columns (backtracks, skipped,
+    outer update flag): the inner loop ends where the multipliers were
+    updated, and at the last iteration."""
+    tr = np.zeros((5, 8))
+    tr[:, 3] = [0, 2, 0, 6, 1]
+    tr[:, 4] = [0, 0, 1, 0, 0]
+    tr[1, 7] = 1
+    rp = O.replay_from_trace(tr)
+    assert rp["count"] == 5
+    assert list(rp["backtracks"]) == [0, 2, 0, 6, 1] and list(rp["skipped"]) == [0, 0, 1, 0, 0]
+    assert list(rp["inner_end"]) == [0, 1, 0, 0, 0]
+
+
+def _ref_matrix_3d(g):
+    """The reference's own 3D projector as a dense count matrix (rays x
+    voxels), read column by column from its forward applied to one-hot voxel
+    vectors (weight 1 per hit)."""
+    g = dict(g, scale=1.0)
+    nvox = int(g["rv_x"]) * int(g["rv_y"]) * int(g["rv_z"])
+    M = np.zeros((int(g["numMPs"]) * int(g["numPaths"]), nvox))
+    e = np.zeros(nvox)
+    for j in range(nvox):
+        e[j] = 1.0
+        M[:, j] = O.ref_project3d(g, e)
+        e[j] = 0.0
+    return M
+
+
+def _list_matrix(op_lists, rows, nvox):
+    ray, off, pix = op_lists
+    M = np.zeros((rows, nvox))
+    for k in range(len(ray)):
+        np.add.at(M[ray[k]], pix[off[k]:off[k + 1]], 1.0)
+    return M
+
+
+def _tie_geometry():
+    p0 = np.array([[0, 0, 0], [0, 0, 0], [0, 0, 0], [5, 5, 5], [1, 2, 3], [7, 0, 3], [3, 3, 3], [0, 7, 7],
+                   [2, 2, 0], [7, 7, 7]])
+    p1 = np.array([[7, 7, 0], [0, 7, 7], [7, 0, 7], [0, 0, 0], [6, 4, 7], [0, 7, 5], [3, 3, 3], [7, 0, 0],
+                   [2, 5, 7], [0, 1, 2]])
+    N = len(p0)
+    return dict(numMPs=1, numPaths=N, E=N, R=N, use_path=(np.eye(N, dtype=np.int32) * np.arange(1, N + 1)).ravel(),
+                xe=p0[:, 0], ye=p0[:, 1], ze=p0[:, 2], xr=p1[:, 0], yr=p1[:, 1], zr=p1[:, 2], rv_x=8, rv_y=8,
+                rv_z=8, scale=1.0)
+
+
+def moment_probes_3d(nvox):
+    """Integer-valued voxel probes whose projections identify each ray's voxel
+    set: the hit count, residues of the voxel index and a multiplicative hash
+    (every projection is an integer well below 2^24, exact in FP32 too)."""
+    j = np.arange(nvox, dtype=np.int64)
+    return [np.ones(nvox), (j % 7).astype(np.float64), (j % 61).astype(np.float64),
+            ((j * 2654435761) % 251).astype(np.float64), ((j // 97) % 13).astype(np.float64)]
+
+
+@pytest.mark.skipif(not O.ref_available_proj3d(), reason="reference not built here")
+def test_bresenham_3d_lists_match_the_reference_projector():
+    """The restated 3D Bresenham lists equal the reference's live projector
+    (3d/mat_mult.h:148-363) hit for hit: on the tie cases and a 12^3
+    hemisphere (one-hot columns), and with two measurement positions."""
+    cases = [_tie_geometry(), W.hemisphere_geometry(12, 24, 8, 5.0, np.random.default_rng(4))]
+    g2 = dict(cases[1])
+    for a, b_ in (("xe", "ye"), ("xr", "yr")):
+        x, y = np.asarray(g2[a]), np.asarray(g2[b_])
+        g2[a] = np.concatenate([x, 11 - y]).astype(np.int32)
+        g2[b_] = np.concatenate([y, x]).astype(np.int32)
+    for a in ("ze", "zr"):
+        g2[a] = np.concatenate([g2[a], g2[a]]).astype(np.int32)
+    g2["numMPs"] = 2
+    cases.append(g2)
+    for g in cases:
+        nvox = int(g["rv_x"]) * int(g["rv_y"]) * int(g["rv_z"])
+        rows = int(g["numMPs"]) * int(g["numPaths"])
+        Mref = _ref_matrix_3d(g)
+        Mor = _list_matrix(O.Op.ray3d(g).ray_lists(), rows, nvox)
+        np.testing.assert_array_equal(Mor, Mref)
+
+
+@pytest.mark.skipif(not O.ref_available_proj3d(), reason="reference not built here")
+def test_bresenham_3d_moments_match_the_reference_projector():
+    """A 48^3 hemisphere of 256 transducers x 128 receivers (32768 rays):
+    per-ray integer moments of the restated lists equal the reference
+    projector's products of the same probes (forward), and per-voxel ray
+    moments its adjoint."""
+    g = W.hemisphere_geometry(48, 256, 128, 23.0, np.random.default_rng(9))
+    nvox = 48 ** 3
+    rows = int(g["numPaths"])
+    ray, off, pix = O.Op.ray3d(g).ray_lists()
+    row_of = np.repeat(ray, np.diff(off))
+    for p in moment_probes_3d(nvox):
+        want = np.zeros(rows)
+        np.add.at(want, row_of, p[pix])
+        np.testing.assert_array_equal(O.ref_project3d(g, p), want)
+    q = ((np.arange(rows, dtype=np.int64) * 40503) % 211).astype(np.float64)
+    want = np.zeros(nvox)
+    np.add.at(want, pix, q[row_of])
+    np.testing.assert_array_equal(O.ref_project3d(g, q, trans=True), want)

@@ -192,9 +192,9 @@ __global__ void __launch_bounds__(256) k_dense_red(const Inst *tab, TileMap map,
 // (cooperative launch).  Every wait is bounded: one that gives up sets *err
 // and the CTA's abort flag, after which no role waits again (every named
 // barrier is still passed the same number of times) and the producer lets
-// its copies in flight land before the CTA exits.  Every product is
-// accumulated in FP64 (as the gemv kernels do) in a fixed order:
-// deterministic.
+// its copies in flight land before the CTA exits.  Products are summed in
+// FP32 over short runs (a thread's share of one chunk of a row; eight rows of
+// a column) and those sums in FP64, in a fixed order: deterministic.
 // ---------------------------------------------------------------------------
 constexpr int FUSED_THREADS = 512;
 constexpr int FUSED_ROLE = 256;                     // reducer threads
@@ -232,7 +232,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_dense_normal(const Inst *t
 	const Inst &I = tab[inst];
 	if (!pred_ok(*I.ctrl, pred)) return;   // the same in every CTA: ctrl is not written here
 	extern __shared__ __align__(128) unsigned char dsm[];
-	__shared__ double sau[FUSED_GRID_MAX * FUSED_RPC_MAX];   // the band's Au (reducers)
+	__shared__ float sauf[FUSED_GRID_MAX * FUSED_RPC_MAX];   // the band's Au (reducers)
+	__shared__ double sau[FUSED_GRID_MAX * FUSED_RPC_MAX];   // the row groups' column sums
 	__shared__ double spart[2][8];                           // consumer warps' row partials
 	__shared__ volatile int s_done, s_abort;                 // bands reduced; a wait gave up
 	const OpDev &op = I.op;
@@ -301,15 +302,20 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_dense_normal(const Inst *t
 					if (!s_abort && !mbar_wait_warp(full0 + 8u * st, (unsigned)(it / FUSED_NS) & 1u, err))
 						if (lane == 0) s_abort = 1;
 					if (!s_abort) {
+						// the thread's few products of this chunk (at most 19
+						// float4) summed in FP32, the chunk sums in FP64: one
+						// conversion per chunk instead of two per element
 						const int cnt4 = min(FUSED_CH, n - ch * FUSED_CH) >> 2;
 						const float4 *sa = stage_a(st), *su = stage_u(st);
+						float pf = 0.f;
 						for (int k = ct; k < cnt4; k += FUSED_CONS) {
 							const float4 av = sa[k], uv = su[k];
-							acc = fma((double)av.x, (double)uv.x, acc);
-							acc = fma((double)av.y, (double)uv.y, acc);
-							acc = fma((double)av.z, (double)uv.z, acc);
-							acc = fma((double)av.w, (double)uv.w, acc);
+							pf = fmaf(av.x, uv.x, pf);
+							pf = fmaf(av.y, uv.y, pf);
+							pf = fmaf(av.z, uv.z, pf);
+							pf = fmaf(av.w, uv.w, pf);
 						}
+						acc += (double)pf;
 					}
 					__syncwarp();
 					if (lane == 0) mbar_arrive(empty0 + 8u * st);
@@ -348,31 +354,37 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_dense_normal(const Inst *t
 				}
 			}
 			named_sync(2, FUSED_ROLE);
-			for (int k = t; k < rows; k += FUSED_ROLE) sau[k] = (double)__ldcg(au + r0 + k);
+			for (int k = t; k < rows; k += FUSED_ROLE) sauf[k] = __ldcg(au + r0 + k);
 			named_sync(2, FUSED_ROLE);
 			if (act && !s_abort) {
+				// eight rows' products summed in FP32, those sums in FP64
 				const float *a = A + (long long)r0 * n + c0 + 4 * j;
 				int r = q;
 				for (; r + 7 * Q < rows; r += 8 * Q) {
 					float4 v[8];
 #pragma unroll
 					for (int e = 0; e < 8; e++) v[e] = *reinterpret_cast<const float4 *>(a + (long long)(r + e * Q) * n);
+					float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
 #pragma unroll
 					for (int e = 0; e < 8; e++) {
-						const double w = sau[r + e * Q];
-						acc[0] = fma((double)v[e].x, w, acc[0]);
-						acc[1] = fma((double)v[e].y, w, acc[1]);
-						acc[2] = fma((double)v[e].z, w, acc[2]);
-						acc[3] = fma((double)v[e].w, w, acc[3]);
+						const float w = sauf[r + e * Q];
+						p0 = fmaf(v[e].x, w, p0);
+						p1 = fmaf(v[e].y, w, p1);
+						p2 = fmaf(v[e].z, w, p2);
+						p3 = fmaf(v[e].w, w, p3);
 					}
+					acc[0] += (double)p0;
+					acc[1] += (double)p1;
+					acc[2] += (double)p2;
+					acc[3] += (double)p3;
 				}
 				for (; r < rows; r += Q) {
-					const double w = sau[r];
+					const float w = sauf[r];
 					const float4 v = *reinterpret_cast<const float4 *>(a + (long long)r * n);
-					acc[0] = fma((double)v.x, w, acc[0]);
-					acc[1] = fma((double)v.y, w, acc[1]);
-					acc[2] = fma((double)v.z, w, acc[2]);
-					acc[3] = fma((double)v.w, w, acc[3]);
+					acc[0] += (double)(v.x * w);
+					acc[1] += (double)(v.y * w);
+					acc[2] += (double)(v.z * w);
+					acc[3] += (double)(v.w * w);
 				}
 			}
 			named_sync(2, FUSED_ROLE);
