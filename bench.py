@@ -20,12 +20,23 @@ the reference's own stopping rules end it.
   roofline  the dominant kernel timed alone with CUDA events after an L2
           flush, algorithmic bytes / time against the measured HBM copy rate
   cpu_baseline  the reference solver itself (oracle/_ref, compiled from its
-          own sources) on the CSR twin, a bounded sample of iterations
+          own sources) on the CSR twin: one complete solve under its own
+          stopping rules (anisotropic TV: the reference has no isotropic TV)
+  aniso   the same workload with anisotropic TV on the GPU (the reference
+          arm's problem): time to relerr <= 1e-3 and the full solve
+  unit_weight  the literal unit-weight ring, a fixed 20 iterations, against
+          the FP64 oracle's 20 iterations
+  batch   the mixed batch of 64 independent 2D problems (58 GB of dense A
+          drawn on the device from seeded counter-based streams): the
+          batched graph against the plain one-instance-per-launch form, the
+          HBM floor of its dense instances, and the relerr of each instance
+          of its FP64 subset
 
---workload dense2d | hemi3d | batch measures the plain dense 64x64 problem,
-the 128^3 hemisphere and the mixed batch of 64 independent 2D problems
-(batched graph vs plain one-instance-per-launch).
---impl reference runs only the reference CPU solver on the default workload.
+--workload dense2d | hemi3d | batch | mrhs | unrolled measures the plain dense
+64x64 problem, the 128^3 hemisphere, the mixed batch alone, the joint
+multi-RHS solve and the differentiable unrolled solve.
+--impl reference runs only the reference CPU solver (complete solves, at most
+three timed) on the default workload.
 Multi-GPU (torchrun): every rank solves its own replica (no collective in the
 data path); value = total reconstructions / max-over-ranks time.
 """
@@ -52,10 +63,13 @@ def args_():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="tval3g", choices=["tval3g", "reference"])
-    p.add_argument("--workload", default="ring2d", choices=["ring2d", "dense2d", "hemi3d", "batch", "mrhs"])
+    p.add_argument("--workload", default="ring2d",
+                   choices=["ring2d", "dense2d", "hemi3d", "batch", "mrhs", "unrolled"])
     p.add_argument("--profile", action="store_true",
                    help="for ncu: build the plan, run --warmup + --steps solves, print nothing else")
     p.add_argument("--maxit", type=int, default=None, help="override maxit (profiling a short solve)")
+    p.add_argument("--no-batch", action="store_true",
+                   help="ring workload: leave out the mixed-batch sub-record (64 problems, 58 GB of dense A)")
     p.add_argument("--tune", action="store_true",
                    help="single-instance workloads: operators built with the launch-shape autotuner")
     p.add_argument("--plain", action="store_true",
@@ -89,6 +103,10 @@ CONFIGS = {
     "mrhs": {"workload": "dense A 4096 x 16384 N(0,1/m), 32 right-hand sides (128x128 phantoms) solved jointly as "
                          "32 layers, iso TV, mu 2^8, beta 2^5, tol 1e-4, maxit 300",
              "operator": "tcgen05 3xTF32 multi-RHS product (TMA, TMEM, stream-K over all SMs)"},
+    "unrolled": {"workload": "differentiable unrolled solve: 8 phantoms of 128x128 on the ring of 256 transducers x "
+                             "128 receivers (32768 rays), K = 50 iterations with per-iteration (mu_k, beta_k), "
+                             "checkpoint every 10, loss 0.5 |u_K - u_true|^2, gradients w.r.t. b, mu_k, beta_k",
+                 "operator": "on-the-fly Bresenham projector; hand-written adjoint of the unrolled iterations"},
     "batch": {"workload": "64 independent 2D problems, sides {64..256}, dense Gaussian (25-40 % sampling) or ring "
                           "Bresenham (128-512 transducers)",
               "operator": "mixed dense / ray, one batched plan"},
@@ -412,6 +430,10 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
     in_bytes = int(b_host.nbytes + sum(x.nbytes for x in spec.keep))
 
     extra = ring_variants(a, cx, capi, ref) if name == "ring2d" else {}
+    if name == "ring2d" and not a.no_batch:
+        # the metric's "batched vs plain" on the mixed batch (cfg3(i) of the
+        # reference configurations), measured in the same run
+        extra["batch"] = batch_measure(a, cx, capi, dist)
 
     line = {"metric": METRIC, "value": world * 1000.0 / ms, "unit": "reconstructions/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -574,52 +596,121 @@ def run_mrhs(a, cx, capi, world, dist, clocks):
             "clocks": clk, "gpu_launches": launches}
 
 
+def run_unrolled(a, cx, capi, world, dist, clocks):
+    """A step is one forward (K = 50 iterations, 8 instances) and one
+    backward (the gradients of the loss w.r.t. b, mu_k and beta_k) through
+    tval3g_unrolled_*; reported as differentiated reconstructions per second."""
+    from tval3g import workloads as W
+    torch, dev, s = cx.torch, cx.dev, cx.stream.cuda_stream
+    side, T, count, K, ckpt = 128, 256, 8, 50, 10
+    ws = [W.ring2d(seed=11 + i, side=side, T=T, tv_norm=1, normalize=True) for i in range(count)]
+    spec = capi.ray2d_problem((side, side), ws[0]["geom"])
+    opts = W.options(2 ** 8, 2 ** 5, 1e-4, K, tv_norm=1)
+    h = capi.Unrolled(spec, count, opts, K, ckpt=ckpt)
+    mu, beta = 2.0 ** 8 * np.ones(K), 2.0 ** 5 * np.ones(K)
+    d_b = [torch.tensor(w["b"].astype(np.float32), device=dev) for w in ws]
+    d_ut = [torch.tensor(w["u_true"].ravel().astype(np.float32), device=dev) for w in ws]
+    d_U = [torch.empty(spec.n, device=dev) for _ in range(count)]
+    d_gU = [torch.empty(spec.n, device=dev) for _ in range(count)]
+    d_gb = [torch.empty(len(w["b"]), device=dev) for w in ws]
+
+    def fwd():
+        h.forward(d_b, mu, beta, d_U, stream=s)
+
+    def bwd():
+        for u, t, gu in zip(d_U, d_ut, d_gU):
+            torch.sub(u, t, out=gu)   # d loss / d U for 0.5 |U - u_true|^2
+        return h.backward(d_gU, d_gb, stream=s)
+
+    for _ in range(max(a.warmup, 3)):
+        fwd()
+        bwd()
+    if dist:
+        dist.barrier()
+    clocks.start()
+    tf, tb = [], []
+    for _ in range(a.steps):
+        t1, _ = cx.event_time(fwd, 1)
+        t2, g = cx.event_time(bwd, 1)
+        tf += t1
+        tb += t2
+    clk = clocks.stop()
+    ms_f, ms_b = max_over_ranks(dist, [float(np.mean(tf)), float(np.mean(tb))], dev)
+    loss = float(sum(0.5 * float(torch.sum((u - t) ** 2)) for u, t in zip(d_U, d_ut)))
+    h.close()
+    ms = ms_f + ms_b
+    return {"metric": METRIC, "value": world * count * 1000.0 / ms, "unit": "differentiated reconstructions/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 scalar reductions)",
+            "data": "synthetic (seeded phantoms, noise)",
+            "config": dict(CONFIGS["unrolled"], instances=count, K=K, checkpoint=ckpt,
+                           l2="256 MB write before each timed call"),
+            "forward_ms": ms_f, "backward_ms": ms_b, "loss": loss,
+            "grad_mu_norm": float(np.linalg.norm(g[0])), "grad_beta_norm": float(np.linalg.norm(g[1])),
+            "clocks": clk}
+
+
 def batch_problems(capi, torch, dev):
-    """Materialise the mixed batch: dense A drawn on the device (seeded),
-    ring geometries and data on the host."""
+    """Materialise the mixed batch: each dense A drawn on the device from its
+    instance seed (tval3g_gaussian; the oracle regenerates the same stream on
+    the host), b from the library's dense forward; ring geometries and data
+    on the host."""
     from tval3g import workloads as W
     specs, opts, bs, keep = [], [], [], []
     for k, d in enumerate(W.batch_specs()):
-        side = d["side"]
-        n = side * side
-        rng = np.random.default_rng(d["seed"])
         if d["kind"] == "dense":
-            m = int(round(d["sampling"] * n))
-            u = W.ellipse_phantom(side, side, rng, 5, 0.0, lambda r: r.uniform(0.2, 1.0), (side / 16, side / 3.2))
-            g = torch.Generator(device=dev)
-            g.manual_seed(d["seed"])
-            A = torch.randn(m, n, device=dev, generator=g).mul_(1.0 / np.sqrt(m))
-            y = (A @ torch.tensor(u.ravel(), dtype=torch.float32, device=dev)).double().cpu().numpy()
-            b = W.add_noise(y, 0.01, rng).astype(np.float32)
-            spec = capi.dense_problem((side, side), A, device_ptr=A.data_ptr())
+            p = W.batch_dense_parts(d)
+            A = torch.empty(p["m"], p["n"], device=dev)
+            capi.gaussian(A, d["seed"], p["scale"])
+            spec = capi.dense_problem(p["shape"], A, device_ptr=A.data_ptr())
+            op = capi.Operator(spec, device_inputs=True)
+            y = torch.empty(p["m"], device=dev)
+            op.apply(torch.tensor(p["u_true"].ravel().astype(np.float32), device=dev), y)
+            op.close()
+            b = W.add_noise(y.cpu().numpy().astype(np.float64), 0.01, p["rng"]).astype(np.float32)
             keep.append(A)
-            o = W.options(2 ** 8, 2 ** 5, 1e-4, 300, tv_norm=1)
+            o = p["opts"]
         else:
-            w = W.ring2d(seed=d["seed"], side=side, T=d["T"], tv_norm=1, maxit=500, tol=1e-5, normalize=True)
-            spec, b, o = capi.ray2d_problem((side, side), w["geom"]), w["b"], w["opts"]
+            w = W.batch_ray(d)
+            spec, b, o = capi.ray2d_problem(w["shape"], w["geom"]), w["b"], w["opts"]
         specs.append(spec)
         bs.append(torch.tensor(np.ascontiguousarray(b, np.float32), device=dev))
         opts.append(o)
     return specs, opts, bs, keep
 
 
-def run_batch(a, cx, capi, world, dist, clocks):
+def batch_measure(a, cx, capi, dist, clocks=None, ray_subset=True):
+    """The mixed batch of 64 independent 2D problems: the batched graph (one
+    plan, one launch per kernel over all instances) against the plain form
+    (one plan per instance, host-driven loop, instances in sequence), with
+    each instance of the FP64 subset (tests/golden/batch_fp64.npz) checked
+    against its FP64 solution."""
     torch, dev, stream = cx.torch, cx.dev, cx.stream
     specs, opts, bs, keep = batch_problems(capi, torch, dev)
     us = [torch.empty(s.n, device=dev) for s in specs]
     nb = len(specs)
+    fx = os.path.join(GOLDEN, "batch_fp64.npz")
+    fx = dict(np.load(fx)) if os.path.exists(fx) else {}
+    uts = [None] * nb
+    for k in range(nb):
+        if f"U{k}" in fx:
+            uts[k] = torch.tensor(fx[f"U{k}"].ravel().astype(np.float32), device=dev)
+    have_ut = [k for k in range(nb) if uts[k] is not None]
     plan = capi.Plan(specs, opts, graph=True, device_inputs=True)
-    solve = lambda: plan.solve(bs, us, stream=stream.cuda_stream)  # noqa: E731
-    cx.event_time(solve, max(1, a.warmup))
+    solve = lambda: plan.solve(bs, us, d_Ut=uts, stream=stream.cuda_stream)  # noqa: E731
+    cx.event_time(solve, max(1, min(a.warmup, 2)))
     if dist:
         dist.barrier()
-    clocks.start()
-    tb, infos = cx.event_time(solve, a.steps)
+    if clocks:
+        clocks.start()
+    tb, infos = cx.event_time(solve, max(1, min(a.steps, 3)))
     launches = plan.stats()["kernel_launches"]
-    clk = clocks.stop()
+    clk = clocks.stop() if clocks else None
     ms_b = float(np.mean(tb))
     device_bytes = plan.stats()["device_bytes"]
     plan.close()
+    rel = {k: float(infos[k]["rel_error"]) for k in have_ut}
+    fp64_iters = {k: int(fx[f"iters{k}"][1]) for k in have_ut}
     # plain: one instance per plan, host-driven loop, instances one after another
     singles = [capi.Plan([s], [o], graph=False, device_inputs=True) for s, o in zip(specs, opts)]
 
@@ -642,7 +733,7 @@ def run_batch(a, cx, capi, world, dist, clocks):
     # the ray instances alone: where batching removes launch and latency cost
     rays = [k for k, s in enumerate(specs) if s.p.op_kind != capi.OP_DENSE]
     sub = {}
-    if rays:
+    if rays and ray_subset:
         rplan = capi.Plan([specs[k] for k in rays], [opts[k] for k in rays], graph=True, device_inputs=True)
         rsolve = lambda: rplan.solve([bs[k] for k in rays], [us[k] for k in rays], stream=stream.cuda_stream)  # noqa: E731
         cx.event_time(rsolve, 1)
@@ -659,16 +750,35 @@ def run_batch(a, cx, capi, world, dist, clocks):
             p.close()
         sub = {"instances": len(rays), "batched_ms": float(np.mean(trb)), "plain_ms": float(np.mean(trp)),
                "batched_over_plain": float(np.mean(trp)) / float(np.mean(trb))}
-    return {"metric": METRIC, "value": world * nb * 1000.0 / ms_b, "unit": "reconstructions/s", "n_gpus": world,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_b, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantoms and operators)",
-            "config": dict(CONFIGS["batch"], instances=nb, dense_instances=dense,
-                           dense_bytes=int(dense_bytes), plan_device_bytes=int(device_bytes)),
-            "plain": {"value": world * nb * 1000.0 / ms_p, "unit": "reconstructions/s", "ms_per_step": ms_p,
+    del keep
+    return {"instances": nb, "dense_instances": dense, "dense_bytes": int(dense_bytes),
+            "plan_device_bytes": int(device_bytes), "batched_ms": ms_b, "plain_ms": ms_p,
+            "batched_over_plain": ms_p / ms_b, "value": nb * 1000.0 / ms_b, "unit": "reconstructions/s",
+            "plain_value": nb * 1000.0 / ms_p, "iterations_min_max": [min(iters), max(iters)],
+            "dense_hbm_floor_ms": floor_ms, "batched_over_floor": ms_b / floor_ms,
+            "relerr_vs_fp64": {"instances_checked": len(rel), "max": max(rel.values()) if rel else None,
+                               "within_1e-3": sum(1 for v in rel.values() if v <= 1e-3),
+                               "per_instance": {str(k): round(v, 6) for k, v in rel.items()},
+                               "iterations_gpu_vs_fp64": {str(k): [iters[k], fp64_iters[k]] for k in rel},
+                               "subset": "the ring instances of side <= 192 and the dense ones of side <= 96 "
+                                         "(tests/golden/batch_fp64.npz)"},
+            "ray_instances_only": sub, "clocks": clk, "gpu_launches": launches}
+
+
+def run_batch(a, cx, capi, world, dist, clocks):
+    r = batch_measure(a, cx, capi, dist, clocks)
+    return {"metric": METRIC, "value": world * r["value"], "unit": "reconstructions/s", "n_gpus": world,
+            "steps": max(1, min(a.steps, 3)), "warmup": max(1, min(a.warmup, 2)), "ms_per_step": r["batched_ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded phantoms and operators)",
+            "config": dict(CONFIGS["batch"], instances=r["instances"], dense_instances=r["dense_instances"],
+                           dense_bytes=r["dense_bytes"], plan_device_bytes=r["plan_device_bytes"]),
+            "plain": {"value": world * r["plain_value"], "unit": "reconstructions/s", "ms_per_step": r["plain_ms"],
                       "form": "one plan per instance, host-driven loop, instances in sequence"},
-            "batched_over_plain": ms_p / ms_b, "iterations_min_max": [min(iters), max(iters)],
-            "dense_hbm_floor_ms": floor_ms, "ray_instances_only": sub,
-            "clocks": clk, "gpu_launches": launches}
+            "batched_over_plain": r["batched_over_plain"], "iterations_min_max": r["iterations_min_max"],
+            "dense_hbm_floor_ms": r["dense_hbm_floor_ms"], "batched_over_floor": r["batched_over_floor"],
+            "relerr_vs_fp64": r["relerr_vs_fp64"], "ray_instances_only": r["ray_instances_only"],
+            "clocks": r["clocks"], "gpu_launches": r["gpu_launches"]}
 
 
 def main():
@@ -701,6 +811,8 @@ def main():
         line = run_batch(a, cx, capi, world, dist, clocks)
     elif a.workload == "mrhs":
         line = run_mrhs(a, cx, capi, world, dist, clocks)
+    elif a.workload == "unrolled":
+        line = run_unrolled(a, cx, capi, world, dist, clocks)
     else:
         line = run_single(a, cx, capi, a.workload, world, rank, dist, clocks)
     if rank == 0 and line is not None:

@@ -251,6 +251,19 @@ int tval3g_unrolled_backward(tval3g_unrolled *h, const float *const *d_gU, float
 int tval3g_unrolled_decisions(const tval3g_unrolled *h, int index, double *steps, int *outer, double *scl);
 int tval3g_unrolled_destroy(tval3g_unrolled *h);
 
+/* Seeded Gaussian streams (no counterpart in the reference; its callers
+ * bring their own data): out[i] = scale * z(seed, offset + i) for i < count,
+ * z a standard normal value from the counter-based Philox-4x32-10 generator
+ * with a Box-Muller transform in FP64, rounded to FP32.  tval3g_gaussian
+ * writes DEVICE memory on `stream` (stream-ordered); tval3g_gaussian_host
+ * computes the same stream on the host.  The integer streams are identical;
+ * an element may differ by one FP32 unit in the last place between the two
+ * when the math libraries' FP64 log / sin / cos round differently. */
+int tval3g_gaussian(unsigned long long seed, unsigned long long offset, long long count, float scale,
+                    float *d_out, void *stream);
+int tval3g_gaussian_host(unsigned long long seed, unsigned long long offset, long long count, float scale,
+                         float *out);
+
 /* y = A^T x for a dense row-major m x n float matrix, with DEVICE pointers,
  * for callers that cannot allocate device memory at call time (for example
  * when another allocator has reserved the device's memory, or when a

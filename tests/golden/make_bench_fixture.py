@@ -1,6 +1,6 @@
 """FP64 solutions of the benchmark workloads (bench.py), for their relerr checks.
 
-    python tests/golden/make_bench_fixture.py [ring] [dense64] [mrhs]
+    python tests/golden/make_bench_fixture.py [ring] [dense64] [mrhs] [batch]
 
 Solves the 256x256 ring workload (tval3g.workloads.ring2d with normalize=True,
 isotropic TV, maxit 500) with the FP64 oracle restatement and stores U and the
@@ -11,7 +11,10 @@ unit-weight ring (normalize=False, U_unit20).  Also records the reference's
 own float solver on the CSR twin of the same operator with anisotropic TV for
 the drift statement.
 The dense 64x64 workload goes to dense64_fp64.npz and the joint 32-layer
-multi-RHS workload to mrhs32_fp64.npz.
+multi-RHS workload to mrhs32_fp64.npz.  The mixed batch's FP64 subset (its
+ring instances of side <= 192 and its dense instances of side <= 96, dense A
+regenerated from the counter-based Gaussian stream the bench draws on the
+device) goes to batch_fp64.npz as U<k>, iters<k> per batch index k.
 """
 import os
 import sys
@@ -82,11 +85,32 @@ def mrhs():
                         iters=np.array([r.outer_iters, r.total_iters]))
 
 
+def batch():
+    out = {}
+    t0 = time.time()
+    for k, d in enumerate(W.batch_specs()):
+        if d["kind"] == "dense" and d["side"] <= 96:
+            w = W.batch_dense_host(d)
+            op = O.Op.dense(w["A"].astype(np.float64))
+        elif d["kind"] == "ray2d" and d["side"] <= 192:
+            w = W.batch_ray(d)
+            op = O.Op.ray2d(w["geom"], d["side"] ** 2)
+        else:
+            continue
+        r = O.solve(op, w["b"].astype(np.float64), w["shape"], w["opts"])
+        out[f"U{k}"] = r.U.astype(np.float32)
+        out[f"iters{k}"] = np.array([r.outer_iters, r.total_iters])
+        print(f"batch {k}: {d['kind']} side {d['side']}: {r.total_iters} iterations ({time.time() - t0:.0f} s)")
+    np.savez_compressed(os.path.join(HERE, "batch_fp64.npz"), **out)
+
+
 if __name__ == "__main__":
-    parts = sys.argv[1:] or ["ring", "dense64", "mrhs"]
+    parts = sys.argv[1:] or ["ring", "dense64", "mrhs", "batch"]
     if "ring" in parts:
         main()
     if "dense64" in parts:
         dense64()
     if "mrhs" in parts:
         mrhs()
+    if "batch" in parts:
+        batch()

@@ -114,3 +114,32 @@ def test_complex_argument_errors():
     with pytest.raises(capi.TVAL3Error) as e:
         capi.solve(spec, np.zeros(6, np.complex64), _opts())
     assert str(e.value) == "Argument error: b.len must be equal to A.dim_y!"
+
+
+def test_philox_known_answers():
+    """The counter-based generator's core against the published Philox-4x32-10
+    known-answer vectors (Salmon et al., SC 2011; counter, key -> output)."""
+    kat = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+           ((0xffffffff,) * 4, (0xffffffff,) * 2, (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+           ((0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344), (0xa4093822, 0x299f31d0),
+            (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1))]
+    for c, k, want in kat:
+        got = W.philox4x32_10([np.array([v], np.uint64) for v in c], k)
+        assert tuple(int(x[0]) for x in got) == want
+
+
+@pytest.mark.parametrize("seed,offset,count,scale", [(0, 0, 1000, 1.0), (12345678901, 7, 5001, 0.25),
+                                                     ((1 << 40) + 3, (1 << 33) + 1, 4099, 0.125)])
+def test_gaussian_host_equals_numpy(seed, offset, count, scale):
+    """tval3g_gaussian_host (C++) and the numpy restatement give the same
+    stream bit for bit; any window of it equals the same slice of a longer
+    draw (counter-based: offsets compose)."""
+    h = capi.gaussian_host(count, seed, scale, offset)
+    np.testing.assert_array_equal(h, W.philox_gaussian(seed, count, scale, offset))
+    np.testing.assert_array_equal(capi.gaussian_host(count - 5, seed, scale, offset + 5), h[5:])
+
+
+def test_gaussian_stream_statistics():
+    z = capi.gaussian_host(1 << 20, 99)
+    assert abs(z.mean()) < 5e-3 and abs(z.std() - 1) < 5e-3
+    assert abs(np.mean(z ** 4) - 3) < 0.05   # Gaussian kurtosis

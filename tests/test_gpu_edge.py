@@ -93,3 +93,30 @@ def test_two_by_two_by_two_volume(torch_cuda):
              xr=pts[:, 0], yr=pts[:, 1], zr=pts[:, 2], rv_x=2, rv_y=2, rv_z=2, scale=0.5)
     b = np.random.default_rng(5).uniform(0.5, 1.5, k - 1).astype(np.float32)
     _check(capi.ray3d_problem((2, 2, 2), g), O.Op.ray3d(g), b, (2, 2, 2), _opts())
+
+
+def test_bounded_wait_timeout_reports_and_recovers(torch_cuda, monkeypatch):
+    """The failure path of the bounded device waits, without a fault: with
+    the test hook TVAL3G_TEST_FIRST_WAIT_POLLS=0 the tiled ray adjoint's first
+    wait (its ray list) gives up at once; the kernel drains its bulk copies in
+    flight, raises the operator's error word and returns, and the solve
+    reports TVAL3G_ERR_CUDA.  A plan built afterwards, without the hook,
+    solves normally in the same process: bit for bit the solve made before
+    the failure."""
+    from golden.cases import api_problem, build_case
+    torch = torch_cuda
+    c = build_case("ring2d_s64_it20")
+    spec = api_problem(c, capi)
+    U0, info0 = capi.solve(spec, c["b"], c["opts"])
+    monkeypatch.setenv("TVAL3G_TEST_FIRST_WAIT_POLLS", "0")
+    plan = capi.Plan([spec], [dict(c["opts"], maxit=5)], graph=True)
+    monkeypatch.delenv("TVAL3G_TEST_FIRST_WAIT_POLLS")
+    db = [torch.tensor(c["b"], device="cuda")]
+    du = [torch.empty(spec.n, device="cuda")]
+    with pytest.raises(capi.TVAL3Error) as e:
+        plan.solve(db, du)
+    assert e.value.code == capi.ERR_CUDA and "bounded wait" in str(e.value)
+    plan.close()
+    U1, info1 = capi.solve(spec, c["b"], c["opts"])
+    assert info1["status"] == 0 and info1["total_iters"] == info0["total_iters"] == 20
+    np.testing.assert_array_equal(U1, U0)

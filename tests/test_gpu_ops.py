@@ -254,3 +254,19 @@ def test_hemi128_products_match_the_reference_projector(torch_cuda):
     op.apply(_dev(torch, q), dx, trans=True)
     np.testing.assert_array_equal(dx.cpu().numpy().astype(np.float64), O.ref_project3d(g, q, trans=True))
     op.close()
+
+
+def test_gaussian_device_equals_host(torch_cuda):
+    """tval3g_gaussian on the device gives the host stream: the integer
+    streams are identical and every element agrees to one FP32 unit in the
+    last place (the FP64 log / sin / cos of the two math libraries), almost
+    all of them bit for bit."""
+    torch = torch_cuda
+    for seed, off, cnt, sc in [(5, 0, 1 << 20, 1.0), ((1 << 35) + 11, 3, 100003, 1 / 64.0)]:
+        d = torch.empty(cnt, device="cuda")
+        capi.gaussian(d, seed, sc, off)
+        got = d.cpu().numpy()
+        want = capi.gaussian_host(cnt, seed, sc, off)
+        ulp = np.abs(got.view(np.int32).astype(np.int64) - want.view(np.int32).astype(np.int64))
+        print(f"seed {seed}: {np.count_nonzero(ulp)} of {cnt} elements differ (max {ulp.max()} ulp)")
+        assert ulp.max() <= 1 and np.count_nonzero(ulp) <= cnt * 1e-4

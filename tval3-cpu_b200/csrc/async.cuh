@@ -50,9 +50,10 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned
 constexpr unsigned ASYNC_WAIT_LIMIT = 1u << 22;   // polls before a wait gives up
 
 // every lane of the warp polls phase `parity` of bar; false (after raising
-// *err from lane 0) if it does not complete within ASYNC_WAIT_LIMIT polls
-__device__ __forceinline__ bool mbar_wait_warp(unsigned bar, unsigned parity, int *err) {
-	for (unsigned i = 0; i < ASYNC_WAIT_LIMIT; i++)
+// *err from lane 0) if it does not complete within `limit` polls
+__device__ __forceinline__ bool mbar_wait_warp(unsigned bar, unsigned parity, int *err,
+                                               unsigned limit = ASYNC_WAIT_LIMIT) {
+	for (unsigned i = 0; i < limit; i++)
 		if (__all_sync(0xffffffffu, mbar_try(bar, parity))) return true;
 	if ((threadIdx.x & 31) == 0) atomicExch(err, 1);
 	return false;

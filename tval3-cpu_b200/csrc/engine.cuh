@@ -162,6 +162,13 @@ struct OpDev {
 	// the forward (CSR rows) and of the adjoint (CSC columns, 3D ray index)
 	int fwd_lanes;
 	int gcls_fwd, gcls_adj;
+	// polls of the tiled 2D adjoint's first wait (its ray list), plus one;
+	// 0 = the normal limit.  Set only by the failure-path test hook
+	// TVAL3G_TEST_FIRST_WAIT_POLLS, read when the operator is prepared: with
+	// it the wait gives up and the error path (copies in flight drained at
+	// the normal limit, error word raised, TVAL3G_ERR_CUDA) runs without a
+	// fault or an unbounded wait.
+	unsigned first_wait_polls;
 };
 
 #ifndef TVAL3G_RAYT

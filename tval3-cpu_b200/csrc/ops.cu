@@ -744,7 +744,7 @@ __global__ void __launch_bounds__(RAYT_ADJ_THREADS) k_ray_adj_tiled(const Inst *
 	}
 	__syncthreads();   // barrier initialisation seen by every thread
 	const float *y = vsel(I, xs);
-	bool ok = mbar_wait_warp(bar_list, 0u, err);
+	bool ok = mbar_wait_warp(bar_list, 0u, err, op.first_wait_polls ? op.first_wait_polls - 1u : ASYNC_WAIT_LIMIT);
 	if (ok) {   // eight independent gathers in flight per thread
 		constexpr int U8 = 8;
 		int k = threadIdx.x;

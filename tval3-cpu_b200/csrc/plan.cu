@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "plan.cuh"
@@ -374,6 +375,8 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 			if (build_tiled_index(s, (int)p.ld, (int)(n / p.ld), d.nrays, cptr, cind, lo, d, &ib, st.owned)) {
 				st.bytes += ib;
 				st.adj_index_bytes = ib;
+				if (const char *e = std::getenv("TVAL3G_TEST_FIRST_WAIT_POLLS"))   // failure-path test hook
+					d.first_wait_polls = 1u + (unsigned)std::strtoul(e, nullptr, 10);
 			}
 		}
 		if (!d.tiled) {   // pixel-major gather over measurement indices

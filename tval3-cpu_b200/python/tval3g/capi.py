@@ -104,6 +104,9 @@ def lib():
         L.tval3g_unrolled_backward.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(d), C.POINTER(d), vp]
         L.tval3g_unrolled_decisions.argtypes = [vp, i, C.POINTER(d), C.POINTER(i), C.POINTER(d)]
         L.tval3g_unrolled_destroy.argtypes = [vp]
+        u64 = C.c_ulonglong
+        L.tval3g_gaussian.argtypes = [u64, u64, ll, C.c_float, vp, vp]
+        L.tval3g_gaussian_host.argtypes = [u64, u64, ll, C.c_float, vp]
         _LIB = L
     return _LIB
 
@@ -111,6 +114,20 @@ def lib():
 def _check(rc):
     if rc != OK:
         raise TVAL3Error(rc, lib().tval3g_last_error().decode())
+
+
+def gaussian(d_out, seed, scale=1.0, offset=0, stream=None):
+    """Fill the device tensor d_out (float32, contiguous) with the seeded
+    Gaussian stream scale * z(seed, offset + i) (tval3g_gaussian)."""
+    _check(lib().tval3g_gaussian(int(seed), int(offset), int(d_out.numel()), float(scale), d_out.data_ptr(),
+                                 _dptr(stream)))
+
+
+def gaussian_host(count, seed, scale=1.0, offset=0):
+    """The same stream computed on the host (tval3g_gaussian_host)."""
+    out = np.empty(int(count), np.float32)
+    _check(lib().tval3g_gaussian_host(int(seed), int(offset), int(count), float(scale), out.ctypes.data))
+    return out
 
 
 def trim_memory(keep_bytes=0):

@@ -33,6 +33,49 @@ import numpy as np
 # --------------------------------------------------------------------------
 
 
+# --------------------------------------------------------------------------
+# counter-based Gaussian streams (the library's tval3g_gaussian, in numpy)
+# --------------------------------------------------------------------------
+_PH_M0, _PH_M1, _PH_W0, _PH_W1 = 0xD2511F53, 0xCD9E8D57, 0x9E3779B9, 0xBB67AE85
+_M32 = np.uint64(0xFFFFFFFF)
+
+
+def philox4x32_10(c, key):
+    """Philox-4x32-10 (Salmon, Moraes, Dror and Shaw, SC 2011) on arrays of
+    counters: c = four uint32 arrays, key = (k0, k1); returns four uint64
+    arrays holding the 32-bit output words."""
+    c0, c1, c2, c3 = (np.asarray(x, np.uint64) for x in c)
+    k0, k1 = np.uint64(key[0]), np.uint64(key[1])
+    for _ in range(10):
+        p0 = np.uint64(_PH_M0) * c0
+        p1 = np.uint64(_PH_M1) * c2
+        c0, c1, c2, c3 = (p1 >> np.uint64(32)) ^ c1 ^ k0, p1 & _M32, (p0 >> np.uint64(32)) ^ c3 ^ k1, p0 & _M32
+        k0 = (k0 + np.uint64(_PH_W0)) & _M32
+        k1 = (k1 + np.uint64(_PH_W1)) & _M32
+    return c0, c1, c2, c3
+
+
+def philox_gaussian(seed, count, scale=1.0, offset=0):
+    """float32 array: element i = scale * z(seed, offset + i), the stream of
+    tval3g_gaussian (Philox-4x32-10 counter blocks, Box-Muller in FP64)."""
+    e = np.arange(offset, offset + count, dtype=np.uint64)
+    blocks = np.unique(e >> np.uint64(2))
+    j = blocks
+    x = philox4x32_10((j & _M32, j >> np.uint64(32), np.zeros_like(j), np.zeros_like(j)),
+                      (seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF))
+    q = 1.0 / 16777216.0
+    z = np.empty((len(j), 4))
+    two_pi = 6.283185307179586476925286766559
+    for p in range(2):
+        u1 = ((x[2 * p] >> np.uint64(8)) + np.uint64(1)).astype(np.float64) * q
+        t = (x[2 * p + 1] >> np.uint64(8)).astype(np.float64) * q
+        r = np.sqrt(-2.0 * np.log(u1))
+        z[:, 2 * p] = r * np.cos(two_pi * t)
+        z[:, 2 * p + 1] = r * np.sin(two_pi * t)
+    zz = z[(e >> np.uint64(2)) - blocks[0], (e & np.uint64(3)).astype(np.int64)]
+    return (zz * np.float64(np.float32(scale))).astype(np.float32)
+
+
 def options(mu, beta, tol, maxit, tv_norm=1, nonneg=False, tol_inn=1e-3, maxcnt=10, **kw):
     """A full TVAL3 option set (every field set explicitly)."""
     o = dict(mu=float(mu), beta=float(beta), mu0=float(mu), beta0=float(beta), tol=float(tol),
@@ -352,9 +395,11 @@ def mrhs(seed=4, side=128, m=4096, rhs=32, noise=0.01, tv_norm=1, maxit=300, tol
 
 def batch_specs(seed=3, count=64, sides=(64, 96, 128, 192, 256)):
     """The mixed batch of independent 2D problems: per instance a side drawn
-    from `sides`, and either a dense Gaussian A (sampling 25-40 %, drawn on
-    the device from the instance seed) or a ring geometry (128-512
-    transducers).  Returns descriptions; the caller materialises them."""
+    from `sides`, and either a dense Gaussian A (sampling 25-40 %, the
+    counter-based Gaussian stream of the instance seed, drawn on the device
+    or regenerated on the host) or a ring geometry (128-512 transducers).
+    Returns descriptions; batch_dense_parts / batch_dense_host / batch_ray
+    materialise them."""
     rng = np.random.default_rng(seed)
     out = []
     for k in range(count):
@@ -366,6 +411,36 @@ def batch_specs(seed=3, count=64, sides=(64, 96, 128, 192, 256)):
             T = int(rng.choice([128, 192, 256, 384, 512]))
             out.append(dict(kind="ray2d", side=side, T=T, seed=int(rng.integers(1 << 30))))
     return out
+
+
+def batch_dense_parts(d):
+    """The pieces of a dense batch instance that do not need its matrix: the
+    shape (side, side), m, the phantom, the options and the noise generator
+    (drawn after the phantom).  Its A is the Gaussian stream of the instance
+    seed, scaled by 1/sqrt(m) (philox_gaussian / tval3g_gaussian), row-major
+    m x n; b = float32(A u) plus 1 % noise from the returned generator."""
+    side = d["side"]
+    n = side * side
+    m = int(round(d["sampling"] * n))
+    rng = np.random.default_rng(d["seed"])
+    u = ellipse_phantom(side, side, rng, 5, 0.0, lambda r: r.uniform(0.2, 1.0), (side / 16, side / 3.2))
+    return dict(shape=(side, side), m=m, n=n, u_true=u, rng=rng, scale=float(np.float32(1.0 / math.sqrt(m))),
+                opts=options(2 ** 8, 2 ** 5, 1e-4, 300, tv_norm=1))
+
+
+def batch_dense_host(d):
+    """A dense batch instance materialised on the host (A from the numpy
+    restatement of the device generator)."""
+    p = batch_dense_parts(d)
+    A = philox_gaussian(d["seed"], p["m"] * p["n"], p["scale"]).reshape(p["m"], p["n"])
+    y = (A.astype(np.float64) @ p["u_true"].ravel()).astype(np.float32)
+    b = add_noise(y.astype(np.float64), 0.01, p["rng"]).astype(np.float32)
+    return dict(kind="dense", shape=p["shape"], A=A, b=b, u_true=p["u_true"], opts=p["opts"])
+
+
+def batch_ray(d):
+    """A ring batch instance (host geometry and data; hit weight 1/sigma_max)."""
+    return ring2d(seed=d["seed"], side=d["side"], T=d["T"], tv_norm=1, maxit=500, tol=1e-5, normalize=True)
 
 
 def hemi3d(seed=2, side=128, T=2048, receivers=1024, noise=0.005, tv_norm=0, maxit=400, tol=1e-5,
