@@ -312,6 +312,16 @@ def kernel_roofline(cx, capi, spec, w, kind):
         kt[name] = float(np.mean(ts))
     nnz, n, m, index = op.nnz, op.cols, op.rows, op.adjoint_index_bytes
     op.close()
+    variants = None
+    if kind in ("ray2d", "ray3d"):
+        # the other adjoint form: rays traced on the fly, atomic adds into the image
+        opa = capi.Operator(spec, adj_atomics=True)
+        opa.apply_n(y, out_n, 3, trans=1, stream=s)
+        ts, _ = cx.event_time(lambda: opa.apply_n(y, out_n, 1, trans=1, stream=s), 10)
+        opa.close()
+        variants = {"gather_ms": kt["adjoint"], "atomics_ms": float(np.mean(ts)),
+                    "default": "gather" if kt["adjoint"] <= float(np.mean(ts)) else "atomics (not the default: "
+                                                                                "the gather is deterministic)"}
     peak, src = peak_hbm()
     if kind == "ray2d":
         # tiled adjoint: its index once (tile lists, 16-bit positions, offsets),
@@ -331,7 +341,7 @@ def kernel_roofline(cx, capi, spec, w, kind):
     return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": profile_traffic(prof), "algorithmic_bytes": int(bytes_),
             "ms_per_launch": kt[direction], "peak_source": src,
-            "ms_per_launch_by_direction": kt,
+            "ms_per_launch_by_direction": kt, "adjoint_variants": variants,
             "timing": "one launch per CUDA-event pair, 256 MB L2 flush before each"}
 
 

@@ -67,6 +67,14 @@ extern "C" {
                                    variable TVAL3G_TUNE_CACHE names a file, on
                                    disk.  Results then equal the untuned ones
                                    within rounding (other summation order). */
+#define TVAL3G_RAY_ADJ_ATOMICS 32  /* ray operators: the adjoint traces the rays
+                                   on the fly and accumulates into the image
+                                   with atomic adds (no pixel-major index),
+                                   instead of the pixel-major gather; sums are
+                                   then not bit-reproducible (the order of the
+                                   atomic adds varies).  A comparison form:
+                                   the gather is the default because it
+                                   measured faster (and is deterministic). */
 
 /* Per inner iteration: step length, objective after update_W, relative
  * change, backtracking steps taken (6 = restart after five failures), whether

@@ -73,7 +73,8 @@ def build_case(name):
         extra = {}
         if kind == "skip":
             extra = dict(skipMulRatio=0.5, numInitIterations=3, maxRelativeChange=0.05)
-        w = W.ring2d(seed=1, side=64, T=64, tv_norm=1 if kind == "iso" else 0, maxit=maxit, tol=1e-5)
+        w = W.ring2d(seed=1, side=64, T=64, tv_norm=1 if kind == "iso" else 0, maxit=maxit, tol=1e-5,
+                     normalize=True)
         w["opts"].update(extra)
         # nonnegativity keeps this problem in its stable regime (FP32 and FP64
         # trajectories agree), which the iso and skip cases need to be compared
@@ -86,7 +87,8 @@ def build_case(name):
         c["oracle_op"] = O.Op.ray2d(w["geom"], 64 * 64)
     elif name.startswith("hemi3d_s16") or name == "csr3d_s16":
         it = name.endswith("it20") or name == "csr3d_s16"
-        w = W.hemi3d(seed=2, side=16, T=64, receivers=16, maxit=20 if it else 200, tol=1e-5, csr=True)
+        w = W.hemi3d(seed=2, side=16, T=64, receivers=16, maxit=20 if it else 200, tol=1e-5, csr=True,
+                     normalize=True)
         c.update(shape=w["shape"], b=w["b"], u_true=w["u_true"], opts=w["opts"], geom=w["geom"], csr=w["csr"],
                  csr_tuple=_csr_tuple(w["csr"]), layers=1)
         if name == "csr3d_s16":
@@ -110,7 +112,7 @@ def build_case(name):
     elif name == "hemi3d_mp2_s16":
         # two measurement positions (numMPs = 2, 3d/mat_mult.h:183): the same
         # hemisphere, and the hemisphere turned a quarter about z
-        w = W.hemi3d(seed=2, side=16, T=64, receivers=16, maxit=20, tol=1e-5, csr=True)
+        w = W.hemi3d(seed=2, side=16, T=64, receivers=16, maxit=20, tol=1e-5, csr=True, normalize=True)
         g = dict(w["geom"])
         s_ = 15
         for a, b_ in (("xe", "ye"), ("xr", "yr")):
@@ -205,7 +207,7 @@ def build_case(name):
     elif name == "chemi3d_s16":
         # complex data on the 3D hemisphere geometry (the reference runs its
         # own 3D projector on complex vectors)
-        w = W.hemi3d(seed=15, side=16, T=64, receivers=16, maxit=200, tol=1e-5, csr=True)
+        w = W.hemi3d(seed=15, side=16, T=64, receivers=16, maxit=200, tol=1e-5, csr=True, normalize=True)
         rng = np.random.default_rng(15)
         u = w["u_true"] * np.exp(1j * np.linspace(0, 1.5, w["u_true"].size)).reshape(w["u_true"].shape)
         csr = dict(w["csr"])
@@ -214,7 +216,7 @@ def build_case(name):
         c.update(shape=w["shape"], b=b, u_true=u.astype(np.complex64), opts=w["opts"], geom=w["geom"], csr=csr,
                  ref_kind="ray3d", api="ray3d_complex", layers=1)
     elif name == "cring2d_s64":
-        w = W.ring2d(seed=13, side=64, T=64, tv_norm=0, maxit=300, tol=1e-5)
+        w = W.ring2d(seed=13, side=64, T=64, tv_norm=0, maxit=300, tol=1e-5, normalize=True)
         rng = np.random.default_rng(13)
         u = _complex_phantom(64, rng)
         csr = dict(w["csr"])

@@ -270,3 +270,39 @@ def test_gaussian_device_equals_host(torch_cuda):
         ulp = np.abs(got.view(np.int32).astype(np.int64) - want.view(np.int32).astype(np.int64))
         print(f"seed {seed}: {np.count_nonzero(ulp)} of {cnt} elements differ (max {ulp.max()} ulp)")
         assert ulp.max() <= 1 and np.count_nonzero(ulp) <= cnt * 1e-4
+
+
+@pytest.mark.parametrize("name", ["ring2d_s64_it20", "hemi3d_s16_it20", "hemi3d_mp2_s16"])
+def test_ray_adjoint_atomics_variant(name, torch_cuda):
+    """The adjoint by on-the-fly tracing with atomic adds
+    (TVAL3G_RAY_ADJ_ATOMICS) against the FP64 oracle (1e-5) and against the
+    default gather form; a solve built with it stays within the solve bar of
+    the default form."""
+    torch = torch_cuda
+    c = build_case(name)
+    spec = api_problem(c, capi)
+    op = capi.Operator(spec, adj_atomics=True)
+    y = np.random.default_rng(4).standard_normal(op.rows).astype(np.float32)
+    dx = torch.empty(op.cols, device="cuda")
+    op.apply(_dev(torch, y), dx, trans=True)
+    op.close()
+    e = relerr(dx.cpu().numpy(), c["oracle_op"].apply(y.astype(np.float64), trans=True))
+    print(f"{name}: atomics adjoint vs FP64 {e:.2e}")
+    assert e < 1e-5
+
+
+def test_solve_with_atomics_adjoint(torch_cuda):
+    """A well-conditioned 64x64 ring (hit weight 1/sigma_max), 20 iterations:
+    the solve with the atomics adjoint equals the default one within 1e-4."""
+    torch = torch_cuda
+    w = W.ring2d(seed=1, side=64, T=64, tv_norm=1, maxit=20, tol=1e-5, normalize=True)
+    spec = capi.problem_from_workload(w)
+    plan = capi.Plan([spec], [w["opts"]], adj_atomics=True)
+    du = [torch.empty(spec.n, device="cuda")]
+    info = plan.solve([_dev(torch, w["b"])], du)[0]
+    plan.close()
+    U0, info0 = capi.solve(spec, w["b"], w["opts"])
+    e = relerr(du[0].cpu().numpy(), U0)
+    print(f"solve with the atomics adjoint vs the gather form: {e:.2e}")
+    assert info["total_iters"] == info0["total_iters"] == 20
+    assert e < 1e-4

@@ -1,51 +1,75 @@
 """GPU solver parity through the C ABI.
 
-FP32 trajectories of TVAL3 are sensitive: the reference's own float build
-differs from its own double build by 5e-5 (dense, 20 iterations) up to 5.6e-2
-(2D ring, 20 iterations) and 8.9e-2 (3D, at convergence) - see the golden
-fixtures.  The bar for the FP32 GPU solution (relative L2 of U) is therefore
-
-    |U_gpu - U_fp64| <= max(1e-3, 2 * |U_ref_float - U_ref_double|)
-
-i.e. the GPU result is at least as close to the FP64 solution (oracle and the
-reference's double build, which agree to <2e-7) as the reference's own float
-build is, up to a factor 2, and never looser than 1e-3.  Where the reference
-cannot run (isotropic TV) the bar is 1e-3 against the oracle at an iteration
-count where the float trajectory is stable.
+Every case is solved on the GPU with a trace of its decisions (backtracking
+steps, A^T-skip, where the inner loop ended).  The bar, 1e-3 relative L2 of
+U, is checked against the FP64 oracle at the same iteration count and path:
+the oracle's own solve where the GPU took the same decisions, else the
+oracle replaying the GPU's decisions (oracle.replay_from_trace) - FP32 and
+FP64 solves can land on different sides of a threshold test
+(2d/tval3_cpu_2d.cpp:540-574,790-853) and then differ by that decision, not
+by rounding.  Where the GPU took the oracle's decisions the reference's own
+double build (which agrees with the oracle to < 1e-9) is checked too.  The
+ring and hemisphere cases use the hit weight 1/sigma_max(A), which keeps the
+problems well conditioned; every measured error is printed.
 Graph and plain execution, and batched and single solves, run the same
 kernels in the same order with deterministic reductions: bit-identical.
 """
 import numpy as np
 import pytest
 
+import oracle as O
 from golden.cases import CASES, api_problem, build_case
 from helpers import golden, relerr
 from tval3g import capi
 
 pytestmark = pytest.mark.gpu
 
+BAR = 1e-3
 
-def _bar(g):
-    if "ref0_U" not in g:
-        return 1e-3
-    return max(1e-3, 2 * relerr(g["ref0_U"], g["ref2_U"]))
+
+def _traced_solve(torch, c):
+    spec = api_problem(c, capi)
+    plan = capi.Plan([spec], [c["opts"]], graph=True, trace=True)
+    du = [torch.empty(spec.n, device="cuda")]
+    info = plan.solve([torch.tensor(np.ascontiguousarray(c["b"], np.float32), device="cuda")], du)[0]
+    tr = plan.trace(0)
+    plan.close()
+    return du[0].cpu().numpy().reshape(c["shape"]), info, tr
 
 
 @pytest.mark.parametrize("name", CASES)
 def test_solve_matches_oracle_and_reference(name, torch_cuda):
     c = build_case(name)
     g = golden(f"{name}.npz")
-    U, info = capi.solve(api_problem(c, capi), c["b"], c["opts"], Ut=c["u_true"])
+    U, info, tr = _traced_solve(torch_cuda, c)
     assert info["status"] == 0
-    bar = _bar(g)
-    e_or = relerr(U, g["oracle_U"])
-    assert e_or < bar, (name, e_or, bar, info)
-    if "ref2_U" in g:
-        assert relerr(U, g["ref2_U"]) < bar
+    same = int(g["oracle_iters"][1]) == info["total_iters"]
+    e_free = relerr(U, g["oracle_U"])
+    if same:
+        r = O.solve(c["oracle_op"], c["b"].astype(np.float64), c["shape"], c["opts"], record=True)
+        same = [x[3] for x in r.iters] == [int(v) for v in tr[:, 3]] and \
+            [x[4] for x in r.iters] == [int(v) for v in tr[:, 4]]
+    if same:
+        e = e_free
+        what = "the FP64 oracle's own solve (same decisions)"
+    else:
+        r = O.solve(c["oracle_op"], c["b"].astype(np.float64), c["shape"], c["opts"],
+                    replay=O.replay_from_trace(tr))
+        assert r.total_iters == info["total_iters"]
+        e = relerr(U, r.U)
+        what = "the FP64 oracle replaying the GPU's decisions"
+    print(f"{name}: {info['total_iters']} iterations (FP64 oracle {int(g['oracle_iters'][1])}); relerr vs {what} "
+          f"{e:.3e}; vs the free-running FP64 solve {e_free:.3e}")
+    assert e < BAR, (name, e)
+    if same and "ref2_U" in g and int(g["ref2_iters"][1]) == info["total_iters"]:
+        e2 = relerr(U, g["ref2_U"])
+        print(f"{name}: relerr vs the reference's double build {e2:.3e}")
+        assert e2 < BAR
     if name.endswith("it20"):
         assert info["total_iters"] == 20
     # rel_error is ||Ut - U|| / ||Ut|| of the returned U
-    assert abs(info["rel_error"] - relerr(U, c["u_true"])) < 1e-5
+    _, info2 = capi.solve(api_problem(c, capi), c["b"], c["opts"], Ut=c["u_true"])
+    assert abs(info2["rel_error"] - relerr(U, c["u_true"])) < 1e-5
 
 
 @pytest.mark.parametrize("name", ["ring2d_s64_conv", "dense2d_s32_conv", "hemi3d_s16_conv", "ring2d_s64_skip"])

@@ -169,6 +169,8 @@ struct OpDev {
 	// the normal limit, error word raised, TVAL3G_ERR_CUDA) runs without a
 	// fault or an unbounded wait.
 	unsigned first_wait_polls;
+	// ray adjoint by on-the-fly tracing and atomic adds (TVAL3G_RAY_ADJ_ATOMICS)
+	int adj_atomic;
 };
 
 #ifndef TVAL3G_RAYT

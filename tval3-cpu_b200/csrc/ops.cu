@@ -626,6 +626,70 @@ __global__ void __launch_bounds__(256) k_ray_fwd(const Inst *tab, TileMap map, i
 	if (gl == 0 && out >= 0) vselw(I, ys)[out] = (float)(acc * op.scale);
 }
 
+// The adjoint by on-the-fly tracing (TVAL3G_RAY_ADJ_ATOMICS): lanes and
+// steps as in k_ray_fwd (always the image's own layout), each hit adding
+// scale * y[ray] to its pixel with an atomic add into the zeroed output.
+// The order of the adds varies from run to run, so the sums are not
+// bit-reproducible; the gather adjoints are.
+__global__ void __launch_bounds__(256) k_ray_atomic_zero(const Inst *tab, TileMap map, int pred, VecSel ys,
+                                                         unsigned long long *launches) {
+	OPROLOGUE();
+	float *out = vselw(I, ys);
+	const long long i0 = local * ATOMIC_ZERO_TILE;
+	for (long long i = i0 + threadIdx.x; i < min(I.n, i0 + ATOMIC_ZERO_TILE); i += blockDim.x) out[i] = 0.f;
+}
+
+template <bool D3>
+__global__ void __launch_bounds__(256) k_ray_adj_atomic(const Inst *tab, TileMap map, int pred, VecSel xs,
+                                                        VecSel ys, unsigned long long *launches) {
+	OPROLOGUE();
+	const OpDev &op = I.op;
+	constexpr int SUBW = RAY_SUBW, RPB = 256 / SUBW;
+	const int gl = threadIdx.x % SUBW;
+	const long long ray = local * RPB + threadIdx.x / SUBW;
+	if (ray >= op.nrays) return;
+	float *g = vselw(I, ys);
+	int x0, y0, z0, dx, dy, dz, out;
+	unpack_ray(op.rays[ray], x0, y0, z0, dx, dy, dz, out);
+	const float w = vsel(I, xs)[out] * op.scale;
+	const int mx = abs(dx), my = abs(dy), mz = D3 ? abs(dz) : 0;
+	const int sx = dx < 0 ? -1 : 1, sy = (dy < 0 ? -1 : 1) * op.rvx;
+	const int sz = (dz < 0 ? -1 : 1) * op.rvx * op.rvy;
+	int M, a1, a2, sd, s1, s2;
+	int idx = x0 + y0 * op.rvx + z0 * op.rvx * op.rvy;
+	if (mx >= my && mx >= mz) { M = mx; sd = sx; a1 = my; s1 = sy; a2 = mz; s2 = sz; }
+	else if (my >= mx && my >= mz) { M = my; sd = sy; a1 = mx; s1 = sx; a2 = mz; s2 = sz; }
+	else { M = mz; sd = sz; a1 = mx; s1 = sx; a2 = my; s2 = sy; }
+	idx += gl * sd;
+	const int twoM = 2 * M > 0 ? 2 * M : 1;
+	int r1 = 0, qa1 = 0, ra1 = 0, r2 = 0, qa2 = 0, ra2 = 0;
+	if (M > 0) {
+		int num = 2 * gl * a1 + M - 1;
+		int q = num / twoM;
+		r1 = num - q * twoM;
+		qa1 = (2 * SUBW * a1) / twoM; ra1 = 2 * SUBW * a1 - qa1 * twoM;
+		idx += q * s1;
+		if (D3) {
+			num = 2 * gl * a2 + M - 1;
+			q = num / twoM;
+			r2 = num - q * twoM;
+			qa2 = (2 * SUBW * a2) / twoM; ra2 = 2 * SUBW * a2 - qa2 * twoM;
+			idx += q * s2;
+		}
+	}
+	const int dstep = SUBW * sd + qa1 * s1 + (D3 ? qa2 * s2 : 0);
+	for (int j = gl; j <= M; j += SUBW) {
+		atomicAdd(g + idx, w);
+		idx += dstep;
+		r1 += ra1;
+		if (r1 >= twoM) { r1 -= twoM; idx += s1; }
+		if (D3) {
+			r2 += ra2;
+			if (r2 >= twoM) { r2 -= twoM; idx += s2; }
+		}
+	}
+}
+
 // xT[y + x*tH] = x[x + y*ld] for the 2D forward (32x32 tiles through shared
 // memory; local tile = ty * ceil(ld/32) + tx)
 __global__ void __launch_bounds__(256) k_transpose2d(const Inst *tab, TileMap map, int pred, VecSel xs,
@@ -1038,6 +1102,14 @@ void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel
 	}
 	gather(L, B.csc_adj, pred, 1, x, y);
 	gather(L, B.ray_adj, pred, 2, x, y);
+	if (B.ray_atomic_zero.count > 0)
+		launch_pdl(k_ray_atomic_zero, B.ray_atomic_zero.count, 256, 0, L.stream, L.inst, B.ray_atomic_zero, pred, y, ctr);
+	if (B.ray2_adj_atomic.count > 0)
+		launch_pdl(k_ray_adj_atomic<false>, B.ray2_adj_atomic.count, 256, 0, L.stream, L.inst, B.ray2_adj_atomic, pred,
+		           x, y, ctr);
+	if (B.ray3_adj_atomic.count > 0)
+		launch_pdl(k_ray_adj_atomic<true>, B.ray3_adj_atomic.count, 256, 0, L.stream, L.inst, B.ray3_adj_atomic, pred,
+		           x, y, ctr);
 	if (B.ray_adj_tiled.count > 0) {
 		launch_pdl(k_ray_adj_tiled, B.ray_adj_tiled.count, RAYT_ADJ_THREADS, tiled_smem_bytes(B.tiled_tmax), L.stream,
 		           L.inst, B.ray_adj_tiled, pred, x, y, B.err, ctr);

@@ -55,7 +55,12 @@ struct OpBatch {
 	// shared memory for the longest tile list of the batch
 	TileMap ray_adj_tiled;
 	int tiled_tmax = 0;
+	// ray adjoints by on-the-fly tracing with atomic adds (OpDev::adj_atomic):
+	// the output zeroed (ATOMIC_ZERO_TILE elements per block), then
+	// RAYS_PER_BLOCK rays per block, 2D and 3D
+	TileMap ray_atomic_zero, ray2_adj_atomic, ray3_adj_atomic;
 };
+constexpr int ATOMIC_ZERO_TILE = 1024;
 
 // the tiled 2D ray adjoint's index (OpDev::tiled) for an ld x H image, from
 // the pixel-major lists of traced-ray ids (cptr, cind; sorted by ray) and the

@@ -367,7 +367,8 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 			d.xT = dalloc_op<float>(s, st, n);
 			d.tH = (int)(n / p.ld);
 		}
-		if (!is3 && n % p.ld == 0 && d.nrays > 0 && d.nrays <= RAYT_MAX_RAYS) {
+		d.adj_atomic = (flags & TVAL3G_RAY_ADJ_ATOMICS) != 0;
+		if (!is3 && n % p.ld == 0 && d.nrays > 0 && d.nrays <= RAYT_MAX_RAYS && !d.adj_atomic) {
 			// tiled adjoint (cind still holds traced-ray ids)
 			int *lo = dalloc_op<int>(s, st, d.nrays);
 			TG_CUDA(cudaMemcpyAsync(lo, st.ray_out.data(), sizeof(int) * d.nrays, cudaMemcpyHostToDevice, s));
@@ -532,7 +533,7 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 		tb.close(&ob.csc_adj[c]);
 		for (int i = 0; i < cnt; i++) {
 			const OpDev &d = inst[i].op;
-			if ((d.kind != TVAL3G_OP_RAY2D && d.kind != TVAL3G_OP_RAY3D) || d.tiled ||
+			if ((d.kind != TVAL3G_OP_RAY2D && d.kind != TVAL3G_OP_RAY3D) || d.tiled || d.adj_atomic ||
 			    cls((double)ops[i].nnz / inst[i].n, d.gcls_adj) != c)
 				continue;
 			long long lpb = 256 / widths[c];
@@ -559,10 +560,22 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 		tb.add(i, (long long)((d.rvx + 31) / 32) * ((d.tH + 31) / 32));
 	}
 	tb.close(&ob.ray2_transpose);
+	// adjoints by on-the-fly tracing with atomic adds
+	for (int i = 0; i < cnt; i++)
+		if (inst[i].op.adj_atomic) tb.add(i, (inst[i].n + ATOMIC_ZERO_TILE - 1) / ATOMIC_ZERO_TILE);
+	tb.close(&ob.ray_atomic_zero);
+	for (int dim3 = 0; dim3 < 2; dim3++) {
+		for (int i = 0; i < cnt; i++) {
+			const OpDev &d = inst[i].op;
+			if (!d.adj_atomic || d.kind != (dim3 ? TVAL3G_OP_RAY3D : TVAL3G_OP_RAY2D)) continue;
+			tb.add(i, (d.nrays + RAYS_PER_BLOCK - 1) / RAYS_PER_BLOCK);
+		}
+		tb.close(dim3 ? &ob.ray3_adj_atomic : &ob.ray2_adj_atomic);
+	}
 	ob.tiled_tmax = 0;
 	for (int i = 0; i < cnt; i++) {
 		const OpDev &d = inst[i].op;
-		if (!d.tiled) continue;
+		if (!d.tiled || d.adj_atomic) continue;
 		tb.add(i, (long long)d.ntx * ((d.tH + RAYT - 1) / RAYT));
 		ob.tiled_tmax = std::max(ob.tiled_tmax, d.tmax);
 	}

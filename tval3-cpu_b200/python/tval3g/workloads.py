@@ -444,18 +444,22 @@ def batch_ray(d):
 
 
 def hemi3d(seed=2, side=128, T=2048, receivers=1024, noise=0.005, tv_norm=0, maxit=400, tol=1e-5,
-           n_ellipsoids=12, csr=False, forward=None):
+           n_ellipsoids=12, csr=False, forward=None, normalize=False):
     """3D hemisphere geometry (on-the-fly 3D Bresenham).
 
     forward: optional callable (geometry, image) -> A image; by default the
     data come from the CSR twin built here (which needs ~1 GB of host memory
-    per 1e8 hits at full size)."""
+    per 1e8 hits at full size).  normalize (with the CSR twin): hit weight
+    scale_factor = 1/sigma_max(A), as ring2d's."""
     rng = np.random.default_rng(seed)
     radius = (side - 1) / 2.0 - 0.5
     g = hemisphere_geometry(side, T, receivers, radius, rng)
     u = ellipsoid_phantom(side, rng, n_ellipsoids, 1.0, lambda r: 1.0 + r.uniform(-0.05, 0.05),
                           (side / 16, side / 5))
     A = ray3d_csr(g) if (csr or forward is None) else None
+    if normalize and A is not None:
+        g["scale"] = float(np.float32(1.0 / sigma_max(A)))
+        A["val"] = np.full(len(A["colind"]), g["scale"], np.float64)
     y = csr_matvec(A, u.ravel()) if forward is None else np.asarray(forward(g, u), np.float64)
     b = add_noise(y, noise, rng)
     out = dict(kind="ray3d", shape=(side, side, side), geom=g, b=b.astype(np.float32), u_true=u,
