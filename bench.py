@@ -572,6 +572,7 @@ def run_mrhs(a, cx, capi, world, dist, clocks):
     if ref is not None:
         R = ref["U"].reshape(N, -1)
         per_rhs = [float(np.linalg.norm(U[k] - R[k]) / np.linalg.norm(R[k])) for k in range(N)]
+    indep = mrhs_independent(a, cx, capi, w, d_A, d_b)
     # the product alone: forward (split + tcgen05 kernel + reduce), L2 flushed
     op = capi.Operator(spec, tensor=True, device_inputs=True)
     x = torch.rand(op.cols, device=dev)
@@ -596,7 +597,7 @@ def run_mrhs(a, cx, capi, world, dist, clocks):
             "gemv_path": {"ms_per_step": res[False][0], "iterations": res[False][1]["total_iters"],
                           "relerr_vs_fp64": float(res[False][1]["rel_error"]) if ref is not None else None,
                           "form": "same graph, FP64-accumulating gemv kernels, A read once per layer"},
-            "tensor_over_gemv": res[False][0] / ms,
+            "tensor_over_gemv": res[False][0] / ms, "independent": indep,
             "roofline": {"bound": "hbm", "kernel": "k_mrhs_split + k_mrhs<32> + k_mrhs_red (A X^T)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": profile_traffic("mrhs_tcgen05_4096x16384.md"), "algorithmic_bytes": bytes_,
@@ -658,6 +659,43 @@ def run_unrolled(a, cx, capi, world, dist, clocks):
             "forward_ms": ms_f, "backward_ms": ms_b, "loss": loss,
             "grad_mu_norm": float(np.linalg.norm(g[0])), "grad_beta_norm": float(np.linalg.norm(g[1])),
             "clocks": clk}
+
+
+def mrhs_independent(a, cx, capi, w, d_A, d_b):
+    """The 32 right-hand sides solved independently: 32 one-layer instances
+    of one plan sharing the device matrix, so that every product of the
+    group is one tensor-core contraction while each instance keeps its own
+    scaling, step lengths, line search and stopping; against the same plan
+    on the FP64-accumulating gemv kernels and against each right-hand side's
+    FP64 solution (tests/golden/mrhs32_indep_fp64.npz)."""
+    torch, dev, s = cx.torch, cx.dev, cx.stream.cuda_stream
+    N, (m, n) = w["layers"], w["A"].shape
+    side = int(round(np.sqrt(n)))
+    specs = [capi.dense_problem((side, side), w["A"], device_ptr=d_A.data_ptr()) for _ in range(N)]
+    bs = [d_b[k * m:(k + 1) * m] for k in range(N)]
+    us = [torch.empty(n, device=dev) for _ in range(N)]
+    fx = os.path.join(GOLDEN, "mrhs32_indep_fp64.npz")
+    fx = dict(np.load(fx)) if os.path.exists(fx) else None
+    uts = [torch.tensor(fx["U"][k], device=dev) for k in range(N)] if fx is not None else None
+    out = {}
+    for tensor in (True, False):
+        plan = capi.Plan(specs, [w["opts"]] * N, graph=True, device_inputs=True, tensor=tensor)
+        run = lambda: plan.solve(bs, us, d_Ut=uts, stream=s)  # noqa: E731
+        cx.event_time(run, 1)
+        ts, infos = cx.event_time(run, max(1, min(a.steps, 3)))
+        plan.close()
+        rel = [float(i["rel_error"]) for i in infos] if uts is not None else None
+        its = [i["total_iters"] for i in infos]
+        out["tensor" if tensor else "gemv"] = {
+            "ms_per_step": float(np.mean(ts)), "value": N * 1000.0 / float(np.mean(ts)),
+            "unit": "reconstructions/s (right-hand sides)", "iterations_min_max": [min(its), max(its)],
+            "relerr_vs_fp64_max": max(rel) if rel else None,
+            "relerr_vs_fp64_per_rhs": [round(e, 6) for e in rel] if rel else None,
+            "iterations_vs_fp64": [[i, int(fx["iters"][k][1])] for k, i in enumerate(its)] if fx is not None else None}
+    out["form"] = ("32 one-layer instances of one plan sharing the device matrix (per-instance control); 'tensor': "
+                   "each product of the group one tcgen05 3xTF32 contraction; 'gemv': FP64-accumulating gemv "
+                   "kernels per instance")
+    return out
 
 
 def batch_problems(capi, torch, dev):

@@ -11,7 +11,8 @@ unit-weight ring (normalize=False, U_unit20).  Also records the reference's
 own float solver on the CSR twin of the same operator with anisotropic TV for
 the drift statement.
 The dense 64x64 workload goes to dense64_fp64.npz and the joint 32-layer
-multi-RHS workload to mrhs32_fp64.npz.  The mixed batch's FP64 subset (its
+multi-RHS workload to mrhs32_fp64.npz, its 32 right-hand sides solved
+independently to mrhs32_indep_fp64.npz.  The mixed batch's FP64 subset (its
 ring instances of side <= 192 and its dense instances of side <= 96, dense A
 regenerated from the counter-based Gaussian stream the bench draws on the
 device) goes to batch_fp64.npz as U<k>, iters<k> per batch index k.
@@ -85,6 +86,23 @@ def mrhs():
                         iters=np.array([r.outer_iters, r.total_iters]))
 
 
+def mrhs_indep():
+    """The same 32 right-hand sides solved independently (one layer each,
+    each with its own scaling, step lengths and stopping), as 32 calls of the
+    reference with one layer would: U (32 x 16384) and iteration counts."""
+    w = W.mrhs()
+    N, (m, n) = w["layers"], w["A"].shape
+    op = O.Op.dense(w["A"].astype(np.float64))
+    Us, its = [], []
+    t = time.time()
+    for k in range(N):
+        r = O.solve(op, w["b"][k * m:(k + 1) * m].astype(np.float64), (128, 128), w["opts"])
+        Us.append(r.U.ravel().astype(np.float32))
+        its.append([r.outer_iters, r.total_iters])
+        print(f"independent right-hand side {k}: {r.total_iters} iterations ({time.time() - t:.0f} s)")
+    np.savez_compressed(os.path.join(HERE, "mrhs32_indep_fp64.npz"), U=np.stack(Us), iters=np.array(its))
+
+
 def batch():
     out = {}
     t0 = time.time()
@@ -105,12 +123,14 @@ def batch():
 
 
 if __name__ == "__main__":
-    parts = sys.argv[1:] or ["ring", "dense64", "mrhs", "batch"]
+    parts = sys.argv[1:] or ["ring", "dense64", "mrhs", "mrhs_indep", "batch"]
     if "ring" in parts:
         main()
     if "dense64" in parts:
         dense64()
     if "mrhs" in parts:
         mrhs()
+    if "mrhs_indep" in parts:
+        mrhs_indep()
     if "batch" in parts:
         batch()

@@ -79,3 +79,46 @@ def test_layered_solve_matches_oracle(torch_cuda):
     assert out[True][1] == out[False][1] == ref.total_iters
     e_t, e_g = relerr(out[True][0], ref.U.ravel()), relerr(out[False][0], ref.U.ravel())
     assert e_t <= 1e-3 and e_g <= 1e-3, (e_t, e_g)
+
+
+@pytest.mark.parametrize("count", [16, 35])
+def test_independent_right_hand_sides(count, torch_cuda):
+    """Independent right-hand sides: one-layer instances of one plan sharing
+    a device matrix are grouped (16 or 32 of them; the 3 left over of 35 keep
+    their gemv products) and every product of a group is one tensor-core
+    contraction, while each instance keeps its own scaling, step lengths,
+    line search and stopping.  Each instance against the FP64 oracle
+    replaying that instance's decisions (1e-3), and against the same plan on
+    the gemv kernels (the grouping changes no decision and only the rounding
+    of the products)."""
+    torch = torch_cuda
+    side, m = 16, 128
+    rng = np.random.default_rng(count)
+    n = side * side
+    A = (rng.standard_normal((m, n)) / np.sqrt(m)).astype(np.float32)
+    us = [W.ellipse_phantom(side, side, rng, 3, 0.0, lambda r: r.uniform(0.2, 1.0), (2, 6)) for _ in range(count)]
+    bs = [W.add_noise(A.astype(np.float64) @ u.ravel(), 0.01, rng).astype(np.float32) for u in us]
+    opts = W.options(2 ** 8, 2 ** 5, 1e-4, 60, tv_norm=1)
+    d_A = torch.tensor(A, device="cuda")
+    specs = [capi.dense_problem((side, side), A, device_ptr=d_A.data_ptr()) for _ in range(count)]
+    db = [torch.tensor(b, device="cuda") for b in bs]
+    out = {}
+    for tensor in (True, False):
+        plan = capi.Plan(specs, [opts] * count, graph=True, device_inputs=True, trace=True, tensor=tensor)
+        du = [torch.empty(n, device="cuda") for _ in range(count)]
+        infos = plan.solve(db, du)
+        out[tensor] = ([u.cpu().numpy() for u in du], infos, [plan.trace(k) for k in range(count)],
+                       plan.stats()["device_bytes"])
+        plan.close()
+    op64 = O.Op.dense(A.astype(np.float64))
+    worst, worst_g = 0.0, 0.0
+    for k in range(count):
+        U, info, tr = out[True][0][k], out[True][1][k], out[True][2][k]
+        r = O.solve(op64, bs[k].astype(np.float64), (side, side), opts, replay=O.replay_from_trace(tr))
+        assert r.total_iters == info["total_iters"]
+        worst = max(worst, relerr(U, r.U.ravel()))
+        worst_g = max(worst_g, relerr(U, out[False][0][k]))
+    print(f"{count} independent right-hand sides: worst relerr vs replayed FP64 {worst:.2e}, "
+          f"vs the gemv plan {worst_g:.2e}")
+    assert worst <= 1e-3 and worst_g <= 1e-3
+    assert out[True][3] > out[False][3]   # the group's tensor-core operator was built

@@ -182,6 +182,8 @@ __device__ __forceinline__ bool wait_warp(unsigned bar, unsigned parity, volatil
 struct MrhsArgs {
 	const Inst *tab;
 	int inst, pred;
+	const int *members;   // independent right-hand sides (MrhsOp::members) or NULL
+	int N;
 	int M;          // rows of D
 	int ks;         // K steps of BK
 	int J;          // partial slots per CTA
@@ -195,7 +197,13 @@ template <int N>
 __global__ void __launch_bounds__(THREADS, 1)
     k_mrhs(const __grid_constant__ CUtensorMap tmP, const __grid_constant__ CUtensorMap tmQh,
            const __grid_constant__ CUtensorMap tmQl, MrhsArgs a) {
-	if (!pred_ok(*a.tab[a.inst].ctrl, a.pred)) return;
+	if (a.members) {   // independent right-hand sides: run if any of them takes part
+		bool any = false;
+		for (int l = 0; l < a.N && !any; l++) any = pred_ok(*a.tab[a.members[l]].ctrl, a.pred);
+		if (!any) return;
+	} else if (!pred_ok(*a.tab[a.inst].ctrl, a.pred)) {
+		return;
+	}
 	if (a.launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(a.launches, 1ull);
 	extern __shared__ unsigned char smem_raw[];
 	const unsigned raw = smem_u32(smem_raw);
@@ -360,15 +368,18 @@ __global__ void __launch_bounds__(THREADS, 1)
 }
 
 // D[r, l] = sum over the CTAs whose range meets tile r / BM of their partial
+// (independent right-hand sides: row r of column l goes to element r of
+// instance members[l], where its predicate holds)
 __global__ void __launch_bounds__(256) k_mrhs_red(const Inst *tab, int inst, int pred, VecSel ys, const float *part,
-                                                  int M, int N, int ks, long long T, int G, int J,
+                                                  int M, int N, int ks, long long T, int G, int J, const int *members,
                                                   unsigned long long *launches) {
-	const Inst &I = tab[inst];
-	if (!pred_ok(*I.ctrl, pred)) return;
+	if (!members && !pred_ok(*tab[inst].ctrl, pred)) return;
 	if (launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);
 	const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= (long long)N * M) return;
 	const int l = (int)(idx / M), r = (int)(idx - (long long)l * M);
+	const Inst &I = tab[members ? members[l] : inst];
+	if (members && !pred_ok(*I.ctrl, pred)) return;
 	const int t = r / BM, row = r - t * BM;
 	const long long i0 = (long long)t * ks, i1 = i0 + ks - 1;
 	const int c0 = (int)(((i0 + 1) * G - 1) / T), c1 = (int)(((i1 + 1) * G - 1) / T);
@@ -379,18 +390,27 @@ __global__ void __launch_bounds__(256) k_mrhs_red(const Inst *tab, int inst, int
 		s += part[(((long long)c * J + j) * N + l) * BM + row];
 	}
 	float *y = ys.m ? I.vm[ys.idx] : I.vn[ys.idx];
-	y[(long long)l * M + r] = (float)s;
+	y[(members ? 0 : (long long)l * M) + r] = (float)s;
 }
 
 // right-hand sides -> high (TF32-exact) and low parts
+// (independent right-hand sides: column l of length K from instance
+// members[l], zero where its predicate does not hold)
 __global__ void __launch_bounds__(256) k_mrhs_split(const Inst *tab, int inst, int pred, VecSel xs, long long len,
-                                                    float *hi, float *lo, unsigned long long *launches) {
-	const Inst &I = tab[inst];
-	if (!pred_ok(*I.ctrl, pred)) return;
+                                                    long long K, const int *members, float *hi, float *lo,
+                                                    unsigned long long *launches) {
+	if (!members && !pred_ok(*tab[inst].ctrl, pred)) return;
 	if (launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);
-	const float *x = xs.m ? I.vm[xs.idx] : I.vn[xs.idx];
 	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x) {
-		const float v = x[i];
+		float v;
+		if (members) {
+			const long long l = i / K;
+			const Inst &J = tab[members[l]];
+			v = pred_ok(*J.ctrl, pred) ? (xs.m ? J.vm[xs.idx] : J.vn[xs.idx])[i - l * K] : 0.f;
+		} else {
+			const Inst &I = tab[inst];
+			v = (xs.m ? I.vm[xs.idx] : I.vn[xs.idx])[i];
+		}
 		const float h = tf32_rn(v);
 		hi[i] = h;
 		lo[i] = v - h;
@@ -499,6 +519,13 @@ MrhsOp::~MrhsOp() {
 	if (xl) cudaFree(xl);
 	if (part) cudaFree(part);
 	if (err) cudaFree(err);
+	if (members) cudaFree(members);
+}
+
+void mrhs_set_members(cudaStream_t s, MrhsOp &op, const int *members) {
+	if (!op.members) TG_CUDA(cudaMalloc(&op.members, sizeof(int) * (size_t)op.N));
+	TG_CUDA(cudaMemcpyAsync(op.members, members, sizeof(int) * (size_t)op.N, cudaMemcpyHostToDevice, s));
+	TG_CUDA(cudaStreamSynchronize(s));
 }
 
 bool mrhs_eligible(long long m, long long n, int layers) {
@@ -560,12 +587,14 @@ void mrhs_apply(cudaStream_t s, const Inst *tab, int inst, int pred, const MrhsO
 	const long long len = K * op.N;
 	const int G = trans ? op.grid_a : op.grid_f;
 	k_mrhs_split<<<(unsigned)std::min<long long>((len + 255) / 256, 4LL * G), 256, 0, s>>>(
-	    tab, inst, pred, x, len, op.xh, op.xl, launches);
+	    tab, inst, pred, x, len, K, op.members, op.xh, op.xl, launches);
 	TG_CUDA(cudaGetLastError());
 	MrhsArgs a;
 	a.tab = tab;
 	a.inst = inst;
 	a.pred = pred;
+	a.members = op.members;
+	a.N = op.N;
 	a.M = (int)M;
 	a.ks = trans ? op.ks_a : op.ks_f;
 	a.J = trans ? op.j_a : op.j_f;
@@ -586,7 +615,7 @@ void mrhs_apply(cudaStream_t s, const Inst *tab, int inst, int pred, const MrhsO
 	TG_CUDA(cudaGetLastError());
 	const long long outs = M * op.N;
 	k_mrhs_red<<<(unsigned)((outs + 255) / 256), 256, 0, s>>>(tab, inst, pred, y, op.part, (int)M, op.N, a.ks, a.T, G,
-	                                                          a.J, launches);
+	                                                          a.J, op.members, launches);
 	TG_CUDA(cudaGetLastError());
 }
 

@@ -25,6 +25,11 @@ struct MrhsOp {
 	float *xh = nullptr, *xl = nullptr;   // split right-hand sides, N x max(m, n) each
 	float *part = nullptr;      // grid x J x N x 128 partial tiles
 	int *err = nullptr;         // device flag: a bounded wait timed out
+	// independent right-hand sides: column l of X (and of D) belongs to
+	// instance members[l] of the table (one layer each, its own scalar
+	// control), taken only where that instance's predicate holds; NULL: the
+	// N layers of one instance (the reference's joint multi-layer solve)
+	int *members = nullptr;
 	long long bytes = 0;
 	~MrhsOp();
 };
@@ -39,6 +44,9 @@ std::shared_ptr<MrhsOp> mrhs_create(cudaStream_t s, const float *d_A, long long 
 // table, when its predicate holds
 void mrhs_apply(cudaStream_t s, const Inst *tab, int inst, int pred, const MrhsOp &op, bool trans, VecSel x,
                 VecSel y, unsigned long long *launches);
+// independent right-hand sides: the N instances (device table indices,
+// host array) share this operator's products (MrhsOp::members)
+void mrhs_set_members(cudaStream_t s, MrhsOp &op, const int *members);
 // nonzero if a kernel of this operator gave up a bounded wait (resets it)
 int mrhs_take_error(cudaStream_t s, const MrhsOp &op);
 

@@ -8,6 +8,7 @@
 #include "plan.cuh"
 
 #include <map>
+#include <tuple>
 #include <mutex>
 
 namespace tval3g {
@@ -482,8 +483,8 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 	for (int i = 0; i < cnt; i++) {
 		OpDev &d = inst[i].op;
 		if (d.kind != TVAL3G_OP_DENSE) continue;
-		if (d.mrhs) {
-			ob.mrhs.emplace_back(i, ops[i].mrhs);
+		if (d.mrhs) {   // independent right-hand sides: the group's first instance holds the operator
+			if (ops[i].mrhs) ob.mrhs.emplace_back(i, ops[i].mrhs);
 			continue;
 		}
 		long long ct = (d.n + 1023) / 1024;
@@ -601,6 +602,44 @@ void *Plan::dalloc(size_t bytes) {
 	return p;
 }
 
+// Independent right-hand sides: dense instances of one layer whose A is the
+// same device matrix (TVAL3G_DEVICE_INPUTS: the same pointer and shape) are
+// cut into groups of 64, 48, 32 or 16 (largest first, in instance order),
+// and each group shares one tensor-core operator (mrhs.cu): every product of
+// the group is one 3xTF32 contraction over its members' vectors, each member
+// keeping its own scalar control (step lengths, line search, stopping).
+// Members left over (fewer than 16) keep their own gemv products.
+void Plan::group_shared_dense(const tval3g_problem *probs, int flags) {
+	if (!(flags & TVAL3G_DEVICE_INPUTS) || (flags & TVAL3G_NO_TENSOR)) return;
+	std::map<std::tuple<const float *, int, int, int>, std::vector<int>> by_a;
+	for (int i = 0; i < count_; i++) {
+		const tval3g_problem &p = probs[i];
+		if (p.op_kind == TVAL3G_OP_DENSE && ops_[i].dev.layers == 1 && !p.complex_data && p.A && !ops_[i].dev.mrhs)
+			by_a[std::make_tuple(p.A, p.m, p.n_cols, p.dims)].push_back(i);
+	}
+	for (const auto &kv : by_a) {
+		const std::vector<int> &v = kv.second;
+		const long long m = std::get<1>(kv.first), n = std::get<2>(kv.first);
+		size_t k = 0;
+		while (v.size() - k >= 16) {
+			int sz = 0;
+			for (int c : {64, 48, 32, 16})
+				if ((size_t)c <= v.size() - k && mrhs_eligible(m, n, c)) { sz = c; break; }
+			if (!sz) break;
+			std::vector<int> mem(v.begin() + k, v.begin() + k + sz);
+			auto op = mrhs_create(stream_, ops_[mem[0]].dev.A, m, n, sz);
+			mrhs_set_members(stream_, *op, mem.data());
+			ops_[mem[0]].mrhs = op;
+			ops_[mem[0]].bytes += op->bytes;
+			for (int i : mem) {
+				ops_[i].dev.mrhs = 1;
+				h_inst_[i].op.mrhs = 1;
+			}
+			k += sz;
+		}
+	}
+}
+
 Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, int flags)
 	: count_(count), flags_(flags), graph_mode_((flags & TVAL3G_GRAPH) != 0) {
 	TG_ARG(count >= 1, "Argument error: count must be >= 1");
@@ -642,6 +681,7 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 			if (flags & TVAL3G_TUNE) autotune_operator(stream_, ops_[i], I);
 			I.op = ops_[i].dev;
 		}
+		group_shared_dense(probs, flags);
 		// vectors: one arena, every vector 256-byte aligned
 		long long total = 0;
 		std::vector<long long> base(count);

@@ -105,6 +105,7 @@ private:
 
 	void *dalloc(size_t bytes);
 	void release();
+	void group_shared_dense(const tval3g_problem *probs, int flags);
 	KArgs kargs(MapKind mk, int pred, int stage = 0) const;
 	LaunchCtx lctx() const;
 	void emit_program();
