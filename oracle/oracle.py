@@ -42,7 +42,7 @@ class OrcOpts(C.Structure):
                                           "gam", "rate_gam", "rate_cnt", "skipMulRatio",
                                           "maxRelativeChange")] + \
                [(k, C.c_int) for k in ("maxit", "maxcnt", "nonneg", "isreal", "numInitIterations",
-                                       "tv_norm")]
+                                       "tv_norm", "cplx")]
 
 
 class RefOpts(C.Structure):
@@ -236,6 +236,35 @@ def replay_from_trace(trace):
             "inner_end": inner_end}
 
 
+def complex_real_form(M):
+    """The real form [[Re M, -Im M], [Im M, Re M]] of a complex matrix (dense
+    array or scipy sparse) as an oracle CSR operator on planar vectors (real
+    plane, imaginary plane); its transpose is the real form of M^H."""
+    import scipy.sparse as sp
+    M = sp.csr_matrix(M)
+    R = sp.bmat([[M.real, -M.imag], [M.imag, M.real]], format="csr")
+    R.sort_indices()
+    return Op.csr(R.shape[0], R.shape[1], R.indptr, R.indices, R.data)
+
+
+def solve_complex(op: Op, b, shape, opts: dict, Ut=None, record=False, replay=None) -> Result:
+    """FP64 oracle solve of complex data (the reference's complex<T>
+    overloads): op is the real form of the operator (complex_real_form), b
+    and Ut complex; the solve runs on planar vectors and U comes back
+    complex."""
+    b = np.asarray(b).ravel()
+    bp = np.concatenate([b.real, b.imag])
+    Utp = None
+    if Ut is not None:
+        Ut = np.asarray(Ut).ravel()
+        Utp = np.concatenate([Ut.real, Ut.imag])
+    r = solve(op, bp, shape, dict(opts, cplx=1), Ut=Utp, record=record, replay=replay)
+    n = int(np.prod(shape))
+    U = r.U.ravel()
+    r.U = (U[:n] + 1j * U[n:]).reshape(shape)
+    return r
+
+
 def solve(op: Op, b, shape, opts: dict, Ut=None, record=False, replay=None) -> Result:
     """FP64 oracle solve; shape = (dim_y, dim_x) or (dim_z, dim_y, dim_x).
 
@@ -248,7 +277,7 @@ def solve(op: Op, b, shape, opts: dict, Ut=None, record=False, replay=None) -> R
         dz, dy, dx = 1, shape[0], shape[1]
     else:
         dz, dy, dx = shape
-    U = np.zeros(dz * dy * dx)
+    U = np.zeros(dz * dy * dx * (2 if opts.get("cplx") else 1))
     o = _fill(OrcOpts, opts)
     info = Info()
     its = (Iter * max(int(opts["maxit"]), 1))() if record else None
@@ -268,8 +297,8 @@ def solve(op: Op, b, shape, opts: dict, Ut=None, record=False, replay=None) -> R
         rec = [(its[k].tau, its[k].f, its[k].relchg, its[k].backtracks, its[k].skipped)
                for k in range(info.total_iters)]
         rec_end = [its[k].inner_end for k in range(info.total_iters)]
-    res = Result(U.reshape(shape), info.secs, info.outer_iters, info.total_iters, info.rel_chg,
-                 info.rel_error, rec)
+    res = Result(U if opts.get("cplx") else U.reshape(shape), info.secs, info.outer_iters, info.total_iters,
+                 info.rel_chg, info.rel_error, rec)
     if record:
         res.inner_end = rec_end
     return res

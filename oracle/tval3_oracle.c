@@ -408,6 +408,8 @@ double orc_shrink(int dims, int n, int tv_norm, double beta, const double *Ux, c
 typedef struct {
 	int dims, p, q, r;
 	long n, m;
+	int planes;     /* 2: complex data (real plane, imaginary plane) */
+	long np, mp;    /* elements per plane */
 	double mu, beta, muDbeta;
 	double *delta, *sx, *sy, *sz;
 	double f, lam1, lam2, lam3, lam4, lam5;
@@ -437,7 +439,16 @@ static void vadd(long n, const double *x, double a, const double *y, double *z) 
 static void cpy(long n, const double *x, double *y) { memcpy(y, x, sizeof(double) * n); }
 
 static void Dst(st_t *s, const double *U, double *Ux, double *Uy, double *Uz) {
-	orc_D(s->dims, s->p, s->q, s->r, U, Ux, Uy, Uz);
+	for (int k = 0; k < s->planes; k++) {
+		const long o = k * s->np;
+		orc_D(s->dims, s->p, s->q, s->r, U + o, Ux + o, Uy + o, Uz ? Uz + o : NULL);
+	}
+}
+static void Dts(st_t *s, const double *X, const double *Y, const double *Z, double *res) {
+	for (int k = 0; k < s->planes; k++) {
+		const long o = k * s->np;
+		orc_Dt(s->dims, s->p, s->q, s->r, X + o, Y + o, Z ? Z + o : NULL, res + o);
+	}
 }
 
 /* get_g_mult: generic with the A^T-skip heuristic 2d:300-357 / 3d:433-493;
@@ -499,7 +510,7 @@ static void get_g(st_t *s, const double *U, const double *b, int force) {
 	get_g_mult(s, U, force);
 	axpy(s->n, -1, s->Atb, s->g);
 	form_V(s);
-	orc_Dt(s->dims, s->p, s->q, s->r, s->V[0], s->V[1], s->V[2], s->g2);
+	Dts(s, s->V[0], s->V[1], s->V[2], s->g2);
 	lam24(s);
 	lam35(s, b);
 	s->f = fval(s);
@@ -523,14 +534,22 @@ static double get_tau(st_t *s, int fst) {
 	cpy(s->n, s->dg2, s->tmp_n);
 	axpy(s->n, s->muDbeta, s->dg, s->tmp_n);
 	double sy = dot(s->n, s->uup, s->tmp_n);
+	if (s->planes == 2) {   /* complex: |ss / sy| with sy = <uup, tmp> complex (2d:446-451) */
+		const long h = s->np;
+		double syi = 0;
+		for (long i = 0; i < h; i++) syi += s->uup[i] * s->tmp_n[i + h] - s->uup[i + h] * s->tmp_n[i];
+		return fabs(ss) / sqrt(sy * sy + syi * syi);
+	}
 	return fabs(ss / sy);
 }
 
 /* descend 2d:481-493 (nonneg 2d:455-465) */
 static void descend(st_t *s, double *U, const double *b, double tau, int nonneg, int force) {
 	axpy(s->n, -tau, s->d, U);
-	if (nonneg)
-		for (long i = 0; i < s->n; i++) U[i] = U[i] < 0 ? 0 : U[i];
+	if (nonneg) {
+		for (long i = 0; i < s->np; i++) U[i] = U[i] < 0 ? 0 : U[i];
+		for (long i = s->np; i < s->n; i++) U[i] = 0;   /* complex: Im = 0 (2d:467-479) */
+	}
 	Dst(s, U, s->Ux, s->Uy, s->Uz);
 	get_g(s, U, b, force);
 }
@@ -596,7 +615,37 @@ static void get_gradient(st_t *s, const double *DtsAtd) {
 	axpy(s->n, s->muDbeta, s->g, s->d);
 }
 
+/* complex shrinkage 2d:614-649 / 3d:876-947 (each component's complex
+ * modulus; the reference's 3D z component takes the y component's direction) */
+static double shrink_complex(st_t *s) {
+	const long h = s->np;
+	const int nc = s->dims == 3 ? 3 : 2;
+	double *const U[3] = {s->Ux, s->Uy, s->Uz}, *const S[3] = {s->sx, s->sy, s->sz}, *const W[3] = {s->Wx, s->Wy, s->Wz};
+	double sum = 0;
+	for (long i = 0; i < h; i++) {
+		double re[3], im[3], ab[3], t[3];
+		for (int c = 0; c < nc; c++) {
+			re[c] = U[c][i] - S[c][i] / s->beta;
+			im[c] = U[c][i + h] - S[c][i + h] / s->beta;
+			ab[c] = sqrt(re[c] * re[c] + im[c] * im[c]);
+			t[c] = ab[c] - 1 / s->beta;
+			t[c] = t[c] >= 0 ? t[c] : 0;
+			sum += t[c];
+		}
+		for (int c = 0; c < nc; c++) {
+			const int dir = c == 2 ? 1 : c;   /* 3d/tval3_cpu_3d.cpp:934-937 */
+			W[c][i] = ab[c] > 0 ? t[c] * re[dir] / ab[c] : 0;
+			W[c][i + h] = ab[c] > 0 ? t[c] * im[dir] / ab[c] : 0;
+		}
+	}
+	return sum;
+}
+
 static void shrinkage(st_t *s) {
+	if (s->planes == 2) {
+		s->lam1 = shrink_complex(s);
+		return;
+	}
 	s->lam1 = orc_shrink(s->dims, (int)s->n, s->tv_norm, s->beta, s->Ux, s->Uy, s->Uz, s->sx, s->sy,
 	                     s->sz, s->Wx, s->Wy, s->Wz);
 }
@@ -606,7 +655,7 @@ static void update_W(st_t *s) {
 	s->f -= (s->lam1 + s->beta / 2 * s->lam2 - s->lam4);
 	shrinkage(s);
 	form_V(s);
-	orc_Dt(s->dims, s->p, s->q, s->r, s->V[0], s->V[1], s->V[2], s->g2);
+	Dts(s, s->V[0], s->V[1], s->V[2], s->g2);
 	lam24(s);
 	s->f += (s->lam1 + s->beta / 2 * s->lam2 - s->lam4);
 }
@@ -627,6 +676,28 @@ static void update_mlp(st_t *s, const double *b) {
 }
 
 /* scaleb 2d:229-266 */
+/* complex data (planes of length h): the entries of least and largest
+ * modulus, scl from the modulus of their difference */
+static double scaleb_complex(double *b, long h) {
+	double scl = 1;
+	if (h > 0) {
+		long imin = 0, imax = 0;
+		double amin = sqrt(b[0] * b[0] + b[h] * b[h]), amax = amin;
+		for (long i = 0; i < h; i++) {
+			double a = sqrt(b[i] * b[i] + b[i + h] * b[i + h]);
+			if (a < amin) { imin = i; amin = a; }
+			if (a > amax) { imax = i; amax = a; }
+		}
+		double dr = b[imax] - b[imin], di = b[imax + h] - b[imin + h];
+		double dif = sqrt(dr * dr + di * di);
+		if (dif < 0.5) scl = 0.5 / dif;
+		else if (dif > 1.5) scl = 1.5 / dif;
+		if (dif < 0.5 || dif > 1.5)
+			for (long i = 0; i < 2 * h; i++) b[i] *= scl;
+	}
+	return scl;
+}
+
 static double scaleb(double *b, long len) {
 	double scl = 1;
 	if (len > 0) {
@@ -657,8 +728,13 @@ static int solve_impl(int dims, int dim_y, int dim_x, int dim_z, const orc_op *o
 	st_t S, *s = &S;
 	memset(s, 0, sizeof(S));
 	s->dims = dims; s->p = dim_y; s->q = dim_x; s->r = dims == 3 ? dim_z : 1;
-	s->n = (long)dim_y * dim_x * s->r;
+	s->planes = o->cplx ? 2 : 1;
+	if (o->cplx && o->tv_norm != 0) return -4;
+	if (o->cplx && blen % 2) return -1;
+	s->np = (long)dim_y * dim_x * s->r;
+	s->n = s->np * s->planes;
 	s->m = blen;
+	s->mp = blen / s->planes;
 	s->op = op; s->tv_norm = o->tv_norm;
 	if (op->m * op->layers != blen) return -1;
 	if (op->n * op->layers != s->n) return -2;
@@ -680,7 +756,7 @@ static int solve_impl(int dims, int dim_y, int dim_x, int dim_z, const orc_op *o
 	double muf = o->mu, betaf = o->beta, beta0 = 0;
 	double *DtsAtd = zeros(n), *rcdU = zeros(n), *UrcdU = zeros(n);
 	double gam = o->gam;
-	double scl = scaleb(bs, m);
+	double scl = s->planes == 2 ? scaleb_complex(bs, s->mp) : scaleb(bs, m);
 	orc_apply(op, 1, bs, s->Atb);
 	cpy(n, s->Atb, U);
 	if (s->mu > muf) s->mu = muf;
@@ -738,6 +814,8 @@ static int solve_impl(int dims, int dim_y, int dim_x, int dim_z, const orc_op *o
 		get_gradient(s, DtsAtd);
 		gam = o->gam; Q = 1; C = s->f;
 	}
+	if (s->planes == 2 && o->isreal)   /* keep the real part (2d:855-859) */
+		for (long i = s->np; i < n; i++) U[i] = 0;
 	for (long i = 0; i < n; i++) U[i] = U[i] / scl;
 
 	info->secs = now() - t0;

@@ -28,6 +28,16 @@ typedef struct {
 	double mu, beta, mu0, beta0, tol, tol_inn, c, gamma, gam, rate_gam, rate_cnt;
 	double skipMulRatio, maxRelativeChange;
 	int maxit, maxcnt, nonneg, isreal, numInitIterations, tv_norm;
+	/* 1: complex data as two planes (the reference's complex<T> overloads,
+	 * 2d/tval3_cpu_2d.cpp:913-929): U, b and every vector hold the real
+	 * plane then the imaginary plane, the operator is the caller's real form
+	 * [[Re A, -Im A], [Im A, Re A]] (its transpose is A^H), D and Dt act per
+	 * plane, the shrinkage takes each gradient component's complex modulus
+	 * (2d:614-649; 3D with the reference's z quirk, 3d/tval3_cpu_3d.cpp:934-937),
+	 * scaleb complex moduli (2d:229-266), nonneg Re >= 0 and Im = 0
+	 * (2d:467-479), isreal keeps the real plane (2d:855-859).  Anisotropic
+	 * TV only (the reference has no other). */
+	int cplx;
 } orc_opts;
 
 typedef struct {

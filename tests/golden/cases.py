@@ -202,12 +202,16 @@ def build_case(name):
         u = ur + 1j * ui
         A = ((rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))) / math.sqrt(2 * m)).astype(np.complex64)
         b = _complex_noise(A.astype(np.complex128) @ u.ravel(), 0.01, rng).astype(np.complex64)
+        # 100 iterations: beyond them the problem is chaotic (two FP64 solves
+        # with different summation orders part by 1e-2 at 150)
         c.update(shape=(sd, sd, sd), A=A, b=b, u_true=u.astype(np.complex64), ref_kind="dense", api="dense",
-                 layers=1, opts=W.options(2 ** 8, 2 ** 5, 1e-4, 200, tv_norm=0))
+                 layers=1, opts=W.options(2 ** 8, 2 ** 5, 1e-4, 100, tv_norm=0))
     elif name == "chemi3d_s16":
         # complex data on the 3D hemisphere geometry (the reference runs its
         # own 3D projector on complex vectors)
-        w = W.hemi3d(seed=15, side=16, T=64, receivers=16, maxit=200, tol=1e-5, csr=True, normalize=True)
+        # 40 iterations: the problem is chaotic beyond them (two FP64 solves
+        # with different summation orders part by 1e-4 at 60)
+        w = W.hemi3d(seed=15, side=16, T=64, receivers=16, maxit=40, tol=1e-5, csr=True, normalize=True)
         rng = np.random.default_rng(15)
         u = w["u_true"] * np.exp(1j * np.linspace(0, 1.5, w["u_true"].size)).reshape(w["u_true"].shape)
         csr = dict(w["csr"])
@@ -227,6 +231,22 @@ def build_case(name):
     else:
         raise KeyError(name)
     return c
+
+
+def complex_oracle_op(c):
+    """The oracle operator of a complex case: the real form of its complex
+    operator over all layers (layer-major, block diagonal)."""
+    import scipy.sparse as sp
+    L = c.get("layers", 1)
+    if "A" in c:
+        M = sp.csr_matrix(c["A"].astype(np.complex128))
+    else:
+        A = c["csr"]
+        M = sp.csr_matrix((np.asarray(A["val"]).astype(np.complex128), A["colind"], A["rowptr"]),
+                          shape=(A["m"], A["n"]))
+    if L > 1:
+        M = sp.kron(sp.identity(L), M, format="csr")
+    return O.complex_real_form(M)
 
 
 def api_problem(c, capi):

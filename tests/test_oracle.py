@@ -333,3 +333,20 @@ def test_bresenham_3d_moments_match_the_reference_projector():
     want = np.zeros(nvox)
     np.add.at(want, pix, q[row_of])
     np.testing.assert_array_equal(O.ref_project3d(g, q, trans=True), want)
+
+
+@pytest.mark.parametrize("name", COMPLEX_CASES)
+def test_complex_restatement_matches_reference(name):
+    """The oracle's complex mode (planar vectors, the real form of the
+    operator, complex shrinkage, scaleb and Barzilai-Borwein step) against
+    the reference's own complex<double> build (the golden fixture): the same
+    iteration counts, 1e-12 after 20 iterations, 1e-6 at the end."""
+    from golden.cases import complex_oracle_op
+    c = build_case(name)
+    g = golden(f"{name}.npz")
+    op = complex_oracle_op(c)
+    r = O.solve_complex(op, c["b"], c["shape"], c["opts"])
+    r20 = O.solve_complex(op, c["b"], c["shape"], dict(c["opts"], maxit=20))
+    assert r.total_iters == int(g["ref4_iters"][1])
+    assert relerr(r20.U, g["ref4_U_it20"]) < 1e-12
+    assert relerr(r.U, g["ref4_U"]) < 1e-6

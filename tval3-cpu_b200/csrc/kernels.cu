@@ -507,7 +507,8 @@ __global__ void __launch_bounds__(BLOCK) k_shrink_grad(KArgs a) {
 	// the next iteration's Barzilai-Borwein step (get_tau, 2d:444-451) from
 	// this iteration's uup, g - gp, g2 - g2p (schedule mode: k_tau_prep, as
 	// mu and beta change before that step)
-	const bool bb = !I.sched;
+	// (complex data: k_tau_bb_cplx, which needs the other plane's g2)
+	const bool bb = !I.sched && !I.cplx;
 	const float *__restrict__ gp = I.vn[vGp], *__restrict__ g2p = I.vn[vG2p];
 	// lam1, lam2, lam4, |d|^2, |Up|^2, |uup|^2, |U/scl - Ut|^2, |Ut|^2, <uup, dg2 + muDbeta dg>
 	double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -593,6 +594,41 @@ __global__ void __launch_bounds__(BLOCK) k_shrink_grad(KArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// The Barzilai-Borwein step of complex data (2d:444-451, 3d:605-616):
+// tau = |ss / sy| with ss = <uup, uup> and sy = <uup, dg2 + muDbeta dg> the
+// complex inner product; on the planar vectors (real plane, imaginary plane
+// of h elements each) Re sy = sum over both planes of uup tmp and
+// Im sy = sum_i uup_i tmp_{i+h} - uup_{i+h} tmp_i.  It runs after
+// k_shrink_grad (which writes the imaginary plane's g2 too); real instances
+// take the step from k_shrink_grad.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(BLOCK) k_tau_bb_cplx(KArgs a) {
+	KPROLOGUE(a);
+	if (!I.cplx) return;
+	Ctrl &c = *I.ctrl;
+	const float mdb = (float)c.muDbeta;
+	const int h = (int)(I.n >> 1);
+	const float *__restrict__ gv = I.vn[vG], *__restrict__ gp = I.vn[vGp];
+	const float *__restrict__ g2 = I.vn[vG2], *__restrict__ g2p = I.vn[vG2p], *__restrict__ uup = I.vn[vUUP];
+	double v[3] = {0, 0, 0};   // ss, Re sy, Im sy
+	FOR_TILE(local * TILE, h, i) {
+		const float ur = uup[i], ui = uup[i + h];
+		const float tr = fmaf(mdb, gv[i] - gp[i], g2[i] - g2p[i]);
+		const float ti = fmaf(mdb, gv[i + h] - gp[i + h], g2[i + h] - g2p[i + h]);
+		v[0] += (double)ur * ur + (double)ui * ui;
+		v[1] += (double)ur * tr + (double)ui * ti;
+		v[2] += (double)ur * ti - (double)ui * tr;
+	}
+	double tot[3];
+	if (!tile_reduce<3>(I, local, I.ntn, v, tot)) return;
+	if (threadIdx.x != 0) return;
+	if (c.active && !c.inner_break && !c.fst) {
+		c.tau = fabs(tot[0]) / sqrt(tot[1] * tot[1] + tot[2] * tot[2]);
+		if (bad(c.tau)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; }
+	}
+}
+
+// ---------------------------------------------------------------------------
 // get_tau (2d:425-453), first part.  First iteration (or restart): dDd =
 // |D d|^2 and request A d.  Otherwise Barzilai-Borwein from uup, dg, dg2.
 // ---------------------------------------------------------------------------
@@ -602,7 +638,7 @@ __global__ void __launch_bounds__(BLOCK) k_tau_prep(KArgs a) {
 	const bool first = c.restart || c.fst;
 	const float mdb = (float)c.muDbeta;
 	Geo g(I);
-	double v[2] = {0, 0};
+	double v[3] = {0, 0, 0};
 	const float *__restrict__ d = I.vn[vD];
 	if (first) {
 		FOR_TILE(local * TILE, g.n, i) {
@@ -624,16 +660,21 @@ __global__ void __launch_bounds__(BLOCK) k_tau_prep(KArgs a) {
 			float tmp = fmaf(mdb, dg, dg2);
 			v[0] += (double)uu * uu;
 			v[1] += (double)uu * tmp;
+			if (I.cplx && i < g.n / 2) {   // Im sy (complex data, as k_tau_bb_cplx)
+				const int j = i + g.n / 2;
+				const float tj = fmaf(mdb, gv[j] - gp[j], g2[j] - g2p[j]);
+				v[2] += (double)uu * tj - (double)uup[j] * tmp;
+			}
 		}
 	}
-	double tot[2];
-	if (!tile_reduce<2>(I, local, I.ntn, v, tot)) return;
+	double tot[3];
+	if (!tile_reduce<3>(I, local, I.ntn, v, tot)) return;
 	if (threadIdx.x != 0) return;
 	if (first) {
 		c.dDd = tot[0];
 		c.need_Ad = 1;
 	} else {
-		c.tau = fabs(tot[0] / tot[1]);
+		c.tau = fabs(tot[0]) / sqrt(tot[1] * tot[1] + tot[2] * tot[2]);
 		if (bad(c.tau)) { c.status = TVAL3G_ERR_NONFINITE; c.active = 0; }
 	}
 	set_conds(a.cs, c);
@@ -1036,6 +1077,7 @@ LAUNCHER(launch_getg, k_getg)
 LAUNCHER(launch_grad, k_grad)
 LAUNCHER(launch_shrink_grad, k_shrink_grad)
 LAUNCHER(launch_tau_prep, k_tau_prep)
+LAUNCHER(launch_tau_bb_cplx, k_tau_bb_cplx)
 LAUNCHER(launch_tau_first, k_tau_first)
 LAUNCHER(launch_descend, k_descend)
 LAUNCHER(launch_bt_search, k_bt_search)

@@ -49,6 +49,7 @@ void launch_getg(cudaStream_t s, const KArgs &a);
 void launch_grad(cudaStream_t s, const KArgs &a);
 void launch_shrink_grad(cudaStream_t s, const KArgs &a);
 void launch_tau_prep(cudaStream_t s, const KArgs &a);
+void launch_tau_bb_cplx(cudaStream_t s, const KArgs &a);
 void launch_tau_first(cudaStream_t s, const KArgs &a);
 void launch_descend(cudaStream_t s, const KArgs &a);
 void launch_bt_search(cudaStream_t s, const KArgs &a);

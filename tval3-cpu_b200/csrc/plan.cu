@@ -678,6 +678,7 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 			I.numInit = o.numInitIterations;
 			I.skip_enabled = (o.skipMulRatio != 0 && p.op_kind != TVAL3G_OP_DENSE);
 			any_skip_ |= I.skip_enabled != 0;
+			any_cplx_ |= I.cplx != 0;
 			if (flags & TVAL3G_TUNE) autotune_operator(stream_, ops_[i], I);
 			I.op = ops_[i].dev;
 		}
@@ -1017,6 +1018,7 @@ void Plan::emit_iteration(unsigned long long h_active) {
 	// update_W, reference values, gradient, inner stopping test
 	const unsigned long long h_brk = cond_handle();
 	launch_shrink_grad(es(), kargs(MAP_N, P_ACTIVE, ST_LOOP).cond(h_brk, P_INNER_BREAK).cond(h_active, P_ACTIVE));
+	if (any_cplx_ && !sched_mode_) launch_tau_bb_cplx(es(), kargs(MAP_N, P_ACTIVE));
 	// outer step: stopping test, multipliers, continuation
 	if_(P_INNER_BREAK, [&] {
 		launch_outer(es(), kargs(MAP_N, P_INNER_BREAK));

@@ -74,6 +74,7 @@ private:
 	int flags_;
 	bool graph_mode_;
 	bool any_skip_ = false;
+	bool any_cplx_ = false;   // complex instances: their Barzilai-Borwein step in k_tau_bb_cplx
 	bool sched_mode_ = false;
 	double *d_sched_ = nullptr;
 	cudaStream_t stream_ = nullptr;   // the plan's own stream
