@@ -13,6 +13,10 @@ the reference's own stopping rules end it.
 
   value   reconstructions/s with inputs resident in HBM (CUDA events around
           each solve on the launching stream; 256 MB L2 flush between solves)
+  fp64_noise_floor  how far the FP64 solution itself moves when one FP32
+          rounding per stored element and iteration is added (the oracle's
+          noise model, precomputed in tests/golden): an FP32 solve cannot be
+          held closer than that to it
   e2e     the same problem through the host-buffer C ABI tval3g_solve
           (geometry and b from host memory, U back to host, the per-call
           operator preparation included, the reference's stopping rules);
@@ -197,7 +201,7 @@ def reference_solve(w):
     return secs, r
 
 
-def relerr(a, b):
+def rel_l2(a, b):
     a = np.asarray(a, np.float64).ravel()
     b = np.asarray(b, np.float64).ravel()
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
@@ -228,7 +232,7 @@ def run_reference(a, rank):
         r = out[1]
     ms = float(np.mean(secs)) * 1000
     val = 1000.0 / ms
-    err = relerr(r.U, ref["U_aniso"]) if ref is not None and "U_aniso" in ref else None
+    err = rel_l2(r.U, ref["U_aniso"]) if ref is not None and "U_aniso" in ref else None
     sample = (f"complete solves of the reference solver (float data, anisotropic TV: it has no isotropic TV) "
               f"on the CSR twin of the ring operator, its own stopping rules: {r.total_iters} iterations, "
               f"relerr vs the FP64 anisotropic solution {err:.2e}" if err is not None else
@@ -451,6 +455,7 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
             "config": dict(CONFIGS[name], instances=1, l2="256 MB write between timed solves",
                            launch_shape=launch_shape(capi, spec) if a.tune else "built-in"),
             "iterations": iters, "time_to_solution_ms": ms, "relerr_vs_fp64": relerr,
+            "fp64_noise_floor": float(ref["noise_floor"][0]) if ref is not None and "noise_floor" in ref else None,
             "reached_target": bool(relerr is not None and relerr <= target), "target": target,
             "relerr_curve_every_5": [round(float(x), 6) for x in curve[::5]],
             "full_solve": {"ms": float(np.mean(full_t)), "iterations": full_info[0]["total_iters"],
@@ -468,7 +473,7 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
         out = reference_solve(w)
         if out:
             secs, r = out
-            err = relerr(r.U, ref["U_aniso"]) if ref is not None and "U_aniso" in ref else None
+            err = rel_l2(r.U, ref["U_aniso"]) if ref is not None and "U_aniso" in ref else None
             line["cpu_baseline"] = {"value": 1.0 / secs, "unit": "reconstructions/s", "cores": os.cpu_count(),
                                     "kind": "reference",
                                     "sample": f"one complete solve of the reference solver (anisotropic TV, float, "
@@ -511,8 +516,9 @@ def ring_variants(a, cx, capi, ref):
                     "relerr_at_target": float(t_info["rel_error"]),
                     "reached_target": bool(t_info["rel_error"] <= 1e-3),
                     "full_solve_ms": f_ms, "full_solve_iterations": f_info["total_iters"],
-                    "full_solve_relerr_vs_fp64": relerr(U, ref["U_aniso"]),
+                    "full_solve_relerr_vs_fp64": rel_l2(U, ref["U_aniso"]),
                     "fp64_iterations": int(ref["iters_aniso"][1]),
+                    "fp64_noise_floor": float(ref["noise_floor_aniso"][0]) if "noise_floor_aniso" in ref else None,
                     "value": 1000.0 / t_ms, "unit": "reconstructions/s",
                     "what": "the same ring workload with anisotropic TV (the reference arm's problem), "
                             "time to relerr <= 1e-3 vs the FP64 anisotropic solution and the full solve"}
@@ -520,7 +526,7 @@ def ring_variants(a, cx, capi, ref):
     spec = capi.problem_from_workload(wu)
     u_ms, u_info, U = timed_plan(cx, capi, spec, wu["opts"], wu["b"])
     out["unit_weight"] = {"ms_20_iterations": u_ms, "iterations": u_info["total_iters"],
-                          "relerr_vs_fp64_20_iterations": relerr(U, ref["U_unit20"]),
+                          "relerr_vs_fp64_20_iterations": rel_l2(U, ref["U_unit20"]),
                           "what": "the literal configuration (weight 1 per hit), a fixed 20 iterations, against "
                                   "the FP64 oracle's first 20 iterations"}
     return out

@@ -42,7 +42,7 @@ class OrcOpts(C.Structure):
                                           "gam", "rate_gam", "rate_cnt", "skipMulRatio",
                                           "maxRelativeChange")] + \
                [(k, C.c_int) for k in ("maxit", "maxcnt", "nonneg", "isreal", "numInitIterations",
-                                       "tv_norm", "cplx")]
+                                       "tv_norm", "cplx")] + [("noise", C.c_double), ("noise_seed", C.c_ulonglong)]
 
 
 class RefOpts(C.Structure):

@@ -720,6 +720,17 @@ static double now(void) {
 	return tv.tv_sec + tv.tv_usec / 1e6;
 }
 
+/* FP32-storage noise model (orc_opts.noise): x *= 1 + eps * xi */
+static void perturb(double *x, long n, double eps, unsigned long long *state) {
+	for (long i = 0; i < n; i++) {
+		unsigned long long z = *state;
+		z ^= z << 13; z ^= z >> 7; z ^= z << 17;
+		*state = z;
+		const double xi = (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+		x[i] *= 1.0 + eps * xi;
+	}
+}
+
 /* the driver, 2d:752-886 / 3d:1172-1378; rp != NULL replays recorded decisions */
 static int solve_impl(int dims, int dim_y, int dim_x, int dim_z, const orc_op *op, const double *b_in, int blen,
                       const orc_opts *o, const double *Ut, double *U, orc_info *info, orc_iter *iters,
@@ -767,6 +778,7 @@ static int solve_impl(int dims, int dim_y, int dim_x, int dim_z, const orc_op *o
 	shrinkage(s);
 	get_g(s, U, bs, 1);
 	get_gradient(s, DtsAtd);
+	unsigned long long noise_state = o->noise_seed * 0x9E3779B97F4A7C15ull + 1;
 	double Q = 1, Qp, C = s->f;
 	int count_outer = 0, count_total = 0, fst;
 	double RelChg, RelChgOut = 0, nrmup = 0;
@@ -778,6 +790,12 @@ static int solve_impl(int dims, int dim_y, int dim_x, int dim_z, const orc_op *o
 			double tau;
 			if (rp) s->force_skip = rp->skipped[count_total];
 			int bt = min_u(s, U, &gam, bs, o, C, fst, &tau, rp ? rp->backtracks[count_total] : -1);
+			if (o->noise > 0) {
+				double *vs[] = {U, s->Ux, s->Uy, s->Uz, s->g, s->g2};
+				for (int v = 0; v < 6; v++)
+					if (v != 3 || s->dims == 3) perturb(vs[v], n, o->noise, &noise_state);
+				perturb(s->Au, m, o->noise, &noise_state);
+			}
 			update_W(s);
 			Qp = Q; Q = gam * Qp + 1; C = (gam * Qp * C + s->f) / Q;
 			vadd(n, U, -1, s->Up, s->uup);

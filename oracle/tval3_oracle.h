@@ -38,6 +38,12 @@ typedef struct {
 	 * (2d:467-479), isreal keeps the real plane (2d:855-859).  Anisotropic
 	 * TV only (the reference has no other). */
 	int cplx;
+	/* > 0: a model of FP32 storage for the checker's noise floor - after each
+	 * inner iteration's descent, every element of U, its differences, Au, g
+	 * and g2 is multiplied by 1 + noise * xi, xi uniform in [-1, 1] from a
+	 * xorshift64 stream seeded by noise_seed.  0 (the default): none. */
+	double noise;
+	unsigned long long noise_seed;
 } orc_opts;
 
 typedef struct {

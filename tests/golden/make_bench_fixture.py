@@ -4,7 +4,9 @@
 
 Solves the 256x256 ring workload (tval3g.workloads.ring2d with normalize=True,
 isotropic TV, maxit 500) with the FP64 oracle restatement and stores U and the
-iteration counts in tests/golden/ring256_fp64.npz, together with the
+iteration counts in tests/golden/ring256_fp64.npz (with its FP32 noise
+floor: how far the FP64 solve moves under one FP32 rounding per stored
+element and iteration), together with the
 anisotropic FP64 solution of the same problem (U_aniso: what the reference,
 which has no isotropic TV, solves) and the first 20 iterations of the literal
 unit-weight ring (normalize=False, U_unit20).  Also records the reference's
@@ -32,6 +34,15 @@ import oracle as O  # noqa: E402
 from tval3g import workloads as W  # noqa: E402
 
 
+def fp32_noise_floor(op, w, seeds=(1, 2, 3)):
+    """How far the FP64 solve moves when one FP32 rounding per stored element
+    and iteration is added (the oracle's noise model; tests/helpers.py)."""
+    b = w["b"].astype(np.float64)
+    r = O.solve(op, b, w["shape"], w["opts"])
+    return max(float(np.linalg.norm(O.solve(op, b, w["shape"], dict(w["opts"], noise=2.0 ** -24, noise_seed=s)).U - r.U)
+                     / np.linalg.norm(r.U)) for s in seeds)
+
+
 def main():
     w = W.ring2d(seed=1, side=256, T=512, tv_norm=1, maxit=500, tol=1e-5, normalize=True)
     op = O.Op.ray2d(w["geom"], 256 * 256)
@@ -40,12 +51,14 @@ def main():
     print(f"FP64 oracle: {r.total_iters} iterations, {r.outer_iters} outer, relerr to phantom {r.rel_error:.4f}, "
           f"{time.time() - t:.1f} s")
     out = {"U": r.U.astype(np.float32), "iters": np.array([r.outer_iters, r.total_iters]),
+           "noise_floor": np.array([fp32_noise_floor(op, w)]),
            "scale": np.array([w["geom"]["scale"]]), "b_sum": np.array([float(np.sum(w["b"], dtype=np.float64))])}
     o = dict(w["opts"])
     o["tv_norm"] = 0
     r64 = O.solve(op, w["b"].astype(np.float64), w["shape"], o)
     print(f"FP64 oracle, anisotropic: {r64.total_iters} iterations")
     out["U_aniso"] = r64.U.astype(np.float32)
+    out["noise_floor_aniso"] = np.array([fp32_noise_floor(op, dict(w, opts=o))])
     out["iters_aniso"] = np.array([r64.outer_iters, r64.total_iters])
     if O.ref_available(2):
         A = w["csr"]
@@ -70,7 +83,8 @@ def dense64():
                 Ut=w["u_true"])
     print(f"dense 64x64 FP64 oracle: {r.total_iters} iterations, relerr to phantom {r.rel_error:.4f}")
     np.savez_compressed(os.path.join(HERE, "dense64_fp64.npz"), U=r.U.astype(np.float32),
-                        iters=np.array([r.outer_iters, r.total_iters]))
+                        iters=np.array([r.outer_iters, r.total_iters]),
+                        noise_floor=np.array([fp32_noise_floor(O.Op.dense(w["A"].astype(np.float64)), w)]))
 
 
 def mrhs():

@@ -78,15 +78,15 @@ def test_double_overloads_accuracy_vs_reference_double(name, torch_cuda):
     double overload equals the float C ABI bit for bit,
     test_dropin_solves_equal_c_abi), so against the reference's own double
     build it is as accurate as an FP32 solve with FP64 reductions: measured
-    and bounded here at a fixed 20 iterations, 1e-4 relative (the reference's
-    own float build is printed beside it)."""
+    and bounded here at a fixed iteration count, 1e-4 relative (the reference's
+    own float build is printed beside it); the cases run 20 to 40 iterations."""
     from golden.cases import api_problem, build_case
     from helpers import golden, relerr
     from tval3g import capi
     c = build_case(name)
     g = golden(f"{name}.npz")
     U, info = capi.solve(api_problem(c, capi), c["b"].astype(np.float64).astype(np.float32), c["opts"])
-    assert info["total_iters"] == int(g["ref2_iters"][1]) == 20
+    assert info["total_iters"] == int(g["ref2_iters"][1])
     e, e_ref = relerr(U, g["ref2_U"]), relerr(g["ref0_U"], g["ref2_U"])
     print(f"{name}: drop-in vs the reference's double build {e:.2e} (the reference's float build {e_ref:.2e})")
     assert e <= 1e-4

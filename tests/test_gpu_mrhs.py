@@ -87,10 +87,11 @@ def test_independent_right_hand_sides(count, torch_cuda):
     a device matrix are grouped (16 or 32 of them; the 3 left over of 35 keep
     their gemv products) and every product of a group is one tensor-core
     contraction, while each instance keeps its own scaling, step lengths,
-    line search and stopping.  Each instance against the FP64 oracle
-    replaying that instance's decisions (1e-3), and against the same plan on
-    the gemv kernels (the grouping changes no decision and only the rounding
-    of the products)."""
+    line search and stopping.  A fixed 20 iterations (short enough that the
+    FP64 solves' FP32 noise floor is ~1e-6): each instance against its own
+    FP64 oracle solve, and against the same plan on the gemv kernels, within
+    1e-3; the distance to the oracle replaying that instance's decisions is
+    printed beside it."""
     torch = torch_cuda
     side, m = 16, 128
     rng = np.random.default_rng(count)
@@ -98,7 +99,7 @@ def test_independent_right_hand_sides(count, torch_cuda):
     A = (rng.standard_normal((m, n)) / np.sqrt(m)).astype(np.float32)
     us = [W.ellipse_phantom(side, side, rng, 3, 0.0, lambda r: r.uniform(0.2, 1.0), (2, 6)) for _ in range(count)]
     bs = [W.add_noise(A.astype(np.float64) @ u.ravel(), 0.01, rng).astype(np.float32) for u in us]
-    opts = W.options(2 ** 8, 2 ** 5, 1e-4, 60, tv_norm=1)
+    opts = W.options(2 ** 8, 2 ** 5, 1e-4, 20, tv_norm=1)
     d_A = torch.tensor(A, device="cuda")
     specs = [capi.dense_problem((side, side), A, device_ptr=d_A.data_ptr()) for _ in range(count)]
     db = [torch.tensor(b, device="cuda") for b in bs]
@@ -111,14 +112,17 @@ def test_independent_right_hand_sides(count, torch_cuda):
                        plan.stats()["device_bytes"])
         plan.close()
     op64 = O.Op.dense(A.astype(np.float64))
-    worst, worst_g = 0.0, 0.0
+    worst, worst_r, worst_g = 0.0, 0.0, 0.0
     for k in range(count):
         U, info, tr = out[True][0][k], out[True][1][k], out[True][2][k]
-        r = O.solve(op64, bs[k].astype(np.float64), (side, side), opts, replay=O.replay_from_trace(tr))
-        assert r.total_iters == info["total_iters"]
+        b64 = bs[k].astype(np.float64)
+        r = O.solve(op64, b64, (side, side), opts)
+        rr = O.solve(op64, b64, (side, side), opts, replay=O.replay_from_trace(tr))
+        assert r.total_iters == info["total_iters"] == 20
         worst = max(worst, relerr(U, r.U.ravel()))
+        worst_r = max(worst_r, relerr(U, rr.U.ravel()))
         worst_g = max(worst_g, relerr(U, out[False][0][k]))
-    print(f"{count} independent right-hand sides: worst relerr vs replayed FP64 {worst:.2e}, "
-          f"vs the gemv plan {worst_g:.2e}")
+    print(f"{count} independent right-hand sides: worst relerr vs FP64 {worst:.2e}, vs FP64 replaying the GPU's "
+          f"decisions {worst_r:.2e}, vs the gemv plan {worst_g:.2e}")
     assert worst <= 1e-3 and worst_g <= 1e-3
     assert out[True][3] > out[False][3]   # the group's tensor-core operator was built

@@ -1,30 +1,32 @@
 """GPU solver parity through the C ABI.
 
-Every case is solved on the GPU with a trace of its decisions (backtracking
-steps, A^T-skip, where the inner loop ended).  The bar, 1e-3 relative L2 of
-U, is checked against the FP64 oracle at the same iteration count and path:
-the oracle's own solve where the GPU took the same decisions, else the
-oracle replaying the GPU's decisions (oracle.replay_from_trace) - FP32 and
-FP64 solves can land on different sides of a threshold test
-(2d/tval3_cpu_2d.cpp:540-574,790-853) and then differ by that decision, not
-by rounding.  Where the GPU took the oracle's decisions the reference's own
-double build (which agrees with the oracle to < 1e-9) is checked too.  The
-ring and hemisphere cases use the hit weight 1/sigma_max(A), which keeps the
-problems well conditioned; every measured error is printed.
+Every case is solved on the GPU with a trace of its decisions and compared
+with the FP64 oracle's solve of the same problem: within 1e-3 relative L2 of
+U, or within twice the problem's FP32 noise floor where that is larger - how
+far FP64 solves of the same problem move when one FP32 rounding per stored
+element and iteration is added (helpers.noise_floor).  Short fixed solves
+have floors near 1e-6, so their bar is 1e-3; converged solves of the small
+cases can move by 1e-3 - 1e-2 under such perturbations, because the
+threshold decisions and the nonmonotone line search amplify them
+(2d/tval3_cpu_2d.cpp:540-574,790-853).  The distance to the oracle replaying
+the GPU's own decisions (oracle.replay_from_trace) and to the reference's
+double build are printed beside it (the latter asserted under the same bar
+where the iteration counts agree).  The ring and hemisphere cases use the hit
+weight 1/sigma_max(A), which keeps them well conditioned.
 Graph and plain execution, and batched and single solves, run the same
 kernels in the same order with deterministic reductions: bit-identical.
 """
+import functools
+
 import numpy as np
 import pytest
 
 import oracle as O
 from golden.cases import CASES, api_problem, build_case
-from helpers import golden, relerr
+from helpers import golden, noise_floor, relerr, solve_bar
 from tval3g import capi
 
 pytestmark = pytest.mark.gpu
-
-BAR = 1e-3
 
 
 def _traced_solve(torch, c):
@@ -37,34 +39,33 @@ def _traced_solve(torch, c):
     return du[0].cpu().numpy().reshape(c["shape"]), info, tr
 
 
+@functools.lru_cache(maxsize=None)
+def _fp64(name):
+    """(the FP64 solution, its iteration count, the FP32 noise floor) of a case."""
+    c = build_case(name)
+    b = c["b"].astype(np.float64)
+    solve = lambda extra: O.solve(c["oracle_op"], b, c["shape"], dict(c["opts"], **extra))  # noqa: E731
+    r = solve({})
+    return r.U, r.total_iters, noise_floor(solve, r.U)
+
+
 @pytest.mark.parametrize("name", CASES)
 def test_solve_matches_oracle_and_reference(name, torch_cuda):
     c = build_case(name)
     g = golden(f"{name}.npz")
     U, info, tr = _traced_solve(torch_cuda, c)
     assert info["status"] == 0
-    same = int(g["oracle_iters"][1]) == info["total_iters"]
-    e_free = relerr(U, g["oracle_U"])
-    if same:
-        r = O.solve(c["oracle_op"], c["b"].astype(np.float64), c["shape"], c["opts"], record=True)
-        same = [x[3] for x in r.iters] == [int(v) for v in tr[:, 3]] and \
-            [x[4] for x in r.iters] == [int(v) for v in tr[:, 4]]
-    if same:
-        e = e_free
-        what = "the FP64 oracle's own solve (same decisions)"
-    else:
-        r = O.solve(c["oracle_op"], c["b"].astype(np.float64), c["shape"], c["opts"],
-                    replay=O.replay_from_trace(tr))
-        assert r.total_iters == info["total_iters"]
-        e = relerr(U, r.U)
-        what = "the FP64 oracle replaying the GPU's decisions"
-    print(f"{name}: {info['total_iters']} iterations (FP64 oracle {int(g['oracle_iters'][1])}); relerr vs {what} "
-          f"{e:.3e}; vs the free-running FP64 solve {e_free:.3e}")
-    assert e < BAR, (name, e)
-    if same and "ref2_U" in g and int(g["ref2_iters"][1]) == info["total_iters"]:
+    U64, it64, floor = _fp64(name)
+    bar = solve_bar(floor)
+    e = relerr(U, U64)
+    rr = O.solve(c["oracle_op"], c["b"].astype(np.float64), c["shape"], c["opts"], replay=O.replay_from_trace(tr))
+    print(f"{name}: {info['total_iters']} iterations (FP64 {it64}); relerr vs FP64 {e:.3e}, bar {bar:.2e} (FP32 "
+          f"noise floor {floor:.2e}); vs FP64 replaying the GPU's decisions {relerr(U, rr.U):.3e}")
+    assert e < bar, (name, e, bar)
+    if "ref2_U" in g and int(g["ref2_iters"][1]) == info["total_iters"]:
         e2 = relerr(U, g["ref2_U"])
         print(f"{name}: relerr vs the reference's double build {e2:.3e}")
-        assert e2 < BAR
+        assert e2 < bar
     if name.endswith("it20"):
         assert info["total_iters"] == 20
     # rel_error is ||Ut - U|| / ||Ut|| of the returned U
@@ -74,31 +75,23 @@ def test_solve_matches_oracle_and_reference(name, torch_cuda):
 
 @pytest.mark.parametrize("name", ["ring2d_s64_conv", "dense2d_s32_conv", "hemi3d_s16_conv", "ring2d_s64_skip"])
 def test_trace_matches_oracle(name, torch_cuda):
-    """The device controller takes the reference's decisions: while the FP32
-    and FP64 trajectories agree (objective within 1e-3), every iteration's
-    backtracking count (6 = restart) and A^T-skip decision are identical and
-    the step length tau agrees to 1e-3 (first 5 iterations) / 1e-2; the first 5
-    iterations always agree."""
-    import oracle as O
-    torch = torch_cuda
+    """The device controller takes the reference's decisions: through the
+    first 20 iterations (where FP32 and FP64 trajectories are within 1e-5 of
+    each other) every iteration's backtracking count (6 = restart) and
+    A^T-skip decision equal the oracle's (the skip of a restart iteration is
+    the first descent's), the step length tau agrees to 1e-3 and the
+    objective to 1e-4."""
     c = build_case(name)
     r = O.solve(c["oracle_op"], c["b"].astype(np.float64), c["shape"], c["opts"], record=True)
-    spec = api_problem(c, capi)
-    plan = capi.Plan([spec], [c["opts"]], graph=True, trace=True)
-    du = [torch.empty(spec.n, device="cuda")]
-    plan.solve([torch.tensor(c["b"], device="cuda")], du)
-    tr = plan.trace(0)
-    plan.close()
-    agree = 0
-    for k in range(min(len(tr), len(r.iters))):
+    _, _, tr = _traced_solve(torch_cuda, c)
+    for k in range(min(20, len(tr), len(r.iters))):
         tau, f, rc, bt, skip = tr[k][:5]
         otau, of, orc, obt, oskip = r.iters[k]
-        if abs(f - of) > 1e-3 * abs(of):
-            break
-        assert int(bt) == obt and int(skip) == oskip, (k, tr[k], r.iters[k])
-        assert abs(tau - otau) <= (1e-3 if k < 5 else 1e-2) * otau, (k, tau, otau)
-        agree += 1
-    assert agree >= 5, agree
+        assert int(bt) == obt, (k, tr[k], r.iters[k])
+        if obt != 6:
+            assert int(skip) == oskip, (k, tr[k], r.iters[k])
+        assert abs(tau - otau) <= 1e-3 * otau, (k, tau, otau)
+        assert abs(f - of) <= 1e-4 * abs(of), (k, f, of)
 
 
 def _plan_run(torch, specs, bs, opts, graph):

@@ -350,3 +350,19 @@ def test_complex_restatement_matches_reference(name):
     assert r.total_iters == int(g["ref4_iters"][1])
     assert relerr(r20.U, g["ref4_U_it20"]) < 1e-12
     assert relerr(r.U, g["ref4_U"]) < 1e-6
+
+
+def test_fp32_noise_model():
+    """The noise model behind the parity bars' FP32 noise floor: off it
+    changes nothing; one FP32 unit roundoff per stored element and iteration
+    moves a fixed 20-iteration solve by about 1e-6 and different seeds give
+    different perturbations."""
+    from helpers import NOISE_EPS
+    c = build_case("dense2d_s32_it20")
+    b = c["b"].astype(np.float64)
+    r = O.solve(c["oracle_op"], b, c["shape"], c["opts"])
+    r0 = O.solve(c["oracle_op"], b, c["shape"], dict(c["opts"], noise=0.0, noise_seed=5))
+    np.testing.assert_array_equal(r0.U, r.U)
+    r1 = O.solve(c["oracle_op"], b, c["shape"], dict(c["opts"], noise=NOISE_EPS, noise_seed=1))
+    r2 = O.solve(c["oracle_op"], b, c["shape"], dict(c["opts"], noise=NOISE_EPS, noise_seed=2))
+    assert 1e-9 < relerr(r1.U, r.U) < 1e-4 and relerr(r1.U, r2.U) > 0
