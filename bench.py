@@ -323,9 +323,18 @@ def kernel_roofline(cx, capi, spec, w, kind):
         opa.apply_n(y, out_n, 3, trans=1, stream=s)
         ts, _ = cx.event_time(lambda: opa.apply_n(y, out_n, 1, trans=1, stream=s), 10)
         opa.close()
-        variants = {"gather_ms": kt["adjoint"], "atomics_ms": float(np.mean(ts)),
-                    "default": "gather" if kt["adjoint"] <= float(np.mean(ts)) else "atomics (not the default: "
-                                                                                "the gather is deterministic)"}
+        opp = capi.Operator(spec, adj_plain=True)
+        opp.apply_n(y, out_n, 3, trans=1, stream=s)
+        tp, _ = cx.event_time(lambda: opp.apply_n(y, out_n, 1, trans=1, stream=s), 10)
+        plain_index = opp.adjoint_index_bytes
+        opp.close()
+        variants = {"tiled_gather_ms": kt["adjoint"], "plain_gather_ms": float(np.mean(tp)),
+                    "atomics_ms": float(np.mean(ts)), "tiled_index_bytes": int(index),
+                    "plain_index_bytes": int(plain_index),
+                    "default": "tiled gather (deterministic)",
+                    "forms": "tiled: measurements of each 2D tile / 3D brick staged in shared memory, 16-bit "
+                             "positions per hit; plain: 4-byte traced-ray id per hit, measurements from L2; "
+                             "atomics: rays traced on the fly, atomic adds into the image"}
     peak, src = peak_hbm()
     if kind == "ray2d":
         # tiled adjoint: its index once (tile lists, 16-bit positions, offsets),
@@ -333,8 +342,10 @@ def kernel_roofline(cx, capi, spec, w, kind):
         bytes_ = index + 4 * m + 4 * n
         kname, prof, direction = "k_ray_adj_tiled (ray adjoint)", "ray_adjoint_tiled_ring256.md", "adjoint"
     elif kind == "ray3d":
-        bytes_ = index + 4 * m + 4 * n   # pixel pointers and ray ids, y once, image once
-        kname, prof, direction = "k_gather<ray adjoint>", "ray_adjoint_gather_hemi128.md", "adjoint"
+        # brick-tiled adjoint: its index once (brick lists, 16-bit positions,
+        # offsets), the measurement vector once, the image once
+        bytes_ = index + 4 * m + 4 * n
+        kname, prof, direction = "k_ray_adj_tiled (3D bricks)", "ray_adjoint_brick_hemi128.md", "adjoint"
     else:
         A = w["A"]
         # the solve's normal product A^T (A u): A once, u read, Au written and

@@ -67,6 +67,14 @@ extern "C" {
                                    variable TVAL3G_TUNE_CACHE names a file, on
                                    disk.  Results then equal the untuned ones
                                    within rounding (other summation order). */
+#define TVAL3G_RAY_ADJ_PLAIN 64    /* ray operators: the plain pixel-major gather
+                                   adjoint (4-byte traced-ray ids per hit,
+                                   measurements gathered from L2) instead of
+                                   the tiled one (2D: 16 x 16 pixel tiles; 3D:
+                                   8 x 8 x 4 voxel bricks; each tile's rays'
+                                   measurements staged in shared memory and
+                                   16-bit positions per hit).  A comparison
+                                   form; results equal within rounding. */
 #define TVAL3G_RAY_ADJ_ATOMICS 32  /* ray operators: the adjoint traces the rays
                                    on the fly and accumulates into the image
                                    with atomic adds (no pixel-major index),

@@ -306,3 +306,32 @@ def test_solve_with_atomics_adjoint(torch_cuda):
     print(f"solve with the atomics adjoint vs the gather form: {e:.2e}")
     assert info["total_iters"] == info0["total_iters"] == 20
     assert e < 1e-4
+
+
+@pytest.mark.parametrize("which", ["ring2d_s64_it20", "hemi3d_s16_it20", "hemi3d_mp2_s16", "ragged3d"])
+def test_tiled_adjoint_equals_plain_gather(which, torch_cuda):
+    """The tiled adjoint (2D tiles; 3D bricks of 8 x 8 x 4 voxels with their
+    rays' measurements staged in shared memory and 16-bit positions) against
+    the plain pixel-major gather (TVAL3G_RAY_ADJ_PLAIN) and the FP64 oracle,
+    on a volume whose sides are not multiples of the brick."""
+    torch = torch_cuda
+    if which == "ragged3d":
+        g = W.hemisphere_geometry(20, 96, 24, 8.5, np.random.default_rng(8))
+        g = dict(g, rv_x=20, rv_y=20, rv_z=20)
+        shape = (20, 20, 20)
+        spec, ref = capi.ray3d_problem(shape, g), O.Op.ray3d(g)
+    else:
+        c = build_case(which)
+        spec, ref = api_problem(c, capi), c["oracle_op"]
+    tiled, plain = capi.Operator(spec), capi.Operator(spec, adj_plain=True)
+    y = np.random.default_rng(2).standard_normal(tiled.rows).astype(np.float32)
+    a, b = torch.empty(tiled.cols, device="cuda"), torch.empty(tiled.cols, device="cuda")
+    tiled.apply(_dev(torch, y), a, trans=True)
+    plain.apply(_dev(torch, y), b, trans=True)
+    e64 = relerr(a.cpu().numpy(), ref.apply(y.astype(np.float64), trans=True))
+    ep = relerr(a.cpu().numpy(), b.cpu().numpy())
+    print(f"{which}: tiled adjoint vs FP64 {e64:.2e}, vs the plain gather {ep:.2e}; index bytes "
+          f"{tiled.adjoint_index_bytes} (tiled) vs {plain.adjoint_index_bytes} (plain)")
+    assert e64 < 1e-5 and ep < 1e-6
+    tiled.close()
+    plain.close()

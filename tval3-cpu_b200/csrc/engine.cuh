@@ -146,6 +146,9 @@ struct OpDev {
 	// tiles by decreasing list length, so the longest start first and the
 	// short ones fill the SMs that finish early.
 	int tiled;
+	int tile3;              // 3D: tiles are bricks of 8 x 8 x 4 voxels (x, y, z), ntx x nty per z layer
+	int ntiles;             // tiles (bricks) of the tiled adjoint
+	int nty;
 	int ntx;
 	int tmax;               // longest tile list
 	const int *tptr, *tmeas, *woff;

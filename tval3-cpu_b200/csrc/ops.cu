@@ -855,6 +855,15 @@ __global__ void __launch_bounds__(RAYT_ADJ_THREADS) k_ray_adj_tiled(const Inst *
 	if (half || !good) return;
 	acc += sacc[pw * 32 + lane];   // first half + second half
 	const int px = __ldg(op.tperm + (long long)t * RAYT_THREADS + threadIdx.x);   // this thread's pixel of the tile
+	if (op.tile3) {   // brick of BRICK_X x BRICK_Y x BRICK_Z voxels
+		const int bxy = op.ntx * op.nty;
+		const int x = (t % op.ntx) * BRICK_X + px % BRICK_X;
+		const int y = ((t % bxy) / op.ntx) * BRICK_Y + (px / BRICK_X) % BRICK_Y;
+		const int z = (t / bxy) * BRICK_Z + px / (BRICK_X * BRICK_Y);
+		if (x < op.rvx && y < op.rvy && (long long)z * op.rvx * op.rvy < I.n)
+			vselw(I, ys)[x + (long long)y * op.rvx + (long long)z * op.rvx * op.rvy] = (float)(acc * op.scale);
+		return;
+	}
 	const int x = (t % op.ntx) * RAYT + (px % RAYT), row = (t / op.ntx) * RAYT + (px / RAYT);
 	if (x < op.rvx && row < op.tH) vselw(I, ys)[x + row * op.rvx] = (float)(acc * op.scale);
 }
@@ -1036,6 +1045,8 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 		                             tiled_smem_bytes(RAYT_MAX_LIST)));
 		d.tiled = 1;
 		d.ntx = ntx;
+		d.nty = nty;
+		d.ntiles = nt;
 		d.tmax = (int)tmax;
 		d.tptr = tptr32; d.tmeas = tmeas; d.woff = woff32; d.sidx = sidx; d.tperm = perm;
 		owned.push_back(perm);
@@ -1046,6 +1057,234 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 	}
 	dev_free(tlen, s);
 	dev_free(tptr, s);
+	dev_free(wlen, s);
+	dev_free(woff, s);
+	return ok;
+}
+
+// --- 3D brick index (once per operator) --------------------------------------
+__global__ void k_entry_rows(long long rows, const int *rptr, int *row_of);
+static_assert(BRICK_X * BRICK_Y * BRICK_Z == RAYT_THREADS, "a brick has as many voxels as a 2D tile has pixels");
+
+__device__ __forceinline__ int brick_of(int v, int rvx, int rvy, int nbx, int nby) {
+	const int x = v % rvx, y = (v / rvx) % rvy, z = v / (rvx * rvy);
+	return x / BRICK_X + (y / BRICK_Y) * nbx + (z / BRICK_Z) * nbx * nby;
+}
+
+// run starts: hit k starts a run if it is its ray's first hit or lies in
+// another brick than the hit before it (row_of: the ray of every hit)
+__global__ void k_run_flags(long long total, const int *rptr, const int *row_of, const int *rind, int rvx, int rvy,
+                            int nbx, int nby, long long *flag) {
+	for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+	     k += (long long)gridDim.x * blockDim.x) {
+		const int r = row_of[k];
+		const int b = brick_of(rind[k], rvx, rvy, nbx, nby);
+		flag[k] = (k == rptr[r] || b != brick_of(rind[k - 1], rvx, rvy, nbx, nby)) ? 1 : 0;
+	}
+}
+
+// per run (rs: exclusive scan of the flags): its brick and its ray; the
+// identity row pointers of the run -> brick matrix
+__global__ void k_run_info(long long total, const long long *flag, const long long *rs, const int *row_of,
+                           const int *rind, int rvx, int rvy, int nbx, int nby, int *run_brick, int *run_ray,
+                           int *ident, long long runs) {
+	for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+	     k += (long long)gridDim.x * blockDim.x)
+		if (flag[k]) {
+			const long long j = rs[k];
+			run_brick[j] = brick_of(rind[k], rvx, rvy, nbx, nby);
+			run_ray[j] = row_of[k];
+		}
+	for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j <= runs; j += (long long)gridDim.x * blockDim.x)
+		ident[j] = (int)j;
+}
+
+// runs in brick order (bruns, brick offsets bptr): position of each run in
+// its brick's list, and the list of measurement indices (padded offsets tptr)
+__global__ void k_run_pos(long long runs, const int *bruns, const int *bptr, const int *run_brick, const int *run_ray,
+                          const int *live_out, const int *tptr, int *pos_of_run, int *tmeas) {
+	for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < runs;
+	     j += (long long)gridDim.x * blockDim.x) {
+		const int r = bruns[j], b = run_brick[r];
+		const int pos = (int)(j - bptr[b]);
+		pos_of_run[r] = pos;
+		tmeas[tptr[b] + pos] = live_out[run_ray[r]];
+	}
+}
+
+// per hit in traced order: its 1-based position in its brick's list
+__global__ void k_hit_pos(long long total, const long long *rs, const int *pos_of_run, float *posf) {
+	for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+	     k += (long long)gridDim.x * blockDim.x)
+		posf[k] = (float)(pos_of_run[rs[k + 1] - 1] + 1);
+}
+
+__device__ __forceinline__ int brick_voxel(int t, int px, int rvx, int rvy, int rvz, int nbx, int nby) {
+	const int bxy = nbx * nby;
+	const int x = (t % nbx) * BRICK_X + px % BRICK_X;
+	const int y = ((t % bxy) / nbx) * BRICK_Y + (px / BRICK_X) % BRICK_Y;
+	const int z = (t / bxy) * BRICK_Z + px / (BRICK_X * BRICK_Y);
+	return (x < rvx && y < rvy && z < rvz) ? x + y * rvx + z * rvx * rvy : -1;
+}
+
+// per brick: its voxels by decreasing list length (perm[rank] = voxel of the
+// brick), the word count of every warp of ranks (32 x its longest list in
+// 16-byte words of eight positions)
+__global__ void __launch_bounds__(RAYT_THREADS) k_brick_count(int rvx, int rvy, int rvz, int nbx, int nby,
+                                                              const int *cptr, long long *wlen, unsigned char *perm) {
+	__shared__ int cnt[RAYT_THREADS];
+	__shared__ int byrank[RAYT_THREADS];
+	const int t = blockIdx.x;
+	const int p = brick_voxel(t, threadIdx.x, rvx, rvy, rvz, nbx, nby);
+	const int mine = p >= 0 ? cptr[p + 1] - cptr[p] : 0;
+	cnt[threadIdx.x] = mine;
+	__syncthreads();
+	int rank = 0;
+	for (int q = 0; q < RAYT_THREADS; q++) {
+		const int o = cnt[q];
+		rank += (o > mine || (o == mine && q < (int)threadIdx.x)) ? 1 : 0;
+	}
+	perm[(long long)t * RAYT_THREADS + rank] = (unsigned char)threadIdx.x;
+	byrank[rank] = mine;
+	__syncthreads();
+	const int nv = __reduce_max_sync(0xffffffffu, (byrank[threadIdx.x] + 7) >> 3);
+	if ((threadIdx.x & 31) == 0) wlen[(long long)t * RAYT_WARPS + (threadIdx.x >> 5)] = 32LL * nv;
+}
+
+// per brick, thread = rank: its voxel's positions packed eight to a 16-byte
+// word, the words of a warp's 32 voxels interleaved, padded with 0
+__global__ void __launch_bounds__(RAYT_THREADS) k_brick_fill(int rvx, int rvy, int rvz, int nbx, int nby,
+                                                             const int *cptr, const float *cval, const long long *woff,
+                                                             const unsigned char *perm, uint4 *sidx) {
+	const int t = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	const int p = brick_voxel(t, perm[(long long)t * RAYT_THREADS + threadIdx.x], rvx, rvy, rvz, nbx, nby);
+	const long long wl = (long long)t * RAYT_WARPS + wid;
+	const long long v0 = woff[wl];
+	const int nv = (int)((woff[wl + 1] - v0) >> 5);
+	int k = p >= 0 ? cptr[p] : 0;
+	const int k1 = p >= 0 ? cptr[p + 1] : 0;
+	for (int v = 0; v < nv; v++) {
+		unsigned e[8];
+#pragma unroll
+		for (int j = 0; j < 8; j++) e[j] = k < k1 ? (unsigned)cval[k++] : 0u;
+		sidx[v0 + 32LL * v + lane] = make_uint4(e[0] | (e[1] << 16), e[2] | (e[3] << 16), e[4] | (e[5] << 16),
+		                                        e[6] | (e[7] << 16));
+	}
+}
+
+float *brick_positions(cudaStream_t s, int rvx, int rvy, int rvz, int nrays, long long total, const int *rptr,
+                       const int *rind, const int *live_out, BrickLists &bl, std::vector<void *> &owned) {
+	if (nrays <= 0 || total <= 0) return nullptr;
+	bl.nbx = (rvx + BRICK_X - 1) / BRICK_X;
+	bl.nby = (rvy + BRICK_Y - 1) / BRICK_Y;
+	bl.nbz = (rvz + BRICK_Z - 1) / BRICK_Z;
+	const long long nb = (long long)bl.nbx * bl.nby * bl.nbz;
+	if (nb >= (1LL << 31)) return nullptr;
+	bl.nb = (int)nb;
+	const unsigned grid = (unsigned)std::min(8192LL, (total + 255) / 256);
+	int *row_of = (int *)dev_alloc(sizeof(int) * (size_t)total, s);
+	long long *flag = (long long *)dev_alloc(sizeof(long long) * (size_t)(total + 1), s);
+	long long *rs = (long long *)dev_alloc(sizeof(long long) * (size_t)(total + 1), s);
+	k_entry_rows<<<(unsigned)(((long long)nrays * 32 + 255) / 256), 256, 0, s>>>(nrays, rptr, row_of);
+	k_run_flags<<<grid, 256, 0, s>>>(total, rptr, row_of, rind, rvx, rvy, bl.nbx, bl.nby, flag);
+	TG_CUDA(cudaGetLastError());
+	scan_counts(s, flag, rs, total);
+	long long runs = 0;
+	TG_CUDA(cudaMemcpyAsync(&runs, rs + total, sizeof(long long), cudaMemcpyDeviceToHost, s));
+	TG_CUDA(cudaStreamSynchronize(s));
+	float *posf = nullptr;
+	int *run_brick = (int *)dev_alloc(sizeof(int) * (size_t)runs, s);
+	int *run_ray = (int *)dev_alloc(sizeof(int) * (size_t)runs, s);
+	int *ident = (int *)dev_alloc(sizeof(int) * (size_t)(runs + 1), s);
+	int *bptr = (int *)dev_alloc(sizeof(int) * (size_t)(nb + 1), s);
+	int *bruns = (int *)dev_alloc(sizeof(int) * (size_t)runs, s);
+	k_run_info<<<grid, 256, 0, s>>>(total, flag, rs, row_of, rind, rvx, rvy, bl.nbx, bl.nby, run_brick, run_ray, ident,
+	                                runs);
+	TG_CUDA(cudaGetLastError());
+	// the runs of every brick in traced (ray) order: the transpose of the
+	// run -> brick matrix
+	build_transpose(s, runs, nb, runs, ident, run_brick, nullptr, bptr, bruns, nullptr);
+	std::vector<int> h_bptr((size_t)nb + 1);
+	TG_CUDA(cudaMemcpyAsync(h_bptr.data(), bptr, sizeof(int) * (size_t)(nb + 1), cudaMemcpyDeviceToHost, s));
+	TG_CUDA(cudaStreamSynchronize(s));
+	bl.h_tptr.assign((size_t)nb + 1, 0);
+	bl.tmax = 0;
+	for (long long b = 0; b < nb; b++) {
+		const long long len = h_bptr[b + 1] - h_bptr[b];
+		bl.tmax = std::max(bl.tmax, len);
+		bl.h_tptr[b + 1] = bl.h_tptr[b] + (len + 3) / 4 * 4;
+	}
+	if (bl.tmax <= RAYT_MAX_LIST && bl.h_tptr[nb] < (1LL << 31)) {
+		std::vector<int> t32((size_t)nb + 1);
+		for (long long b = 0; b <= nb; b++) t32[b] = (int)bl.h_tptr[b];
+		bl.tptr = (int *)dev_alloc(sizeof(int) * (size_t)(nb + 1), s);
+		owned.push_back(bl.tptr);
+		TG_CUDA(cudaMemcpyAsync(bl.tptr, t32.data(), sizeof(int) * (size_t)(nb + 1), cudaMemcpyHostToDevice, s));
+		const long long tl = std::max(bl.h_tptr[nb], 4LL);
+		bl.tmeas = (int *)dev_alloc(sizeof(int) * (size_t)tl, s);
+		owned.push_back(bl.tmeas);
+		TG_CUDA(cudaMemsetAsync(bl.tmeas, 0, sizeof(int) * (size_t)tl, s));
+		int *pos_of_run = (int *)dev_alloc(sizeof(int) * (size_t)runs, s);
+		k_run_pos<<<(unsigned)std::min(8192LL, (runs + 255) / 256), 256, 0, s>>>(runs, bruns, bptr, run_brick, run_ray,
+		                                                                          live_out, bl.tptr, pos_of_run, bl.tmeas);
+		posf = (float *)dev_alloc(sizeof(float) * (size_t)total, s);
+		k_hit_pos<<<grid, 256, 0, s>>>(total, rs, pos_of_run, posf);
+		TG_CUDA(cudaGetLastError());
+		dev_free(pos_of_run, s);
+	}
+	dev_free(row_of, s);
+	dev_free(flag, s);
+	dev_free(rs, s);
+	dev_free(run_brick, s);
+	dev_free(run_ray, s);
+	dev_free(ident, s);
+	dev_free(bptr, s);
+	dev_free(bruns, s);
+	return posf;
+}
+
+bool build_brick_words(cudaStream_t s, int rvx, int rvy, int rvz, const int *cptr, const float *cval,
+                       BrickLists &bl, OpDev &d, long long *bytes, std::vector<void *> &owned) {
+	const int nb = bl.nb;
+	const long long nw = (long long)nb * RAYT_WARPS;
+	long long *wlen = (long long *)dev_alloc(sizeof(long long) * (size_t)(nw + 1), s);
+	long long *woff = (long long *)dev_alloc(sizeof(long long) * (size_t)(nw + 1), s);
+	unsigned char *perm = (unsigned char *)dev_alloc((size_t)nb * RAYT_THREADS, s);
+	k_brick_count<<<nb, RAYT_THREADS, 0, s>>>(rvx, rvy, rvz, bl.nbx, bl.nby, cptr, wlen, perm);
+	TG_CUDA(cudaGetLastError());
+	scan_counts(s, wlen, woff, nw);
+	long long words = 0;
+	TG_CUDA(cudaMemcpyAsync(&words, woff + nw, sizeof(long long), cudaMemcpyDeviceToHost, s));
+	TG_CUDA(cudaStreamSynchronize(s));
+	const bool ok = words < (1LL << 31);
+	if (ok) {
+		std::vector<int> order(nb);
+		for (int t = 0; t < nb; t++) order[t] = t;
+		std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+			return bl.h_tptr[a + 1] - bl.h_tptr[a] > bl.h_tptr[b + 1] - bl.h_tptr[b];
+		});
+		int *torder = (int *)dev_alloc(sizeof(int) * nb, s);
+		TG_CUDA(cudaMemcpyAsync(torder, order.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
+		uint4 *sidx = (uint4 *)dev_alloc(sizeof(uint4) * (size_t)std::max(words, 1LL), s);
+		int *woff32 = (int *)dev_alloc(sizeof(int) * (size_t)(nw + 1), s);
+		owned.push_back(torder); owned.push_back(sidx); owned.push_back(woff32); owned.push_back(perm);
+		k_brick_fill<<<nb, RAYT_THREADS, 0, s>>>(rvx, rvy, rvz, bl.nbx, bl.nby, cptr, cval, woff, perm, sidx);
+		k_to_int<<<(unsigned)((nw + 1 + 255) / 256), 256, 0, s>>>(woff, woff32, nw + 1);
+		TG_CUDA(cudaGetLastError());
+		TG_CUDA(cudaFuncSetAttribute(k_ray_adj_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                             tiled_smem_bytes(RAYT_MAX_LIST)));
+		d.tiled = 1;
+		d.tile3 = 1;
+		d.ntx = bl.nbx;
+		d.nty = bl.nby;
+		d.ntiles = nb;
+		d.tmax = (int)bl.tmax;
+		d.tptr = bl.tptr; d.tmeas = bl.tmeas; d.woff = woff32; d.sidx = sidx; d.tperm = perm; d.torder = torder;
+		*bytes = (long long)sizeof(uint4) * words + (long long)sizeof(int) * (bl.h_tptr[nb] + 2 * (long long)nb + nw + 2) +
+		         (long long)nb * RAYT_THREADS;
+	} else {
+		dev_free(perm, s);
+	}
 	dev_free(wlen, s);
 	dev_free(woff, s);
 	return ok;

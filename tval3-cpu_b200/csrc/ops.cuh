@@ -1,6 +1,7 @@
 // Measurement operators of the TVAL3 solve (modk/tval3-cpu 2d/mat_mult.h,
 // 3d/mat_mult.h), batched over the instances of a plan.
 #pragma once
+#include <vector>
 #include <memory>
 #include <utility>
 
@@ -71,6 +72,31 @@ constexpr int ATOMIC_ZERO_TILE = 1024;
 bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr, const int *cind,
                        const int *live_out, OpDev &d, long long *bytes, std::vector<void *> &owned);
 int tiled_smem_bytes(int tmax);
+
+// The same tiled adjoint for 3D rays, over bricks of BRICK_X x BRICK_Y x
+// BRICK_Z voxels (as many as the 2D tile's pixels).  Built in two steps
+// around the voxel-major transpose of the traced hits:
+//  brick_positions (before it): splits every traced ray into its runs of
+//    consecutive hits in one brick (a Bresenham ray enters a brick once: its
+//    coordinates are monotone), lists each brick's rays in traced order
+//    (tmeas, padded to multiples of 4 from 16-byte boundaries) and returns,
+//    per hit in traced order, its 1-based position in its brick's list as a
+//    float (exact), for the transpose to carry; NULL when a list would exceed
+//    RAYT_MAX_LIST (the plain gather then stays).
+//  build_brick_words (after it, with the voxel-major positions cval): the
+//    per-brick voxel order, the interleaved 16-bit position words and the
+//    launch order; fills d's tiled fields.
+constexpr int BRICK_X = 8, BRICK_Y = 8, BRICK_Z = 4;
+struct BrickLists {
+	int nbx = 0, nby = 0, nbz = 0, nb = 0;
+	std::vector<long long> h_tptr;   // padded list offsets (host copy), nb + 1
+	int *tptr = nullptr, *tmeas = nullptr;
+	long long tmax = 0;
+};
+float *brick_positions(cudaStream_t s, int rvx, int rvy, int rvz, int nrays, long long total, const int *rptr,
+                       const int *rind, const int *live_out, BrickLists &bl, std::vector<void *> &owned);
+bool build_brick_words(cudaStream_t s, int rvx, int rvy, int rvz, const int *cptr, const float *cval,
+                       BrickLists &bl, OpDev &d, long long *bytes, std::vector<void *> &owned);
 // the dense normal product's launch: CTAs (one per SM), and rows per CTA per
 // band for an m x n operator A (0: the operator does not suit it - n not a
 // multiple of 4, A not 16-byte aligned, its slab or two bands do not fit),

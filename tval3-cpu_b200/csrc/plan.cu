@@ -361,15 +361,37 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		int *rind = dalloc_op<int>(s, st, total);
 		trace_rays(s, d.nrays, drays, d.rvx, d.rvy, rptr, rind, &total);
 		st.nnz = total;
+		d.adj_atomic = (flags & TVAL3G_RAY_ADJ_ATOMICS) != 0;
+		const bool tile_ok = !d.adj_atomic && !(flags & TVAL3G_RAY_ADJ_PLAIN);
+		// 3D: each hit's position in its brick's ray list, carried through the
+		// transpose (the brick-tiled adjoint)
+		BrickLists bl;
+		float *posf = nullptr, *cposf = nullptr;
+		if (is3 && tile_ok) {
+			int *lo = dalloc_op<int>(s, st, std::max(d.nrays, 1));
+			if (d.nrays > 0)
+				TG_CUDA(cudaMemcpyAsync(lo, st.ray_out.data(), sizeof(int) * d.nrays, cudaMemcpyHostToDevice, s));
+			posf = brick_positions(s, p.rv_x, p.rv_y, p.rv_z, d.nrays, total, rptr, rind, lo, bl, st.owned);
+			if (posf) cposf = (float *)dev_alloc(sizeof(float) * (size_t)std::max(total, 1LL), s);
+		}
 		int *cptr = dalloc_op<int>(s, st, n + 1);
 		int *cind = dalloc_op<int>(s, st, total);
-		build_transpose(s, d.nrays, n, total, rptr, rind, nullptr, cptr, cind, nullptr);
+		build_transpose(s, d.nrays, n, total, rptr, rind, posf, cptr, cind, cposf);
+		if (posf) {
+			long long ib = 0;
+			if (build_brick_words(s, p.rv_x, p.rv_y, p.rv_z, cptr, cposf, bl, d, &ib, st.owned)) {
+				st.bytes += ib;
+				st.adj_index_bytes = ib;
+			}
+			TG_CUDA(cudaStreamSynchronize(s));
+			dev_free(posf, s);
+			dev_free(cposf, s);
+		}
 		if (!is3 && n % p.ld == 0) {   // transposed image for the y-driven rays
 			d.xT = dalloc_op<float>(s, st, n);
 			d.tH = (int)(n / p.ld);
 		}
-		d.adj_atomic = (flags & TVAL3G_RAY_ADJ_ATOMICS) != 0;
-		if (!is3 && n % p.ld == 0 && d.nrays > 0 && d.nrays <= RAYT_MAX_RAYS && !d.adj_atomic) {
+		if (!is3 && n % p.ld == 0 && d.nrays > 0 && d.nrays <= RAYT_MAX_RAYS && tile_ok) {
 			// tiled adjoint (cind still holds traced-ray ids)
 			int *lo = dalloc_op<int>(s, st, d.nrays);
 			TG_CUDA(cudaMemcpyAsync(lo, st.ray_out.data(), sizeof(int) * d.nrays, cudaMemcpyHostToDevice, s));
@@ -577,7 +599,7 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 	for (int i = 0; i < cnt; i++) {
 		const OpDev &d = inst[i].op;
 		if (!d.tiled || d.adj_atomic) continue;
-		tb.add(i, (long long)d.ntx * ((d.tH + RAYT - 1) / RAYT));
+		tb.add(i, d.ntiles);
 		ob.tiled_tmax = std::max(ob.tiled_tmax, d.tmax);
 	}
 	tb.close(&ob.ray_adj_tiled);

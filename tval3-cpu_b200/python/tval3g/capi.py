@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(PKG, "lib", "libtval3g.so")
 OK, ERR_ARGUMENT, ERR_CUDA, ERR_NO_DEVICE, ERR_NONFINITE, ERR_INTERNAL = 0, -1, -2, -3, -4, -5
 OP_DENSE, OP_CSR, OP_RAY2D, OP_RAY3D = 0, 1, 2, 3
 TV_ANISO, TV_ISO = 0, 1
-DEVICE_INPUTS, GRAPH, TRACE, NO_TENSOR, TUNE, RAY_ADJ_ATOMICS = 1, 2, 4, 8, 16, 32
+DEVICE_INPUTS, GRAPH, TRACE, NO_TENSOR, TUNE, RAY_ADJ_ATOMICS, RAY_ADJ_PLAIN = 1, 2, 4, 8, 16, 32, 64
 
 _OPT_D = ("mu", "beta", "mu0", "beta0", "tol", "tol_inn", "c", "gamma", "gam", "rate_gam", "rate_cnt",
           "skipMulRatio", "maxRelativeChange")
@@ -306,7 +306,7 @@ class Plan:
     iteration loop is one CUDA graph with conditional nodes)."""
 
     def __init__(self, specs, opts_list, graph=True, device_inputs=False, trace=False, tensor=True, tune=False,
-                 adj_atomics=False):
+                 adj_atomics=False, adj_plain=False):
         n = len(specs)
         self.specs = specs
         self.count = n
@@ -315,7 +315,8 @@ class Plan:
         opts = (Options * n)(*[Options.from_dict(o) for o in opts_list])
         h = C.c_void_p()
         flags = (GRAPH if graph else 0) | (DEVICE_INPUTS if device_inputs else 0) | (TRACE if trace else 0) | \
-            (0 if tensor else NO_TENSOR) | (TUNE if tune else 0) | (RAY_ADJ_ATOMICS if adj_atomics else 0)
+            (0 if tensor else NO_TENSOR) | (TUNE if tune else 0) | (RAY_ADJ_ATOMICS if adj_atomics else 0) | \
+            (RAY_ADJ_PLAIN if adj_plain else 0)
         _check(lib().tval3g_plan_create(C.byref(h), n, probs, opts, flags))
         self.h = h
 
@@ -360,10 +361,11 @@ class Plan:
 class Operator:
     """A measurement operator on the device: apply(x, trans) with torch tensors."""
 
-    def __init__(self, spec: ProblemSpec, tensor=True, device_inputs=False, tune=False, adj_atomics=False):
+    def __init__(self, spec: ProblemSpec, tensor=True, device_inputs=False, tune=False, adj_atomics=False,
+                 adj_plain=False):
         h = C.c_void_p()
         flags = (0 if tensor else NO_TENSOR) | (DEVICE_INPUTS if device_inputs else 0) | (TUNE if tune else 0) | \
-            (RAY_ADJ_ATOMICS if adj_atomics else 0)
+            (RAY_ADJ_ATOMICS if adj_atomics else 0) | (RAY_ADJ_PLAIN if adj_plain else 0)
         _check(lib().tval3g_op_create(C.byref(h), C.byref(spec.p), flags))
         self.h = h
         r, c, z = C.c_longlong(), C.c_longlong(), C.c_longlong()
