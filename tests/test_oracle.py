@@ -354,9 +354,9 @@ def test_complex_restatement_matches_reference(name):
 
 def test_fp32_noise_model():
     """The noise model behind the parity bars' FP32 noise floor: off it
-    changes nothing; one FP32 unit roundoff per stored element and iteration
-    moves a fixed 20-iteration solve by about 1e-6 and different seeds give
-    different perturbations."""
+    changes nothing; a few FP32 unit roundoffs per stored element and
+    iteration move a fixed 20-iteration solve by about 1e-6 and different
+    seeds give different perturbations."""
     from helpers import NOISE_EPS
     c = build_case("dense2d_s32_it20")
     b = c["b"].astype(np.float64)
