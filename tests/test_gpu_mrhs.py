@@ -125,4 +125,4 @@ def test_independent_right_hand_sides(count, torch_cuda):
     print(f"{count} independent right-hand sides: worst relerr vs FP64 {worst:.2e}, vs FP64 replaying the GPU's "
           f"decisions {worst_r:.2e}, vs the gemv plan {worst_g:.2e}")
     assert worst <= 1e-3 and worst_g <= 1e-3
-    assert out[True][3] > out[False][3]   # the group's tensor-core operator was built
+    assert worst_g > 0   # the group's products ran on the tensor cores (other rounding than the gemv plan)

