@@ -776,6 +776,7 @@ def batch_measure(a, cx, capi, dist, clocks=None, ray_subset=True):
     plan.close()
     rel = {k: float(infos[k]["rel_error"]) for k in have_ut}
     fp64_iters = {k: int(fx[f"iters{k}"][1]) for k in have_ut}
+    floors = {k: float(fx[f"floor{k}"][0]) for k in have_ut if f"floor{k}" in fx}
     # plain: one instance per plan, host-driven loop, instances one after another
     singles = [capi.Plan([s], [o], graph=False, device_inputs=True) for s, o in zip(specs, opts)]
 
@@ -823,6 +824,12 @@ def batch_measure(a, cx, capi, dist, clocks=None, ray_subset=True):
             "dense_hbm_floor_ms": floor_ms, "batched_over_floor": ms_b / floor_ms,
             "relerr_vs_fp64": {"instances_checked": len(rel), "max": max(rel.values()) if rel else None,
                                "within_1e-3": sum(1 for v in rel.values() if v <= 1e-3),
+                               "within_noise_bar": sum(1 for k, v in rel.items() if k in floors and
+                                                       v <= max(1e-3, 2 * floors[k])),
+                               "noise_bar": "max(1e-3, 2 x the instance's FP32 noise floor: how far its FP64 "
+                                            "solve moves under a few FP32 roundings per stored element and "
+                                            "iteration)",
+                               "fp32_noise_floor": {str(k): round(v, 6) for k, v in floors.items()},
                                "per_instance": {str(k): round(v, 6) for k, v in rel.items()},
                                "iterations_gpu_vs_fp64": {str(k): [iters[k], fp64_iters[k]] for k in rel},
                                "subset": "the ring instances of side <= 192 and the dense ones of side <= 96 "

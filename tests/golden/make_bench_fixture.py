@@ -17,7 +17,8 @@ multi-RHS workload to mrhs32_fp64.npz, its 32 right-hand sides solved
 independently to mrhs32_indep_fp64.npz.  The mixed batch's FP64 subset (its
 ring instances of side <= 192 and its dense instances of side <= 96, dense A
 regenerated from the counter-based Gaussian stream the bench draws on the
-device) goes to batch_fp64.npz as U<k>, iters<k> per batch index k.
+device) goes to batch_fp64.npz as U<k>, iters<k> and the FP32 noise floor
+floor<k> (three seeds) per batch index k.
 """
 import os
 import sys
@@ -134,6 +135,7 @@ def batch():
         r = O.solve(op, w["b"].astype(np.float64), w["shape"], w["opts"])
         out[f"U{k}"] = r.U.astype(np.float32)
         out[f"iters{k}"] = np.array([r.outer_iters, r.total_iters])
+        out[f"floor{k}"] = np.array([fp32_noise_floor(op, w, seeds=(1, 2, 3))])
         print(f"batch {k}: {d['kind']} side {d['side']}: {r.total_iters} iterations ({time.time() - t0:.0f} s)")
     np.savez_compressed(os.path.join(HERE, "batch_fp64.npz"), **out)
 
