@@ -816,8 +816,25 @@ def batch_measure(a, cx, capi, dist, clocks=None, ray_subset=True):
             p.close()
         sub = {"instances": len(rays), "batched_ms": float(np.mean(trb)), "plain_ms": float(np.mean(trp)),
                "batched_over_plain": float(np.mean(trp)) / float(np.mean(trb))}
+    # the one-pass dense normal product A^T (A u) on the batch's largest matrix
+    big = max((k for k, s_ in enumerate(specs) if s_.p.op_kind == capi.OP_DENSE),
+              key=lambda k: specs[k].p.m * specs[k].p.n_cols, default=None)
+    normal = None
+    if big is not None:
+        sp = specs[big]
+        op = capi.Operator(sp, device_inputs=True)
+        xv, yv = torch.rand(op.cols, device=dev), torch.empty(op.cols, device=dev)
+        op.apply_n(xv, yv, 2, trans=2, stream=stream.cuda_stream)
+        tn, _ = cx.event_time(lambda: op.apply_n(xv, yv, 1, trans=2, stream=stream.cuda_stream), 5)
+        op.close()
+        a_bytes = 4.0 * sp.p.m * sp.p.n_cols + 4.0 * (2 * sp.p.n_cols + 2 * sp.p.m)
+        t_ms = float(np.mean(tn))
+        normal = {"m": sp.p.m, "n": sp.p.n_cols, "ms_per_launch": t_ms,
+                  "achieved_gbs": a_bytes / (t_ms * 1e-3) / 1e9, "frac": a_bytes / (t_ms * 1e-3) / 1e9 / peak,
+                  "kernel": "k_dense_normal (A read once: Au and A^T Au)"}
     del keep
     return {"instances": nb, "dense_instances": dense, "dense_bytes": int(dense_bytes),
+            "dense_normal_largest": normal,
             "plan_device_bytes": int(device_bytes), "batched_ms": ms_b, "plain_ms": ms_p,
             "batched_over_plain": ms_p / ms_b, "value": nb * 1000.0 / ms_b, "unit": "reconstructions/s",
             "plain_value": nb * 1000.0 / ms_p, "iterations_min_max": [min(iters), max(iters)],
@@ -849,6 +866,7 @@ def run_batch(a, cx, capi, world, dist, clocks):
                       "form": "one plan per instance, host-driven loop, instances in sequence"},
             "batched_over_plain": r["batched_over_plain"], "iterations_min_max": r["iterations_min_max"],
             "dense_hbm_floor_ms": r["dense_hbm_floor_ms"], "batched_over_floor": r["batched_over_floor"],
+            "dense_normal_largest": r["dense_normal_largest"],
             "relerr_vs_fp64": r["relerr_vs_fp64"], "ray_instances_only": r["ray_instances_only"],
             "clocks": r["clocks"], "gpu_launches": r["gpu_launches"]}
 
