@@ -128,8 +128,8 @@ def test_full_ring_operator_properties(torch_cuda):
 
 @pytest.mark.parametrize("m, shape", [
     (1229, (64, 64)),      # one band
-    (3000, (200, 200)),    # wide rows (n = 40000): CTAs own column slabs, A 480 MB
-    (601, (256, 256)),     # the widest slab (n = 65536), a ragged last row block
+    (3000, (200, 200)),    # rows too long for the band form (n = 40000): two-pass gemv, A 480 MB
+    (601, (256, 256)),     # n = 65536
     (2000, (100, 100)),    # the band form (n = 10000): bands of rows
     (100, (16, 20)),       # fewer rows than CTAs
     (500, (31, 33)),       # n not a multiple of 4: scalar loads

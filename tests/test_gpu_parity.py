@@ -136,9 +136,8 @@ def test_mrhs_10_iterations(torch_cuda):
 
 
 def test_dense128_wide_rows_20_iterations(torch_cuda):
-    """Dense 128x128 (A 4915 x 16384: rows long enough for the wide-row form
-    of the one-pass normal product, k_dense_normal_wide), 20 iterations,
-    within 1e-3 of the FP64 oracle."""
+    """Dense 128x128 (A 4915 x 16384, 322 MB: the one-pass normal product
+    with many bands), 20 iterations, within 1e-3 of the FP64 oracle."""
     w = W.dense2d(seed=5, side=128, sampling=0.3, tv_norm=1, maxit=20, tol=1e-4)
     U, info, tr = _gpu(torch_cuda, capi.problem_from_workload(w), w["b"], w["opts"])
     _check("dense 128^2", U, info, tr, O.Op.dense(w["A"].astype(np.float64)), w["b"], w["shape"], w["opts"], False)

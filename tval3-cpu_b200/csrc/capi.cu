@@ -26,7 +26,6 @@ struct tval3g_operator {
 	int2 *d_tiles = nullptr;
 	float *d_part = nullptr;
 	int *d_fused = nullptr;   // band flags of the one-pass dense normal product
-	float *d_fused_part = nullptr;   // its wide-row form's partial row dots
 	int *d_err = nullptr;     // set by a kernel whose bounded wait gave up
 	float *d_au = nullptr;    // A x of a normal product (trans = 2)
 	cudaStream_t s = nullptr;
@@ -255,10 +254,6 @@ int tval3g_op_create(tval3g_operator **out, const tval3g_problem *prob, int flag
 			TG_CUDA(cudaMalloc(&op->d_part, sizeof(float) * dense_part));
 			op->ob.dense_part = op->d_part;
 		}
-		if (op->ob.fused_part_words > 0) {
-			TG_CUDA(cudaMalloc(&op->d_fused_part, sizeof(float) * op->ob.fused_part_words));
-			op->ob.fused_part = op->d_fused_part;
-		}
 		if (op->ob.fused_words > 0) {
 			TG_CUDA(cudaMalloc(&op->d_fused, sizeof(int) * op->ob.fused_words));
 			TG_CUDA(cudaMemsetAsync(op->d_fused, 0, sizeof(int) * op->ob.fused_words, op->s));
@@ -388,7 +383,6 @@ int tval3g_op_destroy(tval3g_operator *op) {
 		cudaFree(op->d_tiles);
 		cudaFree(op->d_part);
 		cudaFree(op->d_fused);
-		cudaFree(op->d_fused_part);
 		cudaFree(op->d_err);
 		cudaFree(op->d_au);
 		if (op->s) cudaStreamDestroy(op->s);

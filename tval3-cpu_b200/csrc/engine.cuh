@@ -123,7 +123,6 @@ struct OpDev {
 	int dense_kchunks;     // row chunks of the transposed product
 	int fused_rpc;         // rows per CTA per band of the one-pass normal product (0: not used)
 	int fused_slab;        // its column slab per CTA
-	int fused_wide;        // 1: the wide-row form (k_dense_normal_wide: CTAs own column slabs of every row)
 	long long dense_part;  // offset of this instance in the dense partial buffer (floats)
 	// compressed gather operators: forward rows (CSR) and transpose (CSC)
 	const int *rptr, *rind;

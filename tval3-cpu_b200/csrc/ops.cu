@@ -408,221 +408,11 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_dense_normal(const Inst *t
 	}
 }
 
-// ---------------------------------------------------------------------------
-// The one-pass dense normal product for wide rows (k_dense_normal_wide).
-// The band form above keeps two bands of whole rows in L2, which rows of
-// 64K columns no longer fit (a band of 148 such rows is 38 MB).  Here CTA c
-// owns the column slab [c S, c S + S) of every row instead, and the rows go
-// by blocks of WIDE_RB:
-//   producer (warp 0): bulk-copies the block's slab tile (WIDE_RB row
-//     segments of S floats, 16-byte aligned) into a ring of WIDE_NS stages;
-//   consumers (warps 1-7, two rows each): the tile's partial row dots over
-//     the slab (FP32), written to part[row][c]; after the block, a release
-//     increment of flagA[block];
-//   reducers (warps 8-15): CTA block % grid sums the block's grid partials of
-//     every row in CTA order (FP64) into Au and releases flagB[block]; every
-//     CTA then reads those Au rows and adds tile^T Au into the slab's FP64
-//     accumulators - from the tile still in shared memory - and frees the
-//     stage.
-// A is read from HBM once and never from L2 again; each CTA writes its own
-// columns of g, so no cross-CTA reduction of g is needed.  The producer runs
-// up to WIDE_NS blocks ahead, which hides the two flag hops.  All CTAs must
-// be co-resident (cooperative launch).  Every wait is bounded: one that
-// gives up sets *err and the CTA's abort flag, after which no role waits
-// again, the named barriers are still passed the same number of times, every
-// stage is still released, and the producer lets its copies in flight land
-// before the CTA exits.  Deterministic: fixed summation orders throughout.
-// ---------------------------------------------------------------------------
-constexpr int WIDE_RB = 14;                        // rows per block (two per consumer warp)
-constexpr int WIDE_NS = 6;                         // stages
-constexpr int WIDE_SMAX = 512;                     // slab width limit (floats)
-constexpr long long WIDE_MIN_N = 16384;            // below: the band form
-constexpr int WIDE_STAGE_BYTES = WIDE_RB * WIDE_SMAX * 4;
-constexpr int WIDE_DYN_BYTES = WIDE_NS * WIDE_STAGE_BYTES + WIDE_SMAX * 4 + (2 * WIDE_NS + 1) * 8;
-
-__global__ void __launch_bounds__(FUSED_THREADS, 1) k_dense_normal_wide(const Inst *tab, int inst, int pred,
-                                                                        VecSel us, VecSel aus, VecSel gs, int *flags,
-                                                                        float *part, int *err,
-                                                                        unsigned long long *launches) {
-	if (launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);
-	const Inst &I = tab[inst];
-	if (!pred_ok(*I.ctrl, pred)) return;   // the same in every CTA: ctrl is not written here
-	extern __shared__ __align__(128) unsigned char dsm[];
-	__shared__ float sau[WIDE_RB];
-	__shared__ double sred[FUSED_ROLE * 4];
-	__shared__ volatile int s_abort;
-	const OpDev &op = I.op;
-	const int m = (int)op.m, n = (int)op.n;
-	const int G = gridDim.x, c = blockIdx.x;
-	const int S = op.fused_slab;
-	const int c0 = min(n, c * S), c1 = min(n, c0 + S), Sc = c1 - c0;   // this CTA's slab (Sc % 4 == 0)
-	const int nb = (m + WIDE_RB - 1) / WIDE_RB;
-	int *flagA = flags, *flagB = flags + nb;
-	const float *A = op.A;
-	float *st_base = reinterpret_cast<float *>(dsm);
-	float *su = reinterpret_cast<float *>(dsm + WIDE_NS * WIDE_STAGE_BYTES);   // u over the slab
-	const unsigned full0 = smem_u32(dsm + WIDE_NS * WIDE_STAGE_BYTES + WIDE_SMAX * 4);
-	const unsigned empty0 = full0 + 8u * WIDE_NS, ubar = empty0 + 8u * WIDE_NS;
-	auto stage = [&](int st) { return st_base + st * (WIDE_RB * WIDE_SMAX); };
-	if (threadIdx.x == 0) {
-		s_abort = 0;
-		for (int st = 0; st < WIDE_NS; st++) {
-			mbar_init(full0 + 8u * st, 1);
-			mbar_init(empty0 + 8u * st, FUSED_ROLE / 32);   // the reducer warps
-		}
-		mbar_init(ubar, 1);
-		fence_mbar_init();
-	}
-	__syncthreads();
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	if (warp == 0) {
-		// ---- producer ----
-		if (lane == 0) {
-			const float *u = vsel(I, us);
-			mbar_expect_tx(ubar, 4u * Sc);
-			if (Sc > 0) bulk_g2s(smem_u32(su), u + c0, 4u * Sc, ubar);
-			int k = 0;
-			for (; k < nb && !s_abort; k++) {
-				const int st = k % WIDE_NS;
-				if (k >= WIDE_NS && !mbar_wait1(empty0 + 8u * st, (unsigned)(k / WIDE_NS - 1) & 1u, err)) {
-					s_abort = 1;
-					break;
-				}
-				const int r0 = k * WIDE_RB, rows = min(WIDE_RB, m - r0);
-				mbar_expect_tx(full0 + 8u * st, 4u * Sc * rows);
-				if (Sc > 0)
-					for (int r = 0; r < rows; r++)
-						bulk_g2s(smem_u32(stage(st) + r * WIDE_SMAX), A + (long long)(r0 + r) * n + c0, 4u * Sc,
-						         full0 + 8u * st);
-			}
-			if (s_abort) {   // let the copies in flight land before the CTA exits (bounded)
-				mbar_wait1(ubar, 0u, err);
-				for (int kk = k > WIDE_NS ? k - WIDE_NS : 0; kk < k; kk++)
-					mbar_wait1(full0 + 8u * (kk % WIDE_NS), (unsigned)(kk / WIDE_NS) & 1u, err);
-			}
-		}
-	} else if (warp < 8) {
-		// ---- consumers: partial row dots over the slab ----
-		const int cw = warp - 1, ct = threadIdx.x - 32;
-		if (!mbar_wait_warp(ubar, 0u, err) && lane == 0) s_abort = 1;
-		for (int k = 0; k < nb; k++) {
-			const int st = k % WIDE_NS;
-			const int r0 = k * WIDE_RB, rows = min(WIDE_RB, m - r0);
-			if (!s_abort && !mbar_wait_warp(full0 + 8u * st, (unsigned)(k / WIDE_NS) & 1u, err))
-				if (lane == 0) s_abort = 1;
-			if (!s_abort)
-				for (int r = cw; r < rows; r += FUSED_CONS / 32) {
-					const float *a = stage(st) + r * WIDE_SMAX;
-					float p = 0.f;
-					for (int j = lane * 4; j < Sc; j += 128) {
-						const float4 av = *reinterpret_cast<const float4 *>(a + j);
-						const float4 uv = *reinterpret_cast<const float4 *>(su + j);
-						p = fmaf(av.x, uv.x, p);
-						p = fmaf(av.y, uv.y, p);
-						p = fmaf(av.z, uv.z, p);
-						p = fmaf(av.w, uv.w, p);
-					}
-					p = warp_sumf(p);
-					if (lane == 0) part[(long long)(r0 + r) * G + c] = p;
-				}
-			__threadfence();
-			named_sync(1, FUSED_CONS);
-			if (ct == 0 && !s_abort) atomicAdd(&flagA[k], 1);
-		}
-	} else {
-		// ---- reducers ----
-		const int t = threadIdx.x - FUSED_ROLE;
-		const int SV = Sc / 4;                                        // float4 columns of the slab (<= 128)
-		const int Q = SV > 0 ? FUSED_ROLE / SV : 1;                  // row groups
-		const int j = SV > 0 ? t % SV : 0, q = SV > 0 ? t / SV : FUSED_ROLE;
-		const bool act = SV > 0 && q < Q;
-		float *au = vselw(I, aus);
-		double acc[4] = {0.0, 0.0, 0.0, 0.0};
-		for (int k = 0; k < nb; k++) {
-			const int st = k % WIDE_NS;
-			const int r0 = k * WIDE_RB, rows = min(WIDE_RB, m - r0);
-			if (k % G == c) {   // this CTA sums the block's partials into Au
-				if (t == 0 && !s_abort) {
-					unsigned sp = 0;
-					while (ld_acquire(flagA + k) < G) {
-						if (++sp > FUSED_SPIN_MAX) { atomicExch(err, 1); s_abort = 1; break; }
-						__nanosleep(32);
-					}
-				}
-				named_sync(2, FUSED_ROLE);
-				if (!s_abort && t < rows) {
-					double sum = 0.0;
-					const float *pr = part + (long long)(r0 + t) * G;
-					for (int cc = 0; cc < G; cc++) sum += (double)__ldcg(pr + cc);
-					au[r0 + t] = (float)sum;
-					__threadfence();
-				}
-				named_sync(2, FUSED_ROLE);
-				if (t == 0 && !s_abort) atomicExch(&flagB[k], 1);
-			}
-			if (t == 0 && !s_abort) {
-				unsigned sp = 0;
-				while (ld_acquire(flagB + k) < 1) {
-					if (++sp > FUSED_SPIN_MAX) { atomicExch(err, 1); s_abort = 1; break; }
-					__nanosleep(32);
-				}
-			}
-			named_sync(2, FUSED_ROLE);
-			if (!s_abort && t < rows) sau[t] = __ldcg(au + r0 + t);
-			// the tile landed (this CTA's consumers published the block after it did)
-			if (!s_abort && !mbar_wait_warp(full0 + 8u * st, (unsigned)(k / WIDE_NS) & 1u, err) && lane == 0)
-				s_abort = 1;
-			named_sync(2, FUSED_ROLE);
-			if (act && !s_abort) {
-				const float *a = stage(st) + 4 * j;
-				float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
-				for (int r = q; r < rows; r += Q) {
-					const float4 v = *reinterpret_cast<const float4 *>(a + r * WIDE_SMAX);
-					const float w = sau[r];
-					p0 = fmaf(v.x, w, p0);
-					p1 = fmaf(v.y, w, p1);
-					p2 = fmaf(v.z, w, p2);
-					p3 = fmaf(v.w, w, p3);
-				}
-				acc[0] += (double)p0; acc[1] += (double)p1; acc[2] += (double)p2; acc[3] += (double)p3;
-			}
-			named_sync(2, FUSED_ROLE);
-			if (lane == 0) mbar_arrive(empty0 + 8u * st);   // the stage is free (also after an abort)
-		}
-		// the row groups' sums of each column, in group order
-		if (act)
-#pragma unroll
-			for (int e = 0; e < 4; e++) sred[q * (4 * SV) + 4 * j + e] = acc[e];
-		named_sync(2, FUSED_ROLE);
-		float *gv = vselw(I, gs);
-		if (!s_abort)
-			for (int col = t; col < Sc; col += FUSED_ROLE) {
-				double tot = 0.0;
-				for (int qq = 0; qq < Q; qq++) tot += sred[qq * (4 * SV) + col];
-				gv[c0 + col] = (float)tot;
-			}
-	}
-}
-
-bool fused_wide_fits(long long m, long long n, int grid, const float *A, int *slab, long long *blocks,
-                     long long *part_floats) {
-	if (m < 1 || n < WIDE_MIN_N || m >= (1LL << 31) / 2 || n % 4 != 0 || (reinterpret_cast<uintptr_t>(A) & 15) != 0)
-		return false;
-	long long S = (n + grid - 1) / grid;
-	S = (S + 3) / 4 * 4;
-	if (S > WIDE_SMAX || (FUSED_ROLE / (S / 4)) * S > FUSED_ROLE * 4) return false;
-	*slab = (int)S;
-	*blocks = (m + WIDE_RB - 1) / WIDE_RB;
-	*part_floats = *blocks * WIDE_RB * grid;
-	return true;
-}
-
 int fused_grid() {
 	int dev = 0, sms = 0;
 	TG_CUDA(cudaGetDevice(&dev));
 	TG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
 	TG_CUDA(cudaFuncSetAttribute(k_dense_normal, cudaFuncAttributeMaxDynamicSharedMemorySize, FUSED_DYN_BYTES));
-	TG_CUDA(cudaFuncSetAttribute(k_dense_normal_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, WIDE_DYN_BYTES));
 	return std::max(1, std::min(sms, FUSED_GRID_MAX));
 }
 
@@ -1572,14 +1362,6 @@ void op_fused_normal(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, V
 		TG_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * f.bands, L.stream));
 		int inst = f.inst;
 		const Inst *tab = L.inst;
-		if (f.wide) {   // f.bands = 2 x row blocks (flagA, flagB)
-			float *part = B.fused_part;
-			void *args[] = {(void *)&tab, (void *)&inst, (void *)&pred, (void *)&x, (void *)&y, (void *)&z,
-			                (void *)&flags, (void *)&part, (void *)&err, (void *)&ctr};
-			TG_CUDA(cudaLaunchCooperativeKernel((const void *)k_dense_normal_wide, dim3(B.fused_grid),
-			                                    dim3(FUSED_THREADS), args, WIDE_DYN_BYTES, L.stream));
-			continue;
-		}
 		void *args[] = {(void *)&tab, (void *)&inst, (void *)&pred, (void *)&x, (void *)&y, (void *)&z,
 		                (void *)&flags, (void *)&err, (void *)&ctr};
 		TG_CUDA(cudaLaunchCooperativeKernel((const void *)k_dense_normal, dim3(B.fused_grid), dim3(FUSED_THREADS),

@@ -31,11 +31,8 @@ struct OpBatch {
 		int inst;
 		int bands;
 		long long off;   // of its band flags in fused_flags
-		int wide;        // the wide-row form (bands = 2 x its row blocks of flags)
 	};
 	std::vector<Fused> fused;
-	float *fused_part = nullptr;   // wide-row form: the CTAs' partial row dots (max m_pad x grid floats)
-	long long fused_part_words = 0;
 	TileMap dense_fwd_nf, dense_adj_nf, dense_red_nf;
 	int fused_grid = 0;
 	long long fused_words = 0;   // band flags of all fused instances
@@ -106,11 +103,6 @@ bool build_brick_words(cudaStream_t s, int rvx, int rvy, int rvz, const int *cpt
 // with the slab width
 int fused_grid();
 int fused_rows_per_cta(long long m, long long n, int grid, const float *A, int *slab);
-// the wide-row form of the one-pass normal product (rows too long for two
-// bands of the band form to stay in L2): true with its slab width, and the
-// row blocks, flag words and partial floats it needs
-bool fused_wide_fits(long long m, long long n, int grid, const float *A, int *slab, long long *blocks,
-                     long long *part_floats);
 // Au = A u and g = A^T Au for the fused dense instances (A read once)
 void op_fused_normal(const LaunchCtx &L, const OpBatch &B, int pred, VecSel u, VecSel au, VecSel g);
 // the normal product of every instance: fused dense instances in one pass,

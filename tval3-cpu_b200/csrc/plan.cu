@@ -482,27 +482,15 @@ static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStor
 	ob.fused.clear();
 	ob.fused_grid = fused_grid();
 	ob.fused_words = 0;
-	ob.fused_part_words = 0;
 	for (int i = 0; i < cnt; i++) {
 		OpDev &d = inst[i].op;
 		d.fused_rpc = 0;
-		d.fused_wide = 0;
 		if (d.kind != TVAL3G_OP_DENSE || d.mrhs || d.layers != 1) continue;
-		long long blocks = 0, pf = 0;
-		if (fused_wide_fits(d.m, d.n, ob.fused_grid, d.A, &d.fused_slab, &blocks, &pf)) {
-			// rows too long for the band form: CTAs own column slabs of every row
-			d.fused_rpc = 1;   // marks the instance as fused (its gemv maps are left out)
-			d.fused_wide = 1;
-			ob.fused.push_back({i, (int)(2 * blocks), ob.fused_words, 1});
-			ob.fused_words += 2 * blocks;
-			ob.fused_part_words = std::max(ob.fused_part_words, pf);
-			continue;
-		}
 		d.fused_rpc = fused_rows_per_cta(d.m, d.n, ob.fused_grid, d.A, &d.fused_slab);
 		if (d.fused_rpc <= 0) continue;
 		const long long R = (long long)ob.fused_grid * d.fused_rpc;
 		const int bands = (int)((d.m + R - 1) / R);
-		ob.fused.push_back({i, bands, ob.fused_words, 0});
+		ob.fused.push_back({i, bands, ob.fused_words});
 		ob.fused_words += bands;
 	}
 	// dense gemv maps: all dense instances, then those outside the fused set
@@ -776,7 +764,6 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 		d_tiles_ = tb.upload(stream_);
 		allocs_.push_back(d_tiles_);
 		if (dense_part > 0) ob_.dense_part = (float *)dalloc(sizeof(float) * (size_t)dense_part);
-		if (ob_.fused_part_words > 0) ob_.fused_part = (float *)dalloc(sizeof(float) * (size_t)ob_.fused_part_words);
 		if (ob_.fused_words > 0) {
 			ob_.fused_flags = (int *)dalloc(sizeof(int) * (size_t)ob_.fused_words);
 			TG_CUDA(cudaMemsetAsync(ob_.fused_flags, 0, sizeof(int) * (size_t)ob_.fused_words, stream_));
