@@ -43,6 +43,12 @@ __device__ __forceinline__ void set_conds(const CondSet &cs, const Ctrl &c) {
 #define FOR_TILE_M(i0, len, i)                                \
 	_Pragma("unroll") for (int k_ = 0; k_ < EPT_M; k_++)      \
 		if (const int i = (i0) + (int)threadIdx.x + k_ * BLOCK; i < (len))
+// The loads of all EPT_M elements first, then the stores: the compiler cannot
+// tell that two vectors do not alias, so a load that follows a store in
+// program order would wait for the store's data.
+#define LOAD_TILE_M(i0, len, reg, expr)              \
+	float reg[EPT_M];                                \
+	FOR_TILE_M(i0, len, i) reg[k_] = (expr);
 
 struct Geo {
 	int dims, p, q, r, S, n;
@@ -394,18 +400,27 @@ __global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
 		FOR_TILE(local * TILE, g.n, i) {
 			int x, y, z;
 			g.coords(i, x, y, z);
-			gv[i] = gv[i] - atb[i];
+			// every load before the first store (the vectors do not alias)
+			const float gi = gv[i] - atb[i];
 			// in the inner loop k_shrink_grad forms g2 again from the new W
 			// before anything reads it, so only the initialisation needs it
-			if (a.stage == ST_INIT) g2[i] = g2_at_u(I, g, i, x, y, z);
+			const float g2i = a.stage == ST_INIT ? g2_at_u(I, g, i, x, y, z) : 0.f;
 			float du[3] = {dxf(U, g, i, x), dyf(U, g, i, y), g.dims == 3 ? dzf(U, g, i, z) : 0.f};
+			float wc[3], sc[3];
+#pragma unroll
+			for (int cc = 0; cc < 3; cc++) {
+				wc[cc] = cc < g.dims ? Wc[cc][i] : 0.f;
+				sc[cc] = cc < g.dims ? Sc[cc][i] : 0.f;
+			}
+			gv[i] = gi;
+			if (a.stage == ST_INIT) g2[i] = g2i;
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++)
 				if (cc < g.dims) {
 					Uc[cc][i] = du[cc];
-					float vv = du[cc] - Wc[cc][i];
+					float vv = du[cc] - wc[cc];
 					v[0] += (double)vv * vv;
-					v[1] += (double)Sc[cc][i] * vv;
+					v[1] += (double)sc[cc] * vv;
 				}
 		}
 	} else {
@@ -453,13 +468,12 @@ __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 	const float *__restrict__ g2 = I.vn[vG2], *__restrict__ gv = I.vn[vG];
 	double v[1] = {0};   // |d|^2
 	FOR_TILE(local * TILE, (int)I.n, i) {
-		float t = dts[i];
-		if (a.stage == ST_OUTER) {
-			t = d[i] * bscale;
-			dts[i] = t;
-		}
-		float dv = t + g2[i];
-		dv = fmaf(mdb, gv[i], dv);
+		// every load before the first store
+		float t = a.stage == ST_OUTER ? d[i] * bscale : dts[i];
+		const float g2i = g2[i], gvi = gv[i];
+		if (a.stage == ST_OUTER) dts[i] = t;
+		float dv = t + g2i;
+		dv = fmaf(mdb, gvi, dv);
 		d[i] = dv;
 		v[0] += (double)dv * dv;
 	}
@@ -489,7 +503,7 @@ __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 // values Q and C, 2d:802) and then the inner loop's (RelChg, stopping test,
 // trace, time-to-solution target).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(BLOCK) k_shrink_grad(KArgs a) {
+__global__ void __launch_bounds__(BLOCK, 3) k_shrink_grad(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	Geo g(I);
@@ -520,7 +534,6 @@ __global__ void __launch_bounds__(BLOCK) k_shrink_grad(KArgs a) {
 #pragma unroll
 		for (int cc = 0; cc < 3; cc++)
 			if (cc < dims) {
-				I.vn[vWx + cc][i] = w[cc];
 				const float vv = u[cc] - w[cc];
 				v[1] += (double)vv * vv;
 				v[2] += (double)s[cc] * vv;
@@ -534,24 +547,32 @@ __global__ void __launch_bounds__(BLOCK) k_shrink_grad(KArgs a) {
 				return uj[cc] - wj[cc];
 			};
 		};
+		// every load before the first store (the vectors do not alias: a load
+		// the compiler kept behind a store would wait for the store's data)
 		const float g2i = dt_at(g, i, x, y, z, V(0), V(1), V(2));
+		const float dtsi = dts[i], gvi = gv[i], up = Up[i], Ui = U[i];
+		const float gpi = bb ? gp[i] : 0.f, g2pi = bb ? g2p[i] : 0.f;
+		const float uti = ut ? I.ut_user[cplx_index(I, i, I.n)] : 0.f;
+#pragma unroll
+		for (int cc = 0; cc < 3; cc++)
+			if (cc < dims) I.vn[vWx + cc][i] = w[cc];
 		I.vn[vG2][i] = g2i;
-		float dv = dts[i] + g2i;
-		dv = fmaf(mdb, gv[i], dv);
+		float dv = dtsi + g2i;
+		dv = fmaf(mdb, gvi, dv);
 		d[i] = dv;
 		v[3] += (double)dv * dv;
-		const float up = Up[i], uu = U[i] - up;
+		const float uu = Ui - up;
 		uup[i] = uu;
 		v[4] += (double)up * up;
 		v[5] += (double)uu * uu;
 		if (bb) {
-			const float tmp = fmaf(mdb, gv[i] - gp[i], g2i - g2p[i]);
+			const float tmp = fmaf(mdb, gvi - gpi, g2i - g2pi);
 			v[8] += (double)uu * tmp;
 		}
 		if (ut) {
-			const float t = I.ut_user[cplx_index(I, i, I.n)], e = U[i] * rscl - t;
+			const float e = Ui * rscl - uti;
 			v[6] += (double)e * e;
-			v[7] += (double)t * t;
+			v[7] += (double)uti * uti;
 		}
 	}
 	double tot[9];
@@ -720,20 +741,29 @@ __global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
 		const int ld = I.op.rvx, tH = I.op.tH;   // the geometry's row length (its ld)
 		FOR_TILE(local * TILE, (int)I.n, i) {
 			float u;
+			const float dv = d[i];
 			if (snap) {
+				// every load before the first store: the compiler cannot tell that
+				// the vectors do not alias, and a load after a store would wait
+				// for the store's data
 				u = U[i];
+				const float gi = I.vn[vG][i], g2i = I.vn[vG2][i];
+				float uc[3];
+#pragma unroll
+				for (int cc = 0; cc < 3; cc++) uc[cc] = cc < I.dims ? I.vn[vUx + cc][i] : 0.f;
+				const float dts = I.sched ? I.vn[vDts][i] : 0.f;
 				Up[i] = u;
-				I.vn[vGp][i] = I.vn[vG][i];
-				I.vn[vG2p][i] = I.vn[vG2][i];
+				I.vn[vGp][i] = gi;
+				I.vn[vG2p][i] = g2i;
 #pragma unroll
 				for (int cc = 0; cc < 3; cc++)
-					if (cc < I.dims) I.vn[vUxp + cc][i] = I.vn[vUx + cc][i];
+					if (cc < I.dims) I.vn[vUxp + cc][i] = uc[cc];
 				// schedule mode: DtsAtd = -(Dt sigma + At delta) / beta for this iteration's beta
-				if (I.sched) I.vn[vDts][i] *= sratio;
+				if (I.sched) I.vn[vDts][i] = dts * sratio;
 			} else {
 				u = Up[i];
 			}
-			u = fmaf(ntau, d[i], u);
+			u = fmaf(ntau, dv, u);
 			if (I.nonneg) u = (I.cplx && i >= (int)(I.n >> 1)) ? 0.f : (u < 0.f ? 0.f : u);   // complex: Re >= 0, Im = 0 (2d:467-479)
 			U[i] = u;
 			if (xT) {
@@ -742,7 +772,9 @@ __global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
 			}
 		}
 	} else if (snap) {
-		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) I.vm[vAup][i] = I.vm[vAu][i];
+		const int i0 = (local - I.ntn) * TILE_M;
+		LOAD_TILE_M(i0, (int)I.m, au, I.vm[vAu][i])
+		FOR_TILE_M(i0, (int)I.m, i) I.vm[vAup][i] = au[k_];
 	}
 }
 
@@ -823,24 +855,25 @@ __global__ void __launch_bounds__(BLOCK) k_lerp(KArgs a) {
 	const float al = (float)I.ctrl->alpha;
 	if (local < I.ntn) {
 		FOR_TILE(local * TILE, (int)I.n, i) {
-			float *__restrict__ g = I.vn[vG];
-			float *__restrict__ u = I.vn[vU];
-			g[i] = fmaf(al, g[i] - I.vn[vGp][i], I.vn[vGp][i]);
-			u[i] = fmaf(al, u[i] - I.vn[vUp][i], I.vn[vUp][i]);
+			// every load before the first store
+			const float gi = I.vn[vG][i], gpi = I.vn[vGp][i], ui = I.vn[vU][i], upi = I.vn[vUp][i];
+			float uc[3], ucp[3];
+#pragma unroll
+			for (int cc = 0; cc < 3; cc++) {
+				uc[cc] = cc < I.dims ? I.vn[vUx + cc][i] : 0.f;
+				ucp[cc] = cc < I.dims ? I.vn[vUxp + cc][i] : 0.f;
+			}
+			I.vn[vG][i] = fmaf(al, gi - gpi, gpi);
+			I.vn[vU][i] = fmaf(al, ui - upi, upi);
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++)
-				if (cc < I.dims) {
-					float *__restrict__ ux = I.vn[vUx + cc];
-					const float p = I.vn[vUxp + cc][i];
-					ux[i] = fmaf(al, ux[i] - p, p);
-				}
+				if (cc < I.dims) I.vn[vUx + cc][i] = fmaf(al, uc[cc] - ucp[cc], ucp[cc]);
 		}
 	} else {
-		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) {
-			float *__restrict__ au = I.vm[vAu];
-			const float p = I.vm[vAup][i];
-			au[i] = fmaf(al, au[i] - p, p);
-		}
+		const int i0 = (local - I.ntn) * TILE_M;
+		LOAD_TILE_M(i0, (int)I.m, au, I.vm[vAu][i])
+		LOAD_TILE_M(i0, (int)I.m, aup, I.vm[vAup][i])
+		FOR_TILE_M(i0, (int)I.m, i) I.vm[vAu][i] = fmaf(al, au[k_] - aup[k_], aup[k_]);
 	}
 }
 
@@ -879,21 +912,28 @@ __global__ void __launch_bounds__(BLOCK) k_mlp(KArgs a) {
 	double v[2] = {0, 0};   // lam4, lam5
 	if (local < I.ntn) {
 		FOR_TILE(local * TILE, (int)I.n, i) {
+			float vv[3], sv[3];   // every load before the first store
+#pragma unroll
+			for (int cc = 0; cc < 3; cc++) {
+				vv[cc] = cc < I.dims ? I.vn[vUx + cc][i] - I.vn[vWx + cc][i] : 0.f;
+				sv[cc] = cc < I.dims ? I.vn[vSx + cc][i] : 0.f;
+			}
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++)
 				if (cc < I.dims) {
-					float vv = I.vn[vUx + cc][i] - I.vn[vWx + cc][i];
-					float s = fmaf(nbeta, vv, I.vn[vSx + cc][i]);
+					float s = fmaf(nbeta, vv[cc], sv[cc]);
 					I.vn[vSx + cc][i] = s;
-					v[0] += (double)s * vv;
+					v[0] += (double)s * vv[cc];
 				}
 		}
 	} else {
-		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) {
-			float r = I.vm[vAu][i] - I.vm[vB][i];
-			float dl = fmaf(nmu, r, I.vm[vDelta][i]);
+		const int i0 = (local - I.ntn) * TILE_M;
+		LOAD_TILE_M(i0, (int)I.m, r, I.vm[vAu][i] - I.vm[vB][i])
+		LOAD_TILE_M(i0, (int)I.m, dl0, I.vm[vDelta][i])
+		FOR_TILE_M(i0, (int)I.m, i) {
+			const float dl = fmaf(nmu, r[k_], dl0[k_]);
 			I.vm[vDelta][i] = dl;
-			v[1] += (double)dl * r;
+			v[1] += (double)dl * r[k_];
 		}
 	}
 	double tot[2];
@@ -965,7 +1005,8 @@ __global__ void __launch_bounds__(BLOCK) k_skip_norms(KArgs a) {
 __global__ void __launch_bounds__(BLOCK) k_copy_lastau(KArgs a) {
 	KPROLOGUE(a);
 	if (!I.skip_enabled) return;
-	FOR_TILE_M(local * TILE_M, (int)I.m, i) I.vm[vLastAu][i] = I.vm[vAu][i];
+	LOAD_TILE_M(local * TILE_M, (int)I.m, au, I.vm[vAu][i])
+	FOR_TILE_M(local * TILE_M, (int)I.m, i) I.vm[vLastAu][i] = au[k_];
 }
 
 __global__ void k_cond(const Inst *tab, int count, int pred, int *flag, unsigned long long handle,

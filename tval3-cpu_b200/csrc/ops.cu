@@ -1000,6 +1000,17 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 	const int smem_count = (int)sizeof(unsigned) * nwords, smem_fill = 2 * smem_count;
 	TG_CUDA(cudaFuncSetAttribute(k_tile_count, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_count));
 	TG_CUDA(cudaFuncSetAttribute(k_tile_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_fill));
+	// Each thread walks its own pixel's list of ray ids, so a warp touches 32
+	// cache lines per load and reuses each over the next 31 loads: the lines
+	// must stay in L1.  With no preference the driver would size shared memory
+	// for the most blocks that fit (7 of 32 KB), leaving L1 little room, while
+	// there are only nt blocks (256 for a 256x256 image): ask for shared memory
+	// for two blocks per SM and leave the rest to L1.
+	for (auto kv : {std::make_pair((const void *)k_tile_count, smem_count),
+	                std::make_pair((const void *)k_tile_fill, smem_fill)}) {
+		const int pct = (int)std::min<long long>(100, (2LL * (kv.second + 2048) * 100 + 232447) / 232448);
+		TG_CUDA(cudaFuncSetAttribute(kv.first, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+	}
 	long long *tlen = nullptr, *tptr = nullptr, *wlen = nullptr, *woff = nullptr;
 	tlen = (decltype(tlen))dev_alloc(sizeof(long long) * (nt + 1), s);
 	tptr = (decltype(tptr))dev_alloc(sizeof(long long) * (nt + 1), s);
@@ -1421,6 +1432,7 @@ __global__ void __launch_bounds__(1024) k_scan_totals(long long *tot, int nb, lo
 	const int t = threadIdx.x, per = (nb + 1023) / 1024;
 	const int b0 = min(nb, t * per), b1 = min(nb, b0 + per);
 	long long s = 0;
+#pragma unroll 8
 	for (int b = b0; b < b1; b++) s += tot[b];
 	const int lane = t & 31, wid = t >> 5;
 	long long incl = s;
@@ -1441,10 +1453,18 @@ __global__ void __launch_bounds__(1024) k_scan_totals(long long *tot, int nb, lo
 	}
 	__syncthreads();
 	long long run = sh[wid] + incl - s;
-	for (int b = b0; b < b1; b++) {
-		const long long v = tot[b];
-		tot[b] = run;
-		run += v;
+	// eight loads before their stores: a load after a store to the same array
+	// would wait for the store's data
+	for (int b = b0; b < b1; b += 8) {
+		long long v[8];
+#pragma unroll
+		for (int j = 0; j < 8; j++) v[j] = b + j < b1 ? tot[b + j] : 0;
+#pragma unroll
+		for (int j = 0; j < 8; j++)
+			if (b + j < b1) {
+				tot[b + j] = run;
+				run += v[j];
+			}
 	}
 	if (t == 1023) out[n] = sh[wid] + incl;
 }
