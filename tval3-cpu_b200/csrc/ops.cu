@@ -880,11 +880,17 @@ __device__ __forceinline__ int tile_pixel(int t, int px, int ntx, int ld, int H)
 __device__ void tile_bitmap(unsigned *bm, int nwords, int p, const int *cptr, const int *cind) {
 	for (int w = threadIdx.x; w < nwords; w += blockDim.x) bm[w] = 0u;
 	__syncthreads();
-	if (p >= 0)
-		for (int k = cptr[p]; k < cptr[p + 1]; k++) {
-			const int r = cind[k];
-			atomicOr(&bm[r >> 5], 1u << (r & 31));
+	if (p >= 0) {
+		const int k1 = cptr[p + 1];
+		for (int k = cptr[p]; k < k1; k += 8) {   // eight loads in flight, then their updates
+			int r[8];
+#pragma unroll
+			for (int j = 0; j < 8; j++) r[j] = k + j < k1 ? cind[k + j] : -1;
+#pragma unroll
+			for (int j = 0; j < 8; j++)
+				if (r[j] >= 0) atomicOr(&bm[r[j] >> 5], 1u << (r[j] & 31));
 		}
+	}
 	__syncthreads();
 }
 
@@ -929,10 +935,14 @@ __global__ void __launch_bounds__(RAYT_THREADS) k_tile_count(int ld, int H, int 
 
 // the tile's list (measurement indices in traced order) and its pixels'
 // 1-based positions in it, padded with 0 to the warp's word count
-__global__ void __launch_bounds__(RAYT_THREADS) k_tile_fill(int ld, int H, int ntx, int nrays, const int *cptr,
-                                                            const int *cind, const int *live_out,
-                                                            const long long *tptr, const long long *woff,
-                                                            const unsigned char *perm, int *tmeas, uint4 *sidx) {
+__global__ void __launch_bounds__(RAYT_THREADS) k_tile_fill(int ld, int H, int ntx, int nrays,
+                                                            const int *__restrict__ cptr,
+                                                            const int *__restrict__ cind,
+                                                            const int *__restrict__ live_out,
+                                                            const long long *__restrict__ tptr,
+                                                            const long long *__restrict__ woff,
+                                                            const unsigned char *__restrict__ perm,
+                                                            int *__restrict__ tmeas, uint4 *__restrict__ sidx) {
 	extern __shared__ unsigned bm[];   // nwords bits, then nwords exclusive prefix counts
 	__shared__ int ws[RAYT_WARPS];
 	const int t = blockIdx.x, nwords = (nrays + 31) >> 5;
@@ -975,17 +985,15 @@ __global__ void __launch_bounds__(RAYT_THREADS) k_tile_fill(int ld, int H, int n
 	const int nv = (int)((woff[wl + 1] - v0) >> 5);
 	int k = p >= 0 ? cptr[p] : 0;
 	const int k1 = p >= 0 ? cptr[p + 1] : 0;
-	for (int v = 0; v < nv; v++) {
+	for (int v = 0; v < nv; v++, k += 8) {
+		int r[8];   // the word's eight loads first, then their positions
+#pragma unroll
+		for (int j = 0; j < 8; j++) r[j] = k + j < k1 ? cind[k + j] : -1;
 		unsigned e[8];
 #pragma unroll
-		for (int j = 0; j < 8; j++) {
-			unsigned pos = 0;
-			if (k < k1) {
-				const int r = cind[k++];
-				pos = 1u + (unsigned)pre[r >> 5] + __popc(bm[r >> 5] & ((1u << (r & 31)) - 1u));
-			}
-			e[j] = pos;
-		}
+		for (int j = 0; j < 8; j++)
+			e[j] = r[j] < 0 ? 0u
+			                : 1u + (unsigned)pre[r[j] >> 5] + __popc(bm[r[j] >> 5] & ((1u << (r[j] & 31)) - 1u));
 		sidx[v0 + 32LL * v + lane] = make_uint4(e[0] | (e[1] << 16), e[2] | (e[3] << 16), e[4] | (e[5] << 16),
 		                                        e[6] | (e[7] << 16));
 	}
@@ -1165,8 +1173,11 @@ __global__ void __launch_bounds__(RAYT_THREADS) k_brick_count(int rvx, int rvy, 
 // per brick, thread = rank: its voxel's positions packed eight to a 16-byte
 // word, the words of a warp's 32 voxels interleaved, padded with 0
 __global__ void __launch_bounds__(RAYT_THREADS) k_brick_fill(int rvx, int rvy, int rvz, int nbx, int nby,
-                                                             const int *cptr, const float *cval, const long long *woff,
-                                                             const unsigned char *perm, uint4 *sidx) {
+                                                             const int *__restrict__ cptr,
+                                                             const float *__restrict__ cval,
+                                                             const long long *__restrict__ woff,
+                                                             const unsigned char *__restrict__ perm,
+                                                             uint4 *__restrict__ sidx) {
 	const int t = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 	const int p = brick_voxel(t, perm[(long long)t * RAYT_THREADS + threadIdx.x], rvx, rvy, rvz, nbx, nby);
 	const long long wl = (long long)t * RAYT_WARPS + wid;
@@ -1174,10 +1185,10 @@ __global__ void __launch_bounds__(RAYT_THREADS) k_brick_fill(int rvx, int rvy, i
 	const int nv = (int)((woff[wl + 1] - v0) >> 5);
 	int k = p >= 0 ? cptr[p] : 0;
 	const int k1 = p >= 0 ? cptr[p + 1] : 0;
-	for (int v = 0; v < nv; v++) {
+	for (int v = 0; v < nv; v++, k += 8) {
 		unsigned e[8];
 #pragma unroll
-		for (int j = 0; j < 8; j++) e[j] = k < k1 ? (unsigned)cval[k++] : 0u;
+		for (int j = 0; j < 8; j++) e[j] = k + j < k1 ? (unsigned)cval[k + j] : 0u;
 		sidx[v0 + 32LL * v + lane] = make_uint4(e[0] | (e[1] << 16), e[2] | (e[3] << 16), e[4] | (e[5] << 16),
 		                                        e[6] | (e[7] << 16));
 	}
@@ -1656,8 +1667,7 @@ __global__ void k_ray_trace(int nrays, const int4 *rays, int rvx, int rvy, const
 	}
 }
 
-void trace_rays(cudaStream_t s, int nrays, const int4 *rays, int rvx, int rvy, int *rptr, int *rind,
-                long long *total_out) {
+int *trace_rays(cudaStream_t s, int nrays, const int4 *rays, int rvx, int rvy, int *rptr, long long *total_out) {
 	long long *len = nullptr, *off = nullptr;
 	len = (decltype(len))dev_alloc(sizeof(long long) * (nrays + 1), s);
 	off = (decltype(off))dev_alloc(sizeof(long long) * (nrays + 1), s);
@@ -1673,10 +1683,12 @@ void trace_rays(cudaStream_t s, int nrays, const int4 *rays, int rvx, int rvy, i
 		throw Error{TVAL3G_ERR_ARGUMENT, "Argument error: the ray operator has more than 2^31-1 hits"};
 	}
 	k_to_int<<<(unsigned)((nrays + 1 + 255) / 256), 256, 0, s>>>(off, rptr, nrays + 1);
-	if (rind && nrays > 0) k_ray_trace<<<(unsigned)(((long long)nrays * 32 + 255) / 256), 256, 0, s>>>(nrays, rays, rvx, rvy, rptr, rind);
+	int *rind = (int *)dev_alloc(sizeof(int) * (size_t)std::max(total, 1LL), s);
+	if (nrays > 0) k_ray_trace<<<(unsigned)(((long long)nrays * 32 + 255) / 256), 256, 0, s>>>(nrays, rays, rvx, rvy, rptr, rind);
 	TG_CUDA(cudaGetLastError());
 	dev_free(len, s);
 	dev_free(off, s);
+	return rind;
 }
 
 }  // namespace tval3g

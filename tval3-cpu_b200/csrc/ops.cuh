@@ -115,9 +115,10 @@ void scan_counts(cudaStream_t s, const long long *cnt, long long *out, long long
 // CSR (rows x cols, rptr int32) -> CSC sorted by row within a column; cval may be NULL
 void build_transpose(cudaStream_t s, long long rows, long long cols, long long nnz, const int *rptr,
                      const int *rind, const float *rval, int *cptr, int *cind, float *cval);
-// rasterise nrays packed rays into CSR over rays (offsets int32, indices int32)
-void trace_rays(cudaStream_t s, int nrays, const int4 *rays, int rvx, int rvy, int *rptr, int *rind,
-                long long *total_out);
+// rasterise nrays packed rays into CSR over rays (offsets int32 into rptr,
+// nrays + 1 of them; the indices, int32, in a new stream-ordered allocation
+// that the caller owns: dev_free)
+int *trace_rays(cudaStream_t s, int nrays, const int4 *rays, int rvx, int rvy, int *rptr, long long *total_out);
 // apply one instance's operator outside a plan (C ABI)
 void apply_single(cudaStream_t s, const Inst *dtab, const OpDev &op, int trans, long long rows,
                   long long cols, const OpBatch &B);

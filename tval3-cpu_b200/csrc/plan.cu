@@ -357,9 +357,9 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		// index of the adjoint, entries = measurement indices sorted by ray
 		int *rptr = dalloc_op<int>(s, st, (long long)d.nrays + 1);
 		long long total = 0;
-		trace_rays(s, d.nrays, drays, d.rvx, d.rvy, rptr, nullptr, &total);
-		int *rind = dalloc_op<int>(s, st, total);
-		trace_rays(s, d.nrays, drays, d.rvx, d.rvy, rptr, rind, &total);
+		int *rind = trace_rays(s, d.nrays, drays, d.rvx, d.rvy, rptr, &total);
+		st.owned.push_back(rind);
+		st.bytes += (long long)sizeof(int) * std::max(total, 1LL);
 		st.nnz = total;
 		d.adj_atomic = (flags & TVAL3G_RAY_ADJ_ATOMICS) != 0;
 		const bool tile_ok = !d.adj_atomic && !(flags & TVAL3G_RAY_ADJ_PLAIN);
@@ -383,7 +383,6 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 				st.bytes += ib;
 				st.adj_index_bytes = ib;
 			}
-			TG_CUDA(cudaStreamSynchronize(s));
 			dev_free(posf, s);
 			dev_free(cposf, s);
 		}
@@ -420,8 +419,7 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		d.cval = nullptr;
 		st.ray_rptr = rptr; st.ray_rind = rind;
 		st.b_len = mtot;
-		if (!keep_ray_csr) {
-			TG_CUDA(cudaStreamSynchronize(s));
+		if (!keep_ray_csr) {   // (stream-ordered frees: the kernels queued before them still read them)
 			for (void *&q : st.owned)
 				if (q == rptr || q == rind) { dev_free(q, s); q = nullptr; }
 			st.ray_rptr = st.ray_rind = nullptr;
@@ -775,6 +773,12 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 		d_flag_ = (int *)dalloc(sizeof(int));
 		d_launches_ = (unsigned long long *)dalloc(sizeof(unsigned long long));
 		for (auto &o : ops_) device_bytes_ += o.bytes;
+		// the graph is captured and instantiated while the operator
+		// preparation still runs on the device, and uploaded behind it
+		if (graph_mode_) {
+			build_graph();
+			TG_CUDA(cudaGraphUpload(exec_, stream_));
+		}
 		TG_CUDA(cudaStreamSynchronize(stream_));
 	} catch (...) {
 		release();
