@@ -360,6 +360,27 @@ def kernel_roofline(cx, capi, spec, w, kind):
             "timing": "one launch per CUDA-event pair, 256 MB L2 flush before each"}
 
 
+def stencil_roofline(plan, spec, w, ut):
+    """The iteration's image-sized vector kernels, each timed alone (20
+    launches back to back after the solve; at 128^3 each touches more than
+    the L2): algorithmic bytes = the vectors each reads and writes once."""
+    ms = plan.time_stencils(20)
+    n, m = spec.n, int(np.asarray(w["b"]).size)
+    dims = len(w["shape"])
+    xT = w["kind"] == "ray2d"   # the descent also writes the transposed image for the 2D ray forward
+    byts = {"getg": 4 * n * ((3 + 2 * dims) + (1 + dims)) + 12 * m,      # g, Atb, U, W, S -> g, D U; Au, b, delta
+            "descend": 4 * n * (2 * (4 + dims) + (1 if xT else 0)) + 8 * m,  # U, g, g2, D U, d -> snapshots, U; Au -> Aup
+            "shrink_grad": 4 * n * (3 * dims + 9 + (1 if ut else 0))}    # D U, S, Dts, g, Up, U, gp, g2p -> W, g2, d, uup
+    peak, src = peak_hbm()
+    out = {}
+    for k, t in ms.items():
+        gbs = byts[k] / (t * 1e-3) / 1e9
+        out[k] = {"ms_per_launch": t, "algorithmic_bytes": int(byts[k]), "achieved_gbs": gbs, "frac": gbs / peak}
+    out["peak_source"] = src
+    out["timing"] = "20 launches back to back after the solve, CUDA events on the plan's stream"
+    return out
+
+
 def launch_shape(capi, spec):
     """The autotuner's choice for spec's operator (from its cache, filled by
     the plan): lanes per ray of the ray forward, forward / adjoint gather
@@ -432,6 +453,7 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
 
     plan.set_target(0.0)   # the full solve under the reference's stopping rules alone
     full_t, full_info = cx.event_time(lambda: solve(plan), 2)
+    stencils = stencil_roofline(plan, spec, w, ut=uts is not None)
     plan.close()
 
     plan_plain = capi.Plan([spec], [opts], graph=False, tune=a.tune)   # host-driven loop, same kernels
@@ -477,7 +499,7 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
             "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "reconstructions/s", "h2d_bytes_per_step": in_bytes,
                     "d2h_bytes_per_step": int(spec.n * 4), "ms_each": [round(x, 3) for x in et],
                     "ms_inside_library": [round(x, 3) for x in ec]},
-            "roofline": kernel_roofline(cx, capi, spec, w, w["kind"]),
+            "roofline": dict(kernel_roofline(cx, capi, spec, w, w["kind"]), stencils=stencils),
             "clocks": clk, "gpu_launches": launches}
     line.update(extra)
     if rank == 0 and world == 1 and name != "hemi3d":

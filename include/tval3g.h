@@ -180,6 +180,15 @@ int tval3g_plan_solve(tval3g_plan *plan, const float *const *d_b, const float *c
 /* Kernel launches issued by the last tval3g_plan_solve (graph mode: kernel
  * nodes executed, counted on the device), and the plan's device bytes. */
 int tval3g_plan_stats(const tval3g_plan *plan, long long *kernel_launches, long long *device_bytes);
+/* Measurement: the mean device time in ms of one launch of each of the
+ * iteration's image-sized vector kernels over all instances - ms[0] the
+ * gradient epilogue (g -= Atb, D U, the objective's sums), ms[1] the descent
+ * (U = U - tau d with the snapshot of the previous iterate), ms[2] the
+ * shrinkage with Dt(DU - W), d and the step-length sums - each launched reps
+ * times back to back on the plan's stream after a solve.  It overwrites the
+ * plan's state (the next solve starts afresh).  No counterpart in the
+ * reference. */
+int tval3g_plan_time_stencils(tval3g_plan *plan, int reps, double *ms);
 /* Time-to-solution mode: with target > 0, every instance solved with a Ut
  * also stops after the first inner iteration at which
  * ||U/scl - Ut|| <= target * ||Ut|| (checked on the device each iteration);

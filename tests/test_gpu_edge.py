@@ -120,3 +120,54 @@ def test_bounded_wait_timeout_reports_and_recovers(torch_cuda, monkeypatch):
     U1, info1 = capi.solve(spec, c["b"], c["opts"])
     assert info1["status"] == 0 and info1["total_iters"] == info0["total_iters"] == 20
     np.testing.assert_array_equal(U1, U0)
+
+
+def _ray_error(spec):
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.Operator(spec)
+    assert e.value.code == capi.ERR_ARGUMENT
+    return str(e.value)
+
+
+def test_ray_geometry_argument_errors(torch_cuda):
+    """The rays are packed on the device; an endpoint outside the image or
+    volume and a 3D use_path index beyond numPaths are still reported with
+    the reference's messages (2d/tval3_cpu_2d.cpp:696-750,
+    3d/tval3_cpu_3d.cpp:1028-1165), the first offending ray in the
+    reference's loop order (plane, emitter, receiver) deciding which."""
+    g2 = dict(use_path=np.ones(6, np.int32), xe=[0, 1], ye=[0, 2], xr=[3, 4, 9], yr=[1, 1, 1], ld=5, scale=1.0)
+    assert "lies outside the image" in _ray_error(capi.ray2d_problem((4, 5), g2))
+    g3 = W.hemisphere_geometry(8, 8, 4, 3.0, np.random.default_rng(1))
+    bad = dict(g3, use_path=np.array(g3["use_path"]))
+    k = int(np.nonzero(bad["use_path"])[0][-1])      # the last used path: beyond numPaths
+    bad["use_path"][k] = g3["numPaths"] + 1
+    assert "use_path index exceeds numPaths" in _ray_error(capi.ray3d_problem((8, 8, 8), bad))
+    both = dict(bad, xe=np.array(g3["xe"]))          # and an endpoint error on a later emitter
+    e_last = len(both["xe"]) - 1
+    both["xe"][e_last] = 99
+    first_bad_emitter = k // g3["R"]
+    msg = _ray_error(capi.ray3d_problem((8, 8, 8), both))
+    if first_bad_emitter < e_last:
+        assert "use_path index exceeds numPaths" in msg
+    else:
+        assert "lies outside the volume" in msg
+    ok = capi.Operator(capi.ray3d_problem((8, 8, 8), g3))   # the unaltered geometry still builds
+    ok.close()
+
+
+def test_time_stencils_after_a_solve(torch_cuda):
+    """tval3g_plan_time_stencils times the three vector kernels after a solve;
+    the next solve starts afresh and gives the same result as the first."""
+    torch = torch_cuda
+    w = W.ring2d(seed=1, side=64, T=64, tv_norm=1, maxit=20, tol=1e-5, normalize=True)
+    spec = capi.problem_from_workload(w)
+    plan = capi.Plan([spec], [w["opts"]])
+    db = [torch.tensor(np.asarray(w["b"], np.float32), device="cuda")]
+    u1, u2 = [torch.empty(spec.n, device="cuda")], [torch.empty(spec.n, device="cuda")]
+    i1 = plan.solve(db, u1)[0]
+    ms = plan.time_stencils(5)
+    i2 = plan.solve(db, u2)[0]
+    plan.close()
+    print("stencil ms per launch:", ms)
+    assert all(v > 0 for v in ms.values())
+    assert i1["total_iters"] == i2["total_iters"] and torch.equal(u1[0], u2[0])

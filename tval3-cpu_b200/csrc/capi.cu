@@ -194,6 +194,13 @@ int tval3g_plan_stats(const tval3g_plan *plan, long long *kernel_launches, long 
 	CAPI_END
 }
 
+int tval3g_plan_time_stencils(tval3g_plan *plan, int reps, double *ms) {
+	CAPI_BEGIN
+	TG_ARG(plan && plan->p && ms && reps >= 1, "Argument error: NULL plan or output, or reps < 1");
+	plan->p->time_stencils(reps, ms);
+	CAPI_END
+}
+
 int tval3g_plan_set_target(tval3g_plan *plan, double target) {
 	CAPI_BEGIN
 	TG_ARG(plan && plan->p && target >= 0, "Argument error: NULL plan or negative target");

@@ -214,6 +214,7 @@ struct Inst {
 	double *trace;               // maxit records of 5 doubles, or NULL
 	double *part;                // this instance's partial sums
 	int ntn, ntm;                // tiles over n and m
+	int ept;                     // image elements per thread of an n tile (a tile is BLOCK x ept elements)
 	// options (2d/tval3_cpu_2d.cpp:769-772)
 	double muf, betaf, mu0, beta0, tol, tol_inn, c, gamma, gam0, rate_gam, rate_cnt;
 	double skipRatio, maxRelChange;
@@ -238,13 +239,24 @@ __device__ __forceinline__ long long cplx_index(const Inst &I, long long i, long
 	return i < h ? 2 * i : 2 * (i - h) + 1;
 }
 
-// Tiles: image vectors one element per thread (a 256^2 image is 256 blocks),
-// measurement vectors four (their kernels do little per element, and fewer
-// tiles contend less for the instance's reduction ticket)
-constexpr int TILE = 256;
+// Tiles: image vectors BLOCK x Inst::ept elements - one element per thread
+// for images of up to about 0.6M elements (a 256^2 image is 256 blocks), up
+// to eight for large ones, so that a block's fixed costs (descriptor loads,
+// its tile sums, the ticket) are spread over more elements while the grid
+// still fills the GPU twice (ept_for); measurement vectors four elements per
+// thread (their kernels do little per element, and fewer tiles contend less
+// for the instance's reduction ticket)
+constexpr int TILE = 256;   // n tile of ept 1
 constexpr int TILE_M = 1024;
 constexpr int BLOCK = 256;
-constexpr int EPT = TILE / BLOCK;
+// elements per thread of the n tiles of an image of n elements: the largest
+// power of two up to 8 that leaves at least two waves of 4 blocks per SM on
+// 148 SMs
+inline int ept_for(long long n) {
+	int e = 1;
+	while (e < 8 && n >= 2LL * (2 * 148 * 4) * BLOCK * e) e *= 2;
+	return e;
+}
 constexpr int EPT_M = TILE_M / BLOCK;
 constexpr int NSUM = 10;         // partial sums per tile
 constexpr int TRACE_DOUBLES = (int)(sizeof(tval3g_trace_record) / sizeof(double));
@@ -342,10 +354,26 @@ __device__ __forceinline__ bool tile_reduce(const Inst &I, int local, int ntiles
 	double acc[NS];
 #pragma unroll
 	for (int s = 0; s < NS; s++) acc[s] = 0.0;
-	// fixed assignment of tiles to threads, then a fixed-shape block tree
-	for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
+	// fixed assignment of tiles to threads (thread t adds tiles t, t + B,
+	// t + 2B, ... in that order), then a fixed-shape block tree.  This block
+	// runs alone at the end of the launch, so the loads of U tiles are issued
+	// before their adds (U x NS of them in flight): a 128^3 image has 10240
+	// tiles, 40 per thread.
+	constexpr int U = NS <= 2 ? 8 : (16 / NS > 1 ? 16 / NS : 1);
+	const int B = blockDim.x;
+	for (int t0 = threadIdx.x; t0 < ntiles; t0 += U * B) {
+		double x[U][NS];
 #pragma unroll
-		for (int s = 0; s < NS; s++) acc[s] += __ldcg(&I.part[(long long)t * NSUM + s]);
+		for (int u = 0; u < U; u++)
+#pragma unroll
+			for (int s = 0; s < NS; s++)
+				x[u][s] = t0 + u * B < ntiles ? __ldcg(&I.part[(long long)(t0 + u * B) * NSUM + s]) : 0.0;
+#pragma unroll
+		for (int u = 0; u < U; u++)
+			if (t0 + u * B < ntiles)
+#pragma unroll
+				for (int s = 0; s < NS; s++) acc[s] += x[u][s];
+	}
 	block_sums<NS>(acc, sh);
 	if (threadIdx.x == 0) {
 #pragma unroll

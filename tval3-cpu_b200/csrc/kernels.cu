@@ -35,10 +35,17 @@ __device__ __forceinline__ void set_conds(const CondSet &cs, const Ctrl &c) {
 		return;                                                                             \
 	}
 
-// element k of this thread in a tile of image elements starting at i0
-#define FOR_TILE(i0, len, i)                                  \
-	_Pragma("unroll") for (int k_ = 0; k_ < EPT; k_++)        \
-		if (const int i = (i0) + (int)threadIdx.x + k_ * BLOCK; i < (len))
+// element k of this thread in the instance's n tile `local` (BLOCK x I.ept
+// elements; each element's loads precede its stores, so the elements run one
+// after the other).  Every kernel comes in two forms: MULTI = false for
+// launches whose instances all have ept 1 (one element per thread, the small
+// images, compiled as straight-line code), MULTI = true for the others (the
+// element loop, with launch bounds that give the large images' grids more
+// resident warps).
+#define FOR_TILE(local, len, i)                                                      \
+	_Pragma("unroll 1") for (int k_ = 0; k_ < (MULTI ? I.ept : 1); k_++)             \
+		if (const int i = (int)(local) * (BLOCK * (MULTI ? I.ept : 1)) + (int)threadIdx.x + k_ * BLOCK; \
+		    i < (len))
 // the same over a tile of measurement elements (TILE_M = BLOCK x EPT_M)
 #define FOR_TILE_M(i0, len, i)                                \
 	_Pragma("unroll") for (int k_ = 0; k_ < EPT_M; k_++)      \
@@ -128,6 +135,14 @@ struct Shrink {
 		}
 		return lam;
 	}
+	// one component of the anisotropic shrinkage (apply's per-component
+	// arithmetic): W_c depends on U_c and sigma_c alone
+	__device__ __forceinline__ float apply1(float u, float s) const {
+		const float ub = u - s * rbeta;
+		float t = fabsf(ub) - thr;
+		t = t >= 0.f ? t : 0.f;
+		return ub >= 0.f ? t : -t;
+	}
 	// complex data: (u, s) of this plane and (up, sp) of the other plane at
 	// the same pixel; anisotropic: each component's Ubar = (re, im) shrinks
 	// by its modulus, W = max(|Ubar| - 1/beta, 0) Ubar / |Ubar| (2d:614-649);
@@ -209,6 +224,7 @@ __device__ __forceinline__ void better_max(float &a, int &ia, float b, int ib) {
 	if (b > a || (b == a && ib < ia)) { a = b; ia = ib; }
 }
 
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_scaleb(KArgs a) {
 	KPROLOGUE(a);
 	// complex data: over the m / 2 complex entries, |b| their modulus
@@ -272,11 +288,12 @@ __global__ void __launch_bounds__(BLOCK) k_scaleb(KArgs a) {
 // ---------------------------------------------------------------------------
 // initial state (2d:767-779): zero the vectors, bs = b*scl, scalar defaults
 // ---------------------------------------------------------------------------
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_init(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	if (local < I.ntn) {
-		FOR_TILE(local * TILE, (int)I.n, i) {
+		FOR_TILE(local, (int)I.n, i) {
 #pragma unroll
 			for (int v = 0; v < NVN; v++) I.vn[v][i] = 0.f;
 		}
@@ -307,9 +324,10 @@ __global__ void __launch_bounds__(BLOCK) k_init(KArgs a) {
 }
 
 // U = Atb, rcdU = U (2d:775,779)
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_init_u(KArgs a) {
 	KPROLOGUE(a);
-	FOR_TILE(local * TILE, (int)I.n, i) {
+	FOR_TILE(local, (int)I.n, i) {
 		float u = I.vn[vAtb][i];
 		I.vn[vU][i] = u;
 		I.vn[vRcd][i] = u;
@@ -317,12 +335,13 @@ __global__ void __launch_bounds__(BLOCK) k_init_u(KArgs a) {
 }
 
 // (Ux, Uy[, Uz]) = D U
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_D(KArgs a) {
 	KPROLOGUE(a);
 	Geo g(I);
 	const float *__restrict__ U = I.vn[vU];
 	float *__restrict__ ux = I.vn[vUx], *__restrict__ uy = I.vn[vUy], *__restrict__ uz = I.vn[vUz];
-	FOR_TILE(local * TILE, g.n, i) {
+	FOR_TILE(local, g.n, i) {
 		int x, y, z;
 		g.coords(i, x, y, z);
 		ux[i] = dxf(U, g, i, x);
@@ -336,6 +355,7 @@ __global__ void __launch_bounds__(BLOCK) k_D(KArgs a) {
 // lambda4 (g2 follows in k_getg).  In the inner loop update_W runs inside
 // k_shrink_grad.
 // ---------------------------------------------------------------------------
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_shrink(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
@@ -344,7 +364,7 @@ __global__ void __launch_bounds__(BLOCK) k_shrink(KArgs a) {
 	const float *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
 	const float *const Sc[3] = {I.vn[vSx], I.vn[vSy], I.vn[vSz]};
 	double v[3] = {0, 0, 0};   // lam1, lam2, lam4
-	FOR_TILE(local * TILE, n, i) {
+	FOR_TILE(local, n, i) {
 		float u[3], s[3], w[3];
 		v[0] += shrink_at(I, sh, i, Uc, Sc, u, s, w);
 #pragma unroll
@@ -384,7 +404,8 @@ __device__ __forceinline__ float g2_at_u(const Inst &I, const Geo &g, int i, int
 // (2d:543-548).  The gradient components (Ux, Uy[, Uz]) = D U of the new U
 // (the end of descend, 2d:481-493) are formed here and stored.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
+template <bool MULTI>
+__global__ void __launch_bounds__(BLOCK, MULTI ? 6 : 1) k_getg(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	double v[4] = {0, 0, 0, 0};   // lam2, lam4, lam3, lam5
@@ -397,7 +418,7 @@ __global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
 		float *__restrict__ gv = I.vn[vG];
 		float *__restrict__ g2 = I.vn[vG2];
 		const float *__restrict__ atb = I.vn[vAtb];
-		FOR_TILE(local * TILE, g.n, i) {
+		FOR_TILE(local, g.n, i) {
 			int x, y, z;
 			g.coords(i, x, y, z);
 			// every load before the first store (the vectors do not alias)
@@ -459,6 +480,7 @@ __global__ void __launch_bounds__(BLOCK) k_getg(KArgs a) {
 //   ST_INIT:  d = DtsAtd + g2 + muDbeta*g (DtsAtd = 0); Q = 1, C = f
 //   ST_OUTER: DtsAtd = (beta0/beta) d; d = ... (2d:844-852)
 // ---------------------------------------------------------------------------
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
@@ -467,7 +489,7 @@ __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 	float *__restrict__ dts = I.vn[vDts], *__restrict__ d = I.vn[vD];
 	const float *__restrict__ g2 = I.vn[vG2], *__restrict__ gv = I.vn[vG];
 	double v[1] = {0};   // |d|^2
-	FOR_TILE(local * TILE, (int)I.n, i) {
+	FOR_TILE(local, (int)I.n, i) {
 		// every load before the first store
 		float t = a.stage == ST_OUTER ? d[i] * bscale : dts[i];
 		const float g2i = g2[i], gvi = gv[i];
@@ -503,7 +525,8 @@ __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 // values Q and C, 2d:802) and then the inner loop's (RelChg, stopping test,
 // trace, time-to-solution target).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(BLOCK, 3) k_shrink_grad(KArgs a) {
+template <bool MULTI>
+__global__ void __launch_bounds__(BLOCK, MULTI ? 4 : 3) k_shrink_grad(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	Geo g(I);
@@ -526,7 +549,7 @@ __global__ void __launch_bounds__(BLOCK, 3) k_shrink_grad(KArgs a) {
 	const float *__restrict__ gp = I.vn[vGp], *__restrict__ g2p = I.vn[vG2p];
 	// lam1, lam2, lam4, |d|^2, |Up|^2, |uup|^2, |U/scl - Ut|^2, |Ut|^2, <uup, dg2 + muDbeta dg>
 	double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-	FOR_TILE(local * TILE, g.n, i) {
+	FOR_TILE(local, g.n, i) {
 		int x, y, z;
 		g.coords(i, x, y, z);
 		float u[3], s[3], w[3];
@@ -539,9 +562,15 @@ __global__ void __launch_bounds__(BLOCK, 3) k_shrink_grad(KArgs a) {
 				v[2] += (double)s[cc] * vv;
 			}
 		// component cc of DU - W at j (the neighbours' W recomputed)
+		// (anisotropic real data: only component cc of U and sigma at j)
+		const bool one = !sh.iso && !I.cplx;
 		auto V = [&](int cc) {
 			return [&, cc](int j) -> float {
 				if (j == i) return u[cc] - w[cc];
+				if (one) {
+					const float uj = Uc[cc][j];
+					return uj - sh.apply1(uj, Sc[cc][j]);
+				}
 				float uj[3], sj[3], wj[3];
 				shrink_at(I, sh, j, Uc, Sc, uj, sj, wj);
 				return uj[cc] - wj[cc];
@@ -623,6 +652,7 @@ __global__ void __launch_bounds__(BLOCK, 3) k_shrink_grad(KArgs a) {
 // k_shrink_grad (which writes the imaginary plane's g2 too); real instances
 // take the step from k_shrink_grad.
 // ---------------------------------------------------------------------------
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_tau_bb_cplx(KArgs a) {
 	KPROLOGUE(a);
 	if (!I.cplx) return;
@@ -632,7 +662,7 @@ __global__ void __launch_bounds__(BLOCK) k_tau_bb_cplx(KArgs a) {
 	const float *__restrict__ gv = I.vn[vG], *__restrict__ gp = I.vn[vGp];
 	const float *__restrict__ g2 = I.vn[vG2], *__restrict__ g2p = I.vn[vG2p], *__restrict__ uup = I.vn[vUUP];
 	double v[3] = {0, 0, 0};   // ss, Re sy, Im sy
-	FOR_TILE(local * TILE, h, i) {
+	FOR_TILE(local, h, i) {
 		const float ur = uup[i], ui = uup[i + h];
 		const float tr = fmaf(mdb, gv[i] - gp[i], g2[i] - g2p[i]);
 		const float ti = fmaf(mdb, gv[i + h] - gp[i + h], g2[i + h] - g2p[i + h]);
@@ -653,6 +683,7 @@ __global__ void __launch_bounds__(BLOCK) k_tau_bb_cplx(KArgs a) {
 // get_tau (2d:425-453), first part.  First iteration (or restart): dDd =
 // |D d|^2 and request A d.  Otherwise Barzilai-Borwein from uup, dg, dg2.
 // ---------------------------------------------------------------------------
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_tau_prep(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
@@ -662,7 +693,7 @@ __global__ void __launch_bounds__(BLOCK) k_tau_prep(KArgs a) {
 	double v[3] = {0, 0, 0};
 	const float *__restrict__ d = I.vn[vD];
 	if (first) {
-		FOR_TILE(local * TILE, g.n, i) {
+		FOR_TILE(local, g.n, i) {
 			int x, y, z;
 			g.coords(i, x, y, z);
 			float t = dxf(d, g, i, x);
@@ -674,7 +705,7 @@ __global__ void __launch_bounds__(BLOCK) k_tau_prep(KArgs a) {
 	} else {
 		const float *__restrict__ gv = I.vn[vG], *__restrict__ gp = I.vn[vGp];
 		const float *__restrict__ g2 = I.vn[vG2], *__restrict__ g2p = I.vn[vG2p], *__restrict__ uup = I.vn[vUUP];
-		FOR_TILE(local * TILE, g.n, i) {
+		FOR_TILE(local, g.n, i) {
 			float dg = gv[i] - gp[i];
 			float dg2 = g2[i] - g2p[i];
 			float uu = uup[i];
@@ -702,6 +733,7 @@ __global__ void __launch_bounds__(BLOCK) k_tau_prep(KArgs a) {
 }
 
 // first-iteration step: tau = |dd / (dDd + muDbeta * |A d|^2)| (2d:430-442)
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_tau_first(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
@@ -728,7 +760,8 @@ __global__ void __launch_bounds__(BLOCK) k_tau_first(KArgs a) {
 //   ST_RESTART: U = Up - tau d (2d:565-566)
 // then nonneg (2d:455-465)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
+template <bool MULTI>
+__global__ void __launch_bounds__(BLOCK, MULTI ? 6 : 1) k_descend(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	const float ntau = (float)(-1 * c.tau);
@@ -739,7 +772,7 @@ __global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
 		const float *__restrict__ d = I.vn[vD];
 		float *__restrict__ xT = I.op.xT;   // 2D ray operators: the new U transposed for the forward
 		const int ld = I.op.rvx, tH = I.op.tH;   // the geometry's row length (its ld)
-		FOR_TILE(local * TILE, (int)I.n, i) {
+		FOR_TILE(local, (int)I.n, i) {
 			float u;
 			const float dv = d[i];
 			if (snap) {
@@ -790,13 +823,14 @@ __global__ void __launch_bounds__(BLOCK) k_descend(KArgs a) {
 // vectors to the accepted alpha once, with the reference's float arithmetic
 // (fmaf(alpha, U - Up, Up)).  When all five steps fail the vectors are not
 // moved: the restart (2d:561-567) recomputes every one of them from Up.
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_bt_search(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	// |E0|^2, <E0, dU'>, |dU'|^2, <S, E0>; |R0|^2, <R0, dAu>, |dAu|^2, <delta, R0>
 	double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 	if (local < I.ntn) {
-		FOR_TILE(local * TILE, (int)I.n, i) {
+		FOR_TILE(local, (int)I.n, i) {
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++)
 				if (cc < I.dims) {
@@ -850,11 +884,12 @@ __global__ void __launch_bounds__(BLOCK) k_bt_search(KArgs a) {
 
 // the accepted backtracking step: U' = U'p + alpha (U' - U'p) for U, g, Ux,
 // Uy (, Uz) and Au (g2 is formed again by k_shrink_grad, which follows)
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_lerp(KArgs a) {
 	KPROLOGUE(a);
 	const float al = (float)I.ctrl->alpha;
 	if (local < I.ntn) {
-		FOR_TILE(local * TILE, (int)I.n, i) {
+		FOR_TILE(local, (int)I.n, i) {
 			// every load before the first store
 			const float gi = I.vn[vG][i], gpi = I.vn[vGp][i], ui = I.vn[vU][i], upi = I.vn[vUp][i];
 			float uc[3], ucp[3];
@@ -878,13 +913,14 @@ __global__ void __launch_bounds__(BLOCK) k_lerp(KArgs a) {
 }
 
 // outer stopping test (2d:820-828): RelChgOut = |U - rcdU| / nrmup; rcdU = U
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_outer(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	double v[1] = {0};
 	float *__restrict__ rcd = I.vn[vRcd];
 	const float *__restrict__ U = I.vn[vU];
-	FOR_TILE(local * TILE, (int)I.n, i) {
+	FOR_TILE(local, (int)I.n, i) {
 		float u = U[i];
 		float dlt = u - rcd[i];
 		v[0] += (double)dlt * dlt;
@@ -905,13 +941,14 @@ __global__ void __launch_bounds__(BLOCK) k_outer(KArgs a) {
 }
 
 // update_mlp (2d:673-694) and the continuation step (2d:834-842)
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_mlp(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	const float nbeta = (float)(-1 * c.beta), nmu = (float)(-1 * c.mu);
 	double v[2] = {0, 0};   // lam4, lam5
 	if (local < I.ntn) {
-		FOR_TILE(local * TILE, (int)I.n, i) {
+		FOR_TILE(local, (int)I.n, i) {
 			float vv[3], sv[3];   // every load before the first store
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++) {
@@ -954,12 +991,13 @@ __global__ void __launch_bounds__(BLOCK) k_mlp(KArgs a) {
 }
 
 // final scaling and rel_error (2d:855-877)
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_final(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	const float scl = (float)c.scl;
 	double v[2] = {0, 0};
-	FOR_TILE(local * TILE, (int)I.n, i) {
+	FOR_TILE(local, (int)I.n, i) {
 		float u = I.vn[vU][i];
 		if (I.cplx && I.isreal && i >= (int)(I.n >> 1)) u = 0.f;   // isreal: U = real(U) before scaling
 		u = u / scl;
@@ -979,6 +1017,7 @@ __global__ void __launch_bounds__(BLOCK) k_final(KArgs a) {
 }
 
 // A^T-skip heuristic (2d:306-355), decision part (not forced)
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_skip_norms(KArgs a) {
 	KPROLOGUE(a);
 	if (!I.skip_enabled) return;
@@ -1002,6 +1041,7 @@ __global__ void __launch_bounds__(BLOCK) k_skip_norms(KArgs a) {
 	c.skip_adj = !mul;
 }
 
+template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_copy_lastau(KArgs a) {
 	KPROLOGUE(a);
 	if (!I.skip_enabled) return;
@@ -1107,7 +1147,8 @@ __global__ void k_shrink_plain(int dims, long long n, int iso, double beta, cons
 #define LAUNCHER(name, kern)                                                  \
 	void name(cudaStream_t s, const KArgs &a) {                               \
 		if (a.map.count <= 0) return;                                         \
-		launch_pdl(kern, a.map.count, BLOCK, 0, s, a);                        \
+		if (a.multi) launch_pdl(kern<true>, a.map.count, BLOCK, 0, s, a);     \
+		else launch_pdl(kern<false>, a.map.count, BLOCK, 0, s, a);            \
 	}
 LAUNCHER(launch_scaleb, k_scaleb)
 LAUNCHER(launch_init, k_init)

@@ -32,6 +32,7 @@ struct KArgs {
 	TileMap map;
 	int pred;
 	int stage;
+	int multi;   // some instance has n tiles of more than one element per thread (Inst::ept)
 	unsigned long long *launches;
 	CondSet cs;
 	KArgs &cond(unsigned long long h, int p) {

@@ -901,7 +901,7 @@ __device__ void tile_bitmap(unsigned *bm, int nwords, int p, const int *cptr, co
 // the longest of its pixels' lists, in 16-byte words
 __global__ void __launch_bounds__(RAYT_THREADS) k_tile_count(int ld, int H, int ntx, int nrays, const int *cptr,
                                                              const int *cind, long long *tlen, long long *wlen,
-                                                             unsigned char *perm) {
+                                                             unsigned char *perm, unsigned *gbm) {
 	extern __shared__ unsigned bm[];
 	__shared__ int ws[RAYT_WARPS];
 	__shared__ int cnt[RAYT_THREADS];
@@ -910,7 +910,10 @@ __global__ void __launch_bounds__(RAYT_THREADS) k_tile_count(int ld, int H, int 
 	const int p = tile_pixel(t, threadIdx.x, ntx, ld, H);
 	tile_bitmap(bm, nwords, p, cptr, cind);
 	int c = 0;
-	for (int w = threadIdx.x; w < nwords; w += blockDim.x) c += __popc(bm[w]);
+	for (int w = threadIdx.x; w < nwords; w += blockDim.x) {
+		c += __popc(bm[w]);
+		if (gbm) gbm[(long long)t * nwords + w] = bm[w];   // kept for k_tile_fill
+	}
 	c = __reduce_add_sync(0xffffffffu, c);
 	const int mine = p >= 0 ? cptr[p + 1] - cptr[p] : 0;
 	cnt[threadIdx.x] = mine;
@@ -942,14 +945,20 @@ __global__ void __launch_bounds__(RAYT_THREADS) k_tile_fill(int ld, int H, int n
                                                             const long long *__restrict__ tptr,
                                                             const long long *__restrict__ woff,
                                                             const unsigned char *__restrict__ perm,
-                                                            int *__restrict__ tmeas, uint4 *__restrict__ sidx) {
+                                                            int *__restrict__ tmeas, uint4 *__restrict__ sidx,
+                                                            const unsigned *__restrict__ gbm) {
 	extern __shared__ unsigned bm[];   // nwords bits, then nwords exclusive prefix counts
 	__shared__ int ws[RAYT_WARPS];
 	const int t = blockIdx.x, nwords = (nrays + 31) >> 5;
 	int *pre = reinterpret_cast<int *>(bm + nwords);
 	// thread = rank: its pixel in the order of decreasing list length
 	const int p = tile_pixel(t, perm[(long long)t * RAYT_THREADS + threadIdx.x], ntx, ld, H);
-	tile_bitmap(bm, nwords, p, cptr, cind);
+	if (gbm) {   // the bitmap k_tile_count built
+		for (int w = threadIdx.x; w < nwords; w += blockDim.x) bm[w] = gbm[(long long)t * nwords + w];
+		__syncthreads();
+	} else {
+		tile_bitmap(bm, nwords, p, cptr, cind);
+	}
 	// exclusive prefix of the words' popcounts: thread i scans a contiguous run
 	const int per = (nwords + RAYT_THREADS - 1) / RAYT_THREADS;
 	const int w0 = min(nwords, (int)threadIdx.x * per), w1 = min(nwords, w0 + per);
@@ -1025,7 +1034,11 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 	wlen = (decltype(wlen))dev_alloc(sizeof(long long) * (nw + 1), s);
 	woff = (decltype(woff))dev_alloc(sizeof(long long) * (nw + 1), s);
 	unsigned char *perm = (unsigned char *)dev_alloc((size_t)nt * RAYT_THREADS, s);
-	k_tile_count<<<nt, RAYT_THREADS, smem_count, s>>>(ld, H, ntx, nrays, cptr, cind, tlen, wlen, perm);
+	// the tiles' ray bitmaps, kept from the count for the fill when they take
+	// at most 512 MB (else the fill builds them again)
+	const long long gbm_bytes = (long long)nt * nwords * (long long)sizeof(unsigned);
+	unsigned *gbm = gbm_bytes <= (512LL << 20) ? (unsigned *)dev_alloc((size_t)gbm_bytes, s) : nullptr;
+	k_tile_count<<<nt, RAYT_THREADS, smem_count, s>>>(ld, H, ntx, nrays, cptr, cind, tlen, wlen, perm, gbm);
 	TG_CUDA(cudaGetLastError());
 	scan_counts(s, tlen, tptr, nt);
 	scan_counts(s, wlen, woff, nw);
@@ -1055,7 +1068,7 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 		int *woff32 = (int *)dev_alloc(sizeof(int) * (nw + 1), s);
 		owned.push_back(tmeas); owned.push_back(sidx); owned.push_back(tptr32); owned.push_back(woff32);
 		k_tile_fill<<<nt, RAYT_THREADS, smem_fill, s>>>(ld, H, ntx, nrays, cptr, cind, live_out, tptr, woff, perm,
-		                                                tmeas, sidx);
+		                                                tmeas, sidx, gbm);
 		TG_CUDA(cudaGetLastError());
 		k_to_int<<<(unsigned)((nt + 1 + 255) / 256), 256, 0, s>>>(tptr, tptr32, nt + 1);
 		k_to_int<<<(unsigned)((nw + 1 + 255) / 256), 256, 0, s>>>(woff, woff32, nw + 1);
@@ -1074,6 +1087,7 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 	} else {
 		dev_free(perm, s);
 	}
+	dev_free(gbm, s);
 	dev_free(tlen, s);
 	dev_free(tptr, s);
 	dev_free(wlen, s);
@@ -1502,11 +1516,6 @@ __global__ void k_to_int(const long long *in, int *out, long long n) {
 	if (i < n) out[i] = (int)in[i];
 }
 
-__global__ void k_count_cols(const int *rind, long long nnz, long long *cnt) {
-	for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (long long)gridDim.x * blockDim.x)
-		atomicAdd((unsigned long long *)&cnt[rind[k]], 1ull);
-}
-
 // The transpose is a stable least-significant-digit radix sort of the CSR
 // entries by column, 8 bits per pass: the entries arrive in row order, so
 // each column's rows come out ascending, with no per-column sort and no
@@ -1541,31 +1550,63 @@ __global__ void __launch_bounds__(RADIX_T) k_radix_hist(const int *key, long lon
 // stable scatter of one tile by its digit: within the tile an entry's rank
 // among the entries of its digit follows the input order (round j holds
 // entries j*256 + t; a warp ranks its lanes with __match_any_sync, and the
-// per-digit pass over the warps orders the warps)
-__global__ void __launch_bounds__(RADIX_T) k_radix_scatter(const int *key, const int *val, const float *fval,
-                                                           long long nnz, int shift, const long long *off,
-                                                           int *key_out, int *val_out, float *fval_out) {
+// per-digit pass over the warps orders the warps).  The tile's entries,
+// loaded up front, are first placed in shared memory in digit order (digit
+// d's slots start at the exclusive sum of the tile's counts below d, from
+// k_radix_hist), then written out in slot order: consecutive threads write
+// the consecutive entries of one digit to consecutive addresses, instead of
+// one scattered 4-byte write per entry.
+constexpr int RADIX_DYN_BYTES = RADIX_TILE * 3 * 4;   // keys, values, float values
+__global__ void __launch_bounds__(RADIX_T) k_radix_scatter(const int *__restrict__ key, const int *__restrict__ val,
+                                                           const float *__restrict__ fval, long long nnz, int shift,
+                                                           const long long *__restrict__ off,
+                                                           const long long *__restrict__ hist,
+                                                           int *__restrict__ key_out, int *__restrict__ val_out,
+                                                           float *__restrict__ fval_out) {
+	extern __shared__ int stage[];   // RADIX_TILE keys, then values, then float values (fval only)
+	int *sk = stage, *sv = stage + RADIX_TILE;
+	float *sf = reinterpret_cast<float *>(stage + 2 * RADIX_TILE);
 	__shared__ int wcnt[RADIX_WARPS][256];
 	__shared__ int wbase[RADIX_WARPS][256];
 	__shared__ long long tile_off[256];
+	__shared__ int lstart[256];
+	__shared__ int wsum[RADIX_WARPS];
 	const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-	tile_off[t] = off[(long long)t * gridDim.x + blockIdx.x];
-	int running = 0;   // entries of digit t in the earlier rounds
+	const long long tiles = gridDim.x;
+	tile_off[t] = off[(long long)t * tiles + blockIdx.x];
+	{   // lstart: exclusive sum of the tile's digit counts
+		const int c = (int)hist[(long long)t * tiles + blockIdx.x];
+		int inc = c;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const int u = __shfl_up_sync(0xffffffffu, inc, o);
+			if (lane >= o) inc += u;
+		}
+		if (lane == 31) wsum[w] = inc;
+		__syncthreads();
+		int pre = 0;
+		for (int q = 0; q < w; q++) pre += wsum[q];
+		lstart[t] = pre + inc - c;
+	}
 	const long long base = (long long)blockIdx.x * RADIX_TILE;
+	int kv[RADIX_ITEMS], vv[RADIX_ITEMS];
+	float fv[RADIX_ITEMS];
+#pragma unroll
+	for (int j = 0; j < RADIX_ITEMS; j++) {   // every load up front
+		const long long k = base + j * RADIX_T + t;
+		const bool ok = k < nnz;
+		kv[j] = ok ? key[k] : 0;
+		vv[j] = ok ? val[k] : 0;
+		fv[j] = ok && fval ? fval[k] : 0.f;
+	}
+	int running = 0;   // entries of digit t in the earlier rounds
+#pragma unroll
 	for (int j = 0; j < RADIX_ITEMS; j++) {
 #pragma unroll
 		for (int q = 0; q < RADIX_WARPS; q++) wcnt[q][t] = 0;
 		__syncthreads();
-		const long long k = base + j * RADIX_T + t;
-		const bool ok = k < nnz;
-		int kv = 0, vv = 0;
-		float fv = 0.f;
-		if (ok) {
-			kv = key[k];
-			vv = val[k];
-			if (fval) fv = fval[k];
-		}
-		const int d = ok ? (kv >> shift) & 255 : 256;
+		const bool ok = base + j * RADIX_T + t < nnz;
+		const int d = ok ? (kv[j] >> shift) & 255 : 256;
 		const unsigned peers = __match_any_sync(0xffffffffu, d);
 		const int rank = __popc(peers & ((1u << lane) - 1u));
 		if (ok && rank == 0) wcnt[w][d] = __popc(peers);
@@ -1581,27 +1622,40 @@ __global__ void __launch_bounds__(RADIX_T) k_radix_scatter(const int *key, const
 		}
 		__syncthreads();
 		if (ok) {
-			const long long pos = tile_off[d] + wbase[w][d] + rank;
-			if (key_out) key_out[pos] = kv;
-			val_out[pos] = vv;
-			if (fval_out) fval_out[pos] = fv;
+			const int slot = lstart[d] + wbase[w][d] + rank;
+			sk[slot] = kv[j];
+			sv[slot] = vv[j];
+			if (fval) sf[slot] = fv[j];
 		}
+	}
+	__syncthreads();
+	const int cnt = (int)min((long long)RADIX_TILE, nnz - base);
+	for (int i = t; i < cnt; i += RADIX_T) {
+		const int kk = sk[i], d = (kk >> shift) & 255;
+		const long long pos = tile_off[d] + (i - lstart[d]);
+		if (key_out) key_out[pos] = kk;
+		val_out[pos] = sv[i];
+		if (fval_out) fval_out[pos] = sf[i];
+	}
+}
+
+// a column's entries are contiguous in the sorted keys: its count is (its
+// last entry + 1) - (its first entry), two atomic adds per column
+__global__ void k_col_counts(const int *skey, long long nnz, long long *cnt) {
+	for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nnz;
+	     k += (long long)gridDim.x * blockDim.x) {
+		const int c = skey[k];
+		if (k == nnz - 1 || skey[k + 1] != c) atomicAdd((unsigned long long *)&cnt[c], (unsigned long long)(k + 1));
+		if (k == 0 || skey[k - 1] != c) atomicAdd((unsigned long long *)&cnt[c], (unsigned long long)(-k));
 	}
 }
 
 void build_transpose(cudaStream_t s, long long rows, long long cols, long long nnz, const int *rptr,
                      const int *rind, const float *rval, int *cptr, int *cind, float *cval) {
-	long long *cnt = nullptr, *off = nullptr;
-	cnt = (decltype(cnt))dev_alloc(sizeof(long long) * (cols + 1), s);
-	off = (decltype(off))dev_alloc(sizeof(long long) * (cols + 1), s);
-	TG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(long long) * (cols + 1), s));
-	if (nnz > 0) k_count_cols<<<(unsigned)min(4096LL, (nnz + 255) / 256), 256, 0, s>>>(rind, nnz, cnt);
-	scan_counts(s, cnt, off, cols);
-	k_to_int<<<(unsigned)((cols + 1 + 255) / 256), 256, 0, s>>>(off, cptr, cols + 1);
-	TG_CUDA(cudaGetLastError());
-	dev_free(cnt, s);
-	dev_free(off, s);
-	if (nnz <= 0 || rows <= 0) return;
+	if (nnz <= 0 || rows <= 0) {
+		TG_CUDA(cudaMemsetAsync(cptr, 0, sizeof(int) * (cols + 1), s));
+		return;
+	}
 	int bits = 1;
 	while (bits < 31 && (1LL << bits) < cols) bits++;
 	const int passes = (bits + 7) / 8;
@@ -1612,8 +1666,8 @@ void build_transpose(cudaStream_t s, long long rows, long long cols, long long n
 	hist = (decltype(hist))dev_alloc(sizeof(long long) * (256 * tiles + 1), s);
 	hoff = (decltype(hoff))dev_alloc(sizeof(long long) * (256 * tiles + 1), s);
 	v0 = (decltype(v0))dev_alloc(sizeof(int) * nnz, s);
+	k0 = (decltype(k0))dev_alloc(sizeof(int) * nnz, s);
 	if (passes > 1) {
-		k0 = (decltype(k0))dev_alloc(sizeof(int) * nnz, s);
 		k1 = (decltype(k1))dev_alloc(sizeof(int) * nnz, s);
 		v1 = (decltype(v1))dev_alloc(sizeof(int) * nnz, s);
 		if (rval) {
@@ -1622,27 +1676,102 @@ void build_transpose(cudaStream_t s, long long rows, long long cols, long long n
 		}
 	}
 	k_entry_rows<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(rows, rptr, v0);
+	TG_CUDA(cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, RADIX_DYN_BYTES));
 	// pass p reads (key, row, value) from the previous pass (the CSR itself
-	// first) and writes the next pair of buffers; the last pass writes cind
-	// and cval and drops the keys
+	// first) and writes the next triple of buffers; the last pass writes
+	// cind and cval, and its keys for the column offsets
 	const int *kin = rind, *vin = v0;
 	const float *fin = rval;
 	for (int p = 0; p < passes; p++) {
 		const bool last = p == passes - 1;
-		int *kout = last ? nullptr : (p % 2 == 0 ? k0 : k1);
+		int *kout = p % 2 == 0 ? k0 : k1;
 		int *vout = last ? cind : (p % 2 == 0 ? v1 : v0);
 		float *fout = !rval ? nullptr : last ? cval : (p % 2 == 0 ? f0 : f1);
 		k_radix_hist<<<(unsigned)tiles, RADIX_T, 0, s>>>(kin, nnz, 8 * p, hist);
 		scan_counts(s, hist, hoff, 256 * tiles);
-		k_radix_scatter<<<(unsigned)tiles, RADIX_T, 0, s>>>(kin, vin, fin, nnz, 8 * p, hoff, kout, vout, fout);
+		const int dyn = RADIX_TILE * 4 * (fin ? 3 : 2);   // float values staged only when there are some
+		k_radix_scatter<<<(unsigned)tiles, RADIX_T, dyn, s>>>(kin, vin, fin, nnz, 8 * p, hoff, hist, kout, vout, fout);
 		kin = kout;
 		vin = vout;
 		fin = fout;
 	}
+	long long *cnt = (long long *)dev_alloc(sizeof(long long) * (cols + 1), s);
+	long long *off = (long long *)dev_alloc(sizeof(long long) * (cols + 1), s);
+	TG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(long long) * (cols + 1), s));
+	k_col_counts<<<(unsigned)std::min(8192LL, (nnz + 255) / 256), 256, 0, s>>>(kin, nnz, cnt);
+	scan_counts(s, cnt, off, cols);
+	k_to_int<<<(unsigned)((cols + 1 + 255) / 256), 256, 0, s>>>(off, cptr, cols + 1);
 	TG_CUDA(cudaGetLastError());
 	for (void *ptr : {(void *)hist, (void *)hoff, (void *)v0, (void *)v1, (void *)k0, (void *)k1, (void *)f0,
-	                  (void *)f1})
+	                  (void *)f1, (void *)cnt, (void *)off})
 		if (ptr) dev_free(ptr, s);
+}
+
+__global__ void k_ray_flags(long long cand, const int *up, long long ER, long long *flag) {
+	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < cand;
+	     i += (long long)gridDim.x * blockDim.x)
+		flag[i] = up[i % ER] != 0 ? 1 : 0;
+}
+
+// err[0] / err[1]: the first candidate (loop order) with an endpoint outside
+// the image / a use_path index beyond numPaths
+__global__ void k_ray_pack(RayGeo g, long long cand, const long long *flag, const long long *slot, int4 *rays,
+                           int *out, unsigned long long *err) {
+	const long long ER = (long long)g.E * g.R;
+	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < cand;
+	     i += (long long)gridDim.x * blockDim.x) {
+		if (!flag[i]) continue;
+		const long long mp = i / ER, er = i - mp * ER;
+		const int e = (int)(er / g.R), r = (int)(er - (long long)e * g.R);
+		const int u = g.up[er];
+		const long long ie = mp * g.E + e, ir = mp * g.R + r;
+		const int x0 = g.xe[ie], y0 = g.ye[ie], x1 = g.xr[ir], y1 = g.yr[ir];
+		const int z0 = g.is3 ? g.ze[ie] : 0, z1 = g.is3 ? g.zr[ir] : 0;
+		const bool inside = x0 >= 0 && x0 < g.nx && x1 >= 0 && x1 < g.nx && y0 >= 0 && y0 < g.ny && y1 >= 0 &&
+		                    y1 < g.ny && z0 >= 0 && z0 < g.nz && z1 >= 0 && z1 < g.nz;
+		const long long o = g.is3 ? mp * g.numPaths + u - 1 : er;
+		const bool path_ok = !g.is3 || (u >= 1 && o < g.mtot);
+		if (!inside) atomicMin(err, (unsigned long long)i);
+		else if (!path_ok) atomicMin(err + 1, (unsigned long long)i);
+		else {
+			rays[slot[i]] = pack_ray(x0, y0, z0, x1 - x0, y1 - y0, z1 - z0, (int)o);
+			out[slot[i]] = (int)o;
+		}
+	}
+}
+
+void pack_rays(cudaStream_t s, const RayGeo &g, long long cand, long long *nrays, int4 **rays, int **out) {
+	long long *flag = (long long *)dev_alloc(sizeof(long long) * (size_t)(cand + 1), s);
+	long long *slot = (long long *)dev_alloc(sizeof(long long) * (size_t)(cand + 1), s);
+	unsigned long long *err = (unsigned long long *)dev_alloc(2 * sizeof(unsigned long long), s);
+	const unsigned grid = (unsigned)std::max(1LL, std::min(8192LL, (cand + 255) / 256));
+	if (cand > 0) k_ray_flags<<<grid, 256, 0, s>>>(cand, g.up, (long long)g.E * g.R, flag);
+	scan_counts(s, flag, slot, cand);
+	TG_CUDA(cudaMemsetAsync(err, 0xff, 2 * sizeof(unsigned long long), s));
+	long long nr = 0;
+	TG_CUDA(cudaMemcpyAsync(&nr, slot + cand, sizeof(long long), cudaMemcpyDeviceToHost, s));
+	TG_CUDA(cudaStreamSynchronize(s));
+	int4 *r = (int4 *)dev_alloc(sizeof(int4) * (size_t)std::max(nr, 1LL), s);
+	int *o = (int *)dev_alloc(sizeof(int) * (size_t)std::max(nr, 1LL), s);
+	if (cand > 0) k_ray_pack<<<grid, 256, 0, s>>>(g, cand, flag, slot, r, o, err);
+	TG_CUDA(cudaGetLastError());
+	unsigned long long h_err[2];
+	TG_CUDA(cudaMemcpyAsync(h_err, err, sizeof(h_err), cudaMemcpyDeviceToHost, s));
+	TG_CUDA(cudaStreamSynchronize(s));
+	dev_free(flag, s);
+	dev_free(slot, s);
+	dev_free(err, s);
+	if (h_err[0] != ~0ull || h_err[1] != ~0ull) {
+		dev_free(r, s);
+		dev_free(o, s);
+		if (h_err[0] <= h_err[1])
+			throw Error{TVAL3G_ERR_ARGUMENT, g.is3 ? "Argument error: a ray endpoint lies outside the volume"
+			                                       : "Argument error: a ray endpoint lies outside the image"};
+		throw Error{TVAL3G_ERR_ARGUMENT, "Argument error: use_path index exceeds numPaths"};
+	}
+	*nrays = nr;
+	*rays = r;
+	*out = o;
 }
 
 __global__ void k_ray_len(int nrays, const int4 *rays, long long *len) {

@@ -115,6 +115,21 @@ void scan_counts(cudaStream_t s, const long long *cnt, long long *out, long long
 // CSR (rows x cols, rptr int32) -> CSC sorted by row within a column; cval may be NULL
 void build_transpose(cudaStream_t s, long long rows, long long cols, long long nnz, const int *rptr,
                      const int *rind, const float *rval, int *cptr, int *cind, float *cval);
+// The traced rays of a ray geometry, packed on the device in the reference's
+// loop order (measurement plane, emitter, receiver; a ray for every nonzero
+// use_path entry): 2D: out = e R + r; 3D: out = mp numPaths + use_path - 1.
+// All arrays are device copies of the geometry's.  pack_rays allocates the
+// packed rays and their measurement indices (stream-ordered, the caller's)
+// and throws the reference's argument error for the first offending ray in
+// loop order (an endpoint outside the image or volume; a use_path index
+// beyond numPaths).
+struct RayGeo {
+	int E, R, is3, numPaths;
+	long long mtot;
+	int nx, ny, nz;   // endpoint bounds (2D: ld and min(height, 32767))
+	const int *up, *xe, *ye, *ze, *xr, *yr, *zr;
+};
+void pack_rays(cudaStream_t s, const RayGeo &g, long long cand, long long *nrays, int4 **rays, int **out);
 // rasterise nrays packed rays into CSR over rays (offsets int32 into rptr,
 // nrays + 1 of them; the indices, int32, in a new stream-ordered allocation
 // that the caller owns: dev_free)

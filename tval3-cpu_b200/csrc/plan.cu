@@ -308,51 +308,53 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		st.adj_index_bytes = (long long)sizeof(int) * (d.n + 1) + 8LL * p.nnz;
 		st.b_len = (long long)p.m * d.layers;
 	} else {
-		// traced rays in the reference's loop order (mp, emitter, receiver)
-		std::vector<int4> rays;
-		rays.reserve((size_t)((p.op_kind == TVAL3G_OP_RAY3D ? p.numMPs : 1) * (long long)p.num_emitters * p.num_receivers));
-		st.ray_out.reserve(rays.capacity());
+		// traced rays in the reference's loop order (mp, emitter, receiver),
+		// packed on the device from the geometry (use_path and endpoints)
 		const bool is3 = p.op_kind == TVAL3G_OP_RAY3D;
 		const int E = p.num_emitters, R = p.num_receivers, nmp = is3 ? p.numMPs : 1;
 		const long long mtot = is3 ? (long long)p.numPaths * p.numMPs : (long long)E * R;
-		const int ny = is3 ? 0 : (int)std::min<long long>(n / p.ld, 32767);
-		st.ray_out.clear();
-		for (int mp = 0; mp < nmp; mp++)
-			for (int e = 0; e < E; e++)
-				for (int r = 0; r < R; r++) {
-					const int up = p.use_path[(long long)e * R + r];
-					if (up == 0) continue;
-					int x0, y0, z0 = 0, x1, y1, z1 = 0;
-					long long out;
-					if (!is3) {
-						x0 = p.x_emitters[e]; y0 = p.y_emitters[e];
-						x1 = p.x_receivers[r]; y1 = p.y_receivers[r];
-						TG_ARG(x0 >= 0 && x0 < p.ld && x1 >= 0 && x1 < p.ld && y0 >= 0 && y0 < ny && y1 >= 0 && y1 < ny,
-						       "Argument error: a ray endpoint lies outside the image");
-						out = (long long)e * R + r;
-					} else {
-						const long long ie = (long long)mp * E + e, ir = (long long)mp * R + r;
-						x0 = p.x_emitters[ie]; y0 = p.y_emitters[ie]; z0 = p.z_emitters[ie];
-						x1 = p.x_receivers[ir]; y1 = p.y_receivers[ir]; z1 = p.z_receivers[ir];
-						TG_ARG(x0 >= 0 && x0 < p.rv_x && x1 >= 0 && x1 < p.rv_x && y0 >= 0 && y0 < p.rv_y && y1 >= 0 &&
-						           y1 < p.rv_y && z0 >= 0 && z0 < p.rv_z && z1 >= 0 && z1 < p.rv_z,
-						       "Argument error: a ray endpoint lies outside the volume");
-						out = (long long)mp * p.numPaths + up - 1;
-						TG_ARG(up >= 1 && out < mtot, "Argument error: use_path index exceeds numPaths");
-					}
-					rays.push_back(pack_ray(x0, y0, z0, x1 - x0, y1 - y0, z1 - z0, (int)out));
-					st.ray_out.push_back((int)out);
-				}
-		TG_ARG(rays.size() < (1u << 31), "Argument error: too many rays");
-		d.nrays = (int)rays.size();
+		RayGeo g{};
+		g.E = E; g.R = R; g.is3 = is3; g.numPaths = is3 ? p.numPaths : 0; g.mtot = mtot;
+		g.nx = is3 ? p.rv_x : (int)p.ld;
+		g.ny = is3 ? p.rv_y : (int)std::min<long long>(n / p.ld, 32767);
+		g.nz = is3 ? p.rv_z : 1;
+		const long long ER = (long long)E * R, cand = (long long)nmp * ER;
+		std::vector<void *> tmp;
+		auto up = [&](const int *h, long long cnt) {   // a temporary device copy of a geometry array
+			int *dp = (int *)dev_alloc(sizeof(int) * (size_t)std::max(cnt, 1LL), s);
+			tmp.push_back(dp);
+			if (cnt > 0) TG_CUDA(cudaMemcpyAsync(dp, h, sizeof(int) * (size_t)cnt, cudaMemcpyHostToDevice, s));
+			return (const int *)dp;
+		};
+		g.up = up(p.use_path, ER);
+		g.xe = up(p.x_emitters, (long long)nmp * E); g.ye = up(p.y_emitters, (long long)nmp * E);
+		g.xr = up(p.x_receivers, (long long)nmp * R); g.yr = up(p.y_receivers, (long long)nmp * R);
+		g.ze = is3 ? up(p.z_emitters, (long long)nmp * E) : nullptr;
+		g.zr = is3 ? up(p.z_receivers, (long long)nmp * R) : nullptr;
+		long long nr = 0;
+		int4 *drays = nullptr;
+		int *dout = nullptr;
+		try {
+			pack_rays(s, g, cand, &nr, &drays, &dout);   // throws the reference's argument errors
+		} catch (...) {
+			for (void *q : tmp) dev_free(q, s);
+			throw;
+		}
+		for (void *q : tmp) dev_free(q, s);
+		TG_ARG(nr < (1LL << 31), "Argument error: too many rays");
+		st.owned.push_back(drays); st.owned.push_back(dout);
+		st.bytes += (long long)(sizeof(int4) + sizeof(int)) * std::max(nr, 1LL);
+		d.nrays = (int)nr;
 		d.m = mtot; d.n = n;
 		d.rvx = is3 ? p.rv_x : p.ld;
 		d.rvy = is3 ? p.rv_y : 1;
 		d.scale = p.scale_factor;
-		int4 *drays = dalloc_op<int4>(s, st, d.nrays);
-		if (d.nrays > 0)
-			TG_CUDA(cudaMemcpyAsync(drays, rays.data(), sizeof(int4) * rays.size(), cudaMemcpyHostToDevice, s));
 		d.rays = drays;
+		st.ray_out.clear();
+		if (keep_ray_csr && nr > 0) {   // the host copy the CSR export and the complex form read
+			st.ray_out.resize((size_t)nr);
+			TG_CUDA(cudaMemcpyAsync(st.ray_out.data(), dout, sizeof(int) * (size_t)nr, cudaMemcpyDeviceToHost, s));
+		}
 		// forward CSR over traced rays, then its transpose: the pixel-major
 		// index of the adjoint, entries = measurement indices sorted by ray
 		int *rptr = dalloc_op<int>(s, st, (long long)d.nrays + 1);
@@ -368,9 +370,7 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		BrickLists bl;
 		float *posf = nullptr, *cposf = nullptr;
 		if (is3 && tile_ok) {
-			int *lo = dalloc_op<int>(s, st, std::max(d.nrays, 1));
-			if (d.nrays > 0)
-				TG_CUDA(cudaMemcpyAsync(lo, st.ray_out.data(), sizeof(int) * d.nrays, cudaMemcpyHostToDevice, s));
+			const int *lo = dout;
 			posf = brick_positions(s, p.rv_x, p.rv_y, p.rv_z, d.nrays, total, rptr, rind, lo, bl, st.owned);
 			if (posf) cposf = (float *)dev_alloc(sizeof(float) * (size_t)std::max(total, 1LL), s);
 		}
@@ -392,8 +392,7 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		}
 		if (!is3 && n % p.ld == 0 && d.nrays > 0 && d.nrays <= RAYT_MAX_RAYS && tile_ok) {
 			// tiled adjoint (cind still holds traced-ray ids)
-			int *lo = dalloc_op<int>(s, st, d.nrays);
-			TG_CUDA(cudaMemcpyAsync(lo, st.ray_out.data(), sizeof(int) * d.nrays, cudaMemcpyHostToDevice, s));
+			const int *lo = dout;
 			long long ib = 0;
 			if (build_tiled_index(s, (int)p.ld, (int)(n / p.ld), d.nrays, cptr, cind, lo, d, &ib, st.owned)) {
 				st.bytes += ib;
@@ -687,7 +686,8 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 			I.cplx = p.complex_data != 0;
 			n = I.n;
 			b_len = I.m;
-			I.ntn = (int)((n + TILE - 1) / TILE);
+			I.ept = ept_for(n);
+			I.ntn = (int)((n + (long long)BLOCK * I.ept - 1) / ((long long)BLOCK * I.ept));
 			I.ntm = (int)((b_len + TILE_M - 1) / TILE_M);
 			const tval3g_options &o = opts[i];
 			I.muf = o.mu; I.betaf = o.beta; I.mu0 = o.mu0; I.beta0 = o.beta0; I.tol = o.tol; I.tol_inn = o.tol_inn;
@@ -788,6 +788,40 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 
 Plan::~Plan() { release(); }
 
+void Plan::time_stencils(int reps, double ms[3]) {
+	cur_ = stream_;
+	const bool gm = graph_mode_;
+	graph_mode_ = false;   // es() is the launch stream
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	try {
+		TG_CUDA(cudaEventCreate(&e0));
+		TG_CUDA(cudaEventCreate(&e1));
+		for (int k = 0; k < 3; k++) {
+			auto launch = [&] {
+				if (k == 0) launch_getg(stream_, kargs(MAP_NM, P_ALL, ST_DESCEND));
+				else if (k == 1) launch_descend(stream_, kargs(MAP_NM, P_ALL, ST_DESCEND));
+				else launch_shrink_grad(stream_, kargs(MAP_N, P_ALL, ST_LOOP));
+			};
+			launch();   // warm
+			TG_CUDA(cudaEventRecord(e0, stream_));
+			for (int r = 0; r < reps; r++) launch();
+			TG_CUDA(cudaEventRecord(e1, stream_));
+			TG_CUDA(cudaEventSynchronize(e1));
+			float t = 0.f;
+			TG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+			ms[k] = (double)t / std::max(reps, 1);
+		}
+	} catch (...) {
+		graph_mode_ = gm;
+		if (e0) cudaEventDestroy(e0);
+		if (e1) cudaEventDestroy(e1);
+		throw;
+	}
+	graph_mode_ = gm;
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+}
+
 int Plan::trace(int index, tval3g_trace_record *out, int cap) const {
 	TG_ARG(d_trace_ != nullptr, "Argument error: the plan was created without TVAL3G_TRACE");
 	TG_ARG(index >= 0 && index < count_, "Argument error: instance index out of range");
@@ -821,6 +855,8 @@ KArgs Plan::kargs(MapKind mk, int pred, int stage) const {
 	a.map = maps_[mk];
 	a.pred = pred;
 	a.stage = stage;
+	a.multi = 0;
+	for (const Inst &I : h_inst_) a.multi |= I.ept > 1 ? 1 : 0;
 	a.launches = d_launches_;
 	return a;
 }

@@ -64,6 +64,10 @@ public:
 	int maxit() const { return h_inst_.empty() ? 0 : h_inst_[0].maxit; }
 	// the instances' scalar state after the last solve
 	std::vector<Ctrl> ctrl() const;
+	// mean device time (ms) of one launch of k_getg (descent stage), k_descend
+	// (descent stage) and k_shrink_grad over every instance, each launched reps
+	// times back to back after the last solve (whose state they overwrite)
+	void time_stencils(int reps, double ms[3]);
 
 private:
 	struct Frame {

@@ -85,6 +85,7 @@ def lib():
         L.tval3g_plan_stats.argtypes = [vp, C.POINTER(ll), C.POINTER(ll)]
         L.tval3g_plan_trace.argtypes = [vp, i, C.POINTER(C.c_double), i, C.POINTER(i)]
         L.tval3g_plan_set_target.argtypes = [vp, d]
+        L.tval3g_plan_time_stencils.argtypes = [vp, i, C.POINTER(d)]
         L.tval3g_plan_destroy.argtypes = [vp]
         L.tval3g_trim_memory.argtypes = [ll]
         L.tval3g_tune_stats.argtypes = [C.POINTER(ll), C.POINTER(ll)]
@@ -145,6 +146,7 @@ def tune_stats():
 
 EXPORTS = ("tval3g_last_error", "tval3g_version", "tval3g_solve", "tval3g_solve_batch", "tval3g_plan_create",
            "tval3g_plan_solve", "tval3g_plan_stats", "tval3g_plan_trace", "tval3g_plan_set_target",
+           "tval3g_plan_time_stencils",
            "tval3g_plan_destroy", "tval3g_trim_memory", "tval3g_tune_stats", "tval3g_op_launch_shape",
            "tval3g_op_create", "tval3g_op_shape",
            "tval3g_op_apply", "tval3g_op_apply_n", "tval3g_op_ray_csr", "tval3g_op_adjoint_index_bytes",
@@ -328,6 +330,13 @@ class Plan:
         infos = (Info * n)()
         _check(lib().tval3g_plan_solve(self.h, bp, utp, up, infos, _dptr(stream)))
         return [i.as_dict() for i in infos]
+
+    def time_stencils(self, reps=20):
+        """Mean ms per launch of the gradient epilogue, the descent and the
+        shrinkage kernels (after a solve; overwrites the plan's state)."""
+        ms = (C.c_double * 3)()
+        _check(lib().tval3g_plan_time_stencils(self.h, int(reps), ms))
+        return {"getg": ms[0], "descend": ms[1], "shrink_grad": ms[2]}
 
     def stats(self):
         a, b = C.c_longlong(), C.c_longlong()
