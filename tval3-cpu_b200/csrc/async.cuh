@@ -47,6 +47,36 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned
 	             : "memory");
 }
 
+// L2 cache policies (createpolicy): evict_last keeps lines that will be read
+// again soon; evict_first marks lines at their last use
+__device__ __forceinline__ unsigned long long l2_policy_evict_last() {
+	unsigned long long p;
+	asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+	return p;
+}
+__device__ __forceinline__ unsigned long long l2_policy_evict_first() {
+	unsigned long long p;
+	asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+	return p;
+}
+// bulk_g2s with an L2 cache policy for the source lines
+__device__ __forceinline__ void bulk_g2s_hint(unsigned dst, const void *src, unsigned bytes, unsigned bar,
+                                              unsigned long long policy) {
+	asm volatile(
+	    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+	        dst),
+	    "l"(src), "r"(bytes), "r"(bar), "l"(policy)
+	    : "memory");
+}
+// a 16-byte global load with an L2 cache policy
+__device__ __forceinline__ float4 ld_f4_hint(const float *p, unsigned long long policy) {
+	float4 v;
+	asm volatile("ld.global.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+	             : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+	             : "l"(p), "l"(policy));
+	return v;
+}
+
 constexpr unsigned ASYNC_WAIT_LIMIT = 1u << 22;   // polls before a wait gives up
 
 // every lane of the warp polls phase `parity` of bar; false (after raising

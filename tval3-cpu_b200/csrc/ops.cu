@@ -261,6 +261,9 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_dense_normal(const Inst *t
 		// ---- producer ----
 		if (lane == 0) {
 			const float *u = vsel(I, us);
+			// A's lines are read again by the reducers of other CTAs (from L2):
+			// kept there until then; u is read for every row
+			const unsigned long long keep = l2_policy_evict_last();
 			long long it = 0;
 			for (int b = 0; b < nb && !s_abort; b++) {
 				for (unsigned sp = 0; s_done < b - 1 && !s_abort; sp++) {
@@ -278,9 +281,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_dense_normal(const Inst *t
 						}
 						const int cnt = min(FUSED_CH, n - ch * FUSED_CH);
 						mbar_expect_tx(full0 + 8u * st, 8u * cnt);
-						bulk_g2s(smem_u32(stage_a(st)), A + (long long)(r0 + j) * n + (long long)ch * FUSED_CH, 4u * cnt,
-						         full0 + 8u * st);
-						bulk_g2s(smem_u32(stage_u(st)), u + (long long)ch * FUSED_CH, 4u * cnt, full0 + 8u * st);
+						bulk_g2s_hint(smem_u32(stage_a(st)), A + (long long)(r0 + j) * n + (long long)ch * FUSED_CH,
+						              4u * cnt, full0 + 8u * st, keep);
+						bulk_g2s_hint(smem_u32(stage_u(st)), u + (long long)ch * FUSED_CH, 4u * cnt, full0 + 8u * st,
+						              keep);
 					}
 			}
 			if (s_abort)   // let the copies in flight land before the CTA exits (bounded)
@@ -342,6 +346,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_dense_normal(const Inst *t
 		const int Q = SV >= FUSED_ROLE ? 1 : FUSED_ROLE / SV;   // row groups
 		const int j = t % SV, q = t / SV;
 		const bool act = q < Q && c0 + 4 * j < c1;
+		const unsigned long long last_use = l2_policy_evict_first();   // the second and last read of A's lines
 		double acc[4] = {0.0, 0.0, 0.0, 0.0};
 		for (int b = 0; b < nb; b++) {
 			const int r0 = b * R, rows = min(R, m - r0);
@@ -363,7 +368,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_dense_normal(const Inst *t
 				for (; r + 7 * Q < rows; r += 8 * Q) {
 					float4 v[8];
 #pragma unroll
-					for (int e = 0; e < 8; e++) v[e] = *reinterpret_cast<const float4 *>(a + (long long)(r + e * Q) * n);
+					for (int e = 0; e < 8; e++) v[e] = ld_f4_hint(a + (long long)(r + e * Q) * n, last_use);
 					float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
 #pragma unroll
 					for (int e = 0; e < 8; e++) {
@@ -380,7 +385,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) k_dense_normal(const Inst *t
 				}
 				for (; r < rows; r += Q) {
 					const float w = sauf[r];
-					const float4 v = *reinterpret_cast<const float4 *>(a + (long long)r * n);
+					const float4 v = ld_f4_hint(a + (long long)r * n, last_use);
 					acc[0] += (double)(v.x * w);
 					acc[1] += (double)(v.y * w);
 					acc[2] += (double)(v.z * w);
