@@ -5,15 +5,16 @@
  * (3d/tval3_cpu_3d.cpp:32-146, defined at :1384-1581), with the same names,
  * argument types and defaults, so existing callers relink against
  * libtval3_gpu_3d.so (which exports the same C++ symbols) without source
- * changes.  Each forwards to tval3g_solve (include/tval3g.h).
+ * changes.  Each forwards to tval3g_solve or, for double data,
+ * tval3g_solve_f64 (include/tval3g.h).
  *
  * Differences from the reference:
- *   - float data (mat<float>, with tval3_options<float> or <double>) and
- *     complex<float> data run on the GPU; double and complex<double> data
- *     run through float / complex<float> copies (FP32 storage with FP64
- *     reductions: float accuracy, not double - against the reference's own
- *     double build about 1e-5 relative after 20 iterations, bounded by 1e-4
- *     in tests/test_dropin.py; the reference's float build is further off);
+ *   - float and complex<float> data run on the FP32 engine (FP32 storage,
+ *     FP64 reductions: closer to the reference's double build than the
+ *     reference's own float build is); double and complex<double> data run
+ *     on the FP64 engine (tval3g_solve_f64: double storage and arithmetic,
+ *     as the reference's double instantiations compute), held to the
+ *     reference's double builds in tests/test_gpu_f64.py;
  *   - submat_mb and virtual_procs_per_core are accepted and ignored (they
  *     tune the reference's CPU cache blocking and thread count);
  *   - ray endpoints outside the volume are rejected with an argument error

@@ -14,6 +14,8 @@
  *                       889-1016) and tval3_cpu_3d (3d/tval3_cpu_3d.cpp:32-146,
  *                       1384-1581) for float data, through the templated driver
  *                       (2d/tval3_cpu_2d.cpp:752-886, 3d/tval3_cpu_3d.cpp:1172-1378)
+ *   tval3g_solve_f64    the same overloads for double and complex<double> data
+ *                       (the driver's double instantiations), solved in double
  *   tval3g_solve_batch  no reference counterpart: many independent solves in one
  *                       batched launch sequence (each one as tval3g_solve)
  *   tval3g_plan_*       no reference counterpart: the same solves with device-
@@ -160,6 +162,22 @@ int tval3g_version(void);
  * autotuner (TVAL3G_TUNE). */
 int tval3g_solve(const tval3g_problem *prob, const float *b, int b_len, const tval3g_options *opts,
                  const float *Ut, int ut_len, float *U, tval3g_info *info);
+
+/* One solve in double precision with host buffers: the FP64 build of the
+ * engine (double vectors, double operator values and products, double
+ * stencils and shrinkage; the same kernels' algorithm as tval3g_solve, with
+ * the pixel-major gather adjoint for ray operators and the gemv kernels for
+ * dense ones).  prob describes the problem as for tval3g_solve except that
+ * its float arrays A and csr_val are not read: A64 holds the dense matrix
+ * (DENSE: m x n_cols row-major) or the CSR values (CSR: nnz of them), and is
+ * NULL for ray geometries; b (b_len), Ut (ut_len: 0 or n; may be NULL) and U
+ * (n, output) are doubles.  With complex_data = 1 every one of these arrays
+ * holds interleaved (re, im) double pairs, and the lengths count complex
+ * elements.  Replaces the double and complex<double> instantiations of the
+ * drivers (2d/tval3_cpu_2d.cpp:905-1016, 3d/tval3_cpu_3d.cpp:1408-1581),
+ * which compute in double. */
+int tval3g_solve_f64(const tval3g_problem *prob, const double *A64, const double *b, int b_len,
+                     const tval3g_options *opts, const double *Ut, int ut_len, double *U, tval3g_info *info);
 
 /* count independent solves with host buffers, run as one batch (flags:
  * TVAL3G_GRAPH, TVAL3G_TUNE).  Arrays are indexed by problem; Ut may be NULL. */

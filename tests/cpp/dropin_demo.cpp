@@ -4,8 +4,10 @@
 //   dropin_demo errors   argument errors only (no GPU needed): prints one
 //                        exception message per line
 //   dropin_demo solve    a small dense, CSR and 2D-ray solve through
-//                        tval3_cpu_2d, each compared with tval3g_solve on the
-//                        same inputs; prints "<case> <max |diff|> <iters>"
+//                        tval3_cpu_2d, each compared with tval3g_solve (float
+//                        and complex<float> data) or tval3g_solve_f64 (double
+//                        data) on the same inputs; prints
+//                        "<case> <rc> <max |diff|> <iters> <C ABI iters>"
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -113,18 +115,26 @@ static void solve_cases() {
 	tval3g_info ci;
 	int rc = tval3g_solve(&pr, b.data(), m, &co, 0, 0, U2.data(), &ci);
 	std::printf("dense %d %.3e %d %d\n", rc, maxdiff(U.data(), U2.data(), n), info.total_iters, ci.total_iters);
-	{   // double data through the double overload: FP32 copies of the same values, the same solve
+	tval3_options<double> od;
+	od.mu = o.mu; od.beta = o.beta; od.mu0 = o.mu0; od.beta0 = o.beta0; od.tol = o.tol; od.tol_inn = o.tol_inn;
+	od.maxit = o.maxit; od.maxcnt = o.maxcnt;
+	od.c = o.c; od.gamma = o.gamma; od.gam = o.gam; od.rate_gam = o.rate_gam; od.rate_cnt = o.rate_cnt;
+	{   // double data through the double overload and through tval3g_solve_f64 (the FP64 engine)
 		mat<double> Ad(m, n, mat_row_major), Ud(p, q, mat_col_major), bd(m), Utd(0, mat_col_major);
 		for (int i = 0; i < m * n; i++) Ad[i] = A[i];
 		for (int r = 0; r < m; r++) bd[r] = b[r];
-		tval3_options<double> od;
-		od.mu = o.mu; od.beta = o.beta; od.mu0 = o.mu0; od.beta0 = o.beta0; od.tol = o.tol; od.tol_inn = o.tol_inn;
-		od.maxit = o.maxit; od.maxcnt = o.maxcnt;
-		od.c = o.c; od.gamma = o.gamma; od.gam = o.gam; od.rate_gam = o.rate_gam; od.rate_cnt = o.rate_cnt;
 		tval3_info<double> infod = tval3_cpu_2d(Ud, Ad, bd, od, Utd);
-		double d = 0;
-		for (int i = 0; i < n; i++) d = std::fmax(d, std::fabs(Ud[i] - (double)U2[i]));
-		std::printf("dense_f64 0 %.3e %d %d\n", d, infod.total_iters, ci.total_iters);
+		tval3g_problem pd = pr;
+		pd.A = 0;
+		std::vector<double> Ud2(n);
+		tval3g_info cid;
+		int rcd = tval3g_solve_f64(&pd, Ad.data(), bd.data(), m, &co, 0, 0, Ud2.data(), &cid);
+		double d = 0, df = 0;
+		for (int i = 0; i < n; i++) {
+			d = std::fmax(d, std::fabs(Ud[i] - Ud2[i]));
+			df = std::fmax(df, std::fabs(Ud[i] - (double)U2[i]));
+		}
+		std::printf("dense_f64 %d %.3e %d %d %.3e\n", rcd, d, infod.total_iters, cid.total_iters, df);
 	}
 	// CSR twin of A restricted to |a| > 0.2
 	std::vector<int> ptr(1, 0), ind;
@@ -160,6 +170,17 @@ static void solve_cases() {
 	pr.x_emitters = xs; pr.y_emitters = ys; pr.x_receivers = xs; pr.y_receivers = ys; pr.ld = q; pr.scale_factor = 1.f;
 	rc = tval3g_solve(&pr, br.data(), T * T, &co, 0, 0, U2.data(), &ci);
 	std::printf("ray2d %d %.3e %d %d\n", rc, maxdiff(Ur.data(), U2.data(), n), info.total_iters, ci.total_iters);
+	{   // the same rays with double data: the double overload and tval3g_solve_f64
+		mat<double> Urd(p, q, mat_row_major), brd(T * T), Utrd(0, mat_row_major);
+		for (int i = 0; i < T * T; i++) brd[i] = br[i];
+		tval3_info<double> infod = tval3_cpu_2d(Urd, g, brd, od, Utrd);
+		std::vector<double> Ud2(n);
+		tval3g_info cid;
+		int rcd = tval3g_solve_f64(&pr, 0, brd.data(), T * T, &co, 0, 0, Ud2.data(), &cid);
+		double d = 0;
+		for (int i = 0; i < n; i++) d = std::fmax(d, std::fabs(Urd[i] - Ud2[i]));
+		std::printf("ray2d_f64 %d %.3e %d %d\n", rcd, d, infod.total_iters, cid.total_iters);
+	}
 	{   // complex data through the complex<float> overload and through the C ABI
 		mat<std::complex<float> > Ac(m, n, mat_row_major), Uc(p, q, mat_col_major), bc(m), Utc(0, mat_col_major);
 		for (int i = 0; i < m * n; i++) Ac[i] = std::complex<float>(A[i], frand() / std::sqrt((float)m));

@@ -64,29 +64,9 @@ def test_argument_errors_match_reference(demo):
 def test_dropin_solves_equal_c_abi(demo, torch_cuda):
     out = subprocess.run([demo, "solve"], capture_output=True, text=True, check=True).stdout.strip().splitlines()
     rows = {line.split()[0]: line.split()[1:] for line in out}
-    for case in ("dense", "dense_f64", "csr", "ray2d", "cdense"):
-        rc, diff, it1, it2 = rows[case]
+    for case in ("dense", "dense_f64", "csr", "ray2d", "ray2d_f64", "cdense"):
+        rc, diff, it1, it2 = rows[case][:4]
         assert rc == "0" and float(diff) == 0.0 and it1 == it2, (case, rows[case])
-
-
-@pytest.mark.gpu
-@pytest.mark.parametrize("name", ["dense2d_s32_it20", "ring2d_s64_it20", "hemi3d_s16_it20", "csr3d_s16",
-                                  "dense3d_s8"])
-def test_double_overloads_accuracy_vs_reference_double(name, torch_cuda):
-    """What a caller of the reference's double overloads (2d:905, 3d:1408)
-    gets from the drop-in: the solve runs on FP32 copies of its data (the
-    double overload equals the float C ABI bit for bit,
-    test_dropin_solves_equal_c_abi), so against the reference's own double
-    build it is as accurate as an FP32 solve with FP64 reductions: measured
-    and bounded here at a fixed iteration count, 1e-4 relative (the reference's
-    own float build is printed beside it); the cases run 20 to 40 iterations."""
-    from golden.cases import api_problem, build_case
-    from helpers import golden, relerr
-    from tval3g import capi
-    c = build_case(name)
-    g = golden(f"{name}.npz")
-    U, info = capi.solve(api_problem(c, capi), c["b"].astype(np.float64).astype(np.float32), c["opts"])
-    assert info["total_iters"] == int(g["ref2_iters"][1])
-    e, e_ref = relerr(U, g["ref2_U"]), relerr(g["ref0_U"], g["ref2_U"])
-    print(f"{name}: drop-in vs the reference's double build {e:.2e} (the reference's float build {e_ref:.2e})")
-    assert e <= 1e-4
+    # double data is solved in double: not the float solve of the same values
+    print("dense: double overload vs the float solve of the same values", rows["dense_f64"][4])
+    assert float(rows["dense_f64"][4]) > 0.0

@@ -56,21 +56,54 @@ inline void set_image(tval3g_problem &p, int dims, const mat<T> &U) {
 	p.dim_z = dims == 3 ? U.dim_z : 1;
 }
 
-// the float view of float or complex<float> data (interleaved re, im)
-inline const float *fdata(const mat<float> &a) { return a.data(); }
-inline float *fdata(mat<float> &a) { return a.data(); }
-inline const float *fdata(const mat<std::complex<float> > &a) { return reinterpret_cast<const float *>(a.data()); }
-inline float *fdata(mat<std::complex<float> > &a) { return reinterpret_cast<float *>(a.data()); }
+// element type of real or complex data (complex: interleaved re, im)
+template <class T> struct elem { typedef T type; };
+template <class T> struct elem<std::complex<T> > { typedef T type; };
+template <class T>
+inline const typename elem<T>::type *edata(const mat<T> &a) {
+	return reinterpret_cast<const typename elem<T>::type *>(a.data());
+}
+template <class T>
+inline typename elem<T>::type *edata(mat<T> &a) {
+	return reinterpret_cast<typename elem<T>::type *>(a.data());
+}
+// the operator values of a dense or sparse matrix as the problem's A /
+// csr_val fields hold them: float data as it is; double data still in
+// double, which c_solve passes on to tval3g_solve_f64 as its A64 argument
+template <class T>
+inline const float *raw_values(const T *v) {
+	return reinterpret_cast<const float *>(v);
+}
 
-// run a solve (T = float, or complex<float> with p.complex_data = 1); throws
-// tval3_exception with the C ABI's message on failure
+// float and complex<float> data: the FP32 engine
+inline int c_solve(const tval3g_problem &p, const float *b, int b_len, const tval3g_options *o, const float *Ut,
+                   int ut_len, float *U, tval3g_info *info) {
+	return tval3g_solve(&p, b, b_len, o, Ut, ut_len, U, info);
+}
+// double and complex<double> data: the FP64 engine (the reference's double
+// instantiations, 2d/tval3_cpu_2d.cpp:905,948,991 and 3d/tval3_cpu_3d.cpp:
+// 1408,1475,1542, compute in double)
+inline int c_solve(const tval3g_problem &p, const double *b, int b_len, const tval3g_options *o,
+                   const double *Ut, int ut_len, double *U, tval3g_info *info) {
+	const double *A64 = p.op_kind == TVAL3G_OP_DENSE ? reinterpret_cast<const double *>(p.A)
+	                    : p.op_kind == TVAL3G_OP_CSR ? reinterpret_cast<const double *>(p.csr_val)
+	                                                 : 0;
+	tval3g_problem q = p;
+	q.A = 0;
+	q.csr_val = 0;
+	return tval3g_solve_f64(&q, A64, b, b_len, o, Ut, ut_len, U, info);
+}
+
+// run a solve (T = float or double, or their complex forms with
+// p.complex_data = 1); throws tval3_exception with the C ABI's message on
+// failure
 template <class S, class T>
 inline tval3_info<S> solve(const tval3g_problem &p, mat<T> &U, const mat<T> &b, const tval3_options<S> &opts,
                            const mat<T> &Ut) {
 	tval3g_options o = to_c(opts);
 	tval3g_info info;
 	std::memset(&info, 0, sizeof(info));
-	int rc = tval3g_solve(&p, fdata(b), b.len, &o, Ut.len > 0 ? fdata(Ut) : 0, Ut.len, fdata(U), &info);
+	int rc = c_solve(p, edata(b), b.len, &o, Ut.len > 0 ? edata(Ut) : 0, Ut.len, edata(U), &info);
 	if (rc != TVAL3G_OK) {
 		std::string msg = tval3g_last_error();
 		if (rc == TVAL3G_ERR_ARGUMENT) throw tval3_exception(msg);
@@ -78,55 +111,6 @@ inline tval3_info<S> solve(const tval3g_problem &p, mat<T> &U, const mat<T> &b, 
 	}
 	return from_c<S>(info);
 }
-
-// Double data (the reference's double overloads, 2d/tval3_cpu_2d.cpp:905,
-// 948,991 and 3d/tval3_cpu_3d.cpp:1408,1475,1542) runs through the FP32
-// engine: FP32 copies of the arrays (shape and format kept), the FP32 solve
-// with its FP64 reductions, the solution widened into the caller's U.  The
-// result therefore carries FP32 storage error, not double precision.
-inline mat<float> narrow(const mat<double> &a) {
-	mat<float> f(a.dim_y, a.dim_x, a.dim_z, a.format);
-	for (int i = 0; i < a.len; i++) f[i] = (float)a[i];
-	return f;
-}
-inline void narrow(const sparse_mat<double> &a, sparse_mat<float> &f) {   // f: sized as a
-	std::memcpy(f.csr_ptr(), a.csr_ptr(), sizeof(int) * ((size_t)a.dim_y + 1));
-	std::memcpy(f.csc_ptr(), a.csc_ptr(), sizeof(int) * ((size_t)a.dim_x + 1));
-	if (a.nnz > 0) {
-		std::memcpy(f.csr_ind(), a.csr_ind(), sizeof(int) * (size_t)a.nnz);
-		std::memcpy(f.csc_ind(), a.csc_ind(), sizeof(int) * (size_t)a.nnz);
-	}
-	for (int k = 0; k < a.nnz; k++) {
-		f.csr_val()[k] = (float)a.csr_val()[k];
-		f.csc_val()[k] = (float)a.csc_val()[k];
-	}
-}
-inline void widen(const mat<float> &f, mat<double> &a) {
-	for (int i = 0; i < a.len && i < f.len; i++) a[i] = (double)f[i];
-}
-// complex<double> data (the reference's complex<double> overloads) likewise
-// through complex<float>
-inline mat<std::complex<float> > narrow(const mat<std::complex<double> > &a) {
-	mat<std::complex<float> > f(a.dim_y, a.dim_x, a.dim_z, a.format);
-	for (int i = 0; i < a.len; i++) f[i] = std::complex<float>((float)a[i].real(), (float)a[i].imag());
-	return f;
-}
-inline void narrow(const sparse_mat<std::complex<double> > &a, sparse_mat<std::complex<float> > &f) {
-	std::memcpy(f.csr_ptr(), a.csr_ptr(), sizeof(int) * ((size_t)a.dim_y + 1));
-	std::memcpy(f.csc_ptr(), a.csc_ptr(), sizeof(int) * ((size_t)a.dim_x + 1));
-	if (a.nnz > 0) {
-		std::memcpy(f.csr_ind(), a.csr_ind(), sizeof(int) * (size_t)a.nnz);
-		std::memcpy(f.csc_ind(), a.csc_ind(), sizeof(int) * (size_t)a.nnz);
-	}
-	for (int k = 0; k < a.nnz; k++) {
-		f.csr_val()[k] = std::complex<float>((float)a.csr_val()[k].real(), (float)a.csr_val()[k].imag());
-		f.csc_val()[k] = std::complex<float>((float)a.csc_val()[k].real(), (float)a.csc_val()[k].imag());
-	}
-}
-inline void widen(const mat<std::complex<float> > &f, mat<std::complex<double> > &a) {
-	for (int i = 0; i < a.len && i < f.len; i++) a[i] = std::complex<double>(f[i].real(), f[i].imag());
-}
-
 
 }  // namespace tval3g_dropin
 

@@ -23,7 +23,7 @@ tval3_info<S> dense2d(mat<T> &U, const mat<T> &A, const mat<T> &b, const tval3_o
 	p.m = A.dim_y;
 	p.n_cols = A.dim_x;
 	p.layers = A.dim_y > 0 ? b.len / A.dim_y : 0;   // 2d/tval3_cpu_2d.cpp:894
-	p.A = fdata(A);
+	p.A = raw_values(A.data());
 	p.complex_data = is_cplx<T>::value;
 	return solve<S>(p, U, b, opts, Ut);
 }
@@ -44,7 +44,7 @@ tval3_info<S> sparse2d(mat<T> &U, const sparse_mat<T> &A, const mat<T> &b, const
 	p.nnz = A.nnz;
 	p.csr_ptr = A.csr_ptr();
 	p.csr_ind = A.csr_ind();
-	p.csr_val = reinterpret_cast<const float *>(A.csr_val());
+	p.csr_val = raw_values(A.csr_val());
 	p.complex_data = is_cplx<T>::value;
 	return solve<S>(p, U, b, opts, Ut);
 }
@@ -82,11 +82,7 @@ const tval3_info<double> tval3_cpu_2d(mat<float> &U, const mat<float> &A, const 
 }
 const tval3_info<double> tval3_cpu_2d(mat<double> &U, const mat<double> &A, const mat<double> &b,
                                       const tval3_options<double> &opts, const mat<double> &Ut, int, int) {
-	mat<float> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
-	mat<float> Af = narrow(A);
-	const tval3_info<double> r = dense2d<double>(Uf, Af, bf, opts, Utf);
-	widen(Uf, U);
-	return r;
+	return dense2d<double>(U, A, b, opts, Ut);
 }
 const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &U, const mat<std::complex<float> > &A,
                                      const mat<std::complex<float> > &b, const tval3_options<float> &opts,
@@ -96,10 +92,7 @@ const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &U, const mat<std
 const tval3_info<double> tval3_cpu_2d(mat<std::complex<double> > &U, const mat<std::complex<double> > &A,
                                       const mat<std::complex<double> > &b, const tval3_options<double> &opts,
                                       const mat<std::complex<double> > &Ut, int, int) {
-	mat<std::complex<float> > Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut), Af = narrow(A);
-	const tval3_info<double> r = dense2d<double>(Uf, Af, bf, opts, Utf);
-	widen(Uf, U);
-	return r;
+	return dense2d<double>(U, A, b, opts, Ut);
 }
 
 // ---- sparse ----------------------------------------------------------------
@@ -113,12 +106,7 @@ const tval3_info<double> tval3_cpu_2d(mat<float> &U, const sparse_mat<float> &A,
 }
 const tval3_info<double> tval3_cpu_2d(mat<double> &U, const sparse_mat<double> &A, const mat<double> &b,
                                       const tval3_options<double> &opts, const mat<double> &Ut, int, int) {
-	mat<float> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
-	sparse_mat<float> Af(A.dim_y, A.dim_x, A.nnz, A.format);
-	narrow(A, Af);
-	const tval3_info<double> r = sparse2d<double>(Uf, Af, bf, opts, Utf);
-	widen(Uf, U);
-	return r;
+	return sparse2d<double>(U, A, b, opts, Ut);
 }
 const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &U, const sparse_mat<std::complex<float> > &A,
                                      const mat<std::complex<float> > &b, const tval3_options<float> &opts,
@@ -128,12 +116,7 @@ const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &U, const sparse_
 const tval3_info<double> tval3_cpu_2d(mat<std::complex<double> > &U, const sparse_mat<std::complex<double> > &A,
                                       const mat<std::complex<double> > &b, const tval3_options<double> &opts,
                                       const mat<std::complex<double> > &Ut, int, int) {
-	mat<std::complex<float> > Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
-	sparse_mat<std::complex<float> > Af(A.dim_y, A.dim_x, A.nnz, A.format);
-	narrow(A, Af);
-	const tval3_info<double> r = sparse2d<double>(Uf, Af, bf, opts, Utf);
-	widen(Uf, U);
-	return r;
+	return sparse2d<double>(U, A, b, opts, Ut);
 }
 
 // ---- geometry --------------------------------------------------------------
@@ -147,10 +130,7 @@ const tval3_info<double> tval3_cpu_2d(mat<float> &U, const geometry &A, const ma
 }
 const tval3_info<double> tval3_cpu_2d(mat<double> &U, const geometry &A, const mat<double> &b,
                                       const tval3_options<double> &opts, const mat<double> &Ut, int, int) {
-	mat<float> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
-	const tval3_info<double> r = ray2d<double>(Uf, A, bf, opts, Utf);
-	widen(Uf, U);
-	return r;
+	return ray2d<double>(U, A, b, opts, Ut);
 }
 const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &U, const geometry &A,
                                      const mat<std::complex<float> > &b, const tval3_options<float> &opts,
@@ -160,8 +140,5 @@ const tval3_info<float> tval3_cpu_2d(mat<std::complex<float> > &U, const geometr
 const tval3_info<double> tval3_cpu_2d(mat<std::complex<double> > &U, const geometry &A,
                                       const mat<std::complex<double> > &b, const tval3_options<double> &opts,
                                       const mat<std::complex<double> > &Ut, int, int) {
-	mat<std::complex<float> > Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
-	const tval3_info<double> r = ray2d<double>(Uf, A, bf, opts, Utf);
-	widen(Uf, U);
-	return r;
+	return ray2d<double>(U, A, b, opts, Ut);
 }

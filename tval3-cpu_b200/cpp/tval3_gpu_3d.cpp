@@ -24,7 +24,7 @@ tval3_info<S> dense3d(mat<T> &U, const mat<T> &A, const mat<T> &b, const tval3_o
 	p.op_kind = TVAL3G_OP_DENSE;
 	p.m = A.dim_y;
 	p.n_cols = A.dim_x;
-	p.A = fdata(A);
+	p.A = raw_values(A.data());
 	p.complex_data = is_cplx<T>::value;
 	return solve<S>(p, U, b, opts, Ut);
 }
@@ -44,7 +44,7 @@ tval3_info<S> sparse3d(mat<T> &U, const sparse_mat<T> &A, const mat<T> &b, const
 	p.nnz = A.nnz;
 	p.csr_ptr = A.csr_ptr();
 	p.csr_ind = A.csr_ind();
-	p.csr_val = reinterpret_cast<const float *>(A.csr_val());
+	p.csr_val = raw_values(A.csr_val());
 	p.complex_data = is_cplx<T>::value;
 	return solve<S>(p, U, b, opts, Ut);
 }
@@ -100,11 +100,7 @@ const tval3_info<double> tval3_cpu_3d(mat<float> &U, const mat<float> &A, const 
 }
 const tval3_info<double> tval3_cpu_3d(mat<double> &U, const mat<double> &A, const mat<double> &b,
                                       const tval3_options<double> &opts, const mat<double> &Ut, int, int) {
-	mat<float> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
-	mat<float> Af = narrow(A);
-	const tval3_info<double> r = dense3d<double>(Uf, Af, bf, opts, Utf);
-	widen(Uf, U);
-	return r;
+	return dense3d<double>(U, A, b, opts, Ut);
 }
 const tval3_info<float> tval3_cpu_3d(mat<cf> &U, const mat<cf> &A, const mat<cf> &b,
                                      const tval3_options<float> &opts, const mat<cf> &Ut, int, int) {
@@ -112,11 +108,7 @@ const tval3_info<float> tval3_cpu_3d(mat<cf> &U, const mat<cf> &A, const mat<cf>
 }
 const tval3_info<double> tval3_cpu_3d(mat<cd> &U, const mat<cd> &A, const mat<cd> &b,
                                       const tval3_options<double> &opts, const mat<cd> &Ut, int, int) {
-	mat<cf> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
-	mat<cf> Af = narrow(A);
-	const tval3_info<double> r = dense3d<double>(Uf, Af, bf, opts, Utf);
-	widen(Uf, U);
-	return r;
+	return dense3d<double>(U, A, b, opts, Ut);
 }
 
 const tval3_info<float> tval3_cpu_3d(mat<float> &U, const sparse_mat<float> &A, const mat<float> &b,
@@ -129,12 +121,7 @@ const tval3_info<double> tval3_cpu_3d(mat<float> &U, const sparse_mat<float> &A,
 }
 const tval3_info<double> tval3_cpu_3d(mat<double> &U, const sparse_mat<double> &A, const mat<double> &b,
                                       const tval3_options<double> &opts, const mat<double> &Ut, int, int) {
-	mat<float> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
-	sparse_mat<float> Af(A.dim_y, A.dim_x, A.nnz, A.format);
-	narrow(A, Af);
-	const tval3_info<double> r = sparse3d<double>(Uf, Af, bf, opts, Utf);
-	widen(Uf, U);
-	return r;
+	return sparse3d<double>(U, A, b, opts, Ut);
 }
 const tval3_info<float> tval3_cpu_3d(mat<cf> &U, const sparse_mat<cf> &A, const mat<cf> &b,
                                      const tval3_options<float> &opts, const mat<cf> &Ut, int, int) {
@@ -142,12 +129,7 @@ const tval3_info<float> tval3_cpu_3d(mat<cf> &U, const sparse_mat<cf> &A, const 
 }
 const tval3_info<double> tval3_cpu_3d(mat<cd> &U, const sparse_mat<cd> &A, const mat<cd> &b,
                                       const tval3_options<double> &opts, const mat<cd> &Ut, int, int) {
-	mat<cf> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
-	sparse_mat<cf> Af(A.dim_y, A.dim_x, A.nnz, A.format);
-	narrow(A, Af);
-	const tval3_info<double> r = sparse3d<double>(Uf, Af, bf, opts, Utf);
-	widen(Uf, U);
-	return r;
+	return sparse3d<double>(U, A, b, opts, Ut);
 }
 
 const tval3_info<float> tval3_cpu_3d(mat<float> &U, const geometry &A, const mat<float> &b,
@@ -160,10 +142,7 @@ const tval3_info<double> tval3_cpu_3d(mat<float> &U, const geometry &A, const ma
 }
 const tval3_info<double> tval3_cpu_3d(mat<double> &U, const geometry &A, const mat<double> &b,
                                       const tval3_options<double> &opts, const mat<double> &Ut, int, int) {
-	mat<float> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
-	const tval3_info<double> r = ray3d<double>(Uf, A, bf, opts, Utf);
-	widen(Uf, U);
-	return r;
+	return ray3d<double>(U, A, b, opts, Ut);
 }
 const tval3_info<float> tval3_cpu_3d(mat<cf> &U, const geometry &A, const mat<cf> &b,
                                      const tval3_options<float> &opts, const mat<cf> &Ut, int, int) {
@@ -171,8 +150,5 @@ const tval3_info<float> tval3_cpu_3d(mat<cf> &U, const geometry &A, const mat<cf
 }
 const tval3_info<double> tval3_cpu_3d(mat<cd> &U, const geometry &A, const mat<cd> &b,
                                       const tval3_options<double> &opts, const mat<cd> &Ut, int, int) {
-	mat<cf> Uf = narrow(U), bf = narrow(b), Utf = narrow(Ut);
-	const tval3_info<double> r = ray3d<double>(Uf, A, bf, opts, Utf);
-	widen(Uf, U);
-	return r;
+	return ray3d<double>(U, A, b, opts, Ut);
 }

@@ -1,8 +1,9 @@
 // Internal declarations of the tval3g engine (sm_100a).
 //
 // Layout in HBM.  A plan holds `count` instances (independent reconstructions).
-// Each instance owns NVN image-sized float vectors and NVM measurement-sized
-// float vectors carved from one arena, a Ctrl block of FP64 scalars and flags,
+// Each instance owns NVN image-sized vectors and NVM measurement-sized
+// vectors (of `real`: float, or double in the FP64 build) carved from one
+// arena, a Ctrl block of FP64 scalars and flags,
 // and a slice of the FP64 partial-sum buffer.  Kernels are launched over tile
 // maps: a tile map is a device array of (instance, local tile) pairs, so one
 // launch covers every instance of a batch; per-instance predicates (Ctrl flags)
@@ -21,6 +22,27 @@
 #include <vector>
 
 #include "../../include/tval3g.h"
+
+// Storage precision of the engine.  The engine's sources are compiled twice:
+// once with FP32 storage (the solver behind tval3g_solve and the float
+// overloads) and once, with TVAL3G_FP64 defined, with FP64 storage (behind
+// tval3g_solve_f64 and the double overloads).  Each build puts its types,
+// kernels and host code in its own inline namespace (tval3g::f32,
+// tval3g::f64); the error reporting and the device-memory pool below are
+// shared.  FP32-only parts (the tcgen05 multi-RHS product, the one-pass dense
+// normal product, the tiled ray adjoints, the autotuner, the unrolled solve)
+// exist only in the FP32 build.
+#ifdef TVAL3G_FP64
+#define TG_PREC f64
+#else
+#define TG_PREC f32
+#endif
+#define TG_BEGIN           \
+	namespace tval3g {     \
+	inline namespace TG_PREC {
+#define TG_END \
+	}          \
+	}
 
 namespace tval3g {
 
@@ -51,6 +73,33 @@ cudaMemPool_t library_pool();   // the current device's pool
 	do {                                                                                            \
 		if (!(cond)) throw ::tval3g::Error{TVAL3G_ERR_ARGUMENT, (msg)};                             \
 	} while (0)
+
+}  // namespace tval3g
+
+TG_BEGIN
+
+// element type of the image and measurement vectors and of dense / CSR
+// operator values
+#ifdef TVAL3G_FP64
+typedef double real;
+#else
+typedef float real;
+#endif
+constexpr bool FP64_BUILD = sizeof(real) == 8;
+// math on `real` (the float forms in the FP32 build, the double forms in the
+// FP64 build)
+__device__ __forceinline__ float tsqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double tsqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float tfabs(float x) { return fabsf(x); }
+__device__ __forceinline__ double tfabs(double x) { return fabs(x); }
+__device__ __forceinline__ float tfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double tfma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float thypot(float a, float b) { return hypotf(a, b); }
+__device__ __forceinline__ double thypot(double a, double b) { return hypot(a, b); }
+// a problem's dense A and CSR values as the build's element type
+// (tval3g_solve_f64 passes its double arrays in these fields)
+inline const real *prob_A(const tval3g_problem &p) { return reinterpret_cast<const real *>(p.A); }
+inline const real *prob_val(const tval3g_problem &p) { return reinterpret_cast<const real *>(p.csr_val); }
 
 // ---------------------------------------------------------------------------
 // per-instance vectors
@@ -118,7 +167,7 @@ struct OpDev {
 	long long m;      // rows of one layer
 	long long n;      // columns of one layer
 	// dense
-	const float *A;
+	const real *A;
 	int mrhs;              // layers on the tcgen05 3xTF32 path (mrhs.cu) instead of the gemv kernels
 	int dense_kchunks;     // row chunks of the transposed product
 	int fused_rpc;         // rows per CTA per band of the one-pass normal product (0: not used)
@@ -126,9 +175,9 @@ struct OpDev {
 	long long dense_part;  // offset of this instance in the dense partial buffer (floats)
 	// compressed gather operators: forward rows (CSR) and transpose (CSC)
 	const int *rptr, *rind;
-	const float *rval;      // NULL = implicit unit weights
+	const real *rval;       // NULL = implicit unit weights
 	const int *cptr, *cind;
-	const float *cval;      // NULL = implicit unit weights
+	const real *cval;       // NULL = implicit unit weights
 	float scale;            // multiplies every implicit weight
 	// rays: packed (x0, y0, z0, dx, dy, dz, out) per traced ray (ops.cuh pack_ray)
 	int nrays;
@@ -157,7 +206,7 @@ struct OpDev {
 	const int *torder;
 	// 2D forward: y-driven rays read a transposed copy of the image (rows of
 	// length tH = n / ld), in which their steps are contiguous; NULL = off
-	float *xT;
+	real *xT;
 	int tH;
 	// launch shapes chosen by the autotuner (tune.cu); 0 = the built-in
 	// choice: lanes per ray of the ray forward (4, 8 or 16), and 1 + the
@@ -205,11 +254,11 @@ struct Inst {
 	int dims, p, q, r;           // image: dim_y, dim_x, dim_z (r = 1 in 2D)
 	FastDiv fq, fp;              // division by q and by p
 	long long n, m;              // vector lengths (n and m include layers)
-	float *vn[NVN];
-	float *vm[NVM];
-	const float *b_user;         // caller's b (device)
-	const float *ut_user;        // caller's Ut (device) or NULL
-	float *u_user;               // caller's U (device)
+	real *vn[NVN];
+	real *vm[NVM];
+	const real *b_user;          // caller's b (device)
+	const real *ut_user;         // caller's Ut (device) or NULL
+	real *u_user;                // caller's U (device)
 	Ctrl *ctrl;
 	double *trace;               // maxit records of 5 doubles, or NULL
 	double *part;                // this instance's partial sums
@@ -407,4 +456,4 @@ void op_forward(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel
                 bool xT_ready = false);
 void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y, bool unfused = false);
 
-}  // namespace tval3g
+TG_END

@@ -1,14 +1,14 @@
 // Fused TVAL3 iteration kernels; see kernels.cuh.
 //
 // Every kernel copies its instance descriptor into registers (a by-value
-// Inst: stores to the float vectors cannot alias it, so its pointers are
+// Inst: stores to the vectors cannot alias it, so its pointers are
 // loaded once), indexes with 32-bit integers (image and measurement lengths
 // are below 2^31) and computes image coordinates with multiply-high division.
 #include <math.h>
 
 #include "kernels.cuh"
 
-namespace tval3g {
+TG_BEGIN
 
 // ---------------------------------------------------------------------------
 // prologue / image geometry
@@ -54,8 +54,12 @@ __device__ __forceinline__ void set_conds(const CondSet &cs, const Ctrl &c) {
 // tell that two vectors do not alias, so a load that follows a store in
 // program order would wait for the store's data.
 #define LOAD_TILE_M(i0, len, reg, expr)              \
-	float reg[EPT_M];                                \
+	real reg[EPT_M];                                \
 	FOR_TILE_M(i0, len, i) reg[k_] = (expr);
+
+// resident blocks per SM asked of the register allocator: the FP64 build's
+// elements take twice the registers, so it asks for half as many blocks
+#define MINB(x) (FP64_BUILD ? ((x) + 1) / 2 : (x))
 
 struct Geo {
 	int dims, p, q, r, S, n;
@@ -73,22 +77,22 @@ struct Geo {
 };
 
 // periodic forward differences at i (2d:268-278, 3d:365-389)
-__device__ __forceinline__ float dxf(const float *__restrict__ U, const Geo &g, int i, int x) {
+__device__ __forceinline__ real dxf(const real *__restrict__ U, const Geo &g, int i, int x) {
 	return (x < g.q - 1) ? U[i + 1] - U[i] : U[i - (g.q - 1)] - U[i];
 }
-__device__ __forceinline__ float dyf(const float *__restrict__ U, const Geo &g, int i, int y) {
+__device__ __forceinline__ real dyf(const real *__restrict__ U, const Geo &g, int i, int y) {
 	return (y < g.p - 1) ? U[i + g.q] - U[i] : U[i - (g.p - 1) * g.q] - U[i];
 }
-__device__ __forceinline__ float dzf(const float *__restrict__ U, const Geo &g, int i, int z) {
+__device__ __forceinline__ real dzf(const real *__restrict__ U, const Geo &g, int i, int z) {
 	return (z < g.r - 1) ? U[i + g.S] - U[i] : U[i - (g.r - 1) * g.S] - U[i];
 }
 
-// Dt at i with component accessors vx(j), vy(j), vz(j); the float additions
+// Dt at i with component accessors vx(j), vy(j), vz(j); the additions (in the element type)
 // are made in the reference's order (2d:280-293, 3d:394-425), including the
 // 3D y term the reference adds on the first row of slices z >= 1.
 template <class FX, class FY, class FZ>
-__device__ __forceinline__ float dt_at(const Geo &g, int i, int x, int y, int z, FX vx, FY vy, FZ vz) {
-	float res = (x > 0) ? vx(i - 1) - vx(i) : vx(i + g.q - 1) - vx(i);
+__device__ __forceinline__ real dt_at(const Geo &g, int i, int x, int y, int z, FX vx, FY vy, FZ vz) {
+	real res = (x > 0) ? vx(i - 1) - vx(i) : vx(i + g.q - 1) - vx(i);
 	if (g.dims == 2) {
 		if (y > 0) { res = res + vy(i - g.q); res = res + (-vy(i)); }
 		else { res = res + vy(i + (g.p - 1) * g.q); res = res + (-vy(i)); }
@@ -108,27 +112,27 @@ __device__ __forceinline__ float dt_at(const Geo &g, int i, int x, int y, int z,
 // division whenever beta is a power of two (beta0 = 2^k and rate_cnt = 2
 // keep it one), within one rounding otherwise.
 struct Shrink {
-	float rbeta, thr;
+	real rbeta, thr;
 	int iso, dims;
 	__device__ Shrink(const Inst &I, double beta_d)
-		: rbeta((float)(1.0 / beta_d)), thr((float)(1.0 / beta_d)), iso(I.tv_norm), dims(I.dims) {}
-	__device__ __forceinline__ float apply(const float (&u)[3], const float (&s)[3], float (&w)[3]) const {
-		float ub[3];
+		: rbeta((real)(1.0 / beta_d)), thr((real)(1.0 / beta_d)), iso(I.tv_norm), dims(I.dims) {}
+	__device__ __forceinline__ real apply(const real (&u)[3], const real (&s)[3], real (&w)[3]) const {
+		real ub[3];
 #pragma unroll
 		for (int c = 0; c < 3; c++) ub[c] = (c < dims) ? u[c] - s[c] * rbeta : 0.f;
 		if (iso) {
-			float nrm = sqrtf(ub[0] * ub[0] + ub[1] * ub[1] + ub[2] * ub[2]);
-			float t = nrm - thr;
+			real nrm = tsqrt(ub[0] * ub[0] + ub[1] * ub[1] + ub[2] * ub[2]);
+			real t = nrm - thr;
 			t = t >= 0.f ? t : 0.f;
-			const float sc = nrm > 0.f ? t / nrm : 0.f;
+			const real sc = nrm > 0.f ? t / nrm : 0.f;
 #pragma unroll
 			for (int c = 0; c < 3; c++) w[c] = sc * ub[c];
 			return t;
 		}
-		float lam = 0.f;
+		real lam = 0.f;
 #pragma unroll
 		for (int c = 0; c < 3; c++) {
-			float t = fabsf(ub[c]) - thr;
+			real t = tfabs(ub[c]) - thr;
 			t = t >= 0.f ? t : 0.f;
 			if (c < dims) lam += t;
 			w[c] = ub[c] >= 0.f ? t : -t;
@@ -137,9 +141,9 @@ struct Shrink {
 	}
 	// one component of the anisotropic shrinkage (apply's per-component
 	// arithmetic): W_c depends on U_c and sigma_c alone
-	__device__ __forceinline__ float apply1(float u, float s) const {
-		const float ub = u - s * rbeta;
-		float t = fabsf(ub) - thr;
+	__device__ __forceinline__ real apply1(real u, real s) const {
+		const real ub = u - s * rbeta;
+		real t = tfabs(ub) - thr;
 		t = t >= 0.f ? t : 0.f;
 		return ub >= 0.f ? t : -t;
 	}
@@ -148,33 +152,33 @@ struct Shrink {
 	// by its modulus, W = max(|Ubar| - 1/beta, 0) Ubar / |Ubar| (2d:614-649);
 	// isotropic: by the modulus over all components.  Returns this plane's
 	// share of lambda1 (the real plane carries it, the imaginary plane 0).
-	__device__ __forceinline__ float apply_c(const float (&u)[3], const float (&s)[3], const float (&up)[3],
-	                                         const float (&sp)[3], bool imag, float (&w)[3]) const {
-		float re[3], im[3];
+	__device__ __forceinline__ real apply_c(const real (&u)[3], const real (&s)[3], const real (&up)[3],
+	                                         const real (&sp)[3], bool imag, real (&w)[3]) const {
+		real re[3], im[3];
 #pragma unroll
 		for (int c = 0; c < 3; c++) {
-			const float a = (c < dims) ? u[c] - s[c] * rbeta : 0.f;
-			const float b = (c < dims) ? up[c] - sp[c] * rbeta : 0.f;
+			const real a = (c < dims) ? u[c] - s[c] * rbeta : 0.f;
+			const real b = (c < dims) ? up[c] - sp[c] * rbeta : 0.f;
 			re[c] = imag ? b : a;
 			im[c] = imag ? a : b;
 		}
 		if (iso) {
-			float nrm2 = 0.f;
+			real nrm2 = 0.f;
 #pragma unroll
 			for (int c = 0; c < 3; c++) nrm2 += re[c] * re[c] + im[c] * im[c];
-			const float nrm = sqrtf(nrm2);
-			float t = nrm - thr;
+			const real nrm = tsqrt(nrm2);
+			real t = nrm - thr;
 			t = t >= 0.f ? t : 0.f;
-			const float sc = nrm > 0.f ? t / nrm : 0.f;
+			const real sc = nrm > 0.f ? t / nrm : 0.f;
 #pragma unroll
 			for (int c = 0; c < 3; c++) w[c] = sc * (imag ? im[c] : re[c]);
 			return imag ? 0.f : t;
 		}
-		float lam = 0.f;
+		real lam = 0.f;
 #pragma unroll
 		for (int c = 0; c < 3; c++) {
-			const float ab = sqrtf(re[c] * re[c] + im[c] * im[c]);
-			float t = ab - thr;
+			const real ab = tsqrt(re[c] * re[c] + im[c] * im[c]);
+			real t = ab - thr;
 			t = t >= 0.f ? t : 0.f;
 			if (c < dims) lam += t;
 			// the reference's 3D complex shrinkage scales the z component's
@@ -190,9 +194,9 @@ struct Shrink {
 // shrinkage at image element j: loads its gradient components u and
 // multipliers s (and, for complex data, the other plane's) and returns the
 // lambda1 share
-__device__ __forceinline__ float shrink_at(const Inst &I, const Shrink &sh, int j, const float *const (&Uc)[3],
-                                           const float *const (&Sc)[3], float (&u)[3], float (&s)[3],
-                                           float (&w)[3]) {
+__device__ __forceinline__ real shrink_at(const Inst &I, const Shrink &sh, int j, const real *const (&Uc)[3],
+                                           const real *const (&Sc)[3], real (&u)[3], real (&s)[3],
+                                           real (&w)[3]) {
 	const int dims = I.dims;
 #pragma unroll
 	for (int c = 0; c < 3; c++) {
@@ -203,7 +207,7 @@ __device__ __forceinline__ float shrink_at(const Inst &I, const Shrink &sh, int 
 	const int h = (int)(I.n >> 1);
 	const bool imag = j >= h;
 	const int jp = imag ? j - h : j + h;
-	float up[3], sp[3];
+	real up[3], sp[3];
 #pragma unroll
 	for (int c = 0; c < 3; c++) {
 		up[c] = c < dims ? Uc[c][jp] : 0.f;
@@ -217,10 +221,10 @@ __device__ __forceinline__ bool bad(double v) { return !isfinite(v); }
 // ---------------------------------------------------------------------------
 // scaleb (2d:229-266): first min |b| and first max |b|, scale into [0.5, 1.5]
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void better_min(float &a, int &ia, float b, int ib) {
+__device__ __forceinline__ void better_min(real &a, int &ia, real b, int ib) {
 	if (b < a || (b == a && ib < ia)) { a = b; ia = ib; }
 }
-__device__ __forceinline__ void better_max(float &a, int &ia, float b, int ib) {
+__device__ __forceinline__ void better_max(real &a, int &ia, real b, int ib) {
 	if (b > a || (b == a && ib < ia)) { a = b; ia = ib; }
 }
 
@@ -229,22 +233,22 @@ __global__ void __launch_bounds__(BLOCK) k_scaleb(KArgs a) {
 	KPROLOGUE(a);
 	// complex data: over the m / 2 complex entries, |b| their modulus
 	const int m = I.cplx ? (int)(I.m >> 1) : (int)I.m, i0 = local * TILE_M;
-	float mn = INFINITY, mx = -INFINITY;
+	real mn = INFINITY, mx = -INFINITY;
 	int imn = INT_MAX, imx = INT_MAX;
 	FOR_TILE_M(i0, m, i) {
-		float v = I.cplx ? hypotf(I.b_user[2 * i], I.b_user[2 * i + 1]) : fabsf(I.b_user[i]);
+		real v = I.cplx ? thypot(I.b_user[2 * i], I.b_user[2 * i + 1]) : tfabs(I.b_user[i]);
 		better_min(mn, imn, v, i);
 		better_max(mx, imx, v, i);
 	}
 	for (int o = 16; o > 0; o >>= 1) {
-		float v = __shfl_xor_sync(0xffffffffu, mn, o);
+		real v = __shfl_xor_sync(0xffffffffu, mn, o);
 		int iv = __shfl_xor_sync(0xffffffffu, imn, o);
 		better_min(mn, imn, v, iv);
 		v = __shfl_xor_sync(0xffffffffu, mx, o);
 		iv = __shfl_xor_sync(0xffffffffu, imx, o);
 		better_max(mx, imx, v, iv);
 	}
-	__shared__ float smn[32], smx[32];
+	__shared__ real smn[32], smx[32];
 	__shared__ int simn[32], simx[32];
 	__shared__ int last;
 	int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -264,18 +268,18 @@ __global__ void __launch_bounds__(BLOCK) k_scaleb(KArgs a) {
 	__syncthreads();
 	if (!last || threadIdx.x != 0) return;
 	__threadfence();
-	float gmn = INFINITY, gmx = -INFINITY;
+	real gmn = INFINITY, gmx = -INFINITY;
 	int gimn = INT_MAX, gimx = INT_MAX;
 	for (int t = 0; t < I.ntm; t++) {   // tiles in index order: first occurrence wins
 		const double *P = I.part + (long long)t * NSUM;
-		better_min(gmn, gimn, (float)__ldcg(P + 0), (int)__ldcg(P + 1));
-		better_max(gmx, gimx, (float)__ldcg(P + 2), (int)__ldcg(P + 3));
+		better_min(gmn, gimn, (real)__ldcg(P + 0), (int)__ldcg(P + 1));
+		better_max(gmx, gimx, (real)__ldcg(P + 2), (int)__ldcg(P + 3));
 	}
 	Ctrl &c = *I.ctrl;
 	double scl = 1.0;
 	if (gimn < m && gimx < m) {   // (all-NaN data leaves no index: no scaling)
-		// |bmax - bmin|; complex: the modulus of the float difference
-		double dif = I.cplx ? (double)hypotf(I.b_user[2 * gimx] - I.b_user[2 * gimn],
+		// |bmax - bmin|; complex: the modulus of the difference (element type)
+		double dif = I.cplx ? (double)thypot(I.b_user[2 * gimx] - I.b_user[2 * gimn],
 		                                     I.b_user[2 * gimx + 1] - I.b_user[2 * gimn + 1])
 		                    : fabs((double)I.b_user[gimx] - (double)I.b_user[gimn]);
 		if (dif < 0.5) scl = 0.5 / dif;
@@ -313,11 +317,11 @@ __global__ void __launch_bounds__(BLOCK) k_init(KArgs a) {
 			c.need_mlp = c.need_Ad = c.skip_adj = 0; c.status = 0;
 		}
 	} else {
-		const float scl = (float)c.scl;
+		const real scl = (real)c.scl;
 		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) {
 #pragma unroll
 			for (int v = 0; v < NVM; v++) I.vm[v][i] = 0.f;
-			const float bu = I.b_user[cplx_index(I, i, I.m)];
+			const real bu = I.b_user[cplx_index(I, i, I.m)];
 			I.vm[vB][i] = scl != 1.f ? bu * scl : bu;
 		}
 	}
@@ -328,7 +332,7 @@ template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_init_u(KArgs a) {
 	KPROLOGUE(a);
 	FOR_TILE(local, (int)I.n, i) {
-		float u = I.vn[vAtb][i];
+		real u = I.vn[vAtb][i];
 		I.vn[vU][i] = u;
 		I.vn[vRcd][i] = u;
 	}
@@ -339,8 +343,8 @@ template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_D(KArgs a) {
 	KPROLOGUE(a);
 	Geo g(I);
-	const float *__restrict__ U = I.vn[vU];
-	float *__restrict__ ux = I.vn[vUx], *__restrict__ uy = I.vn[vUy], *__restrict__ uz = I.vn[vUz];
+	const real *__restrict__ U = I.vn[vU];
+	real *__restrict__ ux = I.vn[vUx], *__restrict__ uy = I.vn[vUy], *__restrict__ uz = I.vn[vUz];
 	FOR_TILE(local, g.n, i) {
 		int x, y, z;
 		g.coords(i, x, y, z);
@@ -361,17 +365,17 @@ __global__ void __launch_bounds__(BLOCK) k_shrink(KArgs a) {
 	Ctrl &c = *I.ctrl;
 	Shrink sh(I, c.beta);
 	const int n = (int)I.n, dims = I.dims;
-	const float *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
-	const float *const Sc[3] = {I.vn[vSx], I.vn[vSy], I.vn[vSz]};
+	const real *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
+	const real *const Sc[3] = {I.vn[vSx], I.vn[vSy], I.vn[vSz]};
 	double v[3] = {0, 0, 0};   // lam1, lam2, lam4
 	FOR_TILE(local, n, i) {
-		float u[3], s[3], w[3];
+		real u[3], s[3], w[3];
 		v[0] += shrink_at(I, sh, i, Uc, Sc, u, s, w);
 #pragma unroll
 		for (int cc = 0; cc < 3; cc++)
 			if (cc < dims) {
 				I.vn[vWx + cc][i] = w[cc];
-				float vv = u[cc] - w[cc];
+				real vv = u[cc] - w[cc];
 				v[1] += (double)vv * vv;
 				v[2] += (double)s[cc] * vv;
 			}
@@ -384,16 +388,16 @@ __global__ void __launch_bounds__(BLOCK) k_shrink(KArgs a) {
 }
 
 // component cc of D U at j, from U (2d:268-278, 3d:365-389)
-__device__ __forceinline__ float du_at(const float *__restrict__ U, const Geo &g, int j, int cc) {
+__device__ __forceinline__ real du_at(const real *__restrict__ U, const Geo &g, int j, int cc) {
 	int x, y, z;
 	g.coords(j, x, y, z);
 	return cc == 0 ? dxf(U, g, j, x) : cc == 1 ? dyf(U, g, j, y) : dzf(U, g, j, z);
 }
 
 // g2 at i: Dt(DU - W) with D U formed from U here (2d:280-293)
-__device__ __forceinline__ float g2_at_u(const Inst &I, const Geo &g, int i, int x, int y, int z) {
-	const float *__restrict__ U = I.vn[vU];
-	const float *const Wc[3] = {I.vn[vWx], I.vn[vWy], I.vn[vWz]};
+__device__ __forceinline__ real g2_at_u(const Inst &I, const Geo &g, int i, int x, int y, int z) {
+	const real *__restrict__ U = I.vn[vU];
+	const real *const Wc[3] = {I.vn[vWx], I.vn[vWy], I.vn[vWz]};
 	auto V = [&](int cc) { return [&, cc](int j) { return du_at(U, g, j, cc) - Wc[cc][j]; }; };
 	return dt_at(g, i, x, y, z, V(0), V(1), V(2));
 }
@@ -405,29 +409,29 @@ __device__ __forceinline__ float g2_at_u(const Inst &I, const Geo &g, int i, int
 // (the end of descend, 2d:481-493) are formed here and stored.
 // ---------------------------------------------------------------------------
 template <bool MULTI>
-__global__ void __launch_bounds__(BLOCK, MULTI ? 6 : 1) k_getg(KArgs a) {
+__global__ void __launch_bounds__(BLOCK, MULTI ? MINB(6) : 1) k_getg(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	double v[4] = {0, 0, 0, 0};   // lam2, lam4, lam3, lam5
 	if (local < I.ntn) {
 		Geo g(I);
-		const float *__restrict__ U = I.vn[vU];
-		float *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
-		const float *const Wc[3] = {I.vn[vWx], I.vn[vWy], I.vn[vWz]};
-		const float *const Sc[3] = {I.vn[vSx], I.vn[vSy], I.vn[vSz]};
-		float *__restrict__ gv = I.vn[vG];
-		float *__restrict__ g2 = I.vn[vG2];
-		const float *__restrict__ atb = I.vn[vAtb];
+		const real *__restrict__ U = I.vn[vU];
+		real *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
+		const real *const Wc[3] = {I.vn[vWx], I.vn[vWy], I.vn[vWz]};
+		const real *const Sc[3] = {I.vn[vSx], I.vn[vSy], I.vn[vSz]};
+		real *__restrict__ gv = I.vn[vG];
+		real *__restrict__ g2 = I.vn[vG2];
+		const real *__restrict__ atb = I.vn[vAtb];
 		FOR_TILE(local, g.n, i) {
 			int x, y, z;
 			g.coords(i, x, y, z);
 			// every load before the first store (the vectors do not alias)
-			const float gi = gv[i] - atb[i];
+			const real gi = gv[i] - atb[i];
 			// in the inner loop k_shrink_grad forms g2 again from the new W
 			// before anything reads it, so only the initialisation needs it
-			const float g2i = a.stage == ST_INIT ? g2_at_u(I, g, i, x, y, z) : 0.f;
-			float du[3] = {dxf(U, g, i, x), dyf(U, g, i, y), g.dims == 3 ? dzf(U, g, i, z) : 0.f};
-			float wc[3], sc[3];
+			const real g2i = a.stage == ST_INIT ? g2_at_u(I, g, i, x, y, z) : 0.f;
+			real du[3] = {dxf(U, g, i, x), dyf(U, g, i, y), g.dims == 3 ? dzf(U, g, i, z) : 0.f};
+			real wc[3], sc[3];
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++) {
 				wc[cc] = cc < g.dims ? Wc[cc][i] : 0.f;
@@ -439,15 +443,15 @@ __global__ void __launch_bounds__(BLOCK, MULTI ? 6 : 1) k_getg(KArgs a) {
 			for (int cc = 0; cc < 3; cc++)
 				if (cc < g.dims) {
 					Uc[cc][i] = du[cc];
-					float vv = du[cc] - wc[cc];
+					real vv = du[cc] - wc[cc];
 					v[0] += (double)vv * vv;
 					v[1] += (double)sc[cc] * vv;
 				}
 		}
 	} else {
-		const float *__restrict__ au = I.vm[vAu], *__restrict__ bb = I.vm[vB], *__restrict__ dl = I.vm[vDelta];
+		const real *__restrict__ au = I.vm[vAu], *__restrict__ bb = I.vm[vB], *__restrict__ dl = I.vm[vDelta];
 		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) {
-			float r = au[i] - bb[i];
+			real r = au[i] - bb[i];
 			v[2] += (double)r * r;
 			v[3] += (double)dl[i] * r;
 		}
@@ -484,18 +488,18 @@ template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
-	const float mdb = (float)c.muDbeta;
-	const float bscale = a.stage == ST_OUTER ? (float)(c.beta0 / c.beta) : 1.f;
-	float *__restrict__ dts = I.vn[vDts], *__restrict__ d = I.vn[vD];
-	const float *__restrict__ g2 = I.vn[vG2], *__restrict__ gv = I.vn[vG];
+	const real mdb = (real)c.muDbeta;
+	const real bscale = a.stage == ST_OUTER ? (real)(c.beta0 / c.beta) : 1.f;
+	real *__restrict__ dts = I.vn[vDts], *__restrict__ d = I.vn[vD];
+	const real *__restrict__ g2 = I.vn[vG2], *__restrict__ gv = I.vn[vG];
 	double v[1] = {0};   // |d|^2
 	FOR_TILE(local, (int)I.n, i) {
 		// every load before the first store
-		float t = a.stage == ST_OUTER ? d[i] * bscale : dts[i];
-		const float g2i = g2[i], gvi = gv[i];
+		real t = a.stage == ST_OUTER ? d[i] * bscale : dts[i];
+		const real g2i = g2[i], gvi = gv[i];
 		if (a.stage == ST_OUTER) dts[i] = t;
-		float dv = t + g2i;
-		dv = fmaf(mdb, gvi, dv);
+		real dv = t + g2i;
+		dv = tfma(mdb, gvi, dv);
 		d[i] = dv;
 		v[0] += (double)dv * dv;
 	}
@@ -526,38 +530,38 @@ __global__ void __launch_bounds__(BLOCK) k_grad(KArgs a) {
 // trace, time-to-solution target).
 // ---------------------------------------------------------------------------
 template <bool MULTI>
-__global__ void __launch_bounds__(BLOCK, MULTI ? 4 : 3) k_shrink_grad(KArgs a) {
+__global__ void __launch_bounds__(BLOCK, MULTI ? MINB(4) : MINB(3)) k_shrink_grad(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	Geo g(I);
 	Shrink sh(I, c.beta);
 	const int dims = I.dims;
-	const float *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
-	const float *const Sc[3] = {I.vn[vSx], I.vn[vSy], I.vn[vSz]};
-	const float mdb = (float)c.muDbeta;
-	float *__restrict__ d = I.vn[vD], *__restrict__ uup = I.vn[vUUP];
-	const float *__restrict__ dts = I.vn[vDts], *__restrict__ gv = I.vn[vG];
-	const float *__restrict__ U = I.vn[vU], *__restrict__ Up = I.vn[vUp];
+	const real *const Uc[3] = {I.vn[vUx], I.vn[vUy], I.vn[vUz]};
+	const real *const Sc[3] = {I.vn[vSx], I.vn[vSy], I.vn[vSz]};
+	const real mdb = (real)c.muDbeta;
+	real *__restrict__ d = I.vn[vD], *__restrict__ uup = I.vn[vUUP];
+	const real *__restrict__ dts = I.vn[vDts], *__restrict__ gv = I.vn[vG];
+	const real *__restrict__ U = I.vn[vU], *__restrict__ Up = I.vn[vUp];
 	// distance to Ut after the iteration (trace / time-to-solution target)
 	const bool ut = I.ut_user && (I.trace || I.target > 0);
-	const float rscl = (float)(1.0 / c.scl);
+	const real rscl = (real)(1.0 / c.scl);
 	// the next iteration's Barzilai-Borwein step (get_tau, 2d:444-451) from
 	// this iteration's uup, g - gp, g2 - g2p (schedule mode: k_tau_prep, as
 	// mu and beta change before that step)
 	// (complex data: k_tau_bb_cplx, which needs the other plane's g2)
 	const bool bb = !I.sched && !I.cplx;
-	const float *__restrict__ gp = I.vn[vGp], *__restrict__ g2p = I.vn[vG2p];
+	const real *__restrict__ gp = I.vn[vGp], *__restrict__ g2p = I.vn[vG2p];
 	// lam1, lam2, lam4, |d|^2, |Up|^2, |uup|^2, |U/scl - Ut|^2, |Ut|^2, <uup, dg2 + muDbeta dg>
 	double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 	FOR_TILE(local, g.n, i) {
 		int x, y, z;
 		g.coords(i, x, y, z);
-		float u[3], s[3], w[3];
+		real u[3], s[3], w[3];
 		v[0] += shrink_at(I, sh, i, Uc, Sc, u, s, w);
 #pragma unroll
 		for (int cc = 0; cc < 3; cc++)
 			if (cc < dims) {
-				const float vv = u[cc] - w[cc];
+				const real vv = u[cc] - w[cc];
 				v[1] += (double)vv * vv;
 				v[2] += (double)s[cc] * vv;
 			}
@@ -565,41 +569,41 @@ __global__ void __launch_bounds__(BLOCK, MULTI ? 4 : 3) k_shrink_grad(KArgs a) {
 		// (anisotropic real data: only component cc of U and sigma at j)
 		const bool one = !sh.iso && !I.cplx;
 		auto V = [&](int cc) {
-			return [&, cc](int j) -> float {
+			return [&, cc](int j) -> real {
 				if (j == i) return u[cc] - w[cc];
 				if (one) {
-					const float uj = Uc[cc][j];
+					const real uj = Uc[cc][j];
 					return uj - sh.apply1(uj, Sc[cc][j]);
 				}
-				float uj[3], sj[3], wj[3];
+				real uj[3], sj[3], wj[3];
 				shrink_at(I, sh, j, Uc, Sc, uj, sj, wj);
 				return uj[cc] - wj[cc];
 			};
 		};
 		// every load before the first store (the vectors do not alias: a load
 		// the compiler kept behind a store would wait for the store's data)
-		const float g2i = dt_at(g, i, x, y, z, V(0), V(1), V(2));
-		const float dtsi = dts[i], gvi = gv[i], up = Up[i], Ui = U[i];
-		const float gpi = bb ? gp[i] : 0.f, g2pi = bb ? g2p[i] : 0.f;
-		const float uti = ut ? I.ut_user[cplx_index(I, i, I.n)] : 0.f;
+		const real g2i = dt_at(g, i, x, y, z, V(0), V(1), V(2));
+		const real dtsi = dts[i], gvi = gv[i], up = Up[i], Ui = U[i];
+		const real gpi = bb ? gp[i] : 0.f, g2pi = bb ? g2p[i] : 0.f;
+		const real uti = ut ? I.ut_user[cplx_index(I, i, I.n)] : 0.f;
 #pragma unroll
 		for (int cc = 0; cc < 3; cc++)
 			if (cc < dims) I.vn[vWx + cc][i] = w[cc];
 		I.vn[vG2][i] = g2i;
-		float dv = dtsi + g2i;
-		dv = fmaf(mdb, gvi, dv);
+		real dv = dtsi + g2i;
+		dv = tfma(mdb, gvi, dv);
 		d[i] = dv;
 		v[3] += (double)dv * dv;
-		const float uu = Ui - up;
+		const real uu = Ui - up;
 		uup[i] = uu;
 		v[4] += (double)up * up;
 		v[5] += (double)uu * uu;
 		if (bb) {
-			const float tmp = fmaf(mdb, gvi - gpi, g2i - g2pi);
+			const real tmp = tfma(mdb, gvi - gpi, g2i - g2pi);
 			v[8] += (double)uu * tmp;
 		}
 		if (ut) {
-			const float e = Ui * rscl - uti;
+			const real e = Ui * rscl - uti;
 			v[6] += (double)e * e;
 			v[7] += (double)uti * uti;
 		}
@@ -657,15 +661,15 @@ __global__ void __launch_bounds__(BLOCK) k_tau_bb_cplx(KArgs a) {
 	KPROLOGUE(a);
 	if (!I.cplx) return;
 	Ctrl &c = *I.ctrl;
-	const float mdb = (float)c.muDbeta;
+	const real mdb = (real)c.muDbeta;
 	const int h = (int)(I.n >> 1);
-	const float *__restrict__ gv = I.vn[vG], *__restrict__ gp = I.vn[vGp];
-	const float *__restrict__ g2 = I.vn[vG2], *__restrict__ g2p = I.vn[vG2p], *__restrict__ uup = I.vn[vUUP];
+	const real *__restrict__ gv = I.vn[vG], *__restrict__ gp = I.vn[vGp];
+	const real *__restrict__ g2 = I.vn[vG2], *__restrict__ g2p = I.vn[vG2p], *__restrict__ uup = I.vn[vUUP];
 	double v[3] = {0, 0, 0};   // ss, Re sy, Im sy
 	FOR_TILE(local, h, i) {
-		const float ur = uup[i], ui = uup[i + h];
-		const float tr = fmaf(mdb, gv[i] - gp[i], g2[i] - g2p[i]);
-		const float ti = fmaf(mdb, gv[i + h] - gp[i + h], g2[i + h] - g2p[i + h]);
+		const real ur = uup[i], ui = uup[i + h];
+		const real tr = tfma(mdb, gv[i] - gp[i], g2[i] - g2p[i]);
+		const real ti = tfma(mdb, gv[i + h] - gp[i + h], g2[i + h] - g2p[i + h]);
 		v[0] += (double)ur * ur + (double)ui * ui;
 		v[1] += (double)ur * tr + (double)ui * ti;
 		v[2] += (double)ur * ti - (double)ui * tr;
@@ -688,33 +692,33 @@ __global__ void __launch_bounds__(BLOCK) k_tau_prep(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	const bool first = c.restart || c.fst;
-	const float mdb = (float)c.muDbeta;
+	const real mdb = (real)c.muDbeta;
 	Geo g(I);
 	double v[3] = {0, 0, 0};
-	const float *__restrict__ d = I.vn[vD];
+	const real *__restrict__ d = I.vn[vD];
 	if (first) {
 		FOR_TILE(local, g.n, i) {
 			int x, y, z;
 			g.coords(i, x, y, z);
-			float t = dxf(d, g, i, x);
+			real t = dxf(d, g, i, x);
 			v[0] += (double)t * t;
 			t = dyf(d, g, i, y);
 			v[0] += (double)t * t;
 			if (g.dims == 3) { t = dzf(d, g, i, z); v[0] += (double)t * t; }
 		}
 	} else {
-		const float *__restrict__ gv = I.vn[vG], *__restrict__ gp = I.vn[vGp];
-		const float *__restrict__ g2 = I.vn[vG2], *__restrict__ g2p = I.vn[vG2p], *__restrict__ uup = I.vn[vUUP];
+		const real *__restrict__ gv = I.vn[vG], *__restrict__ gp = I.vn[vGp];
+		const real *__restrict__ g2 = I.vn[vG2], *__restrict__ g2p = I.vn[vG2p], *__restrict__ uup = I.vn[vUUP];
 		FOR_TILE(local, g.n, i) {
-			float dg = gv[i] - gp[i];
-			float dg2 = g2[i] - g2p[i];
-			float uu = uup[i];
-			float tmp = fmaf(mdb, dg, dg2);
+			real dg = gv[i] - gp[i];
+			real dg2 = g2[i] - g2p[i];
+			real uu = uup[i];
+			real tmp = tfma(mdb, dg, dg2);
 			v[0] += (double)uu * uu;
 			v[1] += (double)uu * tmp;
 			if (I.cplx && i < g.n / 2) {   // Im sy (complex data, as k_tau_bb_cplx)
 				const int j = i + g.n / 2;
-				const float tj = fmaf(mdb, gv[j] - gp[j], g2[j] - g2p[j]);
+				const real tj = tfma(mdb, gv[j] - gp[j], g2[j] - g2p[j]);
 				v[2] += (double)uu * tj - (double)uup[j] * tmp;
 			}
 		}
@@ -738,9 +742,9 @@ __global__ void __launch_bounds__(BLOCK) k_tau_first(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	double v[1] = {0};
-	const float *__restrict__ ad = I.vm[vAd];
+	const real *__restrict__ ad = I.vm[vAd];
 	FOR_TILE_M(local * TILE_M, (int)I.m, i) {
-		float t = ad[i];
+		real t = ad[i];
 		v[0] += (double)t * t;
 	}
 	double tot[1];
@@ -761,30 +765,30 @@ __global__ void __launch_bounds__(BLOCK) k_tau_first(KArgs a) {
 // then nonneg (2d:455-465)
 // ---------------------------------------------------------------------------
 template <bool MULTI>
-__global__ void __launch_bounds__(BLOCK, MULTI ? 6 : 1) k_descend(KArgs a) {
+__global__ void __launch_bounds__(BLOCK, MULTI ? MINB(6) : 1) k_descend(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
-	const float ntau = (float)(-1 * c.tau);
+	const real ntau = (real)(-1 * c.tau);
 	const bool snap = a.stage == ST_DESCEND;
-	const float sratio = (float)c.sched_ratio;
+	const real sratio = (real)c.sched_ratio;
 	if (local < I.ntn) {
-		float *__restrict__ U = I.vn[vU], *__restrict__ Up = I.vn[vUp];
-		const float *__restrict__ d = I.vn[vD];
-		float *__restrict__ xT = I.op.xT;   // 2D ray operators: the new U transposed for the forward
+		real *__restrict__ U = I.vn[vU], *__restrict__ Up = I.vn[vUp];
+		const real *__restrict__ d = I.vn[vD];
+		real *__restrict__ xT = I.op.xT;   // 2D ray operators: the new U transposed for the forward
 		const int ld = I.op.rvx, tH = I.op.tH;   // the geometry's row length (its ld)
 		FOR_TILE(local, (int)I.n, i) {
-			float u;
-			const float dv = d[i];
+			real u;
+			const real dv = d[i];
 			if (snap) {
 				// every load before the first store: the compiler cannot tell that
 				// the vectors do not alias, and a load after a store would wait
 				// for the store's data
 				u = U[i];
-				const float gi = I.vn[vG][i], g2i = I.vn[vG2][i];
-				float uc[3];
+				const real gi = I.vn[vG][i], g2i = I.vn[vG2][i];
+				real uc[3];
 #pragma unroll
 				for (int cc = 0; cc < 3; cc++) uc[cc] = cc < I.dims ? I.vn[vUx + cc][i] : 0.f;
-				const float dts = I.sched ? I.vn[vDts][i] : 0.f;
+				const real dts = I.sched ? I.vn[vDts][i] : 0.f;
 				Up[i] = u;
 				I.vn[vGp][i] = gi;
 				I.vn[vG2p][i] = g2i;
@@ -796,7 +800,7 @@ __global__ void __launch_bounds__(BLOCK, MULTI ? 6 : 1) k_descend(KArgs a) {
 			} else {
 				u = Up[i];
 			}
-			u = fmaf(ntau, dv, u);
+			u = tfma(ntau, dv, u);
 			if (I.nonneg) u = (I.cplx && i >= (int)(I.n >> 1)) ? 0.f : (u < 0.f ? 0.f : u);   // complex: Re >= 0, Im = 0 (2d:467-479)
 			U[i] = u;
 			if (xT) {
@@ -820,8 +824,8 @@ __global__ void __launch_bounds__(BLOCK, MULTI ? 6 : 1) k_descend(KArgs a) {
 //   lam3(a) = |R0 + a dAu|^2,  lam5(a) = <delta, R0> + a <delta, dAu>   (R0 = Aup - b)
 // so k_bt_search forms their coefficients once (lam4(1), lam5(1) come from
 // k_getg) and its last block runs the loop on them; k_lerp then moves the
-// vectors to the accepted alpha once, with the reference's float arithmetic
-// (fmaf(alpha, U - Up, Up)).  When all five steps fail the vectors are not
+// vectors to the accepted alpha once, with the reference's arithmetic in the element type
+// (fma(alpha, U - Up, Up)).  When all five steps fail the vectors are not
 // moved: the restart (2d:561-567) recomputes every one of them from Up.
 template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_bt_search(KArgs a) {
@@ -834,9 +838,9 @@ __global__ void __launch_bounds__(BLOCK) k_bt_search(KArgs a) {
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++)
 				if (cc < I.dims) {
-					const float up = I.vn[vUxp + cc][i];
-					const float du = I.vn[vUx + cc][i] - up;
-					const float e0 = up - I.vn[vWx + cc][i];
+					const real up = I.vn[vUxp + cc][i];
+					const real du = I.vn[vUx + cc][i] - up;
+					const real e0 = up - I.vn[vWx + cc][i];
 					v[0] += (double)e0 * e0;
 					v[1] += (double)e0 * du;
 					v[2] += (double)du * du;
@@ -845,9 +849,9 @@ __global__ void __launch_bounds__(BLOCK) k_bt_search(KArgs a) {
 		}
 	} else {
 		FOR_TILE_M((local - I.ntn) * TILE_M, (int)I.m, i) {
-			const float ap = I.vm[vAup][i];
-			const float da = I.vm[vAu][i] - ap;
-			const float r0 = ap - I.vm[vB][i];
+			const real ap = I.vm[vAup][i];
+			const real da = I.vm[vAu][i] - ap;
+			const real r0 = ap - I.vm[vB][i];
 			v[4] += (double)r0 * r0;
 			v[5] += (double)r0 * da;
 			v[6] += (double)da * da;
@@ -887,28 +891,28 @@ __global__ void __launch_bounds__(BLOCK) k_bt_search(KArgs a) {
 template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_lerp(KArgs a) {
 	KPROLOGUE(a);
-	const float al = (float)I.ctrl->alpha;
+	const real al = (real)I.ctrl->alpha;
 	if (local < I.ntn) {
 		FOR_TILE(local, (int)I.n, i) {
 			// every load before the first store
-			const float gi = I.vn[vG][i], gpi = I.vn[vGp][i], ui = I.vn[vU][i], upi = I.vn[vUp][i];
-			float uc[3], ucp[3];
+			const real gi = I.vn[vG][i], gpi = I.vn[vGp][i], ui = I.vn[vU][i], upi = I.vn[vUp][i];
+			real uc[3], ucp[3];
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++) {
 				uc[cc] = cc < I.dims ? I.vn[vUx + cc][i] : 0.f;
 				ucp[cc] = cc < I.dims ? I.vn[vUxp + cc][i] : 0.f;
 			}
-			I.vn[vG][i] = fmaf(al, gi - gpi, gpi);
-			I.vn[vU][i] = fmaf(al, ui - upi, upi);
+			I.vn[vG][i] = tfma(al, gi - gpi, gpi);
+			I.vn[vU][i] = tfma(al, ui - upi, upi);
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++)
-				if (cc < I.dims) I.vn[vUx + cc][i] = fmaf(al, uc[cc] - ucp[cc], ucp[cc]);
+				if (cc < I.dims) I.vn[vUx + cc][i] = tfma(al, uc[cc] - ucp[cc], ucp[cc]);
 		}
 	} else {
 		const int i0 = (local - I.ntn) * TILE_M;
 		LOAD_TILE_M(i0, (int)I.m, au, I.vm[vAu][i])
 		LOAD_TILE_M(i0, (int)I.m, aup, I.vm[vAup][i])
-		FOR_TILE_M(i0, (int)I.m, i) I.vm[vAu][i] = fmaf(al, au[k_] - aup[k_], aup[k_]);
+		FOR_TILE_M(i0, (int)I.m, i) I.vm[vAu][i] = tfma(al, au[k_] - aup[k_], aup[k_]);
 	}
 }
 
@@ -918,11 +922,11 @@ __global__ void __launch_bounds__(BLOCK) k_outer(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
 	double v[1] = {0};
-	float *__restrict__ rcd = I.vn[vRcd];
-	const float *__restrict__ U = I.vn[vU];
+	real *__restrict__ rcd = I.vn[vRcd];
+	const real *__restrict__ U = I.vn[vU];
 	FOR_TILE(local, (int)I.n, i) {
-		float u = U[i];
-		float dlt = u - rcd[i];
+		real u = U[i];
+		real dlt = u - rcd[i];
 		v[0] += (double)dlt * dlt;
 		rcd[i] = u;
 	}
@@ -945,11 +949,11 @@ template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_mlp(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
-	const float nbeta = (float)(-1 * c.beta), nmu = (float)(-1 * c.mu);
+	const real nbeta = (real)(-1 * c.beta), nmu = (real)(-1 * c.mu);
 	double v[2] = {0, 0};   // lam4, lam5
 	if (local < I.ntn) {
 		FOR_TILE(local, (int)I.n, i) {
-			float vv[3], sv[3];   // every load before the first store
+			real vv[3], sv[3];   // every load before the first store
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++) {
 				vv[cc] = cc < I.dims ? I.vn[vUx + cc][i] - I.vn[vWx + cc][i] : 0.f;
@@ -958,7 +962,7 @@ __global__ void __launch_bounds__(BLOCK) k_mlp(KArgs a) {
 #pragma unroll
 			for (int cc = 0; cc < 3; cc++)
 				if (cc < I.dims) {
-					float s = fmaf(nbeta, vv[cc], sv[cc]);
+					real s = tfma(nbeta, vv[cc], sv[cc]);
 					I.vn[vSx + cc][i] = s;
 					v[0] += (double)s * vv[cc];
 				}
@@ -968,7 +972,7 @@ __global__ void __launch_bounds__(BLOCK) k_mlp(KArgs a) {
 		LOAD_TILE_M(i0, (int)I.m, r, I.vm[vAu][i] - I.vm[vB][i])
 		LOAD_TILE_M(i0, (int)I.m, dl0, I.vm[vDelta][i])
 		FOR_TILE_M(i0, (int)I.m, i) {
-			const float dl = fmaf(nmu, r[k_], dl0[k_]);
+			const real dl = tfma(nmu, r[k_], dl0[k_]);
 			I.vm[vDelta][i] = dl;
 			v[1] += (double)dl * r[k_];
 		}
@@ -995,17 +999,17 @@ template <bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_final(KArgs a) {
 	KPROLOGUE(a);
 	Ctrl &c = *I.ctrl;
-	const float scl = (float)c.scl;
+	const real scl = (real)c.scl;
 	double v[2] = {0, 0};
 	FOR_TILE(local, (int)I.n, i) {
-		float u = I.vn[vU][i];
+		real u = I.vn[vU][i];
 		if (I.cplx && I.isreal && i >= (int)(I.n >> 1)) u = 0.f;   // isreal: U = real(U) before scaling
 		u = u / scl;
 		const long long ui = cplx_index(I, i, I.n);
 		I.u_user[ui] = u;
 		if (I.ut_user) {
-			float t = I.ut_user[ui];
-			float dlt = t - u;
+			real t = I.ut_user[ui];
+			real dlt = t - u;
 			v[0] += (double)dlt * dlt;
 			v[1] += (double)t * t;
 		}
@@ -1024,8 +1028,8 @@ __global__ void __launch_bounds__(BLOCK) k_skip_norms(KArgs a) {
 	Ctrl &c = *I.ctrl;
 	double v[2] = {0, 0};
 	FOR_TILE_M(local * TILE_M, (int)I.m, i) {
-		float au = I.vm[vAu][i];
-		float dl = au - I.vm[vLastAu][i];
+		real au = I.vm[vAu][i];
+		real dl = au - I.vm[vLastAu][i];
 		v[0] += (double)dl * dl;
 		v[1] += (double)au * au;
 	}
@@ -1099,7 +1103,7 @@ __device__ __forceinline__ Geo plain_geo(const PlainGeo &pg) {
 	return Geo(I);
 }
 
-__global__ void k_D_plain(PlainGeo pg, const float *U, float *Ux, float *Uy, float *Uz) {
+__global__ void k_D_plain(PlainGeo pg, const real *U, real *Ux, real *Uy, real *Uz) {
 	Geo g = plain_geo(pg);
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
 		int x, y, z;
@@ -1110,7 +1114,7 @@ __global__ void k_D_plain(PlainGeo pg, const float *U, float *Ux, float *Uy, flo
 	}
 }
 
-__global__ void k_Dt_plain(PlainGeo pg, const float *X, const float *Y, const float *Z, float *res) {
+__global__ void k_Dt_plain(PlainGeo pg, const real *X, const real *Y, const real *Z, real *res) {
 	Geo g = plain_geo(pg);
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
 		int x, y, z;
@@ -1120,18 +1124,18 @@ __global__ void k_Dt_plain(PlainGeo pg, const float *X, const float *Y, const fl
 	}
 }
 
-__global__ void k_shrink_plain(int dims, long long n, int iso, double beta, const float *Ux, const float *Uy,
-                               const float *Uz, const float *sx, const float *sy, const float *sz, float *Wx,
-                               float *Wy, float *Wz, double *lam1) {
+__global__ void k_shrink_plain(int dims, long long n, int iso, double beta, const real *Ux, const real *Uy,
+                               const real *Uz, const real *sx, const real *sy, const real *sz, real *Wx,
+                               real *Wy, real *Wz, double *lam1) {
 	Inst I{};
 	I.dims = dims; I.tv_norm = iso;
 	Shrink sh(I, beta);
 	double acc[1] = {0};
 	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
 	     i += (long long)gridDim.x * blockDim.x) {
-		float u[3] = {Ux[i], Uy[i], dims == 3 ? Uz[i] : 0.f};
-		float s[3] = {sx[i], sy[i], dims == 3 ? sz[i] : 0.f};
-		float w[3];
+		real u[3] = {Ux[i], Uy[i], dims == 3 ? Uz[i] : 0.f};
+		real s[3] = {sx[i], sy[i], dims == 3 ? sz[i] : 0.f};
+		real w[3];
 		acc[0] += sh.apply(u, s, w);
 		Wx[i] = w[0]; Wy[i] = w[1];
 		if (dims == 3) Wz[i] = w[2];
@@ -1192,26 +1196,26 @@ static PlainGeo plain(int dims, int p, int q, int r) {
 	return g;
 }
 
-void launch_D_plain(cudaStream_t s, int dims, int p, int q, int r, const float *U, float *Ux, float *Uy,
-                    float *Uz) {
+void launch_D_plain(cudaStream_t s, int dims, int p, int q, int r, const real *U, real *Ux, real *Uy,
+                    real *Uz) {
 	PlainGeo g = plain(dims, p, q, r);
 	k_D_plain<<<grid_for((long long)p * q * g.r), 256, 0, s>>>(g, U, Ux, Uy, Uz);
 	TG_CUDA(cudaGetLastError());
 }
 
-void launch_Dt_plain(cudaStream_t s, int dims, int p, int q, int r, const float *X, const float *Y,
-                     const float *Z, float *res) {
+void launch_Dt_plain(cudaStream_t s, int dims, int p, int q, int r, const real *X, const real *Y,
+                     const real *Z, real *res) {
 	PlainGeo g = plain(dims, p, q, r);
 	k_Dt_plain<<<grid_for((long long)p * q * g.r), 256, 0, s>>>(g, X, Y, Z, res);
 	TG_CUDA(cudaGetLastError());
 }
 
-void launch_shrink_plain(cudaStream_t s, int dims, long long n, int tv_norm, double beta, const float *Ux,
-                         const float *Uy, const float *Uz, const float *sx, const float *sy, const float *sz,
-                         float *Wx, float *Wy, float *Wz, double *lam1_dev) {
+void launch_shrink_plain(cudaStream_t s, int dims, long long n, int tv_norm, double beta, const real *Ux,
+                         const real *Uy, const real *Uz, const real *sx, const real *sy, const real *sz,
+                         real *Wx, real *Wy, real *Wz, double *lam1_dev) {
 	k_shrink_plain<<<grid_for(n), 256, 0, s>>>(dims, n, tv_norm, beta, Ux, Uy, Uz, sx, sy, sz, Wx, Wy, Wz,
 	                                           lam1_dev);
 	TG_CUDA(cudaGetLastError());
 }
 
-}  // namespace tval3g
+TG_END

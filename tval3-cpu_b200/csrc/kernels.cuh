@@ -7,7 +7,7 @@
 #pragma once
 #include "engine.cuh"
 
-namespace tval3g {
+TG_BEGIN
 
 enum Stage { ST_INIT = 0, ST_LOOP, ST_DESCEND, ST_RESTART, ST_OUTER };
 enum TauMode { TAU_ACTIVE = 0, TAU_RESTART };
@@ -67,12 +67,12 @@ void launch_cond(cudaStream_t s, const Inst *tab, int count, int pred, int *flag
                  unsigned long long handle, unsigned long long *launches);
 
 // standalone stencils (C ABI helpers)
-void launch_D_plain(cudaStream_t s, int dims, int p, int q, int r, const float *U, float *Ux, float *Uy,
-                    float *Uz);
-void launch_Dt_plain(cudaStream_t s, int dims, int p, int q, int r, const float *X, const float *Y,
-                     const float *Z, float *res);
-void launch_shrink_plain(cudaStream_t s, int dims, long long n, int tv_norm, double beta, const float *Ux,
-                         const float *Uy, const float *Uz, const float *sx, const float *sy,
-                         const float *sz, float *Wx, float *Wy, float *Wz, double *lam1_dev);
+void launch_D_plain(cudaStream_t s, int dims, int p, int q, int r, const real *U, real *Ux, real *Uy,
+                    real *Uz);
+void launch_Dt_plain(cudaStream_t s, int dims, int p, int q, int r, const real *X, const real *Y,
+                     const real *Z, real *res);
+void launch_shrink_plain(cudaStream_t s, int dims, long long n, int tv_norm, double beta, const real *Ux,
+                         const real *Uy, const real *Uz, const real *sx, const real *sy,
+                         const real *sz, real *Wx, real *Wy, real *Wz, double *lam1_dev);
 
-}  // namespace tval3g
+TG_END

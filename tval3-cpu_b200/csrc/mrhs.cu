@@ -46,7 +46,7 @@
 
 #include "async.cuh"
 
-namespace tval3g {
+TG_BEGIN
 
 namespace {
 
@@ -627,4 +627,4 @@ int mrhs_take_error(cudaStream_t s, const MrhsOp &op) {
 	return h;
 }
 
-}  // namespace tval3g
+TG_END

@@ -8,7 +8,7 @@
 
 #include "engine.cuh"
 
-namespace tval3g {
+TG_BEGIN
 
 struct MrhsOp {
 	// forward: D[m x N] = A[m x n] X[N x n]^T; adjoint: D[n x N] = At[n x m] R[N x m]^T
@@ -50,4 +50,4 @@ void mrhs_set_members(cudaStream_t s, MrhsOp &op, const int *members);
 // nonzero if a kernel of this operator gave up a bounded wait (resets it)
 int mrhs_take_error(cudaStream_t s, const MrhsOp &op);
 
-}  // namespace tval3g
+TG_END

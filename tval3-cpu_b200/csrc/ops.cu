@@ -17,10 +17,10 @@
 
 #include "async.cuh"
 
-namespace tval3g {
+TG_BEGIN
 
-__device__ __forceinline__ const float *vsel(const Inst &I, VecSel s) { return s.m ? I.vm[s.idx] : I.vn[s.idx]; }
-__device__ __forceinline__ float *vselw(const Inst &I, VecSel s) { return s.m ? I.vm[s.idx] : I.vn[s.idx]; }
+__device__ __forceinline__ const real *vsel(const Inst &I, VecSel s) { return s.m ? I.vm[s.idx] : I.vn[s.idx]; }
+__device__ __forceinline__ real *vselw(const Inst &I, VecSel s) { return s.m ? I.vm[s.idx] : I.vn[s.idx]; }
 
 #define OPROLOGUE()                                                                   \
 	pdl_launch_next();                                                                \
@@ -44,10 +44,10 @@ __global__ void __launch_bounds__(256) k_dense_fwd(const Inst *tab, TileMap map,
 	const long long layer = local / rt;
 	const long long row = (local - layer * rt) * WARPS + warp;
 	if (row >= m) return;
-	const float *a = op.A + row * n;
-	const float *x = vsel(I, xs) + layer * n;
+	const real *a = op.A + row * n;
+	const real *x = vsel(I, xs) + layer * n;
 	double acc = 0.0;   // FP64 accumulation of FP32 products
-	if ((n & 3) == 0 && ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(x)) & 15) == 0) {
+	if (!FP64_BUILD && (n & 3) == 0 && ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(x)) & 15) == 0) {
 		const float4 *a4 = reinterpret_cast<const float4 *>(a);
 		const float4 *x4 = reinterpret_cast<const float4 *>(x);
 		const long long n4 = n >> 2;
@@ -79,12 +79,12 @@ __global__ void __launch_bounds__(256) k_dense_fwd(const Inst *tab, TileMap map,
 		for (long long j = lane; j < n; j += 32) acc = fma((double)__ldg(a + j), (double)__ldg(x + j), acc);
 	}
 	acc = warp_sum(acc);
-	if (lane == 0) vselw(I, ys)[layer * m + row] = (float)acc;
+	if (lane == 0) vselw(I, ys)[layer * m + row] = (real)acc;
 }
 
 // partial column sums of A^T x over one row chunk
 __global__ void __launch_bounds__(256) k_dense_adj(const Inst *tab, TileMap map, int pred, VecSel xs,
-                                                   VecSel ys, float *part, unsigned long long *launches) {
+                                                   VecSel ys, real *part, unsigned long long *launches) {
 	OPROLOGUE();
 	const OpDev &op = I.op;
 	const long long m = op.m, n = op.n;
@@ -96,14 +96,14 @@ __global__ void __launch_bounds__(256) k_dense_adj(const Inst *tab, TileMap map,
 	const long long rows_per = (m + K - 1) / K;
 	const long long r0 = kc * rows_per, r1 = min(m, r0 + rows_per);
 	const long long c0 = ct * 1024 + threadIdx.x * 4;
-	const float *x = vsel(I, xs) + layer * m;
+	const real *x = vsel(I, xs) + layer * m;
 	double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;   // FP64 accumulation
-	if ((n & 3) == 0 && (reinterpret_cast<uintptr_t>(op.A) & 15) == 0) {
+	if (!FP64_BUILD && (n & 3) == 0 && (reinterpret_cast<uintptr_t>(op.A) & 15) == 0) {
 		if (c0 < n) {
 			long long r = r0;
 			// four rows in flight per thread; the FMA order is the plain loop's
 			for (; r + 3 < r1; r += 4) {
-				float xv[4];
+				real xv[4];
 				float4 av[4];
 #pragma unroll
 				for (int u = 0; u < 4; u++) {
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(256) k_dense_adj(const Inst *tab, TileMap map,
 				}
 			}
 			for (; r < r1; r++) {
-				float xv = __ldg(x + r);
+				real xv = __ldg(x + r);
 				float4 av = __ldg(reinterpret_cast<const float4 *>(op.A + r * n + c0));
 				acc0 = fma((double)av.x, (double)xv, acc0);
 				acc1 = fma((double)av.y, (double)xv, acc1);
@@ -129,26 +129,26 @@ __global__ void __launch_bounds__(256) k_dense_adj(const Inst *tab, TileMap map,
 		}
 	} else {
 		for (long long r = r0; r < r1; r++) {
-			float xv = __ldg(x + r);
-			const float *ar = op.A + r * n;
+			real xv = __ldg(x + r);
+			const real *ar = op.A + r * n;
 			if (c0 + 0 < n) acc0 = fma((double)__ldg(ar + c0 + 0), (double)xv, acc0);
 			if (c0 + 1 < n) acc1 = fma((double)__ldg(ar + c0 + 1), (double)xv, acc1);
 			if (c0 + 2 < n) acc2 = fma((double)__ldg(ar + c0 + 2), (double)xv, acc2);
 			if (c0 + 3 < n) acc3 = fma((double)__ldg(ar + c0 + 3), (double)xv, acc3);
 		}
 	}
-	float *p = part + op.dense_part + (layer * K + kc) * n;
-	if (c0 + 0 < n) p[c0 + 0] = (float)acc0;
-	if (c0 + 1 < n) p[c0 + 1] = (float)acc1;
-	if (c0 + 2 < n) p[c0 + 2] = (float)acc2;
-	if (c0 + 3 < n) p[c0 + 3] = (float)acc3;
+	real *p = part + op.dense_part + (layer * K + kc) * n;
+	if (c0 + 0 < n) p[c0 + 0] = (real)acc0;
+	if (c0 + 1 < n) p[c0 + 1] = (real)acc1;
+	if (c0 + 2 < n) p[c0 + 2] = (real)acc2;
+	if (c0 + 3 < n) p[c0 + 3] = (real)acc3;
 }
 
 // y = sum of the K row-chunk partials, 32 columns per block: warp w adds the
 // partials k = w, w + 8, ... of its lane's column, then warp 0 adds the eight
 // warp sums in a fixed order (deterministic)
 __global__ void __launch_bounds__(256) k_dense_red(const Inst *tab, TileMap map, int pred, VecSel xs, VecSel ys,
-                                                   const float *part, unsigned long long *launches) {
+                                                   const real *part, unsigned long long *launches) {
 	OPROLOGUE();
 	__shared__ double ws[8][32];
 	const OpDev &op = I.op;
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(256) k_dense_red(const Inst *tab, TileMap map,
 	const long long layer = local / ct_n, ct = local - layer * ct_n;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const long long c = ct * 32 + lane;
-	const float *p = part + op.dense_part + layer * K * n;
+	const real *p = part + op.dense_part + layer * K * n;
 	double s = 0.0;
 	if (c < n)
 		for (int k = warp; k < K; k += 8) s += p[(long long)k * n + c];
@@ -167,10 +167,11 @@ __global__ void __launch_bounds__(256) k_dense_red(const Inst *tab, TileMap map,
 	if (warp == 0 && c < n) {
 		double t = ws[0][lane];
 		for (int w = 1; w < 8; w++) t += ws[w][lane];
-		vselw(I, ys)[layer * n + c] = (float)t;
+		vselw(I, ys)[layer * n + c] = (real)t;
 	}
 }
 
+#ifndef TVAL3G_FP64   // one-pass dense normal product: FP32 data only
 // ---------------------------------------------------------------------------
 // dense normal product, A read once (get_g_mult's cache-blocked dense path,
 // 2d/tval3_cpu_2d.cpp:361-394): Au = A u and g = A^T Au in one pass over A.
@@ -438,6 +439,10 @@ int fused_rows_per_cta(long long m, long long n, int grid, const float *A, int *
 	return (int)rpc;
 }
 
+#else   // FP64 build: no one-pass normal product (dense normal products take the gemv kernels)
+int fused_grid() { return 1; }
+int fused_rows_per_cta(long long, long long, int, const real *, int *) { return 0; }
+#endif
 // ---------------------------------------------------------------------------
 // compressed gather: y[line] = w * sum_k val[k] * x[ind[k]] over a line's range
 //   kind 0: CSR rows (forward), kind 1: CSC columns (adjoint of CSR),
@@ -449,7 +454,7 @@ __global__ void __launch_bounds__(256) k_gather(const Inst *tab, TileMap map, in
 	OPROLOGUE();
 	const OpDev &op = I.op;
 	const int *ptr, *ind;
-	const float *val;
+	const real *val;
 	long long lines, xlen, ylen;
 	if (kind == 0) { ptr = op.rptr; ind = op.rind; val = op.rval; lines = op.m; xlen = op.n; ylen = op.m; }
 	else if (kind == 1) { ptr = op.cptr; ind = op.cind; val = op.cval; lines = op.n; xlen = op.m; ylen = op.n; }
@@ -459,7 +464,7 @@ __global__ void __launch_bounds__(256) k_gather(const Inst *tab, TileMap map, in
 	const long long layer = local / lt;
 	const long long line = (local - layer * lt) * LPB + threadIdx.x / W;
 	const int gl = threadIdx.x % W;
-	const float *x = vsel(I, xs) + layer * xlen;
+	const real *x = vsel(I, xs) + layer * xlen;
 	double acc = 0.0;   // FP64 accumulation of FP32 products
 	if (line < lines) {
 		// four of the lane's entries per step: their indices, then the four
@@ -469,7 +474,7 @@ __global__ void __launch_bounds__(256) k_gather(const Inst *tab, TileMap map, in
 		if (val) {
 			for (; k + 3 * W < k1; k += 4 * W) {
 				int ii[4];
-				float vv[4], xx[4];
+				real vv[4], xx[4];
 #pragma unroll
 				for (int u = 0; u < 4; u++) {
 					ii[u] = __ldg(ind + k + u * W);
@@ -484,7 +489,7 @@ __global__ void __launch_bounds__(256) k_gather(const Inst *tab, TileMap map, in
 		} else {
 			for (; k + 3 * W < k1; k += 4 * W) {
 				int ii[4];
-				float xx[4];
+				real xx[4];
 #pragma unroll
 				for (int u = 0; u < 4; u++) ii[u] = __ldg(ind + k + u * W);
 #pragma unroll
@@ -497,7 +502,7 @@ __global__ void __launch_bounds__(256) k_gather(const Inst *tab, TileMap map, in
 	}
 #pragma unroll
 	for (int o = W / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-	if (gl == 0 && line < lines) vselw(I, ys)[layer * ylen + line] = (float)(val ? acc : acc * op.scale);
+	if (gl == 0 && line < lines) vselw(I, ys)[layer * ylen + line] = (real)(val ? acc : acc * op.scale);
 }
 
 // ---------------------------------------------------------------------------
@@ -560,7 +565,7 @@ __global__ void __launch_bounds__(256) k_ray_fwd(const Inst *tab, TileMap map, i
 	constexpr int RPB = 256 / SUBW;   // rays per block
 	const int gl = threadIdx.x % SUBW;
 	const long long ray = local * RPB + threadIdx.x / SUBW;
-	const float *x = vsel(I, xs);
+	const real *x = vsel(I, xs);
 	double acc = 0.0;   // FP64 accumulation along the ray (of FP32 sums of four hits)
 	int out = -1;
 	if (ray < op.nrays) {
@@ -611,7 +616,7 @@ __global__ void __launch_bounds__(256) k_ray_fwd(const Inst *tab, TileMap map, i
 		// conversion per four hits)
 		int j = gl;
 		for (; j + 3 * SUBW <= M; j += 4 * SUBW) {
-			float v[4];
+			real v[4];
 #pragma unroll
 			for (int u = 0; u < 4; u++) {
 				v[u] = __ldg(x + idx);
@@ -619,7 +624,7 @@ __global__ void __launch_bounds__(256) k_ray_fwd(const Inst *tab, TileMap map, i
 			}
 			acc += (double)((v[0] + v[1]) + (v[2] + v[3]));
 		}
-		float rest = 0.f;
+		real rest = 0.f;
 		for (; j <= M; j += SUBW) {
 			rest += __ldg(x + idx);
 			step();
@@ -628,7 +633,7 @@ __global__ void __launch_bounds__(256) k_ray_fwd(const Inst *tab, TileMap map, i
 	}
 #pragma unroll
 	for (int o = SUBW / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-	if (gl == 0 && out >= 0) vselw(I, ys)[out] = (float)(acc * op.scale);
+	if (gl == 0 && out >= 0) vselw(I, ys)[out] = (real)(acc * op.scale);
 }
 
 // The adjoint by on-the-fly tracing (TVAL3G_RAY_ADJ_ATOMICS): lanes and
@@ -639,7 +644,7 @@ __global__ void __launch_bounds__(256) k_ray_fwd(const Inst *tab, TileMap map, i
 __global__ void __launch_bounds__(256) k_ray_atomic_zero(const Inst *tab, TileMap map, int pred, VecSel ys,
                                                          unsigned long long *launches) {
 	OPROLOGUE();
-	float *out = vselw(I, ys);
+	real *out = vselw(I, ys);
 	const long long i0 = local * ATOMIC_ZERO_TILE;
 	for (long long i = i0 + threadIdx.x; i < min(I.n, i0 + ATOMIC_ZERO_TILE); i += blockDim.x) out[i] = 0.f;
 }
@@ -653,10 +658,10 @@ __global__ void __launch_bounds__(256) k_ray_adj_atomic(const Inst *tab, TileMap
 	const int gl = threadIdx.x % SUBW;
 	const long long ray = local * RPB + threadIdx.x / SUBW;
 	if (ray >= op.nrays) return;
-	float *g = vselw(I, ys);
+	real *g = vselw(I, ys);
 	int x0, y0, z0, dx, dy, dz, out;
 	unpack_ray(op.rays[ray], x0, y0, z0, dx, dy, dz, out);
-	const float w = vsel(I, xs)[out] * op.scale;
+	const real w = vsel(I, xs)[out] * op.scale;
 	const int mx = abs(dx), my = abs(dy), mz = D3 ? abs(dz) : 0;
 	const int sx = dx < 0 ? -1 : 1, sy = (dy < 0 ? -1 : 1) * op.rvx;
 	const int sz = (dz < 0 ? -1 : 1) * op.rvx * op.rvy;
@@ -700,13 +705,13 @@ __global__ void __launch_bounds__(256) k_ray_adj_atomic(const Inst *tab, TileMap
 __global__ void __launch_bounds__(256) k_transpose2d(const Inst *tab, TileMap map, int pred, VecSel xs,
                                                      unsigned long long *launches) {
 	OPROLOGUE();
-	__shared__ float tile[32][33];
+	__shared__ real tile[32][33];
 	const OpDev &op = I.op;
 	const int ld = op.rvx, H = op.tH;
 	const int ntx = (ld + 31) / 32;
 	const int bx = (int)local % ntx, by = (int)local / ntx;
 	const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-	const float *X = vsel(I, xs);
+	const real *X = vsel(I, xs);
 #pragma unroll
 	for (int j = 0; j < 32; j += 8) {
 		const int x = bx * 32 + tx, y = by * 32 + ty + j;
@@ -720,6 +725,7 @@ __global__ void __launch_bounds__(256) k_transpose2d(const Inst *tab, TileMap ma
 	}
 }
 
+#ifndef TVAL3G_FP64   // tiled ray adjoints: FP32 data only
 // ---------------------------------------------------------------------------
 // tiled 2D ray adjoint
 // ---------------------------------------------------------------------------
@@ -1331,6 +1337,21 @@ bool build_brick_words(cudaStream_t s, int rvx, int rvy, int rvz, const int *cpt
 	return ok;
 }
 
+#else   // FP64 build: the ray adjoints are the pixel-major gathers
+bool build_tiled_index(cudaStream_t, int, int, int, const int *, const int *, const int *, OpDev &, long long *,
+                       std::vector<void *> &) {
+	return false;
+}
+int tiled_smem_bytes(int) { return 0; }
+real *brick_positions(cudaStream_t, int, int, int, int, long long, const int *, const int *, const int *, BrickLists &,
+                      std::vector<void *> &) {
+	return nullptr;
+}
+bool build_brick_words(cudaStream_t, int, int, int, const int *, const real *, BrickLists &, OpDev &, long long *,
+                       std::vector<void *> &) {
+	return false;
+}
+#endif
 // ---------------------------------------------------------------------------
 // dispatch
 // ---------------------------------------------------------------------------
@@ -1349,7 +1370,9 @@ static void gather(const LaunchCtx &L, const TileMap (&maps)[4], int pred, int k
 
 void op_forward(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y, bool unfused, bool xT_ready) {
 	auto *ctr = (unsigned long long *)L.launches;
+#ifndef TVAL3G_FP64
 	for (const auto &e : B.mrhs) mrhs_apply(L.stream, L.inst, e.first, pred, *e.second, false, x, y, ctr);
+#endif
 	const TileMap &df = unfused ? B.dense_fwd_nf : B.dense_fwd;
 	if (df.count > 0) {
 		launch_pdl(k_dense_fwd, df.count, 256, 0, L.stream, L.inst, df, pred, x, y, ctr);
@@ -1374,11 +1397,13 @@ void op_forward(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel
 
 void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y, bool unfused) {
 	auto *ctr = (unsigned long long *)L.launches;
+#ifndef TVAL3G_FP64
 	for (const auto &e : B.mrhs) mrhs_apply(L.stream, L.inst, e.first, pred, *e.second, true, x, y, ctr);
+#endif
 	const TileMap &da = unfused ? B.dense_adj_nf : B.dense_adj, &dr = unfused ? B.dense_red_nf : B.dense_red;
 	if (da.count > 0) {
 		launch_pdl(k_dense_adj, da.count, 256, 0, L.stream, L.inst, da, pred, x, y, B.dense_part, ctr);
-		launch_pdl(k_dense_red, dr.count, 256, 0, L.stream, L.inst, dr, pred, x, y, (const float *)B.dense_part, ctr);
+		launch_pdl(k_dense_red, dr.count, 256, 0, L.stream, L.inst, dr, pred, x, y, (const real *)B.dense_part, ctr);
 	}
 	gather(L, B.csc_adj, pred, 1, x, y);
 	gather(L, B.ray_adj, pred, 2, x, y);
@@ -1390,13 +1415,16 @@ void op_adjoint(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel
 	if (B.ray3_adj_atomic.count > 0)
 		launch_pdl(k_ray_adj_atomic<true>, B.ray3_adj_atomic.count, 256, 0, L.stream, L.inst, B.ray3_adj_atomic, pred,
 		           x, y, ctr);
+#ifndef TVAL3G_FP64
 	if (B.ray_adj_tiled.count > 0) {
 		launch_pdl(k_ray_adj_tiled, B.ray_adj_tiled.count, RAYT_ADJ_THREADS, tiled_smem_bytes(B.tiled_tmax), L.stream,
 		           L.inst, B.ray_adj_tiled, pred, x, y, B.err, ctr);
 	}
+#endif
 }
 
 void op_fused_normal(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y, VecSel z) {
+#ifndef TVAL3G_FP64
 	auto *ctr = (unsigned long long *)L.launches;
 	for (const auto &f : B.fused) {
 		int *flags = B.fused_flags + f.off, *err = B.err;
@@ -1408,6 +1436,9 @@ void op_fused_normal(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, V
 		TG_CUDA(cudaLaunchCooperativeKernel((const void *)k_dense_normal, dim3(B.fused_grid), dim3(FUSED_THREADS),
 		                                    args, FUSED_DYN_BYTES, L.stream));
 	}
+#else
+	(void)L; (void)B; (void)pred; (void)x; (void)y; (void)z;
+#endif
 }
 
 void op_normal(const LaunchCtx &L, const OpBatch &B, int pred, VecSel x, VecSel y, VecSel z) {
@@ -1561,16 +1592,16 @@ __global__ void __launch_bounds__(RADIX_T) k_radix_hist(const int *key, long lon
 // k_radix_hist), then written out in slot order: consecutive threads write
 // the consecutive entries of one digit to consecutive addresses, instead of
 // one scattered 4-byte write per entry.
-constexpr int RADIX_DYN_BYTES = RADIX_TILE * 3 * 4;   // keys, values, float values
+constexpr int RADIX_DYN_BYTES = RADIX_TILE * (8 + (int)sizeof(real));   // keys, values, entry values
 __global__ void __launch_bounds__(RADIX_T) k_radix_scatter(const int *__restrict__ key, const int *__restrict__ val,
-                                                           const float *__restrict__ fval, long long nnz, int shift,
+                                                           const real *__restrict__ fval, long long nnz, int shift,
                                                            const long long *__restrict__ off,
                                                            const long long *__restrict__ hist,
                                                            int *__restrict__ key_out, int *__restrict__ val_out,
-                                                           float *__restrict__ fval_out) {
-	extern __shared__ int stage[];   // RADIX_TILE keys, then values, then float values (fval only)
+                                                           real *__restrict__ fval_out) {
+	extern __shared__ int stage[];   // RADIX_TILE keys, then row values, then entry values (fval only)
 	int *sk = stage, *sv = stage + RADIX_TILE;
-	float *sf = reinterpret_cast<float *>(stage + 2 * RADIX_TILE);
+	real *sf = reinterpret_cast<real *>(stage + 2 * RADIX_TILE);
 	__shared__ int wcnt[RADIX_WARPS][256];
 	__shared__ int wbase[RADIX_WARPS][256];
 	__shared__ long long tile_off[256];
@@ -1595,7 +1626,7 @@ __global__ void __launch_bounds__(RADIX_T) k_radix_scatter(const int *__restrict
 	}
 	const long long base = (long long)blockIdx.x * RADIX_TILE;
 	int kv[RADIX_ITEMS], vv[RADIX_ITEMS];
-	float fv[RADIX_ITEMS];
+	real fv[RADIX_ITEMS];
 #pragma unroll
 	for (int j = 0; j < RADIX_ITEMS; j++) {   // every load up front
 		const long long k = base + j * RADIX_T + t;
@@ -1656,7 +1687,7 @@ __global__ void k_col_counts(const int *skey, long long nnz, long long *cnt) {
 }
 
 void build_transpose(cudaStream_t s, long long rows, long long cols, long long nnz, const int *rptr,
-                     const int *rind, const float *rval, int *cptr, int *cind, float *cval) {
+                     const int *rind, const real *rval, int *cptr, int *cind, real *cval) {
 	if (nnz <= 0 || rows <= 0) {
 		TG_CUDA(cudaMemsetAsync(cptr, 0, sizeof(int) * (cols + 1), s));
 		return;
@@ -1666,7 +1697,7 @@ void build_transpose(cudaStream_t s, long long rows, long long cols, long long n
 	const int passes = (bits + 7) / 8;
 	const long long tiles = (nnz + RADIX_TILE - 1) / RADIX_TILE;
 	int *k0 = nullptr, *k1 = nullptr, *v0 = nullptr, *v1 = nullptr;
-	float *f0 = nullptr, *f1 = nullptr;
+	real *f0 = nullptr, *f1 = nullptr;
 	long long *hist = nullptr, *hoff = nullptr;
 	hist = (decltype(hist))dev_alloc(sizeof(long long) * (256 * tiles + 1), s);
 	hoff = (decltype(hoff))dev_alloc(sizeof(long long) * (256 * tiles + 1), s);
@@ -1676,8 +1707,8 @@ void build_transpose(cudaStream_t s, long long rows, long long cols, long long n
 		k1 = (decltype(k1))dev_alloc(sizeof(int) * nnz, s);
 		v1 = (decltype(v1))dev_alloc(sizeof(int) * nnz, s);
 		if (rval) {
-			f0 = (decltype(f0))dev_alloc(sizeof(float) * nnz, s);
-			f1 = (decltype(f1))dev_alloc(sizeof(float) * nnz, s);
+			f0 = (decltype(f0))dev_alloc(sizeof(real) * nnz, s);
+			f1 = (decltype(f1))dev_alloc(sizeof(real) * nnz, s);
 		}
 	}
 	k_entry_rows<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(rows, rptr, v0);
@@ -1686,15 +1717,15 @@ void build_transpose(cudaStream_t s, long long rows, long long cols, long long n
 	// first) and writes the next triple of buffers; the last pass writes
 	// cind and cval, and its keys for the column offsets
 	const int *kin = rind, *vin = v0;
-	const float *fin = rval;
+	const real *fin = rval;
 	for (int p = 0; p < passes; p++) {
 		const bool last = p == passes - 1;
 		int *kout = p % 2 == 0 ? k0 : k1;
 		int *vout = last ? cind : (p % 2 == 0 ? v1 : v0);
-		float *fout = !rval ? nullptr : last ? cval : (p % 2 == 0 ? f0 : f1);
+		real *fout = !rval ? nullptr : last ? cval : (p % 2 == 0 ? f0 : f1);
 		k_radix_hist<<<(unsigned)tiles, RADIX_T, 0, s>>>(kin, nnz, 8 * p, hist);
 		scan_counts(s, hist, hoff, 256 * tiles);
-		const int dyn = RADIX_TILE * 4 * (fin ? 3 : 2);   // float values staged only when there are some
+		const int dyn = RADIX_TILE * 8 + (fin ? RADIX_TILE * (int)sizeof(real) : 0);   // values staged only when there are some
 		k_radix_scatter<<<(unsigned)tiles, RADIX_T, dyn, s>>>(kin, vin, fin, nnz, 8 * p, hoff, hist, kout, vout, fout);
 		kin = kout;
 		vin = vout;
@@ -1825,4 +1856,4 @@ int *trace_rays(cudaStream_t s, int nrays, const int4 *rays, int rvx, int rvy, i
 	return rind;
 }
 
-}  // namespace tval3g
+TG_END

@@ -8,7 +8,7 @@
 #include "engine.cuh"
 #include "mrhs.cuh"
 
-namespace tval3g {
+TG_BEGIN
 
 constexpr int WARPS = 8;   // warps per block in the operator kernels
 // lanes per ray of the on-the-fly forward projectors: a warp traces
@@ -23,7 +23,7 @@ struct OpBatch {
 	// dense (2d/mat_mult.h:15-36): forward warp-per-row gemv; adjoint over
 	// (column tile, row chunk) blocks into partials, then a column reduction
 	TileMap dense_fwd, dense_adj, dense_red;
-	float *dense_part = nullptr;
+	real *dense_part = nullptr;
 	// dense operators whose normal product A^T (A u) reads A once
 	// (k_dense_normal, one cooperative launch per instance); the gemv maps
 	// without them serve the rest of a normal product
@@ -93,16 +93,16 @@ struct BrickLists {
 	int *tptr = nullptr, *tmeas = nullptr;
 	long long tmax = 0;
 };
-float *brick_positions(cudaStream_t s, int rvx, int rvy, int rvz, int nrays, long long total, const int *rptr,
+real *brick_positions(cudaStream_t s, int rvx, int rvy, int rvz, int nrays, long long total, const int *rptr,
                        const int *rind, const int *live_out, BrickLists &bl, std::vector<void *> &owned);
-bool build_brick_words(cudaStream_t s, int rvx, int rvy, int rvz, const int *cptr, const float *cval,
+bool build_brick_words(cudaStream_t s, int rvx, int rvy, int rvz, const int *cptr, const real *cval,
                        BrickLists &bl, OpDev &d, long long *bytes, std::vector<void *> &owned);
 // the dense normal product's launch: CTAs (one per SM), and rows per CTA per
 // band for an m x n operator A (0: the operator does not suit it - n not a
 // multiple of 4, A not 16-byte aligned, its slab or two bands do not fit),
 // with the slab width
 int fused_grid();
-int fused_rows_per_cta(long long m, long long n, int grid, const float *A, int *slab);
+int fused_rows_per_cta(long long m, long long n, int grid, const real *A, int *slab);
 // Au = A u and g = A^T Au for the fused dense instances (A read once)
 void op_fused_normal(const LaunchCtx &L, const OpBatch &B, int pred, VecSel u, VecSel au, VecSel g);
 // the normal product of every instance: fused dense instances in one pass,
@@ -114,7 +114,7 @@ void op_normal(const LaunchCtx &L, const OpBatch &B, int pred, VecSel u, VecSel 
 void scan_counts(cudaStream_t s, const long long *cnt, long long *out, long long n);
 // CSR (rows x cols, rptr int32) -> CSC sorted by row within a column; cval may be NULL
 void build_transpose(cudaStream_t s, long long rows, long long cols, long long nnz, const int *rptr,
-                     const int *rind, const float *rval, int *cptr, int *cind, float *cval);
+                     const int *rind, const real *rval, int *cptr, int *cind, real *cval);
 // The traced rays of a ray geometry, packed on the device in the reference's
 // loop order (measurement plane, emitter, receiver; a ray for every nonzero
 // use_path entry): 2D: out = e R + r; 3D: out = mp numPaths + use_path - 1.
@@ -155,4 +155,4 @@ __host__ __device__ inline void unpack_ray(int4 r, int &x0, int &y0, int &z0, in
 	out = r.w;
 }
 
-}  // namespace tval3g
+TG_END

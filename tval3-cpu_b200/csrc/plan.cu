@@ -12,7 +12,8 @@
 #include <mutex>
 
 namespace tval3g {
-
+// the device-memory pool is shared by both precision builds (defined once)
+#ifndef TVAL3G_FP64
 cudaMemPool_t library_pool() {
 	static std::mutex mu;
 	static std::map<int, cudaMemPool_t> pools;
@@ -43,6 +44,10 @@ void *dev_alloc(size_t bytes, cudaStream_t s) {
 void dev_free(void *p, cudaStream_t s) {
 	if (p) cudaFreeAsync(p, s);
 }
+#endif
+}  // namespace tval3g
+
+TG_BEGIN
 
 
 // ---------------------------------------------------------------------------
@@ -165,7 +170,7 @@ __global__ void k_map_out(long long nnz, const int4 *rays, int *cind) {
 // [Re x; Im x] -> [Re A x; Im A x], i.e. [[Re A, -Im A], [Im A, Re A]], whose
 // transpose gives [Re A^H y; Im A^H y] - the reference's conjugate-transposed
 // products (2d/mat_mult.h:15-91, CblasConjTrans / 'c').  Dense A and CSR
-// values arrive as interleaved (re, im) floats; a ray geometry (real
+// values arrive as interleaved (re, im) pairs; a ray geometry (real
 // weights, 2D or 3D) becomes the CSR form of diag(A, A) over its traced rays.
 static void prepare_complex_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
                                bool keep_ray_csr) {
@@ -176,10 +181,11 @@ static void prepare_complex_op(cudaStream_t s, const tval3g_problem &p, int flag
 	const long long L = p.dims == 2 && p.op_kind != TVAL3G_OP_RAY2D ? std::max(p.layers, 1) : 1;
 	if (p.op_kind == TVAL3G_OP_DENSE && L == 1) {
 		const long long m = p.m, nc = p.n_cols;
-		std::vector<float> R((size_t)(4 * m * nc));
+		const real *pa = prob_A(p);
+		std::vector<real> R((size_t)(4 * m * nc));
 		for (long long r = 0; r < m; r++)
 			for (long long c = 0; c < nc; c++) {
-				const float ar = p.A[2 * (r * nc + c)], ai = p.A[2 * (r * nc + c) + 1];
+				const real ar = pa[2 * (r * nc + c)], ai = pa[2 * (r * nc + c) + 1];
 				R[(size_t)(r * 2 * nc + c)] = ar;
 				R[(size_t)(r * 2 * nc + nc + c)] = -ai;
 				R[(size_t)((m + r) * 2 * nc + c)] = ai;
@@ -187,7 +193,7 @@ static void prepare_complex_op(cudaStream_t s, const tval3g_problem &p, int flag
 			}
 		q.m = (int)(2 * m);
 		q.n_cols = (int)(2 * nc);
-		q.A = R.data();
+		q.A = reinterpret_cast<const float *>(R.data());   // read back as real (prob_A)
 		prepare_op(s, q, flags, st, keep_ray_csr);   // copies R before it returns
 		return;
 	}
@@ -196,11 +202,11 @@ static void prepare_complex_op(cudaStream_t s, const tval3g_problem &p, int flag
 	// hold all layers' real parts, then all imaginary parts, so layer l's
 	// block maps columns l nc (+ L nc for Im x) to rows l m (+ L m for Im y).
 	auto expand = [&](long long m, long long nc, const std::vector<int> &ptr, const std::vector<int> &ind,
-	                  const float *re, const float *im, int re_stride) {
+	                  const real *re, const real *im, int re_stride) {
 		const long long nnz = ptr[m], P = L * nc;
 		TG_ARG(4 * nnz * L < (1LL << 31), "Argument error: the complex operator has too many entries");
 		std::vector<int> rp((size_t)(2 * m * L + 1)), ri((size_t)(4 * nnz * L));
-		std::vector<float> rv((size_t)(4 * nnz * L));
+		std::vector<real> rv((size_t)(4 * nnz * L));
 		long long o = 0;
 		for (int half = 0; half < 2; half++)
 			for (long long l = 0; l < L; l++)
@@ -208,7 +214,7 @@ static void prepare_complex_op(cudaStream_t s, const tval3g_problem &p, int flag
 					rp[(size_t)(half * m * L + l * m + r)] = (int)o;
 					for (int part = 0; part < 2; part++)   // columns of Re x, then of Im x
 						for (long long k = ptr[r]; k < ptr[r + 1]; k++) {
-							const float vr = re[k * re_stride], vi = im ? im[k * re_stride] : 0.f;
+							const real vr = re[k * re_stride], vi = im ? im[k * re_stride] : 0.f;
 							ri[(size_t)o] = (int)(ind[(size_t)k] + l * nc + (part ? P : 0));
 							// [[Re A, -Im A], [Im A, Re A]]
 							rv[(size_t)o++] = half == 0 ? (part == 0 ? vr : -vi) : (part == 0 ? vi : vr);
@@ -224,20 +230,20 @@ static void prepare_complex_op(cudaStream_t s, const tval3g_problem &p, int flag
 		c.nnz = o;
 		c.csr_ptr = rp.data();
 		c.csr_ind = ri.data();
-		c.csr_val = rv.data();
+		c.csr_val = reinterpret_cast<const float *>(rv.data());   // read back as real (prob_val)
 		prepare_op(s, c, flags, st, keep_ray_csr);
 		TG_CUDA(cudaStreamSynchronize(s));
 	};
 	if (p.op_kind == TVAL3G_OP_CSR) {
 		std::vector<int> ptr(p.csr_ptr, p.csr_ptr + p.m + 1), ind(p.csr_ind, p.csr_ind + p.nnz);
-		expand(p.m, p.n_cols, ptr, ind, p.csr_val, p.csr_val + 1, 2);
+		expand(p.m, p.n_cols, ptr, ind, prob_val(p), prob_val(p) + 1, 2);
 		return;
 	}
 	if (p.op_kind == TVAL3G_OP_DENSE) {   // layered: every entry of A as a CSR entry
 		std::vector<int> ptr((size_t)p.m + 1), ind((size_t)p.m * p.n_cols);
 		for (long long r = 0; r <= p.m; r++) ptr[(size_t)r] = (int)(r * p.n_cols);
 		for (long long k = 0; k < (long long)p.m * p.n_cols; k++) ind[(size_t)k] = (int)(k % p.n_cols);
-		expand(p.m, p.n_cols, ptr, ind, p.A, p.A + 1, 2);
+		expand(p.m, p.n_cols, ptr, ind, prob_A(p), prob_A(p) + 1, 2);
 		return;
 	}
 	// rays: trace on the device, then the CSR over all measurements (2D: E x
@@ -262,7 +268,7 @@ static void prepare_complex_op(cudaStream_t s, const tval3g_problem &p, int flag
 	for (int k = 0; k < nr; k++)
 		std::copy(tri.begin() + trp[(size_t)k], tri.begin() + trp[(size_t)k + 1],
 		          ind.begin() + ptr[(size_t)tmp.ray_out[k]]);
-	std::vector<float> val((size_t)std::max(tmp.nnz, 1LL), scale);
+	std::vector<real> val((size_t)std::max(tmp.nnz, 1LL), (real)scale);
 	expand(m, n, ptr, ind, val.data(), nullptr, 1);
 }
 
@@ -280,13 +286,15 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 	d.scale = 1.f;
 	if (p.op_kind == TVAL3G_OP_DENSE) {
 		d.m = p.m; d.n = p.n_cols;
-		d.A = dcopy(s, st, p.A, (long long)p.m * p.n_cols, borrow);
+		d.A = dcopy(s, st, prob_A(p), (long long)p.m * p.n_cols, borrow);
 		st.b_len = (long long)p.m * d.layers;
+#ifndef TVAL3G_FP64   // the tensor-core path takes FP32 data
 		if (!(flags & TVAL3G_NO_TENSOR) && mrhs_eligible(d.m, d.n, d.layers)) {
 			st.mrhs = mrhs_create(s, d.A, d.m, d.n, d.layers);
 			st.bytes += st.mrhs->bytes;
 			d.mrhs = 1;
 		}
+#endif
 	} else if (p.op_kind == TVAL3G_OP_CSR) {
 		d.m = p.m; d.n = p.n_cols;
 		st.nnz = p.nnz;
@@ -299,10 +307,10 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		}
 		d.rptr = dcopy(s, st, p.csr_ptr, (long long)p.m + 1, borrow);
 		d.rind = dcopy(s, st, p.csr_ind, p.nnz, borrow);
-		d.rval = dcopy(s, st, p.csr_val, p.nnz, borrow);
+		d.rval = dcopy(s, st, prob_val(p), p.nnz, borrow);
 		int *cptr = dalloc_op<int>(s, st, d.n + 1);
 		int *cind = dalloc_op<int>(s, st, p.nnz);
-		float *cval = dalloc_op<float>(s, st, p.nnz);
+		real *cval = dalloc_op<real>(s, st, p.nnz);
 		build_transpose(s, d.m, d.n, p.nnz, d.rptr, d.rind, d.rval, cptr, cind, cval);
 		d.cptr = cptr; d.cind = cind; d.cval = cval;
 		st.adj_index_bytes = (long long)sizeof(int) * (d.n + 1) + 8LL * p.nnz;
@@ -368,11 +376,11 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 		// 3D: each hit's position in its brick's ray list, carried through the
 		// transpose (the brick-tiled adjoint)
 		BrickLists bl;
-		float *posf = nullptr, *cposf = nullptr;
+		real *posf = nullptr, *cposf = nullptr;
 		if (is3 && tile_ok) {
 			const int *lo = dout;
 			posf = brick_positions(s, p.rv_x, p.rv_y, p.rv_z, d.nrays, total, rptr, rind, lo, bl, st.owned);
-			if (posf) cposf = (float *)dev_alloc(sizeof(float) * (size_t)std::max(total, 1LL), s);
+			if (posf) cposf = (real *)dev_alloc(sizeof(real) * (size_t)std::max(total, 1LL), s);
 		}
 		int *cptr = dalloc_op<int>(s, st, n + 1);
 		int *cind = dalloc_op<int>(s, st, total);
@@ -387,7 +395,7 @@ void prepare_op(cudaStream_t s, const tval3g_problem &p, int flags, OpStore &st,
 			dev_free(cposf, s);
 		}
 		if (!is3 && n % p.ld == 0) {   // transposed image for the y-driven rays
-			d.xT = dalloc_op<float>(s, st, n);
+			d.xT = dalloc_op<real>(s, st, n);
 			d.tH = (int)(n / p.ld);
 		}
 		if (!is3 && n % p.ld == 0 && d.nrays > 0 && d.nrays <= RAYT_MAX_RAYS && tile_ok) {
@@ -470,7 +478,7 @@ static int subwarp_for(double avg) {
 	return 4;
 }
 
-// operator tile maps of a batch; returns the dense partial buffer size (floats)
+// operator tile maps of a batch; returns the dense partial buffer size (elements)
 static long long build_op_maps(std::vector<Inst> &inst, const std::vector<OpStore> &ops, TileBuilder &tb,
                                OpBatch &ob) {
 	const int cnt = (int)inst.size();
@@ -629,6 +637,11 @@ void *Plan::dalloc(size_t bytes) {
 // keeping its own scalar control (step lengths, line search, stopping).
 // Members left over (fewer than 16) keep their own gemv products.
 void Plan::group_shared_dense(const tval3g_problem *probs, int flags) {
+#ifdef TVAL3G_FP64   // the tensor-core path takes FP32 data
+	(void)probs;
+	(void)flags;
+	return;
+#else
 	if (!(flags & TVAL3G_DEVICE_INPUTS) || (flags & TVAL3G_NO_TENSOR)) return;
 	std::map<std::tuple<const float *, int, int, int>, std::vector<int>> by_a;
 	for (int i = 0; i < count_; i++) {
@@ -657,6 +670,7 @@ void Plan::group_shared_dense(const tval3g_problem *probs, int flags) {
 			k += sz;
 		}
 	}
+#endif
 }
 
 Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, int flags)
@@ -699,7 +713,9 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 			I.skip_enabled = (o.skipMulRatio != 0 && p.op_kind != TVAL3G_OP_DENSE);
 			any_skip_ |= I.skip_enabled != 0;
 			any_cplx_ |= I.cplx != 0;
+#ifndef TVAL3G_FP64   // the autotuner measures the FP32 kernels
 			if (flags & TVAL3G_TUNE) autotune_operator(stream_, ops_[i], I);
+#endif
 			I.op = ops_[i].dev;
 		}
 		group_shared_dense(probs, flags);
@@ -711,7 +727,7 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 			base[i] = total;
 			total += NVN * np + NVM * mp;
 		}
-		d_arena_ = (float *)dalloc(sizeof(float) * (size_t)total);
+		d_arena_ = (real *)dalloc(sizeof(real) * (size_t)total);
 		long long parts = 0;
 		for (int i = 0; i < count; i++) parts += (long long)(h_inst_[i].ntn + h_inst_[i].ntm) * NSUM;
 		d_part_ = (double *)dalloc(sizeof(double) * (size_t)parts);
@@ -743,7 +759,7 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 		for (int i = 0; i < count; i++) {
 			Inst &I = h_inst_[i];
 			long long np = (I.n + 63) / 64 * 64, mp = (I.m + 63) / 64 * 64;
-			float *b0 = d_arena_ + base[i];
+			real *b0 = d_arena_ + base[i];
 			for (int v = 0; v < NVN; v++) I.vn[v] = b0 + v * np;
 			for (int v = 0; v < NVM; v++) I.vm[v] = b0 + NVN * np + v * mp;
 			I.ctrl = d_ctrl_ + i;
@@ -761,7 +777,7 @@ Plan::Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, i
 		long long dense_part = build_op_maps(h_inst_, ops_, tb, ob_);
 		d_tiles_ = tb.upload(stream_);
 		allocs_.push_back(d_tiles_);
-		if (dense_part > 0) ob_.dense_part = (float *)dalloc(sizeof(float) * (size_t)dense_part);
+		if (dense_part > 0) ob_.dense_part = (real *)dalloc(sizeof(real) * (size_t)dense_part);
 		if (ob_.fused_words > 0) {
 			ob_.fused_flags = (int *)dalloc(sizeof(int) * (size_t)ob_.fused_words);
 			TG_CUDA(cudaMemsetAsync(ob_.fused_flags, 0, sizeof(int) * (size_t)ob_.fused_words, stream_));
@@ -1103,7 +1119,7 @@ void Plan::build_graph() {
 	TG_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
 }
 
-void Plan::solve(const float *const *d_b, const float *const *d_Ut, float *const *d_U, tval3g_info *info,
+void Plan::solve(const real *const *d_b, const real *const *d_Ut, real *const *d_U, tval3g_info *info,
                  cudaStream_t stream) {
 	auto t0 = std::chrono::steady_clock::now();
 	cur_ = stream ? stream : stream_;
@@ -1128,9 +1144,11 @@ void Plan::solve(const float *const *d_b, const float *const *d_Ut, float *const
 	int op_err = 0;
 	TG_CUDA(cudaMemcpyAsync(&op_err, ob_.err, sizeof(int), cudaMemcpyDeviceToHost, cur_));
 	TG_CUDA(cudaStreamSynchronize(cur_));
+#ifndef TVAL3G_FP64
 	for (const auto &e : ob_.mrhs)
 		if (mrhs_take_error(cur_, *e.second))
 			throw Error{TVAL3G_ERR_CUDA, "tensor-core operator: a bounded wait timed out (results invalid)"};
+#endif
 	if (op_err) {
 		TG_CUDA(cudaMemsetAsync(ob_.err, 0, sizeof(int), cur_));
 		throw Error{TVAL3G_ERR_CUDA, "operator: a bounded wait timed out (results invalid)"};
@@ -1151,4 +1169,4 @@ void Plan::solve(const float *const *d_b, const float *const *d_Ut, float *const
 		}
 }
 
-}  // namespace tval3g
+TG_END

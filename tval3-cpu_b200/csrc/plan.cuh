@@ -7,7 +7,7 @@
 #include "mrhs.cuh"
 #include "ops.cuh"
 
-namespace tval3g {
+TG_BEGIN
 
 // device operator storage owned by a plan / operator object
 struct OpStore {
@@ -51,7 +51,7 @@ class Plan {
 public:
 	Plan(int count, const tval3g_problem *probs, const tval3g_options *opts, int flags);
 	~Plan();
-	void solve(const float *const *d_b, const float *const *d_Ut, float *const *d_U, tval3g_info *info,
+	void solve(const real *const *d_b, const real *const *d_Ut, real *const *d_U, tval3g_info *info,
 	           cudaStream_t stream);
 	long long launches() const { return last_launches_; }
 	int trace(int index, tval3g_trace_record *out, int cap) const;
@@ -88,7 +88,7 @@ private:
 	Inst *d_inst_ = nullptr;
 	Ctrl *d_ctrl_ = nullptr;
 	double *d_part_ = nullptr;
-	float *d_arena_ = nullptr;
+	real *d_arena_ = nullptr;
 	int2 *d_tiles_ = nullptr;
 	int *d_flag_ = nullptr;
 	int h_flag_ = 0;                  // host copy of d_flag_ (host-driven plans)
@@ -129,4 +129,4 @@ private:
 	void build_graph();
 };
 
-}  // namespace tval3g
+TG_END

@@ -27,7 +27,7 @@
 #include "ops.cuh"
 #include "plan.cuh"
 
-namespace tval3g {
+TG_BEGIN
 namespace {
 
 struct Choice {
@@ -240,4 +240,4 @@ void autotune_stats(long long *measured, long long *cached) {
 	if (cached) *cached = g_cached;
 }
 
-}  // namespace tval3g
+TG_END

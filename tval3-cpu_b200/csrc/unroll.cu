@@ -38,7 +38,7 @@
 
 #include "plan.cuh"
 
-namespace tval3g {
+TG_BEGIN
 namespace {
 
 constexpr int EW_BLOCKS = 296;   // grid-stride elementwise kernels: 2 blocks per SM
@@ -588,7 +588,7 @@ void Unrolled::backward(const float *const *d_gU, float *const *d_gb, double *g_
 	}
 }
 
-}  // namespace tval3g
+TG_END
 
 using namespace tval3g;
 

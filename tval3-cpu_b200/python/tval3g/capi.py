@@ -79,6 +79,7 @@ def lib():
         P, O, I = C.POINTER(Problem), C.POINTER(Options), C.POINTER(Info)
         L.tval3g_last_error.restype = C.c_char_p
         L.tval3g_solve.argtypes = [P, vp, i, O, vp, i, vp, I]
+        L.tval3g_solve_f64.argtypes = [P, vp, vp, i, O, vp, i, vp, I]
         L.tval3g_solve_batch.argtypes = [i, P, C.POINTER(vp), O, C.POINTER(vp), C.POINTER(vp), I, i]
         L.tval3g_plan_create.argtypes = [C.POINTER(vp), i, P, O, i]
         L.tval3g_plan_solve.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), I, vp]
@@ -144,7 +145,8 @@ def tune_stats():
     return m.value, c.value
 
 
-EXPORTS = ("tval3g_last_error", "tval3g_version", "tval3g_solve", "tval3g_solve_batch", "tval3g_plan_create",
+EXPORTS = ("tval3g_last_error", "tval3g_version", "tval3g_solve", "tval3g_solve_f64", "tval3g_solve_batch",
+           "tval3g_plan_create",
            "tval3g_plan_solve", "tval3g_plan_stats", "tval3g_plan_trace", "tval3g_plan_set_target",
            "tval3g_plan_time_stencils",
            "tval3g_plan_destroy", "tval3g_trim_memory", "tval3g_tune_stats", "tval3g_op_launch_shape",
@@ -275,6 +277,26 @@ def solve(spec: ProblemSpec, b, opts: dict, Ut=None):
     rc = lib().tval3g_solve(C.byref(spec.p), b.ctypes.data, len(b), C.byref(o),
                             Utv.ctypes.data if Utv is not None else None, Utv.size if Utv is not None else 0,
                             U.ctypes.data, C.byref(info))
+    _check(rc)
+    return U.reshape(spec.shape), info.as_dict()
+
+
+def solve_f64(spec: ProblemSpec, b, opts: dict, Ut=None, values=None):
+    """One solve in double precision (tval3g_solve_f64): the FP64 engine.
+    values: the operator's values in double - the dense A (m x n_cols) or the
+    CSR values (nnz), float64, or complex128 for a complex-data problem; None
+    for ray geometries (the spec's own float arrays A / csr_val are not read).
+    Returns (U as spec.shape, float64 or complex128, info dict)."""
+    dt = np.complex128 if spec.p.complex_data else np.float64
+    b = _arr(b, dt).ravel()
+    U = np.zeros(spec.n, dt)
+    Utv = _arr(Ut, dt).ravel() if Ut is not None else None
+    vals = _arr(values, dt).ravel() if values is not None else None
+    info = Info()
+    o = Options.from_dict(opts)
+    rc = lib().tval3g_solve_f64(C.byref(spec.p), vals.ctypes.data if vals is not None else None, b.ctypes.data,
+                                len(b), C.byref(o), Utv.ctypes.data if Utv is not None else None,
+                                Utv.size if Utv is not None else 0, U.ctypes.data, C.byref(info))
     _check(rc)
     return U.reshape(spec.shape), info.as_dict()
 
