@@ -35,6 +35,10 @@ the reference's own stopping rules end it.
           batched graph against the plain one-instance-per-launch form, the
           HBM floor of its dense instances, and the relerr of each instance
           of its FP64 subset
+  configs the other reference configurations in compact records (one GPU
+          only): the dense 64x64 solve, the 128^3 hemisphere, the multi-RHS
+          solve (joint and independent right-hand sides) and the
+          differentiable unrolled solve, two timed steps each
 
 --workload dense2d | hemi3d | batch | mrhs | unrolled measures the plain dense
 64x64 problem, the 128^3 hemisphere, the mixed batch alone, the joint
@@ -77,7 +81,8 @@ def args_():
                         "configuration then, and no FP64 comparison)")
     p.add_argument("--sampling", type=float, default=0.3, help="dense2d: rows of A per pixel (m = sampling n)")
     p.add_argument("--no-batch", action="store_true",
-                   help="ring workload: leave out the mixed-batch sub-record (64 problems, 58 GB of dense A)")
+                   help="ring workload: leave out the mixed-batch sub-record (64 problems, 58 GB of dense A) "
+                        "and the other configurations' records")
     p.add_argument("--tune", action="store_true",
                    help="single-instance workloads: operators built with the launch-shape autotuner")
     p.add_argument("--plain", action="store_true",
@@ -395,7 +400,7 @@ def launch_shape(capi, spec):
     return {"forward_lanes_per_ray": s[0], "forward_gather_class": s[1], "adjoint_gather_class": s[2]}
 
 
-def run_single(a, cx, capi, name, world, rank, dist, clocks):
+def run_single(a, cx, capi, name, world, rank, dist, clocks, cpu=True):
     torch, dev, stream = cx.torch, cx.dev, cx.stream
     fwd3d = None
     if name == "hemi3d":   # data from the GPU operator (no host CSR twin at this size)
@@ -486,6 +491,8 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
         # the metric's "batched vs plain" on the mixed batch (cfg3(i) of the
         # reference configurations), measured in the same run
         extra["batch"] = batch_measure(a, cx, capi, dist)
+        if world == 1:
+            extra["configs"] = other_configs(a, cx, capi, rank, clocks)
 
     line = {"metric": METRIC, "value": world * 1000.0 / ms, "unit": "reconstructions/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -509,7 +516,7 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
             "roofline": dict(kernel_roofline(cx, capi, spec, w, w["kind"]), stencils=stencils),
             "clocks": clk, "gpu_launches": launches}
     line.update(extra)
-    if rank == 0 and world == 1 and name != "hemi3d":
+    if cpu and rank == 0 and world == 1 and name != "hemi3d":
         out = reference_solve(w)
         if out:
             secs, r = out
@@ -522,6 +529,49 @@ def run_single(a, cx, capi, name, world, rank, dist, clocks):
                                               + (f", relerr vs the FP64 anisotropic solution {err:.2e}"
                                                  if err is not None else "")}
     return line
+
+
+def other_configs(a, cx, capi, rank, clocks):
+    """Compact records of the other reference configurations, measured in the
+    default run on one GPU with their own workloads' shapes (two timed steps
+    each after at least three warm-up ones): the plain dense 64x64 solve, the
+    3D 128^3 hemisphere, the multi-RHS dense solve (joint and independent
+    right-hand sides) and the differentiable unrolled solve."""
+    import copy
+    b = copy.copy(a)
+    b.steps, b.warmup, b.maxit, b.side, b.sampling = 2, 3, None, 64, 0.3
+    b.no_batch, b.tune, b.profile, b.plain = True, False, False, False
+    keep = ("value", "unit", "ms_per_step", "iterations", "relerr_vs_fp64", "fp64_noise_floor", "reached_target",
+            "full_solve", "clocks")
+    out = {}
+    for name in ("dense2d", "hemi3d"):
+        t0 = time.perf_counter()
+        r = run_single(b, cx, capi, name, 1, rank, None, clocks, cpu=False)
+        rec = {k: r[k] for k in keep}
+        rec["workload"] = r["config"]["workload"]
+        rec["e2e"] = {k: r["e2e"][k] for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step")}
+        rl = r["roofline"]
+        rec["roofline"] = {k: rl.get(k) for k in ("bound", "kernel", "achieved", "peak", "unit", "frac",
+                                                   "ms_per_launch", "peak_source")}
+        rec["roofline"]["stencils"] = rl.get("stencils")
+        rec["wall_s"] = round(time.perf_counter() - t0, 1)
+        out["dense64" if name == "dense2d" else "hemi128"] = rec
+    t0 = time.perf_counter()
+    r = run_mrhs(b, cx, capi, 1, None, clocks)
+    out["mrhs"] = {k: r[k] for k in ("value", "unit", "ms_per_step", "iterations", "relerr_vs_fp64",
+                                     "relerr_per_rhs_max", "reached_target", "gemv_path", "tensor_over_gemv",
+                                     "independent", "clocks")}
+    out["mrhs"]["workload"] = r["config"]["workload"]
+    out["mrhs"]["roofline"] = {k: r["roofline"][k] for k in ("kernel", "achieved", "frac", "ms_per_launch",
+                                                              "tensor_tflops")}
+    out["mrhs"]["wall_s"] = round(time.perf_counter() - t0, 1)
+    t0 = time.perf_counter()
+    r = run_unrolled(b, cx, capi, 1, None, clocks)
+    out["unrolled"] = {k: r[k] for k in ("value", "unit", "ms_per_step", "forward_ms", "backward_ms", "loss",
+                                         "clocks")}
+    out["unrolled"]["workload"] = r["config"]["workload"]
+    out["unrolled"]["wall_s"] = round(time.perf_counter() - t0, 1)
+    return out
 
 
 def timed_plan(cx, capi, spec, opts, b, Ut=None, target=0.0, reps=3):
