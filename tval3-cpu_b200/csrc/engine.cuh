@@ -289,21 +289,25 @@ __device__ __forceinline__ long long cplx_index(const Inst &I, long long i, long
 }
 
 // Tiles: image vectors BLOCK x Inst::ept elements - one element per thread
-// for images of up to about 0.6M elements (a 256^2 image is 256 blocks), up
+// for images of up to about 0.3M elements (a 256^2 image is 256 blocks), up
 // to eight for large ones, so that a block's fixed costs (descriptor loads,
 // its tile sums, the ticket) are spread over more elements while the grid
-// still fills the GPU twice (ept_for); measurement vectors four elements per
+// still fills the GPU once (ept_for); measurement vectors four elements per
 // thread (their kernels do little per element, and fewer tiles contend less
 // for the instance's reduction ticket)
 constexpr int TILE = 256;   // n tile of ept 1
 constexpr int TILE_M = 1024;
 constexpr int BLOCK = 256;
 // elements per thread of the n tiles of an image of n elements: the largest
-// power of two up to 8 that leaves at least two waves of 4 blocks per SM on
-// 148 SMs
+// power of two up to 8 that leaves at least one wave of 4 blocks per SM on
+// 148 SMs.  Measured on the 128^3 hemisphere solve (the 20-launch stencil
+// timings, µs, and the solve, ms) for 1 / 2 / 4 / 8 / 16 / 32 elements per
+// thread: k_shrink_grad 142 / 101 / 83 / 74 / 72 / 120, k_getg 113 / 66 /
+// 55 / 54 / 55 / 88, solve 150.8 / 135.4 / 129.9 / 127.6 / 127.2 / 136.3:
+// the blocks' fixed costs outweigh the last wave's idle SMs up to 8
 inline int ept_for(long long n) {
 	int e = 1;
-	while (e < 8 && n >= 2LL * (2 * 148 * 4) * BLOCK * e) e *= 2;
+	while (e < 8 && n >= (148LL * 4) * BLOCK * (2 * e)) e *= 2;
 	return e;
 }
 constexpr int EPT_M = TILE_M / BLOCK;
