@@ -38,7 +38,9 @@ the reference's own stopping rules end it.
   configs the other reference configurations in compact records (one GPU
           only): the dense 64x64 solve, the 128^3 hemisphere, the multi-RHS
           solve (joint and independent right-hand sides) and the
-          differentiable unrolled solve, two timed steps each
+          differentiable unrolled solve, two timed steps each; and the
+          double-data path (tval3g_solve_f64) end to end on the ring and the
+          dense 64x64 problem against their FP64 solutions
 
 --workload dense2d | hemi3d | batch | mrhs | unrolled measures the plain dense
 64x64 problem, the 128^3 hemisphere, the mixed batch alone, the joint
@@ -571,6 +573,35 @@ def other_configs(a, cx, capi, rank, clocks):
                                          "clocks")}
     out["unrolled"]["workload"] = r["config"]["workload"]
     out["unrolled"]["wall_s"] = round(time.perf_counter() - t0, 1)
+    out["f64"] = f64_records(capi)
+    return out
+
+
+def f64_records(capi):
+    """The double-data path (tval3g_solve_f64, the FP64 build of the engine
+    behind the reference's double overloads) end to end on the ring and the
+    dense 64x64 workloads, host buffers, the reference's stopping rules: mean
+    wall time of three calls after one, iterations and relerr against the
+    FP64 oracle's solution (tests/golden)."""
+    out = {}
+    for name in ("ring2d", "dense2d"):
+        w = workload(name)
+        spec = capi.problem_from_workload(w)
+        vals = np.asarray(w["A"], np.float64) if w["kind"] == "dense" else None
+        b = np.asarray(w["b"], np.float64)
+        ref = fp64_reference(name)
+        capi.solve_f64(spec, b, w["opts"], values=vals)
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            U, info = capi.solve_f64(spec, b, w["opts"], values=vals)
+            ts.append((time.perf_counter() - t0) * 1000)
+        ms = float(np.mean(ts))
+        out["ring256" if name == "ring2d" else "dense64"] = {
+            "value": 1000.0 / ms, "unit": "reconstructions/s", "ms_per_call": ms, "iterations": info["total_iters"],
+            "fp64_oracle_iterations": int(ref["iters"][1]) if ref is not None else None,
+            "relerr_vs_fp64": rel_l2(U, ref["U"]) if ref is not None else None,
+            "what": "tval3g_solve_f64 with host buffers (operator preparation included), double storage"}
     return out
 
 
