@@ -196,7 +196,9 @@ struct OpDev {
 	// short ones fill the SMs that finish early.
 	int tiled;
 	int tile3;              // 3D: tiles are bricks of 8 x 8 x 4 voxels (x, y, z), ntx x nty per z layer
-	int ntiles;             // tiles (bricks) of the tiled adjoint
+	int ntiles;             // blocks of the tiled adjoint's launch
+	int tfull;              // tiles crossed by rays: torder[0 .. tfull) one block each; the rest,
+	int tcount;             // up to torder[tcount), no ray crosses (zeros, RAYT_ZERO_TILES a block)
 	int nty;
 	int ntx;
 	int tmax;               // longest tile list

@@ -749,6 +749,7 @@ constexpr int RAYT_RING_BYTES = RAYT_ADJ_WARPS * RAYT_STAGES * RAYT_STAGE_WORDS 
 constexpr int RAYT_BAR_BYTES = (RAYT_ADJ_WARPS * RAYT_STAGES + 2) * 8;   // the rings' barriers, the list's
 constexpr int RAYT_SACC_BYTES = RAYT_THREADS * 8;        // the second halves' sums
 constexpr int RAYT_LIST_CHUNK = 8192;                    // list entries per bulk copy
+constexpr int RAYT_ZERO_TILES = 64;                      // tiles without rays zeroed per block
 
 // ring, barriers, second-half sums, then the tile's measurements: slot 0
 // (the zero pad entries read) sits 12 bytes past a 16-byte boundary so that
@@ -774,12 +775,37 @@ __device__ __forceinline__ float word_sum(const float *yt, uint4 q) {
 // pixels in order of decreasing hit count (OpDev::tperm), so a warp's pixels
 // have lists of nearly one length and its words carry little padding.
 // Deterministic, no atomics.
+// g at pixel px (0 .. RAYT^2 - 1, row-major in the tile) of tile (brick) t
+__device__ __forceinline__ void tiled_store(const Inst &I, const OpDev &op, VecSel ys, int t, int px, float v) {
+	if (op.tile3) {   // brick of BRICK_X x BRICK_Y x BRICK_Z voxels
+		const int bxy = op.ntx * op.nty;
+		const int x = (t % op.ntx) * BRICK_X + px % BRICK_X;
+		const int y = ((t % bxy) / op.ntx) * BRICK_Y + (px / BRICK_X) % BRICK_Y;
+		const int z = (t / bxy) * BRICK_Z + px / (BRICK_X * BRICK_Y);
+		if (x < op.rvx && y < op.rvy && (long long)z * op.rvx * op.rvy < I.n)
+			vselw(I, ys)[x + (long long)y * op.rvx + (long long)z * op.rvx * op.rvy] = v;
+		return;
+	}
+	const int x = (t % op.ntx) * RAYT + (px % RAYT), row = (t / op.ntx) * RAYT + (px / RAYT);
+	if (x < op.rvx && row < op.tH) vselw(I, ys)[x + row * op.rvx] = v;
+}
+
 __global__ void __launch_bounds__(RAYT_ADJ_THREADS) k_ray_adj_tiled(const Inst *tab, TileMap map, int pred,
                                                                     VecSel xs, VecSel ys, int *err,
                                                                     unsigned long long *launches) {
 	OPROLOGUE();
 	extern __shared__ __align__(128) unsigned char smem[];
 	const OpDev &op = I.op;
+	if (local >= op.tfull) {
+		// tiles that no ray crosses (the launch order ends with them): zeros,
+		// RAYT_ZERO_TILES tiles per block, none of the list or ring machinery
+		const long long e0 = op.tfull + (local - op.tfull) * RAYT_ZERO_TILES;
+		const long long e1 = min(e0 + RAYT_ZERO_TILES, (long long)op.tcount);
+		const float zero = (float)(0.0 * op.scale);   // the bits a block of this tile would write
+		for (long long e = e0 + threadIdx.x / RAYT_THREADS; e < e1; e += RAYT_ADJ_THREADS / RAYT_THREADS)
+			tiled_store(I, op, ys, __ldg(op.torder + e), threadIdx.x % RAYT_THREADS, zero);
+		return;
+	}
 	const int t = __ldg(op.torder + local);
 	const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int pw = wid % RAYT_WARPS, half = wid / RAYT_WARPS;   // pixel-warp, which half of its words
@@ -866,17 +892,7 @@ __global__ void __launch_bounds__(RAYT_ADJ_THREADS) k_ray_adj_tiled(const Inst *
 	if (half || !good) return;
 	acc += sacc[pw * 32 + lane];   // first half + second half
 	const int px = __ldg(op.tperm + (long long)t * RAYT_THREADS + threadIdx.x);   // this thread's pixel of the tile
-	if (op.tile3) {   // brick of BRICK_X x BRICK_Y x BRICK_Z voxels
-		const int bxy = op.ntx * op.nty;
-		const int x = (t % op.ntx) * BRICK_X + px % BRICK_X;
-		const int y = ((t % bxy) / op.ntx) * BRICK_Y + (px / BRICK_X) % BRICK_Y;
-		const int z = (t / bxy) * BRICK_Z + px / (BRICK_X * BRICK_Y);
-		if (x < op.rvx && y < op.rvy && (long long)z * op.rvx * op.rvy < I.n)
-			vselw(I, ys)[x + (long long)y * op.rvx + (long long)z * op.rvx * op.rvy] = (float)(acc * op.scale);
-		return;
-	}
-	const int x = (t % op.ntx) * RAYT + (px % RAYT), row = (t / op.ntx) * RAYT + (px / RAYT);
-	if (x < op.rvx && row < op.tH) vselw(I, ys)[x + row * op.rvx] = (float)(acc * op.scale);
+	tiled_store(I, op, ys, t, px, (float)(acc * op.scale));
 }
 
 // --- index builder (once per operator) ---------------------------------------
@@ -1089,7 +1105,11 @@ bool build_tiled_index(cudaStream_t s, int ld, int H, int nrays, const int *cptr
 		d.tiled = 1;
 		d.ntx = ntx;
 		d.nty = nty;
-		d.ntiles = nt;
+		int full = 0;   // tiles with rays come first in the order
+		while (full < nt && h_tptr[order[full] + 1] > h_tptr[order[full]]) full++;
+		d.tfull = full;
+		d.tcount = nt;
+		d.ntiles = full + (nt - full + RAYT_ZERO_TILES - 1) / RAYT_ZERO_TILES;
 		d.tmax = (int)tmax;
 		d.tptr = tptr32; d.tmeas = tmeas; d.woff = woff32; d.sidx = sidx; d.tperm = perm;
 		owned.push_back(perm);
@@ -1324,7 +1344,11 @@ bool build_brick_words(cudaStream_t s, int rvx, int rvy, int rvz, const int *cpt
 		d.tile3 = 1;
 		d.ntx = bl.nbx;
 		d.nty = bl.nby;
-		d.ntiles = nb;
+		int full = 0;   // bricks with rays come first in the order
+		while (full < nb && bl.h_tptr[order[full] + 1] > bl.h_tptr[order[full]]) full++;
+		d.tfull = full;
+		d.tcount = nb;
+		d.ntiles = full + (nb - full + RAYT_ZERO_TILES - 1) / RAYT_ZERO_TILES;
 		d.tmax = (int)bl.tmax;
 		d.tptr = bl.tptr; d.tmeas = bl.tmeas; d.woff = woff32; d.sidx = sidx; d.tperm = perm; d.torder = torder;
 		*bytes = (long long)sizeof(uint4) * words + (long long)sizeof(int) * (bl.h_tptr[nb] + 2 * (long long)nb + nw + 2) +
