@@ -799,10 +799,12 @@ __global__ void __launch_bounds__(RAYT_ADJ_THREADS) k_ray_adj_tiled(const Inst *
 	if (local >= op.tfull) {
 		// tiles that no ray crosses (the launch order ends with them): zeros,
 		// RAYT_ZERO_TILES tiles per block, none of the list or ring machinery
-		const long long e0 = op.tfull + (local - op.tfull) * RAYT_ZERO_TILES;
-		const long long e1 = min(e0 + RAYT_ZERO_TILES, (long long)op.tcount);
+		// (32-bit indices: tile counts stay below 2^24, and 64-bit ones here
+		// cost the whole kernel eight registers)
+		const int e0 = op.tfull + ((int)local - op.tfull) * RAYT_ZERO_TILES;
+		const int e1 = min(e0 + RAYT_ZERO_TILES, op.tcount);
 		const float zero = (float)(0.0 * op.scale);   // the bits a block of this tile would write
-		for (long long e = e0 + threadIdx.x / RAYT_THREADS; e < e1; e += RAYT_ADJ_THREADS / RAYT_THREADS)
+		for (int e = e0 + (int)threadIdx.x / RAYT_THREADS; e < e1; e += RAYT_ADJ_THREADS / RAYT_THREADS)
 			tiled_store(I, op, ys, __ldg(op.torder + e), threadIdx.x % RAYT_THREADS, zero);
 		return;
 	}
