@@ -85,6 +85,35 @@ def test_3d_argument_errors():
     assert str(e.value) == "Argument error: the length of U must be equal to A.dim_x!"
 
 
+def test_f64_argument_errors_match_reference():
+    """The double-data entry point validates like the float one (the
+    reference's messages, before any device work)."""
+    spec = _dense_spec()
+    A64 = np.zeros((5, 16), np.float64)
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve_f64(spec, np.zeros(6), _opts(), values=A64)
+    assert e.value.code == capi.ERR_ARGUMENT
+    assert str(e.value) == "Argument error: b.len must be equal to A.dim_y * layers!"
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve_f64(spec, np.zeros(5), _opts(), Ut=np.zeros(7), values=A64)
+    assert str(e.value) == "Argument error: U and Ut must have the same size!"
+    with pytest.raises(capi.TVAL3Error) as e:   # the float A of the spec is not read
+        capi.solve_f64(spec, np.zeros(5), _opts(), values=None)
+    assert str(e.value) == "Argument error: A is NULL"
+
+
+def test_f64_no_device_is_an_error_not_a_fallback():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    with pytest.raises(capi.TVAL3Error) as e:
+        capi.solve_f64(_dense_spec(), np.zeros(5), _opts(), values=np.zeros((5, 16)))
+    assert e.value.code in (capi.ERR_NO_DEVICE, capi.ERR_CUDA)
+
+
 def test_no_device_is_an_error_not_a_fallback():
     try:
         import torch
