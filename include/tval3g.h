@@ -167,7 +167,7 @@ int tval3g_solve(const tval3g_problem *prob, const float *b, int b_len, const tv
  * engine (double vectors, double operator values and products, double
  * stencils and shrinkage; the same kernels' algorithm as tval3g_solve, with
  * the pixel-major gather adjoint for ray operators and the gemv kernels for
- * dense ones).  prob describes the problem as for tval3g_solve except that
+ * dense ones; the autotuner, TVAL3G_TUNE, does not apply).  prob describes the problem as for tval3g_solve except that
  * its float arrays A and csr_val are not read: A64 holds the dense matrix
  * (DENSE: m x n_cols row-major) or the CSR values (CSR: nnz of them), and is
  * NULL for ray geometries; b (b_len), Ut (ut_len: 0 or n; may be NULL) and U
